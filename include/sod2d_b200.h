@@ -1,0 +1,197 @@
+/*
+ * sod2d_b200 — B200-native (sm_100a) explicit spectral-element RHS of SOD2D, C ABI.
+ *
+ * Scope: the compressible Navier–Stokes right-hand side on HEX64 (p=3) elements with GLL
+ * collocation (convection in skew-symmetric split form, viscous/heat/artificial diffusion,
+ * entropy residual and entropy viscosity), the lumped-mass RK4 step that drives it, and the
+ * incompressible pressure-Poisson PCG.  Every entry point below replaces one reference routine
+ * or one reference call site, cited as file:line of the SOD2D sources.
+ *
+ * Conventions shared by all entry points:
+ *  - Arrays keep the reference's Fortran column-major layouts (connec(nelem,nnode),
+ *    He(ndime,ndime,ngaus,nelem), u(npoin,ndime), mu_e(nelem,ngaus) ...).  Node ids in
+ *    connec and lpoin-style arrays are 1-based when index_base == 1 (Fortran callers) and
+ *    0-based when index_base == 0.
+ *  - "dev" pointers are device pointers (cudaMalloc / OpenACC deviceptr / torch tensors);
+ *    "host" pointers are host memory (pageable or pinned).
+ *  - Every function returns SOD_OK or a negative SOD_ERR_* code; sod_last_error() returns a
+ *    thread-local message for the last failure.  Nothing aborts the process.
+ *  - Work is stream-ordered on the cudaStream_t passed in (0 = legacy default stream).  A
+ *    SodMesh handle must be used by one host thread at a time.
+ *  - The precision argument selects SOD_FP64 (all arithmetic in FP64) or SOD_MIXED
+ *    (element-local derivative and flux arithmetic in FP32 on deviation fields; nodal
+ *    assembly, RK state, lumped mass and reductions in FP64).
+ */
+#ifndef SOD2D_B200_H
+#define SOD2D_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef void* sod_stream_t; /* a cudaStream_t */
+
+enum {
+  SOD_OK = 0,
+  SOD_ERR_ARG = -1,           /* invalid argument (null pointer, bad size, bad layout)       */
+  SOD_ERR_CUDA = -2,          /* a CUDA runtime call failed                                  */
+  SOD_ERR_NONFINITE = -3,     /* a NaN/Inf was detected in the state or residual             */
+  SOD_ERR_NOT_CONVERGED = -4, /* CG reached max_iter before the tolerance                    */
+  SOD_ERR_TIMEOUT = -5,       /* a bounded host wait on device work expired                  */
+  SOD_ERR_NOMEM = -6,         /* device allocation failed                                    */
+  SOD_ERR_UNSUPPORTED = -7    /* option outside the implemented path (p != 3, LES ...)        */
+};
+
+typedef enum { SOD_FP64 = 0, SOD_MIXED = 1 } SodPrecision;
+
+/* Physical and numerical parameters.  Defaults (sod_params_default) reproduce
+ * mod_numerical_params.f90:8-99 and the TGV case of TGVSolver.f90:77-103. */
+typedef struct {
+  double gamma_gas;             /* TGVSolver.f90:92                                       */
+  double Rgas;                  /* TGVSolver.f90:95, also nscbc_Rgas_inf (:102)           */
+  double Cp;                    /* TGVSolver.f90:87                                       */
+  double Prt;                   /* TGVSolver.f90:88                                       */
+  double ce, cmax, cglob;       /* mod_numerical_params.f90:24-26                         */
+  double c_rho, c_ener;         /* mod_numerical_params.f90:27-28                         */
+  int32_t flag_normalise_entropy; /* mod_numerical_params.f90:23                          */
+  double cfl_conv, cfl_diff;    /* CFDSolverBase cfl_conv / cfl_diff                      */
+} SodParams;
+
+void sod_params_default(SodParams* p);
+
+/* Mesh description handed to sod_mesh_create.  All arrays host, Fortran layouts.  The
+ * geometry arrays (He, gpvol, Ml, helem, helem_l) are optional: when null they are computed
+ * on the device from coord_orig/connec_orig exactly as the reference's setup does
+ * (elem_jacobian jacobian_oper.f90:9-138, lumped_mass_spectral mass_matrix.f90:11-43,
+ * char_length mod_geom.f90:13-37, char_length_spectral mod_geom.f90:39-66). */
+typedef struct {
+  int32_t nelem;             /* elements                                                 */
+  int32_t npoin;             /* working (unique) nodes: rows of the state arrays         */
+  int32_t npoin_orig;        /* rows of coord_orig (nodes incl. periodic images)         */
+  int32_t porder;            /* must be 3                                                */
+  int32_t index_base;        /* 0 or 1                                                   */
+  const int32_t* connec;     /* (nelem,64) connecParWork: unique node ids                */
+  const int32_t* connec_orig;/* (nelem,64) connecParOrig: ids into coord_orig (optional) */
+  const double* coord_orig;  /* (npoin_orig,3) (optional if geometry is given)           */
+  const double* dlxigp_ip;   /* (64,3,4) 1-D Lagrange derivative table                   */
+  const double* wgp;         /* (64) GLL weights                                          */
+  const int32_t* invAtoIJK;  /* (4,4,4) local node of sod2d (i,j,k), index_base applies  */
+  const int32_t* gmshAtoI;   /* (64) sod2d i of local node (1..4 or 0..3 by index_base)  */
+  const int32_t* gmshAtoJ;
+  const int32_t* gmshAtoK;
+  const double* He;          /* (3,3,64,nelem) optional                                  */
+  const double* gpvol;       /* (1,64,nelem)   optional                                  */
+  const double* Ml;          /* (npoin)        optional                                  */
+  const double* helem;       /* (nelem)        optional                                  */
+  const double* helem_l;     /* (nelem,64)     optional                                  */
+} SodMeshDesc;
+
+typedef struct SodMesh SodMesh;
+
+/* Upload a mesh, build the deterministic node->(element, local node) CSR gather map and the
+ * device geometry.  Replaces the setup calls of CFDSolverBase_run (CFDSolverBase.f90:2115-2233:
+ * evalJacobians :1280-1317, evalMass :1364-1389, evalCharLength :783-800) and the
+ * `!$acc enter data` residency of init_rk4_solver (time_integ.f90:31-95). */
+int sod_mesh_create(const SodMeshDesc* desc, const SodParams* params, SodMesh** out);
+void sod_mesh_destroy(SodMesh* mesh);
+/* Copy the device geometry back in the reference layouts (any pointer may be null). */
+int sod_mesh_get_geometry(SodMesh* mesh, double* He, double* gpvol, double* Ml, double* helem,
+                          double* helem_l);
+int sod_mesh_set_params(SodMesh* mesh, const SodParams* params);
+
+/* Device-resident solver state in the reference's array layouts (level pos=2 only).
+ * Every pointer is a device pointer owned by the caller. */
+typedef struct {
+  double* rho;      /* (npoin)    */
+  double* q;        /* (npoin,3)  */
+  double* E;        /* (npoin)    total energy rho*E */
+  double* u;        /* (npoin,3)  output of the EOS update */
+  double* pr;       /* (npoin)    */
+  double* Tem;      /* (npoin)    */
+  double* e_int;    /* (npoin)    */
+  double* eta;      /* (npoin)    */
+  double* csound;   /* (npoin)    */
+  double* machno;   /* (npoin)    */
+  double* mu_fluid; /* (npoin)    */
+  double* mu_factor;/* (npoin)    input */
+  double* mu_e;     /* (nelem,64) in: frozen entropy viscosity; out: updated */
+  double* Reta;     /* (npoin)    out: -sum b_i Reta_i (time_integ.f90:467-471), may be null */
+} SodState;
+
+/* One explicit RK4 step: rk_4_main (time_integ.f90:137-508) on the periodic compressible
+ * path (noBoundaries, flag_les=0, flag_total_enthalpy=.false., Sutherland on).  dt is read
+ * from dt_dev (device double) so that a captured step needs no host value; when
+ * update_dt != 0 the next dt from adapt_dt_cfl (mod_time_ops.f90:11-61) is written back to
+ * dt_dev after the step (CFDSolverBase.f90:1592). */
+int sod_rk4_main(SodMesh* mesh, SodState* state, const double* dt_dev, double* dt_next_dev,
+                 SodPrecision prec, sod_stream_t stream);
+
+/* nsteps steps of sod_rk4_main captured once into a CUDA graph per (mesh, state, precision)
+ * and replayed; dt evolves on the device.  Returns after enqueueing. */
+int sod_rk4_steps(SodMesh* mesh, SodState* state, double* dt_dev, int nsteps, SodPrecision prec,
+                  sod_stream_t stream);
+
+/* Host-buffer variant of sod_rk4_main for the CPU-side drop-in (the reference's CPU build
+ * calls rk_4_main on host arrays): copies rho,q,E,mu_e,mu_factor in, runs one step and copies
+ * rho,q,E,u,pr,Tem,e_int,eta,csound,machno,mu_fluid,mu_e back.  dt_host in, dt_next_host out. */
+int sod_rk4_main_host(SodMesh* mesh, SodState* host_state, double dt_host, double* dt_next_host,
+                      SodPrecision prec, sod_stream_t stream);
+
+/* Full RHS of one stage at a given conserved state, lumped-mass solved: what rk_4_main's
+ * stage loop forms at time_integ.f90:266-393 (EOS, generic_scalar_convec_ijk, Sutherland,
+ * full_diffusion_ijk, full_convec_ijk, sum, /Ml).  Outputs (npoin) / (npoin,3) device arrays. */
+int sod_rhs(SodMesh* mesh, const double* rho, const double* q, const double* E,
+            const double* mu_e, const double* mu_factor, double* Rmass, double* Rmom,
+            double* Rener, double* Reta, SodPrecision prec, sod_stream_t stream);
+
+/* smart_visc_spectral (mod_entropy_viscosity.f90:14-123) incl. the global entropy
+ * normalisation and the convertIJK 3x3x3 filter (mod_filters.f90:15-55). */
+int sod_smart_visc_spectral(SodMesh* mesh, const double* Reta, const double* rho, const double* u,
+                            const double* csound, const double* Tem, const double* eta,
+                            double* mu_e, sod_stream_t stream);
+
+/* adapt_dt_cfl (mod_time_ops.f90:11-61) with both limits; result written to dt_dev. */
+int sod_adapt_dt_cfl(SodMesh* mesh, const double* u, const double* csound, const double* mu_fluid,
+                     const double* mu_sgs, const double* rho, double* dt_dev, sod_stream_t stream);
+
+/* ---- Per-routine entry points with the reference argument lists (device arrays) -------- */
+
+/* full_convec_ijk (elem_convec.f90:211-460); E is the energy-like field the caller passes
+ * (enthalpy h in rk_4_main, time_integ.f90:364).  Outputs are overwritten. */
+int sod_full_convec_ijk(SodMesh* mesh, const double* u, const double* q, const double* rho,
+                        const double* pr, const double* E, double* Rmass, double* Rmom,
+                        double* Rener, sod_stream_t stream);
+/* generic_scalar_convec_ijk (elem_convec.f90:462-570). */
+int sod_generic_scalar_convec_ijk(SodMesh* mesh, const double* q, const double* eta,
+                                  const double* u, double* Rconvec, sod_stream_t stream);
+/* full_diffusion_ijk (elem_diffu.f90:12-198); mu_sgs may be null (zero). */
+int sod_full_diffusion_ijk(SodMesh* mesh, double Cp, double Pr, const double* rho_n,
+                           const double* rho, const double* u, const double* Tem,
+                           const double* mu_fluid, const double* mu_e, const double* mu_sgs,
+                           double* Rmass, double* Rmom, double* Rener, sod_stream_t stream);
+/* lumped_solver_scal / lumped_solver_vect (mod_solver.f90:23-58): R(:,c) /= Ml, ncomp 1 or 3. */
+int sod_lumped_solver(SodMesh* mesh, double* R, int ncomp, sod_stream_t stream);
+/* sutherland_viscosity (mod_fluid_viscosity.f90:21-41). */
+int sod_sutherland_viscosity(int32_t npoin, const double* Tem, const double* mu_factor,
+                             double* mu_fluid, sod_stream_t stream);
+
+/* ---- Legacy unit-test API ----------------------------------------------------------- */
+
+/* CSR_SpMV_scal (legacy API pinned by unitt/unitt_CSR_SPMV_scal/unitt_CSR_SPMV_scal.f90:14-52):
+ * u = Mc v, rdom 0-based row offsets (npoin+1), cdom 1-based columns.  Device arrays. */
+int sod_csr_spmv_scal(int32_t npoin, int32_t nzdom, const int32_t* rdom, const int32_t* cdom,
+                      const double* Mc, const double* v, double* u, sod_stream_t stream);
+
+/* ---- Diagnostics ------------------------------------------------------------------------ */
+const char* sod_last_error(void);
+const char* sod_version(void);
+/* Number of kernels this library enqueued since load (for launch accounting). */
+int64_t sod_launch_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SOD2D_B200_H */

@@ -1,0 +1,224 @@
+"""ctypes wrapper of the CPU oracle (test infrastructure; see sod2d_oracle.hpp).
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline legs import this module.
+It never backs the product path: the library in sod2d_refmap_b200 has no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liboracle_sod2d.so")
+
+_p = C.c_void_p
+_i32p = C.POINTER(C.c_int32)
+
+
+class ElemCtx(C.Structure):
+    _fields_ = [("nelem", C.c_int), ("npoin", C.c_int), ("connec", _p), ("He", _p), ("gpvol", _p),
+                ("dlxigp_ip", _p), ("invAtoIJK", _p), ("gmshAtoI", _p), ("gmshAtoJ", _p),
+                ("gmshAtoK", _p), ("ncolors", C.c_int), ("color_ptr", _p), ("color_elems", _p)]
+
+
+class Params(C.Structure):
+    _fields_ = [("gamma_gas", C.c_double), ("Rgas", C.c_double), ("Cp", C.c_double), ("Prt", C.c_double),
+                ("ce", C.c_double), ("cmax", C.c_double), ("cglob", C.c_double), ("c_rho", C.c_double),
+                ("c_ener", C.c_double), ("flag_normalise_entropy", C.c_int), ("cfl_conv", C.c_double),
+                ("cfl_diff", C.c_double)]
+
+
+class State(C.Structure):
+    _fields_ = [(n, _p) for n in ("rho", "u", "q", "pr", "E", "Tem", "e_int", "eta", "csound", "machno",
+                                  "mu_fluid", "mu_e", "mu_sgs", "mue_l")]
+
+
+class StageCapture(C.Structure):
+    _fields_ = [("Rmass", _p), ("Rmom", _p), ("Rener", _p), ("Reta", _p), ("stage", C.c_int)]
+
+
+def build() -> str:
+    """Compile the oracle with its Makefile (idempotent)."""
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+    return LIB_PATH
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = C.CDLL(LIB_PATH)
+        L.oracle_adapt_dt_cfl.restype = C.c_double
+        L.oracle_set_threads.restype = C.c_int
+        L.oracle_conjgrad_pressure.restype = C.c_int
+        L.oracle_rk_4_main.argtypes = [C.POINTER(ElemCtx), C.POINTER(Params), _p, _p, _p, _p, _p, _p,
+                                       C.c_double, C.c_int, C.POINTER(State), C.POINTER(StageCapture)]
+        L.oracle_adapt_dt_cfl.argtypes = [C.POINTER(ElemCtx), _p, _p, _p, C.c_double, C.c_double, _p, _p, _p]
+        L.oracle_conjgrad_pressure.argtypes = [C.POINTER(ElemCtx), _p, _p, _p, C.c_int, C.c_double,
+                                               C.POINTER(C.c_double)]
+        _lib = L
+    return _lib
+
+
+def ptr(a: np.ndarray):
+    return C.c_void_p(a.ctypes.data)
+
+
+def set_threads(n: int) -> int:
+    return lib().oracle_set_threads(int(n))
+
+
+def box_colouring(n: int):
+    """Colour classes of an n^3 periodic box such that elements of one class share no node."""
+    e = np.arange(n ** 3, dtype=np.int64)
+    ex, ey, ez = e % n, (e // n) % n, e // (n * n)
+
+    def cl(v):
+        c = v % 2
+        if n % 2 == 1:
+            c = np.where(v == n - 1, 2, c)
+        return c
+
+    col = cl(ex) + 3 * (cl(ey) + 3 * cl(ez))
+    order = np.argsort(col, kind="stable").astype(np.int32)
+    counts = np.bincount(col, minlength=27)
+    ptrs = np.concatenate([[0], np.cumsum(counts)]).astype(np.int32)
+    return ptrs, order
+
+
+class OracleMesh:
+    """Holds a BoxMesh's arrays and the oracle's geometry (He, gpvol, Ml, helem, helem_l)."""
+
+    def __init__(self, mesh, colour: bool = True):
+        L = lib()
+        T = mesh.tables
+        self.mesh = mesh
+        self.nelem, self.npoin = mesh.nelem, mesh.npoin
+        # shape tables restated by the oracle itself (checked against the product's in tests)
+        self.xgp = np.zeros((64, 3), order="F"); self.wgp = np.zeros(64)
+        self.Ngp = np.zeros((64, 64), order="F"); self.dNgp = np.zeros((3, 64, 64), order="F")
+        self.dlxigp_ip = np.zeros((64, 3, 4), order="F")
+        self.invAtoIJK = np.zeros((4, 4, 4), np.int32, order="F")
+        self.gI = np.zeros(64, np.int32); self.gJ = np.zeros(64, np.int32); self.gK = np.zeros(64, np.int32)
+        atoIJK = np.ascontiguousarray(T.atoIJK, dtype=np.int32)
+        L.oracle_shape_tables(ptr(atoIJK), ptr(self.xgp), ptr(self.wgp), ptr(self.Ngp), ptr(self.dNgp),
+                              ptr(self.dlxigp_ip), ptr(self.invAtoIJK), ptr(self.gI), ptr(self.gJ), ptr(self.gK))
+        self.connec = np.asfortranarray(mesh.connec, dtype=np.int32)
+        self.connec_orig = np.asfortranarray(mesh.connec_orig, dtype=np.int32)
+        self.He = np.zeros((3, 3, 64, self.nelem), order="F")
+        self.gpvol = np.zeros((1, 64, self.nelem), order="F")
+        L.oracle_elem_jacobian(self.nelem, mesh.npoin_orig, ptr(self.connec_orig), ptr(mesh.coord_orig),
+                               ptr(self.dNgp), ptr(self.wgp), ptr(self.gpvol), ptr(self.He))
+        self.Ml = np.zeros(self.npoin)
+        L.oracle_lumped_mass(self.nelem, self.npoin, ptr(self.connec), ptr(self.gpvol), ptr(self.Ml))
+        self.helem = np.zeros(self.nelem)
+        L.oracle_char_length(self.nelem, mesh.npoin_orig, ptr(self.connec_orig), ptr(mesh.coord_orig), ptr(self.helem))
+        self.helem_l = np.zeros((self.nelem, 64), order="F")
+        L.oracle_char_length_spectral(self.nelem, mesh.npoin_orig, ptr(self.connec_orig), ptr(mesh.coord_orig),
+                                      ptr(self.helem_l))
+        if colour:
+            self.cptr, self.celems = box_colouring(mesh.n)
+            ncol = len(self.cptr) - 1
+        else:
+            self.cptr, self.celems = np.zeros(1, np.int32), np.zeros(1, np.int32)
+            ncol = 0
+        self.ctx = ElemCtx(self.nelem, self.npoin, ptr(self.connec).value, ptr(self.He).value,
+                           ptr(self.gpvol).value, ptr(self.dlxigp_ip).value, ptr(self.invAtoIJK).value,
+                           ptr(self.gI).value, ptr(self.gJ).value, ptr(self.gK).value, ncol,
+                           ptr(self.cptr).value, ptr(self.celems).value)
+
+
+def params_of(prm) -> Params:
+    return Params(prm.gamma_gas, prm.Rgas, prm.Cp, prm.Prt, prm.ce, prm.cmax, prm.cglob, prm.c_rho,
+                  prm.c_ener, int(prm.flag_normalise_entropy), prm.cfl_conv, prm.cfl_diff)
+
+
+def adapt_dt(om: OracleMesh, st, prm) -> float:
+    return lib().oracle_adapt_dt_cfl(C.byref(om.ctx), ptr(om.helem), ptr(st.u), ptr(st.csound), prm.cfl_conv,
+                                     prm.cfl_diff, ptr(st.mu_fluid), ptr(st.mu_sgs), ptr(st.rho))
+
+
+def rk4(om: OracleMesh, prm, st, dt: float, nsteps: int = 1, capture_stage: int = 0):
+    """Runs nsteps rk_4_main steps in place on st (a FlowState).  Returns the stage residuals of
+    capture_stage (1..4) of the first step when requested."""
+    P = params_of(prm)
+    mue_l = np.zeros((om.nelem, 64), order="F")
+    S = State(*(ptr(a).value for a in (st.rho, st.u, st.q, st.pr, st.E, st.Tem, st.e_int, st.eta, st.csound,
+                                       st.machno, st.mu_fluid, st.mu_e, st.mu_sgs, mue_l)))
+    cap = None
+    out = None
+    if capture_stage:
+        out = dict(Rmass=np.zeros(om.npoin), Rmom=np.zeros((om.npoin, 3), order="F"), Rener=np.zeros(om.npoin),
+                   Reta=np.zeros(om.npoin))
+        cap = StageCapture(ptr(out["Rmass"]).value, ptr(out["Rmom"]).value, ptr(out["Rener"]).value,
+                           ptr(out["Reta"]).value, int(capture_stage))
+    lib().oracle_rk_4_main(C.byref(om.ctx), C.byref(P), ptr(om.Ml), ptr(st.mu_factor), ptr(om.gpvol), ptr(om.wgp),
+                           ptr(om.helem), ptr(om.helem_l), float(dt), int(nsteps), C.byref(S),
+                           C.byref(cap) if cap is not None else None)
+    return out
+
+
+def convec(om: OracleMesh, u, q, rho, pr, E):
+    Rm = np.zeros(om.npoin); Rmo = np.zeros((om.npoin, 3), order="F"); Re = np.zeros(om.npoin)
+    lib().oracle_full_convec_ijk(C.byref(om.ctx), ptr(u), ptr(q), ptr(rho), ptr(pr), ptr(E), ptr(Rm), ptr(Rmo), ptr(Re))
+    return Rm, Rmo, Re
+
+
+def scalar_convec(om: OracleMesh, f, eta, u):
+    R = np.zeros(om.npoin)
+    lib().oracle_generic_scalar_convec_ijk(C.byref(om.ctx), ptr(f), ptr(eta), ptr(u), ptr(R))
+    return R
+
+
+def diffusion(om: OracleMesh, prm, rho_n, rho, u, Tem, mu_fluid, mu_e, mu_sgs):
+    P = params_of(prm)
+    Rm = np.zeros(om.npoin); Rmo = np.zeros((om.npoin, 3), order="F"); Re = np.zeros(om.npoin)
+    lib().oracle_full_diffusion_ijk(C.byref(om.ctx), C.byref(P), ptr(rho_n), ptr(rho), ptr(u), ptr(Tem),
+                                    ptr(mu_fluid), ptr(mu_e), ptr(mu_sgs), ptr(Rm), ptr(Rmo), ptr(Re))
+    return Rm, Rmo, Re
+
+
+def smart_visc(om: OracleMesh, prm, Reta, rho, u, csound, Tem, eta, mu_e_in):
+    P = params_of(prm)
+    mu_e = np.array(mu_e_in, order="F", copy=True)
+    mue_l = np.zeros((om.nelem, 64), order="F")
+    lib().oracle_smart_visc_spectral(C.byref(om.ctx), C.byref(P), ptr(Reta), ptr(om.gpvol), ptr(om.wgp), ptr(rho),
+                                     ptr(u), ptr(csound), ptr(Tem), ptr(eta), ptr(om.helem_l), ptr(om.helem),
+                                     ptr(mu_e), ptr(mue_l))
+    return mu_e
+
+
+def laplacian_mult(om: OracleMesh, p):
+    out = np.zeros(om.npoin)
+    lib().oracle_eval_laplacian_mult(C.byref(om.ctx), ptr(np.ascontiguousarray(p)), ptr(out))
+    return out
+
+
+def laplacian_diag(om: OracleMesh):
+    d = np.zeros(om.npoin)
+    lib().oracle_eval_laplacian_diag(C.byref(om.ctx), ptr(om.dNgp), ptr(d))
+    return d
+
+
+def conjgrad_pressure(om: OracleMesh, rhs, x0=None, max_iter: int = 10000, tol: float = 1e-10):
+    R = np.array(rhs, dtype=np.float64, copy=True)
+    Rp0 = np.zeros(om.npoin) if x0 is None else np.ascontiguousarray(x0, dtype=np.float64)
+    rel = C.c_double(0.0)
+    it = lib().oracle_conjgrad_pressure(C.byref(om.ctx), ptr(om.dNgp), ptr(Rp0), ptr(R), int(max_iter),
+                                        float(tol), C.byref(rel))
+    return R, it, rel.value
+
+
+def csr_spmv_scal(rdom, cdom, Mc, v):
+    rdom = np.ascontiguousarray(rdom, np.int32); cdom = np.ascontiguousarray(cdom, np.int32)
+    Mc = np.ascontiguousarray(Mc, np.float64); v = np.ascontiguousarray(v, np.float64)
+    u = np.zeros(len(rdom) - 1)
+    lib().oracle_csr_spmv_scal(len(u), len(Mc), ptr(rdom), ptr(cdom), ptr(Mc), ptr(v), ptr(u))
+    return u

@@ -1,0 +1,133 @@
+// CPU ORACLE C API — test infrastructure only (see sod2d_oracle.hpp).  Loaded by tests/,
+// __graft_entry__.smoke() and bench.py's CPU-baseline legs through oracle/oracle.py.
+#include "sod2d_oracle.hpp"
+
+using namespace sod_oracle;
+
+extern "C" {
+
+int oracle_set_threads(int n) {
+#ifdef _OPENMP
+  if (n > 0) omp_set_num_threads(n);
+  return omp_get_max_threads();
+#else
+  (void)n;
+  return 1;
+#endif
+}
+
+void oracle_gll(int p, double* xi, double* w) {
+  double vn[32];
+  zelegl(p, xi, vn);
+  welegl(p, xi, vn, w);
+}
+
+void oracle_lagrange(const double* xi, double xp, double* l, double* dl) {
+  eval_lagrange<double>(xi, xp, l);
+  eval_lagrange_deriv<double>(xi, xp, dl);
+}
+
+void oracle_shape_tables(const int32_t* atoIJK, double* xgp, double* wgp, double* Ngp, double* dNgp,
+                         double* dlxigp_ip, int32_t* invAtoIJK, int32_t* gmshAtoI, int32_t* gmshAtoJ,
+                         int32_t* gmshAtoK) {
+  shape_tables(atoIJK, xgp, wgp, Ngp, dNgp, dlxigp_ip, invAtoIJK, gmshAtoI, gmshAtoJ, gmshAtoK);
+}
+
+void oracle_elem_jacobian(int nelem, int npoin, const int32_t* connec, const double* coord,
+                          const double* dNgp, const double* wgp, double* gpvol, double* He) {
+  elem_jacobian<double>(nelem, npoin, connec, coord, dNgp, wgp, gpvol, He);
+}
+
+// Je(i,j) in Fortran order at i + 3*j; He likewise.
+void oracle_cofactor_inverse(const double* Je9, double* He9, double* det) {
+  double Je[3][3];
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) Je[i][j] = Je9[i + 3 * j];
+  cofactor_inverse<double>(Je, He9, *det);
+}
+
+void oracle_lumped_mass(int nelem, int npoin, const int32_t* connec, const double* gpvol, double* Ml) {
+  lumped_mass_spectral<double>(nelem, npoin, connec, gpvol, Ml);
+}
+
+void oracle_char_length(int nelem, int npoin, const int32_t* connec, const double* coord, double* helem) {
+  char_length<double>(nelem, npoin, connec, coord, helem);
+}
+
+void oracle_char_length_spectral(int nelem, int npoin, const int32_t* connec, const double* coord,
+                                 double* helem_l) {
+  char_length_spectral<double>(nelem, npoin, connec, coord, helem_l);
+}
+
+void oracle_full_convec_ijk(const ElemCtx* ctx, const double* u, const double* q, const double* rho,
+                            const double* pr, const double* E, double* Rmass, double* Rmom, double* Rener) {
+  full_convec_ijk(*ctx, u, q, rho, pr, E, Rmass, Rmom, Rener);
+}
+
+void oracle_generic_scalar_convec_ijk(const ElemCtx* ctx, const double* q, const double* eta,
+                                      const double* u, double* R) {
+  generic_scalar_convec_ijk(*ctx, q, eta, u, R);
+}
+
+void oracle_full_diffusion_ijk(const ElemCtx* ctx, const Params* P, const double* rho_n, const double* rho,
+                               const double* u, const double* Tem, const double* mu_fluid,
+                               const double* mu_e, const double* mu_sgs, double* Rmass, double* Rmom,
+                               double* Rener) {
+  full_diffusion_ijk(*ctx, *P, rho_n, rho, u, Tem, mu_fluid, mu_e, mu_sgs, Rmass, Rmom, Rener);
+}
+
+void oracle_smart_visc_spectral(const ElemCtx* ctx, const Params* P, const double* Reta, const double* gpvol,
+                                const double* wgp, const double* rho, const double* u, const double* csound,
+                                const double* Tem, const double* eta, const double* helem_l,
+                                const double* helem, double* mu_e, double* mue_l) {
+  smart_visc_spectral(*ctx, *P, Reta, gpvol, wgp, rho, u, csound, Tem, eta, helem_l, helem, mu_e, mue_l);
+}
+
+void oracle_sutherland(int npoin, const double* Tem, const double* mu_factor, double* mu_fluid) {
+  sutherland_viscosity(npoin, Tem, mu_factor, mu_fluid);
+}
+
+double oracle_adapt_dt_cfl(const ElemCtx* ctx, const double* helem, const double* u, const double* csound,
+                           double cfl_conv, double cfl_diff, const double* mu_fluid, const double* mu_sgs,
+                           const double* rho) {
+  return adapt_dt_cfl(*ctx, helem, u, csound, cfl_conv, cfl_diff, mu_fluid, mu_sgs, rho);
+}
+
+// Runs nsteps explicit RK4 steps of rk_4_main on the state S (level pos=2 only).  When
+// capture is non-null its arrays receive the residuals (after /Ml) of stage capture->stage of
+// the first step.
+void oracle_rk_4_main(const ElemCtx* ctx, const Params* P, const double* Ml, const double* mu_factor,
+                      const double* gpvol, const double* wgp, const double* helem, const double* helem_l,
+                      double dt, int nsteps, State* S, StageCapture* capture) {
+  Rk4Scratch W(ctx->npoin);
+  for (int s = 0; s < nsteps; ++s)
+    rk_4_main(*ctx, *P, Ml, mu_factor, gpvol, wgp, helem, helem_l, dt, *S, W, s == 0 ? capture : nullptr);
+}
+
+void oracle_eval_laplacian_mult(const ElemCtx* ctx, const double* p, double* ResP) {
+  std::vector<double> aux;
+  eval_laplacian_mult(*ctx, p, ResP, aux);
+}
+
+void oracle_eval_laplacian_diag(const ElemCtx* ctx, const double* dNgp, double* d) {
+  eval_laplacian_diag(*ctx, dNgp, d);
+}
+
+int oracle_conjgrad_pressure(const ElemCtx* ctx, const double* dNgp, const double* Rp0, double* R,
+                             int maxIter, double tol, double* final_rel) {
+  return conjGrad_pressure(*ctx, dNgp, Rp0, R, maxIter, tol, final_rel);
+}
+
+// CSR_SpMV_scal as pinned by unitt_CSR_SPMV_scal.f90:14-52: rdom holds 0-based row offsets
+// (npoin+1), cdom 1-based column ids.
+void oracle_csr_spmv_scal(int npoin, int nzdom, const int32_t* rdom, const int32_t* cdom, const double* Mc,
+                          const double* v, double* u) {
+  (void)nzdom;
+  for (int i = 0; i < npoin; ++i) {
+    double s = 0.0;
+    for (int k = rdom[i]; k < rdom[i + 1]; ++k) s += Mc[k] * v[cdom[k] - 1];
+    u[i] = s;
+  }
+}
+
+}  // extern "C"

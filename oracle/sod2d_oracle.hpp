@@ -1,0 +1,1044 @@
+// CPU ORACLE — test infrastructure only, never the product path.
+//
+// A line-by-line C++ restatement of the SOD2D reference routines that make up the explicit
+// spectral-element RHS for HEX64 (p=3) elements.  It is the parity checker for the CUDA
+// library (sod2d_refmap_b200/csrc) and the timed CPU baseline of bench.py.  Only tests/,
+// __graft_entry__.smoke() and bench.py's CPU-baseline legs may load it.
+//
+// Parity pinning: the reference is Fortran+OpenACC+MPI+HDF5 and cannot be compiled in this
+// image (no Fortran compiler, MPI or HDF5).  The restatement is pinned by the known-answer
+// tests that the reference's own unit tests hold (GLL/HEX64 Kronecker property, 3-D Jacobian
+// inverse determinant, CSR SpMV vector, char_length) and by the discrete conservation
+// invariant of the reference's convection/diffusion tests, evaluated on periodic meshes.
+//
+// Array conventions: every array keeps the reference's Fortran column-major layout with the
+// 1-based indices translated to 0-based, e.g. He(idime,jdime,igaus,ielem) is
+// He[idime + 3*(jdime + 3*(igaus + 64*ielem))], connec(ielem,inode) is connec[ielem + nelem*inode]
+// and holds 0-based node ids, u(ipoin,idime) is u[ipoin + npoin*idime].
+#pragma once
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <vector>
+#include <algorithm>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace sod_oracle {
+
+constexpr int porder = 3;
+constexpr int nnode = (porder + 1) * (porder + 1) * (porder + 1);
+constexpr int ngaus = nnode;
+constexpr int ndime = 3;
+
+// ------------------------------------------------------------------------------------------
+// Physical / numerical parameters (mod_numerical_params.f90:8-99, TGVSolver.f90:77-103)
+// ------------------------------------------------------------------------------------------
+struct Params {
+  double gamma_gas;   // TGVSolver.f90:92
+  double Rgas;        // TGVSolver.f90:95 (also nscbc_Rgas_inf, :102)
+  double Cp;          // TGVSolver.f90:87
+  double Prt;         // TGVSolver.f90:88
+  double ce, cmax, cglob, c_rho, c_ener;  // mod_numerical_params.f90:24-28
+  int flag_normalise_entropy;             // mod_numerical_params.f90:23
+  double cfl_conv, cfl_diff;
+};
+
+// ------------------------------------------------------------------------------------------
+// GLL nodes and weights: ZELEGL / WELEGL / VALEPO (mod_maths.f90:46-152), real(8) arithmetic.
+// Nodes are returned in ascending order ET(0..N).
+// ------------------------------------------------------------------------------------------
+inline void valepo(int N, double X, double& Y, double& DY, double& D2Y) {
+  Y = 1.0; DY = 0.0; D2Y = 0.0;
+  if (N == 0) return;
+  Y = X; DY = 1.0; D2Y = 0.0;
+  if (N == 1) return;
+  double YP = 1.0, DYP = 0.0, D2YP = 0.0;
+  for (int I = 2; I <= N; ++I) {
+    double C1 = (double)I, C2 = 2.0 * C1 - 1.0, C4 = C1 - 1.0;
+    double YM = Y;
+    Y = (C2 * X * Y - C4 * YP) / C1;
+    YP = YM;
+    double DYM = DY;
+    DY = (C2 * X * DY - C4 * DYP + C2 * YP) / C1;
+    DYP = DYM;
+    double D2YM = D2Y;
+    D2Y = (C2 * X * D2Y - C4 * D2YP + 2.0 * C2 * DYP) / C1;
+    D2YP = D2YM;
+  }
+}
+
+inline void zelegl(int N, double* ET, double* VN) {
+  if (N == 0) return;
+  int N2 = (N - 1) / 2;
+  double SN = (double)(2 * N - 4 * N2 - 3);
+  ET[0] = -1.0; ET[N] = 1.0; VN[0] = SN; VN[N] = 1.0;
+  if (N == 1) return;
+  ET[N2 + 1] = 0.0;
+  double Y, DY, D2Y;
+  valepo(N, 0.0, Y, DY, D2Y);
+  VN[N2 + 1] = Y;
+  if (N == 2) return;
+  const double v_pi = 2.0 * std::asin(1.0);
+  double C = v_pi / (double)N;
+  for (int I = 1; I <= N2; ++I) {
+    double ETX = std::cos(C * (double)I);
+    for (int IT = 1; IT <= 8; ++IT) {
+      valepo(N, ETX, Y, DY, D2Y);
+      ETX = ETX - DY / D2Y;
+    }
+    ET[I] = -ETX; ET[N - I] = ETX;
+    VN[I] = Y * SN; VN[N - I] = Y;
+  }
+}
+
+inline void welegl(int N, const double* ET, const double* VN, double* WT) {
+  if (N == 0) return;
+  int N2 = (N - 1) / 2;
+  double DN = (double)N;
+  double C = 2.0 / (DN * (DN + 1.0));
+  for (int I = 0; I <= N2; ++I) {
+    double Y = VN[I];
+    double WTX = C / (Y * Y);
+    WT[I] = WTX; WT[N - I] = WTX;
+  }
+  if (N - 1 == 2 * N2) return;
+  double Y = VN[N2 + 1];
+  WT[N2 + 1] = C / (Y * Y);
+}
+
+// ------------------------------------------------------------------------------------------
+// 1-D Lagrange basis and derivative in sod2d 1-D order (1 <-> -1, 2 <-> +1, 3.. interior):
+// eval_lagrangePoly / eval_lagrangePolyDeriv (mod_maths.f90:178-258).  xi[] is ascending.
+// ------------------------------------------------------------------------------------------
+template <class T>
+inline void eval_lagrange(const T* xi, T xp, T* l) {
+  int lorder[porder + 1];
+  lorder[0] = 1; lorder[1] = porder + 1;
+  for (int i = 3; i <= porder + 1; ++i) lorder[i - 1] = i - 1;
+  for (int i = 0; i <= porder; ++i) {
+    l[i] = T(1);
+    for (int j = 0; j <= porder; ++j)
+      if (j != lorder[i] - 1) l[i] = l[i] * ((xp - xi[j]) / (xi[lorder[i] - 1] - xi[j]));
+  }
+}
+
+template <class T>
+inline void eval_lagrange_deriv(const T* xi, T xp, T* dl) {
+  int lorder[porder + 1];
+  lorder[0] = 1; lorder[1] = porder + 1;
+  for (int i = 3; i <= porder + 1; ++i) lorder[i - 1] = i - 1;
+  for (int i = 0; i <= porder; ++i) {
+    dl[i] = T(0);
+    for (int j = 0; j <= porder; ++j) {
+      T aux = T(1);
+      if (j != lorder[i] - 1) {
+        for (int m = 0; m <= porder; ++m)
+          if (m != j && m != lorder[i] - 1) aux = aux * (xp - xi[m]) / (xi[lorder[i] - 1] - xi[m]);
+        dl[i] = dl[i] + (T(1) / (xi[lorder[i] - 1] - xi[j])) * aux;
+      }
+    }
+  }
+}
+
+// TripleTensorProduct (mod_maths.f90:260-298) on the GLL grid; N(a), dN(d,a), dlxigp(d,ii).
+template <class T>
+inline void triple_tensor_product(const T* xi_grid, T s, T t, T z, const int32_t* atoIJK,
+                                  T* N, T* dN, T* dlxigp /* (3,4) or null */) {
+  T lxi[porder + 1], leta[porder + 1], lzeta[porder + 1];
+  T dlxi[porder + 1], dleta[porder + 1], dlzeta[porder + 1];
+  eval_lagrange(xi_grid, s, lxi);
+  eval_lagrange(xi_grid, t, leta);
+  eval_lagrange(xi_grid, z, lzeta);
+  eval_lagrange_deriv(xi_grid, s, dlxi);
+  eval_lagrange_deriv(xi_grid, t, dleta);
+  eval_lagrange_deriv(xi_grid, z, dlzeta);
+  if (dlxigp) {
+    for (int ii = 0; ii <= porder; ++ii) {
+      dlxigp[0 + 3 * ii] = dlxi[ii];
+      dlxigp[1 + 3 * ii] = dleta[ii];
+      dlxigp[2 + 3 * ii] = dlzeta[ii];
+    }
+  }
+  int c = 0;
+  for (int k = 0; k <= porder; ++k)
+    for (int i = 0; i <= porder; ++i)
+      for (int j = 0; j <= porder; ++j) {
+        int a = atoIJK[c++];
+        N[a] = lxi[i] * leta[j] * lzeta[k];
+        dN[0 + 3 * a] = dlxi[i] * leta[j] * lzeta[k];
+        dN[1 + 3 * a] = lxi[i] * dleta[j] * lzeta[k];
+        dN[2 + 3 * a] = lxi[i] * leta[j] * dlzeta[k];
+      }
+}
+
+// Shape-function tables for HEX64 with GLL collocation:
+// GaussLobattoLegendre_hex (quadrature_rules.f90:51-78), hex_highorder (elem_hex.f90:22-43),
+// evalShapeFunctions (CFDSolverBase.f90:1143-1261), atoIJKInverse (mod_geom.f90:123-144).
+// atoIJK: 0-based local node ids.  Outputs in Fortran layouts: xgp(ngaus,3), wgp(ngaus),
+// Ngp(ngaus,nnode), dNgp(3,nnode,ngaus), dlxigp_ip(ngaus,3,4), invAtoIJK(4,4,4), gmshAto*(nnode)
+// (the last two 0-based).
+inline void shape_tables(const int32_t* atoIJK, double* xgp, double* wgp, double* Ngp, double* dNgp,
+                         double* dlxigp_ip, int32_t* invAtoIJK, int32_t* gmshAtoI,
+                         int32_t* gmshAtoJ, int32_t* gmshAtoK) {
+  double xi[porder + 1], w1d[porder + 1], vn[porder + 1];
+  zelegl(porder, xi, vn);
+  welegl(porder, xi, vn, w1d);
+  int lorder[porder + 1];
+  lorder[0] = 1; lorder[1] = porder + 1;
+  for (int i = 3; i <= porder + 1; ++i) lorder[i - 1] = i - 1;
+  int inode = 0;
+  for (int k = 0; k <= porder; ++k)
+    for (int i = 0; i <= porder; ++i)
+      for (int j = 0; j <= porder; ++j) {
+        int a = atoIJK[inode++];
+        xgp[a + ngaus * 0] = xi[lorder[i] - 1];
+        xgp[a + ngaus * 1] = xi[lorder[j] - 1];
+        xgp[a + ngaus * 2] = xi[lorder[k] - 1];
+        wgp[a] = w1d[lorder[i] - 1] * w1d[lorder[j] - 1] * w1d[lorder[k] - 1];
+      }
+  for (int g = 0; g < ngaus; ++g) {
+    double N[nnode], dN[3 * nnode], dl[3 * (porder + 1)];
+    triple_tensor_product<double>(xi, xgp[g], xgp[g + ngaus], xgp[g + 2 * ngaus], atoIJK, N, dN, dl);
+    for (int a = 0; a < nnode; ++a) {
+      Ngp[g + ngaus * a] = N[a];
+      for (int d = 0; d < 3; ++d) dNgp[d + 3 * (a + nnode * g)] = dN[d + 3 * a];
+    }
+    for (int d = 0; d < 3; ++d)
+      for (int ii = 0; ii <= porder; ++ii) dlxigp_ip[g + ngaus * (d + 3 * ii)] = dl[d + 3 * ii];
+  }
+  int c = 0;
+  for (int k = 0; k <= porder; ++k)
+    for (int i = 0; i <= porder; ++i)
+      for (int j = 0; j <= porder; ++j) {
+        int a = atoIJK[c++];
+        invAtoIJK[i + 4 * (j + 4 * k)] = a;
+        gmshAtoI[a] = i; gmshAtoJ[a] = j; gmshAtoK[a] = k;
+      }
+}
+
+template <class T>
+inline void cofactor_inverse(const T (&Je)[3][3], T* He, T& det_out);
+
+// ------------------------------------------------------------------------------------------
+// elem_jacobian (jacobian_oper.f90:9-138), 3-D cofactor inverse.
+// ------------------------------------------------------------------------------------------
+template <class T>
+inline void elem_jacobian(int nelem, int npoin, const int32_t* connec, const T* coord, const T* dNgp,
+                          const T* wgp, T* gpvol, T* He) {
+#pragma omp parallel for schedule(static)
+  for (int e = 0; e < nelem; ++e) {
+    for (int g = 0; g < ngaus; ++g) {
+      T Je[3][3];
+      for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) {
+          T s = T(0);
+          for (int a = 0; a < nnode; ++a)
+            s += dNgp[i + 3 * (a + nnode * g)] * coord[connec[e + (int64_t)nelem * a] + (int64_t)npoin * j];
+          Je[i][j] = T(0) + s;
+        }
+      T H9[9], det;
+      cofactor_inverse(Je, H9, det);
+      T* H = He + 9 * ((int64_t)g + ngaus * (int64_t)e);
+      for (int q = 0; q < 9; ++q) H[q] = H9[q];
+      gpvol[g + ngaus * (int64_t)e] = wgp[g] * det;
+    }
+  }
+}
+
+// 3-D branch of elem_jacobian (jacobian_oper.f90:73-132): determinant, signed minors,
+// transpose and division by det.  He is returned in Fortran order He(i,j) at i + 3*j.
+template <class T>
+inline void cofactor_inverse(const T (&Je)[3][3], T* He, T& det_out) {
+  {
+    {
+      T det = (Je[0][0] * Je[1][1] * Je[2][2] + Je[0][1] * Je[1][2] * Je[2][0] +
+               Je[0][2] * Je[1][0] * Je[2][1] - Je[2][0] * Je[1][1] * Je[0][2] -
+               Je[2][1] * Je[1][2] * Je[0][0] - Je[2][2] * Je[1][0] * Je[0][1]);
+      T a[9], b[9];
+      a[0] = Je[1][1] * Je[2][2] - Je[2][1] * Je[1][2];
+      a[1] = Je[1][0] * Je[2][2] - Je[2][0] * Je[1][2];
+      a[2] = Je[1][0] * Je[2][1] - Je[2][0] * Je[1][1];
+      a[3] = Je[0][1] * Je[2][2] - Je[2][1] * Je[0][2];
+      a[4] = Je[0][0] * Je[2][2] - Je[2][0] * Je[0][2];
+      a[5] = Je[0][0] * Je[2][1] - Je[2][0] * Je[0][1];
+      a[6] = Je[0][1] * Je[1][2] - Je[1][1] * Je[0][2];
+      a[7] = Je[0][0] * Je[1][2] - Je[1][0] * Je[0][2];
+      a[8] = Je[0][0] * Je[1][1] - Je[1][0] * Je[0][1];
+      a[1] = -a[1]; a[3] = -a[3]; a[5] = -a[5]; a[7] = -a[7];
+      for (int q = 0; q < 9; ++q) b[q] = a[q];
+      b[1] = a[3]; b[2] = a[6]; b[3] = a[1]; b[5] = a[7]; b[6] = a[2]; b[7] = a[5];
+      for (int q = 0; q < 9; ++q) b[q] = (T(1) / det) * b[q];
+      T* H = He;
+      // He(i,j): b(1..3) is row 1, b(4..6) row 2, b(7..9) row 3.
+      H[0 + 3 * 0] = b[0]; H[0 + 3 * 1] = b[1]; H[0 + 3 * 2] = b[2];
+      H[1 + 3 * 0] = b[3]; H[1 + 3 * 1] = b[4]; H[1 + 3 * 2] = b[5];
+      H[2 + 3 * 0] = b[6]; H[2 + 3 * 1] = b[7]; H[2 + 3 * 2] = b[8];
+      det_out = det;
+    }
+  }
+}
+
+// lumped_mass_spectral (mass_matrix.f90:11-43)
+template <class T>
+inline void lumped_mass_spectral(int nelem, int npoin, const int32_t* connec, const T* gpvol, T* Ml) {
+  for (int p = 0; p < npoin; ++p) Ml[p] = T(0);
+  for (int e = 0; e < nelem; ++e)
+    for (int a = 0; a < nnode; ++a) Ml[connec[e + (int64_t)nelem * a]] += gpvol[a + ngaus * (int64_t)e];
+}
+
+// char_length + hexa_edges (mod_geom.f90:13-37, elem_hex.f90:45-75): min corner-edge length.
+template <class T>
+inline void char_length(int nelem, int npoin, const int32_t* connec, const T* coord, T* helem) {
+  static const int edges[12][2] = {{1, 0}, {2, 1}, {3, 2}, {0, 3}, {5, 4}, {6, 5},
+                                   {7, 6}, {4, 7}, {4, 0}, {5, 1}, {6, 2}, {7, 3}};
+  for (int e = 0; e < nelem; ++e) {
+    T dist2 = T(1000000000000.0);
+    for (int q = 0; q < 12; ++q) {
+      int32_t pa = connec[e + (int64_t)nelem * edges[q][0]];
+      int32_t pb = connec[e + (int64_t)nelem * edges[q][1]];
+      T s = T(0);
+      for (int d = 0; d < 3; ++d) {
+        T dx = coord[pa + (int64_t)npoin * d] - coord[pb + (int64_t)npoin * d];
+        s += dx * dx;
+      }
+      dist2 = std::min(dist2, (T)std::sqrt(s));
+    }
+    helem[e] = dist2;
+  }
+}
+
+// char_length_spectral (mod_geom.f90:39-66): per node min distance to any other element node.
+template <class T>
+inline void char_length_spectral(int nelem, int npoin, const int32_t* connec, const T* coord, T* helem_l) {
+#pragma omp parallel for schedule(static)
+  for (int e = 0; e < nelem; ++e)
+    for (int a = 0; a < nnode; ++a) {
+      T aux = T(1000000000000.0);
+      for (int b = 0; b < nnode; ++b) {
+        if (a == b) continue;
+        T s = T(0);
+        for (int d = 0; d < 3; ++d) {
+          T dx = coord[connec[e + (int64_t)nelem * a] + (int64_t)npoin * d] -
+                 coord[connec[e + (int64_t)nelem * b] + (int64_t)npoin * d];
+          s += dx * dx;
+        }
+        aux = std::min((T)std::sqrt(s), aux);
+      }
+      helem_l[e + (int64_t)nelem * a] = aux;
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// Element kernels.  Common arguments (in Fortran layouts):
+//   connec(nelem,nnode)  He(3,3,ngaus,nelem)  gpvol(1,ngaus,nelem)  dlxigp_ip(ngaus,3,4)
+//   invAtoIJK(4,4,4)  gmshAtoI/J/K(nnode)
+// Residual assembly (the reference's !$acc atomic scatter) is an ordered scatter-add.  With
+// OpenMP the element loop is split into 8 colour classes of a periodic box so that no two
+// concurrently processed elements share a node, which keeps the result independent of the
+// thread count.  The caller supplies colour lists (elements grouped by colour).
+// ------------------------------------------------------------------------------------------
+struct ElemCtx {
+  int nelem, npoin;
+  const int32_t* connec;
+  const double* He;
+  const double* gpvol;
+  const double* dlxigp_ip;
+  const int32_t* invAtoIJK;
+  const int32_t* gmshAtoI;
+  const int32_t* gmshAtoJ;
+  const int32_t* gmshAtoK;
+  // colouring for race-free parallel scatter: ncolors groups, elements color_elems[color_ptr[c]..)
+  int ncolors;
+  const int32_t* color_ptr;
+  const int32_t* color_elems;
+};
+
+#define SOD_INV(i, j, k) (ctx.invAtoIJK[(i) + 4 * ((j) + 4 * (k))])
+#define SOD_DL(g, d, ii) (ctx.dlxigp_ip[(g) + ngaus * ((d) + 3 * (ii))])
+#define SOD_HE(i, j, g, e) (ctx.He[(i) + 3 * ((j) + 3 * ((int64_t)(g) + ngaus * (int64_t)(e)))])
+#define SOD_GPVOL(g, e) (ctx.gpvol[(g) + ngaus * (int64_t)(e)])
+
+template <class F>
+inline void for_each_element_coloured(const ElemCtx& ctx, F&& body) {
+  if (ctx.ncolors <= 0) {
+    for (int e = 0; e < ctx.nelem; ++e) body(e);
+    return;
+  }
+  for (int c = 0; c < ctx.ncolors; ++c) {
+    int beg = ctx.color_ptr[c], end = ctx.color_ptr[c + 1];
+#pragma omp parallel for schedule(static)
+    for (int q = beg; q < end; ++q) body(ctx.color_elems[q]);
+  }
+}
+
+// full_convec_ijk (elem_convec.f90:211-460).  The caller passes E = enthalpy h (time_integ.f90:364).
+inline void full_convec_ijk(const ElemCtx& ctx, const double* u, const double* q, const double* rho,
+                            const double* pr, const double* E, double* Rmass, double* Rmom,
+                            double* Rener) {
+  const int nelem = ctx.nelem, npoin = ctx.npoin;
+  for (int64_t p = 0; p < (int64_t)npoin * 3; ++p) Rmom[p] = 0.0;
+  for (int p = 0; p < npoin; ++p) { Rmass[p] = 0.0; Rener[p] = 0.0; }
+  for_each_element_coloured(ctx, [&](int ielem) {
+    int ipoin[nnode];
+    double Re_mom[nnode][3], Re_mass[nnode], Re_ener[nnode];
+    double ul[nnode][3], ql[nnode][3], rhol[nnode], prl[nnode], El[nnode], fel[nnode][3];
+    double fl[nnode][3][3], fuul[nnode][3][3], REl[nnode], fuel[nnode][3], kl[nnode], fkl[nnode][3],
+        fukl[nnode][3], Rkl[nnode];
+    for (int a = 0; a < nnode; ++a) ipoin[a] = ctx.connec[ielem + (int64_t)nelem * a];
+    for (int a = 0; a < nnode; ++a) {
+      kl[a] = 0.0;
+      for (int d = 0; d < 3; ++d)
+        kl[a] = kl[a] + u[ipoin[a] + (int64_t)npoin * d] * u[ipoin[a] + (int64_t)npoin * d] * 0.5;
+    }
+    for (int d = 0; d < 3; ++d)
+      for (int a = 0; a < nnode; ++a) {
+        double ud = u[ipoin[a] + (int64_t)npoin * d];
+        ul[a][d] = ud;
+        ql[a][d] = q[ipoin[a] + (int64_t)npoin * d];
+        fel[a][d] = rho[ipoin[a]] * E[ipoin[a]] * ud;
+        fuel[a][d] = E[ipoin[a]] * ud;
+        fkl[a][d] = rho[ipoin[a]] * kl[a] * ud;
+        fukl[a][d] = kl[a] * ud;
+      }
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j)
+        for (int a = 0; a < nnode; ++a) {
+          fl[a][i][j] = q[ipoin[a] + (int64_t)npoin * i] * u[ipoin[a] + (int64_t)npoin * j];
+          fuul[a][i][j] = u[ipoin[a] + (int64_t)npoin * i] * u[ipoin[a] + (int64_t)npoin * j];
+        }
+    for (int a = 0; a < nnode; ++a) {
+      rhol[a] = rho[ipoin[a]];
+      El[a] = E[ipoin[a]];
+      REl[a] = rho[ipoin[a]] * E[ipoin[a]];
+      Rkl[a] = rho[ipoin[a]] * kl[a];
+      prl[a] = pr[ipoin[a]];
+    }
+    for (int igaus = 0; igaus < ngaus; ++igaus) {
+      double dlxi[4], dleta[4], dlzeta[4];
+      for (int ii = 0; ii < 4; ++ii) {
+        dlxi[ii] = SOD_DL(igaus, 0, ii);
+        dleta[ii] = SOD_DL(igaus, 1, ii);
+        dlzeta[ii] = SOD_DL(igaus, 2, ii);
+      }
+      int isoI = ctx.gmshAtoI[igaus], isoJ = ctx.gmshAtoJ[igaus], isoK = ctx.gmshAtoK[igaus];
+      double gIRho[3] = {0, 0, 0}, gIP[3] = {0, 0, 0}, gIE[3] = {0, 0, 0}, gIRE[3] = {0, 0, 0},
+             gIk[3] = {0, 0, 0}, gIRk[3] = {0, 0, 0};
+      double gIU[3][3] = {}, gIQ[3][3] = {}, gIFe[3][3] = {}, gIFue[3][3] = {}, gIFk[3][3] = {},
+             gIFuk[3][3] = {};
+      double gIF[3][3][3] = {}, gIFuu[3][3][3] = {};
+      for (int ii = 0; ii < 4; ++ii) {
+        int a1 = SOD_INV(ii, isoJ, isoK), a2 = SOD_INV(isoI, ii, isoK), a3 = SOD_INV(isoI, isoJ, ii);
+        gIRho[0] += dlxi[ii] * rhol[a1]; gIRho[1] += dleta[ii] * rhol[a2]; gIRho[2] += dlzeta[ii] * rhol[a3];
+        gIP[0] += dlxi[ii] * prl[a1];    gIP[1] += dleta[ii] * prl[a2];    gIP[2] += dlzeta[ii] * prl[a3];
+        gIE[0] += dlxi[ii] * El[a1];     gIE[1] += dleta[ii] * El[a2];     gIE[2] += dlzeta[ii] * El[a3];
+        gIRE[0] += dlxi[ii] * REl[a1];   gIRE[1] += dleta[ii] * REl[a2];   gIRE[2] += dlzeta[ii] * REl[a3];
+        gIk[0] += dlxi[ii] * kl[a1];     gIk[1] += dleta[ii] * kl[a2];     gIk[2] += dlzeta[ii] * kl[a3];
+        gIRk[0] += dlxi[ii] * Rkl[a1];   gIRk[1] += dleta[ii] * Rkl[a2];   gIRk[2] += dlzeta[ii] * Rkl[a3];
+        for (int id = 0; id < 3; ++id) {
+          gIU[id][0] += dlxi[ii] * ul[a1][id];   gIU[id][1] += dleta[ii] * ul[a2][id];   gIU[id][2] += dlzeta[ii] * ul[a3][id];
+          gIQ[id][0] += dlxi[ii] * ql[a1][id];   gIQ[id][1] += dleta[ii] * ql[a2][id];   gIQ[id][2] += dlzeta[ii] * ql[a3][id];
+          gIFe[id][0] += dlxi[ii] * fel[a1][id]; gIFe[id][1] += dleta[ii] * fel[a2][id]; gIFe[id][2] += dlzeta[ii] * fel[a3][id];
+          gIFue[id][0] += dlxi[ii] * fuel[a1][id]; gIFue[id][1] += dleta[ii] * fuel[a2][id]; gIFue[id][2] += dlzeta[ii] * fuel[a3][id];
+          gIFk[id][0] += dlxi[ii] * fkl[a1][id]; gIFk[id][1] += dleta[ii] * fkl[a2][id]; gIFk[id][2] += dlzeta[ii] * fkl[a3][id];
+          gIFuk[id][0] += dlxi[ii] * fukl[a1][id]; gIFuk[id][1] += dleta[ii] * fukl[a2][id]; gIFuk[id][2] += dlzeta[ii] * fukl[a3][id];
+          for (int jd = 0; jd < 3; ++jd) {
+            gIF[id][jd][0] += dlxi[ii] * fl[a1][id][jd];
+            gIF[id][jd][1] += dleta[ii] * fl[a2][id][jd];
+            gIF[id][jd][2] += dlzeta[ii] * fl[a3][id][jd];
+            gIFuu[id][jd][0] += dlxi[ii] * fuul[a1][id][jd];
+            gIFuu[id][jd][1] += dleta[ii] * fuul[a2][id][jd];
+            gIFuu[id][jd][2] += dlzeta[ii] * fuul[a3][id][jd];
+          }
+        }
+      }
+      double gradRho[3] = {0, 0, 0}, gradP[3] = {0, 0, 0}, gradE[3] = {0, 0, 0}, gradRE[3] = {0, 0, 0},
+             gradk[3] = {0, 0, 0}, gradRk[3] = {0, 0, 0};
+      double gradU[3][3] = {}, gradQ[3][3] = {}, divF[3] = {0, 0, 0}, divFuu[3] = {0, 0, 0};
+      double divFe = 0, divFue = 0, divFk = 0, divFuk = 0;
+      for (int id = 0; id < 3; ++id)
+        for (int jd = 0; jd < 3; ++jd) {
+          double h = SOD_HE(id, jd, igaus, ielem);
+          gradRho[id] += h * gIRho[jd];
+          gradP[id] += h * gIP[jd];
+          gradE[id] += h * gIE[jd];
+          gradRE[id] += h * gIRE[jd];
+          divFe += h * gIFe[id][jd];
+          divFue += h * gIFue[id][jd];
+          gradk[id] += h * gIk[jd];
+          gradRk[id] += h * gIRk[jd];
+          divFk += h * gIFk[id][jd];
+          divFuk += h * gIFuk[id][jd];
+          for (int kd = 0; kd < 3; ++kd) {
+            double h2 = SOD_HE(jd, kd, igaus, ielem);
+            gradU[id][jd] += h2 * gIU[id][kd];
+            gradQ[id][jd] += h2 * gIQ[id][kd];
+            divF[id] += h2 * gIF[id][jd][kd];
+            divFuu[id] += h2 * gIFuu[id][jd][kd];
+          }
+        }
+      double divU = gradU[0][0] + gradU[1][1] + gradU[2][2];
+      double divQ = gradQ[0][0] + gradQ[1][1] + gradQ[2][2];
+      Re_mass[igaus] = 0.5 * (divQ + rhol[igaus] * divU);
+      Re_ener[igaus] = 0.25 * (divFe + El[igaus] * divQ + REl[igaus] * divU + rhol[igaus] * divFue) +
+                       0.25 * (divFk + kl[igaus] * divQ + Rkl[igaus] * divU + rhol[igaus] * divFuk);
+      for (int id = 0; id < 3; ++id) {
+        Re_mom[igaus][id] = 0.25 * (divF[id] + ul[igaus][id] * divQ + ql[igaus][id] * divU +
+                                    rhol[igaus] * divFuu[id]) + gradP[id];
+        Re_mass[igaus] = Re_mass[igaus] + 0.5 * (ul[igaus][id] * gradRho[id]);
+        Re_ener[igaus] = Re_ener[igaus] +
+                         0.25 * (ql[igaus][id] * gradE[id] + ul[igaus][id] * gradRE[id] + fuel[igaus][id] * gradRho[id]) +
+                         0.25 * (ql[igaus][id] * gradk[id] + ul[igaus][id] * gradRk[id] + fukl[igaus][id] * gradRho[id]);
+        for (int jd = 0; jd < 3; ++jd)
+          Re_mom[igaus][id] = Re_mom[igaus][id] + 0.25 * (fuul[igaus][id][jd] * gradRho[jd] +
+                                                          ql[igaus][jd] * gradU[id][jd] + ul[igaus][jd] * gradQ[id][jd]);
+        Re_mom[igaus][id] = SOD_GPVOL(igaus, ielem) * Re_mom[igaus][id];
+      }
+      Re_mass[igaus] = SOD_GPVOL(igaus, ielem) * Re_mass[igaus];
+      Re_ener[igaus] = SOD_GPVOL(igaus, ielem) * Re_ener[igaus];
+    }
+    for (int d = 0; d < 3; ++d)
+      for (int a = 0; a < nnode; ++a) Rmom[ipoin[a] + (int64_t)npoin * d] += Re_mom[a][d];
+    for (int a = 0; a < nnode; ++a) {
+      Rmass[ipoin[a]] += Re_mass[a];
+      Rener[ipoin[a]] += Re_ener[a];
+    }
+  });
+}
+
+// generic_scalar_convec_ijk (elem_convec.f90:462-570): Reta from f_eta (=q arg), eta, u.
+inline void generic_scalar_convec_ijk(const ElemCtx& ctx, const double* q, const double* eta,
+                                      const double* u, double* Rconvec) {
+  const int nelem = ctx.nelem, npoin = ctx.npoin;
+  for (int p = 0; p < npoin; ++p) Rconvec[p] = 0.0;
+  for_each_element_coloured(ctx, [&](int ielem) {
+    int ipoin[nnode];
+    double ul[nnode][3], fel[nnode][3], etal[nnode], Re[nnode];
+    for (int a = 0; a < nnode; ++a) ipoin[a] = ctx.connec[ielem + (int64_t)nelem * a];
+    for (int d = 0; d < 3; ++d)
+      for (int a = 0; a < nnode; ++a) {
+        ul[a][d] = u[ipoin[a] + (int64_t)npoin * d];
+        fel[a][d] = q[ipoin[a] + (int64_t)npoin * d];
+      }
+    for (int a = 0; a < nnode; ++a) etal[a] = eta[ipoin[a]];
+    for (int igaus = 0; igaus < ngaus; ++igaus) {
+      int isoI = ctx.gmshAtoI[igaus], isoJ = ctx.gmshAtoJ[igaus], isoK = ctx.gmshAtoK[igaus];
+      double gIE[3] = {0, 0, 0}, gIU[3][3] = {}, gIFe[3][3] = {};
+      for (int ii = 0; ii < 4; ++ii) {
+        int a1 = SOD_INV(ii, isoJ, isoK), a2 = SOD_INV(isoI, ii, isoK), a3 = SOD_INV(isoI, isoJ, ii);
+        double d1 = SOD_DL(igaus, 0, ii), d2 = SOD_DL(igaus, 1, ii), d3 = SOD_DL(igaus, 2, ii);
+        gIE[0] += d1 * etal[a1]; gIE[1] += d2 * etal[a2]; gIE[2] += d3 * etal[a3];
+        for (int id = 0; id < 3; ++id) {
+          gIU[id][0] += d1 * ul[a1][id]; gIU[id][1] += d2 * ul[a2][id]; gIU[id][2] += d3 * ul[a3][id];
+          gIFe[id][0] += d1 * fel[a1][id]; gIFe[id][1] += d2 * fel[a2][id]; gIFe[id][2] += d3 * fel[a3][id];
+        }
+      }
+      double gradE[3] = {0, 0, 0}, divU = 0, divFe = 0;
+      for (int id = 0; id < 3; ++id)
+        for (int jd = 0; jd < 3; ++jd) {
+          double h = SOD_HE(id, jd, igaus, ielem);
+          gradE[id] += h * gIE[jd];
+          divU += h * gIU[id][jd];
+          divFe += h * gIFe[id][jd];
+        }
+      Re[igaus] = 0.5 * (divFe + etal[igaus] * divU);
+      for (int id = 0; id < 3; ++id) Re[igaus] = Re[igaus] + 0.5 * (ul[igaus][id] * gradE[id]);
+      Re[igaus] = SOD_GPVOL(igaus, ielem) * Re[igaus];
+    }
+    for (int a = 0; a < nnode; ++a) Rconvec[ipoin[a]] += Re[a];
+  });
+}
+
+// full_diffusion_ijk (elem_diffu.f90:12-198).  mu_e, mu_sgs are (nelem,ngaus).
+inline void full_diffusion_ijk(const ElemCtx& ctx, const Params& P, const double* rho_n,
+                               const double* rho, const double* u, const double* Tem,
+                               const double* mu_fluid, const double* mu_e, const double* mu_sgs,
+                               double* Rmass, double* Rmom, double* Rener) {
+  const int nelem = ctx.nelem, npoin = ctx.npoin;
+  const double Cp = P.Cp, Pr = P.Prt, c_rho = P.c_rho, c_ener = P.c_ener;
+  const double twoThirds = 2.0 / 3.0;
+  (void)rho;
+  for (int p = 0; p < npoin; ++p) { Rmass[p] = 0.0; Rener[p] = 0.0; }
+  for (int64_t p = 0; p < (int64_t)npoin * 3; ++p) Rmom[p] = 0.0;
+  for_each_element_coloured(ctx, [&](int ielem) {
+    int ipoin[nnode];
+    double ul[nnode][3], rhol[nnode], Teml[nnode], mufluidl[nnode], rhonl[nnode];
+    double tauXl[nnode][3], tauYl[nnode][3], tauZl[nnode][3], gradTl[nnode][3], gradRhol[nnode][3],
+        tauUl[nnode][3];
+    for (int a = 0; a < nnode; ++a) ipoin[a] = ctx.connec[ielem + (int64_t)nelem * a];
+    for (int a = 0; a < nnode; ++a) {
+      rhol[a] = rho[ipoin[a]];
+      rhonl[a] = rho_n[ipoin[a]];
+      Teml[a] = Tem[ipoin[a]];
+      mufluidl[a] = mu_fluid[ipoin[a]];
+    }
+    for (int a = 0; a < nnode; ++a)
+      for (int d = 0; d < 3; ++d) ul[a][d] = u[ipoin[a] + (int64_t)npoin * d];
+    for (int igaus = 0; igaus < ngaus; ++igaus) {
+      double mu_fgp = mufluidl[igaus] + rhonl[igaus] * mu_sgs[ielem + (int64_t)nelem * igaus];
+      double mu_egp = mu_e[ielem + (int64_t)nelem * igaus];
+      int isoI = ctx.gmshAtoI[igaus], isoJ = ctx.gmshAtoJ[igaus], isoK = ctx.gmshAtoK[igaus];
+      double gIRho[3] = {0, 0, 0}, gIT[3] = {0, 0, 0}, gIU[3][3] = {};
+      for (int ii = 0; ii < 4; ++ii) {
+        int a1 = SOD_INV(ii, isoJ, isoK), a2 = SOD_INV(isoI, ii, isoK), a3 = SOD_INV(isoI, isoJ, ii);
+        double d1 = SOD_DL(igaus, 0, ii), d2 = SOD_DL(igaus, 1, ii), d3 = SOD_DL(igaus, 2, ii);
+        gIRho[0] += d1 * rhol[a1]; gIRho[1] += d2 * rhol[a2]; gIRho[2] += d3 * rhol[a3];
+        gIT[0] += d1 * Teml[a1]; gIT[1] += d2 * Teml[a2]; gIT[2] += d3 * Teml[a3];
+        for (int id = 0; id < 3; ++id) {
+          gIU[id][0] += d1 * ul[a1][id]; gIU[id][1] += d2 * ul[a2][id]; gIU[id][2] += d3 * ul[a3][id];
+        }
+      }
+      double gradRho[3] = {0, 0, 0}, gradT[3] = {0, 0, 0}, gradU[3][3] = {};
+      for (int id = 0; id < 3; ++id)
+        for (int jd = 0; jd < 3; ++jd) {
+          double h = SOD_HE(id, jd, igaus, ielem);
+          gradRho[id] += h * gIRho[jd];
+          gradT[id] += h * gIT[jd];
+          for (int kd = 0; kd < 3; ++kd) gradU[id][jd] += SOD_HE(jd, kd, igaus, ielem) * gIU[id][kd];
+        }
+      double divU = gradU[0][0] + gradU[1][1] + gradU[2][2];
+      double tauU[3] = {0, 0, 0}, tau[3][3];
+      for (int id = 0; id < 3; ++id) {
+        for (int jd = 0; jd < 3; ++jd) {
+          tauU[id] = tauU[id] + (mu_fgp + mu_egp) * (gradU[id][jd] + gradU[jd][id]) * ul[igaus][jd];
+          tau[id][jd] = (mu_fgp + mu_egp) * (gradU[id][jd] + gradU[jd][id]);
+        }
+        tauU[id] = tauU[id] - (mu_fgp) * twoThirds * divU * ul[igaus][id];
+        tau[id][id] = tau[id][id] - (mu_fgp) * twoThirds * divU;
+      }
+      for (int id = 0; id < 3; ++id) {
+        tauXl[igaus][id] = tau[0][id];
+        tauYl[igaus][id] = tau[1][id];
+        tauZl[igaus][id] = tau[2][id];
+        gradTl[igaus][id] = gradT[id];
+        gradRhol[igaus][id] = gradRho[id];
+        tauUl[igaus][id] = tauU[id];
+      }
+    }
+    double Rm_l[nnode], Re_l[nnode], Rmo_l[nnode][3];
+    for (int igaus = 0; igaus < ngaus; ++igaus) {
+      double mue = mu_e[ielem + (int64_t)nelem * igaus];
+      double musgs = mu_sgs[ielem + (int64_t)nelem * igaus];
+      double nu_e = c_rho * mue / rhonl[igaus];
+      double kappa_e = mufluidl[igaus] * Cp / Pr + c_ener * mue * Cp / Pr + Cp * rhonl[igaus] * musgs / 0.9;
+      int isoI = ctx.gmshAtoI[igaus], isoJ = ctx.gmshAtoJ[igaus], isoK = ctx.gmshAtoK[igaus];
+      double divDe = 0.0, divDr = 0.0, divDm[3] = {0, 0, 0};
+      for (int ii = 0; ii < 4; ++ii) {
+        int a1 = SOD_INV(ii, isoJ, isoK), a2 = SOD_INV(isoI, ii, isoK), a3 = SOD_INV(isoI, isoJ, ii);
+        for (int id = 0; id < 3; ++id) {
+          double w1 = SOD_HE(id, 0, a1, ielem) * SOD_GPVOL(a1, ielem) * SOD_DL(a1, 0, isoI);
+          double w2 = SOD_HE(id, 1, a2, ielem) * SOD_GPVOL(a2, ielem) * SOD_DL(a2, 1, isoJ);
+          double w3 = SOD_HE(id, 2, a3, ielem) * SOD_GPVOL(a3, ielem) * SOD_DL(a3, 2, isoK);
+          divDr = divDr + w1 * gradRhol[a1][id];
+          divDr = divDr + w2 * gradRhol[a2][id];
+          divDr = divDr + w3 * gradRhol[a3][id];
+          divDe = divDe + w1 * (tauUl[a1][id] + kappa_e * gradTl[a1][id]);
+          divDe = divDe + w2 * (tauUl[a2][id] + kappa_e * gradTl[a2][id]);
+          divDe = divDe + w3 * (tauUl[a3][id] + kappa_e * gradTl[a3][id]);
+          divDm[0] = divDm[0] + w1 * tauXl[a1][id];
+          divDm[0] = divDm[0] + w2 * tauXl[a2][id];
+          divDm[0] = divDm[0] + w3 * tauXl[a3][id];
+          divDm[1] = divDm[1] + w1 * tauYl[a1][id];
+          divDm[1] = divDm[1] + w2 * tauYl[a2][id];
+          divDm[1] = divDm[1] + w3 * tauYl[a3][id];
+          divDm[2] = divDm[2] + w1 * tauZl[a1][id];
+          divDm[2] = divDm[2] + w2 * tauZl[a2][id];
+          divDm[2] = divDm[2] + w3 * tauZl[a3][id];
+        }
+      }
+      Rm_l[igaus] = nu_e * divDr;
+      Re_l[igaus] = divDe;
+      for (int d = 0; d < 3; ++d) Rmo_l[igaus][d] = divDm[d];
+    }
+    for (int igaus = 0; igaus < ngaus; ++igaus) {
+      Rmass[ipoin[igaus]] += Rm_l[igaus];
+      Rener[ipoin[igaus]] += Re_l[igaus];
+      for (int d = 0; d < 3; ++d) Rmom[ipoin[igaus] + (int64_t)npoin * d] += Rmo_l[igaus][d];
+    }
+  });
+}
+
+// smart_visc_spectral (mod_entropy_viscosity.f90:14-123) with init_filters weights and the
+// convertIJK map (mod_filters.f90:15-55).  helem_l is (nelem,nnode) (the dummy named helem),
+// helem is (nelem) (the dummy named helem_k).  Reductions in real(rp)=FP64.
+inline void smart_visc_spectral(const ElemCtx& ctx, const Params& P, const double* Reta,
+                                const double* gpvol, const double* wgp, const double* rho,
+                                const double* u, const double* csound, const double* Tem,
+                                const double* eta, const double* helem_l, const double* helem,
+                                double* mu_e, double* mue_l) {
+  const int nelem = ctx.nelem, npoin = ctx.npoin;
+  const double Rgas = P.Rgas, gamma_gas = P.gamma_gas;
+  const double v_pi = 2.0 * std::asin(1.0);
+  for (int64_t q = 0; q < (int64_t)nelem * nnode; ++q) mue_l[q] = mu_e[q];
+  double norm;
+  if (P.flag_normalise_entropy == 1) {
+    double maxEta_r = 0.0;
+    for (int p = 0; p < npoin; ++p) maxEta_r = maxEta_r + eta[p];
+    double maxEta = maxEta_r / (double)npoin;
+    double norm_r = 0.0;
+    for (int p = 0; p < npoin; ++p) norm_r = std::max(norm_r, std::fabs(eta[p] - maxEta));
+    norm = norm_r;
+  } else {
+    norm = 1.0;
+  }
+  int convertIJK[porder + 3];
+  for (int ii = 3; ii <= porder + 1; ++ii) convertIJK[ii - 1] = ii;
+  convertIJK[0] = 3; convertIJK[1] = 1; convertIJK[porder + 1] = 2; convertIJK[porder + 2] = porder;
+  const double wts[3] = {0.25, 0.5, 0.25};
+#pragma omp parallel for schedule(static)
+  for (int ielem = 0; ielem < nelem; ++ielem) {
+    double maxJe = 0.0, minJe = 1000000.0, maxV = 0.0, maxC = 0.0;
+    for (int g = 0; g < ngaus; ++g) {
+      int p = ctx.connec[ielem + (int64_t)nelem * g];
+      minJe = std::min(minJe, gpvol[g + ngaus * (int64_t)ielem] / wgp[g]);
+      maxJe = std::max(maxJe, gpvol[g + ngaus * (int64_t)ielem] / wgp[g]);
+      double uu = 0;
+      for (int d = 0; d < 3; ++d) uu += u[p + (int64_t)npoin * d] * u[p + (int64_t)npoin * d];
+      maxV = std::max(maxV, std::sqrt(uu));
+      maxC = std::max(maxC, csound[p]);
+    }
+    double M = maxV / maxC;
+    double ceM = std::max(std::tanh(std::pow(M, 15) * v_pi), P.ce);
+    double ced = std::max(1.0 - (minJe / maxJe) * (minJe / maxJe), P.ce);
+    ced = std::max(ced, ceM);
+    double betae = 0.0;
+    for (int a = 0; a < nnode; ++a) {
+      int p = ctx.connec[ielem + (int64_t)nelem * a];
+      double uu = 0;
+      for (int d = 0; d < 3; ++d) uu += u[p + (int64_t)npoin * d] * u[p + (int64_t)npoin * d];
+      double aux2 = std::sqrt(uu);
+      double aux3 = std::sqrt(Rgas * gamma_gas * Tem[p]);
+      double aux1 = aux2 + aux3;
+      betae = std::max(betae, (rho[p] * helem[ielem]) * (P.cmax / (double)porder) * aux1);
+    }
+    for (int a = 0; a < nnode; ++a) {
+      int p = ctx.connec[ielem + (int64_t)nelem * a];
+      double R1 = rho[p] * std::fabs(Reta[p]) / norm;
+      double hl = helem_l[ielem + (int64_t)nelem * a];
+      double Ve = ced * R1 * hl * hl;
+      mue_l[ielem + (int64_t)nelem * a] = P.cglob * std::min(Ve, betae);
+    }
+    for (int ii = 1; ii <= porder + 1; ++ii)
+      for (int jj = 1; jj <= porder + 1; ++jj)
+        for (int kk = 1; kk <= porder + 1; ++kk) {
+          double aux1 = 0.0;
+          for (int ll = -1; ll <= 1; ++ll)
+            for (int mm = -1; mm <= 1; ++mm)
+              for (int nn = -1; nn <= 1; ++nn) {
+                int a = SOD_INV(convertIJK[ii + ll] - 1, convertIJK[jj + mm] - 1, convertIJK[kk + nn] - 1);
+                aux1 = aux1 + wts[ll + 1] * wts[mm + 1] * wts[nn + 1] * mue_l[ielem + (int64_t)nelem * a];
+              }
+          int a = SOD_INV(convertIJK[ii] - 1, convertIJK[jj] - 1, convertIJK[kk] - 1);
+          mu_e[ielem + (int64_t)nelem * a] = aux1;
+        }
+  }
+}
+
+// sutherland_viscosity (mod_fluid_viscosity.f90:21-41)
+inline void sutherland_viscosity(int npoin, const double* Tem, const double* mu_factor, double* mu_fluid) {
+  const double C1 = 0.000001458, S = 110.4;
+  for (int p = 0; p < npoin; ++p) mu_fluid[p] = mu_factor[p] * C1 * std::pow(Tem[p], 1.5) / (Tem[p] + S);
+}
+
+// adapt_dt_cfl (mod_time_ops.f90:11-61) with the diffusive limit; mu_sgs (nelem,nnode).
+inline double adapt_dt_cfl(const ElemCtx& ctx, const double* helem, const double* u, const double* csound,
+                           double cfl_conv, double cfl_diff, const double* mu_fluid, const double* mu_sgs,
+                           const double* rho) {
+  const int nelem = ctx.nelem, npoin = ctx.npoin;
+  double dt_conv = 100000000000000.0, dt_diff = 100000000000000.0, dt_l = 100000000000000.0;
+  for (int e = 0; e < nelem; ++e) {
+    double L3 = 0.0;
+    for (int a = 0; a < nnode; ++a) {
+      int p = ctx.connec[e + (int64_t)nelem * a];
+      double umag = std::fabs(u[p]);
+      umag = std::max(umag, std::fabs(u[p + (int64_t)npoin]));
+      umag = std::max(umag, std::fabs(u[p + 2 * (int64_t)npoin]));
+      L3 = std::max(L3, umag + csound[p]);
+    }
+    double aux2 = cfl_conv * (helem[e] / (double)(2.0 * porder + 1)) / L3;
+    dt_conv = std::min(dt_conv, aux2);
+    double max_MU = 0.0;
+    for (int a = 0; a < nnode; ++a) {
+      int p = ctx.connec[e + (int64_t)nelem * a];
+      max_MU = std::max(max_MU, (rho[p] * mu_sgs[e + (int64_t)nelem * a] + mu_fluid[p]) / rho[p]);
+    }
+    double hh = helem[e] / (double)(2.0 * porder + 1);
+    double aux4 = cfl_diff * (hh * hh) / max_MU;
+    dt_diff = std::min(dt_diff, aux4);
+    dt_l = std::min(dt_conv, dt_diff);
+  }
+  return dt_l;
+}
+
+// ------------------------------------------------------------------------------------------
+// rk_4_main (time_integ.f90:137-508) restricted to the periodic compressible path:
+// noBoundaries, no wall model, no source term, no buffer, flag_les=0, flag_total_enthalpy
+// false, Sutherland on (flag_real_diff=flag_diff_suth=1), RK order 4, single rank.
+// State arrays hold level pos=2 only (the only level rk_4_main reads and writes).
+// ------------------------------------------------------------------------------------------
+struct State {
+  double* rho;    // (npoin)
+  double* u;      // (npoin,3)
+  double* q;      // (npoin,3)
+  double* pr;     // (npoin)
+  double* E;      // (npoin)
+  double* Tem;    // (npoin)
+  double* e_int;  // (npoin)
+  double* eta;    // (npoin)
+  double* csound; // (npoin)
+  double* machno; // (npoin)
+  double* mu_fluid;  // (npoin)
+  double* mu_e;   // (nelem,ngaus)
+  double* mu_sgs; // (nelem,ngaus)
+  double* mue_l;  // (nelem,nnode)
+};
+
+struct Rk4Scratch {
+  std::vector<double> Rmass, Rener, Reta, Rmom, aux_rho, aux_pr, aux_E, aux_Tem, aux_e_int, aux_eta,
+      aux_h, aux_u, aux_q, Rmass_sum, Rener_sum, Reta_sum, Rdiff_mass, Rdiff_ener, Rmom_sum, Rdiff_mom,
+      f_eta;
+  explicit Rk4Scratch(int npoin) {
+    for (auto* v : {&Rmass, &Rener, &Reta, &aux_rho, &aux_pr, &aux_E, &aux_Tem, &aux_e_int, &aux_eta,
+                    &aux_h, &Rmass_sum, &Rener_sum, &Reta_sum, &Rdiff_mass, &Rdiff_ener})
+      v->assign(npoin, 0.0);
+    for (auto* v : {&Rmom, &aux_u, &aux_q, &Rmom_sum, &Rdiff_mom, &f_eta}) v->assign((size_t)npoin * 3, 0.0);
+  }
+};
+
+// Optional per-stage capture of the first stage's residuals (after /Ml), for RHS parity.
+struct StageCapture {
+  double* Rmass;  // (npoin)   null = not captured
+  double* Rmom;   // (npoin,3)
+  double* Rener;  // (npoin)
+  double* Reta;   // (npoin)
+  int stage;      // 1..4
+};
+
+inline void rk_4_main(const ElemCtx& ctx, const Params& P, const double* Ml, const double* mu_factor,
+                      const double* gpvol, const double* wgp, const double* helem, const double* helem_l,
+                      double dt, State& S, Rk4Scratch& W, StageCapture* cap) {
+  const int npoin = ctx.npoin;
+  const int64_t n3 = (int64_t)npoin * 3;
+  const double a_i[4] = {0.0, 0.5, 0.5, 1.0};
+  const double b_i[4] = {1.0 / 6.0, 1.0 / 3.0, 1.0 / 3.0, 1.0 / 6.0};
+  const double g = P.gamma_gas, Rgas = P.Rgas;
+  std::fill(W.Rmass.begin(), W.Rmass.end(), 0.0);
+  std::fill(W.Rener.begin(), W.Rener.end(), 0.0);
+  std::fill(W.Rmom.begin(), W.Rmom.end(), 0.0);
+  std::fill(W.Reta.begin(), W.Reta.end(), 0.0);
+  std::fill(W.Rmass_sum.begin(), W.Rmass_sum.end(), 0.0);
+  std::fill(W.Rener_sum.begin(), W.Rener_sum.end(), 0.0);
+  std::fill(W.Reta_sum.begin(), W.Reta_sum.end(), 0.0);
+  std::fill(W.Rmom_sum.begin(), W.Rmom_sum.end(), 0.0);
+  for (int istep = 0; istep < 4; ++istep) {
+    // stage state (time_integ.f90:239-248)
+#pragma omp parallel for schedule(static)
+    for (int p = 0; p < npoin; ++p) {
+      W.aux_rho[p] = S.rho[p] - dt * a_i[istep] * W.Rmass[p];
+      W.aux_E[p] = S.E[p] - dt * a_i[istep] * W.Rener[p];
+      for (int d = 0; d < 3; ++d)
+        W.aux_q[p + (int64_t)npoin * d] = S.q[p + (int64_t)npoin * d] - dt * a_i[istep] * W.Rmom[p + (int64_t)npoin * d];
+    }
+    // EOS (time_integ.f90:266-285)
+#pragma omp parallel for schedule(static)
+    for (int p = 0; p < npoin; ++p) {
+      double umag = 0.0;
+      for (int d = 0; d < 3; ++d) {
+        W.aux_u[p + (int64_t)npoin * d] = W.aux_q[p + (int64_t)npoin * d] / W.aux_rho[p];
+        umag = umag + W.aux_u[p + (int64_t)npoin * d] * W.aux_u[p + (int64_t)npoin * d];
+      }
+      W.aux_e_int[p] = (W.aux_E[p] / W.aux_rho[p]) - 0.5 * umag;
+      W.aux_pr[p] = W.aux_rho[p] * (g - 1.0) * W.aux_e_int[p];
+      W.aux_h[p] = (g / (g - 1.0)) * W.aux_pr[p] / W.aux_rho[p];
+      W.aux_Tem[p] = W.aux_pr[p] / (W.aux_rho[p] * Rgas);
+      W.aux_eta[p] = (W.aux_rho[p] / (g - 1.0)) * std::log(W.aux_pr[p] / std::pow(W.aux_rho[p], g));
+      for (int d = 0; d < 3; ++d) W.f_eta[p + (int64_t)npoin * d] = W.aux_u[p + (int64_t)npoin * d] * W.aux_eta[p];
+    }
+    generic_scalar_convec_ijk(ctx, W.f_eta.data(), W.aux_eta.data(), W.aux_u.data(), W.Reta.data());
+    for (int p = 0; p < npoin; ++p) W.Reta[p] = W.Reta[p] / Ml[p];
+    sutherland_viscosity(npoin, W.aux_Tem.data(), mu_factor, S.mu_fluid);
+    full_diffusion_ijk(ctx, P, W.aux_rho.data(), W.aux_rho.data(), W.aux_u.data(), W.aux_Tem.data(),
+                       S.mu_fluid, S.mu_e, S.mu_sgs, W.Rdiff_mass.data(), W.Rdiff_mom.data(),
+                       W.Rdiff_ener.data());
+    full_convec_ijk(ctx, W.aux_u.data(), W.aux_q.data(), W.aux_rho.data(), W.aux_pr.data(), W.aux_h.data(),
+                    W.Rmass.data(), W.Rmom.data(), W.Rener.data());
+    for (int p = 0; p < npoin; ++p) {
+      W.Rmass[p] = W.Rmass[p] + W.Rdiff_mass[p];
+      W.Rener[p] = W.Rener[p] + W.Rdiff_ener[p];
+    }
+    for (int64_t p = 0; p < n3; ++p) W.Rmom[p] = W.Rmom[p] + W.Rdiff_mom[p];
+    for (int p = 0; p < npoin; ++p) {
+      W.Rmass[p] = W.Rmass[p] / Ml[p];
+      W.Rener[p] = W.Rener[p] / Ml[p];
+    }
+    for (int d = 0; d < 3; ++d)
+      for (int p = 0; p < npoin; ++p) W.Rmom[p + (int64_t)npoin * d] = W.Rmom[p + (int64_t)npoin * d] / Ml[p];
+    if (cap && cap->stage == istep + 1) {
+      if (cap->Rmass) std::memcpy(cap->Rmass, W.Rmass.data(), sizeof(double) * npoin);
+      if (cap->Rener) std::memcpy(cap->Rener, W.Rener.data(), sizeof(double) * npoin);
+      if (cap->Rmom) std::memcpy(cap->Rmom, W.Rmom.data(), sizeof(double) * n3);
+      if (cap->Reta) std::memcpy(cap->Reta, W.Reta.data(), sizeof(double) * npoin);
+    }
+    for (int p = 0; p < npoin; ++p) {
+      W.Rmass_sum[p] = W.Rmass_sum[p] + b_i[istep] * W.Rmass[p];
+      W.Rener_sum[p] = W.Rener_sum[p] + b_i[istep] * W.Rener[p];
+      W.Reta_sum[p] = W.Reta_sum[p] + b_i[istep] * W.Reta[p];
+      for (int d = 0; d < 3; ++d)
+        W.Rmom_sum[p + (int64_t)npoin * d] = W.Rmom_sum[p + (int64_t)npoin * d] + b_i[istep] * W.Rmom[p + (int64_t)npoin * d];
+    }
+  }
+  // RK update (time_integ.f90:417-426)
+  for (int p = 0; p < npoin; ++p) {
+    S.rho[p] = S.rho[p] - dt * W.Rmass_sum[p];
+    S.E[p] = S.E[p] - dt * W.Rener_sum[p];
+    for (int d = 0; d < 3; ++d) S.q[p + (int64_t)npoin * d] = S.q[p + (int64_t)npoin * d] - dt * W.Rmom_sum[p + (int64_t)npoin * d];
+  }
+  // EOS at the new level (time_integ.f90:445-463)
+  for (int p = 0; p < npoin; ++p) {
+    double umag = 0.0;
+    for (int d = 0; d < 3; ++d) {
+      S.u[p + (int64_t)npoin * d] = S.q[p + (int64_t)npoin * d] / S.rho[p];
+      umag = umag + S.u[p + (int64_t)npoin * d] * S.u[p + (int64_t)npoin * d];
+    }
+    S.e_int[p] = (S.E[p] / S.rho[p]) - 0.5 * umag;
+    S.pr[p] = S.rho[p] * (g - 1.0) * S.e_int[p];
+    S.csound[p] = std::sqrt(g * S.pr[p] / S.rho[p]);
+    umag = std::sqrt(umag);
+    S.machno[p] = umag / S.csound[p];
+    S.Tem[p] = S.pr[p] / (S.rho[p] * Rgas);
+    S.eta[p] = (S.rho[p] / (g - 1.0)) * std::log(S.pr[p] / std::pow(S.rho[p], g));
+  }
+  // Reta = -Reta_sum (time_integ.f90:467-471)
+  for (int p = 0; p < npoin; ++p) W.Reta[p] = -W.Reta_sum[p];
+  sutherland_viscosity(npoin, S.Tem, mu_factor, S.mu_fluid);
+  smart_visc_spectral(ctx, P, W.Reta.data(), gpvol, wgp, S.rho, S.u, S.csound, S.Tem, S.eta, helem_l, helem,
+                      S.mu_e, S.mue_l);
+}
+
+#undef SOD_INV
+#undef SOD_DL
+#undef SOD_HE
+#undef SOD_GPVOL
+
+// ------------------------------------------------------------------------------------------
+// Incompressible pressure operator and PCG (lib_sod2d_incomp).
+// eval_laplacian_mult (mod_operators.f90:20-128), eval_laplacian_diag (:417-461),
+// conjGrad_pressure_incomp (mod_solver_incomp.f90:247-434).  Pinned node lpoin_w(1) = node 0.
+// ------------------------------------------------------------------------------------------
+inline void eval_laplacian_mult(const ElemCtx& ctx, const double* p, double* ResP, std::vector<double>& auxP) {
+  const int nelem = ctx.nelem, npoin = ctx.npoin;
+  auxP.assign(p, p + npoin);
+  for (int q = 0; q < npoin; ++q) ResP[q] = 0.0;
+  auxP[0] = 0.0;
+  const ElemCtx& c = ctx;
+  for_each_element_coloured(ctx, [&](int ielem) {
+    int ipoin[nnode];
+    double pl[nnode], gradPl[nnode][3];
+    for (int a = 0; a < nnode; ++a) ipoin[a] = c.connec[ielem + (int64_t)nelem * a];
+    for (int a = 0; a < nnode; ++a) pl[a] = auxP[ipoin[a]];
+    auto INV = [&](int i, int j, int k) { return c.invAtoIJK[i + 4 * (j + 4 * k)]; };
+    auto DL = [&](int g, int d, int ii) { return c.dlxigp_ip[g + ngaus * (d + 3 * ii)]; };
+    auto HE = [&](int i, int j, int g) { return c.He[i + 3 * (j + 3 * ((int64_t)g + ngaus * (int64_t)ielem))]; };
+    auto GV = [&](int g) { return c.gpvol[g + ngaus * (int64_t)ielem]; };
+    for (int g = 0; g < ngaus; ++g) {
+      int isoI = c.gmshAtoI[g], isoJ = c.gmshAtoJ[g], isoK = c.gmshAtoK[g];
+      double gIP[3] = {0, 0, 0};
+      for (int ii = 0; ii < 4; ++ii) {
+        gIP[0] += DL(g, 0, ii) * pl[INV(ii, isoJ, isoK)];
+        gIP[1] += DL(g, 1, ii) * pl[INV(isoI, ii, isoK)];
+        gIP[2] += DL(g, 2, ii) * pl[INV(isoI, isoJ, ii)];
+      }
+      for (int id = 0; id < 3; ++id) {
+        double s = 0.0;
+        for (int jd = 0; jd < 3; ++jd) s += HE(id, jd, g) * gIP[jd];
+        gradPl[g][id] = s;
+      }
+    }
+    double out[nnode];
+    for (int g = 0; g < ngaus; ++g) {
+      int isoI = c.gmshAtoI[g], isoJ = c.gmshAtoJ[g], isoK = c.gmshAtoK[g];
+      double divDp = 0.0;
+      for (int ii = 0; ii < 4; ++ii) {
+        int a1 = INV(ii, isoJ, isoK), a2 = INV(isoI, ii, isoK), a3 = INV(isoI, isoJ, ii);
+        for (int id = 0; id < 3; ++id) {
+          divDp = divDp + HE(id, 0, a1) * GV(a1) * DL(a1, 0, isoI) * gradPl[a1][id];
+          divDp = divDp + HE(id, 1, a2) * GV(a2) * DL(a2, 1, isoJ) * gradPl[a2][id];
+          divDp = divDp + HE(id, 2, a3) * GV(a3) * DL(a3, 2, isoK) * gradPl[a3][id];
+        }
+      }
+      out[g] = divDp;
+    }
+    for (int g = 0; g < ngaus; ++g) ResP[ipoin[g]] += out[g];
+  });
+  ResP[0] = 0.0;
+}
+
+inline void eval_laplacian_diag(const ElemCtx& ctx, const double* dNgp, double* d) {
+  const int nelem = ctx.nelem, npoin = ctx.npoin;
+  for (int q = 0; q < npoin; ++q) d[q] = 0.0;
+  for (int ielem = 0; ielem < nelem; ++ielem)
+    for (int g = 0; g < ngaus; ++g) {
+      double gpcar[3][nnode];
+      for (int id = 0; id < 3; ++id)
+        for (int a = 0; a < nnode; ++a) {
+          double s = 0.0;
+          for (int jd = 0; jd < 3; ++jd)
+            s += ctx.He[id + 3 * (jd + 3 * ((int64_t)g + ngaus * (int64_t)ielem))] * dNgp[jd + 3 * (a + nnode * g)];
+          gpcar[id][a] = s;
+        }
+      double gv = ctx.gpvol[g + ngaus * (int64_t)ielem];
+      for (int id = 0; id < 3; ++id)
+        for (int a = 0; a < nnode; ++a)
+          d[ctx.connec[ielem + (int64_t)nelem * a]] += gv * gpcar[id][a] * gpcar[id][a];
+    }
+}
+
+// Returns the iteration count; R holds the right-hand side on entry and x0+x on exit.
+inline int conjGrad_pressure(const ElemCtx& ctx, const double* dNgp, const double* Rp0, double* R,
+                             int maxIter, double tol, double* final_rel) {
+  const int npoin = ctx.npoin;
+  std::vector<double> x(npoin, 0.0), r0(npoin, 0.0), p0(npoin, 0.0), qn(npoin, 0.0), b(npoin, 0.0),
+      z0(npoin, 0.0), z1(npoin, 0.0), M(npoin, 0.0), x0(npoin), diag(npoin), auxP;
+  eval_laplacian_diag(ctx, dNgp, diag.data());
+  for (int p = 0; p < npoin; ++p) { M[p] = diag[p]; x0[p] = Rp0[p]; }
+  eval_laplacian_mult(ctx, x0.data(), qn.data(), auxP);
+  for (int p = 0; p < npoin; ++p) b[p] = R[p] - qn[p];
+  b[0] = 0.0; x[0] = 0.0;
+  eval_laplacian_mult(ctx, x.data(), qn.data(), auxP);
+  for (int p = 0; p < npoin; ++p) {
+    r0[p] = b[p] - qn[p];
+    z0[p] = r0[p] / M[p];
+    p0[p] = z0[p];
+  }
+  double auxT1 = 0.0;
+  for (int p = 0; p < npoin; ++p) auxT1 += r0[p] * r0[p];
+  double auxB = std::sqrt(auxT1);
+  double T1 = 0.0;
+  int iter;
+  for (iter = 1; iter <= maxIter; ++iter) {
+    eval_laplacian_mult(ctx, p0.data(), qn.data(), auxP);
+    double Q1 = 0.0, Q2 = 0.0;
+    for (int p = 0; p < npoin; ++p) { Q1 += r0[p] * z0[p]; Q2 += p0[p] * qn[p]; }
+    double alphaCG = Q1 / Q2;
+    for (int p = 0; p < npoin; ++p) x[p] = x[p] + alphaCG * p0[p];
+    for (int p = 0; p < npoin; ++p) {
+      r0[p] = r0[p] - alphaCG * qn[p];
+      z1[p] = z0[p];
+      z0[p] = r0[p] / M[p];
+    }
+    auxT1 = 0.0;
+    for (int p = 0; p < npoin; ++p) auxT1 += r0[p] * r0[p];
+    T1 = auxT1;
+    if (std::sqrt(T1) < tol * auxB) break;
+    auxT1 = 0.0;
+    for (int p = 0; p < npoin; ++p) auxT1 += r0[p] * (z0[p] - z1[p]);
+    double betaCG = auxT1 / Q1;
+    for (int p = 0; p < npoin; ++p) p0[p] = z0[p] + betaCG * p0[p];
+  }
+  if (final_rel) *final_rel = std::sqrt(T1) / auxB;
+  for (int p = 0; p < npoin; ++p) R[p] = x0[p] + x[p];
+  return iter > maxIter ? maxIter : iter;
+}
+
+}  // namespace sod_oracle

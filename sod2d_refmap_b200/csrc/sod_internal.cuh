@@ -1,0 +1,133 @@
+// Internal declarations of libsod2d_b200 (sm_100a).  Not part of the C ABI.
+//
+// Device data layout (all element arrays in the library's own natural-ijk local order
+// d = i + 4*j + 16*k, i,j,k in ascending-coordinate order 0..3):
+//   econn   [e*64 + d]            int32 unique node id
+//   geo64   [(e*10 + c)*64 + d]   FP64: c = 0..8 He(i,j) at c = 3*i + j, c = 9 gpvol
+//   geo32   same, FP32 copy used by the mixed-precision kernels
+//   mue     [e*64 + d]            FP64 entropy viscosity; mue32 FP32 copy
+//   helem_l [e*64 + d]            FP64 min node distance; helem [e]
+//   n2e_ptr [npoin+1], n2e [64*nelem]  CSR node -> packed (e*64 + d), ascending e
+//   Node fields are SoA columns of npoin doubles (the reference's Fortran layout).
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstdio>
+#include <string>
+#include <atomic>
+#include <mutex>
+#include <unordered_map>
+#include <vector>
+#include "../../include/sod2d_b200.h"
+
+namespace sod {
+
+constexpr int P = 3;
+constexpr int NP1 = P + 1;
+constexpr int NN = NP1 * NP1 * NP1;   // 64 nodes / gauss points per element
+constexpr int NGEO = 10;              // 9 He entries + gpvol
+constexpr int NRES = 6;               // element residual fields: mass, mom x3, ener, eta
+// shared-memory field stride: 4 k-planes of 16 values, plane pitch 22 (bank-conflict free
+// for the xi/eta/zeta line reads of a 4x4x2 warp in FP64)
+constexpr int PLANE = 22;
+constexpr int FSTRIDE = 4 * PLANE;    // 88
+__host__ __device__ constexpr int sidx(int i, int j, int k) { return i + 4 * j + PLANE * k; }
+
+void set_error(const char* fmt, ...);
+extern std::atomic<int64_t> g_launches;
+
+#define SOD_CUDA(call)                                                                  \
+  do {                                                                                  \
+    cudaError_t _e = (call);                                                            \
+    if (_e != cudaSuccess) {                                                            \
+      ::sod::set_error("%s:%d %s: %s", __FILE__, __LINE__, #call, cudaGetErrorString(_e)); \
+      return SOD_ERR_CUDA;                                                              \
+    }                                                                                   \
+  } while (0)
+
+#define SOD_CHECK_LAUNCH()                                                              \
+  do {                                                                                  \
+    ::sod::g_launches.fetch_add(1, std::memory_order_relaxed);                          \
+    cudaError_t _e = cudaGetLastError();                                                \
+    if (_e != cudaSuccess) {                                                            \
+      ::sod::set_error("%s:%d kernel launch: %s", __FILE__, __LINE__, cudaGetErrorString(_e)); \
+      return SOD_ERR_CUDA;                                                              \
+    }                                                                                   \
+  } while (0)
+
+#define SOD_ARG(cond, msg)                                                              \
+  do {                                                                                  \
+    if (!(cond)) {                                                                      \
+      ::sod::set_error("invalid argument: %s", msg);                                    \
+      return SOD_ERR_ARG;                                                               \
+    }                                                                                   \
+  } while (0)
+
+struct DevParams {
+  double gamma, Rgas, Cp, Prt, ce, cmax, cglob, c_rho, c_ener, cfl_conv, cfl_diff;
+  int normalise;
+};
+
+// 1-D derivative matrix in natural order: D[m][n] = l_n'(x_m)
+struct DMat {
+  double d[NP1][NP1];
+};
+
+// Scratch owned by a mesh for the step pipeline (allocated lazily, sized by npoin/nelem).
+struct StepBuffers {
+  int64_t npoin = 0, nelem = 0;
+  double* ys = nullptr;      // stage state 5*npoin
+  double* rsum = nullptr;    // RK accumulators 6*npoin (mass, mom x3, ener, eta)
+  void* rel = nullptr;       // element residuals nelem*6*64 (double or float)
+  size_t rel_bytes = 0;
+  double* red = nullptr;     // reduction partials
+  int64_t red_cap = 0;
+  double* scal = nullptr;    // device scalars: [0] eta mean, [1] eta norm, [2] dt, [3] ...
+  unsigned int* counters = nullptr;  // last-block-done counters
+  double* mu_fluid = nullptr;        // stage Sutherland viscosity scratch (unused by fused path)
+};
+
+struct GraphEntry {
+  cudaGraphExec_t exec = nullptr;
+  int nsteps = 0;
+  int nkernels = 0;
+};
+
+}  // namespace sod
+
+struct SodMesh {
+  int32_t nelem = 0, npoin = 0;
+  int device = 0;
+  sod::DevParams prm{};
+  sod::DMat D{};
+  double wgp_nat[sod::NN];
+  int perm_a_of_d[sod::NN];   // reference local node a of library node d
+  int perm_d_of_a[sod::NN];
+  // device arrays
+  int32_t* econn = nullptr;
+  double* geo64 = nullptr;
+  float* geo32 = nullptr;
+  double* Ml = nullptr;
+  double* helem = nullptr;
+  double* helem_l = nullptr;
+  double* jratio = nullptr;  // (minJe/maxJe)^2 per element (smart_visc_spectral :76-83)
+  int32_t* n2e_ptr = nullptr;
+  int32_t* n2e = nullptr;
+  double* mue_int = nullptr;   // internal-layout entropy viscosity (FP64)
+  float* mue32 = nullptr;      // FP32 copy
+  int32_t* a_of_d_dev = nullptr;  // perm table on device (64)
+  sod::StepBuffers buf;
+  std::unordered_map<uint64_t, sod::GraphEntry> graphs;
+  int tuned_epb[2] = {0, 0};
+  std::vector<double*> host_mirror;  // device buffers of sod_rk4_main_host
+};
+
+namespace sod {
+// helpers implemented in sod_mesh.cu
+int ensure_step_buffers(SodMesh* m, bool mixed);
+int mesh_ref_to_internal_elem(SodMesh* m, const double* ref_dev /*(nelem,64) F*/, double* int_dev,
+                              cudaStream_t st);
+int mesh_internal_to_ref_elem(SodMesh* m, const double* int_dev, double* ref_dev, cudaStream_t st);
+int launch_copy_f32(const double* src, float* dst, int64_t n, cudaStream_t st);
+int init_kernel_attrs();
+}  // namespace sod

@@ -1,0 +1,246 @@
+"""Host-side mirror of the reference solver interface over the C ABI.
+
+``Sod2dMesh`` plays the role of the reference's mesh/setup phase (CFDSolverBase_run's
+evalShapeFunctions / evalJacobians / evalMass / evalCharLength, CFDSolverBase.f90:1143-1389),
+``Sod2dState`` the device-resident level-2 arrays of ``rk_4_main`` (time_integ.f90:137-193),
+and ``Sod2dMesh.rk_4_main`` / ``rk4_steps`` the time-loop call of CFDSolverPeriodic.f90:50-52.
+Device memory comes from torch (CUDA tensors are plain device buffers here); every numeric
+operation runs in libsod2d_b200.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from .mesh import BoxMesh, FlowState, TGVParams
+
+
+def _torch():
+    import torch
+    if not torch.cuda.is_available():
+        raise RuntimeError("sod2d_refmap_b200 needs a CUDA device (no CPU fallback)")
+    return torch
+
+
+def _ptr(t) -> int:
+    return 0 if t is None else int(t.data_ptr())
+
+
+def _np_ptr(a) -> C.c_void_p:
+    return C.c_void_p(a.ctypes.data) if a is not None else C.c_void_p(0)
+
+
+def _stream(stream=None) -> C.c_void_p:
+    torch = _torch()
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return C.c_void_p(int(s.cuda_stream))
+
+
+def params_struct(prm: TGVParams) -> _lib.SodParams:
+    return _lib.SodParams(prm.gamma_gas, prm.Rgas, prm.Cp, prm.Prt, prm.ce, prm.cmax, prm.cglob, prm.c_rho, prm.c_ener,
+                          int(prm.flag_normalise_entropy), prm.cfl_conv, prm.cfl_diff)
+
+
+FP64 = _lib.SOD_FP64
+MIXED = _lib.SOD_MIXED
+
+
+class Sod2dState:
+    """Device arrays of one solver state in the reference layouts (level pos=2)."""
+
+    FIELDS = ("rho", "q", "E", "u", "pr", "Tem", "e_int", "eta", "csound", "machno", "mu_fluid", "mu_factor",
+              "mu_e", "Reta")
+
+    def __init__(self, npoin: int, nelem: int, device="cuda"):
+        torch = _torch()
+        f64 = dict(dtype=torch.float64, device=device)
+        self.npoin, self.nelem = npoin, nelem
+        # (npoin,3) Fortran arrays are stored as (3,npoin) torch tensors (same memory order)
+        self.rho = torch.zeros(npoin, **f64)
+        self.q = torch.zeros(3, npoin, **f64)
+        self.E = torch.zeros(npoin, **f64)
+        self.u = torch.zeros(3, npoin, **f64)
+        self.pr = torch.zeros(npoin, **f64)
+        self.Tem = torch.zeros(npoin, **f64)
+        self.e_int = torch.zeros(npoin, **f64)
+        self.eta = torch.zeros(npoin, **f64)
+        self.csound = torch.zeros(npoin, **f64)
+        self.machno = torch.zeros(npoin, **f64)
+        self.mu_fluid = torch.zeros(npoin, **f64)
+        self.mu_factor = torch.zeros(npoin, **f64)
+        self.mu_e = torch.zeros(64, nelem, **f64)   # (nelem,64) Fortran
+        self.Reta = torch.zeros(npoin, **f64)
+        self.dt = torch.zeros(1, **f64)
+
+    @classmethod
+    def from_host(cls, st: FlowState, nelem: int) -> "Sod2dState":
+        torch = _torch()
+        s = cls(len(st.rho), nelem)
+        for name in ("rho", "E", "pr", "Tem", "e_int", "eta", "csound", "machno", "mu_fluid", "mu_factor"):
+            getattr(s, name).copy_(torch.from_numpy(np.ascontiguousarray(getattr(st, name))))
+        s.q.copy_(torch.from_numpy(np.ascontiguousarray(st.q.T)))
+        s.u.copy_(torch.from_numpy(np.ascontiguousarray(st.u.T)))
+        s.mu_e.copy_(torch.from_numpy(np.ascontiguousarray(st.mu_e.T)))
+        return s
+
+    def struct(self) -> _lib.SodState:
+        return _lib.SodState(*(_ptr(getattr(self, f)) for f in self.FIELDS))
+
+    def to_host(self) -> dict:
+        out = {}
+        for f in self.FIELDS:
+            t = getattr(self, f)
+            a = t.detach().cpu().numpy()
+            out[f] = np.asfortranarray(a.T) if t.dim() == 2 else a.copy()
+        return out
+
+
+class Sod2dMesh:
+    """A SodMesh handle built from a BoxMesh (or any reference-layout mesh arrays)."""
+
+    def __init__(self, mesh: BoxMesh, prm: TGVParams | None = None, geometry: dict | None = None):
+        _torch()
+        L = _lib.load()
+        self.box = mesh
+        self.prm = prm or TGVParams()
+        T = mesh.tables
+        self._keep = []
+        def keep(a):
+            self._keep.append(a)
+            return _np_ptr(a)
+        desc = _lib.SodMeshDesc()
+        desc.nelem, desc.npoin, desc.npoin_orig, desc.porder, desc.index_base = (
+            mesh.nelem, mesh.npoin, mesh.npoin_orig, 3, 0)
+        desc.connec = keep(np.asfortranarray(mesh.connec, dtype=np.int32))
+        desc.connec_orig = keep(np.asfortranarray(mesh.connec_orig, dtype=np.int32))
+        desc.coord_orig = keep(np.asfortranarray(mesh.coord_orig, dtype=np.float64))
+        desc.dlxigp_ip = keep(np.asfortranarray(T.dlxigp_ip))
+        desc.wgp = keep(np.ascontiguousarray(T.wgp))
+        desc.invAtoIJK = keep(np.asfortranarray(T.invAtoIJK, dtype=np.int32))
+        desc.gmshAtoI = keep(np.ascontiguousarray(T.gmshAtoI, dtype=np.int32))
+        desc.gmshAtoJ = keep(np.ascontiguousarray(T.gmshAtoJ, dtype=np.int32))
+        desc.gmshAtoK = keep(np.ascontiguousarray(T.gmshAtoK, dtype=np.int32))
+        if geometry:
+            for k in ("He", "gpvol", "Ml", "helem", "helem_l"):
+                if geometry.get(k) is not None:
+                    setattr(desc, k, keep(np.asfortranarray(geometry[k], dtype=np.float64)))
+        p = params_struct(self.prm)
+        h = C.c_void_p(0)
+        _lib.check(L.sod_mesh_create(C.byref(desc), C.byref(p), C.byref(h)))
+        self.handle = h
+        self.nelem, self.npoin = mesh.nelem, mesh.npoin
+        self._keep = []  # the library copied everything it needs
+
+    def close(self):
+        if getattr(self, "handle", None) and self.handle.value:
+            _lib.load().sod_mesh_destroy(self.handle)
+            self.handle = C.c_void_p(0)
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def geometry(self) -> dict:
+        E, N = self.nelem, self.npoin
+        out = dict(He=np.zeros((3, 3, 64, E), order="F"), gpvol=np.zeros((1, 64, E), order="F"), Ml=np.zeros(N),
+                   helem=np.zeros(E), helem_l=np.zeros((E, 64), order="F"))
+        _lib.check(_lib.load().sod_mesh_get_geometry(self.handle, *(_np_ptr(out[k]) for k in
+                                                                    ("He", "gpvol", "Ml", "helem", "helem_l"))))
+        return out
+
+    def set_params(self, prm: TGVParams):
+        self.prm = prm
+        p = params_struct(prm)
+        _lib.check(_lib.load().sod_mesh_set_params(self.handle, C.byref(p)))
+
+    # ---- time integration --------------------------------------------------------------
+    def rk_4_main(self, state: Sod2dState, precision: int = FP64, update_dt: bool = True, stream=None):
+        st = state.struct()
+        _lib.check(_lib.load().sod_rk4_main(self.handle, C.byref(st), C.c_void_p(_ptr(state.dt)),
+                                           C.c_void_p(_ptr(state.dt) if update_dt else 0), int(precision),
+                                           _stream(stream)))
+
+    def rk4_steps(self, state: Sod2dState, nsteps: int, precision: int = FP64, stream=None):
+        st = state.struct()
+        _lib.check(_lib.load().sod_rk4_steps(self.handle, C.byref(st), C.c_void_p(_ptr(state.dt)), int(nsteps),
+                                            int(precision), _stream(stream)))
+
+    def rhs(self, state: Sod2dState, precision: int = FP64, stream=None):
+        torch = _torch()
+        N = self.npoin
+        out = dict(Rmass=torch.zeros(N, dtype=torch.float64, device="cuda"),
+                   Rmom=torch.zeros(3, N, dtype=torch.float64, device="cuda"),
+                   Rener=torch.zeros(N, dtype=torch.float64, device="cuda"),
+                   Reta=torch.zeros(N, dtype=torch.float64, device="cuda"))
+        _lib.check(_lib.load().sod_rhs(self.handle, *(C.c_void_p(_ptr(t)) for t in (
+            state.rho, state.q, state.E, state.mu_e, state.mu_factor, out["Rmass"], out["Rmom"], out["Rener"],
+            out["Reta"])), int(precision), _stream(stream)))
+        return out
+
+    def adapt_dt(self, state: Sod2dState, stream=None):
+        _lib.check(_lib.load().sod_adapt_dt_cfl(self.handle, *(C.c_void_p(_ptr(t)) for t in (
+            state.u, state.csound, state.mu_fluid)), C.c_void_p(0), C.c_void_p(_ptr(state.rho)),
+            C.c_void_p(_ptr(state.dt)), _stream(stream)))
+        return state.dt
+
+    # ---- per-routine entry points (reference argument lists) ----------------------------
+    def full_convec_ijk(self, u, q, rho, pr, E, stream=None):
+        torch = _torch()
+        N = self.npoin
+        Rm = torch.empty(N, dtype=torch.float64, device="cuda")
+        Rmo = torch.empty(3, N, dtype=torch.float64, device="cuda")
+        Re = torch.empty(N, dtype=torch.float64, device="cuda")
+        _lib.check(_lib.load().sod_full_convec_ijk(self.handle, *(C.c_void_p(_ptr(t)) for t in (
+            u, q, rho, pr, E, Rm, Rmo, Re)), _stream(stream)))
+        return Rm, Rmo, Re
+
+    def generic_scalar_convec_ijk(self, f, eta, u, stream=None):
+        torch = _torch()
+        R = torch.empty(self.npoin, dtype=torch.float64, device="cuda")
+        _lib.check(_lib.load().sod_generic_scalar_convec_ijk(self.handle, *(C.c_void_p(_ptr(t)) for t in (
+            f, eta, u, R)), _stream(stream)))
+        return R
+
+    def full_diffusion_ijk(self, rho_n, rho, u, Tem, mu_fluid, mu_e, mu_sgs=None, stream=None):
+        torch = _torch()
+        N = self.npoin
+        Rm = torch.empty(N, dtype=torch.float64, device="cuda")
+        Rmo = torch.empty(3, N, dtype=torch.float64, device="cuda")
+        Re = torch.empty(N, dtype=torch.float64, device="cuda")
+        _lib.check(_lib.load().sod_full_diffusion_ijk(self.handle, C.c_double(self.prm.Cp), C.c_double(self.prm.Prt),
+                                                     *(C.c_void_p(_ptr(t)) for t in (rho_n, rho, u, Tem, mu_fluid,
+                                                                                     mu_e, mu_sgs, Rm, Rmo, Re)),
+                                                     _stream(stream)))
+        return Rm, Rmo, Re
+
+    def lumped_solver(self, R, stream=None):
+        ncomp = 3 if R.dim() == 2 else 1
+        _lib.check(_lib.load().sod_lumped_solver(self.handle, C.c_void_p(_ptr(R)), ncomp, _stream(stream)))
+        return R
+
+    def smart_visc_spectral(self, Reta, rho, u, csound, Tem, eta, stream=None):
+        torch = _torch()
+        mu_e = torch.zeros(64, self.nelem, dtype=torch.float64, device="cuda")
+        _lib.check(_lib.load().sod_smart_visc_spectral(self.handle, *(C.c_void_p(_ptr(t)) for t in (
+            Reta, rho, u, csound, Tem, eta, mu_e)), _stream(stream)))
+        return mu_e
+
+
+def sutherland_viscosity(Tem, mu_factor, stream=None):
+    torch = _torch()
+    mu = torch.empty_like(Tem)
+    _lib.check(_lib.load().sod_sutherland_viscosity(int(Tem.numel()), C.c_void_p(_ptr(Tem)), C.c_void_p(_ptr(mu_factor)),
+                                                   C.c_void_p(_ptr(mu)), _stream(stream)))
+    return mu
+
+
+def csr_spmv_scal(rdom, cdom, Mc, v, stream=None):
+    torch = _torch()
+    u = torch.empty(rdom.numel() - 1, dtype=torch.float64, device="cuda")
+    _lib.check(_lib.load().sod_csr_spmv_scal(int(u.numel()), int(Mc.numel()), *(C.c_void_p(_ptr(t)) for t in (
+        rdom, cdom, Mc, v, u)), _stream(stream)))
+    return u
