@@ -1,0 +1,381 @@
+"""Benchmark: SOD2D explicit spectral-element RHS (HEX64, p=3) on B200.
+
+Workload (config "c1"): triply periodic [0,2pi]^3 box of 64^3 HEX64 elements
+(7,077,888 unique nodes, 5 conserved fields), nodes jittered by a seeded Gaussian
+(sigma = 0.05 x GLL node spacing, periodic-consistent), Taylor-Green vortex + seeded
++-1e-3 velocity perturbation, Re=1600, Ma=0.1, entropy viscosity on, dt from CFL 0.5.
+A "step" is one explicit RK4 step (4 RHS stages + lumped-mass update + entropy viscosity
++ next dt), timed as K graph-replayed steps.  Metric: Gdof.stage/s = 5*N*4*K / time.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--n 64]
+
+--impl reference times the CPU restatement of the reference loops (the Fortran reference
+cannot be built in this image: no Fortran compiler, MPI or HDF5) on all host cores.
+Multi-GPU runs are independent replicas (the path has no inter-GPU exchange on one GPU's
+scope): value = total node-stages of all ranks / max-over-ranks time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "RHS Gdof.stage/s (mixed FP32-element/FP64-assembly; FP64 alongside)"
+UNIT = "Gdof.stage/s"
+
+
+def _peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d.get("hbm_gbs", 6650.0)), "measured"
+    return 6650.0, "fallback"
+
+
+def _workload(n: int):
+    from sod2d_refmap_b200 import mesh as M
+    m = M.periodic_box(n, jitter=0.05, seed=1)
+    prm = M.TGVParams()
+    st = M.taylor_green_state(m, prm, pert_amp=1e-3, seed=0)
+    return M, m, prm, st
+
+
+def _config(n: int, m, extra: dict | None = None) -> dict:
+    c = {"workload": f"c1: TGV periodic {n}^3 HEX64 (p=3), jittered 0.05 node spacing, RK4 steps",
+         "elements": m.nelem, "nodes": m.npoin, "dofs": 5 * m.npoin, "porder": 3,
+         "l2": "inputs larger than L2 (state+geometry > 2 GB vs 126 MB L2)", "parallelism": "replicas"}
+    if extra:
+        c.update(extra)
+    return c
+
+
+# ------------------------------------------------------------------------------------------
+# CPU sample: one RK4 step of the CPU restatement on a slab of element layers of the same mesh
+# ------------------------------------------------------------------------------------------
+def _slab_oracle(m, prm, st, layers: int):
+    """Oracle mesh restricted to the first `layers` element layers in z of mesh m (geometry
+    computed by the oracle for those elements, state sliced to their nodes)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    from sod2d_refmap_b200 import mesh as M
+    n = m.n
+    E = n * n * layers
+    conn = np.asarray(m.connec[:E], dtype=np.int64)
+    nodes, inv = np.unique(conn, return_inverse=True)
+    sub = M.BoxMesh(n=n, L=m.L, nelem=E, npoin=len(nodes), npoin_orig=m.npoin_orig,
+                    connec=np.asfortranarray(inv.reshape(E, 64).astype(np.int32)),
+                    connec_orig=np.asfortranarray(m.connec_orig[:E]), coord=np.asfortranarray(m.coord[nodes]),
+                    coord_orig=m.coord_orig, master=m.master, tables=m.tables)
+    om = O.OracleMesh(sub, colour=False)
+    # colour classes of the slab (parity in x, y, z) so the scatter stays race-free in parallel
+    e = np.arange(E)
+    ex, ey, ez = e % n, (e // n) % n, e // (n * n)
+    col = (ex % 2) + 2 * (ey % 2) + 4 * (ez % 2)
+    order = np.argsort(col, kind="stable").astype(np.int32)
+    ptrs = np.concatenate([[0], np.cumsum(np.bincount(col, minlength=8))]).astype(np.int32)
+    om.cptr, om.celems = ptrs, order
+    om.ctx.ncolors = 8
+    om.ctx.color_ptr = O.ptr(om.cptr).value
+    om.ctx.color_elems = O.ptr(om.celems).value
+    s = st.copy()
+    for k in ("rho", "E", "pr", "Tem", "e_int", "eta", "csound", "machno", "mu_fluid", "mu_factor"):
+        setattr(s, k, np.ascontiguousarray(getattr(st, k)[nodes]))
+    s.u = np.asfortranarray(st.u[nodes]); s.q = np.asfortranarray(st.q[nodes])
+    s.mu_e = np.zeros((E, 64), order="F"); s.mu_sgs = np.zeros((E, 64), order="F")
+    return O, om, s
+
+
+def cpu_sample(m, prm, st, layers: int, reps: int, threads: int):
+    """Times `reps` RK4 steps of the oracle on the slab; returns (Gdof.stage/s, seconds, desc)."""
+    O, om, s = _slab_oracle(m, prm, st, layers)
+    threads = O.set_threads(threads)
+    dt = O.adapt_dt(om, s, prm)
+    O.rk4(om, prm, s.copy(), dt, 1)  # warm-up
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        O.rk4(om, prm, s, dt, 1)
+    sec = time.perf_counter() - t0
+    node_stages = 27 * om.nelem * 4 * reps   # 27 unique nodes per element of the periodic box
+    desc = (f"{reps} RK4 step(s) of the CPU restatement on a {layers}-layer slab "
+            f"({om.nelem} elements = {27 * om.nelem} node-equivalents) of the same mesh")
+    return 5 * node_stages / sec / 1e9, sec, desc, threads
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    M, m, prm, st = _workload(args.n)
+    layers = args.ref_layers
+    O, om, s = _slab_oracle(m, prm, st, layers)
+    threads = O.set_threads(os.cpu_count() or 1)
+    dt = O.adapt_dt(om, s, prm)
+    for _ in range(args.warmup):
+        O.rk4(om, prm, s, dt, 1)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        O.rk4(om, prm, s, dt, 1)
+        times.append(time.perf_counter() - t0)
+    tot = sum(times)
+    node_stages = 27 * om.nelem * 4 * args.steps
+    value = 5 * node_stages / tot / 1e9
+    sample = (f"each step: one RK4 step of the CPU restatement of the reference loops (oracle/, OpenMP, "
+              f"{threads} threads) on a {layers}-layer slab ({om.nelem} elements) of the {args.n}^3 mesh")
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded TGV on a generated periodic HEX64 mesh)",
+            "config": _config(args.n, m, {"sample_elements": om.nelem}),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "note": "the Fortran/OpenACC reference needs a Fortran compiler, MPI and HDF5, absent here; "
+                    "this arm times its line-by-line C++ restatement"}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ------------------------------------------------------------------------------------------
+# GPU arm
+# ------------------------------------------------------------------------------------------
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms while the timed region runs."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        time.sleep(0.5)  # let the sampler start before the timed region
+        return self
+
+    def __exit__(self, *exc):
+        self.lines = []
+        if self.proc:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [ln for ln in out.splitlines() if ln.strip()]
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in getattr(self, "lines", []):
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def _rel_l2(a, b):
+    a = a.double().flatten(); b = b.double().flatten()
+    nb = float(b.norm())
+    return float((a - b).norm()) / (nb if nb > 0 else 1.0)
+
+
+def kr_bytes_per_launch(nelem: int, npoin: int, mixed: bool) -> float:
+    """Algorithmic HBM bytes of one fused-RHS launch: per element the geometry (9 He + gpvol),
+    mu_e and connectivity read and the 6x64 element residuals written; per node the 5
+    conserved fields and mu_factor read once."""
+    r = 4 if mixed else 8
+    per_elem = 64 * (10 * r + r + 4 + 6 * r)
+    per_node = 6 * 8
+    return per_elem * nelem + per_node * npoin
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    torch.cuda.set_device(local)
+    from sod2d_refmap_b200 import solver as S, _lib
+    M, m, prm, st0 = _workload(args.n)
+    gm = S.Sod2dMesh(m, prm)
+    base = S.Sod2dState.from_host(st0, gm.nelem)
+    gm.adapt_dt(base)
+    torch.cuda.synchronize()
+    dt0 = float(base.dt.item())
+    stream = torch.cuda.current_stream()
+    N, K, W = m.npoin, args.steps, args.warmup
+
+    def fresh():
+        s = S.Sod2dState(gm.npoin, gm.nelem)
+        for f in S.Sod2dState.FIELDS + ("dt",):
+            getattr(s, f).copy_(getattr(base, f))
+        return s
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    results = {}
+    states = {}
+    clocks = None
+    for prec, name in ((S.FP64, "fp64"), (S.MIXED, "mixed")):
+        s = fresh()
+        gm.rk4_steps(s, W, precision=prec)          # warm-up (also captures the graph)
+        s = fresh()
+        torch.cuda.synchronize(); barrier(); torch.cuda.synchronize()
+        l0 = _lib.launch_count()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with ClockSampler(torch.cuda.current_device()) as cs:
+            ev0.record(stream)
+            gm.rk4_steps(s, K, precision=prec)
+            ev1.record(stream)
+            torch.cuda.synchronize()
+        barrier(); torch.cuda.synchronize()
+        ms = ev0.elapsed_time(ev1)
+        launches = _lib.launch_count() - l0
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        if world > 1:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        results[name] = dict(ms=float(t.item()), launches=launches)
+        states[name] = s
+        if name == "mixed":
+            clocks = cs.summary()
+    # accuracy of the mixed path against the FP64 path after K steps (same start, same dt0)
+    acc = {k: _rel_l2(getattr(states["mixed"], k), getattr(states["fp64"], k)) for k in ("rho", "q", "E")}
+    s = fresh()
+    r64 = gm.rhs(s, precision=S.FP64)
+    r32 = gm.rhs(s, precision=S.MIXED)
+    acc_rhs = {k: _rel_l2(r32[k], r64[k]) for k in r64}
+    # per-kernel durations (CUDA events on the launching stream, eager steps)
+    prof = {}
+    for prec, name in ((S.FP64, "fp64"), (S.MIXED, "mixed")):
+        s = fresh()
+        prof[name] = gm.step_profile(s, 5, precision=prec)
+    # end to end through the host-buffer C-ABI call (pinned host arrays, copies in the timed region)
+    e2e = None
+    if rank == 0 or True:
+        host = {}
+        for f in S.Sod2dState.FIELDS:
+            t_ = getattr(base, f)
+            h = torch.empty(t_.shape, dtype=torch.float64, pin_memory=True)
+            h.copy_(t_)
+            host[f] = h.numpy()
+        host["Reta"] = None
+        n_e2e = max(3, min(K, 10))
+        gm.rk4_main_host(host, dt0, precision=S.MIXED)
+        torch.cuda.synchronize(); barrier()
+        t0 = time.perf_counter()
+        dt = dt0
+        for _ in range(n_e2e):
+            dt = gm.rk4_main_host(host, dt, precision=S.MIXED)
+        sec = time.perf_counter() - t0
+        tt = torch.tensor([sec], device="cuda", dtype=torch.float64)
+        if world > 1:
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        sec = float(tt.item())
+        E_ = gm.nelem
+        h2d = 8 * (N + 3 * N + N + N) + 8 * 64 * E_ + 8
+        d2h = 8 * (N + 3 * N + N + 3 * N + 7 * N) + 8 * 64 * E_ + 8
+        e2e = {"value": 5 * N * 4 * n_e2e * world / sec / 1e9, "unit": UNIT, "h2d_bytes_per_step": h2d,
+               "d2h_bytes_per_step": d2h, "steps": n_e2e, "precision": "mixed",
+               "api": "sod_rk4_main_host (host arrays in the reference layouts)"}
+    value = 5 * N * 4 * K * world / (results["mixed"]["ms"] / 1e3) / 1e9
+    value64 = 5 * N * 4 * K * world / (results["fp64"]["ms"] / 1e3) / 1e9
+    hbm, peak_kind = _peaks()
+    kr_ms = prof["mixed"][0]
+    kr_bytes = kr_bytes_per_launch(gm.nelem, N, True)
+    achieved = kr_bytes / (kr_ms / 1e3) / 1e9
+    kr64_bytes = kr_bytes_per_launch(gm.nelem, N, False)
+    roof = {"bound": "hbm", "kernel": "k_rhs_fused<float,true,4> (fused element RHS, mixed)",
+            "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+            "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)" if peak_kind == "measured" else "fallback 6650 GB/s",
+            "traffic": None, "bytes_per_launch": kr_bytes, "ms_per_launch": kr_ms,
+            "fp64_kernel": {"ms_per_launch": prof["fp64"][0], "bytes_per_launch": kr64_bytes,
+                            "achieved_GBs": kr64_bytes / (prof["fp64"][0] / 1e3) / 1e9},
+            "kernel_ms": {"mixed": {"rhs": prof["mixed"][0], "gather_rk": prof["mixed"][1], "visc_dt": prof["mixed"][2]},
+                          "fp64": {"rhs": prof["fp64"][0], "gather_rk": prof["fp64"][1], "visc_dt": prof["fp64"][2]}}}
+    tr = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tr):
+        with open(tr) as f:
+            tj = json.load(f)
+        per_elem = tj.get("k_rhs_fused_mixed_bytes_per_element")
+        if per_elem:
+            roof["traffic"] = per_elem * gm.nelem
+            roof["traffic_source"] = tj.get("source")
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        v, sec, desc, thr = cpu_sample(m, prm, st0, layers=args.cpu_layers, reps=args.cpu_reps,
+                                       threads=os.cpu_count() or 1)
+        cpu = {"value": v, "unit": UNIT, "cores": thr, "kind": "port", "sample": desc, "seconds": sec}
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
+                "ms_per_step": results["mixed"]["ms"] / K, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32-element/f64-assembly",
+                "data": "synthetic (seeded TGV on a generated periodic HEX64 mesh)",
+                "config": _config(args.n, m, {"dt0": dt0}),
+                "fp64": {"value": value64, "ms_per_step": results["fp64"]["ms"] / K, "dtype": "f64",
+                         "speedup_mixed_over_fp64": value / value64},
+                "mixed_rel_l2_vs_fp64": {"state_after_steps": acc, "rhs_stage": acc_rhs},
+                "gpu_launches": results["mixed"]["launches"],
+                "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks}
+        print(json.dumps(line), flush=True)
+    for s in states.values():
+        del s
+    gm.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=64)
+    ap.add_argument("--cpu-layers", type=int, default=4)
+    ap.add_argument("--cpu-reps", type=int, default=10)
+    ap.add_argument("--ref-layers", type=int, default=1)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -134,6 +134,12 @@ int sod_rk4_main(SodMesh* mesh, SodState* state, const double* dt_dev, double* d
 int sod_rk4_steps(SodMesh* mesh, SodState* state, double* dt_dev, int nsteps, SodPrecision prec,
                   sod_stream_t stream);
 
+/* nsteps eager steps with CUDA events around every kernel; ms_out[0..2] receive the mean
+ * duration of one fused-RHS launch, one gather/RK-stage launch and one entropy-viscosity+dt
+ * launch.  Used for the live roofline figures. */
+int sod_step_profile(SodMesh* mesh, SodState* state, double* dt_dev, int nsteps, SodPrecision prec,
+                     sod_stream_t stream, float* ms_out);
+
 /* Host-buffer variant of sod_rk4_main for the CPU-side drop-in (the reference's CPU build
  * calls rk_4_main on host arrays): copies rho,q,E,mu_e,mu_factor in, runs one step and copies
  * rho,q,E,u,pr,Tem,e_int,eta,csound,machno,mu_fluid,mu_e back.  dt_host in, dt_next_host out. */

@@ -55,6 +55,7 @@ _SIGS = {
     "sod_rk4_main": (_i, [_p, _p, _p, _p, _i, _p]),
     "sod_rk4_steps": (_i, [_p, _p, _p, _i, _i, _p]),
     "sod_rk4_main_host": (_i, [_p, _p, _d, _p, _i, _p]),
+    "sod_step_profile": (_i, [_p, _p, _p, _i, _i, _p, _p]),
     "sod_rhs": (_i, [_p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _i, _p]),
     "sod_smart_visc_spectral": (_i, [_p, _p, _p, _p, _p, _p, _p, _p, _p]),
     "sod_adapt_dt_cfl": (_i, [_p, _p, _p, _p, _p, _p, _p, _p]),

@@ -43,6 +43,7 @@ struct GeoArgs {
   double* helem;
   double* helem_l;
   double* jratio;
+  int* bad;                   // set to 1 when some detJ <= 0 (inverted or degenerate gauss point)
 };
 
 __global__ void __launch_bounds__(64) k_geometry(const GeoArgs a) {
@@ -80,6 +81,7 @@ __global__ void __launch_bounds__(64) k_geometry(const GeoArgs a) {
   b[2] = Je[0][1] * Je[1][2] - Je[1][1] * Je[0][2];
   b[5] = -(Je[0][0] * Je[1][2] - Je[1][0] * Je[0][2]);
   b[8] = Je[0][0] * Je[1][1] - Je[1][0] * Je[0][1];
+  if (!(det > 0.0)) atomicOr(a.bad, 1);
   const double inv = 1.0 / det;
   double* G = a.geo64 + (int64_t)e * NGEO * NN;
 #pragma unroll
@@ -374,7 +376,10 @@ int sod_mesh_create(const SodMeshDesc* desc, const SodParams* params, SodMesh** 
       }
     int32_t* dco = nullptr;
     double* dxyz = nullptr;
+    int* dbad = nullptr;
     ALLOC(dco, sizeof(int32_t) * E * NN);
+    ALLOC(dbad, sizeof(int));
+    cudaMemset(dbad, 0, sizeof(int));
     if (cudaMalloc(&dxyz, sizeof(double) * 3 * (size_t)desc->npoin_orig) != cudaSuccess) {
       cudaFree(dco);
       set_error("cudaMalloc coord failed");
@@ -386,15 +391,22 @@ int sod_mesh_create(const SodMeshDesc* desc, const SodParams* params, SodMesh** 
     ga.nelem = E; ga.conn_orig = dco; ga.coord = dxyz; ga.npoin_orig = desc->npoin_orig; ga.D = m->D;
     for (int d = 0; d < NN; ++d) ga.w[d] = m->wgp_nat[d];
     for (int c = 0; c < 8; ++c) ga.corner_d[c] = m->perm_d_of_a[c];
-    ga.geo64 = m->geo64; ga.helem = m->helem; ga.helem_l = m->helem_l; ga.jratio = m->jratio;
+    ga.geo64 = m->geo64; ga.helem = m->helem; ga.helem_l = m->helem_l; ga.jratio = m->jratio; ga.bad = dbad;
     k_geometry<<<E, 64>>>(ga);
     g_launches.fetch_add(1);
     cudaError_t err = cudaDeviceSynchronize();
+    int hbad = 0;
+    cudaMemcpy(&hbad, dbad, sizeof(int), cudaMemcpyDeviceToHost);
     cudaFree(dco);
     cudaFree(dxyz);
+    cudaFree(dbad);
     if (err != cudaSuccess) {
       set_error("k_geometry: %s", cudaGetErrorString(err));
       return fail(SOD_ERR_CUDA);
+    }
+    if (hbad && !(desc->He && desc->gpvol)) {
+      set_error("invalid argument: non-positive Jacobian determinant at some gauss point (inverted element)");
+      return fail(SOD_ERR_ARG);
     }
   }
   if (have_geo) {

@@ -803,8 +803,10 @@ static double* reta_scratch(SodMesh* m) {
   return m->buf.rsum + 5 * (size_t)m->npoin;  // rsum eta column is dead after stage 4 reads it
 }
 
-// One RK4 step on device state (mu_e already in m->mue_int / mue32).
-int run_step(SodMesh* m, SodState* s, const double* dt_dev, double* dt_next, bool mixed, cudaStream_t st) {
+// One RK4 step on device state (mu_e already in m->mue_int / mue32).  When ev is non-null,
+// ev[2*slot] / ev[2*slot+1] bracket each kernel: slots 0-3 KR stages, 4-7 KG stages, 8 KV.
+int run_step(SodMesh* m, SodState* s, const double* dt_dev, double* dt_next, bool mixed, cudaStream_t st,
+             cudaEvent_t* ev = nullptr) {
   const size_t N = m->npoin;
   const int epb = m->tuned_epb[mixed ? 1 : 0] ? m->tuned_epb[mixed ? 1 : 0] : (mixed ? 4 : 2);
   SodState loc = *s;
@@ -821,18 +823,24 @@ int run_step(SodMesh* m, SodState* s, const double* dt_dev, double* dt_next, boo
     const double* src_q1 = stage == 1 ? s->q + N : m->buf.ys + 2 * N;
     const double* src_q2 = stage == 1 ? s->q + 2 * N : m->buf.ys + 3 * N;
     const double* src_E = stage == 1 ? s->E : m->buf.ys + 4 * N;
+    if (ev) cudaEventRecord(ev[2 * (stage - 1)], st);
     rc = launch_rhs(m, mixed, epb, src_rho, src_q0, src_q1, src_q2, src_E, s->mu_factor, nullptr, st);
     if (rc) return rc;
+    if (ev) cudaEventRecord(ev[2 * (stage - 1) + 1], st);
     GatherArgs g{};
     g.dt = dt_dev;
     g.y[0] = s->rho; g.y[1] = s->q; g.y[2] = s->q + N; g.y[3] = s->q + 2 * N; g.y[4] = s->E;
     g.u0 = s->u; g.u1 = s->u + N; g.u2 = s->u + 2 * N;
     g.pr = s->pr; g.Tem = s->Tem; g.e_int = s->e_int; g.eta = s->eta; g.csound = s->csound;
     g.machno = s->machno; g.mu_fluid = s->mu_fluid; g.Reta = loc.Reta; g.mu_factor = s->mu_factor;
+    if (ev) cudaEventRecord(ev[2 * (3 + stage)], st);
     rc = launch_gather(m, mixed, stage, g, st);
     if (rc) return rc;
+    if (ev) cudaEventRecord(ev[2 * (3 + stage) + 1], st);
   }
+  if (ev) cudaEventRecord(ev[16], st);
   rc = launch_visc_dt(m, &loc, dt_next, mixed ? m->mue32 : nullptr, st);
+  if (ev) cudaEventRecord(ev[17], st);
   return rc;
 }
 
@@ -921,6 +929,43 @@ int sod_rk4_steps(SodMesh* m, SodState* s, double* dt_dev, int nsteps, SodPrecis
       g_launches.fetch_add(it->second.nkernels);
     }
   }
+  return mesh_internal_to_ref_elem(m, m->mue_int, s->mu_e, st);
+}
+
+int sod_step_profile(SodMesh* m, SodState* s, double* dt_dev, int nsteps, SodPrecision prec, sod_stream_t stream,
+                     float* ms_out) {
+  int rc = check_state(m, s);
+  if (rc) return rc;
+  SOD_ARG(dt_dev && nsteps > 0 && ms_out, "dt_dev/nsteps/ms_out");
+  SOD_ARG(prec == SOD_FP64 || prec == SOD_MIXED, "precision");
+  cudaStream_t st = (cudaStream_t)stream;
+  const bool mixed = prec == SOD_MIXED;
+  rc = ensure_step_buffers(m, mixed);
+  if (rc) return rc;
+  rc = mesh_ref_to_internal_elem(m, s->mu_e, m->mue_int, st);
+  if (rc) return rc;
+  if (mixed) {
+    rc = launch_copy_f32(m->mue_int, m->mue32, (int64_t)m->nelem * NN, st);
+    if (rc) return rc;
+  }
+  cudaEvent_t ev[18];
+  for (int q = 0; q < 18; ++q) SOD_CUDA(cudaEventCreate(&ev[q]));
+  double acc[3] = {0, 0, 0};
+  for (int t = 0; t < nsteps && rc == SOD_OK; ++t) {
+    rc = run_step(m, s, dt_dev, dt_dev, mixed, st, ev);
+    if (rc) break;
+    if (cudaEventSynchronize(ev[17]) != cudaSuccess) { rc = SOD_ERR_CUDA; break; }
+    for (int q = 0; q < 9; ++q) {
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, ev[2 * q], ev[2 * q + 1]);
+      acc[q < 4 ? 0 : (q < 8 ? 1 : 2)] += ms;
+    }
+  }
+  for (int q = 0; q < 18; ++q) cudaEventDestroy(ev[q]);
+  if (rc) return rc;
+  ms_out[0] = (float)(acc[0] / (4.0 * nsteps));
+  ms_out[1] = (float)(acc[1] / (4.0 * nsteps));
+  ms_out[2] = (float)(acc[2] / nsteps);
   return mesh_internal_to_ref_elem(m, m->mue_int, s->mu_e, st);
 }
 

@@ -169,6 +169,22 @@ class Sod2dMesh:
         _lib.check(_lib.load().sod_rk4_steps(self.handle, C.byref(st), C.c_void_p(_ptr(state.dt)), int(nsteps),
                                             int(precision), _stream(stream)))
 
+    def step_profile(self, state: Sod2dState, nsteps: int, precision: int = FP64, stream=None):
+        """Mean ms per launch of (fused RHS, gather/RK stage, entropy viscosity + dt)."""
+        ms = (C.c_float * 3)()
+        st = state.struct()
+        _lib.check(_lib.load().sod_step_profile(self.handle, C.byref(st), C.c_void_p(_ptr(state.dt)), int(nsteps),
+                                               int(precision), _stream(stream), ms))
+        return tuple(float(x) for x in ms)
+
+    def rk4_main_host(self, host: dict, dt: float, precision: int = FP64, stream=None) -> float:
+        """sod_rk4_main_host on host arrays (numpy, reference layouts; pinned for speed)."""
+        st = _lib.SodState(*(int(host[f].ctypes.data) if host.get(f) is not None else 0 for f in Sod2dState.FIELDS))
+        dtn = C.c_double(0.0)
+        _lib.check(_lib.load().sod_rk4_main_host(self.handle, C.byref(st), C.c_double(dt), C.byref(dtn),
+                                                int(precision), _stream(stream)))
+        return dtn.value
+
     def rhs(self, state: Sod2dState, precision: int = FP64, stream=None):
         torch = _torch()
         N = self.npoin

@@ -37,7 +37,8 @@ def test_jitter_periodic_consistent():
     for c in range(3):
         d = np.zeros(m.npoin); d[m.master] = disp[:, c]
         assert np.allclose(disp[:, c], d[m.master])
-    assert np.abs(disp).max() <= 3 * 0.05 * m.L / 4 + 1e-15
+    hnode = (1 - 1 / np.sqrt(5)) / 2 * m.L / 4
+    assert np.abs(disp).max() <= 3 * 0.05 * hnode + 1e-15
 
 
 def test_splitmix_deterministic():
