@@ -184,6 +184,27 @@ int sod_lumped_solver(SodMesh* mesh, double* R, int ncomp, sod_stream_t stream);
 int sod_sutherland_viscosity(int32_t npoin, const double* Tem, const double* mu_factor,
                              double* mu_fluid, sod_stream_t stream);
 
+/* Allocation-free full_convec_ijk, for callers that cannot allocate device memory: host codes
+ * whose device memory is owned by the OpenACC runtime or by their own fixed pool (as SOD2D's
+ * GPU build keeps its arrays in OpenACC present tables / managed memory) cannot create a
+ * SodMesh, which allocates.  This entry point has no counterpart in the reference; it computes
+ * what sod_full_convec_ijk / full_convec_ijk compute from the reference-layout device arrays
+ * alone (connec(nelem,64), He(3,3,64,nelem), gpvol(1,64,nelem), dlxigp_ip(64,3,4),
+ * gmshAtoI/J/K(64); ids index_base-based) and allocates nothing.  Its scratch (element
+ * residuals and the node->element gather map, about 14 MB) is one static device array that
+ * each GPU loading the library holds until exit, which limits a call to
+ * SOD_NOALLOC_MAX_ELEM elements and 64*SOD_NOALLOC_MAX_ELEM nodes (larger: SOD_ERR_ARG).
+ * All calls share that array: calls that overlap on the GPU race.  The first call on a
+ * device looks up the array's address; make it before any stream capture.  The call waits
+ * for its stream to finish so it can report bad node ids. */
+#define SOD_NOALLOC_MAX_ELEM 4096
+int sod_full_convec_ijk_noalloc(int32_t nelem, int32_t npoin, int32_t index_base, const int32_t* connec,
+                                const double* He, const double* gpvol, const double* dlxigp_ip,
+                                const int32_t* gmshAtoI, const int32_t* gmshAtoJ, const int32_t* gmshAtoK,
+                                const double* u, const double* q, const double* rho, const double* pr,
+                                const double* E, double* Rmass, double* Rmom, double* Rener,
+                                sod_stream_t stream);
+
 /* ---- Legacy unit-test API ----------------------------------------------------------- */
 
 /* CSR_SpMV_scal (legacy API pinned by unitt/unitt_CSR_SPMV_scal/unitt_CSR_SPMV_scal.f90:14-52):

@@ -60,6 +60,7 @@ _SIGS = {
     "sod_smart_visc_spectral": (_i, [_p, _p, _p, _p, _p, _p, _p, _p, _p]),
     "sod_adapt_dt_cfl": (_i, [_p, _p, _p, _p, _p, _p, _p, _p]),
     "sod_full_convec_ijk": (_i, [_p, _p, _p, _p, _p, _p, _p, _p, _p, _p]),
+    "sod_full_convec_ijk_noalloc": (_i, [C.c_int32, C.c_int32, C.c_int32] + [_p] * 16),
     "sod_generic_scalar_convec_ijk": (_i, [_p, _p, _p, _p, _p, _p]),
     "sod_full_diffusion_ijk": (_i, [_p, _d, _d, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p]),
     "sod_lumped_solver": (_i, [_p, _p, _i, _p]),
