@@ -140,6 +140,11 @@ int sod_rk4_steps(SodMesh* mesh, SodState* state, double* dt_dev, int nsteps, So
 int sod_step_profile(SodMesh* mesh, SodState* state, double* dt_dev, int nsteps, SodPrecision prec,
                      sod_stream_t stream, float* ms_out);
 
+/* Autotuner of the fused RHS kernel: times elements-per-CTA candidates ({1,2,4} FP64,
+ * {1,2,4,8} mixed) on the given state and keeps the fastest for this mesh and precision. */
+int sod_autotune(SodMesh* mesh, SodState* state, SodPrecision prec, int* best_epb, float* best_ms,
+                 sod_stream_t stream);
+
 /* Host-buffer variant of sod_rk4_main for the CPU-side drop-in (the reference's CPU build
  * calls rk_4_main on host arrays): copies rho,q,E,mu_e,mu_factor in, runs one step and copies
  * rho,q,E,u,pr,Tem,e_int,eta,csound,machno,mu_fluid,mu_e back.  dt_host in, dt_next_host out. */

@@ -73,6 +73,24 @@ struct DMat {
   double d[NP1][NP1];
 };
 
+// Arguments of the fused element-RHS kernels.
+struct RhsArgs {
+  int nelem;
+  const int32_t* __restrict__ econn;
+  const void* geo;                 // R [e][10][64]
+  const void* mue;                 // R [e][64]
+  const double* __restrict__ musgs;  // FP64 [e][64] or null
+  const double* __restrict__ rho;
+  const double* __restrict__ q0;
+  const double* __restrict__ q1;
+  const double* __restrict__ q2;
+  const double* __restrict__ E;
+  const double* __restrict__ mu_factor;  // per node
+  void* rel;                       // R [e][6][64]
+  DMat D;
+  DevParams prm;
+};
+
 // Scratch owned by a mesh for the step pipeline (allocated lazily, sized by npoin/nelem).
 struct StepBuffers {
   int64_t npoin = 0, nelem = 0;
@@ -130,4 +148,7 @@ int mesh_ref_to_internal_elem(SodMesh* m, const double* ref_dev /*(nelem,64) F*/
 int mesh_internal_to_ref_elem(SodMesh* m, const double* int_dev, double* ref_dev, cudaStream_t st);
 int launch_copy_f32(const double* src, float* dst, int64_t n, cudaStream_t st);
 int init_kernel_attrs();
+// packed-FP32 (FFMA2) variant of the mixed fused RHS kernel (sod_rhs_mixed.cu)
+int launch_rhs_mixed2(const RhsArgs& a, int epb, cudaStream_t st);
+int init_rhs_mixed2_attrs();
 }  // namespace sod

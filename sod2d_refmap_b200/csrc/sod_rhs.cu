@@ -31,23 +31,6 @@ namespace sod {
 constexpr double kSuthC1 = 0.000001458;
 constexpr double kSuthS = 110.4;
 
-struct RhsArgs {
-  int nelem;
-  const int32_t* __restrict__ econn;
-  const void* geo;                 // R [e][10][64]
-  const void* mue;                 // R [e][64]
-  const double* __restrict__ musgs;  // FP64 [e][64] or null
-  const double* __restrict__ rho;
-  const double* __restrict__ q0;
-  const double* __restrict__ q1;
-  const double* __restrict__ q2;
-  const double* __restrict__ E;
-  const double* __restrict__ mu_factor;  // per node
-  void* rel;                       // R [e][6][64]
-  DMat D;
-  DevParams prm;
-};
-
 template <typename R>
 __device__ __forceinline__ void giso(const R* __restrict__ f, int i, int j, int k, const R* Dx, const R* Dy,
                                      const R* Dz, R& gx, R& gy, R& gz) {
@@ -447,7 +430,23 @@ __global__ void __launch_bounds__(256) k_gather_rk(const GatherArgs a) {
     const R* rel = reinterpret_cast<const R*>(a.rel);
     double r[6] = {0, 0, 0, 0, 0, 0};
     const int beg = a.ptr[n], end = a.ptr[n + 1];
-    for (int c = beg; c < end; ++c) {
+    int c = beg;
+    // groups of 4 contributions: all loads issued before the (ascending, fixed-order) sums
+    for (; c + 4 <= end; c += 4) {
+      R v[4][6];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int pk = a.idx[c + q];
+        const R* src = rel + (size_t)(pk >> 6) * NRES * NN + (pk & 63);
+#pragma unroll
+        for (int f = 0; f < 6; ++f) v[q][f] = src[f * NN];
+      }
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
+#pragma unroll
+        for (int f = 0; f < 6; ++f) r[f] += (double)v[q][f];
+    }
+    for (; c < end; ++c) {
       const int pk = a.idx[c];
       const R* src = rel + (size_t)(pk >> 6) * NRES * NN + (pk & 63);
 #pragma unroll
@@ -518,6 +517,7 @@ __global__ void __launch_bounds__(256) k_gather_rk(const GatherArgs a) {
       __threadfence();
       // fixed-order final reduction by the last block (deterministic)
       double ts = 0.0, tmx = -1e300, tmn = 1e300;
+#pragma unroll 4
       for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x) {
         ts += __ldcg(a.red + 3 * b);
         tmx = fmax(tmx, __ldcg(a.red + 3 * b + 1));
@@ -563,8 +563,7 @@ struct ViscArgs {
   const double* __restrict__ scal;   // [0] mean, [1] norm
   double* mue;                       // out FP64 [e][64]
   float* mue32;                      // optional FP32 copy
-  double* red;                       // dt partials [nblocks]
-  unsigned int* counter;
+  double* dt_bits;                   // scratch scalar receiving the min dt (bits, pre-set large)
   double* dt_out;                    // device scalar (may be null)
   DevParams prm;
 };
@@ -574,26 +573,30 @@ __device__ __forceinline__ int nb_filter(int x) {
   return (x < 0) ? 1 : ((x > 3) ? 1 : x);
 }
 
-__global__ void __launch_bounds__(128) k_visc_dt(const ViscArgs a) {
-  constexpr int EPB = 2;
-  __shared__ double ml[EPB][NN];
-  __shared__ double dtb[EPB];
-  __shared__ bool last;
+constexpr int KV_EPB = 4;
+
+__global__ void __launch_bounds__(64 * KV_EPB) k_visc_dt(const ViscArgs a) {
+  __shared__ double ml[KV_EPB][NN];
+  __shared__ double wm[KV_EPB][2][5];
+  __shared__ double elem_s[KV_EPB][2];  // ced, dt limit of the element
   const int es = threadIdx.x >> 6, d = threadIdx.x & 63;
-  const int e = blockIdx.x * EPB + es;
+  const int e = blockIdx.x * KV_EPB + es;
   const bool act = e < a.nelem;
   const int ee = act ? e : a.nelem - 1;
   const int n = a.econn[(size_t)ee * NN + d];
   const double rho = a.rho[n], u0 = a.u0[n], u1 = a.u1[n], u2 = a.u2[n], cs = a.csound[n], T = a.Tem[n];
   const double vmag = sqrt(u0 * u0 + u1 * u1 + u2 * u2);
   const double he = a.helem[ee];
-  const double beta_n = (rho * he) * (a.prm.cmax / 3.0) * (vmag + sqrt(a.prm.Rgas * a.prm.gamma * T));
+  // betae node term (mod_entropy_viscosity.f90:90-95)
+  const double beta_n = (rho * he) * (a.prm.cmax / (double)P) * (vmag + sqrt(a.prm.Rgas * a.prm.gamma * T));
+  // CFL node terms (mod_time_ops.f90:36-50)
   const double umax = fmax(fmax(fabs(u0), fabs(u1)), fabs(u2));
   const double L3n = umax + cs;
   const double musgs = a.musgs ? a.musgs[(size_t)ee * NN + d] : 0.0;
   const double mun = (rho * musgs + a.mu_fluid[n]) / rho;
   // element maxima over the 64 nodes (two warps per element)
   double mV = vmag, mC = cs, mB = beta_n, mL = L3n, mM = mun;
+#pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
     mV = fmax(mV, __shfl_xor_sync(0xffffffffu, mV, o));
     mC = fmax(mC, __shfl_xor_sync(0xffffffffu, mC, o));
@@ -601,73 +604,52 @@ __global__ void __launch_bounds__(128) k_visc_dt(const ViscArgs a) {
     mL = fmax(mL, __shfl_xor_sync(0xffffffffu, mL, o));
     mM = fmax(mM, __shfl_xor_sync(0xffffffffu, mM, o));
   }
-  __shared__ double wm[EPB][2][5];
   const int wi = d >> 5;
   if ((d & 31) == 0) { wm[es][wi][0] = mV; wm[es][wi][1] = mC; wm[es][wi][2] = mB; wm[es][wi][3] = mL; wm[es][wi][4] = mM; }
   __syncthreads();
-  mV = fmax(wm[es][0][0], wm[es][1][0]);
-  mC = fmax(wm[es][0][1], wm[es][1][1]);
+  if (d == 0) {
+    // shock sensor and cap, once per element (mod_entropy_viscosity.f90:81-84); M**15 as an
+    // integer power like the reference
+    const double M = fmax(wm[es][0][0], wm[es][1][0]) / fmax(wm[es][0][1], wm[es][1][1]);
+    const double M2 = M * M, M4 = M2 * M2, M8 = M4 * M4;
+    const double M15 = M8 * M4 * M2 * M;
+    const double ceM = fmax(tanh(M15 * 3.141592653589793), a.prm.ce);
+    double ced = fmax(1.0 - a.jratio[ee], a.prm.ce);
+    elem_s[es][0] = fmax(ced, ceM);
+    const double hh = he / (double)(2.0 * P + 1);
+    const double L3 = fmax(wm[es][0][3], wm[es][1][3]);
+    const double maxMU = fmax(wm[es][0][4], wm[es][1][4]);
+    elem_s[es][1] = fmin(a.prm.cfl_conv * hh / L3, a.prm.cfl_diff * (hh * hh) / maxMU);
+  }
+  __syncthreads();
+  const double ced = elem_s[es][0];
   mB = fmax(wm[es][0][2], wm[es][1][2]);
-  mL = fmax(wm[es][0][3], wm[es][1][3]);
-  mM = fmax(wm[es][0][4], wm[es][1][4]);
-  const double v_pi = 2.0 * asin(1.0);
-  const double M = mV / mC;
-  const double ceM = fmax(tanh(pow(M, 15.0) * v_pi), a.prm.ce);
-  double ced = fmax(1.0 - a.jratio[ee], a.prm.ce);
-  ced = fmax(ced, ceM);
   const double norm = a.scal[1];
   const double R1 = (norm > 0.0) ? rho * fabs(a.Reta[n]) / norm : 0.0;
   const double hl = a.helem_l[(size_t)ee * NN + d];
   const double Ve = ced * R1 * hl * hl;
   ml[es][d] = a.prm.cglob * fmin(Ve, mB);
   __syncthreads();
+  // 3x3x3 filter with weights (1/4,1/2,1/4) through convertIJK (mod_entropy_viscosity.f90:102-120)
   const int i = d & 3, j = (d >> 2) & 3, k = d >> 4;
+  const int ix[3] = {nb_filter(i - 1), i, nb_filter(i + 1)};
+  const int jx[3] = {nb_filter(j - 1), j, nb_filter(j + 1)};
+  const int kx[3] = {nb_filter(k - 1), k, nb_filter(k + 1)};
   const double w[3] = {0.25, 0.5, 0.25};
   double acc = 0.0;
 #pragma unroll
-  for (int l = -1; l <= 1; ++l)
+  for (int l = 0; l < 3; ++l)
 #pragma unroll
-    for (int mm = -1; mm <= 1; ++mm)
+    for (int mm = 0; mm < 3; ++mm)
 #pragma unroll
-      for (int nn = -1; nn <= 1; ++nn)
-        acc = acc + w[l + 1] * w[mm + 1] * w[nn + 1] * ml[es][nb_filter(i + l) + 4 * nb_filter(j + mm) + 16 * nb_filter(k + nn)];
+      for (int nn = 0; nn < 3; ++nn)
+        acc = acc + w[l] * w[mm] * w[nn] * ml[es][ix[l] + 4 * jx[mm] + 16 * kx[nn]];
   if (act) {
     a.mue[(size_t)e * NN + d] = acc;
     if (a.mue32) a.mue32[(size_t)e * NN + d] = (float)acc;
-  }
-  // dt (mod_time_ops.f90:43-54)
-  if (a.dt_out) {
-    if (d == 0) {
-      const double hh = he / (double)(2.0 * P + 1);
-      const double dtc = a.prm.cfl_conv * hh / mL;
-      const double dtd = a.prm.cfl_diff * (hh * hh) / mM;
-      dtb[es] = act ? fmin(dtc, dtd) : 1e300;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      double mn = dtb[0];
-      for (int q = 1; q < EPB; ++q) mn = fmin(mn, dtb[q]);
-      a.red[blockIdx.x] = mn;
-      __threadfence();
-      unsigned int done = atomicAdd(a.counter, 1u);
-      last = (done == gridDim.x - 1);
-    }
-    __syncthreads();
-    if (last) {
-      __threadfence();
-      double mn = 1e300;
-      for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x) mn = fmin(mn, __ldcg(a.red + b));
-      for (int o = 16; o > 0; o >>= 1) mn = fmin(mn, __shfl_xor_sync(0xffffffffu, mn, o));
-      __shared__ double wmn[4];
-      if ((threadIdx.x & 31) == 0) wmn[threadIdx.x >> 5] = mn;
-      __syncthreads();
-      if (threadIdx.x == 0) {
-        double r = wmn[0];
-        for (int q = 1; q < (int)(blockDim.x >> 5); ++q) r = fmin(r, wmn[q]);
-        *a.dt_out = r;
-        *a.counter = 0u;
-      }
-    }
+    // next dt: order-independent min over elements on the bit pattern of a positive double
+    if (a.dt_out && d == 0)
+      atomicMin(reinterpret_cast<unsigned long long*>(a.dt_bits), (unsigned long long)__double_as_longlong(elem_s[es][1]));
   }
 }
 
@@ -685,8 +667,7 @@ int init_kernel_attrs() {
   static bool done = false;
   if (done) return SOD_OK;
   int rc = set_rhs_attr<double, false, 1>() | set_rhs_attr<double, false, 2>() | set_rhs_attr<double, false, 4>() |
-           set_rhs_attr<float, true, 1>() | set_rhs_attr<float, true, 2>() | set_rhs_attr<float, true, 4>() |
-           set_rhs_attr<float, true, 8>();
+           init_rhs_mixed2_attrs();
   if (rc) return SOD_ERR_CUDA;
   done = true;
   return SOD_OK;
@@ -722,12 +703,7 @@ int launch_rhs(SodMesh* m, bool mixed, int epb, const double* rho, const double*
       default: return launch_rhs_t<double, false, 2>(a, st);
     }
   } else {
-    switch (epb) {
-      case 1: return launch_rhs_t<float, true, 1>(a, st);
-      case 2: return launch_rhs_t<float, true, 2>(a, st);
-      case 8: return launch_rhs_t<float, true, 8>(a, st);
-      default: return launch_rhs_t<float, true, 4>(a, st);
-    }
+    return launch_rhs_mixed2(a, epb, st);
   }
 }
 
@@ -788,13 +764,14 @@ int launch_visc_dt(SodMesh* m, const SodState* s, double* dt_out, float* mue32, 
   v.scal = m->buf.scal;
   v.mue = m->mue_int;
   v.mue32 = mue32;
-  v.red = m->buf.red;
-  v.counter = m->buf.counters + 1;
+  v.dt_bits = m->buf.scal + 3;
   v.dt_out = dt_out;
   v.prm = m->prm;
-  const int grid = (m->nelem + 1) / 2;
-  k_visc_dt<<<grid, 128, 0, st>>>(v);
+  if (dt_out) SOD_CUDA(cudaMemsetAsync(v.dt_bits, 0x7F, sizeof(double), st));  // 1.38e306
+  const int grid = (m->nelem + KV_EPB - 1) / KV_EPB;
+  k_visc_dt<<<grid, 64 * KV_EPB, 0, st>>>(v);
   SOD_CHECK_LAUNCH();
+  if (dt_out) SOD_CUDA(cudaMemcpyAsync(dt_out, v.dt_bits, sizeof(double), cudaMemcpyDeviceToDevice, st));
   return SOD_OK;
 }
 
@@ -967,6 +944,56 @@ int sod_step_profile(SodMesh* m, SodState* s, double* dt_dev, int nsteps, SodPre
   ms_out[1] = (float)(acc[1] / (4.0 * nsteps));
   ms_out[2] = (float)(acc[2] / nsteps);
   return mesh_internal_to_ref_elem(m, m->mue_int, s->mu_e, st);
+}
+
+// Elements-per-CTA autotuner for the fused RHS kernel: times every candidate on the caller's
+// state (3 warm-up + 10 timed launches each, CUDA events on the stream) and keeps the fastest
+// for this mesh and precision; later steps and newly captured graphs use it.
+int sod_autotune(SodMesh* m, SodState* s, SodPrecision prec, int* best_epb, float* best_ms, sod_stream_t stream) {
+  int rc = check_state(m, s);
+  if (rc) return rc;
+  SOD_ARG(prec == SOD_FP64 || prec == SOD_MIXED, "precision");
+  cudaStream_t st = (cudaStream_t)stream;
+  const bool mixed = prec == SOD_MIXED;
+  rc = ensure_step_buffers(m, mixed);
+  if (rc) return rc;
+  rc = mesh_ref_to_internal_elem(m, s->mu_e, m->mue_int, st);
+  if (rc) return rc;
+  if (mixed) {
+    rc = launch_copy_f32(m->mue_int, m->mue32, (int64_t)m->nelem * NN, st);
+    if (rc) return rc;
+  }
+  const size_t N = m->npoin;
+  const int fp64_cand[] = {1, 2, 4};
+  const int mixed_cand[] = {1, 2, 4, 8};
+  const int* cand = mixed ? mixed_cand : fp64_cand;
+  const int nc = mixed ? 4 : 3;
+  cudaEvent_t e0, e1;
+  SOD_CUDA(cudaEventCreate(&e0));
+  SOD_CUDA(cudaEventCreate(&e1));
+  int best = 0;
+  float bms = 1e30f;
+  for (int c = 0; c < nc && rc == SOD_OK; ++c) {
+    for (int r = 0; r < 3 && rc == SOD_OK; ++r)
+      rc = launch_rhs(m, mixed, cand[c], s->rho, s->q, s->q + N, s->q + 2 * N, s->E, s->mu_factor, nullptr, st);
+    cudaEventRecord(e0, st);
+    for (int r = 0; r < 10 && rc == SOD_OK; ++r)
+      rc = launch_rhs(m, mixed, cand[c], s->rho, s->q, s->q + N, s->q + 2 * N, s->E, s->mu_factor, nullptr, st);
+    cudaEventRecord(e1, st);
+    if (rc) break;
+    if (cudaEventSynchronize(e1) != cudaSuccess) { rc = SOD_ERR_CUDA; break; }
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    ms /= 10.f;
+    if (ms < bms) { bms = ms; best = cand[c]; }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc) return rc;
+  m->tuned_epb[mixed ? 1 : 0] = best;
+  if (best_epb) *best_epb = best;
+  if (best_ms) *best_ms = bms;
+  return SOD_OK;
 }
 
 int sod_rhs(SodMesh* m, const double* rho, const double* q, const double* E, const double* mu_e,

@@ -1,0 +1,376 @@
+// Mixed-precision fused element RHS with packed FP32 arithmetic (sm_100a FFMA2).
+//
+// Same mathematics as k_rhs_fused<float, true, EPB> in sod_rhs.cu (the reference element loops
+// of full_convec_ijk elem_convec.f90:211-460, full_diffusion_ijk elem_diffu.f90:12-198 and
+// generic_scalar_convec_ijk elem_convec.f90:462-570, FP32 on deviation fields), with the
+// nodal fields staged in shared memory as float2 pairs: one 8-byte shared load and one packed
+// __ffma2_rn serve two fields, and the xi-lines are read as two 16-byte loads.  Pairing:
+//   batch A  (rho',p') (u0',u1') (u2',q0') (q1',q2') (h',rho h') (k',rho k') (eta',T')
+//   batch BC (fe,fue)x3 (fk,fuk)x3 (feta,F0.)x3 (F1.,F2.)x3 (Fuu0.,Fuu1.)x3 (Fuu22,0)
+//   pass 2   (gradRho^,tauU^)x3 (gradT^,tauX^)x3 (tauY^,tauZ^)x3   (one slot per direction)
+// where F = (q-q_r) x (u-u_r), Fuu = (u-u_r) x (u-u_r) and ^ marks contravariant fluxes.
+#include "sod_internal.cuh"
+#include <cmath>
+
+namespace sod {
+namespace mx2 {
+
+constexpr double kC1 = 0.000001458;
+constexpr double kS = 110.4;
+constexpr int NA = 7;    // batch A slots
+constexpr int NBC = 16;  // batch B+C slots
+constexpr int NP2 = 9;   // pass-2 slots
+constexpr int NSLOT = NBC + NP2;  // batch A reuses the first NA slots of the BC area
+constexpr int NREF = 16;
+
+__host__ __device__ constexpr size_t smem_bytes(int epb) {
+  return sizeof(double) * (size_t)epb * NREF + sizeof(float2) * (size_t)epb * NSLOT * FSTRIDE;
+}
+
+__device__ __forceinline__ float2 F2(float a) { return make_float2(a, a); }
+__device__ __forceinline__ float2 FMA2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 MUL2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 ADD2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+
+// iso derivatives of a field pair: xi-line as two 16-byte loads, eta/zeta lines as 8-byte loads
+__device__ __forceinline__ void giso2(const float2* __restrict__ f, int i, int j, int k, const float2* Dx,
+                                      const float2* Dy, const float2* Dz, float2& gx, float2& gy, float2& gz) {
+  const float2* fx = f + 4 * j + PLANE * k;
+  const float4 a01 = *reinterpret_cast<const float4*>(fx);
+  const float4 a23 = *reinterpret_cast<const float4*>(fx + 2);
+  gx = MUL2(Dx[0], make_float2(a01.x, a01.y));
+  gx = FMA2(Dx[1], make_float2(a01.z, a01.w), gx);
+  gx = FMA2(Dx[2], make_float2(a23.x, a23.y), gx);
+  gx = FMA2(Dx[3], make_float2(a23.z, a23.w), gx);
+  const float2* fy = f + i + PLANE * k;
+  gy = MUL2(Dy[0], fy[0]);
+  gy = FMA2(Dy[1], fy[4], gy);
+  gy = FMA2(Dy[2], fy[8], gy);
+  gy = FMA2(Dy[3], fy[12], gy);
+  const float2* fz = f + i + 4 * j;
+  gz = MUL2(Dz[0], fz[0]);
+  gz = FMA2(Dz[1], fz[PLANE], gz);
+  gz = FMA2(Dz[2], fz[2 * PLANE], gz);
+  gz = FMA2(Dz[3], fz[3 * PLANE], gz);
+}
+
+// physical gradient component r of a pair: He(r,0) gx + He(r,1) gy + He(r,2) gz
+__device__ __forceinline__ float2 physr(const float2* H2, int r, float2 gx, float2 gy, float2 gz) {
+  return FMA2(H2[3 * r + 2], gz, FMA2(H2[3 * r + 1], gy, MUL2(H2[3 * r], gx)));
+}
+
+// weak divergence of a pair: sum_m D[m][i] fx(m,j,k) + D[m][j] fy(i,m,k) + D[m][k] fz(i,j,m)
+__device__ __forceinline__ float2 divT2(const float2* fx, const float2* fy, const float2* fz, int i, int j, int k,
+                                        const float2* DTx, const float2* DTy, const float2* DTz) {
+  const float2* ax = fx + 4 * j + PLANE * k;
+  const float4 a01 = *reinterpret_cast<const float4*>(ax);
+  const float4 a23 = *reinterpret_cast<const float4*>(ax + 2);
+  float2 s = MUL2(DTx[0], make_float2(a01.x, a01.y));
+  s = FMA2(DTx[1], make_float2(a01.z, a01.w), s);
+  s = FMA2(DTx[2], make_float2(a23.x, a23.y), s);
+  s = FMA2(DTx[3], make_float2(a23.z, a23.w), s);
+  const float2* ay = fy + i + PLANE * k;
+  float2 t = MUL2(DTy[0], ay[0]);
+  t = FMA2(DTy[1], ay[4], t);
+  t = FMA2(DTy[2], ay[8], t);
+  t = FMA2(DTy[3], ay[12], t);
+  const float2* az = fz + i + 4 * j;
+  float2 u = MUL2(DTz[0], az[0]);
+  u = FMA2(DTz[1], az[PLANE], u);
+  u = FMA2(DTz[2], az[2 * PLANE], u);
+  u = FMA2(DTz[3], az[3 * PLANE], u);
+  return ADD2(ADD2(s, t), u);
+}
+
+template <int EPB>
+__global__ void __launch_bounds__(64 * EPB, (EPB >= 8 ? 1 : 8 / EPB)) k_rhs_mixed2(const RhsArgs a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double* refs_all = reinterpret_cast<double*>(smem_raw);
+  float2* buf_all = reinterpret_cast<float2*>(smem_raw + sizeof(double) * EPB * NREF);
+  const int tid = threadIdx.x;
+  const int es = tid >> 6;
+  const int d = tid & 63;
+  const int i = d & 3, j = (d >> 2) & 3, k = d >> 4;
+  const int e = blockIdx.x * EPB + es;
+  const bool active = e < a.nelem;
+  const int ee = active ? e : a.nelem - 1;
+  double* refs = refs_all + es * NREF;
+  float2* buf = buf_all + (size_t)es * NSLOT * FSTRIDE;
+  float2* p2 = buf + NBC * FSTRIDE;
+  const int s_me = sidx(i, j, k);
+  const float* geo = reinterpret_cast<const float*>(a.geo) + (size_t)ee * NGEO * NN;
+
+  float2 Dx[4], Dy[4], Dz[4];
+#pragma unroll
+  for (int m = 0; m < 4; ++m) {
+    Dx[m] = F2((float)a.D.d[i][m]);
+    Dy[m] = F2((float)a.D.d[j][m]);
+    Dz[m] = F2((float)a.D.d[k][m]);
+  }
+  float H[9];
+#pragma unroll
+  for (int c = 0; c < 9; ++c) H[c] = geo[c * NN + d];
+  const float gpv = geo[9 * NN + d];
+  float2 H2[9];
+#pragma unroll
+  for (int c = 0; c < 9; ++c) H2[c] = F2(H[c]);
+
+  // ---- own node: stage EOS in FP64 (time_integ.f90:266-285)
+  const int32_t n = a.econn[(size_t)ee * NN + d];
+  const double g = a.prm.gamma;
+  const double rho = a.rho[n];
+  const double qv[3] = {a.q0[n], a.q1[n], a.q2[n]};
+  const double Et = a.E[n];
+  // one FP64 reciprocal serves every division of the EOS (the deviations below need FP64)
+  const double irho = 1.0 / rho;
+  const double uv[3] = {qv[0] * irho, qv[1] * irho, qv[2] * irho};
+  const double umag = uv[0] * uv[0] + uv[1] * uv[1] + uv[2] * uv[2];
+  const double kk = 0.5 * umag;
+  const double e_int = Et * irho - 0.5 * umag;
+  const double p = rho * (g - 1.0) * e_int;
+  const double h = (g / (g - 1.0)) * p * irho;
+  const double T = p * irho * (1.0 / a.prm.Rgas);
+  const float mufac = (float)a.mu_factor[n];
+  const float mue = reinterpret_cast<const float*>(a.mue)[(size_t)ee * NN + d];
+  const double musgs = a.musgs ? a.musgs[(size_t)ee * NN + d] : 0.0;
+
+  // element references: FP64 values of local node 0
+  if (d == 0) {
+    refs[0] = rho; refs[1] = uv[0]; refs[2] = uv[1]; refs[3] = uv[2];
+    refs[4] = qv[0]; refs[5] = qv[1]; refs[6] = qv[2]; refs[7] = p; refs[8] = h; refs[9] = kk;
+    const double L = log(p) - g * log(rho);
+    refs[10] = (rho / (g - 1.0)) * L;
+    refs[11] = T;
+    refs[12] = L;
+  }
+  __syncthreads();
+  const double r_rho = refs[0], r_p = refs[7], r_h = refs[8], r_k = refs[9], r_eta = refs[10], r_T = refs[11],
+               r_L = refs[12];
+  const double r_u[3] = {refs[1], refs[2], refs[3]};
+  const double r_q[3] = {refs[4], refs[5], refs[6]};
+  const double s_h = h - r_h, s_k = kk - r_k;
+  // eta - eta_r = ((rho-rho_r) L_r + rho (L - L_r)) / (gamma-1), L - L_r by log1p of small ratios
+  const float drho = (float)(rho - r_rho);
+  const float dL = log1pf((float)((p - r_p) / r_p)) - (float)g * log1pf(drho / (float)r_rho);
+  const double s_eta = ((double)drho * r_L + rho * (double)dL) / (g - 1.0);
+  const float Tf = (float)T;
+  const float muf = mufac * (float)kC1 * (Tf * sqrtf(Tf)) / (Tf + (float)kS);
+  const float su[3] = {(float)(uv[0] - r_u[0]), (float)(uv[1] - r_u[1]), (float)(uv[2] - r_u[2])};
+  const float sq[3] = {(float)(qv[0] - r_q[0]), (float)(qv[1] - r_q[1]), (float)(qv[2] - r_q[2])};
+
+  // ---- batch A (7 pairs)
+  buf[0 * FSTRIDE + s_me] = make_float2((float)(rho - r_rho), (float)(p - r_p));
+  buf[1 * FSTRIDE + s_me] = make_float2(su[0], su[1]);
+  buf[2 * FSTRIDE + s_me] = make_float2(su[2], sq[0]);
+  buf[3 * FSTRIDE + s_me] = make_float2(sq[1], sq[2]);
+  buf[4 * FSTRIDE + s_me] = make_float2((float)s_h, (float)(rho * s_h));
+  buf[5 * FSTRIDE + s_me] = make_float2((float)s_k, (float)(rho * s_k));
+  buf[6 * FSTRIDE + s_me] = make_float2((float)s_eta, (float)(T - r_T));
+  __syncthreads();
+
+  float gradRho[3], gradP[3], gradU[3][3], gradQ[3][3], gradH[3], gradRH[3], gradK[3], gradRK[3], gradEta[3],
+      gradT[3];
+  {
+    float2 gx, gy, gz, o;
+#define SOD_PAIR_GRAD(slot, A, B)                                              \
+    giso2(buf + (slot) * FSTRIDE, i, j, k, Dx, Dy, Dz, gx, gy, gz);            \
+    _Pragma("unroll") for (int r = 0; r < 3; ++r) {                            \
+      o = physr(H2, r, gx, gy, gz);                                            \
+      A[r] = o.x;                                                              \
+      B[r] = o.y;                                                              \
+    }
+    SOD_PAIR_GRAD(0, gradRho, gradP)
+    SOD_PAIR_GRAD(1, gradU[0], gradU[1])
+    SOD_PAIR_GRAD(2, gradU[2], gradQ[0])
+    SOD_PAIR_GRAD(3, gradQ[1], gradQ[2])
+    SOD_PAIR_GRAD(4, gradH, gradRH)
+    SOD_PAIR_GRAD(5, gradK, gradRK)
+    SOD_PAIR_GRAD(6, gradEta, gradT)
+#undef SOD_PAIR_GRAD
+  }
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    gradRH[c] += (float)r_h * gradRho[c];
+    gradRK[c] += (float)r_k * gradRho[c];
+  }
+  const float divU = gradU[0][0] + gradU[1][1] + gradU[2][2];
+  const float divQ = gradQ[0][0] + gradQ[1][1] + gradQ[2][2];
+  const float rhoR = (float)rho, hR = (float)h, kR = (float)kk;
+  const float etaR = (float)(r_eta + s_eta);
+  const float uR[3] = {(float)uv[0], (float)uv[1], (float)uv[2]};
+  const float qR[3] = {(float)qv[0], (float)qv[1], (float)qv[2]};
+  const float rhR = (float)(rho * h), rkR = (float)(rho * kk);
+
+  // ---- convective terms available after batch A (elem_convec.f90:412-432) + reference parts
+  float Rm = 0.5f * (divQ + rhoR * divU);
+  float Ren = 0.25f * (hR * divQ + rhR * divU) + 0.25f * (kR * divQ + rkR * divU);
+  float Rmo[3];
+  float Ret = 0.5f * (etaR * divU);
+  {
+    const float rh = (float)r_h, rk = (float)r_k, re = (float)r_eta;
+    Ren += 0.25f * (rh * divQ + rhoR * (rh * divU)) + 0.25f * (rk * divQ + rhoR * (rk * divU));
+    Ret += 0.5f * (re * divU);
+  }
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    Rmo[c] = 0.25f * (uR[c] * divQ + qR[c] * divU) + gradP[c];
+    Rm += 0.5f * (uR[c] * gradRho[c]);
+    Ren += 0.25f * (qR[c] * gradH[c] + uR[c] * gradRH[c] + (hR * uR[c]) * gradRho[c]) +
+           0.25f * (qR[c] * gradK[c] + uR[c] * gradRK[c] + (kR * uR[c]) * gradRho[c]);
+    Ret += 0.5f * (uR[c] * gradEta[c]);
+    float dF = (float)r_q[c] * divU, dFuu = (float)r_u[c] * divU;
+#pragma unroll
+    for (int jd = 0; jd < 3; ++jd) {
+      Rmo[c] += 0.25f * ((uR[c] * uR[jd]) * gradRho[jd] + qR[jd] * gradU[c][jd] + uR[jd] * gradQ[c][jd]);
+      dF += (float)r_u[jd] * gradQ[c][jd];
+      dFuu += (float)r_u[jd] * gradU[c][jd];
+    }
+    Rmo[c] += 0.25f * (dF + rhoR * dFuu);
+  }
+
+  // ---- diffusion pass 1 (elem_diffu.f90:70-140) -> contravariant flux pairs per direction
+  {
+    const float mufgp = muf + (float)(rho * musgs);
+    const float mut = mufgp + mue;
+    const float twoThirds = 2.0f / 3.0f;
+    float tau[3][3];
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) tau[r][c] = mut * (gradU[r][c] + gradU[c][r]);
+#pragma unroll
+    for (int r = 0; r < 3; ++r) tau[r][r] = tau[r][r] - mufgp * twoThirds * divU;
+    float tauU[3];
+#pragma unroll
+    for (int r = 0; r < 3; ++r) tauU[r] = tau[r][0] * uR[0] + tau[r][1] * uR[1] + tau[r][2] * uR[2];
+    const float2 g2 = F2(gpv);
+    auto emit = [&](int slot0, const float* Va, const float* Vb) {
+#pragma unroll
+      for (int dir = 0; dir < 3; ++dir) {
+        float2 v = MUL2(H2[0 + dir], make_float2(Va[0], Vb[0]));
+        v = FMA2(H2[3 + dir], make_float2(Va[1], Vb[1]), v);
+        v = FMA2(H2[6 + dir], make_float2(Va[2], Vb[2]), v);
+        p2[(slot0 + dir) * FSTRIDE + s_me] = MUL2(g2, v);
+      }
+    };
+    emit(0, gradRho, tauU);
+    emit(3, gradT, tau[0]);
+    emit(6, tau[1], tau[2]);
+  }
+  __syncthreads();  // batch A reads done
+
+  // ---- batch B+C (16 pairs)
+  {
+    const float sh = (float)s_h, sk = (float)s_k, se = (float)s_eta;
+    const float rsh = (float)(rho * s_h), rsk = (float)(rho * s_k);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      buf[(0 + c) * FSTRIDE + s_me] = make_float2(rsh * uR[c], sh * uR[c]);
+      buf[(3 + c) * FSTRIDE + s_me] = make_float2(rsk * uR[c], sk * uR[c]);
+      buf[(6 + c) * FSTRIDE + s_me] = make_float2(se * uR[c], sq[0] * su[c]);
+      buf[(9 + c) * FSTRIDE + s_me] = make_float2(sq[1] * su[c], sq[2] * su[c]);
+      buf[(12 + c) * FSTRIDE + s_me] = make_float2(su[0] * su[c], su[1] * su[c]);
+    }
+    buf[15 * FSTRIDE + s_me] = make_float2(su[2] * su[2], 0.0f);
+  }
+  __syncthreads();
+  {
+    // divergence of a pair of 3-vectors held in slots s0..s0+2
+    auto div2 = [&](int s0) {
+      float2 acc = make_float2(0.f, 0.f);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        float2 gx, gy, gz;
+        giso2(buf + (s0 + c) * FSTRIDE, i, j, k, Dx, Dy, Dz, gx, gy, gz);
+        acc = FMA2(H2[3 * c + 2], gz, FMA2(H2[3 * c + 1], gy, FMA2(H2[3 * c], gx, acc)));
+      }
+      return acc;
+    };
+    const float2 dA = div2(0);   // (div fe, div fue)
+    const float2 dB = div2(3);   // (div fk, div fuk)
+    const float2 dC = div2(6);   // (div feta, div F0.)
+    const float2 dD = div2(9);   // (div F1., div F2.)
+    Ren += 0.25f * (dA.x + rhoR * dA.y) + 0.25f * (dB.x + rhoR * dB.y);
+    Ret += 0.5f * dC.x;
+    // Fuu rows 0,1 from slots 12..14 and row 2 from (Fuu02, Fuu12, Fuu22)
+    float2 dE = make_float2(0.f, 0.f);
+    float dFuu2 = 0.f;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      float2 gx, gy, gz;
+      giso2(buf + (12 + c) * FSTRIDE, i, j, k, Dx, Dy, Dz, gx, gy, gz);
+      dE = FMA2(H2[3 * c + 2], gz, FMA2(H2[3 * c + 1], gy, FMA2(H2[3 * c], gx, dE)));
+      if (c == 2) {
+        dFuu2 += H[0] * gx.x + H[1] * gy.x + H[2] * gz.x;   // d/dx_0 Fuu20 (= Fuu02)
+        dFuu2 += H[3] * gx.y + H[4] * gy.y + H[5] * gz.y;   // d/dx_1 Fuu21 (= Fuu12)
+      }
+    }
+    {
+      float2 gx, gy, gz;
+      giso2(buf + 15 * FSTRIDE, i, j, k, Dx, Dy, Dz, gx, gy, gz);
+      dFuu2 += H[6] * gx.x + H[7] * gy.x + H[8] * gz.x;     // d/dx_2 Fuu22
+    }
+    Rmo[0] += 0.25f * (dC.y + rhoR * dE.x);
+    Rmo[1] += 0.25f * (dD.x + rhoR * dE.y);
+    Rmo[2] += 0.25f * (dD.y + rhoR * dFuu2);
+  }
+
+  // ---- diffusion pass 2 (elem_diffu.f90:142-194)
+  float2 DTx[4], DTy[4], DTz[4];
+#pragma unroll
+  for (int m = 0; m < 4; ++m) {
+    DTx[m] = F2((float)a.D.d[m][i]);
+    DTy[m] = F2((float)a.D.d[m][j]);
+    DTz[m] = F2((float)a.D.d[m][k]);
+  }
+  const float2 vA = divT2(p2 + 0 * FSTRIDE, p2 + 1 * FSTRIDE, p2 + 2 * FSTRIDE, i, j, k, DTx, DTy, DTz);
+  const float2 vB = divT2(p2 + 3 * FSTRIDE, p2 + 4 * FSTRIDE, p2 + 5 * FSTRIDE, i, j, k, DTx, DTy, DTz);
+  const float2 vC = divT2(p2 + 6 * FSTRIDE, p2 + 7 * FSTRIDE, p2 + 8 * FSTRIDE, i, j, k, DTx, DTy, DTz);
+  const float nu_e = (float)a.prm.c_rho * mue / rhoR;
+  const float CpPr = (float)(a.prm.Cp / a.prm.Prt);
+  const float kappa_e = muf * CpPr + (float)a.prm.c_ener * mue * CpPr + (float)(a.prm.Cp * rho * musgs / 0.9);
+  if (active) {
+    float* out = reinterpret_cast<float*>(a.rel) + (size_t)e * NRES * NN + d;
+    out[0 * NN] = gpv * Rm + nu_e * vA.x;
+    out[1 * NN] = gpv * Rmo[0] + vB.y;
+    out[2 * NN] = gpv * Rmo[1] + vC.x;
+    out[3 * NN] = gpv * Rmo[2] + vC.y;
+    out[4 * NN] = gpv * Ren + (vA.y + kappa_e * vB.x);
+    out[5 * NN] = gpv * Ret;
+  }
+}
+
+template <int EPB>
+static int set_attr() {
+  SOD_CUDA(cudaFuncSetAttribute(k_rhs_mixed2<EPB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes(EPB)));
+  return SOD_OK;
+}
+
+template <int EPB>
+static int launch(const RhsArgs& a, cudaStream_t st) {
+  const int grid = (a.nelem + EPB - 1) / EPB;
+  k_rhs_mixed2<EPB><<<grid, 64 * EPB, smem_bytes(EPB), st>>>(a);
+  SOD_CHECK_LAUNCH();
+  return SOD_OK;
+}
+
+}  // namespace mx2
+
+int init_rhs_mixed2_attrs() {
+  static bool done = false;
+  if (done) return SOD_OK;
+  if (mx2::set_attr<1>() || mx2::set_attr<2>() || mx2::set_attr<4>() || mx2::set_attr<8>()) return SOD_ERR_CUDA;
+  done = true;
+  return SOD_OK;
+}
+
+int launch_rhs_mixed2(const RhsArgs& a, int epb, cudaStream_t st) {
+  switch (epb) {
+    case 1: return mx2::launch<1>(a, st);
+    case 2: return mx2::launch<2>(a, st);
+    case 8: return mx2::launch<8>(a, st);
+    default: return mx2::launch<4>(a, st);
+  }
+}
+
+}  // namespace sod

@@ -185,6 +185,14 @@ class Sod2dMesh:
                                                 int(precision), _stream(stream)))
         return dtn.value
 
+    def autotune(self, state: Sod2dState, precision: int = FP64, stream=None):
+        """Pick elements-per-CTA of the fused RHS kernel by timing the candidates."""
+        best = C.c_int(0); ms = C.c_float(0.0)
+        st = state.struct()
+        _lib.check(_lib.load().sod_autotune(self.handle, C.byref(st), int(precision), C.byref(best), C.byref(ms),
+                                           _stream(stream)))
+        return best.value, ms.value
+
     def rhs(self, state: Sod2dState, precision: int = FP64, stream=None):
         torch = _torch()
         N = self.npoin
