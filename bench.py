@@ -216,6 +216,45 @@ def kr_bytes_per_launch(nelem: int, npoin: int, mixed: bool) -> float:
     return per_elem * nelem + per_node * npoin
 
 
+def bench_cg(n: int):
+    """Config c4: pressure-Poisson Jacobi PCG on an n^3 jittered periodic HEX64 mesh (seed 6),
+    zero-mean Gaussian right-hand side (seed 7), stop at ||r|| < 1e-10 ||r0||; FP64 CG and FP32
+    inner CG + FP64 refinement, time to solution by CUDA events (assembly excluded)."""
+    import torch
+    from sod2d_refmap_b200 import mesh as M, solver as S
+    m = M.periodic_box(n, jitter=0.05, seed=6)
+    gm = S.Sod2dMesh(m, M.TGVParams())
+    P = S.Sod2dPoisson(gm)
+    rng = np.random.default_rng(7)
+    rhs = rng.standard_normal(m.npoin)
+    rhs -= rhs.mean()
+    b = torch.from_numpy(rhs).cuda()
+    out = {"mesh": f"{n}^3 HEX64 jittered periodic", "nodes": m.npoin, "nnz": P.nnz, "tol": 1e-10}
+    P.solve(b, tol=1e-6)  # warm-up
+    sols = {}
+    for mixed, name in ((False, "fp64"), (True, "mixed")):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        x, it, rel = P.solve(b, tol=1e-10, mixed=mixed)
+        e1.record()
+        torch.cuda.synchronize()
+        sols[name] = x
+        out[name] = {"iterations": it, "final_rel_residual": rel, "seconds": e0.elapsed_time(e1) / 1e3}
+    out["mixed"]["rel_l2_vs_fp64"] = float((sols["mixed"] - sols["fp64"]).norm() / sols["fp64"].norm())
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(10):
+        P.apply(b)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / 10
+    out["spmv_fp64"] = {"ms": ms, "GBs": (P.nnz * 12 + m.npoin * 8 * 3) / ms / 1e6}
+    P.close()
+    gm.close()
+    return out
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -337,6 +376,7 @@ def run_ours(args):
         if per_elem:
             roof["traffic"] = per_elem * gm.nelem
             roof["traffic_source"] = tj.get("source")
+    cg = None if args.no_cg else bench_cg(args.cg_n)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         v, sec, desc, thr = cpu_sample(m, prm, st0, layers=args.cpu_layers, reps=args.cpu_reps,
@@ -352,7 +392,7 @@ def run_ours(args):
                          "speedup_mixed_over_fp64": value / value64},
                 "mixed_rel_l2_vs_fp64": {"state_after_steps": acc, "rhs_stage": acc_rhs},
                 "gpu_launches": results["mixed"]["launches"],
-                "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks}
+                "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks, "c4_pressure_cg": cg}
         print(json.dumps(line), flush=True)
     for s in states.values():
         del s
@@ -374,6 +414,8 @@ def main():
     ap.add_argument("--cpu-reps", type=int, default=10)
     ap.add_argument("--ref-layers", type=int, default=1)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-cg", action="store_true")
+    ap.add_argument("--cg-n", type=int, default=48)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":

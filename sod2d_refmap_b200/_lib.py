@@ -69,6 +69,7 @@ _SIGS = {
     "sod_poisson_destroy": (None, [_p]),
     "sod_poisson_nnz": (_i, [_p, _p]),
     "sod_poisson_apply": (_i, [_p, _p, _p, _p]),
+    "sod_poisson_diag": (_i, [_p, _p, _p]),
     "sod_conjgrad_pressure": (_i, [_p, _p, _p, _i, _d, _i, _p, _p, _p]),
     "sod_csr_spmv_scal": (_i, [C.c_int32, C.c_int32, _p, _p, _p, _p, _p, _p]),
     "sod_rhs_vjp": (_i, [_p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p]),

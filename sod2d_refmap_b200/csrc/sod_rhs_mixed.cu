@@ -17,10 +17,9 @@ namespace mx2 {
 
 constexpr double kC1 = 0.000001458;
 constexpr double kS = 110.4;
-constexpr int NA = 7;    // batch A slots
 constexpr int NBC = 16;  // batch B+C slots
 constexpr int NP2 = 9;   // pass-2 slots
-constexpr int NSLOT = NBC + NP2;  // batch A reuses the first NA slots of the BC area
+constexpr int NSLOT = NBC + NP2;  // batch A (7 pairs) reuses the first slots of the BC area
 constexpr int NREF = 16;
 
 __host__ __device__ constexpr size_t smem_bytes(int epb) {

@@ -268,3 +268,52 @@ def csr_spmv_scal(rdom, cdom, Mc, v, stream=None):
     _lib.check(_lib.load().sod_csr_spmv_scal(int(u.numel()), int(Mc.numel()), *(C.c_void_p(_ptr(t)) for t in (
         rdom, cdom, Mc, v, u)), _stream(stream)))
     return u
+
+
+class Sod2dPoisson:
+    """Pressure-Poisson operator and PCG of lib_sod2d_incomp over the C ABI
+    (eval_laplacian_mult / eval_laplacian_diag / conjGrad_pressure_incomp)."""
+
+    def __init__(self, mesh: "Sod2dMesh"):
+        _torch()
+        h = C.c_void_p(0)
+        _lib.check(_lib.load().sod_poisson_create(mesh.handle, C.byref(h)))
+        self.handle = h
+        self.n = mesh.npoin
+        nnz = C.c_int64(0)
+        _lib.check(_lib.load().sod_poisson_nnz(h, C.byref(nnz)))
+        self.nnz = nnz.value
+
+    def close(self):
+        if getattr(self, "handle", None) and self.handle.value:
+            _lib.load().sod_poisson_destroy(self.handle)
+            self.handle = C.c_void_p(0)
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def apply(self, x, stream=None):
+        torch = _torch()
+        y = torch.empty_like(x)
+        _lib.check(_lib.load().sod_poisson_apply(self.handle, C.c_void_p(_ptr(x)), C.c_void_p(_ptr(y)), _stream(stream)))
+        return y
+
+    def diag(self, stream=None):
+        torch = _torch()
+        d = torch.empty(self.n, dtype=torch.float64, device="cuda")
+        _lib.check(_lib.load().sod_poisson_diag(self.handle, C.c_void_p(_ptr(d)), _stream(stream)))
+        return d
+
+    def solve(self, rhs, x0=None, max_iter: int = 100000, tol: float = 1e-10, mixed: bool = False, stream=None):
+        """conjGrad_pressure_incomp: returns (x0 + x, iterations, final relative residual)."""
+        torch = _torch()
+        R = rhs.clone()
+        Rp0 = torch.zeros_like(rhs) if x0 is None else x0
+        it = C.c_int(0); rel = C.c_double(0.0)
+        _lib.check(_lib.load().sod_conjgrad_pressure(self.handle, C.c_void_p(_ptr(Rp0)), C.c_void_p(_ptr(R)),
+                                                    int(max_iter), C.c_double(tol), int(bool(mixed)), C.byref(it),
+                                                    C.byref(rel), _stream(stream)))
+        return R, it.value, rel.value
