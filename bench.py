@@ -216,6 +216,62 @@ def kr_bytes_per_launch(nelem: int, npoin: int, mixed: bool) -> float:
     return per_elem * nelem + per_node * npoin
 
 
+def bench_batch(nmember: int, steps: int):
+    """Config c3: ensemble of periodic HEX64 boxes, n per side log-uniform in [4, 24]
+    (seed 4), Re uniform in [400, 3200] (seed 5), own TGV state and dt; `steps` RK4 steps of
+    every member, one launch per stage for the whole ensemble, each step a captured graph.
+    Compared with the same members advanced one after another (one graph per member)."""
+    import torch
+    from sod2d_refmap_b200 import mesh as M, solver as S, _lib
+    r4 = np.random.default_rng(4)
+    r5 = np.random.default_rng(5)
+    ns = np.rint(np.exp(r4.uniform(math.log(4), math.log(24), nmember))).astype(int)
+    res = r5.uniform(400.0, 3200.0, nmember)
+    prm = M.TGVParams()
+    meshes = [M.periodic_box(int(n), jitter=0.05, seed=100 + i) for i, n in enumerate(ns)]
+    states = [M.taylor_green_state(m, prm, seed=1000 + i, re=float(re)) for i, (m, re) in enumerate(zip(meshes, res))]
+    N = sum(m.npoin for m in meshes)
+    E = sum(m.nelem for m in meshes)
+    B = S.Sod2dBatch(meshes, states, prm)
+    B.adapt_dt()
+    dt0 = B.dt()
+    out = {"members": nmember, "elements": E, "nodes": N, "steps": steps,
+           "n_per_side": {"min": int(ns.min()), "max": int(ns.max()), "mean": float(ns.mean())}}
+    out["elements_per_cta"] = {"mixed": B.autotune(S.MIXED)[0], "fp64": B.autotune(S.FP64)[0]}
+    for prec, name in ((S.MIXED, "mixed"), (S.FP64, "fp64")):
+        B.set_dt(dt0)
+        B.rk4_steps(3, precision=prec)
+        torch.cuda.synchronize()
+        l0 = _lib.launch_count()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        B.rk4_steps(steps, precision=prec)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        out[name] = {"value": 5 * N * 4 * steps / (ms / 1e3) / 1e9, "unit": UNIT, "ms_per_step": ms / steps,
+                     "launches_per_step": (_lib.launch_count() - l0) / steps}
+    B.close()
+    # the same members one at a time (each its own mesh, graph and launches)
+    total = 0.0
+    for m, st in zip(meshes, states):
+        gm = S.Sod2dMesh(m, prm)
+        s_ = S.Sod2dState.from_host(st, gm.nelem)
+        gm.adapt_dt(s_)
+        gm.rk4_steps(s_, 1, precision=S.MIXED)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        gm.rk4_steps(s_, steps, precision=S.MIXED)
+        e1.record()
+        torch.cuda.synchronize()
+        total += e0.elapsed_time(e1)
+        gm.close()
+    out["sequential_mixed"] = {"value": 5 * N * 4 * steps / (total / 1e3) / 1e9, "unit": UNIT,
+                               "ms_per_step": total / steps}
+    return out
+
+
 def bench_cg(n: int):
     """Config c4: pressure-Poisson Jacobi PCG on an n^3 jittered periodic HEX64 mesh (seed 6),
     zero-mean Gaussian right-hand side (seed 7), stop at ||r|| < 1e-10 ||r0||; FP64 CG and FP32
@@ -377,6 +433,7 @@ def run_ours(args):
             roof["traffic"] = per_elem * gm.nelem
             roof["traffic_source"] = tj.get("source")
     cg = None if args.no_cg else bench_cg(args.cg_n)
+    batch = None if args.no_batch else bench_batch(args.batch_members, args.batch_steps)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         v, sec, desc, thr = cpu_sample(m, prm, st0, layers=args.cpu_layers, reps=args.cpu_reps,
@@ -392,7 +449,8 @@ def run_ours(args):
                          "speedup_mixed_over_fp64": value / value64},
                 "mixed_rel_l2_vs_fp64": {"state_after_steps": acc, "rhs_stage": acc_rhs},
                 "gpu_launches": results["mixed"]["launches"],
-                "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks, "c4_pressure_cg": cg}
+                "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks, "c4_pressure_cg": cg,
+                "c3_ensemble": batch}
         print(json.dumps(line), flush=True)
     for s in states.values():
         del s
@@ -416,6 +474,9 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-cg", action="store_true")
     ap.add_argument("--cg-n", type=int, default=48)
+    ap.add_argument("--no-batch", action="store_true")
+    ap.add_argument("--batch-members", type=int, default=256)
+    ap.add_argument("--batch-steps", type=int, default=20)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":

@@ -210,6 +210,31 @@ int sod_full_convec_ijk_noalloc(int32_t nelem, int32_t npoin, int32_t index_base
                                 const double* E, double* Rmass, double* Rmom, double* Rener,
                                 sod_stream_t stream);
 
+/* ---- Ensemble batching: many independent periodic meshes in one launch per stage -------
+ * The reference runs ensembles as separate MPI applications (mod_mpi.f90:39-51,
+ * TGVMultiSolver.f90:30-60); here the members are concatenated into one block-diagonal mesh
+ * so each RK stage is one fused-RHS and one gather launch over all members and a step is one
+ * CUDA graph.  Per member: its own state, Reynolds number (mu_factor), dt, entropy
+ * normalisation and CFL limit.  The batch copies what it needs from the member meshes. */
+typedef struct SodBatch SodBatch;
+int sod_batch_create(SodMesh* const* meshes, int nmesh, SodBatch** out);
+void sod_batch_destroy(SodBatch* B);
+/* Host arrays of one member in the reference layouts: rho, q(N_i,3), E, mu_factor and
+ * mu_e(E_i,64) are required; u(N_i,3), csound, mu_fluid are used by sod_batch_adapt_dt. */
+int sod_batch_set_member(SodBatch* B, int member, const SodState* host);
+/* Copy any non-null field of one member back to host arrays (reference layouts). */
+int sod_batch_get_member(SodBatch* B, int member, SodState* host);
+int sod_batch_set_dt(SodBatch* B, const double* dt_host);   /* [nmember] */
+int sod_batch_get_dt(SodBatch* B, double* dt_host);         /* [nmember] */
+/* adapt_dt_cfl (mod_time_ops.f90:11-61) per member from the members' u, csound, mu_fluid, rho. */
+int sod_batch_adapt_dt(SodBatch* B, sod_stream_t stream);
+/* The concatenated mesh (for sod_autotune and diagnostics; owned by the batch). */
+int sod_batch_mesh(SodBatch* B, SodMesh** mesh);
+/* sod_autotune on the concatenated ensemble state. */
+int sod_batch_autotune(SodBatch* B, SodPrecision prec, int* best_epb, float* best_ms, sod_stream_t stream);
+/* nsteps RK4 steps of every member, each step one captured graph; dt evolves per member. */
+int sod_batch_rk4_steps(SodBatch* B, int nsteps, SodPrecision prec, sod_stream_t stream);
+
 /* ---- Incompressible pressure Poisson (lib_sod2d_incomp) --------------------------------- */
 
 typedef struct SodPoisson SodPoisson;

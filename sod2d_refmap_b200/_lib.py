@@ -75,7 +75,14 @@ _SIGS = {
     "sod_rhs_vjp": (_i, [_p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p]),
     "sod_batch_create": (_i, [_p, _i, _p]),
     "sod_batch_destroy": (None, [_p]),
-    "sod_batch_rk4_steps": (_i, [_p, _p, _p, _i, _i, _p]),
+    "sod_batch_set_member": (_i, [_p, _i, _p]),
+    "sod_batch_get_member": (_i, [_p, _i, _p]),
+    "sod_batch_set_dt": (_i, [_p, _p]),
+    "sod_batch_get_dt": (_i, [_p, _p]),
+    "sod_batch_adapt_dt": (_i, [_p, _p]),
+    "sod_batch_mesh": (_i, [_p, _p]),
+    "sod_batch_autotune": (_i, [_p, _i, _p, _p, _p]),
+    "sod_batch_rk4_steps": (_i, [_p, _i, _i, _p]),
     "sod_autotune": (_i, [_p, _p, _i, _p, _p, _p]),
     "sod_last_error": (C.c_char_p, []),
     "sod_version": (C.c_char_p, []),

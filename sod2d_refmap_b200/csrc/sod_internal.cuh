@@ -138,6 +138,13 @@ struct SodMesh {
   std::unordered_map<uint64_t, sod::GraphEntry> graphs;
   int tuned_epb[2] = {0, 0};
   std::vector<double*> host_mirror;  // device buffers of sod_rk4_main_host
+  // ensemble members (a SodBatch's concatenated mesh); nmember == 0 for a single mesh
+  int nmember = 0;
+  int32_t* node_member = nullptr;   // [npoin]
+  int32_t* elem_member = nullptr;   // [nelem]
+  int32_t* member_node_off = nullptr;  // [nmember+1] contiguous node ranges
+  double* member_scal = nullptr;    // [nmember][2] eta mean, eta norm
+  double* member_dt_bits = nullptr; // [nmember] scratch for the per-member dt min
 };
 
 namespace sod {

@@ -386,7 +386,9 @@ struct GatherArgs {
   const int32_t* __restrict__ idx;
   const void* rel;
   const double* __restrict__ Ml;
-  const double* __restrict__ dt;  // device scalar
+  const double* __restrict__ dt;  // device scalar, or per-member array when node_member is set
+  const int32_t* __restrict__ node_member;
+  int member_reduce;              // stage 4: eta sums done by the per-member kernel instead
   double a_next, b_cur;
   // state (level pos=2) columns
   double* y[5];
@@ -461,7 +463,7 @@ __global__ void __launch_bounds__(256) k_gather_rk(const GatherArgs a) {
       for (int f = 0; f < 6; ++f)
         if (a.out[f]) a.out[f][n] = r[f];
     } else {
-      const double dt = *a.dt;
+      const double dt = a.node_member ? a.dt[a.node_member[n]] : *a.dt;
       double rs[6];
 #pragma unroll
       for (int f = 0; f < 6; ++f) rs[f] = (STAGE == 1 ? 0.0 : a.rsum[f * N + n]) + a.b_cur * r[f];
@@ -499,6 +501,7 @@ __global__ void __launch_bounds__(256) k_gather_rk(const GatherArgs a) {
     }
   }
   if constexpr (STAGE == 4) {
+    if (a.member_reduce) return;  // uniform across the grid
     // entropy normalisation (mod_entropy_viscosity.f90:43-66): sum, max, min of eta
     __shared__ double sh[3 * 8];
     __shared__ bool last;
@@ -563,7 +566,9 @@ struct ViscArgs {
   const double* __restrict__ scal;   // [0] mean, [1] norm
   double* mue;                       // out FP64 [e][64]
   float* mue32;                      // optional FP32 copy
-  double* dt_bits;                   // scratch scalar receiving the min dt (bits, pre-set large)
+  double* dt_bits;                   // scratch scalar(s) receiving the min dt (bits, pre-set large)
+  const int32_t* __restrict__ elem_member;  // ensemble: member of each element (null = one mesh)
+  const double* __restrict__ member_scal;   // ensemble: [member][2] eta mean, norm
   double* dt_out;                    // device scalar (may be null)
   DevParams prm;
 };
@@ -624,7 +629,8 @@ __global__ void __launch_bounds__(64 * KV_EPB) k_visc_dt(const ViscArgs a) {
   __syncthreads();
   const double ced = elem_s[es][0];
   mB = fmax(wm[es][0][2], wm[es][1][2]);
-  const double norm = a.scal[1];
+  const int mem = a.elem_member ? a.elem_member[ee] : 0;
+  const double norm = a.elem_member ? a.member_scal[2 * mem + 1] : a.scal[1];
   const double R1 = (norm > 0.0) ? rho * fabs(a.Reta[n]) / norm : 0.0;
   const double hl = a.helem_l[(size_t)ee * NN + d];
   const double Ve = ced * R1 * hl * hl;
@@ -649,7 +655,8 @@ __global__ void __launch_bounds__(64 * KV_EPB) k_visc_dt(const ViscArgs a) {
     if (a.mue32) a.mue32[(size_t)e * NN + d] = (float)acc;
     // next dt: order-independent min over elements on the bit pattern of a positive double
     if (a.dt_out && d == 0)
-      atomicMin(reinterpret_cast<unsigned long long*>(a.dt_bits), (unsigned long long)__double_as_longlong(elem_s[es][1]));
+      atomicMin(reinterpret_cast<unsigned long long*>(a.dt_bits) + mem,
+                (unsigned long long)__double_as_longlong(elem_s[es][1]));
   }
 }
 
@@ -764,15 +771,42 @@ int launch_visc_dt(SodMesh* m, const SodState* s, double* dt_out, float* mue32, 
   v.scal = m->buf.scal;
   v.mue = m->mue_int;
   v.mue32 = mue32;
-  v.dt_bits = m->buf.scal + 3;
+  const int nm = m->nmember > 0 ? m->nmember : 1;
+  v.dt_bits = m->nmember > 0 ? m->member_dt_bits : m->buf.scal + 3;
+  v.elem_member = m->nmember > 0 ? m->elem_member : nullptr;
+  v.member_scal = m->member_scal;
   v.dt_out = dt_out;
   v.prm = m->prm;
-  if (dt_out) SOD_CUDA(cudaMemsetAsync(v.dt_bits, 0x7F, sizeof(double), st));  // 1.38e306
+  if (dt_out) SOD_CUDA(cudaMemsetAsync(v.dt_bits, 0x7F, sizeof(double) * nm, st));  // 1.38e306 each
   const int grid = (m->nelem + KV_EPB - 1) / KV_EPB;
   k_visc_dt<<<grid, 64 * KV_EPB, 0, st>>>(v);
   SOD_CHECK_LAUNCH();
-  if (dt_out) SOD_CUDA(cudaMemcpyAsync(dt_out, v.dt_bits, sizeof(double), cudaMemcpyDeviceToDevice, st));
+  if (dt_out) SOD_CUDA(cudaMemcpyAsync(dt_out, v.dt_bits, sizeof(double) * nm, cudaMemcpyDeviceToDevice, st));
   return SOD_OK;
+}
+
+// Ensemble: per-member eta sum/max/min over its contiguous node range, one block per member.
+__global__ void __launch_bounds__(512) k_member_eta(const int32_t* __restrict__ off, const double* __restrict__ eta,
+                                                    double* scal, int normalise) {
+  const int mbr = blockIdx.x;
+  const int b = off[mbr], e = off[mbr + 1];
+  double s = 0.0, mx = -1e300, mn = 1e300;
+  for (int t = b + threadIdx.x; t < e; t += blockDim.x) {
+    const double v = eta[t];
+    s += v; mx = fmax(mx, v); mn = fmin(mn, v);
+  }
+  __shared__ double sh[3 * 16];
+  block_reduce3(s, mx, mn, sh);
+  if (threadIdx.x == 0) {
+    if (normalise) {
+      const double mean = s / (double)(e - b);
+      scal[2 * mbr] = mean;
+      scal[2 * mbr + 1] = fmax(mx - mean, mean - mn);
+    } else {
+      scal[2 * mbr] = 0.0;
+      scal[2 * mbr + 1] = 1.0;
+    }
+  }
 }
 
 // Reta scratch when the caller passes none
@@ -810,9 +844,15 @@ int run_step(SodMesh* m, SodState* s, const double* dt_dev, double* dt_next, boo
     g.u0 = s->u; g.u1 = s->u + N; g.u2 = s->u + 2 * N;
     g.pr = s->pr; g.Tem = s->Tem; g.e_int = s->e_int; g.eta = s->eta; g.csound = s->csound;
     g.machno = s->machno; g.mu_fluid = s->mu_fluid; g.Reta = loc.Reta; g.mu_factor = s->mu_factor;
+    g.node_member = m->nmember > 0 ? m->node_member : nullptr;
+    g.member_reduce = m->nmember > 0 ? 1 : 0;
     if (ev) cudaEventRecord(ev[2 * (3 + stage)], st);
     rc = launch_gather(m, mixed, stage, g, st);
     if (rc) return rc;
+    if (stage == 4 && m->nmember > 0) {
+      k_member_eta<<<m->nmember, 512, 0, st>>>(m->member_node_off, s->eta, m->member_scal, m->prm.normalise);
+      SOD_CHECK_LAUNCH();
+    }
     if (ev) cudaEventRecord(ev[2 * (3 + stage) + 1], st);
   }
   if (ev) cudaEventRecord(ev[16], st);

@@ -317,3 +317,73 @@ class Sod2dPoisson:
                                                     int(max_iter), C.c_double(tol), int(bool(mixed)), C.byref(it),
                                                     C.byref(rel), _stream(stream)))
         return R, it.value, rel.value
+
+
+class Sod2dBatch:
+    """Ensemble of independent periodic meshes advanced together (one launch per RK stage)."""
+
+    def __init__(self, meshes: list, states: list, prm: TGVParams | None = None):
+        _torch()
+        L = _lib.load()
+        self.prm = prm or TGVParams()
+        members = [Sod2dMesh(m, self.prm) for m in meshes]
+        arr = (C.c_void_p * len(members))(*[mm.handle.value for mm in members])
+        h = C.c_void_p(0)
+        _lib.check(L.sod_batch_create(arr, len(members), C.byref(h)))
+        self.handle = h
+        self.sizes = [(m.npoin, m.nelem) for m in meshes]
+        for mm in members:
+            mm.close()
+        for i, st in enumerate(states):
+            self.set_member(i, st)
+
+    def close(self):
+        if getattr(self, "handle", None) and self.handle.value:
+            _lib.load().sod_batch_destroy(self.handle)
+            self.handle = C.c_void_p(0)
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @staticmethod
+    def _host_struct(d: dict) -> _lib.SodState:
+        return _lib.SodState(*(int(d[f].ctypes.data) if d.get(f) is not None else 0 for f in Sod2dState.FIELDS))
+
+    def set_member(self, i: int, st: FlowState):
+        d = {f: np.asfortranarray(getattr(st, f)) for f in ("rho", "q", "E", "u", "csound", "mu_fluid", "mu_factor",
+                                                             "mu_e")}
+        _lib.check(_lib.load().sod_batch_set_member(self.handle, int(i), C.byref(self._host_struct(d))))
+
+    def get_member(self, i: int) -> dict:
+        N, E = self.sizes[i]
+        d = {f: np.zeros(N) for f in ("rho", "E", "pr", "Tem", "e_int", "eta", "csound", "machno", "mu_fluid",
+                                      "Reta")}
+        d["q"] = np.zeros((N, 3), order="F"); d["u"] = np.zeros((N, 3), order="F")
+        d["mu_e"] = np.zeros((E, 64), order="F")
+        _lib.check(_lib.load().sod_batch_get_member(self.handle, int(i), C.byref(self._host_struct(d))))
+        return d
+
+    def adapt_dt(self, stream=None):
+        _lib.check(_lib.load().sod_batch_adapt_dt(self.handle, _stream(stream)))
+
+    def dt(self) -> np.ndarray:
+        out = np.zeros(len(self.sizes))
+        _lib.check(_lib.load().sod_batch_get_dt(self.handle, C.c_void_p(out.ctypes.data)))
+        return out
+
+    def set_dt(self, dt):
+        a = np.ascontiguousarray(dt, dtype=np.float64)
+        _lib.check(_lib.load().sod_batch_set_dt(self.handle, C.c_void_p(a.ctypes.data)))
+
+    def rk4_steps(self, nsteps: int, precision: int = FP64, stream=None):
+        _lib.check(_lib.load().sod_batch_rk4_steps(self.handle, int(nsteps), int(precision), _stream(stream)))
+
+    def autotune(self, precision: int = FP64, stream=None):
+        """Tune elements-per-CTA of the fused RHS kernel on the concatenated ensemble mesh."""
+        best = C.c_int(0); ms = C.c_float(0.0)
+        _lib.check(_lib.load().sod_batch_autotune(self.handle, int(precision), C.byref(best), C.byref(ms),
+                                                 _stream(stream)))
+        return best.value, ms.value
