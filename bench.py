@@ -272,6 +272,84 @@ def bench_batch(nmember: int, steps: int):
     return out
 
 
+def bench_adjoint(n: int, steps: int, every: int):
+    """Config c2: loss 1/2 ||rho u||^2 after `steps` FP64 RK4 steps on an n^3 jittered periodic
+    HEX64 mesh (seed 3), gradient w.r.t. the initial (rho, q, E) by the checkpointed adjoint
+    (checkpoint every `every` steps; mu_e and dt frozen at their forward values).  Times the
+    forward (with checkpointing) and the backward by CUDA events, and checks the directional
+    derivative along a seeded Gaussian direction (seed 9) against central differences of the
+    frozen-coefficient forward map at h = 1e-4 and 1e-6."""
+    import torch
+    from sod2d_refmap_b200 import mesh as M, solver as S
+    from sod2d_refmap_b200.adjoint import Sod2dRollout, replay, trajectory_coefficients, _clone_state
+    m = M.periodic_box(n, jitter=0.05, seed=3)
+    prm = M.TGVParams()
+    gm = S.Sod2dMesh(m, prm)
+    s = S.Sod2dState.from_host(M.taylor_green_state(m, prm), gm.nelem)
+    gm.adapt_dt(s)
+    gm.rk_4_main(s, S.FP64, update_dt=True)  # a state with mu_e > 0
+
+    def run(K):
+        rho = s.rho.clone().requires_grad_(True)
+        q = s.q.clone().requires_grad_(True)
+        E = s.E.clone().requires_grad_(True)
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        torch.cuda.synchronize()
+        ev[0].record()
+        _, qK, _ = Sod2dRollout.apply(gm, s, rho, q, E, K, every)
+        loss = 0.5 * (qK * qK).sum()
+        ev[1].record()
+        loss.backward()
+        ev[2].record()
+        torch.cuda.synchronize()
+        return (rho.grad, q.grad, E.grad), float(loss.item()), ev[0].elapsed_time(ev[1]), ev[1].elapsed_time(ev[2])
+
+    run(2)  # warm-up
+    grads, loss, t_fwd, t_bwd = run(steps)
+    # the plain forward (no checkpoint copies): eager steps and a captured graph
+    t = _clone_state(s)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        gm.rk_4_main(t, S.FP64, update_dt=True)
+    e1.record()
+    torch.cuda.synchronize()
+    t_plain = e0.elapsed_time(e1)
+    t = _clone_state(s)
+    gm.rk4_steps(t, 1, precision=S.FP64)
+    t = _clone_state(s)
+    torch.cuda.synchronize()
+    e0.record()
+    gm.rk4_steps(t, steps, precision=S.FP64)
+    e1.record()
+    torch.cuda.synchronize()
+    t_graph = e0.elapsed_time(e1)
+    # directional derivative vs central differences of the frozen-coefficient map
+    mus, dts = trajectory_coefficients(gm, s, steps)
+    g = torch.Generator(device="cuda")
+    g.manual_seed(9)
+    v = [torch.randn(x.shape, dtype=torch.float64, device="cuda", generator=g) * x.abs().mean()
+         for x in (s.rho, s.q, s.E)]
+    dL = float(sum((gi * vi).sum() for gi, vi in zip(grads, v)).item())
+
+    def L_at(h):
+        u = _clone_state(s)
+        u.rho.add_(h * v[0]); u.q.add_(h * v[1]); u.E.add_(h * v[2])
+        replay(gm, u, mus, dts)
+        return 0.5 * float((u.q * u.q).sum().item())
+    fd = {}
+    for h in (1e-4, 1e-6):
+        d = (L_at(h) - L_at(-h)) / (2 * h)
+        fd[f"{h:g}"] = {"fd": d, "rel_err": abs(d - dL) / abs(dL)}
+    gm.close()
+    return {"mesh": f"{n}^3 HEX64 jittered periodic", "nodes": m.npoin, "steps": steps, "checkpoint_every": every,
+            "precision": "fp64", "loss": loss, "directional_derivative": dL, "finite_differences": fd,
+            "ms": {"forward_with_checkpoints": t_fwd, "backward": t_bwd, "forward_plain_eager": t_plain,
+                   "forward_plain_graph": t_graph},
+            "adjoint_over_forward": {"backward/forward_with_checkpoints": t_bwd / t_fwd,
+                                     "backward/forward_plain_graph": t_bwd / t_graph}}
+
+
 def bench_cg(n: int):
     """Config c4: pressure-Poisson Jacobi PCG on an n^3 jittered periodic HEX64 mesh (seed 6),
     zero-mean Gaussian right-hand side (seed 7), stop at ||r|| < 1e-10 ||r0||; FP64 CG and FP32
@@ -434,6 +512,7 @@ def run_ours(args):
             roof["traffic_source"] = tj.get("source")
     cg = None if args.no_cg else bench_cg(args.cg_n)
     batch = None if args.no_batch else bench_batch(args.batch_members, args.batch_steps)
+    adjoint = None if args.no_adjoint else bench_adjoint(args.adj_n, args.adj_steps, args.adj_every)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         v, sec, desc, thr = cpu_sample(m, prm, st0, layers=args.cpu_layers, reps=args.cpu_reps,
@@ -450,7 +529,7 @@ def run_ours(args):
                 "mixed_rel_l2_vs_fp64": {"state_after_steps": acc, "rhs_stage": acc_rhs},
                 "gpu_launches": results["mixed"]["launches"],
                 "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks, "c4_pressure_cg": cg,
-                "c3_ensemble": batch}
+                "c3_ensemble": batch, "c2_adjoint": adjoint}
         print(json.dumps(line), flush=True)
     for s in states.values():
         del s
@@ -477,6 +556,10 @@ def main():
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--batch-members", type=int, default=256)
     ap.add_argument("--batch-steps", type=int, default=20)
+    ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--adj-n", type=int, default=32)
+    ap.add_argument("--adj-steps", type=int, default=50)
+    ap.add_argument("--adj-every", type=int, default=10)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":

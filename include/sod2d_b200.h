@@ -257,6 +257,31 @@ int sod_poisson_diag(SodPoisson* P, double* d, sod_stream_t stream);
 int sod_conjgrad_pressure(SodPoisson* P, const double* Rp0, double* R, int max_iter, double tol,
                           int mixed, int* iters, double* final_rel, sod_stream_t stream);
 
+/* ---- Adjoint (reverse mode) of the RHS and of one RK4 step ------------------------------ */
+/* No counterpart in the reference (SOD2D has no adjoint); these differentiate the FP64 path of
+ * sod_rhs / sod_rk4_main with the entropy viscosity mu_e (and dt) frozen at the given values,
+ * Sutherland's law differentiated, no SGS viscosity.  All arrays are device arrays in the
+ * SodState layouts (q and its adjoints: 3 columns of npoin). */
+
+/* VJP of the stage RHS of sod_rhs (Rmass, Rmom, Rener, already divided by Ml): given seeds
+ * (bar_Rmass, bar_Rmom, bar_Rener) writes grad = (dR/d(rho,q,E))^T seed (overwritten). */
+int sod_rhs_vjp(SodMesh* mesh, const double* rho, const double* q, const double* E,
+                const double* mu_e, const double* mu_factor, const double* bar_Rmass,
+                const double* bar_Rmom, const double* bar_Rener, double* grad_rho, double* grad_q,
+                double* grad_E, sod_stream_t stream);
+/* sod_rk4_main (FP64) that also writes its stage states Y2, Y3, Y4 to stages (device,
+ * 15*npoin doubles: 3 stages x (rho, q x3, E) columns) for sod_rk4_step_vjp. */
+int sod_rk4_main_record(SodMesh* mesh, SodState* state, const double* dt_dev, double* dt_next_dev,
+                        double* stages, sod_stream_t stream);
+/* VJP of one RK4 step y_{n+1} = y_n - dt sum_s b_s R(Y_s) (rk_4_main, time_integ.f90:288-426)
+ * at the state (rho, q, E) with mu_e and dt_dev frozen: out = (dy_{n+1}/dy_n)^T bar.  stages
+ * from sod_rk4_main_record, or null to recompute them; out may alias bar. */
+int sod_rk4_step_vjp(SodMesh* mesh, const double* rho, const double* q, const double* E,
+                     const double* mu_e, const double* mu_factor, const double* dt_dev,
+                     const double* stages, const double* bar_rho, const double* bar_q,
+                     const double* bar_E, double* out_rho, double* out_q, double* out_E,
+                     sod_stream_t stream);
+
 /* ---- Legacy unit-test API ----------------------------------------------------------- */
 
 /* CSR_SpMV_scal (legacy API pinned by unitt/unitt_CSR_SPMV_scal/unitt_CSR_SPMV_scal.f90:14-52):

@@ -68,7 +68,8 @@ def lib():
 
 
 def ptr(a: np.ndarray):
-    return C.c_void_p(a.ctypes.data)
+    """A pointer to a's data that keeps a alive (safe for temporaries in an argument list)."""
+    return a.ctypes.data_as(C.c_void_p)
 
 
 def set_threads(n: int) -> int:
@@ -222,3 +223,24 @@ def csr_spmv_scal(rdom, cdom, Mc, v):
     u = np.zeros(len(rdom) - 1)
     lib().oracle_csr_spmv_scal(len(u), len(Mc), ptr(rdom), ptr(cdom), ptr(Mc), ptr(v), ptr(u))
     return u
+
+
+def rhs_stage(om: OracleMesh, prm, st, mu_e=None):
+    """Stage RHS (mass, mom x3, energy; /Ml) without the entropy residual: (5, npoin) array."""
+    P = params_of(prm)
+    R = np.zeros(5 * om.npoin)
+    mue = np.asfortranarray(st.mu_e if mu_e is None else mu_e)
+    lib().oracle_rhs_stage(C.byref(om.ctx), C.byref(P), ptr(om.Ml), ptr(st.mu_factor), ptr(mue), None, ptr(st.rho),
+                           ptr(np.asfortranarray(st.q)), ptr(st.E), ptr(R))
+    return R.reshape(5, om.npoin)
+
+
+def rhs_jvp(om: OracleMesh, prm, st, drho, dq, dE, mu_e=None):
+    """Exact JVP of rhs_stage along (drho, dq(npoin,3), dE): returns (R, dR) as (5, npoin)."""
+    P = params_of(prm)
+    R = np.zeros(5 * om.npoin); dR = np.zeros(5 * om.npoin)
+    mue = np.asfortranarray(st.mu_e if mu_e is None else mu_e)
+    lib().oracle_rhs_jvp(C.byref(om.ctx), C.byref(P), ptr(om.Ml), ptr(st.mu_factor), ptr(mue), None, ptr(st.rho),
+                         ptr(np.asfortranarray(st.q)), ptr(st.E), ptr(np.ascontiguousarray(drho)),
+                         ptr(np.asfortranarray(dq)), ptr(np.ascontiguousarray(dE)), ptr(R), ptr(dR))
+    return R.reshape(5, om.npoin), dR.reshape(5, om.npoin)

@@ -131,3 +131,31 @@ void oracle_csr_spmv_scal(int npoin, int nzdom, const int32_t* rdom, const int32
 }
 
 }  // extern "C"
+
+extern "C" {
+
+// Stage RHS (mass, mom x3, energy; /Ml) of rk_4_main without the entropy residual; state in
+// (rho, q(npoin,3), E), R out as 5 columns of npoin.  mu_sgs may be null (zero).
+void oracle_rhs_stage(const ElemCtx* ctx, const Params* P, const double* Ml, const double* mu_factor,
+                      const double* mu_e, const double* mu_sgs, const double* rho, const double* q, const double* E,
+                      double* R) {
+  std::vector<double> zeros;
+  if (!mu_sgs) { zeros.assign((size_t)ctx->nelem * nnode, 0.0); mu_sgs = zeros.data(); }
+  rhs_stage_t<double>(*ctx, *P, Ml, mu_factor, mu_e, mu_sgs, rho, q, E, R);
+}
+
+// Exact JVP of oracle_rhs_stage by forward-mode dual numbers: dR = (dR/dU) dU, U = (rho,q,E).
+void oracle_rhs_jvp(const ElemCtx* ctx, const Params* P, const double* Ml, const double* mu_factor,
+                    const double* mu_e, const double* mu_sgs, const double* rho, const double* q, const double* E,
+                    const double* drho, const double* dq, const double* dE, double* R, double* dR) {
+  const int64_t N = ctx->npoin;
+  std::vector<double> zeros;
+  if (!mu_sgs) { zeros.assign((size_t)ctx->nelem * nnode, 0.0); mu_sgs = zeros.data(); }
+  std::vector<Dual> r(N), qq(3 * N), e(N), out(5 * N);
+  for (int64_t p = 0; p < N; ++p) { r[p] = Dual(rho[p], drho[p]); e[p] = Dual(E[p], dE[p]); }
+  for (int64_t p = 0; p < 3 * N; ++p) qq[p] = Dual(q[p], dq[p]);
+  rhs_stage_t<Dual>(*ctx, *P, Ml, mu_factor, mu_e, mu_sgs, r.data(), qq.data(), e.data(), out.data());
+  for (int64_t p = 0; p < 5 * N; ++p) { if (R) R[p] = out[p].v; dR[p] = out[p].d; }
+}
+
+}  // extern "C"

@@ -659,6 +659,315 @@ inline void full_diffusion_ijk(const ElemCtx& ctx, const Params& P, const double
   });
 }
 
+
+// ------------------------------------------------------------------------------------------
+// Forward-mode dual numbers and the stage RHS in a generic scalar type: exact directional
+// derivatives (JVPs) of the RHS for the adjoint checks.  Only arithmetic, sqrt and pow occur
+// on the state-dependent path of the convection/diffusion RHS.
+// ------------------------------------------------------------------------------------------
+struct Dual {
+  double v = 0.0, d = 0.0;
+  Dual() = default;
+  Dual(double a) : v(a), d(0.0) {}
+  Dual(double a, double b) : v(a), d(b) {}
+};
+inline Dual operator+(Dual a, Dual b) { return {a.v + b.v, a.d + b.d}; }
+inline Dual operator-(Dual a, Dual b) { return {a.v - b.v, a.d - b.d}; }
+inline Dual operator-(Dual a) { return {-a.v, -a.d}; }
+inline Dual operator*(Dual a, Dual b) { return {a.v * b.v, a.d * b.v + a.v * b.d}; }
+inline Dual operator/(Dual a, Dual b) { return {a.v / b.v, (a.d * b.v - a.v * b.d) / (b.v * b.v)}; }
+inline Dual operator+(Dual a, double b) { return {a.v + b, a.d}; }
+inline Dual operator+(double a, Dual b) { return {a + b.v, b.d}; }
+inline Dual operator-(Dual a, double b) { return {a.v - b, a.d}; }
+inline Dual operator-(double a, Dual b) { return {a - b.v, -b.d}; }
+inline Dual operator*(Dual a, double b) { return {a.v * b, a.d * b}; }
+inline Dual operator*(double a, Dual b) { return {a * b.v, a * b.d}; }
+inline Dual operator/(Dual a, double b) { return {a.v / b, a.d / b}; }
+inline Dual operator/(double a, Dual b) { return {a / b.v, -a * b.d / (b.v * b.v)}; }
+inline Dual& operator+=(Dual& a, Dual b) { a = a + b; return a; }
+inline Dual& operator-=(Dual& a, Dual b) { a = a - b; return a; }
+inline Dual sqrt(Dual a) { double s = std::sqrt(a.v); return {s, a.d / (2.0 * s)}; }
+inline Dual pow(Dual a, double e) { double p = std::pow(a.v, e); return {p, e * std::pow(a.v, e - 1.0) * a.d}; }
+inline double sqrt(double a) { return std::sqrt(a); }
+inline double pow(double a, double e) { return std::pow(a, e); }
+inline double value(double a) { return a; }
+inline double value(Dual a) { return a.v; }
+
+template <class T>
+inline void full_convec_ijk_t(const ElemCtx& ctx, const T* u, const T* q, const T* rho,
+                            const T* pr, const T* E, T* Rmass, T* Rmom,
+                            T* Rener) {
+  const int nelem = ctx.nelem, npoin = ctx.npoin;
+  for (int64_t p = 0; p < (int64_t)npoin * 3; ++p) Rmom[p] = 0.0;
+  for (int p = 0; p < npoin; ++p) { Rmass[p] = 0.0; Rener[p] = 0.0; }
+  for_each_element_coloured(ctx, [&](int ielem) {
+    int ipoin[nnode];
+    T Re_mom[nnode][3], Re_mass[nnode], Re_ener[nnode];
+    T ul[nnode][3], ql[nnode][3], rhol[nnode], prl[nnode], El[nnode], fel[nnode][3];
+    T fl[nnode][3][3], fuul[nnode][3][3], REl[nnode], fuel[nnode][3], kl[nnode], fkl[nnode][3],
+        fukl[nnode][3], Rkl[nnode];
+    for (int a = 0; a < nnode; ++a) ipoin[a] = ctx.connec[ielem + (int64_t)nelem * a];
+    for (int a = 0; a < nnode; ++a) {
+      kl[a] = 0.0;
+      for (int d = 0; d < 3; ++d)
+        kl[a] = kl[a] + u[ipoin[a] + (int64_t)npoin * d] * u[ipoin[a] + (int64_t)npoin * d] * 0.5;
+    }
+    for (int d = 0; d < 3; ++d)
+      for (int a = 0; a < nnode; ++a) {
+        T ud = u[ipoin[a] + (int64_t)npoin * d];
+        ul[a][d] = ud;
+        ql[a][d] = q[ipoin[a] + (int64_t)npoin * d];
+        fel[a][d] = rho[ipoin[a]] * E[ipoin[a]] * ud;
+        fuel[a][d] = E[ipoin[a]] * ud;
+        fkl[a][d] = rho[ipoin[a]] * kl[a] * ud;
+        fukl[a][d] = kl[a] * ud;
+      }
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j)
+        for (int a = 0; a < nnode; ++a) {
+          fl[a][i][j] = q[ipoin[a] + (int64_t)npoin * i] * u[ipoin[a] + (int64_t)npoin * j];
+          fuul[a][i][j] = u[ipoin[a] + (int64_t)npoin * i] * u[ipoin[a] + (int64_t)npoin * j];
+        }
+    for (int a = 0; a < nnode; ++a) {
+      rhol[a] = rho[ipoin[a]];
+      El[a] = E[ipoin[a]];
+      REl[a] = rho[ipoin[a]] * E[ipoin[a]];
+      Rkl[a] = rho[ipoin[a]] * kl[a];
+      prl[a] = pr[ipoin[a]];
+    }
+    for (int igaus = 0; igaus < ngaus; ++igaus) {
+      double dlxi[4], dleta[4], dlzeta[4];
+      for (int ii = 0; ii < 4; ++ii) {
+        dlxi[ii] = SOD_DL(igaus, 0, ii);
+        dleta[ii] = SOD_DL(igaus, 1, ii);
+        dlzeta[ii] = SOD_DL(igaus, 2, ii);
+      }
+      int isoI = ctx.gmshAtoI[igaus], isoJ = ctx.gmshAtoJ[igaus], isoK = ctx.gmshAtoK[igaus];
+      T gIRho[3] = {0, 0, 0}, gIP[3] = {0, 0, 0}, gIE[3] = {0, 0, 0}, gIRE[3] = {0, 0, 0},
+             gIk[3] = {0, 0, 0}, gIRk[3] = {0, 0, 0};
+      T gIU[3][3] = {}, gIQ[3][3] = {}, gIFe[3][3] = {}, gIFue[3][3] = {}, gIFk[3][3] = {},
+             gIFuk[3][3] = {};
+      T gIF[3][3][3] = {}, gIFuu[3][3][3] = {};
+      for (int ii = 0; ii < 4; ++ii) {
+        int a1 = SOD_INV(ii, isoJ, isoK), a2 = SOD_INV(isoI, ii, isoK), a3 = SOD_INV(isoI, isoJ, ii);
+        gIRho[0] += dlxi[ii] * rhol[a1]; gIRho[1] += dleta[ii] * rhol[a2]; gIRho[2] += dlzeta[ii] * rhol[a3];
+        gIP[0] += dlxi[ii] * prl[a1];    gIP[1] += dleta[ii] * prl[a2];    gIP[2] += dlzeta[ii] * prl[a3];
+        gIE[0] += dlxi[ii] * El[a1];     gIE[1] += dleta[ii] * El[a2];     gIE[2] += dlzeta[ii] * El[a3];
+        gIRE[0] += dlxi[ii] * REl[a1];   gIRE[1] += dleta[ii] * REl[a2];   gIRE[2] += dlzeta[ii] * REl[a3];
+        gIk[0] += dlxi[ii] * kl[a1];     gIk[1] += dleta[ii] * kl[a2];     gIk[2] += dlzeta[ii] * kl[a3];
+        gIRk[0] += dlxi[ii] * Rkl[a1];   gIRk[1] += dleta[ii] * Rkl[a2];   gIRk[2] += dlzeta[ii] * Rkl[a3];
+        for (int id = 0; id < 3; ++id) {
+          gIU[id][0] += dlxi[ii] * ul[a1][id];   gIU[id][1] += dleta[ii] * ul[a2][id];   gIU[id][2] += dlzeta[ii] * ul[a3][id];
+          gIQ[id][0] += dlxi[ii] * ql[a1][id];   gIQ[id][1] += dleta[ii] * ql[a2][id];   gIQ[id][2] += dlzeta[ii] * ql[a3][id];
+          gIFe[id][0] += dlxi[ii] * fel[a1][id]; gIFe[id][1] += dleta[ii] * fel[a2][id]; gIFe[id][2] += dlzeta[ii] * fel[a3][id];
+          gIFue[id][0] += dlxi[ii] * fuel[a1][id]; gIFue[id][1] += dleta[ii] * fuel[a2][id]; gIFue[id][2] += dlzeta[ii] * fuel[a3][id];
+          gIFk[id][0] += dlxi[ii] * fkl[a1][id]; gIFk[id][1] += dleta[ii] * fkl[a2][id]; gIFk[id][2] += dlzeta[ii] * fkl[a3][id];
+          gIFuk[id][0] += dlxi[ii] * fukl[a1][id]; gIFuk[id][1] += dleta[ii] * fukl[a2][id]; gIFuk[id][2] += dlzeta[ii] * fukl[a3][id];
+          for (int jd = 0; jd < 3; ++jd) {
+            gIF[id][jd][0] += dlxi[ii] * fl[a1][id][jd];
+            gIF[id][jd][1] += dleta[ii] * fl[a2][id][jd];
+            gIF[id][jd][2] += dlzeta[ii] * fl[a3][id][jd];
+            gIFuu[id][jd][0] += dlxi[ii] * fuul[a1][id][jd];
+            gIFuu[id][jd][1] += dleta[ii] * fuul[a2][id][jd];
+            gIFuu[id][jd][2] += dlzeta[ii] * fuul[a3][id][jd];
+          }
+        }
+      }
+      T gradRho[3] = {0, 0, 0}, gradP[3] = {0, 0, 0}, gradE[3] = {0, 0, 0}, gradRE[3] = {0, 0, 0},
+             gradk[3] = {0, 0, 0}, gradRk[3] = {0, 0, 0};
+      T gradU[3][3] = {}, gradQ[3][3] = {}, divF[3] = {0, 0, 0}, divFuu[3] = {0, 0, 0};
+      T divFe = 0, divFue = 0, divFk = 0, divFuk = 0;
+      for (int id = 0; id < 3; ++id)
+        for (int jd = 0; jd < 3; ++jd) {
+          double h = SOD_HE(id, jd, igaus, ielem);
+          gradRho[id] += h * gIRho[jd];
+          gradP[id] += h * gIP[jd];
+          gradE[id] += h * gIE[jd];
+          gradRE[id] += h * gIRE[jd];
+          divFe += h * gIFe[id][jd];
+          divFue += h * gIFue[id][jd];
+          gradk[id] += h * gIk[jd];
+          gradRk[id] += h * gIRk[jd];
+          divFk += h * gIFk[id][jd];
+          divFuk += h * gIFuk[id][jd];
+          for (int kd = 0; kd < 3; ++kd) {
+            double h2 = SOD_HE(jd, kd, igaus, ielem);
+            gradU[id][jd] += h2 * gIU[id][kd];
+            gradQ[id][jd] += h2 * gIQ[id][kd];
+            divF[id] += h2 * gIF[id][jd][kd];
+            divFuu[id] += h2 * gIFuu[id][jd][kd];
+          }
+        }
+      T divU = gradU[0][0] + gradU[1][1] + gradU[2][2];
+      T divQ = gradQ[0][0] + gradQ[1][1] + gradQ[2][2];
+      Re_mass[igaus] = 0.5 * (divQ + rhol[igaus] * divU);
+      Re_ener[igaus] = 0.25 * (divFe + El[igaus] * divQ + REl[igaus] * divU + rhol[igaus] * divFue) +
+                       0.25 * (divFk + kl[igaus] * divQ + Rkl[igaus] * divU + rhol[igaus] * divFuk);
+      for (int id = 0; id < 3; ++id) {
+        Re_mom[igaus][id] = 0.25 * (divF[id] + ul[igaus][id] * divQ + ql[igaus][id] * divU +
+                                    rhol[igaus] * divFuu[id]) + gradP[id];
+        Re_mass[igaus] = Re_mass[igaus] + 0.5 * (ul[igaus][id] * gradRho[id]);
+        Re_ener[igaus] = Re_ener[igaus] +
+                         0.25 * (ql[igaus][id] * gradE[id] + ul[igaus][id] * gradRE[id] + fuel[igaus][id] * gradRho[id]) +
+                         0.25 * (ql[igaus][id] * gradk[id] + ul[igaus][id] * gradRk[id] + fukl[igaus][id] * gradRho[id]);
+        for (int jd = 0; jd < 3; ++jd)
+          Re_mom[igaus][id] = Re_mom[igaus][id] + 0.25 * (fuul[igaus][id][jd] * gradRho[jd] +
+                                                          ql[igaus][jd] * gradU[id][jd] + ul[igaus][jd] * gradQ[id][jd]);
+        Re_mom[igaus][id] = SOD_GPVOL(igaus, ielem) * Re_mom[igaus][id];
+      }
+      Re_mass[igaus] = SOD_GPVOL(igaus, ielem) * Re_mass[igaus];
+      Re_ener[igaus] = SOD_GPVOL(igaus, ielem) * Re_ener[igaus];
+    }
+    for (int d = 0; d < 3; ++d)
+      for (int a = 0; a < nnode; ++a) Rmom[ipoin[a] + (int64_t)npoin * d] += Re_mom[a][d];
+    for (int a = 0; a < nnode; ++a) {
+      Rmass[ipoin[a]] += Re_mass[a];
+      Rener[ipoin[a]] += Re_ener[a];
+    }
+  });
+}
+
+template <class T>
+inline void full_diffusion_ijk_t(const ElemCtx& ctx, const Params& P, const T* rho_n,
+                               const T* rho, const T* u, const T* Tem,
+                               const T* mu_fluid, const double* mu_e, const double* mu_sgs,
+                               T* Rmass, T* Rmom, T* Rener) {
+  const int nelem = ctx.nelem, npoin = ctx.npoin;
+  const double Cp = P.Cp, Pr = P.Prt, c_rho = P.c_rho, c_ener = P.c_ener;
+  const double twoThirds = 2.0 / 3.0;
+  (void)rho;
+  for (int p = 0; p < npoin; ++p) { Rmass[p] = 0.0; Rener[p] = 0.0; }
+  for (int64_t p = 0; p < (int64_t)npoin * 3; ++p) Rmom[p] = 0.0;
+  for_each_element_coloured(ctx, [&](int ielem) {
+    int ipoin[nnode];
+    T ul[nnode][3], rhol[nnode], Teml[nnode], mufluidl[nnode], rhonl[nnode];
+    T tauXl[nnode][3], tauYl[nnode][3], tauZl[nnode][3], gradTl[nnode][3], gradRhol[nnode][3],
+        tauUl[nnode][3];
+    for (int a = 0; a < nnode; ++a) ipoin[a] = ctx.connec[ielem + (int64_t)nelem * a];
+    for (int a = 0; a < nnode; ++a) {
+      rhol[a] = rho[ipoin[a]];
+      rhonl[a] = rho_n[ipoin[a]];
+      Teml[a] = Tem[ipoin[a]];
+      mufluidl[a] = mu_fluid[ipoin[a]];
+    }
+    for (int a = 0; a < nnode; ++a)
+      for (int d = 0; d < 3; ++d) ul[a][d] = u[ipoin[a] + (int64_t)npoin * d];
+    for (int igaus = 0; igaus < ngaus; ++igaus) {
+      T mu_fgp = mufluidl[igaus] + rhonl[igaus] * mu_sgs[ielem + (int64_t)nelem * igaus];
+      double mu_egp = mu_e[ielem + (int64_t)nelem * igaus];
+      int isoI = ctx.gmshAtoI[igaus], isoJ = ctx.gmshAtoJ[igaus], isoK = ctx.gmshAtoK[igaus];
+      T gIRho[3] = {0, 0, 0}, gIT[3] = {0, 0, 0}, gIU[3][3] = {};
+      for (int ii = 0; ii < 4; ++ii) {
+        int a1 = SOD_INV(ii, isoJ, isoK), a2 = SOD_INV(isoI, ii, isoK), a3 = SOD_INV(isoI, isoJ, ii);
+        double d1 = SOD_DL(igaus, 0, ii), d2 = SOD_DL(igaus, 1, ii), d3 = SOD_DL(igaus, 2, ii);
+        gIRho[0] += d1 * rhol[a1]; gIRho[1] += d2 * rhol[a2]; gIRho[2] += d3 * rhol[a3];
+        gIT[0] += d1 * Teml[a1]; gIT[1] += d2 * Teml[a2]; gIT[2] += d3 * Teml[a3];
+        for (int id = 0; id < 3; ++id) {
+          gIU[id][0] += d1 * ul[a1][id]; gIU[id][1] += d2 * ul[a2][id]; gIU[id][2] += d3 * ul[a3][id];
+        }
+      }
+      T gradRho[3] = {0, 0, 0}, gradT[3] = {0, 0, 0}, gradU[3][3] = {};
+      for (int id = 0; id < 3; ++id)
+        for (int jd = 0; jd < 3; ++jd) {
+          double h = SOD_HE(id, jd, igaus, ielem);
+          gradRho[id] += h * gIRho[jd];
+          gradT[id] += h * gIT[jd];
+          for (int kd = 0; kd < 3; ++kd) gradU[id][jd] += SOD_HE(jd, kd, igaus, ielem) * gIU[id][kd];
+        }
+      T divU = gradU[0][0] + gradU[1][1] + gradU[2][2];
+      T tauU[3] = {0, 0, 0}, tau[3][3];
+      for (int id = 0; id < 3; ++id) {
+        for (int jd = 0; jd < 3; ++jd) {
+          tauU[id] = tauU[id] + (mu_fgp + mu_egp) * (gradU[id][jd] + gradU[jd][id]) * ul[igaus][jd];
+          tau[id][jd] = (mu_fgp + mu_egp) * (gradU[id][jd] + gradU[jd][id]);
+        }
+        tauU[id] = tauU[id] - (mu_fgp) * twoThirds * divU * ul[igaus][id];
+        tau[id][id] = tau[id][id] - (mu_fgp) * twoThirds * divU;
+      }
+      for (int id = 0; id < 3; ++id) {
+        tauXl[igaus][id] = tau[0][id];
+        tauYl[igaus][id] = tau[1][id];
+        tauZl[igaus][id] = tau[2][id];
+        gradTl[igaus][id] = gradT[id];
+        gradRhol[igaus][id] = gradRho[id];
+        tauUl[igaus][id] = tauU[id];
+      }
+    }
+    T Rm_l[nnode], Re_l[nnode], Rmo_l[nnode][3];
+    for (int igaus = 0; igaus < ngaus; ++igaus) {
+      double mue = mu_e[ielem + (int64_t)nelem * igaus];
+      double musgs = mu_sgs[ielem + (int64_t)nelem * igaus];
+      T nu_e = c_rho * mue / rhonl[igaus];
+      T kappa_e = mufluidl[igaus] * Cp / Pr + c_ener * mue * Cp / Pr + Cp * rhonl[igaus] * musgs / 0.9;
+      int isoI = ctx.gmshAtoI[igaus], isoJ = ctx.gmshAtoJ[igaus], isoK = ctx.gmshAtoK[igaus];
+      T divDe = 0.0, divDr = 0.0, divDm[3] = {0, 0, 0};
+      for (int ii = 0; ii < 4; ++ii) {
+        int a1 = SOD_INV(ii, isoJ, isoK), a2 = SOD_INV(isoI, ii, isoK), a3 = SOD_INV(isoI, isoJ, ii);
+        for (int id = 0; id < 3; ++id) {
+          double w1 = SOD_HE(id, 0, a1, ielem) * SOD_GPVOL(a1, ielem) * SOD_DL(a1, 0, isoI);
+          double w2 = SOD_HE(id, 1, a2, ielem) * SOD_GPVOL(a2, ielem) * SOD_DL(a2, 1, isoJ);
+          double w3 = SOD_HE(id, 2, a3, ielem) * SOD_GPVOL(a3, ielem) * SOD_DL(a3, 2, isoK);
+          divDr = divDr + w1 * gradRhol[a1][id];
+          divDr = divDr + w2 * gradRhol[a2][id];
+          divDr = divDr + w3 * gradRhol[a3][id];
+          divDe = divDe + w1 * (tauUl[a1][id] + kappa_e * gradTl[a1][id]);
+          divDe = divDe + w2 * (tauUl[a2][id] + kappa_e * gradTl[a2][id]);
+          divDe = divDe + w3 * (tauUl[a3][id] + kappa_e * gradTl[a3][id]);
+          divDm[0] = divDm[0] + w1 * tauXl[a1][id];
+          divDm[0] = divDm[0] + w2 * tauXl[a2][id];
+          divDm[0] = divDm[0] + w3 * tauXl[a3][id];
+          divDm[1] = divDm[1] + w1 * tauYl[a1][id];
+          divDm[1] = divDm[1] + w2 * tauYl[a2][id];
+          divDm[1] = divDm[1] + w3 * tauYl[a3][id];
+          divDm[2] = divDm[2] + w1 * tauZl[a1][id];
+          divDm[2] = divDm[2] + w2 * tauZl[a2][id];
+          divDm[2] = divDm[2] + w3 * tauZl[a3][id];
+        }
+      }
+      Rm_l[igaus] = nu_e * divDr;
+      Re_l[igaus] = divDe;
+      for (int d = 0; d < 3; ++d) Rmo_l[igaus][d] = divDm[d];
+    }
+    for (int igaus = 0; igaus < ngaus; ++igaus) {
+      Rmass[ipoin[igaus]] += Rm_l[igaus];
+      Rener[ipoin[igaus]] += Re_l[igaus];
+      for (int d = 0; d < 3; ++d) Rmom[ipoin[igaus] + (int64_t)npoin * d] += Rmo_l[igaus][d];
+    }
+  });
+}
+
+// The stage RHS of rk_4_main without the entropy residual (time_integ.f90:266-393): EOS,
+// Sutherland, full_diffusion_ijk + full_convec_ijk (energy with h), sum, /Ml.  State in
+// (rho, q(npoin,3), E); R is 5 columns of npoin: mass, mom x3, energy.  mu_e frozen.
+template <class T>
+inline void rhs_stage_t(const ElemCtx& ctx, const Params& P, const double* Ml, const double* mu_factor,
+                        const double* mu_e, const double* mu_sgs, const T* rho, const T* q, const T* E, T* R) {
+  const int npoin = ctx.npoin;
+  const int64_t N = npoin;
+  const double g = P.gamma_gas, Rgas = P.Rgas;
+  std::vector<T> u(3 * N), pr(N), h(N), Tem(N), muf(N), Rm(N), Rmo(3 * N), Re(N), Dm(N), Dmo(3 * N), De(N);
+  for (int p = 0; p < npoin; ++p) {
+    T umag = T(0.0);
+    for (int d = 0; d < 3; ++d) {
+      u[p + N * d] = q[p + N * d] / rho[p];
+      umag = umag + u[p + N * d] * u[p + N * d];
+    }
+    T e_int = (E[p] / rho[p]) - 0.5 * umag;
+    pr[p] = rho[p] * (g - 1.0) * e_int;
+    h[p] = (g / (g - 1.0)) * pr[p] / rho[p];
+    Tem[p] = pr[p] / (rho[p] * Rgas);
+    muf[p] = mu_factor[p] * 0.000001458 * pow(Tem[p], 1.5) / (Tem[p] + 110.4);
+  }
+  full_diffusion_ijk_t<T>(ctx, P, rho, rho, u.data(), Tem.data(), muf.data(), mu_e, mu_sgs, Dm.data(), Dmo.data(),
+                          De.data());
+  full_convec_ijk_t<T>(ctx, u.data(), q, rho, pr.data(), h.data(), Rm.data(), Rmo.data(), Re.data());
+  for (int p = 0; p < npoin; ++p) {
+    R[p] = (Rm[p] + Dm[p]) / Ml[p];
+    for (int d = 0; d < 3; ++d) R[p + N * (1 + d)] = (Rmo[p + N * d] + Dmo[p + N * d]) / Ml[p];
+    R[p + N * 4] = (Re[p] + De[p]) / Ml[p];
+  }
+}
+
 // smart_visc_spectral (mod_entropy_viscosity.f90:14-123) with init_filters weights and the
 // convertIJK map (mod_filters.f90:15-55).  helem_l is (nelem,nnode) (the dummy named helem),
 // helem is (nelem) (the dummy named helem_k).  Reductions in real(rp)=FP64.

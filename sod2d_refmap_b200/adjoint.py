@@ -1,0 +1,137 @@
+"""Checkpointed adjoint of K RK4 steps behind ``torch.autograd.Function``.
+
+The forward model is the FP64 ``rk_4_main`` time loop (time_integ.f90:137-493) with the entropy
+viscosity mu_e and the time step dt *frozen* along the trajectory: each step n uses the mu_e_n
+and dt_n that the undifferentiated solver produced for it (smart_visc_spectral and adapt_dt_cfl
+run in the forward pass, but their outputs are treated as constants).  The gradient therefore
+is the exact gradient of ``replay`` (the frozen-coefficient map), which is what the dot-product
+and finite-difference checks compare against.
+
+Memory: states (rho, q, E, mu_e, dt) are kept every ``checkpoint_every`` steps; the backward
+pass re-runs each segment from its checkpoint (bitwise identical, the solver is deterministic)
+and applies the hand-written step VJP (sod_rk4_step_vjp) in reverse.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+from .solver import FP64, Sod2dMesh, Sod2dState, _torch
+
+
+@dataclass
+class _Ckpt:
+    rho: object
+    q: object
+    E: object
+    mu_e: object
+    dt: object
+
+
+def _clone_state(src: Sod2dState) -> Sod2dState:
+    dst = Sod2dState(src.npoin, src.nelem)
+    for f in Sod2dState.FIELDS:
+        getattr(dst, f).copy_(getattr(src, f))
+    dst.dt.copy_(src.dt)
+    return dst
+
+
+def _ckpt(s: Sod2dState) -> _Ckpt:
+    return _Ckpt(s.rho.clone(), s.q.clone(), s.E.clone(), s.mu_e.clone(), s.dt.clone())
+
+
+def _load(s: Sod2dState, c: _Ckpt):
+    s.rho.copy_(c.rho)
+    s.q.copy_(c.q)
+    s.E.copy_(c.E)
+    s.mu_e.copy_(c.mu_e)
+    s.dt.copy_(c.dt)
+
+
+def rollout(mesh: Sod2dMesh, state: Sod2dState, nsteps: int, checkpoint_every: int = 10):
+    """Run nsteps FP64 steps in place (dt from the CFL condition after every step, as
+    rk_4_main) and return the checkpoints [(step index, _Ckpt)] at multiples of checkpoint_every."""
+    ck = []
+    for n in range(nsteps):
+        if n % checkpoint_every == 0:
+            ck.append((n, _ckpt(state)))
+        mesh.rk_4_main(state, FP64, update_dt=True)
+    return ck
+
+
+def replay(mesh: Sod2dMesh, state: Sod2dState, mu_e_seq, dt_seq):
+    """The frozen-coefficient forward map: step n with mu_e_seq[n] and dt_seq[n] (device (1,))."""
+    for mu_e, dt in zip(mu_e_seq, dt_seq):
+        state.mu_e.copy_(mu_e)
+        state.dt.copy_(dt)
+        mesh.rk_4_main(state, FP64, update_dt=False)
+    return state
+
+
+def trajectory_coefficients(mesh: Sod2dMesh, state: Sod2dState, nsteps: int):
+    """(mu_e_n, dt_n) of each step of the unfrozen forward run from a copy of state."""
+    s = _clone_state(state)
+    mus, dts = [], []
+    for _ in range(nsteps):
+        mus.append(s.mu_e.clone())
+        dts.append(s.dt.clone())
+        mesh.rk_4_main(s, FP64, update_dt=True)
+    return mus, dts
+
+
+def backward_through(mesh: Sod2dMesh, template: Sod2dState, ckpts, nsteps: int, bar_rho, bar_q, bar_E,
+                     store_stages: bool = True):
+    """Adjoint of nsteps steps: (bar_rho, bar_q, bar_E) at step nsteps -> at step 0, in place.
+    Each segment is re-run from its checkpoint; with store_stages the re-run keeps the RK stage
+    states (15*npoin doubles per step) so that the step VJPs need no second recompute."""
+    torch = _torch()
+    s = _clone_state(template)
+    bounds = [c[0] for c in ckpts] + [nsteps]
+    longest = max(bounds[i + 1] - bounds[i] for i in range(len(ckpts)))
+    stages = (torch.empty(longest, 15 * s.npoin, dtype=torch.float64, device="cuda") if store_stages else None)
+    for seg in range(len(ckpts) - 1, -1, -1):
+        n0, c = ckpts[seg]
+        n1 = bounds[seg + 1]
+        _load(s, c)
+        stack = []
+        for t in range(n1 - n0):
+            stack.append(_ckpt(s))
+            if store_stages:
+                mesh.rk_4_main_record(s, stages[t], update_dt=True)
+            else:
+                mesh.rk_4_main(s, FP64, update_dt=True)
+        for t in range(n1 - n0 - 1, -1, -1):
+            cs = stack[t]
+            mesh.rk4_step_vjp(cs.rho, cs.q, cs.E, cs.mu_e, template.mu_factor, cs.dt, bar_rho, bar_q, bar_E,
+                              out=(bar_rho, bar_q, bar_E), stages=stages[t] if store_stages else None)
+    return bar_rho, bar_q, bar_E
+
+
+class Sod2dRollout:
+    """``Sod2dRollout.apply(mesh, state, rho, q, E, nsteps, checkpoint_every)`` -> (rho_K, q_K, E_K)
+    as a differentiable torch function of the initial conserved fields (rho, q, E)."""
+
+    @staticmethod
+    def apply(mesh: Sod2dMesh, state: Sod2dState, rho, q, E, nsteps: int, checkpoint_every: int = 10,
+              store_stages: bool = True):
+        torch = _torch()
+
+        class _Fn(torch.autograd.Function):
+            @staticmethod
+            def forward(ctx, rho_, q_, E_):
+                s = _clone_state(state)
+                s.rho.copy_(rho_)
+                s.q.copy_(q_)
+                s.E.copy_(E_)
+                ck = rollout(mesh, s, nsteps, checkpoint_every)
+                ctx.ck = ck
+                ctx.template = state
+                return s.rho.clone(), s.q.clone(), s.E.clone()
+
+            @staticmethod
+            def backward(ctx, g_rho, g_q, g_E):
+                z = lambda g, like: torch.zeros_like(like) if g is None else g.contiguous().clone()
+                br, bq, bE = z(g_rho, rho), z(g_q, q), z(g_E, E)
+                backward_through(mesh, ctx.template, ctx.ck, nsteps, br, bq, bE, store_stages)
+                return br, bq, bE
+
+        return _Fn.apply(rho, q, E)

@@ -1,0 +1,580 @@
+// Hand-written adjoint (vector-Jacobian product) of the stage RHS and of one RK4 step (sm_100a).
+//
+// The stage RHS is R(U) = (1/Ml) Gather_e[ gpvol * conv_e(U) + diff_e(U) ] with U = (rho, q, E),
+// conv from full_convec_ijk (elem_convec.f90:211-460, energy with h), diff from
+// full_diffusion_ijk (elem_diffu.f90:12-198), the stage EOS of time_integ.f90:266-285 and
+// Sutherland's law (mod_fluid_viscosity.f90:21-41) - Sutherland is differentiated, the entropy
+// viscosity mu_e is frozen at its forward value (it is updated once per step from the state
+// after the step, time_integ.f90:492-493), as is dt.
+//
+// k_rhs_vjp (one element per CTA, one thread per gauss point, FP64) recomputes the forward
+// derivative quantities, then runs the reverse sweep:
+//   diffusion  output seeds -> D applied along lines (the transpose of pass 2's D^T) ->
+//              contravariant-flux adjoints -> stress/heat-flux adjoints
+//   convection the split-form combination reversed pointwise
+//   both       derivative adjoints mapped back with He^T and D^T along lines to nodal product
+//              fields, then the product rule, the EOS and u = q/rho in reverse.
+// Element-node adjoints are assembled by the same ordered CSR gather as the forward path.
+#include "sod_internal.cuh"
+#include <cmath>
+
+namespace sod {
+int ensure_step_buffers(SodMesh* m, bool mixed);
+int launch_rhs(SodMesh* m, bool mixed, int epb, const double* rho, const double* q0, const double* q1,
+               const double* q2, const double* E, const double* mu_factor, const double* musgs_int, cudaStream_t st);
+
+namespace adj {
+
+constexpr double kC1 = 0.000001458;
+constexpr double kS = 110.4;
+// forward fields staged in shared memory
+enum { F_RHO = 0, F_H, F_RH, F_K, F_RK, F_U0, F_U1, F_U2, F_Q0, F_Q1, F_Q2, F_T,
+       F_FUE0, F_FUE1, F_FUE2, F_FUK0, F_FUK1, F_FUK2, F_UU00, F_UU01, F_UU02, F_UU11, F_UU12, F_UU22, NF_FWD };
+// adjoint fields (nodal product fields receiving D^T sums)
+enum { A_RHO = 0, A_P, A_H, A_RH, A_K, A_RK, A_T, A_U0, A_U1, A_U2, A_Q0, A_Q1, A_Q2,
+       A_FE0, A_FE1, A_FE2, A_FUE0, A_FUE1, A_FUE2, A_FK0, A_FK1, A_FK2, A_FUK0, A_FUK1, A_FUK2,
+       A_F00, A_F01, A_F02, A_F10, A_F11, A_F12, A_F20, A_F21, A_F22,
+       A_UU00, A_UU01, A_UU02, A_UU11, A_UU12, A_UU22, NF_ADJ };
+
+constexpr size_t kSmemBytes = sizeof(double) * FSTRIDE * (size_t)(3 * NF_ADJ + 6 + 6);
+
+struct VjpArgs {
+  int nelem;
+  const int32_t* __restrict__ econn;
+  const double* __restrict__ geo;
+  const double* __restrict__ mue;        // internal [e][64]
+  const double* __restrict__ rho;
+  const double* __restrict__ q0;
+  const double* __restrict__ q1;
+  const double* __restrict__ q2;
+  const double* __restrict__ E;
+  const double* __restrict__ mu_factor;
+  const double* __restrict__ w;          // seeds / Ml: 5 columns of npoin (mass, mom x3, energy)
+  int64_t npoin;
+  double* out;                           // [e][5][64] element-node adjoints (rho, q x3, E)
+  DMat D;
+  DevParams prm;
+};
+
+__device__ __forceinline__ void giso_line(const double* f, int i, int j, int k, const double (&D)[NP1][NP1],
+                                          double& gx, double& gy, double& gz) {
+  gx = D[i][0] * f[sidx(0, j, k)] + D[i][1] * f[sidx(1, j, k)] + D[i][2] * f[sidx(2, j, k)] + D[i][3] * f[sidx(3, j, k)];
+  gy = D[j][0] * f[sidx(i, 0, k)] + D[j][1] * f[sidx(i, 1, k)] + D[j][2] * f[sidx(i, 2, k)] + D[j][3] * f[sidx(i, 3, k)];
+  gz = D[k][0] * f[sidx(i, j, 0)] + D[k][1] * f[sidx(i, j, 1)] + D[k][2] * f[sidx(i, j, 2)] + D[k][3] * f[sidx(i, j, 3)];
+}
+
+// sum_m D[m][i] fx(m,j,k) + D[m][j] fy(i,m,k) + D[m][k] fz(i,j,m)
+__device__ __forceinline__ double divT_line(const double* fx, const double* fy, const double* fz, int i, int j, int k,
+                                            const double (&D)[NP1][NP1]) {
+  double s = 0.0;
+#pragma unroll
+  for (int m = 0; m < NP1; ++m)
+    s += D[m][i] * fx[sidx(m, j, k)] + D[m][j] * fy[sidx(i, m, k)] + D[m][k] * fz[sidx(i, j, m)];
+  return s;
+}
+
+__global__ void __launch_bounds__(64) k_rhs_vjp(const VjpArgs a) {
+  extern __shared__ __align__(16) double sm[];
+  double* G = sm;                                   // adjoint line arrays [NF_ADJ][3][FSTRIDE]
+  double* S6 = sm + (size_t)3 * NF_ADJ * FSTRIDE;    // diffusion output seeds [6][FSTRIDE]
+  double* V6 = S6 + 6 * FSTRIDE;                     // contravariant gradRho/gradT [6][FSTRIDE]
+  double* Fw = G;                                    // forward fields reuse the adjoint area
+  __shared__ DMat Ds;
+  const int e = blockIdx.x, d = threadIdx.x;
+  const int i = d & 3, j = (d >> 2) & 3, k = d >> 4, s = sidx(i, j, k);
+  if (d < 16) Ds.d[d >> 2][d & 3] = a.D.d[d >> 2][d & 3];
+  const double* Ge = a.geo + (size_t)e * NGEO * NN;
+  double H[9];
+#pragma unroll
+  for (int c = 0; c < 9; ++c) H[c] = Ge[c * NN + d];
+  const double gpv = Ge[9 * NN + d];
+  const int n = a.econn[(size_t)e * NN + d];
+  const double g = a.prm.gamma, Rg = a.prm.Rgas;
+  const double rho = a.rho[n];
+  const double qv[3] = {a.q0[n], a.q1[n], a.q2[n]};
+  const double Et = a.E[n];
+  const double uv[3] = {qv[0] / rho, qv[1] / rho, qv[2] / rho};
+  const double umag = uv[0] * uv[0] + uv[1] * uv[1] + uv[2] * uv[2];
+  const double kk = 0.5 * umag;
+  const double p = rho * (g - 1.0) * ((Et / rho) - 0.5 * umag);
+  const double h = (g / (g - 1.0)) * p / rho;
+  const double T = p / (rho * Rg);
+  const double mf = a.mu_factor[n];
+  const double muf = mf * kC1 * (T * sqrt(T)) / (T + kS);
+  const double dmuf_dT = mf * kC1 * (1.5 * sqrt(T) * (T + kS) - T * sqrt(T)) / ((T + kS) * (T + kS));
+  const double mue = a.mue[(size_t)e * NN + d];
+
+  // ---------------- forward recompute of the derivative quantities ----------------
+  Fw[F_RHO * FSTRIDE + s] = rho;
+  Fw[F_H * FSTRIDE + s] = h;
+  Fw[F_RH * FSTRIDE + s] = rho * h;
+  Fw[F_K * FSTRIDE + s] = kk;
+  Fw[F_RK * FSTRIDE + s] = rho * kk;
+  Fw[F_T * FSTRIDE + s] = T;
+  for (int c = 0; c < 3; ++c) {
+    Fw[(F_U0 + c) * FSTRIDE + s] = uv[c];
+    Fw[(F_Q0 + c) * FSTRIDE + s] = qv[c];
+    Fw[(F_FUE0 + c) * FSTRIDE + s] = h * uv[c];
+    Fw[(F_FUK0 + c) * FSTRIDE + s] = kk * uv[c];
+  }
+  Fw[F_UU00 * FSTRIDE + s] = uv[0] * uv[0];
+  Fw[F_UU01 * FSTRIDE + s] = uv[0] * uv[1];
+  Fw[F_UU02 * FSTRIDE + s] = uv[0] * uv[2];
+  Fw[F_UU11 * FSTRIDE + s] = uv[1] * uv[1];
+  Fw[F_UU12 * FSTRIDE + s] = uv[1] * uv[2];
+  Fw[F_UU22 * FSTRIDE + s] = uv[2] * uv[2];
+  __syncthreads();
+  auto grad = [&](int f, double* o) {
+    double gx, gy, gz;
+    giso_line(Fw + f * FSTRIDE, i, j, k, Ds.d, gx, gy, gz);
+    for (int r = 0; r < 3; ++r) o[r] = H[3 * r] * gx + H[3 * r + 1] * gy + H[3 * r + 2] * gz;
+  };
+  auto divg = [&](int f0) {
+    double sd = 0.0;
+    for (int c = 0; c < 3; ++c) {
+      double o[3];
+      grad(f0 + c, o);
+      sd += o[c];
+    }
+    return sd;
+  };
+  double gRho[3], gH[3], gRH[3], gK[3], gRK[3], gU[3][3], gQ[3][3], gT[3];
+  grad(F_RHO, gRho); grad(F_H, gH); grad(F_RH, gRH); grad(F_K, gK); grad(F_RK, gRK); grad(F_T, gT);
+  for (int c = 0; c < 3; ++c) { grad(F_U0 + c, gU[c]); grad(F_Q0 + c, gQ[c]); }
+  const double divFue = divg(F_FUE0), divFuk = divg(F_FUK0);
+  double divFuu[3];
+  {
+    // rows of the symmetric u x u: row0 = (00,01,02), row1 = (01,11,12), row2 = (02,12,22)
+    const int rows[3][3] = {{F_UU00, F_UU01, F_UU02}, {F_UU01, F_UU11, F_UU12}, {F_UU02, F_UU12, F_UU22}};
+    for (int r = 0; r < 3; ++r) {
+      double sd = 0.0;
+      for (int c = 0; c < 3; ++c) {
+        double o[3];
+        grad(rows[r][c], o);
+        sd += o[c];
+      }
+      divFuu[r] = sd;
+    }
+  }
+  const double divU = gU[0][0] + gU[1][1] + gU[2][2];
+  const double divQ = gQ[0][0] + gQ[1][1] + gQ[2][2];
+  // diffusion pass 1 (stresses) and the contravariant gradRho / gradT fluxes for pass 2
+  const double mut = muf + mue;
+  double tau[3][3];
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c) tau[r][c] = mut * (gU[r][c] + gU[c][r]);
+  for (int r = 0; r < 3; ++r) tau[r][r] -= muf * (2.0 / 3.0) * divU;
+  for (int dir = 0; dir < 3; ++dir) {
+    V6[dir * FSTRIDE + s] = gpv * (H[dir] * gRho[0] + H[3 + dir] * gRho[1] + H[6 + dir] * gRho[2]);
+    V6[(3 + dir) * FSTRIDE + s] = gpv * (H[dir] * gT[0] + H[3 + dir] * gT[1] + H[6 + dir] * gT[2]);
+  }
+  __syncthreads();  // forward fields no longer needed; V6 complete
+  const double divDr = divT_line(V6, V6 + FSTRIDE, V6 + 2 * FSTRIDE, i, j, k, Ds.d);
+  const double divDgT = divT_line(V6 + 3 * FSTRIDE, V6 + 4 * FSTRIDE, V6 + 5 * FSTRIDE, i, j, k, Ds.d);
+
+  // ---------------- reverse sweep ----------------
+  const int64_t N = a.npoin;
+  const double wm = a.w[n], we = a.w[n + 4 * N];
+  const double wmo[3] = {a.w[n + N], a.w[n + 2 * N], a.w[n + 3 * N]};
+  double rb = 0.0, hb = 0.0, kb = 0.0, pb = 0.0, Tb = 0.0, mufb = 0.0;
+  double ub[3] = {0, 0, 0}, qb[3] = {0, 0, 0};
+  double gRhob[3] = {0, 0, 0}, gPb[3] = {0, 0, 0}, gHb[3] = {0, 0, 0}, gRHb[3] = {0, 0, 0}, gKb[3] = {0, 0, 0},
+         gRKb[3] = {0, 0, 0}, gTb[3] = {0, 0, 0};
+  double gUb[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}}, gQb[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+  double dFeb = 0.0, dFueb = 0.0, dFkb = 0.0, dFukb = 0.0, divUb = 0.0, divQb = 0.0;
+  double dFb[3] = {0, 0, 0}, dFuub[3] = {0, 0, 0};
+
+  // diffusion outputs (elem_diffu.f90:143-193): nu_e*divD(gradRho), divD(tauU) + kappa*divD(gradT),
+  // divD(tau row r); nu_e and kappa belong to the output node
+  const double CpPr = a.prm.Cp / a.prm.Prt;
+  const double nu_e = a.prm.c_rho * mue / rho;
+  const double kappa = muf * CpPr + a.prm.c_ener * mue * CpPr;
+  rb += wm * divDr * (-a.prm.c_rho * mue / (rho * rho));
+  mufb += we * divDgT * CpPr;
+  S6[0 * FSTRIDE + s] = nu_e * wm;
+  S6[1 * FSTRIDE + s] = we;
+  S6[2 * FSTRIDE + s] = kappa * we;
+  for (int r = 0; r < 3; ++r) S6[(3 + r) * FSTRIDE + s] = wmo[r];
+  __syncthreads();
+  {
+    double taub[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+    for (int v = 0; v < 6; ++v) {
+      double gx, gy, gz;
+      giso_line(S6 + v * FSTRIDE, i, j, k, Ds.d, gx, gy, gz);  // adjoint of D^T: D along lines
+      double Vb[3];
+      for (int r = 0; r < 3; ++r) Vb[r] = gpv * (H[3 * r] * gx + H[3 * r + 1] * gy + H[3 * r + 2] * gz);
+      if (v == 0) {
+        for (int r = 0; r < 3; ++r) gRhob[r] += Vb[r];
+      } else if (v == 1) {  // tauU_r = sum_c tau_rc u_c
+        for (int r = 0; r < 3; ++r)
+          for (int c = 0; c < 3; ++c) {
+            taub[r][c] += Vb[r] * uv[c];
+            ub[c] += Vb[r] * tau[r][c];
+          }
+      } else if (v == 2) {
+        for (int r = 0; r < 3; ++r) gTb[r] += Vb[r];
+      } else {
+        for (int c = 0; c < 3; ++c) taub[v - 3][c] += Vb[c];
+      }
+    }
+    // tau_rc = (muf+mue)(du_r/dx_c + du_c/dx_r) - delta_rc muf 2/3 div u
+    for (int r = 0; r < 3; ++r)
+      for (int c = 0; c < 3; ++c) {
+        gUb[r][c] += mut * taub[r][c];
+        gUb[c][r] += mut * taub[r][c];
+        mufb += taub[r][c] * (gU[r][c] + gU[c][r]);
+      }
+    for (int r = 0; r < 3; ++r) {
+      mufb += -taub[r][r] * (2.0 / 3.0) * divU;
+      divUb += -muf * (2.0 / 3.0) * taub[r][r];
+    }
+  }
+
+  // convection (elem_convec.f90:412-434), seeds times gpvol
+  {
+    const double mm = gpv * wm, me = gpv * we;
+    const double mc[3] = {gpv * wmo[0], gpv * wmo[1], gpv * wmo[2]};
+    const double rh = rho * h, rk = rho * kk;
+    // mass
+    divQb += 0.5 * mm; rb += 0.5 * divU * mm; divUb += 0.5 * rho * mm;
+    for (int c = 0; c < 3; ++c) { ub[c] += 0.5 * gRho[c] * mm; gRhob[c] += 0.5 * uv[c] * mm; }
+    // energy
+    dFeb += 0.25 * me; hb += 0.25 * divQ * me; divQb += 0.25 * h * me;
+    rb += 0.25 * h * divU * me; hb += 0.25 * rho * divU * me; divUb += 0.25 * rh * me;
+    rb += 0.25 * divFue * me; dFueb += 0.25 * rho * me;
+    dFkb += 0.25 * me; kb += 0.25 * divQ * me; divQb += 0.25 * kk * me;
+    rb += 0.25 * kk * divU * me; kb += 0.25 * rho * divU * me; divUb += 0.25 * rk * me;
+    rb += 0.25 * divFuk * me; dFukb += 0.25 * rho * me;
+    for (int c = 0; c < 3; ++c) {
+      qb[c] += 0.25 * gH[c] * me; gHb[c] += 0.25 * qv[c] * me;
+      ub[c] += 0.25 * gRH[c] * me; gRHb[c] += 0.25 * uv[c] * me;
+      hb += 0.25 * uv[c] * gRho[c] * me; ub[c] += 0.25 * h * gRho[c] * me; gRhob[c] += 0.25 * h * uv[c] * me;
+      qb[c] += 0.25 * gK[c] * me; gKb[c] += 0.25 * qv[c] * me;
+      ub[c] += 0.25 * gRK[c] * me; gRKb[c] += 0.25 * uv[c] * me;
+      kb += 0.25 * uv[c] * gRho[c] * me; ub[c] += 0.25 * kk * gRho[c] * me; gRhob[c] += 0.25 * kk * uv[c] * me;
+    }
+    // momentum
+    for (int c = 0; c < 3; ++c) {
+      const double mu_c = mc[c];
+      dFb[c] += 0.25 * mu_c;
+      ub[c] += 0.25 * divQ * mu_c; divQb += 0.25 * uv[c] * mu_c;
+      qb[c] += 0.25 * divU * mu_c; divUb += 0.25 * qv[c] * mu_c;
+      rb += 0.25 * divFuu[c] * mu_c; dFuub[c] += 0.25 * rho * mu_c;
+      gPb[c] += mu_c;
+      for (int jd = 0; jd < 3; ++jd) {
+        ub[c] += 0.25 * uv[jd] * gRho[jd] * mu_c;
+        ub[jd] += 0.25 * uv[c] * gRho[jd] * mu_c;
+        gRhob[jd] += 0.25 * uv[c] * uv[jd] * mu_c;
+        qb[jd] += 0.25 * gU[c][jd] * mu_c;
+        gUb[c][jd] += 0.25 * qv[jd] * mu_c;
+        ub[jd] += 0.25 * gQ[c][jd] * mu_c;
+        gQb[c][jd] += 0.25 * uv[jd] * mu_c;
+      }
+    }
+    for (int c = 0; c < 3; ++c) {
+      gUb[c][c] += divUb;
+      gQb[c][c] += divQb;
+    }
+  }
+
+  // derivative adjoints -> iso adjoints (He^T) in shared memory, 3 line arrays per field
+  {
+    auto putg = [&](int f, const double* gb) {
+      for (int dir = 0; dir < 3; ++dir)
+        G[(f * 3 + dir) * FSTRIDE + s] = H[dir] * gb[0] + H[3 + dir] * gb[1] + H[6 + dir] * gb[2];
+    };
+    auto putd = [&](int f, int comp, double db) {  // field is component comp of a vector whose divergence has adjoint db
+      for (int dir = 0; dir < 3; ++dir) G[(f * 3 + dir) * FSTRIDE + s] = H[3 * comp + dir] * db;
+    };
+    putg(A_RHO, gRhob); putg(A_P, gPb); putg(A_H, gHb); putg(A_RH, gRHb); putg(A_K, gKb); putg(A_RK, gRKb);
+    putg(A_T, gTb);
+    for (int c = 0; c < 3; ++c) {
+      putg(A_U0 + c, gUb[c]);
+      putg(A_Q0 + c, gQb[c]);
+      putd(A_FE0 + c, c, dFeb);
+      putd(A_FUE0 + c, c, dFueb);
+      putd(A_FK0 + c, c, dFkb);
+      putd(A_FUK0 + c, c, dFukb);
+      for (int jd = 0; jd < 3; ++jd) putd(A_F00 + 3 * c + jd, jd, dFb[c]);
+    }
+    for (int dir = 0; dir < 3; ++dir) {
+      G[(A_UU00 * 3 + dir) * FSTRIDE + s] = H[dir] * dFuub[0];
+      G[(A_UU01 * 3 + dir) * FSTRIDE + s] = H[3 + dir] * dFuub[0] + H[dir] * dFuub[1];
+      G[(A_UU02 * 3 + dir) * FSTRIDE + s] = H[6 + dir] * dFuub[0] + H[dir] * dFuub[2];
+      G[(A_UU11 * 3 + dir) * FSTRIDE + s] = H[3 + dir] * dFuub[1];
+      G[(A_UU12 * 3 + dir) * FSTRIDE + s] = H[6 + dir] * dFuub[1] + H[3 + dir] * dFuub[2];
+      G[(A_UU22 * 3 + dir) * FSTRIDE + s] = H[6 + dir] * dFuub[2];
+    }
+  }
+  __syncthreads();
+  auto Wb = [&](int f) {
+    return divT_line(G + (f * 3 + 0) * FSTRIDE, G + (f * 3 + 1) * FSTRIDE, G + (f * 3 + 2) * FSTRIDE, i, j, k, Ds.d);
+  };
+  // nodal product fields -> primitives (product rule)
+  rb += Wb(A_RHO);
+  pb += Wb(A_P);
+  hb += Wb(A_H);
+  { const double t = Wb(A_RH); rb += h * t; hb += rho * t; }
+  kb += Wb(A_K);
+  { const double t = Wb(A_RK); rb += kk * t; kb += rho * t; }
+  Tb += Wb(A_T);
+  for (int c = 0; c < 3; ++c) {
+    ub[c] += Wb(A_U0 + c);
+    qb[c] += Wb(A_Q0 + c);
+    { const double t = Wb(A_FE0 + c); rb += h * uv[c] * t; hb += rho * uv[c] * t; ub[c] += rho * h * t; }
+    { const double t = Wb(A_FUE0 + c); hb += uv[c] * t; ub[c] += h * t; }
+    { const double t = Wb(A_FK0 + c); rb += kk * uv[c] * t; kb += rho * uv[c] * t; ub[c] += rho * kk * t; }
+    { const double t = Wb(A_FUK0 + c); kb += uv[c] * t; ub[c] += kk * t; }
+    for (int jd = 0; jd < 3; ++jd) {
+      const double t = Wb(A_F00 + 3 * c + jd);  // F_cj = q_c u_j
+      qb[c] += uv[jd] * t;
+      ub[jd] += qv[c] * t;
+    }
+  }
+  { const double t = Wb(A_UU00); ub[0] += 2.0 * uv[0] * t; }
+  { const double t = Wb(A_UU11); ub[1] += 2.0 * uv[1] * t; }
+  { const double t = Wb(A_UU22); ub[2] += 2.0 * uv[2] * t; }
+  { const double t = Wb(A_UU01); ub[0] += uv[1] * t; ub[1] += uv[0] * t; }
+  { const double t = Wb(A_UU02); ub[0] += uv[2] * t; ub[2] += uv[0] * t; }
+  { const double t = Wb(A_UU12); ub[1] += uv[2] * t; ub[2] += uv[1] * t; }
+  // Sutherland, EOS and u = q/rho in reverse (time_integ.f90:266-285, mod_fluid_viscosity.f90:37)
+  Tb += mufb * dmuf_dT;
+  pb += hb * g / ((g - 1.0) * rho);
+  rb += -hb * h / rho;
+  pb += Tb / (rho * Rg);
+  rb += -Tb * T / rho;
+  const double Eb = (g - 1.0) * pb;
+  rb += -(g - 1.0) * kk * pb;
+  kb += -(g - 1.0) * rho * pb;
+  for (int c = 0; c < 3; ++c) ub[c] += uv[c] * kb;
+  for (int c = 0; c < 3; ++c) {
+    qb[c] += ub[c] / rho;
+    rb += -uv[c] * ub[c] / rho;
+  }
+  double* o = a.out + (size_t)e * NRES * NN + d;
+  o[0] = rb;
+  o[NN] = qb[0];
+  o[2 * NN] = qb[1];
+  o[3 * NN] = qb[2];
+  o[4 * NN] = Eb;
+  o[5 * NN] = 0.0;
+}
+
+}  // namespace adj
+}  // namespace sod
+
+// ---------------------------------------------------------------------------------------------
+// node-side kernels of the adjoint: seeds, ordered gathers, stage states
+// ---------------------------------------------------------------------------------------------
+namespace sod {
+namespace adj {
+
+struct Cols5 {
+  const double* c[5];
+};
+struct MCols5 {
+  double* c[5];
+};
+
+// w = scale * src / Ml (scale = -dt * coef when dt is given, else 1)
+__global__ void k_seed(int64_t N, Cols5 src, const double* __restrict__ Ml, const double* __restrict__ dt,
+                       double coef, double* __restrict__ w, MCols5 keep) {
+  const int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= N) return;
+  const double sc = dt ? -(*dt) * coef : 1.0;
+  const double inv = 1.0 / Ml[n];
+#pragma unroll
+  for (int f = 0; f < 5; ++f) {
+    const double v = src.c[f][n];
+    w[f * N + n] = sc * v * inv;
+    if (keep.c[f]) keep.c[f][n] = v;
+  }
+}
+
+// Ordered gather of the element-node adjoints [e][6][64] (ascending element order, like the
+// forward assembly).  Ybar = sum; out = Ybar (mode 0) or acc += Ybar (mode 1, acc = out);
+// when wnext is set: wnext = -dt (cb * ybar + ca * Ybar) / Ml.
+__global__ void __launch_bounds__(256) k_gather_vjp(int64_t N, const int32_t* __restrict__ ptr,
+                                                    const int32_t* __restrict__ idx, const double* __restrict__ el,
+                                                    MCols5 out, int mode, const double* __restrict__ ybar,
+                                                    const double* __restrict__ Ml, const double* __restrict__ dt,
+                                                    double cb, double ca, double* __restrict__ wnext) {
+  const int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= N) return;
+  double r[5] = {0, 0, 0, 0, 0};
+  const int beg = ptr[n], end = ptr[n + 1];
+  for (int c = beg; c < end; ++c) {
+    const int pk = idx[c];
+    const double* src = el + (size_t)(pk >> 6) * NRES * NN + (pk & 63);
+#pragma unroll
+    for (int f = 0; f < 5; ++f) r[f] += src[f * NN];
+  }
+#pragma unroll
+  for (int f = 0; f < 5; ++f) {
+    if (mode == 1) out.c[f][n] += r[f];
+    else out.c[f][n] = r[f];
+  }
+  if (wnext) {
+    const double sc = -(*dt) / Ml[n];
+#pragma unroll
+    for (int f = 0; f < 5; ++f) wnext[f * N + n] = sc * (cb * ybar[f * N + n] + ca * r[f]);
+  }
+}
+
+// stage state: ys = y - coef * dt * gather(rel)/Ml   (time_integ.f90:301-318)
+__global__ void __launch_bounds__(256) k_stage_state(int64_t N, const int32_t* __restrict__ ptr,
+                                                     const int32_t* __restrict__ idx, const double* __restrict__ el,
+                                                     const double* __restrict__ Ml, const double* __restrict__ dt,
+                                                     double coef, Cols5 y, double* __restrict__ ys) {
+  const int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= N) return;
+  double r[5] = {0, 0, 0, 0, 0};
+  const int beg = ptr[n], end = ptr[n + 1];
+  for (int c = beg; c < end; ++c) {
+    const int pk = idx[c];
+    const double* src = el + (size_t)(pk >> 6) * NRES * NN + (pk & 63);
+#pragma unroll
+    for (int f = 0; f < 5; ++f) r[f] += src[f * NN];
+  }
+  // same operation order as the forward stage gather, so the stage states match it bit for bit
+  const double ml = Ml[n];
+  const double da = (*dt) * coef;
+#pragma unroll
+  for (int f = 0; f < 5; ++f) ys[f * N + n] = y.c[f][n] - da * (r[f] / ml);
+}
+
+static int g_vjp_attr_done = 0;
+
+static int launch_vjp(SodMesh* m, const double* rho, const double* q0, const double* q1, const double* q2,
+                      const double* E, const double* mu_factor, const double* w, cudaStream_t st) {
+  if (!g_vjp_attr_done) {
+    SOD_CUDA(cudaFuncSetAttribute(k_rhs_vjp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBytes));
+    g_vjp_attr_done = 1;
+  }
+  VjpArgs a;
+  a.nelem = m->nelem;
+  a.econn = m->econn;
+  a.geo = m->geo64;
+  a.mue = m->mue_int;
+  a.rho = rho; a.q0 = q0; a.q1 = q1; a.q2 = q2; a.E = E;
+  a.mu_factor = mu_factor;
+  a.w = w;
+  a.npoin = m->npoin;
+  a.out = reinterpret_cast<double*>(m->buf.rel);
+  a.D = m->D;
+  a.prm = m->prm;
+  k_rhs_vjp<<<m->nelem, NN, kSmemBytes, st>>>(a);
+  SOD_CHECK_LAUNCH();
+  return SOD_OK;
+}
+
+static int ensure_adj(SodMesh* m, size_t len) {
+  if (m->adj_len >= len) return SOD_OK;
+  if (m->adj) cudaFree(m->adj);
+  m->adj = nullptr;
+  m->adj_len = 0;
+  SOD_CUDA(cudaMalloc(&m->adj, len * sizeof(double)));
+  m->adj_len = len;
+  return SOD_OK;
+}
+
+static inline unsigned nblk(int64_t n) { return (unsigned)((n + 255) / 256); }
+
+}  // namespace adj
+}  // namespace sod
+
+using namespace sod;
+using namespace sod::adj;
+
+extern "C" {
+
+int sod_rhs_vjp(SodMesh* m, const double* rho, const double* q, const double* E, const double* mu_e,
+                const double* mu_factor, const double* bar_Rmass, const double* bar_Rmom, const double* bar_Rener,
+                double* grad_rho, double* grad_q, double* grad_E, sod_stream_t stream) {
+  SOD_ARG(m && rho && q && E && mu_e && mu_factor, "inputs null");
+  SOD_ARG(bar_Rmass && bar_Rmom && bar_Rener && grad_rho && grad_q && grad_E, "adjoint arrays null");
+  cudaStream_t st = (cudaStream_t)stream;
+  int rc = ensure_step_buffers(m, false);
+  if (rc) return rc;
+  const int64_t N = m->npoin;
+  rc = ensure_adj(m, 5 * (size_t)N);
+  if (rc) return rc;
+  rc = mesh_ref_to_internal_elem(m, mu_e, m->mue_int, st);
+  if (rc) return rc;
+  double* w = m->adj;
+  Cols5 src{{bar_Rmass, bar_Rmom, bar_Rmom + N, bar_Rmom + 2 * N, bar_Rener}};
+  MCols5 none{{nullptr, nullptr, nullptr, nullptr, nullptr}};
+  k_seed<<<nblk(N), 256, 0, st>>>(N, src, m->Ml, nullptr, 1.0, w, none);
+  SOD_CHECK_LAUNCH();
+  rc = launch_vjp(m, rho, q, q + N, q + 2 * N, E, mu_factor, w, st);
+  if (rc) return rc;
+  MCols5 out{{grad_rho, grad_q, grad_q + N, grad_q + 2 * N, grad_E}};
+  k_gather_vjp<<<nblk(N), 256, 0, st>>>(N, m->n2e_ptr, m->n2e, reinterpret_cast<const double*>(m->buf.rel), out, 0,
+                                         nullptr, nullptr, nullptr, 0.0, 0.0, nullptr);
+  SOD_CHECK_LAUNCH();
+  return SOD_OK;
+}
+
+int sod_rk4_step_vjp(SodMesh* m, const double* rho, const double* q, const double* E, const double* mu_e,
+                     const double* mu_factor, const double* dt_dev, const double* stages, const double* bar_rho,
+                     const double* bar_q, const double* bar_E, double* out_rho, double* out_q, double* out_E,
+                     sod_stream_t stream) {
+  SOD_ARG(m && rho && q && E && mu_e && mu_factor && dt_dev, "inputs null");
+  SOD_ARG(bar_rho && bar_q && bar_E && out_rho && out_q && out_E, "adjoint arrays null");
+  cudaStream_t st = (cudaStream_t)stream;
+  int rc = ensure_step_buffers(m, false);
+  if (rc) return rc;
+  const int64_t N = m->npoin;
+  // scratch: ybar copy | w | (ys2 ys3 ys4 when the stages are not given)   (5 columns each)
+  rc = ensure_adj(m, (stages ? 10 : 25) * (size_t)N);
+  if (rc) return rc;
+  rc = mesh_ref_to_internal_elem(m, mu_e, m->mue_int, st);
+  if (rc) return rc;
+  double* yb = m->adj;
+  double* w = m->adj + 5 * N;
+  const double* ys[3];
+  const double* rel = reinterpret_cast<const double*>(m->buf.rel);
+  Cols5 y0{{rho, q, q + N, q + 2 * N, E}};
+  if (stages) {
+    for (int t = 0; t < 3; ++t) ys[t] = stages + (size_t)t * 5 * N;
+  } else {
+    // forward recompute of the stage states (mu_e and dt frozen)
+    const int epb = m->tuned_epb[0] ? m->tuned_epb[0] : 2;
+    const double acoef[3] = {0.5, 0.5, 1.0};
+    Cols5 cur = y0;
+    for (int t = 0; t < 3; ++t) {
+      double* b = m->adj + (size_t)(10 + 5 * t) * N;
+      rc = launch_rhs(m, false, epb, cur.c[0], cur.c[1], cur.c[2], cur.c[3], cur.c[4], mu_factor, nullptr, st);
+      if (rc) return rc;
+      k_stage_state<<<nblk(N), 256, 0, st>>>(N, m->n2e_ptr, m->n2e, rel, m->Ml, dt_dev, acoef[t], y0, b);
+      SOD_CHECK_LAUNCH();
+      ys[t] = b;
+      cur = Cols5{{b, b + N, b + 2 * N, b + 3 * N, b + 4 * N}};
+    }
+  }
+  // reverse sweep: kbar4 = -dt/6 ybar, Ybar4 = J4^T kbar4, kbar3 = -dt (ybar/3 + Ybar4), ...
+  Cols5 src{{bar_rho, bar_q, bar_q + N, bar_q + 2 * N, bar_E}};
+  MCols5 keep{{yb, yb + N, yb + 2 * N, yb + 3 * N, yb + 4 * N}};
+  k_seed<<<nblk(N), 256, 0, st>>>(N, src, m->Ml, dt_dev, 1.0 / 6.0, w, keep);
+  SOD_CHECK_LAUNCH();
+  MCols5 acc{{out_rho, out_q, out_q + N, out_q + 2 * N, out_E}};
+  // acc = ybar (copied from the kept columns, so out may alias bar)
+  for (int f = 0; f < 5; ++f)
+    SOD_CUDA(cudaMemcpyAsync(acc.c[f], keep.c[f], N * sizeof(double), cudaMemcpyDeviceToDevice, st));
+  const double cb[4] = {1.0 / 3.0, 1.0 / 3.0, 1.0 / 6.0, 0.0};
+  const double ca[4] = {1.0, 0.5, 0.5, 0.0};
+  for (int stage = 4; stage >= 1; --stage) {
+    const Cols5 ysrc = stage == 1 ? y0
+                                  : Cols5{{ys[stage - 2], ys[stage - 2] + N, ys[stage - 2] + 2 * N,
+                                           ys[stage - 2] + 3 * N, ys[stage - 2] + 4 * N}};
+    rc = launch_vjp(m, ysrc.c[0], ysrc.c[1], ysrc.c[2], ysrc.c[3], ysrc.c[4], mu_factor, w, st);
+    if (rc) return rc;
+    const int t = 4 - stage;
+    k_gather_vjp<<<nblk(N), 256, 0, st>>>(N, m->n2e_ptr, m->n2e, rel, acc, 1, yb, m->Ml, dt_dev, cb[t], ca[t],
+                                           stage > 1 ? w : nullptr);
+    SOD_CHECK_LAUNCH();
+  }
+  return SOD_OK;
+}
+
+}  // extern "C"

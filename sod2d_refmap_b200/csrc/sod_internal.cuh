@@ -145,6 +145,9 @@ struct SodMesh {
   int32_t* member_node_off = nullptr;  // [nmember+1] contiguous node ranges
   double* member_scal = nullptr;    // [nmember][2] eta mean, eta norm
   double* member_dt_bits = nullptr; // [nmember] scratch for the per-member dt min
+  // adjoint scratch (sod_adjoint.cu): stage states, seeds, accumulators
+  double* adj = nullptr;
+  size_t adj_len = 0;
 };
 
 namespace sod {

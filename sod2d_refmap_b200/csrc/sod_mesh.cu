@@ -253,7 +253,7 @@ void sod_mesh_destroy(SodMesh* m) {
     if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
   void* ptrs[] = {m->econn, m->geo64, m->geo32, m->Ml, m->helem, m->helem_l, m->jratio, m->n2e_ptr, m->n2e,
                   m->mue_int, m->mue32, m->a_of_d_dev, m->buf.ys, m->buf.rsum, m->buf.rel, m->buf.red,
-                  m->buf.scal, m->buf.counters, m->buf.mu_fluid};
+                  m->buf.scal, m->buf.counters, m->buf.mu_fluid, m->adj};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   for (double* p : m->host_mirror) cudaFree(p);

@@ -740,7 +740,7 @@ int launch_gather(SodMesh* m, bool mixed, int stage, GatherArgs& a, cudaStream_t
   a.gamma = m->prm.gamma;
   a.Rgas = m->prm.Rgas;
   a.normalise = m->prm.normalise;
-  a.ys = m->buf.ys;
+  if (!a.ys) a.ys = m->buf.ys;
   a.rsum = m->buf.rsum;
   a.red = m->buf.red;
   a.counter = m->buf.counters + 0;
@@ -816,8 +816,10 @@ static double* reta_scratch(SodMesh* m) {
 
 // One RK4 step on device state (mu_e already in m->mue_int / mue32).  When ev is non-null,
 // ev[2*slot] / ev[2*slot+1] bracket each kernel: slots 0-3 KR stages, 4-7 KG stages, 8 KV.
+// When stage_store is non-null the stage states Y2, Y3, Y4 (5 columns of npoin each) are
+// written there instead of the internal stage buffer (for the adjoint's reverse sweep).
 int run_step(SodMesh* m, SodState* s, const double* dt_dev, double* dt_next, bool mixed, cudaStream_t st,
-             cudaEvent_t* ev = nullptr) {
+             cudaEvent_t* ev = nullptr, double* stage_store = nullptr) {
   const size_t N = m->npoin;
   const int epb = m->tuned_epb[mixed ? 1 : 0] ? m->tuned_epb[mixed ? 1 : 0] : (mixed ? 4 : 2);
   SodState loc = *s;
@@ -829,11 +831,12 @@ int run_step(SodMesh* m, SodState* s, const double* dt_dev, double* dt_next, boo
   }
   int rc;
   for (int stage = 1; stage <= 4; ++stage) {
-    const double* src_rho = stage == 1 ? s->rho : m->buf.ys;
-    const double* src_q0 = stage == 1 ? s->q : m->buf.ys + N;
-    const double* src_q1 = stage == 1 ? s->q + N : m->buf.ys + 2 * N;
-    const double* src_q2 = stage == 1 ? s->q + 2 * N : m->buf.ys + 3 * N;
-    const double* src_E = stage == 1 ? s->E : m->buf.ys + 4 * N;
+    double* yin = (stage_store && stage >= 2) ? stage_store + (size_t)(stage - 2) * 5 * N : m->buf.ys;
+    const double* src_rho = stage == 1 ? s->rho : yin;
+    const double* src_q0 = stage == 1 ? s->q : yin + N;
+    const double* src_q1 = stage == 1 ? s->q + N : yin + 2 * N;
+    const double* src_q2 = stage == 1 ? s->q + 2 * N : yin + 3 * N;
+    const double* src_E = stage == 1 ? s->E : yin + 4 * N;
     if (ev) cudaEventRecord(ev[2 * (stage - 1)], st);
     rc = launch_rhs(m, mixed, epb, src_rho, src_q0, src_q1, src_q2, src_E, s->mu_factor, nullptr, st);
     if (rc) return rc;
@@ -846,6 +849,7 @@ int run_step(SodMesh* m, SodState* s, const double* dt_dev, double* dt_next, boo
     g.machno = s->machno; g.mu_fluid = s->mu_fluid; g.Reta = loc.Reta; g.mu_factor = s->mu_factor;
     g.node_member = m->nmember > 0 ? m->node_member : nullptr;
     g.member_reduce = m->nmember > 0 ? 1 : 0;
+    if (stage_store && stage < 4) g.ys = stage_store + (size_t)(stage - 1) * 5 * N;
     if (ev) cudaEventRecord(ev[2 * (3 + stage)], st);
     rc = launch_gather(m, mixed, stage, g, st);
     if (rc) return rc;
@@ -892,6 +896,21 @@ int sod_rk4_main(SodMesh* m, SodState* s, const double* dt_dev, double* dt_next_
     if (rc) return rc;
   }
   rc = run_step(m, s, dt_dev, dt_next_dev, mixed, st);
+  if (rc) return rc;
+  return mesh_internal_to_ref_elem(m, m->mue_int, s->mu_e, st);
+}
+
+int sod_rk4_main_record(SodMesh* m, SodState* s, const double* dt_dev, double* dt_next_dev, double* stages,
+                        sod_stream_t stream) {
+  int rc = check_state(m, s);
+  if (rc) return rc;
+  SOD_ARG(dt_dev && stages, "dt_dev/stages null");
+  cudaStream_t st = (cudaStream_t)stream;
+  rc = ensure_step_buffers(m, false);
+  if (rc) return rc;
+  rc = mesh_ref_to_internal_elem(m, s->mu_e, m->mue_int, st);
+  if (rc) return rc;
+  rc = run_step(m, s, dt_dev, dt_next_dev, false, st, nullptr, stages);
   if (rc) return rc;
   return mesh_internal_to_ref_elem(m, m->mue_int, s->mu_e, st);
 }

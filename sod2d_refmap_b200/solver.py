@@ -28,8 +28,17 @@ def _ptr(t) -> int:
     return 0 if t is None else int(t.data_ptr())
 
 
+def _contig(t):
+    """t itself, after checking that it is a contiguous float64 CUDA tensor."""
+    torch = _torch()
+    if t.device.type != "cuda" or t.dtype != torch.float64 or not t.is_contiguous():
+        raise ValueError("expected a contiguous float64 CUDA tensor")
+    return t
+
+
 def _np_ptr(a) -> C.c_void_p:
-    return C.c_void_p(a.ctypes.data) if a is not None else C.c_void_p(0)
+    # data_as keeps a reference to the array for as long as the pointer object lives
+    return a.ctypes.data_as(C.c_void_p) if a is not None else C.c_void_p(0)
 
 
 def _stream(stream=None) -> C.c_void_p:
@@ -203,6 +212,43 @@ class Sod2dMesh:
         _lib.check(_lib.load().sod_rhs(self.handle, *(C.c_void_p(_ptr(t)) for t in (
             state.rho, state.q, state.E, state.mu_e, state.mu_factor, out["Rmass"], out["Rmom"], out["Rener"],
             out["Reta"])), int(precision), _stream(stream)))
+        return out
+
+    # ---- adjoint (reverse mode, FP64, mu_e and dt frozen) --------------------------------
+    def rhs_vjp(self, rho, q, E, mu_e, mu_factor, bar_Rmass, bar_Rmom, bar_Rener, stream=None):
+        """(dR/d(rho,q,E))^T (bar_Rmass, bar_Rmom, bar_Rener) for the FP64 stage RHS of rhs()."""
+        torch = _torch()
+        N = self.npoin
+        g_rho = torch.empty(N, dtype=torch.float64, device="cuda")
+        g_q = torch.empty(3, N, dtype=torch.float64, device="cuda")
+        g_E = torch.empty(N, dtype=torch.float64, device="cuda")
+        args = [_contig(t) for t in (rho, q, E, mu_e, mu_factor, bar_Rmass, bar_Rmom, bar_Rener)]
+        _lib.check(_lib.load().sod_rhs_vjp(self.handle, *(C.c_void_p(_ptr(t)) for t in args + [g_rho, g_q, g_E]),
+                                           _stream(stream)))
+        return g_rho, g_q, g_E
+
+    def rk_4_main_record(self, state: Sod2dState, stages, update_dt: bool = True, stream=None):
+        """FP64 rk_4_main that also stores the stage states Y2..Y4 in stages (15*npoin float64)."""
+        st = state.struct()
+        _lib.check(_lib.load().sod_rk4_main_record(self.handle, C.byref(st), C.c_void_p(_ptr(state.dt)),
+                                                  C.c_void_p(_ptr(state.dt) if update_dt else 0),
+                                                  C.c_void_p(_ptr(_contig(stages))), _stream(stream)))
+
+    def rk4_step_vjp(self, rho, q, E, mu_e, mu_factor, dt, bar_rho, bar_q, bar_E, out=None, stages=None,
+                     stream=None):
+        """Adjoint of one FP64 RK4 step from (rho, q, E) with mu_e and dt (device (1,)) frozen;
+        stages from rk_4_main_record of the same step (recomputed when None)."""
+        torch = _torch()
+        N = self.npoin
+        if out is None:
+            out = (torch.empty(N, dtype=torch.float64, device="cuda"),
+                   torch.empty(3, N, dtype=torch.float64, device="cuda"),
+                   torch.empty(N, dtype=torch.float64, device="cuda"))
+        args = [_contig(t) for t in (rho, q, E, mu_e, mu_factor, dt)]
+        args += [None if stages is None else _contig(stages)]
+        args += [_contig(t) for t in (bar_rho, bar_q, bar_E)]
+        _lib.check(_lib.load().sod_rk4_step_vjp(self.handle, *(C.c_void_p(_ptr(t)) for t in args + list(out)),
+                                                _stream(stream)))
         return out
 
     def adapt_dt(self, state: Sod2dState, stream=None):
