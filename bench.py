@@ -389,6 +389,36 @@ def bench_cg(n: int):
     return out
 
 
+def run_profile_case(n: int):
+    """A short, bounded launch sequence for ncu captures (no timing, no autotune): on an n^3
+    jittered periodic mesh, 3 FP64 and 3 mixed RK4 steps (fused RHS, stage gather, entropy
+    viscosity + dt kernels), one RK4-step VJP (adjoint kernels) and 5 Poisson SpMV+dot
+    launches; inputs exceed L2 from n = 24 up."""
+    import torch
+    from sod2d_refmap_b200 import solver as S
+    M, m, prm, st = _workload(n)
+    gm = S.Sod2dMesh(m, prm)
+    for prec in (S.FP64, S.MIXED):
+        s = S.Sod2dState.from_host(st, gm.nelem)
+        gm.adapt_dt(s)
+        for _ in range(3):
+            gm.rk_4_main(s, prec, update_dt=True)
+    s = S.Sod2dState.from_host(st, gm.nelem)
+    gm.adapt_dt(s)
+    gm.rk_4_main(s, S.FP64, update_dt=True)
+    bars = (s.rho.clone(), s.q.clone(), s.E.clone())
+    gm.rk4_step_vjp(s.rho, s.q, s.E, s.mu_e, s.mu_factor, s.dt, *bars)
+    P = S.Sod2dPoisson(gm)
+    x = s.rho.clone()
+    for _ in range(5):
+        P.apply(x)
+    torch.cuda.synchronize()
+    P.close()
+    gm.close()
+    print(json.dumps({"profile_case": f"{n}^3", "elements": m.nelem, "nodes": m.npoin}))
+    return 0
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -502,14 +532,19 @@ def run_ours(args):
                             "achieved_GBs": kr64_bytes / (prof["fp64"][0] / 1e3) / 1e9},
             "kernel_ms": {"mixed": {"rhs": prof["mixed"][0], "gather_rk": prof["mixed"][1], "visc_dt": prof["mixed"][2]},
                           "fp64": {"rhs": prof["fp64"][0], "gather_rk": prof["fp64"][1], "visc_dt": prof["fp64"][2]}}}
-    tr = os.path.join(ROOT, "profiles", "traffic.json")
+    tr = os.path.join(ROOT, "profiles", "traffic.txt")
     if os.path.exists(tr):
+        kv = {}
         with open(tr) as f:
-            tj = json.load(f)
-        per_elem = tj.get("k_rhs_fused_mixed_bytes_per_element")
+            for ln in f:
+                if "=" in ln and not ln.lstrip().startswith("#"):
+                    k_, v_ = ln.split("=", 1)
+                    kv[k_.strip()] = v_.strip()
+        per_elem = kv.get("k_rhs_mixed2_bytes_per_element")
         if per_elem:
-            roof["traffic"] = per_elem * gm.nelem
-            roof["traffic_source"] = tj.get("source")
+            roof["traffic"] = float(per_elem) * gm.nelem
+            roof["traffic_note"] = ("ncu DRAM bytes per element on the 32^3 profile case, scaled by the "
+                                    "element count: " + kv.get("source", ""))
     cg = None if args.no_cg else bench_cg(args.cg_n)
     batch = None if args.no_batch else bench_batch(args.batch_members, args.batch_steps)
     adjoint = None if args.no_adjoint else bench_adjoint(args.adj_n, args.adj_steps, args.adj_every)
@@ -557,11 +592,15 @@ def main():
     ap.add_argument("--batch-members", type=int, default=256)
     ap.add_argument("--batch-steps", type=int, default=20)
     ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--profile-case", type=int, default=0,
+                    help="run the short ncu launch sequence on an n^3 mesh instead of the benchmark")
     ap.add_argument("--adj-n", type=int, default=32)
     ap.add_argument("--adj-steps", type=int, default=50)
     ap.add_argument("--adj-every", type=int, default=10)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    if args.profile_case:
+        return run_profile_case(args.profile_case)
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)
