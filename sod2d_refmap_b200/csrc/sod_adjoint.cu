@@ -14,6 +14,11 @@
 //   convection the split-form combination reversed pointwise
 //   both       derivative adjoints mapped back with He^T and D^T along lines to nodal product
 //              fields, then the product rule, the EOS and u = q/rho in reverse.
+// The energy convection is linear in (h, k) through h + k only (every h term has a k twin with
+// the same structure), so the adjoint works with the total enthalpy H = h + k; q (x) u is
+// symmetric (rho u_c u_j), so its 9 components reduce to 6 like u (x) u.  The 29 nodal adjoint
+// fields go through shared memory in chunks of kChunk fields (3 line arrays each), which keeps
+// the CTA at 21 KB of shared memory.
 // Element-node adjoints are assembled by the same ordered CSR gather as the forward path.
 #include "sod_internal.cuh"
 #include <cmath>
@@ -27,16 +32,18 @@ namespace adj {
 
 constexpr double kC1 = 0.000001458;
 constexpr double kS = 110.4;
-// forward fields staged in shared memory
-enum { F_RHO = 0, F_H, F_RH, F_K, F_RK, F_U0, F_U1, F_U2, F_Q0, F_Q1, F_Q2, F_T,
-       F_FUE0, F_FUE1, F_FUE2, F_FUK0, F_FUK1, F_FUK2, F_UU00, F_UU01, F_UU02, F_UU11, F_UU12, F_UU22, NF_FWD };
-// adjoint fields (nodal product fields receiving D^T sums)
-enum { A_RHO = 0, A_P, A_H, A_RH, A_K, A_RK, A_T, A_U0, A_U1, A_U2, A_Q0, A_Q1, A_Q2,
-       A_FE0, A_FE1, A_FE2, A_FUE0, A_FUE1, A_FUE2, A_FK0, A_FK1, A_FK2, A_FUK0, A_FUK1, A_FUK2,
-       A_F00, A_F01, A_F02, A_F10, A_F11, A_F12, A_F20, A_F21, A_F22,
+// forward fields staged in shared memory (H = h + k total enthalpy)
+enum { F_RHO = 0, F_H, F_RH, F_T, F_U0, F_U1, F_U2, F_Q0, F_Q1, F_Q2, F_HU0, F_HU1, F_HU2,
+       F_UU00, F_UU01, F_UU02, F_UU11, F_UU12, F_UU22, NF_FWD };
+// nodal adjoint fields receiving D^T line sums: 11 gradient fields, rho H u and H u (divergence),
+// q (x) u and u (x) u (symmetric, divergence by rows)
+enum { A_RHO = 0, A_P, A_H, A_RH, A_T, A_U0, A_U1, A_U2, A_Q0, A_Q1, A_Q2,
+       A_FE0, A_FE1, A_FE2, A_FUE0, A_FUE1, A_FUE2,
+       A_F00, A_F01, A_F02, A_F11, A_F12, A_F22,
        A_UU00, A_UU01, A_UU02, A_UU11, A_UU12, A_UU22, NF_ADJ };
-
-constexpr size_t kSmemBytes = sizeof(double) * FSTRIDE * (size_t)(3 * NF_ADJ + 6 + 6);
+constexpr int kChunk = 10;
+constexpr int kArrays = 3 * kChunk;  // >= NF_FWD + 6 (forward phase) and >= 6 (seed phase)
+static_assert(kArrays >= NF_FWD + 6, "shared arrays");
 
 struct VjpArgs {
   int nelem;
@@ -51,7 +58,7 @@ struct VjpArgs {
   const double* __restrict__ mu_factor;
   const double* __restrict__ w;          // seeds / Ml: 5 columns of npoin (mass, mom x3, energy)
   int64_t npoin;
-  double* out;                           // [e][5][64] element-node adjoints (rho, q x3, E)
+  double* out;                           // [e][NRES][64] element-node adjoints (rho, q x3, E, 0)
   DMat D;
   DevParams prm;
 };
@@ -73,12 +80,15 @@ __device__ __forceinline__ double divT_line(const double* fx, const double* fy, 
   return s;
 }
 
-__global__ void __launch_bounds__(64) k_rhs_vjp(const VjpArgs a) {
-  extern __shared__ __align__(16) double sm[];
-  double* G = sm;                                   // adjoint line arrays [NF_ADJ][3][FSTRIDE]
-  double* S6 = sm + (size_t)3 * NF_ADJ * FSTRIDE;    // diffusion output seeds [6][FSTRIDE]
-  double* V6 = S6 + 6 * FSTRIDE;                     // contravariant gradRho/gradT [6][FSTRIDE]
-  double* Fw = G;                                    // forward fields reuse the adjoint area
+// symmetric pair (c, j) of each q(x)u / u(x)u field, in enum order 00 01 02 11 12 22
+__device__ constexpr int sym_c(int t) { return t < 3 ? 0 : (t < 5 ? 1 : 2); }
+__device__ constexpr int sym_j(int t) { return t < 3 ? t : (t < 5 ? t - 2 : 2); }
+
+#ifndef SOD_VJP_MIN_BLOCKS
+#define SOD_VJP_MIN_BLOCKS 1  // CTAs per SM the register allocation must allow
+#endif
+__global__ void __launch_bounds__(64, SOD_VJP_MIN_BLOCKS) k_rhs_vjp(const VjpArgs a) {
+  __shared__ __align__(16) double sm[kArrays * FSTRIDE];
   __shared__ DMat Ds;
   const int e = blockIdx.x, d = threadIdx.x;
   const int i = d & 3, j = (d >> 2) & 3, k = d >> 4, s = sidx(i, j, k);
@@ -99,76 +109,66 @@ __global__ void __launch_bounds__(64) k_rhs_vjp(const VjpArgs a) {
   const double p = rho * (g - 1.0) * ((Et / rho) - 0.5 * umag);
   const double h = (g / (g - 1.0)) * p / rho;
   const double T = p / (rho * Rg);
+  const double Ht = h + kk;
   const double mf = a.mu_factor[n];
   const double muf = mf * kC1 * (T * sqrt(T)) / (T + kS);
   const double dmuf_dT = mf * kC1 * (1.5 * sqrt(T) * (T + kS) - T * sqrt(T)) / ((T + kS) * (T + kS));
   const double mue = a.mue[(size_t)e * NN + d];
 
   // ---------------- forward recompute of the derivative quantities ----------------
+  double* Fw = sm;
   Fw[F_RHO * FSTRIDE + s] = rho;
-  Fw[F_H * FSTRIDE + s] = h;
-  Fw[F_RH * FSTRIDE + s] = rho * h;
-  Fw[F_K * FSTRIDE + s] = kk;
-  Fw[F_RK * FSTRIDE + s] = rho * kk;
+  Fw[F_H * FSTRIDE + s] = Ht;
+  Fw[F_RH * FSTRIDE + s] = rho * Ht;
   Fw[F_T * FSTRIDE + s] = T;
+#pragma unroll
   for (int c = 0; c < 3; ++c) {
     Fw[(F_U0 + c) * FSTRIDE + s] = uv[c];
     Fw[(F_Q0 + c) * FSTRIDE + s] = qv[c];
-    Fw[(F_FUE0 + c) * FSTRIDE + s] = h * uv[c];
-    Fw[(F_FUK0 + c) * FSTRIDE + s] = kk * uv[c];
+    Fw[(F_HU0 + c) * FSTRIDE + s] = Ht * uv[c];
   }
-  Fw[F_UU00 * FSTRIDE + s] = uv[0] * uv[0];
-  Fw[F_UU01 * FSTRIDE + s] = uv[0] * uv[1];
-  Fw[F_UU02 * FSTRIDE + s] = uv[0] * uv[2];
-  Fw[F_UU11 * FSTRIDE + s] = uv[1] * uv[1];
-  Fw[F_UU12 * FSTRIDE + s] = uv[1] * uv[2];
-  Fw[F_UU22 * FSTRIDE + s] = uv[2] * uv[2];
+#pragma unroll
+  for (int t = 0; t < 6; ++t) Fw[(F_UU00 + t) * FSTRIDE + s] = uv[sym_c(t)] * uv[sym_j(t)];
   __syncthreads();
   auto grad = [&](int f, double* o) {
     double gx, gy, gz;
     giso_line(Fw + f * FSTRIDE, i, j, k, Ds.d, gx, gy, gz);
+#pragma unroll
     for (int r = 0; r < 3; ++r) o[r] = H[3 * r] * gx + H[3 * r + 1] * gy + H[3 * r + 2] * gz;
   };
-  auto divg = [&](int f0) {
-    double sd = 0.0;
-    for (int c = 0; c < 3; ++c) {
-      double o[3];
-      grad(f0 + c, o);
-      sd += o[c];
-    }
-    return sd;
+  auto grad_c = [&](int f, int c) {
+    double gx, gy, gz;
+    giso_line(Fw + f * FSTRIDE, i, j, k, Ds.d, gx, gy, gz);
+    return H[3 * c] * gx + H[3 * c + 1] * gy + H[3 * c + 2] * gz;
   };
-  double gRho[3], gH[3], gRH[3], gK[3], gRK[3], gU[3][3], gQ[3][3], gT[3];
-  grad(F_RHO, gRho); grad(F_H, gH); grad(F_RH, gRH); grad(F_K, gK); grad(F_RK, gRK); grad(F_T, gT);
+  double gRho[3], gH[3], gRH[3], gT[3], gU[3][3], gQ[3][3];
+  grad(F_RHO, gRho); grad(F_H, gH); grad(F_RH, gRH); grad(F_T, gT);
+#pragma unroll
   for (int c = 0; c < 3; ++c) { grad(F_U0 + c, gU[c]); grad(F_Q0 + c, gQ[c]); }
-  const double divFue = divg(F_FUE0), divFuk = divg(F_FUK0);
+  const double divHu = grad_c(F_HU0, 0) + grad_c(F_HU1, 1) + grad_c(F_HU2, 2);
   double divFuu[3];
-  {
-    // rows of the symmetric u x u: row0 = (00,01,02), row1 = (01,11,12), row2 = (02,12,22)
-    const int rows[3][3] = {{F_UU00, F_UU01, F_UU02}, {F_UU01, F_UU11, F_UU12}, {F_UU02, F_UU12, F_UU22}};
-    for (int r = 0; r < 3; ++r) {
-      double sd = 0.0;
-      for (int c = 0; c < 3; ++c) {
-        double o[3];
-        grad(rows[r][c], o);
-        sd += o[c];
-      }
-      divFuu[r] = sd;
-    }
-  }
+  // rows of the symmetric u (x) u: row0 = (00,01,02), row1 = (01,11,12), row2 = (02,12,22)
+  divFuu[0] = grad_c(F_UU00, 0) + grad_c(F_UU01, 1) + grad_c(F_UU02, 2);
+  divFuu[1] = grad_c(F_UU01, 0) + grad_c(F_UU11, 1) + grad_c(F_UU12, 2);
+  divFuu[2] = grad_c(F_UU02, 0) + grad_c(F_UU12, 1) + grad_c(F_UU22, 2);
   const double divU = gU[0][0] + gU[1][1] + gU[2][2];
   const double divQ = gQ[0][0] + gQ[1][1] + gQ[2][2];
   // diffusion pass 1 (stresses) and the contravariant gradRho / gradT fluxes for pass 2
   const double mut = muf + mue;
   double tau[3][3];
+#pragma unroll
   for (int r = 0; r < 3; ++r)
+#pragma unroll
     for (int c = 0; c < 3; ++c) tau[r][c] = mut * (gU[r][c] + gU[c][r]);
+#pragma unroll
   for (int r = 0; r < 3; ++r) tau[r][r] -= muf * (2.0 / 3.0) * divU;
+  double* V6 = sm + NF_FWD * FSTRIDE;  // does not overlap the forward fields
+#pragma unroll
   for (int dir = 0; dir < 3; ++dir) {
     V6[dir * FSTRIDE + s] = gpv * (H[dir] * gRho[0] + H[3 + dir] * gRho[1] + H[6 + dir] * gRho[2]);
     V6[(3 + dir) * FSTRIDE + s] = gpv * (H[dir] * gT[0] + H[3 + dir] * gT[1] + H[6 + dir] * gT[2]);
   }
-  __syncthreads();  // forward fields no longer needed; V6 complete
+  __syncthreads();  // forward fields consumed; V6 complete
   const double divDr = divT_line(V6, V6 + FSTRIDE, V6 + 2 * FSTRIDE, i, j, k, Ds.d);
   const double divDgT = divT_line(V6 + 3 * FSTRIDE, V6 + 4 * FSTRIDE, V6 + 5 * FSTRIDE, i, j, k, Ds.d);
 
@@ -176,12 +176,11 @@ __global__ void __launch_bounds__(64) k_rhs_vjp(const VjpArgs a) {
   const int64_t N = a.npoin;
   const double wm = a.w[n], we = a.w[n + 4 * N];
   const double wmo[3] = {a.w[n + N], a.w[n + 2 * N], a.w[n + 3 * N]};
-  double rb = 0.0, hb = 0.0, kb = 0.0, pb = 0.0, Tb = 0.0, mufb = 0.0;
+  double rb = 0.0, Hb = 0.0, pb = 0.0, Tb = 0.0, mufb = 0.0;
   double ub[3] = {0, 0, 0}, qb[3] = {0, 0, 0};
-  double gRhob[3] = {0, 0, 0}, gPb[3] = {0, 0, 0}, gHb[3] = {0, 0, 0}, gRHb[3] = {0, 0, 0}, gKb[3] = {0, 0, 0},
-         gRKb[3] = {0, 0, 0}, gTb[3] = {0, 0, 0};
+  double gRhob[3] = {0, 0, 0}, gPb[3] = {0, 0, 0}, gHb[3] = {0, 0, 0}, gRHb[3] = {0, 0, 0}, gTb[3] = {0, 0, 0};
   double gUb[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}}, gQb[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
-  double dFeb = 0.0, dFueb = 0.0, dFkb = 0.0, dFukb = 0.0, divUb = 0.0, divQb = 0.0;
+  double dFeb = 0.0, dFueb = 0.0, divUb = 0.0, divQb = 0.0;
   double dFb[3] = {0, 0, 0}, dFuub[3] = {0, 0, 0};
 
   // diffusion outputs (elem_diffu.f90:143-193): nu_e*divD(gradRho), divD(tauU) + kappa*divD(gradT),
@@ -191,69 +190,80 @@ __global__ void __launch_bounds__(64) k_rhs_vjp(const VjpArgs a) {
   const double kappa = muf * CpPr + a.prm.c_ener * mue * CpPr;
   rb += wm * divDr * (-a.prm.c_rho * mue / (rho * rho));
   mufb += we * divDgT * CpPr;
+  double* S6 = sm;  // overlaps forward fields only (read before the last barrier), not V6
   S6[0 * FSTRIDE + s] = nu_e * wm;
   S6[1 * FSTRIDE + s] = we;
   S6[2 * FSTRIDE + s] = kappa * we;
+#pragma unroll
   for (int r = 0; r < 3; ++r) S6[(3 + r) * FSTRIDE + s] = wmo[r];
   __syncthreads();
   {
     double taub[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+#pragma unroll
     for (int v = 0; v < 6; ++v) {
       double gx, gy, gz;
       giso_line(S6 + v * FSTRIDE, i, j, k, Ds.d, gx, gy, gz);  // adjoint of D^T: D along lines
       double Vb[3];
+#pragma unroll
       for (int r = 0; r < 3; ++r) Vb[r] = gpv * (H[3 * r] * gx + H[3 * r + 1] * gy + H[3 * r + 2] * gz);
       if (v == 0) {
+#pragma unroll
         for (int r = 0; r < 3; ++r) gRhob[r] += Vb[r];
       } else if (v == 1) {  // tauU_r = sum_c tau_rc u_c
+#pragma unroll
         for (int r = 0; r < 3; ++r)
+#pragma unroll
           for (int c = 0; c < 3; ++c) {
             taub[r][c] += Vb[r] * uv[c];
             ub[c] += Vb[r] * tau[r][c];
           }
       } else if (v == 2) {
+#pragma unroll
         for (int r = 0; r < 3; ++r) gTb[r] += Vb[r];
       } else {
+#pragma unroll
         for (int c = 0; c < 3; ++c) taub[v - 3][c] += Vb[c];
       }
     }
     // tau_rc = (muf+mue)(du_r/dx_c + du_c/dx_r) - delta_rc muf 2/3 div u
+#pragma unroll
     for (int r = 0; r < 3; ++r)
+#pragma unroll
       for (int c = 0; c < 3; ++c) {
         gUb[r][c] += mut * taub[r][c];
         gUb[c][r] += mut * taub[r][c];
         mufb += taub[r][c] * (gU[r][c] + gU[c][r]);
       }
+#pragma unroll
     for (int r = 0; r < 3; ++r) {
       mufb += -taub[r][r] * (2.0 / 3.0) * divU;
       divUb += -muf * (2.0 / 3.0) * taub[r][r];
     }
   }
 
-  // convection (elem_convec.f90:412-434), seeds times gpvol
+  // convection (elem_convec.f90:412-434), seeds times gpvol; energy through H = h + k
   {
     const double mm = gpv * wm, me = gpv * we;
     const double mc[3] = {gpv * wmo[0], gpv * wmo[1], gpv * wmo[2]};
-    const double rh = rho * h, rk = rho * kk;
-    // mass
+    // mass: 1/2 (div q + rho div u + u . grad rho)
     divQb += 0.5 * mm; rb += 0.5 * divU * mm; divUb += 0.5 * rho * mm;
+#pragma unroll
     for (int c = 0; c < 3; ++c) { ub[c] += 0.5 * gRho[c] * mm; gRhob[c] += 0.5 * uv[c] * mm; }
-    // energy
-    dFeb += 0.25 * me; hb += 0.25 * divQ * me; divQb += 0.25 * h * me;
-    rb += 0.25 * h * divU * me; hb += 0.25 * rho * divU * me; divUb += 0.25 * rh * me;
-    rb += 0.25 * divFue * me; dFueb += 0.25 * rho * me;
-    dFkb += 0.25 * me; kb += 0.25 * divQ * me; divQb += 0.25 * kk * me;
-    rb += 0.25 * kk * divU * me; kb += 0.25 * rho * divU * me; divUb += 0.25 * rk * me;
-    rb += 0.25 * divFuk * me; dFukb += 0.25 * rho * me;
+    // energy: 1/4 (H div q + rho H div u + q.grad H + u.grad(rho H) + H u.grad rho
+    //              + div(rho H u) + rho div(H u))
+    dFeb += 0.25 * me;
+    Hb += 0.25 * divQ * me; divQb += 0.25 * Ht * me;
+    rb += 0.25 * Ht * divU * me; Hb += 0.25 * rho * divU * me; divUb += 0.25 * rho * Ht * me;
+    rb += 0.25 * divHu * me; dFueb += 0.25 * rho * me;
+#pragma unroll
     for (int c = 0; c < 3; ++c) {
       qb[c] += 0.25 * gH[c] * me; gHb[c] += 0.25 * qv[c] * me;
       ub[c] += 0.25 * gRH[c] * me; gRHb[c] += 0.25 * uv[c] * me;
-      hb += 0.25 * uv[c] * gRho[c] * me; ub[c] += 0.25 * h * gRho[c] * me; gRhob[c] += 0.25 * h * uv[c] * me;
-      qb[c] += 0.25 * gK[c] * me; gKb[c] += 0.25 * qv[c] * me;
-      ub[c] += 0.25 * gRK[c] * me; gRKb[c] += 0.25 * uv[c] * me;
-      kb += 0.25 * uv[c] * gRho[c] * me; ub[c] += 0.25 * kk * gRho[c] * me; gRhob[c] += 0.25 * kk * uv[c] * me;
+      Hb += 0.25 * uv[c] * gRho[c] * me; ub[c] += 0.25 * Ht * gRho[c] * me; gRhob[c] += 0.25 * Ht * uv[c] * me;
     }
-    // momentum
+    // momentum: 1/4 (div(q u) + u div q + q div u + rho div(u u) + u u.grad rho + q.grad u + u.grad q)
+    //           + grad p
+#pragma unroll
     for (int c = 0; c < 3; ++c) {
       const double mu_c = mc[c];
       dFb[c] += 0.25 * mu_c;
@@ -261,6 +271,7 @@ __global__ void __launch_bounds__(64) k_rhs_vjp(const VjpArgs a) {
       qb[c] += 0.25 * divU * mu_c; divUb += 0.25 * qv[c] * mu_c;
       rb += 0.25 * divFuu[c] * mu_c; dFuub[c] += 0.25 * rho * mu_c;
       gPb[c] += mu_c;
+#pragma unroll
       for (int jd = 0; jd < 3; ++jd) {
         ub[c] += 0.25 * uv[jd] * gRho[jd] * mu_c;
         ub[jd] += 0.25 * uv[c] * gRho[jd] * mu_c;
@@ -271,73 +282,86 @@ __global__ void __launch_bounds__(64) k_rhs_vjp(const VjpArgs a) {
         gQb[c][jd] += 0.25 * uv[jd] * mu_c;
       }
     }
+#pragma unroll
     for (int c = 0; c < 3; ++c) {
       gUb[c][c] += divUb;
       gQb[c][c] += divQb;
     }
   }
 
-  // derivative adjoints -> iso adjoints (He^T) in shared memory, 3 line arrays per field
-  {
-    auto putg = [&](int f, const double* gb) {
+  // derivative adjoints -> iso adjoints (He^T) -> D^T line sums, in chunks of kChunk fields
+  auto iso3 = [&](int f, double* o) {
+    if (f <= A_Q2) {  // gradient fields: sum_r He(r,dir) gb_r
+      const double* gb = f == A_RHO ? gRhob : f == A_P ? gPb : f == A_H ? gHb : f == A_RH ? gRHb
+                         : f == A_T ? gTb : f <= A_U2 ? gUb[f - A_U0] : gQb[f - A_Q0];
+#pragma unroll
+      for (int dir = 0; dir < 3; ++dir) o[dir] = H[dir] * gb[0] + H[3 + dir] * gb[1] + H[6 + dir] * gb[2];
+    } else if (f <= A_FUE2) {  // component c of a vector whose divergence has adjoint db
+      const int c = f <= A_FE2 ? f - A_FE0 : f - A_FUE0;
+      const double db = f <= A_FE2 ? dFeb : dFueb;
+#pragma unroll
+      for (int dir = 0; dir < 3; ++dir) o[dir] = H[3 * c + dir] * db;
+    } else {  // symmetric (c,jj) entry: row c takes d/dx_jj, row jj takes d/dx_c
+      const int t = f <= A_F22 ? f - A_F00 : f - A_UU00;
+      const double* db = f <= A_F22 ? dFb : dFuub;
+      const int c = sym_c(t), jj = sym_j(t);
+#pragma unroll
       for (int dir = 0; dir < 3; ++dir)
-        G[(f * 3 + dir) * FSTRIDE + s] = H[dir] * gb[0] + H[3 + dir] * gb[1] + H[6 + dir] * gb[2];
-    };
-    auto putd = [&](int f, int comp, double db) {  // field is component comp of a vector whose divergence has adjoint db
-      for (int dir = 0; dir < 3; ++dir) G[(f * 3 + dir) * FSTRIDE + s] = H[3 * comp + dir] * db;
-    };
-    putg(A_RHO, gRhob); putg(A_P, gPb); putg(A_H, gHb); putg(A_RH, gRHb); putg(A_K, gKb); putg(A_RK, gRKb);
-    putg(A_T, gTb);
-    for (int c = 0; c < 3; ++c) {
-      putg(A_U0 + c, gUb[c]);
-      putg(A_Q0 + c, gQb[c]);
-      putd(A_FE0 + c, c, dFeb);
-      putd(A_FUE0 + c, c, dFueb);
-      putd(A_FK0 + c, c, dFkb);
-      putd(A_FUK0 + c, c, dFukb);
-      for (int jd = 0; jd < 3; ++jd) putd(A_F00 + 3 * c + jd, jd, dFb[c]);
+        o[dir] = H[3 * jj + dir] * db[c] + (c != jj ? H[3 * c + dir] * db[jj] : 0.0);
     }
-    for (int dir = 0; dir < 3; ++dir) {
-      G[(A_UU00 * 3 + dir) * FSTRIDE + s] = H[dir] * dFuub[0];
-      G[(A_UU01 * 3 + dir) * FSTRIDE + s] = H[3 + dir] * dFuub[0] + H[dir] * dFuub[1];
-      G[(A_UU02 * 3 + dir) * FSTRIDE + s] = H[6 + dir] * dFuub[0] + H[dir] * dFuub[2];
-      G[(A_UU11 * 3 + dir) * FSTRIDE + s] = H[3 + dir] * dFuub[1];
-      G[(A_UU12 * 3 + dir) * FSTRIDE + s] = H[6 + dir] * dFuub[1] + H[3 + dir] * dFuub[2];
-      G[(A_UU22 * 3 + dir) * FSTRIDE + s] = H[6 + dir] * dFuub[2];
-    }
-  }
-  __syncthreads();
-  auto Wb = [&](int f) {
-    return divT_line(G + (f * 3 + 0) * FSTRIDE, G + (f * 3 + 1) * FSTRIDE, G + (f * 3 + 2) * FSTRIDE, i, j, k, Ds.d);
   };
-  // nodal product fields -> primitives (product rule)
-  rb += Wb(A_RHO);
-  pb += Wb(A_P);
-  hb += Wb(A_H);
-  { const double t = Wb(A_RH); rb += h * t; hb += rho * t; }
-  kb += Wb(A_K);
-  { const double t = Wb(A_RK); rb += kk * t; kb += rho * t; }
-  Tb += Wb(A_T);
-  for (int c = 0; c < 3; ++c) {
-    ub[c] += Wb(A_U0 + c);
-    qb[c] += Wb(A_Q0 + c);
-    { const double t = Wb(A_FE0 + c); rb += h * uv[c] * t; hb += rho * uv[c] * t; ub[c] += rho * h * t; }
-    { const double t = Wb(A_FUE0 + c); hb += uv[c] * t; ub[c] += h * t; }
-    { const double t = Wb(A_FK0 + c); rb += kk * uv[c] * t; kb += rho * uv[c] * t; ub[c] += rho * kk * t; }
-    { const double t = Wb(A_FUK0 + c); kb += uv[c] * t; ub[c] += kk * t; }
-    for (int jd = 0; jd < 3; ++jd) {
-      const double t = Wb(A_F00 + 3 * c + jd);  // F_cj = q_c u_j
-      qb[c] += uv[jd] * t;
-      ub[jd] += qv[c] * t;
+  // nodal product fields -> primitives (product rule at the output node)
+  auto apply = [&](int f, double t) {
+    if (f == A_RHO) {
+      rb += t;
+    } else if (f == A_P) {
+      pb += t;
+    } else if (f == A_H) {
+      Hb += t;
+    } else if (f == A_RH) {
+      rb += Ht * t; Hb += rho * t;
+    } else if (f == A_T) {
+      Tb += t;
+    } else if (f <= A_U2) {
+      ub[f - A_U0] += t;
+    } else if (f <= A_Q2) {
+      qb[f - A_Q0] += t;
+    } else if (f <= A_FE2) {  // rho H u_c
+      const int c = f - A_FE0;
+      rb += Ht * uv[c] * t; Hb += rho * uv[c] * t; ub[c] += rho * Ht * t;
+    } else if (f <= A_FUE2) {  // H u_c
+      const int c = f - A_FUE0;
+      Hb += uv[c] * t; ub[c] += Ht * t;
+    } else if (f <= A_F22) {  // q_c u_jj
+      const int c = sym_c(f - A_F00), jj = sym_j(f - A_F00);
+      qb[c] += uv[jj] * t; ub[jj] += qv[c] * t;
+    } else {  // u_c u_jj
+      const int c = sym_c(f - A_UU00), jj = sym_j(f - A_UU00);
+      ub[c] += uv[jj] * t; ub[jj] += uv[c] * t;
     }
+  };
+  __syncthreads();  // seed arrays consumed before the chunks overwrite them
+#pragma unroll
+  for (int c0 = 0; c0 < NF_ADJ; c0 += kChunk) {
+#pragma unroll
+    for (int f = c0; f < c0 + kChunk && f < NF_ADJ; ++f) {
+      double o[3];
+      iso3(f, o);
+#pragma unroll
+      for (int dir = 0; dir < 3; ++dir) sm[((f - c0) * 3 + dir) * FSTRIDE + s] = o[dir];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int f = c0; f < c0 + kChunk && f < NF_ADJ; ++f) {
+      const double* b = sm + (size_t)(f - c0) * 3 * FSTRIDE;
+      apply(f, divT_line(b, b + FSTRIDE, b + 2 * FSTRIDE, i, j, k, Ds.d));
+    }
+    if (c0 + kChunk < NF_ADJ) __syncthreads();
   }
-  { const double t = Wb(A_UU00); ub[0] += 2.0 * uv[0] * t; }
-  { const double t = Wb(A_UU11); ub[1] += 2.0 * uv[1] * t; }
-  { const double t = Wb(A_UU22); ub[2] += 2.0 * uv[2] * t; }
-  { const double t = Wb(A_UU01); ub[0] += uv[1] * t; ub[1] += uv[0] * t; }
-  { const double t = Wb(A_UU02); ub[0] += uv[2] * t; ub[2] += uv[0] * t; }
-  { const double t = Wb(A_UU12); ub[1] += uv[2] * t; ub[2] += uv[1] * t; }
-  // Sutherland, EOS and u = q/rho in reverse (time_integ.f90:266-285, mod_fluid_viscosity.f90:37)
+
+  // H = h + k; Sutherland, EOS and u = q/rho in reverse (time_integ.f90:266-285,
+  // mod_fluid_viscosity.f90:37)
+  double hb = Hb, kb = Hb;
   Tb += mufb * dmuf_dT;
   pb += hb * g / ((g - 1.0) * rho);
   rb += -hb * h / rho;
@@ -346,7 +370,9 @@ __global__ void __launch_bounds__(64) k_rhs_vjp(const VjpArgs a) {
   const double Eb = (g - 1.0) * pb;
   rb += -(g - 1.0) * kk * pb;
   kb += -(g - 1.0) * rho * pb;
+#pragma unroll
   for (int c = 0; c < 3; ++c) ub[c] += uv[c] * kb;
+#pragma unroll
   for (int c = 0; c < 3; ++c) {
     qb[c] += ub[c] / rho;
     rb += -uv[c] * ub[c] / rho;
@@ -443,14 +469,8 @@ __global__ void __launch_bounds__(256) k_stage_state(int64_t N, const int32_t* _
   for (int f = 0; f < 5; ++f) ys[f * N + n] = y.c[f][n] - da * (r[f] / ml);
 }
 
-static int g_vjp_attr_done = 0;
-
 static int launch_vjp(SodMesh* m, const double* rho, const double* q0, const double* q1, const double* q2,
                       const double* E, const double* mu_factor, const double* w, cudaStream_t st) {
-  if (!g_vjp_attr_done) {
-    SOD_CUDA(cudaFuncSetAttribute(k_rhs_vjp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBytes));
-    g_vjp_attr_done = 1;
-  }
   VjpArgs a;
   a.nelem = m->nelem;
   a.econn = m->econn;
@@ -463,7 +483,7 @@ static int launch_vjp(SodMesh* m, const double* rho, const double* q0, const dou
   a.out = reinterpret_cast<double*>(m->buf.rel);
   a.D = m->D;
   a.prm = m->prm;
-  k_rhs_vjp<<<m->nelem, NN, kSmemBytes, st>>>(a);
+  k_rhs_vjp<<<m->nelem, NN, 0, st>>>(a);
   SOD_CHECK_LAUNCH();
   return SOD_OK;
 }
