@@ -1,6 +1,6 @@
 """Benchmark: SOD2D explicit spectral-element RHS (HEX64, p=3) on B200.
 
-Workload (config "c1"): triply periodic [0,2pi]^3 box of 64^3 HEX64 elements
+Workload: triply periodic [0,2pi]^3 box of 64^3 HEX64 elements
 (7,077,888 unique nodes, 5 conserved fields), nodes jittered by a seeded Gaussian
 (sigma = 0.05 x GLL node spacing, periodic-consistent), Taylor-Green vortex + seeded
 +-1e-3 velocity perturbation, Re=1600, Ma=0.1, entropy viscosity on, dt from CFL 0.5.
@@ -52,7 +52,7 @@ def _workload(n: int):
 
 
 def _config(n: int, m, extra: dict | None = None) -> dict:
-    c = {"workload": f"c1: TGV periodic {n}^3 HEX64 (p=3), jittered 0.05 node spacing, RK4 steps",
+    c = {"workload": f"TGV periodic {n}^3 HEX64 (p=3), jittered 0.05 node spacing, RK4 steps",
          "elements": m.nelem, "nodes": m.npoin, "dofs": 5 * m.npoin, "porder": 3,
          "l2": "inputs larger than L2 (state+geometry > 2 GB vs 126 MB L2)", "parallelism": "replicas"}
     if extra:
@@ -217,7 +217,7 @@ def kr_bytes_per_launch(nelem: int, npoin: int, mixed: bool) -> float:
 
 
 def bench_batch(nmember: int, steps: int):
-    """Config c3: ensemble of periodic HEX64 boxes, n per side log-uniform in [4, 24]
+    """Ensemble of periodic HEX64 boxes, n per side log-uniform in [4, 24]
     (seed 4), Re uniform in [400, 3200] (seed 5), own TGV state and dt; `steps` RK4 steps of
     every member, one launch per stage for the whole ensemble, each step a captured graph.
     Compared with the same members advanced one after another (one graph per member)."""
@@ -273,7 +273,7 @@ def bench_batch(nmember: int, steps: int):
 
 
 def bench_adjoint(n: int, steps: int, every: int):
-    """Config c2: loss 1/2 ||rho u||^2 after `steps` FP64 RK4 steps on an n^3 jittered periodic
+    """Adjoint: loss 1/2 ||rho u||^2 after `steps` FP64 RK4 steps on an n^3 jittered periodic
     HEX64 mesh (seed 3), gradient w.r.t. the initial (rho, q, E) by the checkpointed adjoint
     (checkpoint every `every` steps; mu_e and dt frozen at their forward values).  Times the
     forward (with checkpointing) and the backward by CUDA events, and checks the directional
@@ -351,7 +351,7 @@ def bench_adjoint(n: int, steps: int, every: int):
 
 
 def bench_cg(n: int):
-    """Config c4: pressure-Poisson Jacobi PCG on an n^3 jittered periodic HEX64 mesh (seed 6),
+    """Pressure-Poisson Jacobi PCG on an n^3 jittered periodic HEX64 mesh (seed 6),
     zero-mean Gaussian right-hand side (seed 7), stop at ||r|| < 1e-10 ||r0||; FP64 CG and FP32
     inner CG + FP64 refinement, time to solution by CUDA events (assembly excluded)."""
     import torch
@@ -419,6 +419,22 @@ def run_profile_case(n: int):
     return 0
 
 
+def max_over_ranks(x: float, world: int, device="cuda") -> float:
+    """The maximum of x over all ranks (the job's time is its slowest rank's)."""
+    if world == 1:
+        return float(x)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_throughput(units_per_rank: float, world: int, seconds_max: float) -> float:
+    """Whole-job throughput of independent replicas: all ranks' units over the slowest time."""
+    return units_per_rank * world / seconds_max
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -471,10 +487,7 @@ def run_ours(args):
         barrier(); torch.cuda.synchronize()
         ms = ev0.elapsed_time(ev1)
         launches = _lib.launch_count() - l0
-        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        if world > 1:
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        results[name] = dict(ms=float(t.item()), launches=launches)
+        results[name] = dict(ms=max_over_ranks(ms, world), launches=launches)
         states[name] = s
         if name == "mixed":
             clocks = cs.summary()
@@ -491,7 +504,7 @@ def run_ours(args):
         prof[name] = gm.step_profile(s, 5, precision=prec)
     # end to end through the host-buffer C-ABI call (pinned host arrays, copies in the timed region)
     e2e = None
-    if rank == 0 or True:
+    if True:
         host = {}
         for f in S.Sod2dState.FIELDS:
             t_ = getattr(base, f)
@@ -501,24 +514,23 @@ def run_ours(args):
         host["Reta"] = None
         n_e2e = max(3, min(K, 10))
         gm.rk4_main_host(host, dt0, precision=S.MIXED)
-        torch.cuda.synchronize(); barrier()
-        t0 = time.perf_counter()
+        torch.cuda.synchronize(); barrier(); torch.cuda.synchronize()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
         dt = dt0
         for _ in range(n_e2e):
-            dt = gm.rk4_main_host(host, dt, precision=S.MIXED)
-        sec = time.perf_counter() - t0
-        tt = torch.tensor([sec], device="cuda", dtype=torch.float64)
-        if world > 1:
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        sec = float(tt.item())
+            dt = gm.rk4_main_host(host, dt, precision=S.MIXED, stream=stream)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        sec = max_over_ranks(ev0.elapsed_time(ev1) / 1e3, world)
         E_ = gm.nelem
         h2d = 8 * (N + 3 * N + N + N) + 8 * 64 * E_ + 8
         d2h = 8 * (N + 3 * N + N + 3 * N + 7 * N) + 8 * 64 * E_ + 8
-        e2e = {"value": 5 * N * 4 * n_e2e * world / sec / 1e9, "unit": UNIT, "h2d_bytes_per_step": h2d,
+        e2e = {"value": job_throughput(5 * N * 4 * n_e2e, world, sec) / 1e9, "unit": UNIT, "h2d_bytes_per_step": h2d,
                "d2h_bytes_per_step": d2h, "steps": n_e2e, "precision": "mixed",
                "api": "sod_rk4_main_host (host arrays in the reference layouts)"}
-    value = 5 * N * 4 * K * world / (results["mixed"]["ms"] / 1e3) / 1e9
-    value64 = 5 * N * 4 * K * world / (results["fp64"]["ms"] / 1e3) / 1e9
+    value = job_throughput(5 * N * 4 * K, world, results["mixed"]["ms"] / 1e3) / 1e9
+    value64 = job_throughput(5 * N * 4 * K, world, results["fp64"]["ms"] / 1e3) / 1e9
     hbm, peak_kind = _peaks()
     kr_ms = prof["mixed"][0]
     kr_bytes = kr_bytes_per_launch(gm.nelem, N, True)
@@ -563,8 +575,8 @@ def run_ours(args):
                          "speedup_mixed_over_fp64": value / value64},
                 "mixed_rel_l2_vs_fp64": {"state_after_steps": acc, "rhs_stage": acc_rhs},
                 "gpu_launches": results["mixed"]["launches"],
-                "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks, "c4_pressure_cg": cg,
-                "c3_ensemble": batch, "c2_adjoint": adjoint}
+                "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks, "pressure_cg": cg,
+                "ensemble": batch, "adjoint": adjoint}
         print(json.dumps(line), flush=True)
     for s in states.values():
         del s

@@ -70,7 +70,7 @@ def test_shape_tables_match_product(oracle):
 
 
 @pytest.fixture(scope="module")
-def c0(oracle):
+def box4(oracle):
     m = M.periodic_box(4, jitter=0.05, seed=3)
     om = oracle.OracleMesh(m)
     prm = M.TGVParams()
