@@ -4,11 +4,15 @@
 // of full_convec_ijk elem_convec.f90:211-460, full_diffusion_ijk elem_diffu.f90:12-198 and
 // generic_scalar_convec_ijk elem_convec.f90:462-570, FP32 on deviation fields), with the
 // nodal fields staged in shared memory as float2 pairs: one 8-byte shared load and one packed
-// __ffma2_rn serve two fields, and the xi-lines are read as two 16-byte loads.  Pairing:
-//   batch A  (rho',p') (u0',u1') (u2',q0') (q1',q2') (h',rho h') (k',rho k') (eta',T')
-//   batch BC (fe,fue)x3 (fk,fuk)x3 (feta,F0.)x3 (F1.,F2.)x3 (Fuu0.,Fuu1.)x3 (Fuu22,0)
+// __ffma2_rn serve two fields, and the xi-lines are read as two 16-byte loads.  The energy
+// convection is linear in (h, k) and every h term has a k twin of the same form (the two
+// skew-symmetric quartets of elem_convec.f90:415-425), so both quartets are evaluated at once
+// on the total enthalpy H = h + k: same mathematics, 4 field pairs fewer.  Pairing:
+//   batch A  (rho',p') (u0',u1') (u2',q0') (q1',q2') (H',rho H') (eta',T')
+//   batch BC (fe,fue)x3 (feta,F0.)x3 (F1.,F2.)x3 (Fuu0.,Fuu1.)x3 (Fuu22,0)
 //   pass 2   (gradRho^,tauU^)x3 (gradT^,tauX^)x3 (tauY^,tauZ^)x3   (one slot per direction)
-// where F = (q-q_r) x (u-u_r), Fuu = (u-u_r) x (u-u_r) and ^ marks contravariant fluxes.
+// where fe = rho H' u, fue = H' u, F = (q-q_r) x (u-u_r), Fuu = (u-u_r) x (u-u_r) and ^ marks
+// contravariant fluxes.
 #include "sod_internal.cuh"
 #include <cmath>
 
@@ -17,9 +21,9 @@ namespace mx2 {
 
 constexpr double kC1 = 0.000001458;
 constexpr double kS = 110.4;
-constexpr int NBC = 16;  // batch B+C slots
+constexpr int NBC = 13;  // batch B+C slots
 constexpr int NP2 = 9;   // pass-2 slots
-constexpr int NSLOT = NBC + NP2;  // batch A (7 pairs) reuses the first slots of the BC area
+constexpr int NSLOT = NBC + NP2;  // batch A (6 pairs) reuses the first slots of the BC area
 constexpr int NREF = 16;
 
 __host__ __device__ constexpr size_t smem_bytes(int epb) {
@@ -81,8 +85,12 @@ __device__ __forceinline__ float2 divT2(const float2* fx, const float2* fy, cons
   return ADD2(ADD2(s, t), u);
 }
 
+#ifndef SOD_MX2_MIN_CTAS
+#define SOD_MX2_MIN_CTAS 8  // resident 64-thread element groups per SM the register budget must allow
+#endif
 template <int EPB>
-__global__ void __launch_bounds__(64 * EPB, (EPB >= 8 ? 1 : 8 / EPB)) k_rhs_mixed2(const RhsArgs a) {
+__global__ void __launch_bounds__(64 * EPB, (EPB >= SOD_MX2_MIN_CTAS ? 1 : SOD_MX2_MIN_CTAS / EPB))
+    k_rhs_mixed2(const RhsArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   double* refs_all = reinterpret_cast<double*>(smem_raw);
   float2* buf_all = reinterpret_cast<float2*>(smem_raw + sizeof(double) * EPB * NREF);
@@ -147,7 +155,8 @@ __global__ void __launch_bounds__(64 * EPB, (EPB >= 8 ? 1 : 8 / EPB)) k_rhs_mixe
                r_L = refs[12];
   const double r_u[3] = {refs[1], refs[2], refs[3]};
   const double r_q[3] = {refs[4], refs[5], refs[6]};
-  const double s_h = h - r_h, s_k = kk - r_k;
+  const double s_H = (h - r_h) + (kk - r_k);  // deviation of the total enthalpy H = h + k
+  const double r_H = r_h + r_k;
   // eta - eta_r = ((rho-rho_r) L_r + rho (L - L_r)) / (gamma-1), L - L_r by log1p of small ratios
   const float drho = (float)(rho - r_rho);
   const float dL = log1pf((float)((p - r_p) / r_p)) - (float)g * log1pf(drho / (float)r_rho);
@@ -157,18 +166,16 @@ __global__ void __launch_bounds__(64 * EPB, (EPB >= 8 ? 1 : 8 / EPB)) k_rhs_mixe
   const float su[3] = {(float)(uv[0] - r_u[0]), (float)(uv[1] - r_u[1]), (float)(uv[2] - r_u[2])};
   const float sq[3] = {(float)(qv[0] - r_q[0]), (float)(qv[1] - r_q[1]), (float)(qv[2] - r_q[2])};
 
-  // ---- batch A (7 pairs)
+  // ---- batch A (6 pairs)
   buf[0 * FSTRIDE + s_me] = make_float2((float)(rho - r_rho), (float)(p - r_p));
   buf[1 * FSTRIDE + s_me] = make_float2(su[0], su[1]);
   buf[2 * FSTRIDE + s_me] = make_float2(su[2], sq[0]);
   buf[3 * FSTRIDE + s_me] = make_float2(sq[1], sq[2]);
-  buf[4 * FSTRIDE + s_me] = make_float2((float)s_h, (float)(rho * s_h));
-  buf[5 * FSTRIDE + s_me] = make_float2((float)s_k, (float)(rho * s_k));
-  buf[6 * FSTRIDE + s_me] = make_float2((float)s_eta, (float)(T - r_T));
+  buf[4 * FSTRIDE + s_me] = make_float2((float)s_H, (float)(rho * s_H));
+  buf[5 * FSTRIDE + s_me] = make_float2((float)s_eta, (float)(T - r_T));
   __syncthreads();
 
-  float gradRho[3], gradP[3], gradU[3][3], gradQ[3][3], gradH[3], gradRH[3], gradK[3], gradRK[3], gradEta[3],
-      gradT[3];
+  float gradRho[3], gradP[3], gradU[3][3], gradQ[3][3], gradH[3], gradRH[3], gradEta[3], gradT[3];
   {
     float2 gx, gy, gz, o;
 #define SOD_PAIR_GRAD(slot, A, B)                                              \
@@ -183,39 +190,34 @@ __global__ void __launch_bounds__(64 * EPB, (EPB >= 8 ? 1 : 8 / EPB)) k_rhs_mixe
     SOD_PAIR_GRAD(2, gradU[2], gradQ[0])
     SOD_PAIR_GRAD(3, gradQ[1], gradQ[2])
     SOD_PAIR_GRAD(4, gradH, gradRH)
-    SOD_PAIR_GRAD(5, gradK, gradRK)
-    SOD_PAIR_GRAD(6, gradEta, gradT)
+    SOD_PAIR_GRAD(5, gradEta, gradT)
 #undef SOD_PAIR_GRAD
   }
 #pragma unroll
-  for (int c = 0; c < 3; ++c) {
-    gradRH[c] += (float)r_h * gradRho[c];
-    gradRK[c] += (float)r_k * gradRho[c];
-  }
+  for (int c = 0; c < 3; ++c) gradRH[c] += (float)r_H * gradRho[c];
   const float divU = gradU[0][0] + gradU[1][1] + gradU[2][2];
   const float divQ = gradQ[0][0] + gradQ[1][1] + gradQ[2][2];
-  const float rhoR = (float)rho, hR = (float)h, kR = (float)kk;
+  const float rhoR = (float)rho, HR = (float)(h + kk);
   const float etaR = (float)(r_eta + s_eta);
   const float uR[3] = {(float)uv[0], (float)uv[1], (float)uv[2]};
   const float qR[3] = {(float)qv[0], (float)qv[1], (float)qv[2]};
-  const float rhR = (float)(rho * h), rkR = (float)(rho * kk);
+  const float rHR = (float)(rho * (h + kk));
 
   // ---- convective terms available after batch A (elem_convec.f90:412-432) + reference parts
   float Rm = 0.5f * (divQ + rhoR * divU);
-  float Ren = 0.25f * (hR * divQ + rhR * divU) + 0.25f * (kR * divQ + rkR * divU);
+  float Ren = 0.25f * (HR * divQ + rHR * divU);
   float Rmo[3];
   float Ret = 0.5f * (etaR * divU);
   {
-    const float rh = (float)r_h, rk = (float)r_k, re = (float)r_eta;
-    Ren += 0.25f * (rh * divQ + rhoR * (rh * divU)) + 0.25f * (rk * divQ + rhoR * (rk * divU));
+    const float rH = (float)r_H, re = (float)r_eta;
+    Ren += 0.25f * (rH * divQ + rhoR * (rH * divU));
     Ret += 0.5f * (re * divU);
   }
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
     Rmo[c] = 0.25f * (uR[c] * divQ + qR[c] * divU) + gradP[c];
     Rm += 0.5f * (uR[c] * gradRho[c]);
-    Ren += 0.25f * (qR[c] * gradH[c] + uR[c] * gradRH[c] + (hR * uR[c]) * gradRho[c]) +
-           0.25f * (qR[c] * gradK[c] + uR[c] * gradRK[c] + (kR * uR[c]) * gradRho[c]);
+    Ren += 0.25f * (qR[c] * gradH[c] + uR[c] * gradRH[c] + (HR * uR[c]) * gradRho[c]);
     Ret += 0.5f * (uR[c] * gradEta[c]);
     float dF = (float)r_q[c] * divU, dFuu = (float)r_u[c] * divU;
 #pragma unroll
@@ -258,19 +260,18 @@ __global__ void __launch_bounds__(64 * EPB, (EPB >= 8 ? 1 : 8 / EPB)) k_rhs_mixe
   }
   __syncthreads();  // batch A reads done
 
-  // ---- batch B+C (16 pairs)
+  // ---- batch B+C (13 pairs)
   {
-    const float sh = (float)s_h, sk = (float)s_k, se = (float)s_eta;
-    const float rsh = (float)(rho * s_h), rsk = (float)(rho * s_k);
+    const float sH = (float)s_H, se = (float)s_eta;
+    const float rsH = (float)(rho * s_H);
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      buf[(0 + c) * FSTRIDE + s_me] = make_float2(rsh * uR[c], sh * uR[c]);
-      buf[(3 + c) * FSTRIDE + s_me] = make_float2(rsk * uR[c], sk * uR[c]);
-      buf[(6 + c) * FSTRIDE + s_me] = make_float2(se * uR[c], sq[0] * su[c]);
-      buf[(9 + c) * FSTRIDE + s_me] = make_float2(sq[1] * su[c], sq[2] * su[c]);
-      buf[(12 + c) * FSTRIDE + s_me] = make_float2(su[0] * su[c], su[1] * su[c]);
+      buf[(0 + c) * FSTRIDE + s_me] = make_float2(rsH * uR[c], sH * uR[c]);
+      buf[(3 + c) * FSTRIDE + s_me] = make_float2(se * uR[c], sq[0] * su[c]);
+      buf[(6 + c) * FSTRIDE + s_me] = make_float2(sq[1] * su[c], sq[2] * su[c]);
+      buf[(9 + c) * FSTRIDE + s_me] = make_float2(su[0] * su[c], su[1] * su[c]);
     }
-    buf[15 * FSTRIDE + s_me] = make_float2(su[2] * su[2], 0.0f);
+    buf[12 * FSTRIDE + s_me] = make_float2(su[2] * su[2], 0.0f);
   }
   __syncthreads();
   {
@@ -286,18 +287,17 @@ __global__ void __launch_bounds__(64 * EPB, (EPB >= 8 ? 1 : 8 / EPB)) k_rhs_mixe
       return acc;
     };
     const float2 dA = div2(0);   // (div fe, div fue)
-    const float2 dB = div2(3);   // (div fk, div fuk)
-    const float2 dC = div2(6);   // (div feta, div F0.)
-    const float2 dD = div2(9);   // (div F1., div F2.)
-    Ren += 0.25f * (dA.x + rhoR * dA.y) + 0.25f * (dB.x + rhoR * dB.y);
+    const float2 dC = div2(3);   // (div feta, div F0.)
+    const float2 dD = div2(6);   // (div F1., div F2.)
+    Ren += 0.25f * (dA.x + rhoR * dA.y);
     Ret += 0.5f * dC.x;
-    // Fuu rows 0,1 from slots 12..14 and row 2 from (Fuu02, Fuu12, Fuu22)
+    // Fuu rows 0,1 from slots 9..11 and row 2 from (Fuu02, Fuu12, Fuu22)
     float2 dE = make_float2(0.f, 0.f);
     float dFuu2 = 0.f;
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       float2 gx, gy, gz;
-      giso2(buf + (12 + c) * FSTRIDE, i, j, k, Dx, Dy, Dz, gx, gy, gz);
+      giso2(buf + (9 + c) * FSTRIDE, i, j, k, Dx, Dy, Dz, gx, gy, gz);
       dE = FMA2(H2[3 * c + 2], gz, FMA2(H2[3 * c + 1], gy, FMA2(H2[3 * c], gx, dE)));
       if (c == 2) {
         dFuu2 += H[0] * gx.x + H[1] * gy.x + H[2] * gz.x;   // d/dx_0 Fuu20 (= Fuu02)
@@ -306,7 +306,7 @@ __global__ void __launch_bounds__(64 * EPB, (EPB >= 8 ? 1 : 8 / EPB)) k_rhs_mixe
     }
     {
       float2 gx, gy, gz;
-      giso2(buf + 15 * FSTRIDE, i, j, k, Dx, Dy, Dz, gx, gy, gz);
+      giso2(buf + 12 * FSTRIDE, i, j, k, Dx, Dy, Dz, gx, gy, gz);
       dFuu2 += H[6] * gx.x + H[7] * gy.x + H[8] * gz.x;     // d/dx_2 Fuu22
     }
     Rmo[0] += 0.25f * (dC.y + rhoR * dE.x);
