@@ -24,7 +24,7 @@ constexpr double kS = 110.4;
 constexpr int NBC = 13;  // batch B+C slots
 constexpr int NP2 = 9;   // pass-2 slots
 constexpr int NSLOT = NBC + NP2;  // batch A (6 pairs) reuses the first slots of the BC area
-constexpr int NREF = 16;
+constexpr int NREF = 16 + 36 + 18;  // node-0 refs, 3 corner values of the 12 batch-A fields, FP32 slopes
 
 __host__ __device__ constexpr size_t smem_bytes(int epb) {
   return sizeof(double) * (size_t)epb * NREF + sizeof(float2) * (size_t)epb * NSLOT * FSTRIDE;
@@ -166,13 +166,49 @@ __global__ void __launch_bounds__(64 * EPB, (EPB >= SOD_MX2_MIN_CTAS ? 1 : SOD_M
   const float su[3] = {(float)(uv[0] - r_u[0]), (float)(uv[1] - r_u[1]), (float)(uv[2] - r_u[2])};
   const float sq[3] = {(float)(qv[0] - r_q[0]), (float)(qv[1] - r_q[1]), (float)(qv[2] - r_q[2])};
 
-  // ---- batch A (6 pairs)
-  buf[0 * FSTRIDE + s_me] = make_float2((float)(rho - r_rho), (float)(p - r_p));
-  buf[1 * FSTRIDE + s_me] = make_float2(su[0], su[1]);
-  buf[2 * FSTRIDE + s_me] = make_float2(su[2], sq[0]);
-  buf[3 * FSTRIDE + s_me] = make_float2(sq[1], sq[2]);
-  buf[4 * FSTRIDE + s_me] = make_float2((float)s_H, (float)(rho * s_H));
-  buf[5 * FSTRIDE + s_me] = make_float2((float)s_eta, (float)(T - r_T));
+  // ---- batch A (6 pairs).  The nodal fields differentiated directly (except rho and p, whose
+  // rounding does not reach the 1e-7 level of the residuals) get an element reference that is
+  // affine in xi: v' = v - sum_d a_d (xi_d + 1), a_d = v(corner_d)/2 (v is the FP64
+  // deviation from local node 0, so v = 0 there).  D differentiates linear functions exactly,
+  // so D v = D v' + a, and v' (second order in the element size) loses far less to the FP32
+  // cast than v.  Product fields (batch B+C) keep the constant node-0 reference, whose exact
+  // expansion the discrete product derivative needs.
+  const double dev[12] = {rho - r_rho, p - r_p, uv[0] - r_u[0], uv[1] - r_u[1], uv[2] - r_u[2],
+                          qv[0] - r_q[0], qv[1] - r_q[1], qv[2] - r_q[2], s_H, rho * s_H, s_eta, T - r_T};
+  double* crn = refs + 16;  // [dir][12]: values at local nodes (3,0,0), (0,3,0), (0,0,3)
+  float2* slopes = reinterpret_cast<float2*>(refs + 16 + 36);  // [dir][6 pairs]: a_dir in FP32
+  {
+    const int cdir = d == 3 ? 0 : (d == 12 ? 1 : (d == 48 ? 2 : -1));
+    if (cdir >= 0) {
+#pragma unroll
+      for (int f = 0; f < 12; ++f) crn[cdir * 12 + f] = dev[f];
+#pragma unroll
+      for (int t = 0; t < 6; ++t)
+        slopes[cdir * 6 + t] = t == 0 ? make_float2(0.f, 0.f)
+                                      : make_float2((float)(0.5 * dev[2 * t]), (float)(0.5 * dev[2 * t + 1]));
+    }
+  }
+  __syncthreads();
+  {
+    constexpr double kX = 0.44721359549995793928;  // interior GLL nodes of p = 3: +-sqrt(1/5)
+    auto xh = [&](int t) {  // (xi_t + 1)/2 of the natural 1-D node order
+      return t == 0 ? 0.0 : (t == 1 ? 0.5 * (1.0 - kX) : (t == 2 ? 0.5 * (1.0 + kX) : 1.0));
+    };
+    const double wx = xh(i), wy = xh(j), wz = xh(k);
+    float vp[12];
+    vp[0] = (float)dev[0];  // rho' and p' keep the constant reference (their rounding is harmless)
+    vp[1] = (float)dev[1];
+#pragma unroll
+    for (int f = 2; f < 12; f += 2) {
+      const double2 cx = *reinterpret_cast<const double2*>(crn + f);
+      const double2 cy = *reinterpret_cast<const double2*>(crn + 12 + f);
+      const double2 cz = *reinterpret_cast<const double2*>(crn + 24 + f);
+      vp[f] = (float)(dev[f] - (cx.x * wx + cy.x * wy + cz.x * wz));
+      vp[f + 1] = (float)(dev[f + 1] - (cx.y * wx + cy.y * wy + cz.y * wz));
+    }
+#pragma unroll
+    for (int t = 0; t < 6; ++t) buf[t * FSTRIDE + s_me] = make_float2(vp[2 * t], vp[2 * t + 1]);
+  }
   __syncthreads();
 
   float gradRho[3], gradP[3], gradU[3][3], gradQ[3][3], gradH[3], gradRH[3], gradEta[3], gradT[3];
@@ -180,6 +216,11 @@ __global__ void __launch_bounds__(64 * EPB, (EPB >= SOD_MX2_MIN_CTAS ? 1 : SOD_M
     float2 gx, gy, gz, o;
 #define SOD_PAIR_GRAD(slot, A, B)                                              \
     giso2(buf + (slot) * FSTRIDE, i, j, k, Dx, Dy, Dz, gx, gy, gz);            \
+    if ((slot) > 0) {                                                          \
+      gx = ADD2(gx, slopes[0 * 6 + (slot)]);                                   \
+      gy = ADD2(gy, slopes[1 * 6 + (slot)]);                                   \
+      gz = ADD2(gz, slopes[2 * 6 + (slot)]);                                   \
+    }                                                                          \
     _Pragma("unroll") for (int r = 0; r < 3; ++r) {                            \
       o = physr(H2, r, gx, gy, gz);                                            \
       A[r] = o.x;                                                              \
