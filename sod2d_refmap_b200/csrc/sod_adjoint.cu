@@ -58,7 +58,7 @@ struct VjpArgs {
   const double* __restrict__ mu_factor;
   const double* __restrict__ w;          // seeds / Ml: 5 columns of npoin (mass, mom x3, energy)
   int64_t npoin;
-  double* out;                           // [e][NRES][64] element-node adjoints (rho, q x3, E, 0)
+  double* out;                           // [(e*64 + d)*NRES + f] element-node adjoints (rho, q x3, E, 0)
   DMat D;
   DevParams prm;
 };
@@ -377,13 +377,7 @@ __global__ void __launch_bounds__(64, SOD_VJP_MIN_BLOCKS) k_rhs_vjp(const VjpArg
     qb[c] += ub[c] / rho;
     rb += -uv[c] * ub[c] / rho;
   }
-  double* o = a.out + (size_t)e * NRES * NN + d;
-  o[0] = rb;
-  o[NN] = qb[0];
-  o[2 * NN] = qb[1];
-  o[3 * NN] = qb[2];
-  o[4 * NN] = Eb;
-  o[5 * NN] = 0.0;
+  store_res6<double>(a.out, (size_t)e * NN + d, rb, qb[0], qb[1], qb[2], Eb, 0.0);
 }
 
 }  // namespace adj
@@ -430,10 +424,10 @@ __global__ void __launch_bounds__(256) k_gather_vjp(int64_t N, const int32_t* __
   double r[5] = {0, 0, 0, 0, 0};
   const int beg = ptr[n], end = ptr[n + 1];
   for (int c = beg; c < end; ++c) {
-    const int pk = idx[c];
-    const double* src = el + (size_t)(pk >> 6) * NRES * NN + (pk & 63);
+    double v[6];
+    load_res6<double>(el, (size_t)idx[c], v);
 #pragma unroll
-    for (int f = 0; f < 5; ++f) r[f] += src[f * NN];
+    for (int f = 0; f < 5; ++f) r[f] += v[f];
   }
 #pragma unroll
   for (int f = 0; f < 5; ++f) {
@@ -457,10 +451,10 @@ __global__ void __launch_bounds__(256) k_stage_state(int64_t N, const int32_t* _
   double r[5] = {0, 0, 0, 0, 0};
   const int beg = ptr[n], end = ptr[n + 1];
   for (int c = beg; c < end; ++c) {
-    const int pk = idx[c];
-    const double* src = el + (size_t)(pk >> 6) * NRES * NN + (pk & 63);
+    double v[6];
+    load_res6<double>(el, (size_t)idx[c], v);
 #pragma unroll
-    for (int f = 0; f < 5; ++f) r[f] += src[f * NN];
+    for (int f = 0; f < 5; ++f) r[f] += v[f];
   }
   // same operation order as the forward stage gather, so the stage states match it bit for bit
   const double ml = Ml[n];

@@ -92,6 +92,27 @@ struct RhsArgs {
 };
 
 // Scratch owned by a mesh for the step pipeline (allocated lazily, sized by npoin/nelem).
+// Element residuals of the fused path are node-major: rel[(e*64 + d)*NRES + f], so that one
+// gathered contribution (6 fields) is 3 vector loads of contiguous memory.
+template <typename R> struct Vec2;
+template <> struct Vec2<float> { using T = float2; };
+template <> struct Vec2<double> { using T = double2; };
+template <typename R>
+__device__ __forceinline__ void store_res6(R* rel, size_t node, R a0, R a1, R a2, R a3, R a4, R a5) {
+  using V = typename Vec2<R>::T;
+  V* o = reinterpret_cast<V*>(rel + node * NRES);
+  o[0] = V{a0, a1};
+  o[1] = V{a2, a3};
+  o[2] = V{a4, a5};
+}
+template <typename R>
+__device__ __forceinline__ void load_res6(const R* rel, size_t node, R (&v)[6]) {
+  using V = typename Vec2<R>::T;
+  const V* s = reinterpret_cast<const V*>(rel + node * NRES);
+  const V x = s[0], y = s[1], z = s[2];
+  v[0] = x.x; v[1] = x.y; v[2] = y.x; v[3] = y.y; v[4] = z.x; v[5] = z.y;
+}
+
 struct StepBuffers {
   int64_t npoin = 0, nelem = 0;
   double* ys = nullptr;      // stage state 5*npoin

@@ -366,13 +366,8 @@ __global__ void __launch_bounds__(64 * EPB) k_rhs_fused(const RhsArgs a) {
   const R kappa_e = (R)(muf * a.prm.Cp / a.prm.Prt) + (R)a.prm.c_ener * mue * (R)(a.prm.Cp / a.prm.Prt) +
                     (R)(a.prm.Cp * rho * musgs / 0.9);
   if (active) {
-    R* out = reinterpret_cast<R*>(a.rel) + (size_t)e * NRES * NN + d;
-    out[0 * NN] = gpv * Rm + nu_e * dv[0];
-    out[1 * NN] = gpv * Rmo[0] + dv[3];
-    out[2 * NN] = gpv * Rmo[1] + dv[4];
-    out[3 * NN] = gpv * Rmo[2] + dv[5];
-    out[4 * NN] = gpv * Ren + (dv[1] + kappa_e * dv[2]);
-    out[5 * NN] = gpv * Ret;
+    store_res6<R>(reinterpret_cast<R*>(a.rel), (size_t)e * NN + d, gpv * Rm + nu_e * dv[0], gpv * Rmo[0] + dv[3],
+                  gpv * Rmo[1] + dv[4], gpv * Rmo[2] + dv[5], gpv * Ren + (dv[1] + kappa_e * dv[2]), gpv * Ret);
   }
 }
 
@@ -423,8 +418,11 @@ __device__ __forceinline__ void block_reduce3(double& s, double& mx, double& mn,
   }
 }
 
+#ifndef SOD_KG_MIN_BLOCKS
+#define SOD_KG_MIN_BLOCKS 7  // resident 256-thread blocks per SM the register budget must allow
+#endif
 template <typename R, int STAGE>
-__global__ void __launch_bounds__(256) k_gather_rk(const GatherArgs a) {
+__global__ void __launch_bounds__(256, SOD_KG_MIN_BLOCKS) k_gather_rk(const GatherArgs a) {
   const int n = blockIdx.x * blockDim.x + threadIdx.x;
   const bool act = n < a.npoin;
   double eta_n = 0.0;
@@ -437,22 +435,17 @@ __global__ void __launch_bounds__(256) k_gather_rk(const GatherArgs a) {
     for (; c + 4 <= end; c += 4) {
       R v[4][6];
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const int pk = a.idx[c + q];
-        const R* src = rel + (size_t)(pk >> 6) * NRES * NN + (pk & 63);
-#pragma unroll
-        for (int f = 0; f < 6; ++f) v[q][f] = src[f * NN];
-      }
+      for (int q = 0; q < 4; ++q) load_res6<R>(rel, (size_t)a.idx[c + q], v[q]);
 #pragma unroll
       for (int q = 0; q < 4; ++q)
 #pragma unroll
         for (int f = 0; f < 6; ++f) r[f] += (double)v[q][f];
     }
     for (; c < end; ++c) {
-      const int pk = a.idx[c];
-      const R* src = rel + (size_t)(pk >> 6) * NRES * NN + (pk & 63);
+      R v[6];
+      load_res6<R>(rel, (size_t)a.idx[c], v);
 #pragma unroll
-      for (int f = 0; f < 6; ++f) r[f] += (double)src[f * NN];
+      for (int f = 0; f < 6; ++f) r[f] += (double)v[f];
     }
     const double ml = a.Ml[n];
 #pragma unroll

@@ -370,13 +370,9 @@ __global__ void __launch_bounds__(64 * EPB, (EPB >= SOD_MX2_MIN_CTAS ? 1 : SOD_M
   const float CpPr = (float)(a.prm.Cp / a.prm.Prt);
   const float kappa_e = muf * CpPr + (float)a.prm.c_ener * mue * CpPr + (float)(a.prm.Cp * rho * musgs / 0.9);
   if (active) {
-    float* out = reinterpret_cast<float*>(a.rel) + (size_t)e * NRES * NN + d;
-    out[0 * NN] = gpv * Rm + nu_e * vA.x;
-    out[1 * NN] = gpv * Rmo[0] + vB.y;
-    out[2 * NN] = gpv * Rmo[1] + vC.x;
-    out[3 * NN] = gpv * Rmo[2] + vC.y;
-    out[4 * NN] = gpv * Ren + (vA.y + kappa_e * vB.x);
-    out[5 * NN] = gpv * Ret;
+    store_res6<float>(reinterpret_cast<float*>(a.rel), (size_t)e * NN + d, gpv * Rm + nu_e * vA.x,
+                      gpv * Rmo[0] + vB.y, gpv * Rmo[1] + vC.x, gpv * Rmo[2] + vC.y,
+                      gpv * Ren + (vA.y + kappa_e * vB.x), gpv * Ret);
   }
 }
 
