@@ -573,7 +573,10 @@ __device__ __forceinline__ int nb_filter(int x) {
 
 constexpr int KV_EPB = 4;
 
-__global__ void __launch_bounds__(64 * KV_EPB) k_visc_dt(const ViscArgs a) {
+#ifndef SOD_KV_MIN_BLOCKS
+#define SOD_KV_MIN_BLOCKS 8  // resident blocks per SM the register budget must allow
+#endif
+__global__ void __launch_bounds__(64 * KV_EPB, SOD_KV_MIN_BLOCKS) k_visc_dt(const ViscArgs a) {
   __shared__ double ml[KV_EPB][NN];
   __shared__ double wm[KV_EPB][2][5];
   __shared__ double elem_s[KV_EPB][2];  // ced, dt limit of the element
