@@ -35,26 +35,19 @@ __device__ __forceinline__ float2 FMA2(float2 a, float2 b, float2 c) { return __
 __device__ __forceinline__ float2 MUL2(float2 a, float2 b) { return __fmul2_rn(a, b); }
 __device__ __forceinline__ float2 ADD2(float2 a, float2 b) { return __fadd2_rn(a, b); }
 
-// iso derivatives of a field pair: xi-line as two 16-byte loads, eta/zeta lines as 8-byte loads
+// iso derivatives of a field pair: xi-line as two 16-byte loads, eta/zeta lines as 8-byte loads;
+// each 4-term line sum as two independent halves (shorter dependency chains)
 __device__ __forceinline__ void giso2(const float2* __restrict__ f, int i, int j, int k, const float2* Dx,
                                       const float2* Dy, const float2* Dz, float2& gx, float2& gy, float2& gz) {
   const float2* fx = f + 4 * j + PLANE * k;
   const float4 a01 = *reinterpret_cast<const float4*>(fx);
   const float4 a23 = *reinterpret_cast<const float4*>(fx + 2);
-  gx = MUL2(Dx[0], make_float2(a01.x, a01.y));
-  gx = FMA2(Dx[1], make_float2(a01.z, a01.w), gx);
-  gx = FMA2(Dx[2], make_float2(a23.x, a23.y), gx);
-  gx = FMA2(Dx[3], make_float2(a23.z, a23.w), gx);
+  gx = ADD2(FMA2(Dx[1], make_float2(a01.z, a01.w), MUL2(Dx[0], make_float2(a01.x, a01.y))),
+            FMA2(Dx[3], make_float2(a23.z, a23.w), MUL2(Dx[2], make_float2(a23.x, a23.y))));
   const float2* fy = f + i + PLANE * k;
-  gy = MUL2(Dy[0], fy[0]);
-  gy = FMA2(Dy[1], fy[4], gy);
-  gy = FMA2(Dy[2], fy[8], gy);
-  gy = FMA2(Dy[3], fy[12], gy);
+  gy = ADD2(FMA2(Dy[1], fy[4], MUL2(Dy[0], fy[0])), FMA2(Dy[3], fy[12], MUL2(Dy[2], fy[8])));
   const float2* fz = f + i + 4 * j;
-  gz = MUL2(Dz[0], fz[0]);
-  gz = FMA2(Dz[1], fz[PLANE], gz);
-  gz = FMA2(Dz[2], fz[2 * PLANE], gz);
-  gz = FMA2(Dz[3], fz[3 * PLANE], gz);
+  gz = ADD2(FMA2(Dz[1], fz[PLANE], MUL2(Dz[0], fz[0])), FMA2(Dz[3], fz[3 * PLANE], MUL2(Dz[2], fz[2 * PLANE])));
 }
 
 // physical gradient component r of a pair: He(r,0) gx + He(r,1) gy + He(r,2) gz
@@ -86,7 +79,7 @@ __device__ __forceinline__ float2 divT2(const float2* fx, const float2* fy, cons
 }
 
 #ifndef SOD_MX2_MIN_CTAS
-#define SOD_MX2_MIN_CTAS 8  // resident 64-thread element groups per SM the register budget must allow
+#define SOD_MX2_MIN_CTAS 10  // resident 64-thread element groups per SM the register budget must allow
 #endif
 template <int EPB>
 __global__ void __launch_bounds__(64 * EPB, (EPB >= SOD_MX2_MIN_CTAS ? 1 : SOD_MX2_MIN_CTAS / EPB))
