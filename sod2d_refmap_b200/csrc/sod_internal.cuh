@@ -66,6 +66,7 @@ extern std::atomic<int64_t> g_launches;
 struct DevParams {
   double gamma, Rgas, Cp, Prt, ce, cmax, cglob, c_rho, c_ener, cfl_conv, cfl_diff;
   int normalise;
+  double g_gm1, inv_gm1, inv_Rgas;  // gamma/(gamma-1), 1/(gamma-1), 1/Rgas (host-computed)
 };
 
 // 1-D derivative matrix in natural order: D[m][n] = l_n'(x_m)

@@ -239,6 +239,9 @@ static void to_dev_params(const SodParams* s, DevParams* d) {
   d->gamma = s->gamma_gas; d->Rgas = s->Rgas; d->Cp = s->Cp; d->Prt = s->Prt;
   d->ce = s->ce; d->cmax = s->cmax; d->cglob = s->cglob; d->c_rho = s->c_rho; d->c_ener = s->c_ener;
   d->cfl_conv = s->cfl_conv; d->cfl_diff = s->cfl_diff; d->normalise = s->flag_normalise_entropy;
+  d->g_gm1 = s->gamma_gas / (s->gamma_gas - 1.0);
+  d->inv_gm1 = 1.0 / (s->gamma_gas - 1.0);
+  d->inv_Rgas = 1.0 / s->Rgas;
 }
 
 int sod_mesh_set_params(SodMesh* m, const SodParams* p) {

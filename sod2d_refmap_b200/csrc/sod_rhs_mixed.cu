@@ -128,8 +128,8 @@ __global__ void __launch_bounds__(64 * EPB, (EPB >= SOD_MX2_MIN_CTAS ? 1 : SOD_M
   const double kk = 0.5 * umag;
   const double e_int = Et * irho - 0.5 * umag;
   const double p = rho * (g - 1.0) * e_int;
-  const double h = (g / (g - 1.0)) * p * irho;
-  const double T = p * irho * (1.0 / a.prm.Rgas);
+  const double h = a.prm.g_gm1 * p * irho;
+  const double T = p * irho * a.prm.inv_Rgas;
   const float mufac = (float)a.mu_factor[n];
   const float mue = reinterpret_cast<const float*>(a.mue)[(size_t)ee * NN + d];
   const double musgs = a.musgs ? a.musgs[(size_t)ee * NN + d] : 0.0;
@@ -142,6 +142,7 @@ __global__ void __launch_bounds__(64 * EPB, (EPB >= SOD_MX2_MIN_CTAS ? 1 : SOD_M
     refs[10] = (rho / (g - 1.0)) * L;
     refs[11] = T;
     refs[12] = L;
+    refs[13] = 1.0 / p;
   }
   __syncthreads();
   const double r_rho = refs[0], r_p = refs[7], r_h = refs[8], r_k = refs[9], r_eta = refs[10], r_T = refs[11],
@@ -152,8 +153,8 @@ __global__ void __launch_bounds__(64 * EPB, (EPB >= SOD_MX2_MIN_CTAS ? 1 : SOD_M
   const double r_H = r_h + r_k;
   // eta - eta_r = ((rho-rho_r) L_r + rho (L - L_r)) / (gamma-1), L - L_r by log1p of small ratios
   const float drho = (float)(rho - r_rho);
-  const float dL = log1pf((float)((p - r_p) / r_p)) - (float)g * log1pf(drho / (float)r_rho);
-  const double s_eta = ((double)drho * r_L + rho * (double)dL) / (g - 1.0);
+  const float dL = log1pf((float)((p - r_p) * refs[13])) - (float)g * log1pf(drho / (float)r_rho);
+  const double s_eta = ((double)drho * r_L + rho * (double)dL) * a.prm.inv_gm1;
   const float Tf = (float)T;
   const float muf = mufac * (float)kC1 * (Tf * sqrtf(Tf)) / (Tf + (float)kS);
   const float su[3] = {(float)(uv[0] - r_u[0]), (float)(uv[1] - r_u[1]), (float)(uv[2] - r_u[2])};
