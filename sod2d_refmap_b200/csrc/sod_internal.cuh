@@ -67,6 +67,8 @@ struct DevParams {
   double gamma, Rgas, Cp, Prt, ce, cmax, cglob, c_rho, c_ener, cfl_conv, cfl_diff;
   int normalise;
   double g_gm1, inv_gm1, inv_Rgas;  // gamma/(gamma-1), 1/(gamma-1), 1/Rgas (host-computed)
+  // FP32 copies for the mixed kernels (host-converted: FP64->FP32 conversions are slow on the GPU)
+  float gamma_f, c_rho_f, c_ener_f, CpPr_f, Cp09_f;  // gamma, c_rho, c_ener, Cp/Prt, Cp/0.9
 };
 
 // 1-D derivative matrix in natural order: D[m][n] = l_n'(x_m)
@@ -87,8 +89,9 @@ struct RhsArgs {
   const double* __restrict__ q2;
   const double* __restrict__ E;
   const double* __restrict__ mu_factor;  // per node
-  void* rel;                       // R [e][6][64]
+  void* rel;                       // R [(e*64 + d)*6 + f]
   DMat D;
+  float Df[NP1][NP1];              // D in FP32 (mixed kernels)
   DevParams prm;
 };
 

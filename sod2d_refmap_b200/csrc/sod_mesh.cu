@@ -242,6 +242,11 @@ static void to_dev_params(const SodParams* s, DevParams* d) {
   d->g_gm1 = s->gamma_gas / (s->gamma_gas - 1.0);
   d->inv_gm1 = 1.0 / (s->gamma_gas - 1.0);
   d->inv_Rgas = 1.0 / s->Rgas;
+  d->gamma_f = (float)s->gamma_gas;
+  d->c_rho_f = (float)s->c_rho;
+  d->c_ener_f = (float)s->c_ener;
+  d->CpPr_f = (float)(s->Cp / s->Prt);
+  d->Cp09_f = (float)(s->Cp / 0.9);
 }
 
 int sod_mesh_set_params(SodMesh* m, const SodParams* p) {

@@ -698,6 +698,8 @@ int launch_rhs(SodMesh* m, bool mixed, int epb, const double* rho, const double*
   a.mu_factor = mu_factor;
   a.rel = m->buf.rel;
   a.D = m->D;
+  for (int r = 0; r < NP1; ++r)
+    for (int c = 0; c < NP1; ++c) a.Df[r][c] = (float)m->D.d[r][c];
   a.prm = m->prm;
   if (!mixed) {
     switch (epb) {

@@ -24,7 +24,7 @@ constexpr double kS = 110.4;
 constexpr int NBC = 13;  // batch B+C slots
 constexpr int NP2 = 9;   // pass-2 slots
 constexpr int NSLOT = NBC + NP2;  // batch A (6 pairs) reuses the first slots of the BC area
-constexpr int NREF = 16 + 36 + 18;  // node-0 refs, 3 corner values of the 12 batch-A fields, FP32 slopes
+constexpr int NREF = 16 + 36 + 18 + 6;  // node-0 refs, corner values of the batch-A fields, FP32 slopes, FP32 refs
 
 __host__ __device__ constexpr size_t smem_bytes(int epb) {
   return sizeof(double) * (size_t)epb * NREF + sizeof(float2) * (size_t)epb * NSLOT * FSTRIDE;
@@ -103,9 +103,9 @@ __global__ void __launch_bounds__(64 * EPB, (EPB >= SOD_MX2_MIN_CTAS ? 1 : SOD_M
   float2 Dx[4], Dy[4], Dz[4];
 #pragma unroll
   for (int m = 0; m < 4; ++m) {
-    Dx[m] = F2((float)a.D.d[i][m]);
-    Dy[m] = F2((float)a.D.d[j][m]);
-    Dz[m] = F2((float)a.D.d[k][m]);
+    Dx[m] = F2(a.Df[i][m]);
+    Dy[m] = F2(a.Df[j][m]);
+    Dz[m] = F2(a.Df[k][m]);
   }
   float H[9];
 #pragma unroll
@@ -143,17 +143,22 @@ __global__ void __launch_bounds__(64 * EPB, (EPB >= SOD_MX2_MIN_CTAS ? 1 : SOD_M
     refs[11] = T;
     refs[12] = L;
     refs[13] = 1.0 / p;
+    // FP32 copies of the references, converted once per element
+    float* rf = reinterpret_cast<float*>(refs + 16 + 36 + 18);
+    rf[0] = (float)rho; rf[1] = (float)uv[0]; rf[2] = (float)uv[1]; rf[3] = (float)uv[2];
+    rf[4] = (float)qv[0]; rf[5] = (float)qv[1]; rf[6] = (float)qv[2];
+    rf[7] = (float)(h + kk); rf[8] = (float)refs[10]; rf[9] = (float)T;
   }
   __syncthreads();
-  const double r_rho = refs[0], r_p = refs[7], r_h = refs[8], r_k = refs[9], r_eta = refs[10], r_T = refs[11],
+  const double r_rho = refs[0], r_p = refs[7], r_h = refs[8], r_k = refs[9], r_T = refs[11],
                r_L = refs[12];
   const double r_u[3] = {refs[1], refs[2], refs[3]};
   const double r_q[3] = {refs[4], refs[5], refs[6]};
   const double s_H = (h - r_h) + (kk - r_k);  // deviation of the total enthalpy H = h + k
-  const double r_H = r_h + r_k;
   // eta - eta_r = ((rho-rho_r) L_r + rho (L - L_r)) / (gamma-1), L - L_r by log1p of small ratios
   const float drho = (float)(rho - r_rho);
-  const float dL = log1pf((float)((p - r_p) * refs[13])) - (float)g * log1pf(drho / (float)r_rho);
+  const float* rf = reinterpret_cast<const float*>(refs + 16 + 36 + 18);  // FP32 references
+  const float dL = log1pf((float)((p - r_p) * refs[13])) - a.prm.gamma_f * log1pf(drho / rf[0]);
   const double s_eta = ((double)drho * r_L + rho * (double)dL) * a.prm.inv_gm1;
   const float Tf = (float)T;
   const float muf = mufac * (float)kC1 * (Tf * sqrtf(Tf)) / (Tf + (float)kS);
@@ -229,14 +234,16 @@ __global__ void __launch_bounds__(64 * EPB, (EPB >= SOD_MX2_MIN_CTAS ? 1 : SOD_M
 #undef SOD_PAIR_GRAD
   }
 #pragma unroll
-  for (int c = 0; c < 3; ++c) gradRH[c] += (float)r_H * gradRho[c];
+  for (int c = 0; c < 3; ++c) gradRH[c] += rf[7] * gradRho[c];
   const float divU = gradU[0][0] + gradU[1][1] + gradU[2][2];
   const float divQ = gradQ[0][0] + gradQ[1][1] + gradQ[2][2];
-  const float rhoR = (float)rho, HR = (float)(h + kk);
-  const float etaR = (float)(r_eta + s_eta);
-  const float uR[3] = {(float)uv[0], (float)uv[1], (float)uv[2]};
-  const float qR[3] = {(float)qv[0], (float)qv[1], (float)qv[2]};
-  const float rHR = (float)(rho * (h + kk));
+  // node values in FP32 as reference + deviation (float adds instead of FP64->FP32 conversions)
+  const float sHf = (float)s_H, sef = (float)s_eta;
+  const float rhoR = rf[0] + drho, HR = rf[7] + sHf;
+  const float etaR = rf[8] + sef;
+  const float uR[3] = {rf[1] + su[0], rf[2] + su[1], rf[3] + su[2]};
+  const float qR[3] = {rf[4] + sq[0], rf[5] + sq[1], rf[6] + sq[2]};
+  const float rHR = rhoR * HR;
 
   // ---- convective terms available after batch A (elem_convec.f90:412-432) + reference parts
   float Rm = 0.5f * (divQ + rhoR * divU);
@@ -244,7 +251,7 @@ __global__ void __launch_bounds__(64 * EPB, (EPB >= SOD_MX2_MIN_CTAS ? 1 : SOD_M
   float Rmo[3];
   float Ret = 0.5f * (etaR * divU);
   {
-    const float rH = (float)r_H, re = (float)r_eta;
+    const float rH = rf[7], re = rf[8];
     Ren += 0.25f * (rH * divQ + rhoR * (rH * divU));
     Ret += 0.5f * (re * divU);
   }
@@ -254,19 +261,19 @@ __global__ void __launch_bounds__(64 * EPB, (EPB >= SOD_MX2_MIN_CTAS ? 1 : SOD_M
     Rm += 0.5f * (uR[c] * gradRho[c]);
     Ren += 0.25f * (qR[c] * gradH[c] + uR[c] * gradRH[c] + (HR * uR[c]) * gradRho[c]);
     Ret += 0.5f * (uR[c] * gradEta[c]);
-    float dF = (float)r_q[c] * divU, dFuu = (float)r_u[c] * divU;
+    float dF = rf[4 + c] * divU, dFuu = rf[1 + c] * divU;
 #pragma unroll
     for (int jd = 0; jd < 3; ++jd) {
       Rmo[c] += 0.25f * ((uR[c] * uR[jd]) * gradRho[jd] + qR[jd] * gradU[c][jd] + uR[jd] * gradQ[c][jd]);
-      dF += (float)r_u[jd] * gradQ[c][jd];
-      dFuu += (float)r_u[jd] * gradU[c][jd];
+      dF += rf[1 + jd] * gradQ[c][jd];
+      dFuu += rf[1 + jd] * gradU[c][jd];
     }
     Rmo[c] += 0.25f * (dF + rhoR * dFuu);
   }
 
   // ---- diffusion pass 1 (elem_diffu.f90:70-140) -> contravariant flux pairs per direction
   {
-    const float mufgp = muf + (float)(rho * musgs);
+    const float mufgp = a.musgs ? muf + (float)(rho * musgs) : muf;
     const float mut = mufgp + mue;
     const float twoThirds = 2.0f / 3.0f;
     float tau[3][3];
@@ -297,8 +304,8 @@ __global__ void __launch_bounds__(64 * EPB, (EPB >= SOD_MX2_MIN_CTAS ? 1 : SOD_M
 
   // ---- batch B+C (13 pairs)
   {
-    const float sH = (float)s_H, se = (float)s_eta;
-    const float rsH = (float)(rho * s_H);
+    const float sH = sHf, se = sef;
+    const float rsH = rhoR * sHf;
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       buf[(0 + c) * FSTRIDE + s_me] = make_float2(rsH * uR[c], sH * uR[c]);
@@ -353,16 +360,16 @@ __global__ void __launch_bounds__(64 * EPB, (EPB >= SOD_MX2_MIN_CTAS ? 1 : SOD_M
   float2 DTx[4], DTy[4], DTz[4];
 #pragma unroll
   for (int m = 0; m < 4; ++m) {
-    DTx[m] = F2((float)a.D.d[m][i]);
-    DTy[m] = F2((float)a.D.d[m][j]);
-    DTz[m] = F2((float)a.D.d[m][k]);
+    DTx[m] = F2(a.Df[m][i]);
+    DTy[m] = F2(a.Df[m][j]);
+    DTz[m] = F2(a.Df[m][k]);
   }
   const float2 vA = divT2(p2 + 0 * FSTRIDE, p2 + 1 * FSTRIDE, p2 + 2 * FSTRIDE, i, j, k, DTx, DTy, DTz);
   const float2 vB = divT2(p2 + 3 * FSTRIDE, p2 + 4 * FSTRIDE, p2 + 5 * FSTRIDE, i, j, k, DTx, DTy, DTz);
   const float2 vC = divT2(p2 + 6 * FSTRIDE, p2 + 7 * FSTRIDE, p2 + 8 * FSTRIDE, i, j, k, DTx, DTy, DTz);
-  const float nu_e = (float)a.prm.c_rho * mue / rhoR;
-  const float CpPr = (float)(a.prm.Cp / a.prm.Prt);
-  const float kappa_e = muf * CpPr + (float)a.prm.c_ener * mue * CpPr + (float)(a.prm.Cp * rho * musgs / 0.9);
+  const float nu_e = a.prm.c_rho_f * mue / rhoR;
+  const float CpPr = a.prm.CpPr_f;
+  const float kappa_e = muf * CpPr + a.prm.c_ener_f * mue * CpPr + (a.musgs ? a.prm.Cp09_f * rhoR * (float)musgs : 0.f);
   if (active) {
     store_res6<float>(reinterpret_cast<float*>(a.rel), (size_t)e * NN + d, gpv * Rm + nu_e * vA.x,
                       gpv * Rmo[0] + vB.y, gpv * Rmo[1] + vC.x, gpv * Rmo[2] + vC.y,
