@@ -24,7 +24,7 @@ constexpr double kS = 110.4;
 constexpr int NBC = 13;  // batch B+C slots
 constexpr int NP2 = 9;   // pass-2 slots
 constexpr int NSLOT = NBC + NP2;  // batch A (6 pairs) reuses the first slots of the BC area
-constexpr int NREF = 16 + 36 + 18 + 6;  // node-0 refs, corner values of the batch-A fields, FP32 slopes, FP32 refs
+constexpr int NREF = 16 + 36 + 18 + 6;  // node-0 refs, corner values of the batch-A fields, FP32 slopes, 12 FP32 refs
 
 __host__ __device__ constexpr size_t smem_bytes(int epb) {
   return sizeof(double) * (size_t)epb * NREF + sizeof(float2) * (size_t)epb * NSLOT * FSTRIDE;
@@ -148,6 +148,7 @@ __global__ void __launch_bounds__(64 * EPB, (EPB >= SOD_MX2_MIN_CTAS ? 1 : SOD_M
     rf[0] = (float)rho; rf[1] = (float)uv[0]; rf[2] = (float)uv[1]; rf[3] = (float)uv[2];
     rf[4] = (float)qv[0]; rf[5] = (float)qv[1]; rf[6] = (float)qv[2];
     rf[7] = (float)(h + kk); rf[8] = (float)refs[10]; rf[9] = (float)T;
+    rf[10] = (float)(1.0 / rho); rf[11] = (float)refs[13];
   }
   __syncthreads();
   const double r_rho = refs[0], r_p = refs[7], r_h = refs[8], r_k = refs[9], r_T = refs[11],
@@ -158,12 +159,9 @@ __global__ void __launch_bounds__(64 * EPB, (EPB >= SOD_MX2_MIN_CTAS ? 1 : SOD_M
   // eta - eta_r = ((rho-rho_r) L_r + rho (L - L_r)) / (gamma-1), L - L_r by log1p of small ratios
   const float drho = (float)(rho - r_rho);
   const float* rf = reinterpret_cast<const float*>(refs + 16 + 36 + 18);  // FP32 references
-  const float dL = log1pf((float)((p - r_p) * refs[13])) - a.prm.gamma_f * log1pf(drho / rf[0]);
+  const float dpf = (float)(p - r_p);
+  const float dL = log1pf(dpf * rf[11]) - a.prm.gamma_f * log1pf(drho * rf[10]);
   const double s_eta = ((double)drho * r_L + rho * (double)dL) * a.prm.inv_gm1;
-  const float Tf = (float)T;
-  const float muf = mufac * (float)kC1 * (Tf * sqrtf(Tf)) / (Tf + (float)kS);
-  const float su[3] = {(float)(uv[0] - r_u[0]), (float)(uv[1] - r_u[1]), (float)(uv[2] - r_u[2])};
-  const float sq[3] = {(float)(qv[0] - r_q[0]), (float)(qv[1] - r_q[1]), (float)(qv[2] - r_q[2])};
 
   // ---- batch A (6 pairs).  The nodal fields differentiated directly (except rho and p, whose
   // rounding does not reach the 1e-7 level of the residuals) get an element reference that is
@@ -174,6 +172,7 @@ __global__ void __launch_bounds__(64 * EPB, (EPB >= SOD_MX2_MIN_CTAS ? 1 : SOD_M
   // expansion the discrete product derivative needs.
   const double dev[12] = {rho - r_rho, p - r_p, uv[0] - r_u[0], uv[1] - r_u[1], uv[2] - r_u[2],
                           qv[0] - r_q[0], qv[1] - r_q[1], qv[2] - r_q[2], s_H, rho * s_H, s_eta, T - r_T};
+  float vp[12];
   double* crn = refs + 16;  // [dir][12]: values at local nodes (3,0,0), (0,3,0), (0,0,3)
   float2* slopes = reinterpret_cast<float2*>(refs + 16 + 36);  // [dir][6 pairs]: a_dir in FP32
   {
@@ -194,9 +193,8 @@ __global__ void __launch_bounds__(64 * EPB, (EPB >= SOD_MX2_MIN_CTAS ? 1 : SOD_M
       return t == 0 ? 0.0 : (t == 1 ? 0.5 * (1.0 - kX) : (t == 2 ? 0.5 * (1.0 + kX) : 1.0));
     };
     const double wx = xh(i), wy = xh(j), wz = xh(k);
-    float vp[12];
-    vp[0] = (float)dev[0];  // rho' and p' keep the constant reference (their rounding is harmless)
-    vp[1] = (float)dev[1];
+    vp[0] = drho;  // rho' and p' keep the constant reference (their rounding is harmless)
+    vp[1] = dpf;
 #pragma unroll
     for (int f = 2; f < 12; f += 2) {
       const double2 cx = *reinterpret_cast<const double2*>(crn + f);
@@ -208,6 +206,25 @@ __global__ void __launch_bounds__(64 * EPB, (EPB >= SOD_MX2_MIN_CTAS ? 1 : SOD_M
 #pragma unroll
     for (int t = 0; t < 6; ++t) buf[t * FSTRIDE + s_me] = make_float2(vp[2 * t], vp[2 * t + 1]);
   }
+  // FP32 deviations from node 0 = affine deviation + affine part (FP32 FMAs instead of
+  // FP64->FP32 conversions, which share the slow XU pipe)
+  float su[3], sq[3], sHf, sef, Tf;
+  {
+    auto xf = [&](int t) {  // xi_t + 1
+      return t == 0 ? 0.f : (t == 1 ? 0.55278640450004206f : (t == 2 ? 1.44721359549995794f : 2.f));
+    };
+    const float2 wx2 = F2(xf(i)), wy2 = F2(xf(j)), wz2 = F2(xf(k));
+    float2 lin[6];
+#pragma unroll
+    for (int t = 1; t < 6; ++t)
+      lin[t] = FMA2(slopes[12 + t], wz2, FMA2(slopes[6 + t], wy2, MUL2(slopes[t], wx2)));
+    su[0] = vp[2] + lin[1].x; su[1] = vp[3] + lin[1].y; su[2] = vp[4] + lin[2].x;
+    sq[0] = vp[5] + lin[2].y; sq[1] = vp[6] + lin[3].x; sq[2] = vp[7] + lin[3].y;
+    sHf = vp[8] + lin[4].x;
+    sef = vp[10] + lin[5].x;
+    Tf = rf[9] + (vp[11] + lin[5].y);
+  }
+  const float muf = mufac * (float)kC1 * (Tf * sqrtf(Tf)) / (Tf + (float)kS);
   __syncthreads();
 
   float gradRho[3], gradP[3], gradU[3][3], gradQ[3][3], gradH[3], gradRH[3], gradEta[3], gradT[3];
@@ -238,7 +255,6 @@ __global__ void __launch_bounds__(64 * EPB, (EPB >= SOD_MX2_MIN_CTAS ? 1 : SOD_M
   const float divU = gradU[0][0] + gradU[1][1] + gradU[2][2];
   const float divQ = gradQ[0][0] + gradQ[1][1] + gradQ[2][2];
   // node values in FP32 as reference + deviation (float adds instead of FP64->FP32 conversions)
-  const float sHf = (float)s_H, sef = (float)s_eta;
   const float rhoR = rf[0] + drho, HR = rf[7] + sHf;
   const float etaR = rf[8] + sef;
   const float uR[3] = {rf[1] + su[0], rf[2] + su[1], rf[3] + su[2]};
