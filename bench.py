@@ -273,12 +273,13 @@ def bench_batch(nmember: int, steps: int):
 
 
 def bench_adjoint(n: int, steps: int, every: int):
-    """Adjoint: loss 1/2 ||rho u||^2 after `steps` FP64 RK4 steps on an n^3 jittered periodic
-    HEX64 mesh (seed 3), gradient w.r.t. the initial (rho, q, E) by the checkpointed adjoint
-    (checkpoint every `every` steps; mu_e and dt frozen at their forward values).  Times the
+    """Adjoint: loss 1/2 ||rho u||^2 after `steps` RK4 steps on an n^3 jittered periodic HEX64
+    mesh (seed 3), gradient w.r.t. the initial (rho, q, E) by the checkpointed adjoint
+    (checkpoint every `every` steps; mu_e and dt frozen at their forward values), with the
+    trajectory in FP64 and in mixed precision (the step VJPs are FP64 in both).  Times the
     forward (with checkpointing) and the backward by CUDA events, and checks the directional
     derivative along a seeded Gaussian direction (seed 9) against central differences of the
-    frozen-coefficient forward map at h = 1e-4 and 1e-6."""
+    frozen-coefficient forward map of the same precision at h = 1e-4 and 1e-6."""
     import torch
     from sod2d_refmap_b200 import mesh as M, solver as S
     from sod2d_refmap_b200.adjoint import Sod2dRollout, replay, trajectory_coefficients, _clone_state
@@ -288,15 +289,19 @@ def bench_adjoint(n: int, steps: int, every: int):
     s = S.Sod2dState.from_host(M.taylor_green_state(m, prm), gm.nelem)
     gm.adapt_dt(s)
     gm.rk_4_main(s, S.FP64, update_dt=True)  # a state with mu_e > 0
+    g = torch.Generator(device="cuda")
+    g.manual_seed(9)
+    v = [torch.randn(x.shape, dtype=torch.float64, device="cuda", generator=g) * x.abs().mean()
+         for x in (s.rho, s.q, s.E)]
 
-    def run(K):
+    def run(K, prec):
         rho = s.rho.clone().requires_grad_(True)
         q = s.q.clone().requires_grad_(True)
         E = s.E.clone().requires_grad_(True)
         ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
         torch.cuda.synchronize()
         ev[0].record()
-        _, qK, _ = Sod2dRollout.apply(gm, s, rho, q, E, K, every)
+        _, qK, _ = Sod2dRollout.apply(gm, s, rho, q, E, K, every, True, prec)
         loss = 0.5 * (qK * qK).sum()
         ev[1].record()
         loss.backward()
@@ -304,50 +309,43 @@ def bench_adjoint(n: int, steps: int, every: int):
         torch.cuda.synchronize()
         return (rho.grad, q.grad, E.grad), float(loss.item()), ev[0].elapsed_time(ev[1]), ev[1].elapsed_time(ev[2])
 
-    run(2)  # warm-up
-    grads, loss, t_fwd, t_bwd = run(steps)
-    # the plain forward (no checkpoint copies): eager steps and a captured graph
-    t = _clone_state(s)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record()
-    for _ in range(steps):
-        gm.rk_4_main(t, S.FP64, update_dt=True)
-    e1.record()
-    torch.cuda.synchronize()
-    t_plain = e0.elapsed_time(e1)
-    t = _clone_state(s)
-    gm.rk4_steps(t, 1, precision=S.FP64)
-    t = _clone_state(s)
-    torch.cuda.synchronize()
-    e0.record()
-    gm.rk4_steps(t, steps, precision=S.FP64)
-    e1.record()
-    torch.cuda.synchronize()
-    t_graph = e0.elapsed_time(e1)
-    # directional derivative vs central differences of the frozen-coefficient map
-    mus, dts = trajectory_coefficients(gm, s, steps)
-    g = torch.Generator(device="cuda")
-    g.manual_seed(9)
-    v = [torch.randn(x.shape, dtype=torch.float64, device="cuda", generator=g) * x.abs().mean()
-         for x in (s.rho, s.q, s.E)]
-    dL = float(sum((gi * vi).sum() for gi, vi in zip(grads, v)).item())
+    out = {"mesh": f"{n}^3 HEX64 jittered periodic", "nodes": m.npoin, "steps": steps, "checkpoint_every": every}
+    dls = {}
+    for prec, name in ((S.FP64, "fp64"), (S.MIXED, "mixed")):
+        run(2, prec)  # warm-up
+        grads, loss, t_fwd, t_bwd = run(steps, prec)
+        t = _clone_state(s)
+        gm.rk4_steps(t, 1, precision=prec)
+        t = _clone_state(s)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        gm.rk4_steps(t, steps, precision=prec)
+        e1.record()
+        torch.cuda.synchronize()
+        t_graph = e0.elapsed_time(e1)
+        mus, dts = trajectory_coefficients(gm, s, steps, prec)
+        dL = float(sum((gi * vi).sum() for gi, vi in zip(grads, v)).item())
+        dls[name] = dL
 
-    def L_at(h):
-        u = _clone_state(s)
-        u.rho.add_(h * v[0]); u.q.add_(h * v[1]); u.E.add_(h * v[2])
-        replay(gm, u, mus, dts)
-        return 0.5 * float((u.q * u.q).sum().item())
-    fd = {}
-    for h in (1e-4, 1e-6):
-        d = (L_at(h) - L_at(-h)) / (2 * h)
-        fd[f"{h:g}"] = {"fd": d, "rel_err": abs(d - dL) / abs(dL)}
+        def L_at(h):
+            u = _clone_state(s)
+            u.rho.add_(h * v[0]); u.q.add_(h * v[1]); u.E.add_(h * v[2])
+            replay(gm, u, mus, dts, prec)
+            return 0.5 * float((u.q * u.q).sum().item())
+        fd = {}
+        for h in (1e-4, 1e-6):
+            d = (L_at(h) - L_at(-h)) / (2 * h)
+            fd[f"{h:g}"] = {"fd": d, "rel_err": abs(d - dL) / abs(dL)}
+        out[name] = {"loss": loss, "directional_derivative": dL, "finite_differences": fd,
+                     "ms": {"forward_with_checkpoints": t_fwd, "backward": t_bwd, "forward_plain_graph": t_graph},
+                     "adjoint_over_forward": {"backward/forward_with_checkpoints": t_bwd / t_fwd,
+                                              "backward/forward_plain_graph": t_bwd / t_graph}}
+    out["mixed"]["directional_derivative_rel_diff_vs_fp64"] = abs(dls["mixed"] - dls["fp64"]) / abs(dls["fp64"])
+    out["note"] = ("step VJPs are FP64 in both; the mixed row differentiates the FP64 map along the mixed "
+                   "trajectory, and FP32 rounding noise of the mixed map limits its finite differences")
     gm.close()
-    return {"mesh": f"{n}^3 HEX64 jittered periodic", "nodes": m.npoin, "steps": steps, "checkpoint_every": every,
-            "precision": "fp64", "loss": loss, "directional_derivative": dL, "finite_differences": fd,
-            "ms": {"forward_with_checkpoints": t_fwd, "backward": t_bwd, "forward_plain_eager": t_plain,
-                   "forward_plain_graph": t_graph},
-            "adjoint_over_forward": {"backward/forward_with_checkpoints": t_bwd / t_fwd,
-                                     "backward/forward_plain_graph": t_bwd / t_graph}}
+    return out
 
 
 def bench_cg(n: int):

@@ -269,10 +269,10 @@ int sod_rhs_vjp(SodMesh* mesh, const double* rho, const double* q, const double*
                 const double* mu_e, const double* mu_factor, const double* bar_Rmass,
                 const double* bar_Rmom, const double* bar_Rener, double* grad_rho, double* grad_q,
                 double* grad_E, sod_stream_t stream);
-/* sod_rk4_main (FP64) that also writes its stage states Y2, Y3, Y4 to stages (device,
- * 15*npoin doubles: 3 stages x (rho, q x3, E) columns) for sod_rk4_step_vjp. */
+/* sod_rk4_main that also writes its stage states Y2, Y3, Y4 to stages (device, 15*npoin
+ * doubles: 3 stages x (rho, q x3, E) columns, FP64 in both precisions) for sod_rk4_step_vjp. */
 int sod_rk4_main_record(SodMesh* mesh, SodState* state, const double* dt_dev, double* dt_next_dev,
-                        double* stages, sod_stream_t stream);
+                        double* stages, SodPrecision prec, sod_stream_t stream);
 /* VJP of one RK4 step y_{n+1} = y_n - dt sum_s b_s R(Y_s) (rk_4_main, time_integ.f90:288-426)
  * at the state (rho, q, E) with mu_e and dt_dev frozen: out = (dy_{n+1}/dy_n)^T bar.  stages
  * from sod_rk4_main_record, or null to recompute them; out may alias bar. */

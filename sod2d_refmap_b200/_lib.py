@@ -74,7 +74,7 @@ _SIGS = {
     "sod_csr_spmv_scal": (_i, [C.c_int32, C.c_int32, _p, _p, _p, _p, _p, _p]),
     "sod_rhs_vjp": (_i, [_p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p]),
     "sod_rk4_step_vjp": (_i, [_p] * 15),
-    "sod_rk4_main_record": (_i, [_p] * 6),
+    "sod_rk4_main_record": (_i, [_p, _p, _p, _p, _p, _i, _p]),
     "sod_batch_create": (_i, [_p, _i, _p]),
     "sod_batch_destroy": (None, [_p]),
     "sod_batch_set_member": (_i, [_p, _i, _p]),

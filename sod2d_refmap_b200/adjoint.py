@@ -10,6 +10,12 @@ and finite-difference checks compare against.
 Memory: states (rho, q, E, mu_e, dt) are kept every ``checkpoint_every`` steps; the backward
 pass re-runs each segment from its checkpoint (bitwise identical, the solver is deterministic)
 and applies the hand-written step VJP (sod_rk4_step_vjp) in reverse.
+
+Precision: the trajectory (forward and re-run) can be the FP64 or the mixed path; the step
+VJPs are always the FP64 Jacobian-transpose evaluated at the stored stage states.  For the
+mixed trajectory the gradient is therefore that of the FP64 map along the mixed trajectory,
+which differs from the exact gradient of the mixed map by the mixed path's rounding
+(relative 1e-7 to 1e-6).
 """
 from __future__ import annotations
 
@@ -47,39 +53,39 @@ def _load(s: Sod2dState, c: _Ckpt):
     s.dt.copy_(c.dt)
 
 
-def rollout(mesh: Sod2dMesh, state: Sod2dState, nsteps: int, checkpoint_every: int = 10):
-    """Run nsteps FP64 steps in place (dt from the CFL condition after every step, as
-    rk_4_main) and return the checkpoints [(step index, _Ckpt)] at multiples of checkpoint_every."""
+def rollout(mesh: Sod2dMesh, state: Sod2dState, nsteps: int, checkpoint_every: int = 10, precision: int = FP64):
+    """Run nsteps steps in place (dt from the CFL condition after every step, as rk_4_main)
+    and return the checkpoints [(step index, _Ckpt)] at multiples of checkpoint_every."""
     ck = []
     for n in range(nsteps):
         if n % checkpoint_every == 0:
             ck.append((n, _ckpt(state)))
-        mesh.rk_4_main(state, FP64, update_dt=True)
+        mesh.rk_4_main(state, precision, update_dt=True)
     return ck
 
 
-def replay(mesh: Sod2dMesh, state: Sod2dState, mu_e_seq, dt_seq):
+def replay(mesh: Sod2dMesh, state: Sod2dState, mu_e_seq, dt_seq, precision: int = FP64):
     """The frozen-coefficient forward map: step n with mu_e_seq[n] and dt_seq[n] (device (1,))."""
     for mu_e, dt in zip(mu_e_seq, dt_seq):
         state.mu_e.copy_(mu_e)
         state.dt.copy_(dt)
-        mesh.rk_4_main(state, FP64, update_dt=False)
+        mesh.rk_4_main(state, precision, update_dt=False)
     return state
 
 
-def trajectory_coefficients(mesh: Sod2dMesh, state: Sod2dState, nsteps: int):
+def trajectory_coefficients(mesh: Sod2dMesh, state: Sod2dState, nsteps: int, precision: int = FP64):
     """(mu_e_n, dt_n) of each step of the unfrozen forward run from a copy of state."""
     s = _clone_state(state)
     mus, dts = [], []
     for _ in range(nsteps):
         mus.append(s.mu_e.clone())
         dts.append(s.dt.clone())
-        mesh.rk_4_main(s, FP64, update_dt=True)
+        mesh.rk_4_main(s, precision, update_dt=True)
     return mus, dts
 
 
 def backward_through(mesh: Sod2dMesh, template: Sod2dState, ckpts, nsteps: int, bar_rho, bar_q, bar_E,
-                     store_stages: bool = True):
+                     store_stages: bool = True, precision: int = FP64):
     """Adjoint of nsteps steps: (bar_rho, bar_q, bar_E) at step nsteps -> at step 0, in place.
     Each segment is re-run from its checkpoint; with store_stages the re-run keeps the RK stage
     states (15*npoin doubles per step) so that the step VJPs need no second recompute."""
@@ -96,9 +102,9 @@ def backward_through(mesh: Sod2dMesh, template: Sod2dState, ckpts, nsteps: int, 
         for t in range(n1 - n0):
             stack.append(_ckpt(s))
             if store_stages:
-                mesh.rk_4_main_record(s, stages[t], update_dt=True)
+                mesh.rk_4_main_record(s, stages[t], update_dt=True, precision=precision)
             else:
-                mesh.rk_4_main(s, FP64, update_dt=True)
+                mesh.rk_4_main(s, precision, update_dt=True)
         for t in range(n1 - n0 - 1, -1, -1):
             cs = stack[t]
             mesh.rk4_step_vjp(cs.rho, cs.q, cs.E, cs.mu_e, template.mu_factor, cs.dt, bar_rho, bar_q, bar_E,
@@ -112,7 +118,7 @@ class Sod2dRollout:
 
     @staticmethod
     def apply(mesh: Sod2dMesh, state: Sod2dState, rho, q, E, nsteps: int, checkpoint_every: int = 10,
-              store_stages: bool = True):
+              store_stages: bool = True, precision: int = FP64):
         torch = _torch()
 
         class _Fn(torch.autograd.Function):
@@ -122,7 +128,7 @@ class Sod2dRollout:
                 s.rho.copy_(rho_)
                 s.q.copy_(q_)
                 s.E.copy_(E_)
-                ck = rollout(mesh, s, nsteps, checkpoint_every)
+                ck = rollout(mesh, s, nsteps, checkpoint_every, precision)
                 ctx.ck = ck
                 ctx.template = state
                 return s.rho.clone(), s.q.clone(), s.E.clone()
@@ -131,7 +137,7 @@ class Sod2dRollout:
             def backward(ctx, g_rho, g_q, g_E):
                 z = lambda g, like: torch.zeros_like(like) if g is None else g.contiguous().clone()
                 br, bq, bE = z(g_rho, rho), z(g_q, q), z(g_E, E)
-                backward_through(mesh, ctx.template, ctx.ck, nsteps, br, bq, bE, store_stages)
+                backward_through(mesh, ctx.template, ctx.ck, nsteps, br, bq, bE, store_stages, precision)
                 return br, bq, bE
 
         return _Fn.apply(rho, q, E)

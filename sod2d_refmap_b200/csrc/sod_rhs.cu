@@ -899,16 +899,22 @@ int sod_rk4_main(SodMesh* m, SodState* s, const double* dt_dev, double* dt_next_
 }
 
 int sod_rk4_main_record(SodMesh* m, SodState* s, const double* dt_dev, double* dt_next_dev, double* stages,
-                        sod_stream_t stream) {
+                        SodPrecision prec, sod_stream_t stream) {
   int rc = check_state(m, s);
   if (rc) return rc;
   SOD_ARG(dt_dev && stages, "dt_dev/stages null");
+  SOD_ARG(prec == SOD_FP64 || prec == SOD_MIXED, "precision");
   cudaStream_t st = (cudaStream_t)stream;
-  rc = ensure_step_buffers(m, false);
+  const bool mixed = prec == SOD_MIXED;
+  rc = ensure_step_buffers(m, mixed);
   if (rc) return rc;
   rc = mesh_ref_to_internal_elem(m, s->mu_e, m->mue_int, st);
   if (rc) return rc;
-  rc = run_step(m, s, dt_dev, dt_next_dev, false, st, nullptr, stages);
+  if (mixed) {
+    rc = launch_copy_f32(m->mue_int, m->mue32, (int64_t)m->nelem * NN, st);
+    if (rc) return rc;
+  }
+  rc = run_step(m, s, dt_dev, dt_next_dev, mixed, st, nullptr, stages);
   if (rc) return rc;
   return mesh_internal_to_ref_elem(m, m->mue_int, s->mu_e, st);
 }

@@ -227,12 +227,14 @@ class Sod2dMesh:
                                            _stream(stream)))
         return g_rho, g_q, g_E
 
-    def rk_4_main_record(self, state: Sod2dState, stages, update_dt: bool = True, stream=None):
-        """FP64 rk_4_main that also stores the stage states Y2..Y4 in stages (15*npoin float64)."""
+    def rk_4_main_record(self, state: Sod2dState, stages, update_dt: bool = True, precision: int = FP64,
+                         stream=None):
+        """rk_4_main that also stores the stage states Y2..Y4 in stages (15*npoin float64)."""
         st = state.struct()
         _lib.check(_lib.load().sod_rk4_main_record(self.handle, C.byref(st), C.c_void_p(_ptr(state.dt)),
                                                   C.c_void_p(_ptr(state.dt) if update_dt else 0),
-                                                  C.c_void_p(_ptr(_contig(stages))), _stream(stream)))
+                                                  C.c_void_p(_ptr(_contig(stages))), int(precision),
+                                                  _stream(stream)))
 
     def rk4_step_vjp(self, rho, q, E, mu_e, mu_factor, dt, bar_rho, bar_q, bar_E, out=None, stages=None,
                      stream=None):

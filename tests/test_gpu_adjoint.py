@@ -242,7 +242,7 @@ def test_stored_stages_match_recompute(env):
     stages = torch.empty(15 * gm.npoin, dtype=torch.float64, device="cuda")
     x0 = (a.rho.clone(), a.q.clone(), a.E.clone(), a.mu_e.clone(), a.dt.clone())
     gm.rk_4_main(a, precision=S.FP64, update_dt=True)
-    gm.rk_4_main_record(b, stages, update_dt=True)
+    gm.rk_4_main_record(b, stages, update_dt=True)  # FP64
     torch.cuda.synchronize()
     for k in ("rho", "q", "E", "mu_e", "dt", "u", "pr", "eta"):
         assert torch.equal(getattr(a, k), getattr(b, k)), k
@@ -273,3 +273,32 @@ def test_rollout_checkpoint_spacing_invariant(env):
     for other in grads[1:]:
         for a, b in zip(grads[0], other):
             assert torch.equal(a, b)
+
+
+def test_mixed_trajectory_adjoint_close_to_fp64(env):
+    """Adjoint along the mixed-precision trajectory (FP64 step VJPs at the mixed stage states):
+    the recorded mixed step equals sod_rk4_main(SOD_MIXED) bit for bit, and the directional
+    derivative stays within 1e-5 of the FP64 one (the mixed state differs by ~1e-9)."""
+    from sod2d_refmap_b200.adjoint import Sod2dRollout
+    torch, gm, S = env["torch"], env["gm"], env["S"]
+    st = env["st"]["st1"]
+    a = S.Sod2dState.from_host(st, gm.nelem); a.dt.fill_(env["dt"])
+    b = S.Sod2dState.from_host(st, gm.nelem); b.dt.fill_(env["dt"])
+    stages = torch.empty(15 * gm.npoin, dtype=torch.float64, device="cuda")
+    gm.rk_4_main(a, precision=S.MIXED, update_dt=True)
+    gm.rk_4_main_record(b, stages, update_dt=True, precision=S.MIXED)
+    torch.cuda.synchronize()
+    for k in ("rho", "q", "E", "mu_e", "dt"):
+        assert torch.equal(getattr(a, k), getattr(b, k)), k
+    rng = np.random.default_rng(12)
+    v = [_dev(torch, x) for x in (lambda d: (d[0], d[1].T, d[2]))(_rand_dir(rng, st))]
+    dl = {}
+    for prec in (S.FP64, S.MIXED):
+        s = _rollout_env(env, 4)
+        rho = s.rho.clone().requires_grad_(True)
+        q = s.q.clone().requires_grad_(True)
+        E = s.E.clone().requires_grad_(True)
+        _, qK, _ = Sod2dRollout.apply(gm, s, rho, q, E, 4, 2, True, prec)
+        (0.5 * (qK * qK).sum()).backward()
+        dl[prec] = float(sum((g * w).sum() for g, w in zip((rho.grad, q.grad, E.grad), v)).item())
+    assert abs(dl[S.MIXED] - dl[S.FP64]) <= 1e-5 * abs(dl[S.FP64]), dl
