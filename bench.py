@@ -206,6 +206,18 @@ def _rel_l2(a, b):
     return float((a - b).norm()) / (nb if nb > 0 else 1.0)
 
 
+# Arithmetic operations of the reference formulation of one stage RHS (mass, momentum, energy
+# residuals incl. EOS, Sutherland, diffusion, convection, assembly and 1/Ml; entropy residual
+# not included) per HEX64 element of a periodic mesh (27 unique nodes per element), counted by
+# the oracle's operation-counting type (oracle_rhs_opcount; sqrt and pow count as one).
+RHS_OPS_PER_ELEMENT = 152800
+
+
+def fp32_peak_tflops(sm_mhz: float) -> float:
+    """Nominal FP32 CUDA-core peak of a B200: 148 SMs x 128 lanes x 2 flops per FMA x clock."""
+    return 148 * 128 * 2 * sm_mhz * 1e6 / 1e12
+
+
 def kr_bytes_per_launch(nelem: int, npoin: int, mixed: bool) -> float:
     """Algorithmic HBM bytes of one fused-RHS launch: per element the geometry (9 He + gpvol),
     mu_e and connectivity read and the 6x64 element residuals written; per node the 5
@@ -540,6 +552,13 @@ def run_ours(args):
             "traffic": None, "bytes_per_launch": kr_bytes, "ms_per_launch": kr_ms,
             "fp64_kernel": {"ms_per_launch": prof["fp64"][0], "bytes_per_launch": kr64_bytes,
                             "achieved_GBs": kr64_bytes / (prof["fp64"][0] / 1e3) / 1e9},
+            "arithmetic": {"ops_per_launch": RHS_OPS_PER_ELEMENT * gm.nelem,
+                           "achieved_tflops": RHS_OPS_PER_ELEMENT * gm.nelem / (kr_ms / 1e3) / 1e12,
+                           "peak_tflops": fp32_peak_tflops(1965.0),
+                           "frac": RHS_OPS_PER_ELEMENT * gm.nelem / (kr_ms / 1e3) / 1e12 / fp32_peak_tflops(1965.0),
+                           "note": "reference-formulation operation count (oracle) over the measured mixed "
+                                   "launch time, against the nominal FP32 CUDA-core peak at 1965 MHz "
+                                   "(148 SMs x 128 lanes x 2); no measured FP32 peak exists for this pool"},
             "kernel_ms": {"mixed": {"rhs": prof["mixed"][0], "gather_rk": prof["mixed"][1], "visc_dt": prof["mixed"][2]},
                           "fp64": {"rhs": prof["fp64"][0], "gather_rk": prof["fp64"][1], "visc_dt": prof["fp64"][2]}}}
     tr = os.path.join(ROOT, "profiles", "traffic.txt")

@@ -235,6 +235,16 @@ def rhs_stage(om: OracleMesh, prm, st, mu_e=None):
     return R.reshape(5, om.npoin)
 
 
+def rhs_opcount(om: OracleMesh, prm, st, mu_e=None) -> float:
+    """Arithmetic operations of one stage RHS evaluation (reference formulation, whole mesh)."""
+    P = params_of(prm)
+    mue = np.asfortranarray(st.mu_e if mu_e is None else mu_e)
+    f = lib().oracle_rhs_opcount
+    f.restype = C.c_double
+    return float(f(C.byref(om.ctx), C.byref(P), ptr(om.Ml), ptr(st.mu_factor), ptr(mue), ptr(st.rho),
+                   ptr(np.asfortranarray(st.q)), ptr(st.E)))
+
+
 def rhs_jvp(om: OracleMesh, prm, st, drho, dq, dE, mu_e=None):
     """Exact JVP of rhs_stage along (drho, dq(npoin,3), dE): returns (R, dR) as (5, npoin)."""
     P = params_of(prm)

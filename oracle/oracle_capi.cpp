@@ -1,3 +1,4 @@
+#include <omp.h>
 // CPU ORACLE C API — test infrastructure only (see sod2d_oracle.hpp).  Loaded by tests/,
 // __graft_entry__.smoke() and bench.py's CPU-baseline legs through oracle/oracle.py.
 #include "sod2d_oracle.hpp"
@@ -156,6 +157,24 @@ void oracle_rhs_jvp(const ElemCtx* ctx, const Params* P, const double* Ml, const
   for (int64_t p = 0; p < 3 * N; ++p) qq[p] = Dual(q[p], dq[p]);
   rhs_stage_t<Dual>(*ctx, *P, Ml, mu_factor, mu_e, mu_sgs, r.data(), qq.data(), e.data(), out.data());
   for (int64_t p = 0; p < 5 * N; ++p) { if (R) R[p] = out[p].v; dR[p] = out[p].d; }
+}
+
+// Number of arithmetic operations (+ - * /, sqrt and pow as one each) of one oracle_rhs_stage
+// evaluation, counted single-threaded with the OpCount type.
+double oracle_rhs_opcount(const ElemCtx* ctx, const Params* P, const double* Ml, const double* mu_factor,
+                          const double* mu_e, const double* rho, const double* q, const double* E) {
+  const int64_t N = ctx->npoin;
+  std::vector<double> zeros((size_t)ctx->nelem * nnode, 0.0);
+  std::vector<OpCount> r(N), qq(3 * N), e(N), out(5 * N);
+  for (int64_t p = 0; p < N; ++p) { r[p] = OpCount(rho[p]); e[p] = OpCount(E[p]); }
+  for (int64_t p = 0; p < 3 * N; ++p) qq[p] = OpCount(q[p]);
+  const int nt = omp_get_max_threads();
+  omp_set_num_threads(1);
+  op_count() = 0;
+  rhs_stage_t<OpCount>(*ctx, *P, Ml, mu_factor, mu_e, zeros.data(), r.data(), qq.data(), e.data(), out.data());
+  const double n = (double)op_count();
+  omp_set_num_threads(nt);
+  return n;
 }
 
 }  // extern "C"

@@ -693,6 +693,38 @@ inline double pow(double a, double e) { return std::pow(a, e); }
 inline double value(double a) { return a; }
 inline double value(Dual a) { return a.v; }
 
+// Operation counter: a double that counts every +, -, *, / (and sqrt, pow as one operation
+// each) applied to it, to give the reference formulation's algorithmic operation count.
+// Counting runs single-threaded.
+struct OpCount {
+  double v = 0.0;
+  OpCount() = default;
+  OpCount(double a) : v(a) {}
+};
+inline uint64_t& op_count() {
+  static uint64_t c = 0;
+  return c;
+}
+inline OpCount opc(double v) { ++op_count(); return OpCount(v); }
+inline OpCount operator+(OpCount a, OpCount b) { return opc(a.v + b.v); }
+inline OpCount operator-(OpCount a, OpCount b) { return opc(a.v - b.v); }
+inline OpCount operator-(OpCount a) { return OpCount(-a.v); }
+inline OpCount operator*(OpCount a, OpCount b) { return opc(a.v * b.v); }
+inline OpCount operator/(OpCount a, OpCount b) { return opc(a.v / b.v); }
+inline OpCount operator+(OpCount a, double b) { return opc(a.v + b); }
+inline OpCount operator+(double a, OpCount b) { return opc(a + b.v); }
+inline OpCount operator-(OpCount a, double b) { return opc(a.v - b); }
+inline OpCount operator-(double a, OpCount b) { return opc(a - b.v); }
+inline OpCount operator*(OpCount a, double b) { return opc(a.v * b); }
+inline OpCount operator*(double a, OpCount b) { return opc(a * b.v); }
+inline OpCount operator/(OpCount a, double b) { return opc(a.v / b); }
+inline OpCount operator/(double a, OpCount b) { return opc(a / b.v); }
+inline OpCount& operator+=(OpCount& a, OpCount b) { a = a + b; return a; }
+inline OpCount& operator-=(OpCount& a, OpCount b) { a = a - b; return a; }
+inline OpCount sqrt(OpCount a) { return opc(std::sqrt(a.v)); }
+inline OpCount pow(OpCount a, double e) { return opc(std::pow(a.v, e)); }
+inline double value(OpCount a) { return a.v; }
+
 template <class T>
 inline void full_convec_ijk_t(const ElemCtx& ctx, const T* u, const T* q, const T* rho,
                             const T* pr, const T* E, T* Rmass, T* Rmom,

@@ -129,3 +129,14 @@ def test_rk4_mass_conservation(oracle):
     oracle.rk4(om, prm, s, dt, nsteps=1)
     assert abs((om.Ml * s.rho).sum() - m0) < 1e-12 * m0
     assert s.mu_e.max() > 0.0
+
+
+def test_rhs_operation_count_constant(oracle):
+    """bench.py's RHS_OPS_PER_ELEMENT is the oracle's count of the reference formulation."""
+    import bench
+    for n in (2, 3):
+        m = M.periodic_box(n, jitter=0.05, seed=1)
+        om = oracle.OracleMesh(m)
+        prm = M.TGVParams()
+        st = M.taylor_green_state(m, prm)
+        assert oracle.rhs_opcount(om, prm, st) == bench.RHS_OPS_PER_ELEMENT * m.nelem
