@@ -254,3 +254,53 @@ def rhs_jvp(om: OracleMesh, prm, st, drho, dq, dE, mu_e=None):
                          ptr(np.asfortranarray(st.q)), ptr(st.E), ptr(np.ascontiguousarray(drho)),
                          ptr(np.asfortranarray(dq)), ptr(np.ascontiguousarray(dE)), ptr(R), ptr(dR))
     return R.reshape(5, om.npoin), dR.reshape(5, om.npoin)
+
+
+# ---- legacy unit-test API (generic gpcar-based element loops; 1-based connec) -------------------
+def _legacy_args(connec, Ngp, gpcar, gpvol):
+    connec = np.asfortranarray(connec, dtype=np.int32)
+    nelem, nnode = connec.shape
+    Ngp = np.asfortranarray(Ngp, dtype=np.float64)
+    gpcar = np.asfortranarray(gpcar, dtype=np.float64)
+    gpvol = np.asfortranarray(gpvol, dtype=np.float64)
+    ndime, _, ngaus, _ = gpcar.shape
+    return nelem, ngaus, nnode, ndime, connec, Ngp, gpcar, gpvol
+
+
+def legacy_mass_convec(connec, Ngp, gpcar, gpvol, q):
+    """mass_convec / generic_scalar_convec: R_a = sum_g gpvol N_a div q (q: (npoin, ndime))."""
+    nelem, ngaus, nnode, ndime, connec, Ngp, gpcar, gpvol = _legacy_args(connec, Ngp, gpcar, gpvol)
+    q = np.asfortranarray(q, dtype=np.float64)
+    R = np.zeros(q.shape[0])
+    lib().oracle_legacy_mass_convec(nelem, ngaus, q.shape[0], nnode, ndime, ptr(connec), ptr(Ngp), ptr(gpcar),
+                                    ptr(gpvol), ptr(q), ptr(R))
+    return R
+
+
+def legacy_mom_convec(connec, Ngp, gpcar, gpvol, u, q, pr):
+    nelem, ngaus, nnode, ndime, connec, Ngp, gpcar, gpvol = _legacy_args(connec, Ngp, gpcar, gpvol)
+    u = np.asfortranarray(u, dtype=np.float64); q = np.asfortranarray(q, dtype=np.float64)
+    pr = np.ascontiguousarray(pr, dtype=np.float64)
+    R = np.zeros(u.shape, order="F")
+    lib().oracle_legacy_mom_convec(nelem, ngaus, u.shape[0], nnode, ndime, ptr(connec), ptr(Ngp), ptr(gpcar),
+                                   ptr(gpvol), ptr(u), ptr(q), ptr(pr), ptr(R))
+    return R
+
+
+def legacy_ener_convec(connec, Ngp, gpcar, gpvol, u, pr, E):
+    nelem, ngaus, nnode, ndime, connec, Ngp, gpcar, gpvol = _legacy_args(connec, Ngp, gpcar, gpvol)
+    u = np.asfortranarray(u, dtype=np.float64)
+    pr = np.ascontiguousarray(pr, dtype=np.float64); E = np.ascontiguousarray(E, dtype=np.float64)
+    R = np.zeros(u.shape[0])
+    lib().oracle_legacy_ener_convec(nelem, ngaus, u.shape[0], nnode, ndime, ptr(connec), ptr(Ngp), ptr(gpcar),
+                                    ptr(gpvol), ptr(u), ptr(pr), ptr(E), ptr(R))
+    return R
+
+
+def legacy_mom_diffusion(connec, Ngp, gpcar, gpvol, u, mu_e):
+    nelem, ngaus, nnode, ndime, connec, Ngp, gpcar, gpvol = _legacy_args(connec, Ngp, gpcar, gpvol)
+    u = np.asfortranarray(u, dtype=np.float64); mu_e = np.ascontiguousarray(mu_e, dtype=np.float64)
+    R = np.zeros(u.shape, order="F")
+    lib().oracle_legacy_mom_diffusion(nelem, ngaus, u.shape[0], nnode, ndime, ptr(connec), ptr(Ngp), ptr(gpcar),
+                                      ptr(gpvol), ptr(u), ptr(mu_e), ptr(R))
+    return R

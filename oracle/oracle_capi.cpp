@@ -178,3 +178,29 @@ double oracle_rhs_opcount(const ElemCtx* ctx, const Params* P, const double* Ml,
 }
 
 }  // extern "C"
+
+extern "C" {
+
+// Legacy unit-test API (1-based connec, Fortran layouts): see legacy_convec / legacy_mom_diffusion.
+void oracle_legacy_mass_convec(int nelem, int ngaus, int npoin, int nnode, int ndime, const int* connec,
+                               const double* Ngp, const double* gpcar, const double* gpvol, const double* q, double* R) {
+  legacy_convec({nelem, ngaus, npoin, nnode, ndime}, connec, Ngp, gpcar, gpvol, 0, q, nullptr, nullptr, R);
+}
+void oracle_legacy_mom_convec(int nelem, int ngaus, int npoin, int nnode, int ndime, const int* connec,
+                              const double* Ngp, const double* gpcar, const double* gpvol, const double* u,
+                              const double* q, const double* pr, double* R) {
+  legacy_convec({nelem, ngaus, npoin, nnode, ndime}, connec, Ngp, gpcar, gpvol, 1, q, u, pr, R);
+}
+void oracle_legacy_ener_convec(int nelem, int ngaus, int npoin, int nnode, int ndime, const int* connec,
+                               const double* Ngp, const double* gpcar, const double* gpvol, const double* u,
+                               const double* pr, const double* E, double* R) {
+  legacy_convec({nelem, ngaus, npoin, nnode, ndime}, connec, Ngp, gpcar, gpvol, 2, u, E, pr, R);
+}
+void oracle_legacy_mom_diffusion(int nelem, int ngaus, int npoin, int nnode, int ndime, const int* connec,
+                                 const double* Ngp, const double* gpcar, const double* gpvol, const double* u,
+                                 const double* mu_e, double* R) {
+  (void)Ngp;
+  legacy_mom_diffusion({nelem, ngaus, npoin, nnode, ndime}, connec, gpcar, gpvol, u, mu_e, R);
+}
+
+}  // extern "C"

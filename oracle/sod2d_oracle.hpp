@@ -1382,4 +1382,98 @@ inline int conjGrad_pressure(const ElemCtx& ctx, const double* dNgp, const doubl
   return iter > maxIter ? maxIter : iter;
 }
 
+// ---------------------------------------------------------------------------------------------
+// Legacy unit-test API (generic gpcar-based element loops).  The routines mass_convec,
+// mom_convec, ener_convec, generic_scalar_convec and mom_diffusion are called by
+// unitt/unitt_{mass,mom,ener,generic_scalar}_convec/*.f90 and unitt/unitt_mom_diffu/*.f90 but
+// are no longer in src/; their arithmetic is given by the unit tests' companion scripts
+// (unitt/unitt_mass_convec/unitt_mass_convec.m: R_a = sum_g gpvol N_a div q;
+//  unitt/unitt_mom_convec/unitt_mom_convec.m: R_a,i = sum_g gpvol N_a (div(q_i u) + d_i p);
+//  unitt/unitt_ener_convec/unitt_ener_convec.m: flux u (E + p)), with fluxes formed at the
+// nodes and differentiated with gpcar.  mom_diffusion has no script: it is restated in weak
+// form, R_a,i = sum_g gpvol sum_j gpcar(j,a) tau_ij with tau = mu_e(elem) (grad u + grad u^T
+// - 2/3 div u I), the stress of full_diffusion_ijk (elem_diffu.f90:70-140); the unit test pins
+// only sum_a R_a,i = 0.  Layouts are Fortran: connec(nelem,nnode) 1-based, Ngp(ngaus,nnode),
+// gpcar(ndime,nnode,ngaus,nelem), gpvol(1,ngaus,nelem), fields (npoin[,ndime]).
+// ---------------------------------------------------------------------------------------------
+struct LegacyDims {
+  int nelem, ngaus, npoin, nnode, ndime;
+};
+
+// mode 0: div of the nodal vector field f(npoin,ndime) into R(npoin)
+// mode 1: momentum, f = q, g = u, s = pr: R(npoin,ndime)
+// mode 2: energy, flux u (E + p): f = u, g = E, s = pr: R(npoin)
+inline void legacy_convec(const LegacyDims& D, const int* connec, const double* Ngp, const double* gpcar,
+                          const double* gpvol, int mode, const double* f, const double* g, const double* s,
+                          double* R) {
+  const int ne = D.nelem, ng = D.ngaus, np = D.npoin, nn = D.nnode, nd = D.ndime;
+  const int ncomp = mode == 1 ? nd : 1;
+  for (int64_t p = 0; p < (int64_t)np * ncomp; ++p) R[p] = 0.0;
+  std::vector<int> ip(nn);
+  std::vector<double> Re((size_t)nn * ncomp);
+  for (int e = 0; e < ne; ++e) {
+    for (int a = 0; a < nn; ++a) ip[a] = connec[e + (int64_t)ne * a] - 1;
+    std::fill(Re.begin(), Re.end(), 0.0);
+    for (int gp = 0; gp < ng; ++gp) {
+      const double* car = gpcar + (size_t)nd * nn * (gp + (size_t)ng * e);
+      const double vol = gpvol[gp + (size_t)ng * e];
+      double val[3] = {0.0, 0.0, 0.0};
+      for (int c = 0; c < ncomp; ++c) {
+        double acc = 0.0;
+        for (int b = 0; b < nn; ++b) {
+          const int pb = ip[b];
+          if (mode == 0) {
+            for (int d = 0; d < nd; ++d) acc += car[d + nd * b] * f[pb + (int64_t)np * d];
+          } else if (mode == 2) {
+            for (int d = 0; d < nd; ++d) acc += car[d + nd * b] * (f[pb + (int64_t)np * d] * (g[pb] + s[pb]));
+          } else {
+            for (int d = 0; d < nd; ++d)
+              acc += car[d + nd * b] * (f[pb + (int64_t)np * c] * g[pb + (int64_t)np * d]);
+            acc += car[c + nd * b] * s[pb];
+          }
+        }
+        val[c] = acc;
+      }
+      for (int a = 0; a < nn; ++a)
+        for (int c = 0; c < ncomp; ++c) Re[a * ncomp + c] += vol * Ngp[gp + (size_t)ng * a] * val[c];
+    }
+    for (int a = 0; a < nn; ++a)
+      for (int c = 0; c < ncomp; ++c) R[ip[a] + (int64_t)np * c] += Re[a * ncomp + c];
+  }
+}
+
+inline void legacy_mom_diffusion(const LegacyDims& D, const int* connec, const double* gpcar, const double* gpvol,
+                                 const double* u, const double* mu_e, double* R) {
+  const int ne = D.nelem, ng = D.ngaus, np = D.npoin, nn = D.nnode, nd = D.ndime;
+  for (int64_t p = 0; p < (int64_t)np * nd; ++p) R[p] = 0.0;
+  std::vector<int> ip(nn);
+  std::vector<double> Re((size_t)nn * nd);
+  for (int e = 0; e < ne; ++e) {
+    for (int a = 0; a < nn; ++a) ip[a] = connec[e + (int64_t)ne * a] - 1;
+    std::fill(Re.begin(), Re.end(), 0.0);
+    for (int gp = 0; gp < ng; ++gp) {
+      const double* car = gpcar + (size_t)nd * nn * (gp + (size_t)ng * e);
+      const double vol = gpvol[gp + (size_t)ng * e];
+      double gu[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};  // gu[i][j] = d u_i / d x_j
+      for (int b = 0; b < nn; ++b)
+        for (int i = 0; i < nd; ++i)
+          for (int j = 0; j < nd; ++j) gu[i][j] += car[j + nd * b] * u[ip[b] + (int64_t)np * i];
+      double divu = 0.0;
+      for (int i = 0; i < nd; ++i) divu += gu[i][i];
+      double tau[3][3];
+      for (int i = 0; i < nd; ++i)
+        for (int j = 0; j < nd; ++j) tau[i][j] = mu_e[e] * (gu[i][j] + gu[j][i]) - (i == j ? mu_e[e] * (2.0 / 3.0) * divu : 0.0);
+      for (int a = 0; a < nn; ++a)
+        for (int i = 0; i < nd; ++i) {
+          double acc = 0.0;
+          for (int j = 0; j < nd; ++j) acc += car[j + nd * a] * tau[i][j];
+          Re[a * nd + i] += vol * acc;
+        }
+    }
+    for (int a = 0; a < nn; ++a)
+      for (int i = 0; i < nd; ++i) R[ip[a] + (int64_t)np * i] += Re[a * nd + i];
+  }
+}
+
 }  // namespace sod_oracle
+

@@ -140,3 +140,28 @@ def test_rhs_operation_count_constant(oracle):
         prm = M.TGVParams()
         st = M.taylor_green_state(m, prm)
         assert oracle.rhs_opcount(om, prm, st) == bench.RHS_OPS_PER_ELEMENT * m.nelem
+
+
+def _legacy(kats, name):
+    c = kats["legacy_" + name]
+    return c, np.array(c["connec"]), np.array(c["Ngp"]), np.array(c["gpcar"]), np.array(c["gpvol"])
+
+
+@pytest.mark.parametrize("name", ["mass_convec", "generic_scalar_convec", "mom_convec", "ener_convec", "mom_diffu"])
+def test_legacy_unit_tests(oracle, kats, name):
+    """The legacy element-loop tests (unitt/unitt_*_convec, unitt_mom_diffu): the oracle's
+    restatement reproduces the companion .m residual and the tests' own check |sum_a R_a| < 1e-14."""
+    c, connec, Ngp, gpcar, gpvol = _legacy(kats, name)
+    if name in ("mass_convec", "generic_scalar_convec"):
+        R = oracle.legacy_mass_convec(connec, Ngp, gpcar, gpvol, np.array(c["q"]))
+    elif name == "mom_convec":
+        R = oracle.legacy_mom_convec(connec, Ngp, gpcar, gpvol, np.array(c["u"]), np.array(c["q"]), np.array(c["pr"]))
+    elif name == "ener_convec":
+        R = oracle.legacy_ener_convec(connec, Ngp, gpcar, gpvol, np.array(c["u"]), np.array(c["pr"]), np.array(c["E"]))
+    else:
+        R = oracle.legacy_mom_diffusion(connec, Ngp, gpcar, gpvol, np.array(c["u"]), np.array(c["mu_e"]))
+    if "R_expected" in c:
+        assert np.abs(R - np.array(c["R_expected"])).max() < 1e-14
+    sums = np.atleast_1d(R.sum(axis=0))
+    assert np.all(np.abs(sums) < c["sum_tol"]), sums
+    assert np.abs(R).max() > 0.1  # a real residual, not zeros
