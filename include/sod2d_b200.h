@@ -289,6 +289,36 @@ int sod_rk4_step_vjp(SodMesh* mesh, const double* rho, const double* q, const do
 int sod_csr_spmv_scal(int32_t npoin, int32_t nzdom, const int32_t* rdom, const int32_t* cdom,
                       const double* Mc, const double* v, double* u, sod_stream_t stream);
 
+/* Legacy element-loop routines of the unit tests (names and argument lists from their call
+ * sites: unitt/unitt_mass_convec/unitt_mass_convec.f90:151, unitt_mom_convec.f90:151,
+ * unitt_ener_convec.f90:151, unitt_generic_scalar_convec.f90:151, unitt_mom_diffu.f90:148;
+ * the routines themselves are no longer in src/).  Generic elements given by the caller's
+ * tables: connec(nelem,nnode) 1-based, Ngp(ngaus,nnode), gpcar(ndime,nnode,ngaus,nelem),
+ * gpvol(1,ngaus,nelem); ndime 2 or 3, nnode and ngaus <= 64; device arrays.  Residuals
+ * R_a = sum_g gpvol N_a div(flux) with the flux formed at the nodes (the unit tests' .m
+ * scripts): mass/generic q; momentum q_i u + p e_i (R(npoin,ndime)); energy u (E + p).
+ * mom_diffusion: R_a,i = sum_g gpvol sum_j gpcar(j,a) tau_ij, tau = mu_e(elem)(grad u +
+ * grad u^T - 2/3 div u I) (R(npoin,ndime), mu_e(nelem)).  Outputs are overwritten. */
+int sod_legacy_mass_convec(int32_t nelem, int32_t ngaus, int32_t npoin, int32_t nnode, int32_t ndime,
+                           const int32_t* connec, const double* Ngp, const double* gpcar,
+                           const double* gpvol, const double* q, double* R, sod_stream_t stream);
+int sod_legacy_generic_scalar_convec(int32_t nelem, int32_t ngaus, int32_t npoin, int32_t nnode,
+                                     int32_t ndime, const int32_t* connec, const double* Ngp,
+                                     const double* gpcar, const double* gpvol, const double* q,
+                                     double* R, sod_stream_t stream);
+int sod_legacy_mom_convec(int32_t nelem, int32_t ngaus, int32_t npoin, int32_t nnode, int32_t ndime,
+                          const int32_t* connec, const double* Ngp, const double* gpcar,
+                          const double* gpvol, const double* u, const double* q, const double* pr,
+                          double* R, sod_stream_t stream);
+int sod_legacy_ener_convec(int32_t nelem, int32_t ngaus, int32_t npoin, int32_t nnode, int32_t ndime,
+                           const int32_t* connec, const double* Ngp, const double* gpcar,
+                           const double* gpvol, const double* u, const double* pr, const double* E,
+                           double* R, sod_stream_t stream);
+int sod_legacy_mom_diffusion(int32_t nelem, int32_t ngaus, int32_t npoin, int32_t nnode, int32_t ndime,
+                             const int32_t* connec, const double* Ngp, const double* gpcar,
+                             const double* gpvol, const double* u, const double* mu_e, double* R,
+                             sod_stream_t stream);
+
 /* ---- Diagnostics ------------------------------------------------------------------------ */
 const char* sod_last_error(void);
 const char* sod_version(void);

@@ -74,6 +74,11 @@ _SIGS = {
     "sod_csr_spmv_scal": (_i, [C.c_int32, C.c_int32, _p, _p, _p, _p, _p, _p]),
     "sod_rhs_vjp": (_i, [_p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p]),
     "sod_rk4_step_vjp": (_i, [_p] * 15),
+    "sod_legacy_mass_convec": (_i, [_i] * 5 + [_p] * 7),
+    "sod_legacy_generic_scalar_convec": (_i, [_i] * 5 + [_p] * 7),
+    "sod_legacy_mom_convec": (_i, [_i] * 5 + [_p] * 9),
+    "sod_legacy_ener_convec": (_i, [_i] * 5 + [_p] * 9),
+    "sod_legacy_mom_diffusion": (_i, [_i] * 5 + [_p] * 8),
     "sod_rk4_main_record": (_i, [_p, _p, _p, _p, _p, _i, _p]),
     "sod_batch_create": (_i, [_p, _i, _p]),
     "sod_batch_destroy": (None, [_p]),

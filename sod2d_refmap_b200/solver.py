@@ -435,3 +435,40 @@ class Sod2dBatch:
         _lib.check(_lib.load().sod_batch_autotune(self.handle, int(precision), C.byref(best), C.byref(ms),
                                                  _stream(stream)))
         return best.value, ms.value
+
+
+# ---- legacy element-loop API of the unit tests (host numpy in, host numpy out) ----------------
+def _legacy_call(fn_name: str, connec, Ngp, gpcar, gpvol, fields, out_shape):
+    torch = _torch()
+    connec = np.asfortranarray(connec, dtype=np.int32)
+    nelem, nnode = connec.shape
+    gpcar = np.asfortranarray(gpcar, dtype=np.float64)
+    ndime, _, ngaus, _ = gpcar.shape
+    dev = lambda a, dt=np.float64: torch.from_numpy(np.ascontiguousarray(np.asarray(a, dtype=dt).ravel(order="F"))).cuda()
+    args = [dev(connec, np.int32), dev(Ngp), dev(gpcar), dev(gpvol)] + [dev(f) for f in fields]
+    npoin = out_shape[0]
+    R = torch.zeros(int(np.prod(out_shape)), dtype=torch.float64, device="cuda")
+    _lib.check(getattr(_lib.load(), fn_name)(nelem, ngaus, npoin, nnode, ndime,
+                                             *(C.c_void_p(_ptr(t)) for t in args + [R]), _stream(None)))
+    return R.cpu().numpy().reshape(out_shape, order="F")
+
+
+def legacy_mass_convec(connec, Ngp, gpcar, gpvol, q):
+    """mass_convec of the unit tests: R_a = sum_g gpvol N_a div q; q (npoin, ndime)."""
+    return _legacy_call("sod_legacy_mass_convec", connec, Ngp, gpcar, gpvol, [q], (np.shape(q)[0],))
+
+
+def legacy_generic_scalar_convec(connec, Ngp, gpcar, gpvol, q):
+    return _legacy_call("sod_legacy_generic_scalar_convec", connec, Ngp, gpcar, gpvol, [q], (np.shape(q)[0],))
+
+
+def legacy_mom_convec(connec, Ngp, gpcar, gpvol, u, q, pr):
+    return _legacy_call("sod_legacy_mom_convec", connec, Ngp, gpcar, gpvol, [u, q, pr], np.shape(u))
+
+
+def legacy_ener_convec(connec, Ngp, gpcar, gpvol, u, pr, E):
+    return _legacy_call("sod_legacy_ener_convec", connec, Ngp, gpcar, gpvol, [u, pr, E], (np.shape(u)[0],))
+
+
+def legacy_mom_diffusion(connec, Ngp, gpcar, gpvol, u, mu_e):
+    return _legacy_call("sod_legacy_mom_diffusion", connec, Ngp, gpcar, gpvol, [u, mu_e], np.shape(u))
