@@ -67,6 +67,7 @@ struct DevParams {
   double gamma, Rgas, Cp, Prt, ce, cmax, cglob, c_rho, c_ener, cfl_conv, cfl_diff;
   int normalise;
   double g_gm1, inv_gm1, inv_Rgas;  // gamma/(gamma-1), 1/(gamma-1), 1/Rgas (host-computed)
+  double CpPr, Cp09;                 // Cp/Prt, Cp/0.9 (host-computed)
   // FP32 copies for the mixed kernels (host-converted: FP64->FP32 conversions are slow on the GPU)
   float gamma_f, c_rho_f, c_ener_f, CpPr_f, Cp09_f;  // gamma, c_rho, c_ener, Cp/Prt, Cp/0.9
 };

@@ -242,6 +242,8 @@ static void to_dev_params(const SodParams* s, DevParams* d) {
   d->g_gm1 = s->gamma_gas / (s->gamma_gas - 1.0);
   d->inv_gm1 = 1.0 / (s->gamma_gas - 1.0);
   d->inv_Rgas = 1.0 / s->Rgas;
+  d->CpPr = s->Cp / s->Prt;
+  d->Cp09 = s->Cp / 0.9;
   d->gamma_f = (float)s->gamma_gas;
   d->c_rho_f = (float)s->c_rho;
   d->c_ener_f = (float)s->c_ener;

@@ -122,13 +122,15 @@ __global__ void __launch_bounds__(64 * EPB) k_rhs_fused(const RhsArgs a) {
   const double rho = a.rho[n];
   const double qv[3] = {a.q0[n], a.q1[n], a.q2[n]};
   const double Et = a.E[n];
-  const double uv[3] = {qv[0] / rho, qv[1] / rho, qv[2] / rho};
+  // one reciprocal serves the divisions by rho; gamma/(gamma-1) and 1/Rgas come from the host
+  const double irho = 1.0 / rho;
+  const double uv[3] = {qv[0] * irho, qv[1] * irho, qv[2] * irho};
   const double umag = uv[0] * uv[0] + uv[1] * uv[1] + uv[2] * uv[2];
   const double kk = 0.5 * umag;
-  const double e_int = (Et / rho) - 0.5 * umag;
+  const double e_int = Et * irho - 0.5 * umag;
   const double p = rho * (g - 1.0) * e_int;
-  const double h = (g / (g - 1.0)) * p / rho;
-  const double T = p / (rho * a.prm.Rgas);
+  const double h = a.prm.g_gm1 * p * irho;
+  const double T = p * irho * a.prm.inv_Rgas;
   const double mufac = a.mu_factor[n];
   const R mue = reinterpret_cast<const R*>(a.mue)[(size_t)ee * NN + d];
   const double musgs = a.musgs ? a.musgs[(size_t)ee * NN + d] : 0.0;
@@ -362,9 +364,8 @@ __global__ void __launch_bounds__(64 * EPB) k_rhs_fused(const RhsArgs a) {
   for (int v = 0; v < 6; ++v)
     dv[v] = divT(p2 + (v * 3 + 0) * FSTRIDE, p2 + (v * 3 + 1) * FSTRIDE, p2 + (v * 3 + 2) * FSTRIDE, i, j, k, DTx,
                  DTy, DTz);
-  const R nu_e = (R)a.prm.c_rho * mue / rhoR;
-  const R kappa_e = (R)(muf * a.prm.Cp / a.prm.Prt) + (R)a.prm.c_ener * mue * (R)(a.prm.Cp / a.prm.Prt) +
-                    (R)(a.prm.Cp * rho * musgs / 0.9);
+  const R nu_e = (R)a.prm.c_rho * mue * (R)irho;
+  const R kappa_e = (R)(muf * a.prm.CpPr) + (R)a.prm.c_ener * mue * (R)a.prm.CpPr + (R)(a.prm.Cp09 * rho * musgs);
   if (active) {
     store_res6<R>(reinterpret_cast<R*>(a.rel), (size_t)e * NN + d, gpv * Rm + nu_e * dv[0], gpv * Rmo[0] + dv[3],
                   gpv * Rmo[1] + dv[4], gpv * Rmo[2] + dv[5], gpv * Ren + (dv[1] + kappa_e * dv[2]), gpv * Ret);
