@@ -504,6 +504,19 @@ def run_ours(args):
             clocks = cs.summary()
     # accuracy of the mixed path against the FP64 path after K steps (same start, same dt0)
     acc = {k: _rel_l2(getattr(states["mixed"], k), getattr(states["fp64"], k)) for k in ("rho", "q", "E")}
+    # TGV diagnostics (volAvg_EK, visc_dissipationRate) of both states after the K steps
+    diag = {}
+    for name in ("fp64", "mixed"):
+        diag[name] = gm.tgv_diagnostics(states[name], prm.rho0)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(10):
+        gm.tgv_diagnostics(states["mixed"], prm.rho0)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    diag["ms_per_call"] = e0.elapsed_time(e1) / 10
+    diag["mixed_rel_diff"] = {k: abs(diag["mixed"][k] - diag["fp64"][k]) / abs(diag["fp64"][k])
+                              for k in ("EK", "eps_S", "eps_T")}
     s = fresh()
     r64 = gm.rhs(s, precision=S.FP64)
     r32 = gm.rhs(s, precision=S.MIXED)
@@ -592,6 +605,7 @@ def run_ours(args):
                 "fp64": {"value": value64, "ms_per_step": results["fp64"]["ms"] / K, "dtype": "f64",
                          "speedup_mixed_over_fp64": value / value64},
                 "mixed_rel_l2_vs_fp64": {"state_after_steps": acc, "rhs_stage": acc_rhs},
+                "tgv_diagnostics_after_steps": diag,
                 "gpu_launches": results["mixed"]["launches"],
                 "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks, "pressure_cg": cg,
                 "ensemble": batch, "adjoint": adjoint}

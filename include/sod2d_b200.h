@@ -257,6 +257,16 @@ int sod_poisson_diag(SodPoisson* P, double* d, sod_stream_t stream);
 int sod_conjgrad_pressure(SodPoisson* P, const double* Rp0, double* R, int max_iter, double tol,
                           int mixed, int* iters, double* final_rel, sod_stream_t stream);
 
+/* ---- Taylor-Green diagnostics ------------------------------------------------------------ */
+/* volAvg_EK and visc_dissipationRate (mod_analysis.f90:10-144), as the time loop calls them
+ * (CFDSolverBase.f90:1413-1414): u(npoin,3), rho, mu_fluid (npoin), mu_e(nelem,64) device
+ * arrays; rho0 = nscbc_rho_inf, volT = the domain volume (<= 0: the sum of gpvol, as the
+ * reference's VolTot, CFDSolverBase.f90:1300-1312); out_dev (device, 5 doubles) receives EK,
+ * eps_S, eps_D, eps_T and the volume used.  Sums are in a fixed order (deterministic). */
+int sod_tgv_diagnostics(SodMesh* mesh, const double* rho, const double* u, const double* mu_fluid,
+                        const double* mu_e, double rho0, double volT, double* out_dev,
+                        sod_stream_t stream);
+
 /* ---- Adjoint (reverse mode) of the RHS and of one RK4 step ------------------------------ */
 /* No counterpart in the reference (SOD2D has no adjoint); these differentiate the FP64 path of
  * sod_rhs / sod_rk4_main with the entropy viscosity mu_e (and dt) frozen at the given values,

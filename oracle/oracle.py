@@ -304,3 +304,18 @@ def legacy_mom_diffusion(connec, Ngp, gpcar, gpvol, u, mu_e):
     lib().oracle_legacy_mom_diffusion(nelem, ngaus, u.shape[0], nnode, ndime, ptr(connec), ptr(Ngp), ptr(gpcar),
                                       ptr(gpvol), ptr(u), ptr(mu_e), ptr(R))
     return R
+
+
+def tgv_diagnostics(om: OracleMesh, tables, rho0: float, st, volT: float, mu_e=None):
+    """(EK, eps_S, eps_D, eps_T) of volAvg_EK and visc_dissipationRate (mod_analysis.f90:10-144)."""
+    L = lib()
+    L.oracle_volavg_ek.restype = C.c_double
+    Ngp = np.asfortranarray(tables.Ngp)
+    dNgp = np.asfortranarray(tables.dNgp)
+    u = np.asfortranarray(st.u)
+    ek = L.oracle_volavg_ek(C.byref(om.ctx), ptr(Ngp), C.c_double(rho0), ptr(st.rho), ptr(u))
+    eps = np.zeros(3)
+    mue = np.asfortranarray(st.mu_e if mu_e is None else mu_e)
+    L.oracle_visc_dissipation_rate(C.byref(om.ctx), ptr(dNgp), C.c_double(rho0), ptr(st.mu_fluid), ptr(mue), ptr(u),
+                                   C.c_double(volT), ptr(eps))
+    return float(ek), float(eps[0]), float(eps[1]), float(eps[2])

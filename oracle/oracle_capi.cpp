@@ -204,3 +204,15 @@ void oracle_legacy_mom_diffusion(int nelem, int ngaus, int npoin, int nnode, int
 }
 
 }  // extern "C"
+
+extern "C" {
+
+double oracle_volavg_ek(const ElemCtx* ctx, const double* Ngp, double rho0, const double* rho, const double* u) {
+  return volAvg_EK(*ctx, Ngp, rho0, rho, u);
+}
+void oracle_visc_dissipation_rate(const ElemCtx* ctx, const double* dNgp, double rho0, const double* mu_fluid,
+                                  const double* mu_e, const double* u, double volT, double* eps3) {
+  visc_dissipationRate(*ctx, dNgp, rho0, mu_fluid, mu_e, u, volT, eps3);
+}
+
+}  // extern "C"

@@ -1475,5 +1475,76 @@ inline void legacy_mom_diffusion(const LegacyDims& D, const int* connec, const d
   }
 }
 
+// volAvg_EK (mod_analysis.f90:10-44): EK = sum_e sum_g sum_a gpvol Ngp(g,a) 1/2 rho_a |u_a|^2
+// / (rho0 (2*3.14159)^3), element sums first (rp), then the real(8) total.
+inline double volAvg_EK(const ElemCtx& ctx, const double* Ngp, double rho0, const double* rho, const double* u) {
+  const int ne = ctx.nelem, np = ctx.npoin;
+  double EK_l = 0.0;
+  for (int e = 0; e < ne; ++e) {
+    double R1 = 0.0;
+    for (int g = 0; g < ngaus; ++g)
+      for (int a = 0; a < nnode; ++a) {
+        const int p = ctx.connec[e + (int64_t)ne * a];
+        double uu = 0.0;
+        for (int d = 0; d < ndime; ++d) uu += u[p + (int64_t)np * d] * u[p + (int64_t)np * d];
+        R1 = R1 + ctx.gpvol[g + (int64_t)ngaus * e] * Ngp[g + ngaus * a] * 0.5 * rho[p] * uu;
+      }
+    EK_l += R1;
+  }
+  return EK_l / (rho0 * std::pow(2.0 * 3.14159, 3.0));
+}
+
+// visc_dissipationRate (mod_analysis.f90:46-144): gpcar = He dNgp, gradU(j,k) = d_j u_k,
+// eps_S = sum gpvol (mu_fluid + mu_e) |curl u|^2 / (rho0 volT), eps_D = 4/3 sum gpvol mu_fluid
+// (div u)^2 / (rho0 volT), eps_T = eps_S + eps_D.
+inline void visc_dissipationRate(const ElemCtx& ctx, const double* dNgp, double rho0, const double* mu_fluid,
+                                 const double* mu_e, const double* u, double volT, double* eps3) {
+  static const double lc[3][3][3] = {{{0, 0, 0}, {0, 0, 1}, {0, -1, 0}},
+                                     {{0, 0, -1}, {0, 0, 0}, {1, 0, 0}},
+                                     {{0, 1, 0}, {-1, 0, 0}, {0, 0, 0}}};  // leviCivi(i,j,k)
+  const int ne = ctx.nelem, np = ctx.npoin;
+  double eS = 0.0, eD = 0.0;
+  for (int e = 0; e < ne; ++e) {
+    double R1 = 0.0, R2 = 0.0;
+    for (int g = 0; g < ngaus; ++g) {
+      double gpcar[3][nnode];
+      for (int i = 0; i < ndime; ++i)
+        for (int a = 0; a < nnode; ++a) {
+          double acc = 0.0;
+          for (int k = 0; k < ndime; ++k)
+            acc += ctx.He[i + 3 * (k + 3 * (g + (int64_t)ngaus * e))] * dNgp[k + ndime * (a + nnode * g)];
+          gpcar[i][a] = acc;
+        }
+      double gU[3][3];
+      for (int jd = 0; jd < ndime; ++jd)
+        for (int kd = 0; kd < ndime; ++kd) {
+          double aux = 0.0;
+          for (int a = 0; a < nnode; ++a) aux += gpcar[jd][a] * u[ctx.connec[e + (int64_t)ne * a] + (int64_t)np * kd];
+          gU[jd][kd] = aux;
+        }
+      double div2 = gU[0][0] + gU[1][1] + gU[2][2];
+      div2 = div2 * div2;
+      double curl2 = 0.0;
+      for (int i = 0; i < 3; ++i) {
+        double a2 = 0.0;
+        for (int jd = 0; jd < 3; ++jd)
+          for (int kd = 0; kd < 3; ++kd) a2 += lc[i][jd][kd] * gU[jd][kd];
+        curl2 += a2 * a2;
+      }
+      const int pg = ctx.connec[e + (int64_t)ne * g];
+      const double vol = ctx.gpvol[g + (int64_t)ngaus * e];
+      R1 += vol * (mu_fluid[pg] + mu_e[e + (int64_t)ne * g]) * curl2;
+      R2 += vol * mu_fluid[pg] * div2;
+    }
+    eS += R1;
+    eD += R2;
+  }
+  const double alpha = 1.0 / (rho0 * volT);
+  eps3[0] = eS * alpha;
+  eps3[1] = (4.0 / 3.0) * eD * alpha;
+  eps3[2] = eps3[0] + eps3[1];
+}
+
 }  // namespace sod_oracle
+
 

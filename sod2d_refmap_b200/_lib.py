@@ -74,6 +74,7 @@ _SIGS = {
     "sod_csr_spmv_scal": (_i, [C.c_int32, C.c_int32, _p, _p, _p, _p, _p, _p]),
     "sod_rhs_vjp": (_i, [_p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p]),
     "sod_rk4_step_vjp": (_i, [_p] * 15),
+    "sod_tgv_diagnostics": (_i, [_p, _p, _p, _p, _p, _d, _d, _p, _p]),
     "sod_legacy_mass_convec": (_i, [_i] * 5 + [_p] * 7),
     "sod_legacy_generic_scalar_convec": (_i, [_i] * 5 + [_p] * 7),
     "sod_legacy_mom_convec": (_i, [_i] * 5 + [_p] * 9),

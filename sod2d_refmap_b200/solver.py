@@ -214,6 +214,17 @@ class Sod2dMesh:
             out["Reta"])), int(precision), _stream(stream)))
         return out
 
+    def tgv_diagnostics(self, state: Sod2dState, rho0: float, volT: float = 0.0, stream=None) -> dict:
+        """volAvg_EK / visc_dissipationRate of the state: EK, eps_S, eps_D, eps_T (volT <= 0:
+        the summed gpvol)."""
+        torch = _torch()
+        out = torch.zeros(5, dtype=torch.float64, device="cuda")
+        _lib.check(_lib.load().sod_tgv_diagnostics(self.handle, *(C.c_void_p(_ptr(t)) for t in (
+            state.rho, state.u, state.mu_fluid, state.mu_e)), C.c_double(rho0), C.c_double(volT),
+            C.c_void_p(_ptr(out)), _stream(stream)))
+        v = out.cpu().tolist()
+        return {"EK": v[0], "eps_S": v[1], "eps_D": v[2], "eps_T": v[3], "volT": v[4]}
+
     # ---- adjoint (reverse mode, FP64, mu_e and dt frozen) --------------------------------
     def rhs_vjp(self, rho, q, E, mu_e, mu_factor, bar_Rmass, bar_Rmom, bar_Rener, stream=None):
         """(dR/d(rho,q,E))^T (bar_Rmass, bar_Rmom, bar_Rener) for the FP64 stage RHS of rhs()."""

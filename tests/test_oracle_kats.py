@@ -165,3 +165,15 @@ def test_legacy_unit_tests(oracle, kats, name):
     sums = np.atleast_1d(R.sum(axis=0))
     assert np.all(np.abs(sums) < c["sum_tol"]), sums
     assert np.abs(R).max() > 0.1  # a real residual, not zeros
+
+
+def test_oracle_tgv_initial_kinetic_energy(oracle):
+    """volAvg_EK of the TGV initial state (V0 = 1): mean 1/2 |u|^2 = 1/8 up to the reference's
+    3.14159, rho = 1 + O(Ma^2) and the 1e-3 perturbation."""
+    m = M.periodic_box(4, jitter=0.0, seed=0)
+    om = oracle.OracleMesh(m)
+    prm = M.TGVParams()
+    st = M.taylor_green_state(m, prm)
+    ek, eS, eD, eT = oracle.tgv_diagnostics(om, m.tables, 1.0, st, float(om.gpvol.sum()))
+    assert abs(ek - 0.125) < 2e-3
+    assert eS > 0 and eD >= 0 and abs(eT - (eS + eD)) < 1e-15 * eT
