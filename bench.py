@@ -536,6 +536,7 @@ def run_ours(args):
             h.copy_(t_)
             host[f] = h.numpy()
         host["Reta"] = None
+        host["mu_sgs"] = None  # no LES in this case
         n_e2e = max(3, min(K, 10))
         gm.rk4_main_host(host, dt0, precision=S.MIXED)
         torch.cuda.synchronize(); barrier(); torch.cuda.synchronize()

@@ -58,6 +58,8 @@ typedef struct {
   double c_rho, c_ener;         /* mod_numerical_params.f90:27-28                         */
   int32_t flag_normalise_entropy; /* mod_numerical_params.f90:23                          */
   double cfl_conv, cfl_diff;    /* CFDSolverBase cfl_conv / cfl_diff                      */
+  int32_t flag_les;             /* 1: Vreman sgs_visc after each step (time_integ.f90:498-506) */
+  double c_sgs;                 /* mod_numerical_params.f90:15 (0.025)                    */
 } SodParams;
 
 void sod_params_default(SodParams* p);
@@ -119,6 +121,8 @@ typedef struct {
   double* mu_factor;/* (npoin)    input */
   double* mu_e;     /* (nelem,64) in: frozen entropy viscosity; out: updated */
   double* Reta;     /* (npoin)    out: -sum b_i Reta_i (time_integ.f90:467-471), may be null */
+  double* mu_sgs;   /* (nelem,64) LES: in the step's frozen SGS viscosity, out updated by
+                       sgs_visc (mod_sgs_viscosity.f90:13-125); null = no SGS (flag_les off) */
 } SodState;
 
 /* One explicit RK4 step: rk_4_main (time_integ.f90:137-508) on the periodic compressible

@@ -28,7 +28,7 @@ class Params(C.Structure):
     _fields_ = [("gamma_gas", C.c_double), ("Rgas", C.c_double), ("Cp", C.c_double), ("Prt", C.c_double),
                 ("ce", C.c_double), ("cmax", C.c_double), ("cglob", C.c_double), ("c_rho", C.c_double),
                 ("c_ener", C.c_double), ("flag_normalise_entropy", C.c_int), ("cfl_conv", C.c_double),
-                ("cfl_diff", C.c_double)]
+                ("cfl_diff", C.c_double), ("flag_les", C.c_int), ("c_sgs", C.c_double)]
 
 
 class State(C.Structure):
@@ -138,7 +138,8 @@ class OracleMesh:
 
 def params_of(prm) -> Params:
     return Params(prm.gamma_gas, prm.Rgas, prm.Cp, prm.Prt, prm.ce, prm.cmax, prm.cglob, prm.c_rho,
-                  prm.c_ener, int(prm.flag_normalise_entropy), prm.cfl_conv, prm.cfl_diff)
+                  prm.c_ener, int(prm.flag_normalise_entropy), prm.cfl_conv, prm.cfl_diff,
+                  int(getattr(prm, "flag_les", 0)), float(getattr(prm, "c_sgs", 0.025)))
 
 
 def adapt_dt(om: OracleMesh, st, prm) -> float:

@@ -43,6 +43,8 @@ struct Params {
   double ce, cmax, cglob, c_rho, c_ener;  // mod_numerical_params.f90:24-28
   int flag_normalise_entropy;             // mod_numerical_params.f90:23
   double cfl_conv, cfl_diff;
+  int flag_les;                           // LES (Vreman sgs_visc) after each step (time_integ.f90:498-506)
+  double c_sgs;                           // mod_numerical_params.f90:15
 };
 
 // ------------------------------------------------------------------------------------------
@@ -1156,6 +1158,62 @@ struct StageCapture {
   int stage;      // 1..4
 };
 
+// sgs_visc (mod_sgs_viscosity.f90:13-125): Vreman eddy viscosity per gauss point from the
+// velocity gradient, hLES = gpvol^(1/3), mue_l = c_sgs sqrt(max(B,1e-10)/alpha) where alpha =
+// |grad u|^2 > 1e-10 (otherwise the previous mu_sgs is kept), then the same 3x3x3 convertIJK
+// filter as smart_visc_spectral.  mu_sgs and mue_l are (nelem,ngaus).
+inline void sgs_visc(const ElemCtx& ctx, const Params& P, const double* u, double* mu_sgs, double* mue_l) {
+  const int nelem = ctx.nelem, npoin = ctx.npoin;
+  for (int64_t q = 0; q < (int64_t)nelem * nnode; ++q) mue_l[q] = mu_sgs[q];
+  int convertIJK[porder + 3];
+  for (int ii = 3; ii <= porder + 1; ++ii) convertIJK[ii - 1] = ii;
+  convertIJK[0] = 3; convertIJK[1] = 1; convertIJK[porder + 1] = 2; convertIJK[porder + 2] = porder;
+  const double wts[3] = {0.25, 0.5, 0.25};
+#pragma omp parallel for schedule(static)
+  for (int ielem = 0; ielem < nelem; ++ielem) {
+    double ul[nnode][3];
+    for (int a = 0; a < nnode; ++a)
+      for (int d = 0; d < 3; ++d) ul[a][d] = u[ctx.connec[ielem + (int64_t)nelem * a] + (int64_t)npoin * d];
+    for (int igaus = 0; igaus < ngaus; ++igaus) {
+      const double hLES = std::pow(SOD_GPVOL(igaus, ielem), 1.0 / 3.0);
+      const int isoI = ctx.gmshAtoI[igaus], isoJ = ctx.gmshAtoJ[igaus], isoK = ctx.gmshAtoK[igaus];
+      double gIU[3][3] = {};
+      for (int ii = 0; ii < 4; ++ii)
+        for (int id = 0; id < 3; ++id) {
+          gIU[id][0] += SOD_DL(igaus, 0, ii) * ul[SOD_INV(ii, isoJ, isoK)][id];
+          gIU[id][1] += SOD_DL(igaus, 1, ii) * ul[SOD_INV(isoI, ii, isoK)][id];
+          gIU[id][2] += SOD_DL(igaus, 2, ii) * ul[SOD_INV(isoI, isoJ, ii)][id];
+        }
+      double gU[3][3] = {};
+      for (int id = 0; id < 3; ++id)
+        for (int jd = 0; jd < 3; ++jd)
+          for (int kd = 0; kd < 3; ++kd) gU[id][jd] += SOD_HE(jd, kd, igaus, ielem) * gIU[id][kd];
+      double alpha = 0.0, V[3][3] = {};
+      for (int id = 0; id < 3; ++id)
+        for (int jd = 0; jd < 3; ++jd) {
+          for (int kd = 0; kd < 3; ++kd) V[id][jd] += gU[kd][id] * gU[kd][jd] * hLES * hLES;
+          alpha += gU[id][jd] * gU[id][jd];
+        }
+      const double B = V[0][0] * V[1][1] + V[0][0] * V[2][2] + V[1][1] * V[2][2] - V[0][1] * V[0][1] -
+                       V[0][2] * V[0][2] - V[1][2] * V[1][2];
+      if (alpha > 1.0e-10) mue_l[ielem + (int64_t)nelem * igaus] = P.c_sgs * std::sqrt(std::max(B, 1.0e-10) / alpha);
+    }
+    for (int ii = 1; ii <= porder + 1; ++ii)
+      for (int jj = 1; jj <= porder + 1; ++jj)
+        for (int kk = 1; kk <= porder + 1; ++kk) {
+          double aux1 = 0.0;
+          for (int ll = -1; ll <= 1; ++ll)
+            for (int mm = -1; mm <= 1; ++mm)
+              for (int nn = -1; nn <= 1; ++nn) {
+                int a = SOD_INV(convertIJK[ii + ll] - 1, convertIJK[jj + mm] - 1, convertIJK[kk + nn] - 1);
+                aux1 = aux1 + wts[ll + 1] * wts[mm + 1] * wts[nn + 1] * mue_l[ielem + (int64_t)nelem * a];
+              }
+          int a = SOD_INV(convertIJK[ii] - 1, convertIJK[jj] - 1, convertIJK[kk] - 1);
+          mu_sgs[ielem + (int64_t)nelem * a] = aux1;
+        }
+  }
+}
+
 inline void rk_4_main(const ElemCtx& ctx, const Params& P, const double* Ml, const double* mu_factor,
                       const double* gpvol, const double* wgp, const double* helem, const double* helem_l,
                       double dt, State& S, Rk4Scratch& W, StageCapture* cap) {
@@ -1255,6 +1313,7 @@ inline void rk_4_main(const ElemCtx& ctx, const Params& P, const double* Ml, con
   sutherland_viscosity(npoin, S.Tem, mu_factor, S.mu_fluid);
   smart_visc_spectral(ctx, P, W.Reta.data(), gpvol, wgp, S.rho, S.u, S.csound, S.Tem, S.eta, helem_l, helem,
                       S.mu_e, S.mue_l);
+  if (P.flag_les == 1) sgs_visc(ctx, P, S.u, S.mu_sgs, S.mue_l);  // time_integ.f90:498-506
 }
 
 #undef SOD_INV

@@ -31,7 +31,7 @@ class SodError(RuntimeError):
 class SodParams(C.Structure):
     _fields_ = [("gamma_gas", _d), ("Rgas", _d), ("Cp", _d), ("Prt", _d), ("ce", _d), ("cmax", _d), ("cglob", _d),
                 ("c_rho", _d), ("c_ener", _d), ("flag_normalise_entropy", C.c_int32), ("cfl_conv", _d),
-                ("cfl_diff", _d)]
+                ("cfl_diff", _d), ("flag_les", C.c_int32), ("c_sgs", _d)]
 
 
 class SodMeshDesc(C.Structure):
@@ -43,7 +43,7 @@ class SodMeshDesc(C.Structure):
 
 class SodState(C.Structure):
     _fields_ = [(n, _p) for n in ("rho", "q", "E", "u", "pr", "Tem", "e_int", "eta", "csound", "machno",
-                                  "mu_fluid", "mu_factor", "mu_e", "Reta")]
+                                  "mu_fluid", "mu_factor", "mu_e", "Reta", "mu_sgs")]
 
 
 _SIGS = {

@@ -70,6 +70,8 @@ struct DevParams {
   double CpPr, Cp09;                 // Cp/Prt, Cp/0.9 (host-computed)
   // FP32 copies for the mixed kernels (host-converted: FP64->FP32 conversions are slow on the GPU)
   float gamma_f, c_rho_f, c_ener_f, CpPr_f, Cp09_f;  // gamma, c_rho, c_ener, Cp/Prt, Cp/0.9
+  int flag_les;
+  double c_sgs;
 };
 
 // 1-D derivative matrix in natural order: D[m][n] = l_n'(x_m)
@@ -171,6 +173,7 @@ struct SodMesh {
   int32_t* member_node_off = nullptr;  // [nmember+1] contiguous node ranges
   double* member_scal = nullptr;    // [nmember][2] eta mean, eta norm
   double* member_dt_bits = nullptr; // [nmember] scratch for the per-member dt min
+  double* musgs_int = nullptr;  // LES: internal-layout SGS viscosity (FP64), allocated on first use
   // adjoint scratch (sod_adjoint.cu): stage states, seeds, accumulators
   double* adj = nullptr;
   size_t adj_len = 0;
@@ -186,5 +189,7 @@ int launch_copy_f32(const double* src, float* dst, int64_t n, cudaStream_t st);
 int init_kernel_attrs();
 // packed-FP32 (FFMA2) variant of the mixed fused RHS kernel (sod_rhs_mixed.cu)
 int launch_rhs_mixed2(const RhsArgs& a, int epb, cudaStream_t st);
+// LES (sod_les.cu): musgs_int <- sgs_visc of the velocity u (3 columns of npoin)
+int launch_sgs(SodMesh* m, const double* u, cudaStream_t st);
 int init_rhs_mixed2_attrs();
 }  // namespace sod

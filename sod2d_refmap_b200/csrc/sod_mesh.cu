@@ -233,6 +233,8 @@ void sod_params_default(SodParams* p) {
   p->flag_normalise_entropy = 1;
   p->cfl_conv = 0.5;
   p->cfl_diff = 0.5;
+  p->flag_les = 0;
+  p->c_sgs = 0.025;
 }
 
 static void to_dev_params(const SodParams* s, DevParams* d) {
@@ -244,6 +246,8 @@ static void to_dev_params(const SodParams* s, DevParams* d) {
   d->inv_Rgas = 1.0 / s->Rgas;
   d->CpPr = s->Cp / s->Prt;
   d->Cp09 = s->Cp / 0.9;
+  d->flag_les = s->flag_les;
+  d->c_sgs = s->c_sgs;
   d->gamma_f = (float)s->gamma_gas;
   d->c_rho_f = (float)s->c_rho;
   d->c_ener_f = (float)s->c_ener;
@@ -263,7 +267,7 @@ void sod_mesh_destroy(SodMesh* m) {
     if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
   void* ptrs[] = {m->econn, m->geo64, m->geo32, m->Ml, m->helem, m->helem_l, m->jratio, m->n2e_ptr, m->n2e,
                   m->mue_int, m->mue32, m->a_of_d_dev, m->buf.ys, m->buf.rsum, m->buf.rel, m->buf.red,
-                  m->buf.scal, m->buf.counters, m->buf.mu_fluid, m->adj};
+                  m->buf.scal, m->buf.counters, m->buf.mu_fluid, m->adj, m->musgs_int};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   for (double* p : m->host_mirror) cudaFree(p);

@@ -751,6 +751,23 @@ int launch_gather(SodMesh* m, bool mixed, int stage, GatherArgs& a, cudaStream_t
   return mixed ? launch_gather_t<float>(stage, a, st) : launch_gather_t<double>(stage, a, st);
 }
 
+// LES is on for a step when the parameters ask for it and the state carries mu_sgs
+static bool les_active(const SodMesh* m, const SodState* s) {
+  return m->prm.flag_les == 1 && s->mu_sgs != nullptr && m->musgs_int != nullptr;
+}
+
+// mu_sgs (nelem,64) in the reference layout -> internal layout before a step (allocates once)
+int les_in(SodMesh* m, const SodState* s, cudaStream_t st) {
+  if (!(m->prm.flag_les == 1 && s->mu_sgs)) return SOD_OK;
+  if (!m->musgs_int) SOD_CUDA(cudaMalloc(&m->musgs_int, sizeof(double) * (size_t)m->nelem * NN));
+  return mesh_ref_to_internal_elem(m, s->mu_sgs, m->musgs_int, st);
+}
+
+int les_out(SodMesh* m, const SodState* s, cudaStream_t st) {
+  if (!les_active(m, s)) return SOD_OK;
+  return mesh_internal_to_ref_elem(m, m->musgs_int, s->mu_sgs, st);
+}
+
 int launch_visc_dt(SodMesh* m, const SodState* s, double* dt_out, float* mue32, cudaStream_t st) {
   ViscArgs v;
   v.nelem = m->nelem;
@@ -763,7 +780,7 @@ int launch_visc_dt(SodMesh* m, const SodState* s, double* dt_out, float* mue32, 
   v.csound = s->csound;
   v.Tem = s->Tem;
   v.mu_fluid = s->mu_fluid;
-  v.musgs = nullptr;
+  v.musgs = les_active(m, s) ? m->musgs_int : nullptr;
   v.helem_l = m->helem_l;
   v.helem = m->helem;
   v.jratio = m->jratio;
@@ -822,6 +839,7 @@ int run_step(SodMesh* m, SodState* s, const double* dt_dev, double* dt_next, boo
   const size_t N = m->npoin;
   const int epb = m->tuned_epb[mixed ? 1 : 0] ? m->tuned_epb[mixed ? 1 : 0] : (mixed ? 4 : 2);
   SodState loc = *s;
+  const bool les = les_active(m, s);
   double* reta_tmp = nullptr;
   if (!loc.Reta) {
     // stage 4 reads rsum[5] before writing Reta, element-wise, so aliasing is safe
@@ -837,7 +855,8 @@ int run_step(SodMesh* m, SodState* s, const double* dt_dev, double* dt_next, boo
     const double* src_q2 = stage == 1 ? s->q + 2 * N : yin + 3 * N;
     const double* src_E = stage == 1 ? s->E : yin + 4 * N;
     if (ev) cudaEventRecord(ev[2 * (stage - 1)], st);
-    rc = launch_rhs(m, mixed, epb, src_rho, src_q0, src_q1, src_q2, src_E, s->mu_factor, nullptr, st);
+    rc = launch_rhs(m, mixed, epb, src_rho, src_q0, src_q1, src_q2, src_E, s->mu_factor, les ? m->musgs_int : nullptr,
+                    st);
     if (rc) return rc;
     if (ev) cudaEventRecord(ev[2 * (stage - 1) + 1], st);
     GatherArgs g{};
@@ -859,6 +878,12 @@ int run_step(SodMesh* m, SodState* s, const double* dt_dev, double* dt_next, boo
     if (ev) cudaEventRecord(ev[2 * (3 + stage) + 1], st);
   }
   if (ev) cudaEventRecord(ev[16], st);
+  if (les) {
+    // sgs_visc after the step (time_integ.f90:498-506), before the dt of the next step uses it
+    // (CFDSolverBase.f90:1592); independent of the entropy viscosity, so it may run first
+    rc = launch_sgs(m, s->u, st);
+    if (rc) return rc;
+  }
   rc = launch_visc_dt(m, &loc, dt_next, mixed ? m->mue32 : nullptr, st);
   if (ev) cudaEventRecord(ev[17], st);
   return rc;
@@ -890,11 +915,15 @@ int sod_rk4_main(SodMesh* m, SodState* s, const double* dt_dev, double* dt_next_
   if (rc) return rc;
   rc = mesh_ref_to_internal_elem(m, s->mu_e, m->mue_int, st);
   if (rc) return rc;
+  rc = les_in(m, s, st);
+  if (rc) return rc;
   if (mixed) {
     rc = launch_copy_f32(m->mue_int, m->mue32, (int64_t)m->nelem * NN, st);
     if (rc) return rc;
   }
   rc = run_step(m, s, dt_dev, dt_next_dev, mixed, st);
+  if (rc) return rc;
+  rc = les_out(m, s, st);
   if (rc) return rc;
   return mesh_internal_to_ref_elem(m, m->mue_int, s->mu_e, st);
 }
@@ -911,11 +940,15 @@ int sod_rk4_main_record(SodMesh* m, SodState* s, const double* dt_dev, double* d
   if (rc) return rc;
   rc = mesh_ref_to_internal_elem(m, s->mu_e, m->mue_int, st);
   if (rc) return rc;
+  rc = les_in(m, s, st);
+  if (rc) return rc;
   if (mixed) {
     rc = launch_copy_f32(m->mue_int, m->mue32, (int64_t)m->nelem * NN, st);
     if (rc) return rc;
   }
   rc = run_step(m, s, dt_dev, dt_next_dev, mixed, st, nullptr, stages);
+  if (rc) return rc;
+  rc = les_out(m, s, st);
   if (rc) return rc;
   return mesh_internal_to_ref_elem(m, m->mue_int, s->mu_e, st);
 }
@@ -931,6 +964,8 @@ int sod_rk4_steps(SodMesh* m, SodState* s, double* dt_dev, int nsteps, SodPrecis
   if (rc) return rc;
   rc = mesh_ref_to_internal_elem(m, s->mu_e, m->mue_int, st);
   if (rc) return rc;
+  rc = les_in(m, s, st);
+  if (rc) return rc;
   if (mixed) {
     rc = launch_copy_f32(m->mue_int, m->mue32, (int64_t)m->nelem * NN, st);
     if (rc) return rc;
@@ -938,7 +973,8 @@ int sod_rk4_steps(SodMesh* m, SodState* s, double* dt_dev, int nsteps, SodPrecis
   if (nsteps > 0) {
     // capture one step into a graph keyed by (state pointers, dt pointer, precision, epb)
     uint64_t key = (uint64_t)(uintptr_t)s->rho ^ ((uint64_t)(uintptr_t)dt_dev << 1) ^ ((uint64_t)mixed << 63) ^
-                   ((uint64_t)(uintptr_t)s->Reta << 3) ^ ((uint64_t)m->tuned_epb[mixed ? 1 : 0] << 56);
+                   ((uint64_t)(uintptr_t)s->Reta << 3) ^ ((uint64_t)m->tuned_epb[mixed ? 1 : 0] << 56) ^
+                   ((uint64_t)(uintptr_t)(les_active(m, s) ? s->mu_sgs : nullptr) << 5);
     auto it = m->graphs.find(key);
     if (it == m->graphs.end()) {
       cudaStream_t cap;
@@ -970,6 +1006,8 @@ int sod_rk4_steps(SodMesh* m, SodState* s, double* dt_dev, int nsteps, SodPrecis
       g_launches.fetch_add(it->second.nkernels);
     }
   }
+  rc = les_out(m, s, st);
+  if (rc) return rc;
   return mesh_internal_to_ref_elem(m, m->mue_int, s->mu_e, st);
 }
 
@@ -984,6 +1022,8 @@ int sod_step_profile(SodMesh* m, SodState* s, double* dt_dev, int nsteps, SodPre
   rc = ensure_step_buffers(m, mixed);
   if (rc) return rc;
   rc = mesh_ref_to_internal_elem(m, s->mu_e, m->mue_int, st);
+  if (rc) return rc;
+  rc = les_in(m, s, st);
   if (rc) return rc;
   if (mixed) {
     rc = launch_copy_f32(m->mue_int, m->mue32, (int64_t)m->nelem * NN, st);
@@ -1007,6 +1047,8 @@ int sod_step_profile(SodMesh* m, SodState* s, double* dt_dev, int nsteps, SodPre
   ms_out[0] = (float)(acc[0] / (4.0 * nsteps));
   ms_out[1] = (float)(acc[1] / (4.0 * nsteps));
   ms_out[2] = (float)(acc[2] / nsteps);
+  rc = les_out(m, s, st);
+  if (rc) return rc;
   return mesh_internal_to_ref_elem(m, m->mue_int, s->mu_e, st);
 }
 
@@ -1022,6 +1064,8 @@ int sod_autotune(SodMesh* m, SodState* s, SodPrecision prec, int* best_epb, floa
   rc = ensure_step_buffers(m, mixed);
   if (rc) return rc;
   rc = mesh_ref_to_internal_elem(m, s->mu_e, m->mue_int, st);
+  if (rc) return rc;
+  rc = les_in(m, s, st);
   if (rc) return rc;
   if (mixed) {
     rc = launch_copy_f32(m->mue_int, m->mue32, (int64_t)m->nelem * NN, st);
@@ -1097,7 +1141,7 @@ int sod_rk4_main_host(SodMesh* m, SodState* h, double dt_host, double* dt_next_h
   const size_t N = m->npoin, EN = (size_t)m->nelem * NN;
   // persistent device mirror owned by the mesh
   auto& mv = m->host_mirror;
-  const size_t sizes[] = {N, 3 * N, N, 3 * N, N, N, N, N, N, N, N, N, EN, N, 1};
+  const size_t sizes[] = {N, 3 * N, N, 3 * N, N, N, N, N, N, N, N, N, EN, N, 1, EN};
   if (mv.empty()) {
     for (size_t s : sizes) {
       double* p = nullptr;
@@ -1105,7 +1149,9 @@ int sod_rk4_main_host(SodMesh* m, SodState* h, double dt_host, double* dt_next_h
       mv.push_back(p);
     }
   }
-  SodState d{mv[0], mv[1], mv[2], mv[3], mv[4], mv[5], mv[6], mv[7], mv[8], mv[9], mv[10], mv[11], mv[12], mv[13]};
+  const bool les_h = h->mu_sgs && m->prm.flag_les == 1;
+  SodState d{mv[0], mv[1], mv[2], mv[3], mv[4], mv[5], mv[6], mv[7], mv[8], mv[9], mv[10], mv[11], mv[12], mv[13],
+             les_h ? mv[15] : nullptr};
   double* ddt = mv[14];
   SOD_CUDA(cudaMemcpyAsync(d.rho, h->rho, N * 8, cudaMemcpyHostToDevice, st));
   SOD_CUDA(cudaMemcpyAsync(d.q, h->q, 3 * N * 8, cudaMemcpyHostToDevice, st));
@@ -1113,13 +1159,14 @@ int sod_rk4_main_host(SodMesh* m, SodState* h, double dt_host, double* dt_next_h
   SOD_CUDA(cudaMemcpyAsync(d.mu_e, h->mu_e, EN * 8, cudaMemcpyHostToDevice, st));
   SOD_CUDA(cudaMemcpyAsync(d.mu_factor, h->mu_factor, N * 8, cudaMemcpyHostToDevice, st));
   SOD_CUDA(cudaMemcpyAsync(ddt, &dt_host, 8, cudaMemcpyHostToDevice, st));
+  if (les_h) SOD_CUDA(cudaMemcpyAsync(d.mu_sgs, h->mu_sgs, EN * 8, cudaMemcpyHostToDevice, st));
   int rc = sod_rk4_main(m, &d, ddt, ddt, prec, stream);
   if (rc) return rc;
   struct Pair { double* hst; double* dev; size_t n; };
   Pair outs[] = {{h->rho, d.rho, N}, {h->q, d.q, 3 * N}, {h->E, d.E, N}, {h->u, d.u, 3 * N}, {h->pr, d.pr, N},
                  {h->Tem, d.Tem, N}, {h->e_int, d.e_int, N}, {h->eta, d.eta, N}, {h->csound, d.csound, N},
                  {h->machno, d.machno, N}, {h->mu_fluid, d.mu_fluid, N}, {h->mu_e, d.mu_e, EN},
-                 {h->Reta, d.Reta, N}};
+                 {h->Reta, d.Reta, N}, {les_h ? h->mu_sgs : nullptr, d.mu_sgs, EN}};
   for (auto& o : outs)
     if (o.hst) SOD_CUDA(cudaMemcpyAsync(o.hst, o.dev, o.n * 8, cudaMemcpyDeviceToHost, st));
   if (dt_next_host) SOD_CUDA(cudaMemcpyAsync(dt_next_host, ddt, 8, cudaMemcpyDeviceToHost, st));

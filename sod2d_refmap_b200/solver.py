@@ -49,7 +49,7 @@ def _stream(stream=None) -> C.c_void_p:
 
 def params_struct(prm: TGVParams) -> _lib.SodParams:
     return _lib.SodParams(prm.gamma_gas, prm.Rgas, prm.Cp, prm.Prt, prm.ce, prm.cmax, prm.cglob, prm.c_rho, prm.c_ener,
-                          int(prm.flag_normalise_entropy), prm.cfl_conv, prm.cfl_diff)
+                          int(prm.flag_normalise_entropy), prm.cfl_conv, prm.cfl_diff, int(prm.flag_les), prm.c_sgs)
 
 
 FP64 = _lib.SOD_FP64
@@ -60,7 +60,7 @@ class Sod2dState:
     """Device arrays of one solver state in the reference layouts (level pos=2)."""
 
     FIELDS = ("rho", "q", "E", "u", "pr", "Tem", "e_int", "eta", "csound", "machno", "mu_fluid", "mu_factor",
-              "mu_e", "Reta")
+              "mu_e", "Reta", "mu_sgs")
 
     def __init__(self, npoin: int, nelem: int, device="cuda"):
         torch = _torch()
@@ -81,6 +81,7 @@ class Sod2dState:
         self.mu_factor = torch.zeros(npoin, **f64)
         self.mu_e = torch.zeros(64, nelem, **f64)   # (nelem,64) Fortran
         self.Reta = torch.zeros(npoin, **f64)
+        self.mu_sgs = torch.zeros(64, nelem, **f64)  # (nelem,64) Fortran; used when flag_les = 1
         self.dt = torch.zeros(1, **f64)
 
     @classmethod
@@ -92,6 +93,7 @@ class Sod2dState:
         s.q.copy_(torch.from_numpy(np.ascontiguousarray(st.q.T)))
         s.u.copy_(torch.from_numpy(np.ascontiguousarray(st.u.T)))
         s.mu_e.copy_(torch.from_numpy(np.ascontiguousarray(st.mu_e.T)))
+        s.mu_sgs.copy_(torch.from_numpy(np.ascontiguousarray(st.mu_sgs.T)))
         return s
 
     def struct(self) -> _lib.SodState:
