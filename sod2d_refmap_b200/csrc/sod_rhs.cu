@@ -13,15 +13,8 @@
 // to contravariant fluxes precomputed at each gauss point.  Element residuals are written to
 // an element-major array and assembled by KG as an ordered CSR gather (no atomics).
 //
-// Precision modes (template R / DEV):
-//   R=double, DEV=false : the reference's formulas on FP64 (parity path).
-//   R=float,  DEV=true  : FP32 element arithmetic on deviation fields.  Each element subtracts
-//                         the FP64 values of its node 0 from rho,u,q,p,h,k,eta,T before the FP32
-//                         cast, and every product flux is expanded exactly around those
-//                         references, e.g. div(rho h u) = h_r div(q) + div(rho (h-h_r) u) and
-//                         div(q x u)_i = q_ri div u + u_r . grad q_i + div((q-q_r)_i (u-u_r)),
-//                         so FP32 rounding acts on small deviations instead of the O(p0) means.
-//                         Assembly, lumped mass, RK state and reductions stay FP64.
+// This is the FP64 parity path: the reference's formulas in FP64 (R = double).  The mixed
+// path (FP32 element arithmetic on deviation fields) is k_rhs_mixed2 in sod_rhs_mixed.cu.
 #include "sod_internal.cuh"
 #include <cmath>
 #include <algorithm>
@@ -78,18 +71,16 @@ __device__ __forceinline__ R divT(const R* fx, const R* fy, const R* fz, int i, 
 
 constexpr int NBUF = 15;  // fields per batch buffer
 constexpr int NP2 = 18;   // 6 contravariant fluxes x 3 directions
-constexpr int NREF = 16;
 
 template <typename R>
 constexpr size_t rhs_smem_bytes(int epb) {
-  return sizeof(double) * (size_t)epb * NREF + sizeof(R) * (size_t)epb * (NBUF + NP2) * FSTRIDE;
+  return sizeof(R) * (size_t)epb * (NBUF + NP2) * FSTRIDE;
 }
 
-template <typename R, bool DEV, int EPB>
+template <typename R, int EPB>
 __global__ void __launch_bounds__(64 * EPB) k_rhs_fused(const RhsArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  double* refs_all = reinterpret_cast<double*>(smem_raw);
-  R* buf_all = reinterpret_cast<R*>(smem_raw + sizeof(double) * EPB * NREF);
+  R* buf_all = reinterpret_cast<R*>(smem_raw);
   const int tid = threadIdx.x;
   const int es = tid >> 6;
   const int d = tid & 63;
@@ -97,7 +88,6 @@ __global__ void __launch_bounds__(64 * EPB) k_rhs_fused(const RhsArgs a) {
   const int e = blockIdx.x * EPB + es;
   const bool active = e < a.nelem;
   const int ee = active ? e : a.nelem - 1;
-  double* refs = refs_all + es * NREF;
   R* buf = buf_all + (size_t)es * (NBUF + NP2) * FSTRIDE;
   R* p2 = buf + NBUF * FSTRIDE;
   const int s_me = sidx(i, j, k);
@@ -135,54 +125,23 @@ __global__ void __launch_bounds__(64 * EPB) k_rhs_fused(const RhsArgs a) {
   const R mue = reinterpret_cast<const R*>(a.mue)[(size_t)ee * NN + d];
   const double musgs = a.musgs ? a.musgs[(size_t)ee * NN + d] : 0.0;
 
-  // element references (node d == 0) for the deviation form
-  double r_rho = 0, r_u[3] = {0, 0, 0}, r_q[3] = {0, 0, 0}, r_p = 0, r_h = 0, r_k = 0, r_eta = 0, r_T = 0, r_L = 0;
-  if constexpr (DEV) {
-    if (d == 0) {
-      refs[0] = rho; refs[1] = uv[0]; refs[2] = uv[1]; refs[3] = uv[2];
-      refs[4] = qv[0]; refs[5] = qv[1]; refs[6] = qv[2]; refs[7] = p; refs[8] = h; refs[9] = kk;
-      const double L = log(p / pow(rho, g));
-      refs[10] = (rho / (g - 1.0)) * L;
-      refs[11] = T;
-      refs[12] = L;
-    }
-    __syncthreads();
-    r_rho = refs[0]; r_u[0] = refs[1]; r_u[1] = refs[2]; r_u[2] = refs[3];
-    r_q[0] = refs[4]; r_q[1] = refs[5]; r_q[2] = refs[6]; r_p = refs[7]; r_h = refs[8]; r_k = refs[9];
-    r_eta = refs[10]; r_T = refs[11]; r_L = refs[12];
-  }
-  // deviation (or full) values
-  const double s_h = h - r_h, s_k = kk - r_k;
-  double s_eta, eta_full;
-  double muf;
-  if constexpr (DEV) {
-    // eta - eta_r = ((rho-rho_r) L_r + rho (L - L_r)) / (gamma-1), L - L_r by log1p of small ratios
-    const float drho = (float)(rho - r_rho);
-    const float dL = log1pf((float)((p - r_p) / r_p)) - (float)g * log1pf(drho / (float)r_rho);
-    s_eta = ((double)drho * r_L + rho * (double)dL) / (g - 1.0);
-    eta_full = r_eta + s_eta;
-    const float Tf = (float)T;
-    muf = (double)((float)mufac * (float)kSuthC1 * (Tf * sqrtf(Tf)) / (Tf + (float)kSuthS));
-  } else {
-    eta_full = (rho / (g - 1.0)) * log(p / pow(rho, g));
-    s_eta = eta_full;
-    muf = mufac * kSuthC1 * (T * sqrt(T)) / (T + kSuthS);
-  }
+  const double eta_full = (rho / (g - 1.0)) * log(p / pow(rho, g));
+  const double muf = mufac * kSuthC1 * (T * sqrt(T)) / (T + kSuthS);
 
   // ---- batch A: primitive and scalar fields
-  buf[0 * FSTRIDE + s_me] = (R)(rho - r_rho);
+  buf[0 * FSTRIDE + s_me] = (R)rho;
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
-    buf[(1 + c) * FSTRIDE + s_me] = (R)(uv[c] - r_u[c]);
-    buf[(4 + c) * FSTRIDE + s_me] = (R)(qv[c] - r_q[c]);
+    buf[(1 + c) * FSTRIDE + s_me] = (R)uv[c];
+    buf[(4 + c) * FSTRIDE + s_me] = (R)qv[c];
   }
-  buf[7 * FSTRIDE + s_me] = (R)(p - r_p);
-  buf[8 * FSTRIDE + s_me] = (R)s_h;
-  buf[9 * FSTRIDE + s_me] = (R)(rho * s_h);
-  buf[10 * FSTRIDE + s_me] = (R)s_k;
-  buf[11 * FSTRIDE + s_me] = (R)(rho * s_k);
-  buf[12 * FSTRIDE + s_me] = (R)s_eta;
-  buf[13 * FSTRIDE + s_me] = (R)(T - r_T);
+  buf[7 * FSTRIDE + s_me] = (R)p;
+  buf[8 * FSTRIDE + s_me] = (R)h;
+  buf[9 * FSTRIDE + s_me] = (R)(rho * h);
+  buf[10 * FSTRIDE + s_me] = (R)kk;
+  buf[11 * FSTRIDE + s_me] = (R)(rho * kk);
+  buf[12 * FSTRIDE + s_me] = (R)eta_full;
+  buf[13 * FSTRIDE + s_me] = (R)T;
   __syncthreads();
 
   R gradRho[3], gradU[3][3], gradQ[3][3], gradP[3], gradH[3], gradRH[3], gradK[3], gradRK[3], gradEta[3], gradT[3];
@@ -212,13 +171,6 @@ __global__ void __launch_bounds__(64 * EPB) k_rhs_fused(const RhsArgs a) {
     giso(buf + 13 * FSTRIDE, i, j, k, Dx, Dy, Dz, gx, gy, gz);
     phys(H, gx, gy, gz, gradT[0], gradT[1], gradT[2]);
   }
-  if constexpr (DEV) {
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      gradRH[c] += (R)r_h * gradRho[c];
-      gradRK[c] += (R)r_k * gradRho[c];
-    }
-  }
   const R divU = gradU[0][0] + gradU[1][1] + gradU[2][2];
   const R divQ = gradQ[0][0] + gradQ[1][1] + gradQ[2][2];
   const R rhoR = (R)rho, hR = (R)h, kR = (R)kk, etaR = (R)eta_full;
@@ -241,22 +193,6 @@ __global__ void __launch_bounds__(64 * EPB) k_rhs_fused(const RhsArgs a) {
 #pragma unroll
     for (int jd = 0; jd < 3; ++jd)
       Rmo[c] += R(0.25) * ((uR[c] * uR[jd]) * gradRho[jd] + qR[jd] * gradU[c][jd] + uR[jd] * gradQ[c][jd]);
-  }
-  if constexpr (DEV) {
-    // reference parts of the batch B/C divergences (exact expansions around the element refs)
-    const R rh = (R)r_h, rk = (R)r_k, re = (R)r_eta;
-    Ren += R(0.25) * (rh * divQ + rhoR * (rh * divU)) + R(0.25) * (rk * divQ + rhoR * (rk * divU));
-    Ret += R(0.5) * (re * divU);
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      R dF = (R)r_q[c] * divU, dFuu = (R)r_u[c] * divU;
-#pragma unroll
-      for (int jd = 0; jd < 3; ++jd) {
-        dF += (R)r_u[jd] * gradQ[c][jd];
-        dFuu += (R)r_u[jd] * gradU[c][jd];
-      }
-      Rmo[c] += R(0.25) * (dF + rhoR * dFuu);
-    }
   }
 
   // ---- diffusion pass 1 (elem_diffu.f90:70-140): stresses and contravariant fluxes
@@ -289,10 +225,10 @@ __global__ void __launch_bounds__(64 * EPB) k_rhs_fused(const RhsArgs a) {
   }
   __syncthreads();  // batch A reads done
 
-  // ---- batch B: product vectors (rho h u, h u, rho k u, k u, eta u) in deviation form
+  // ---- batch B: product vectors (rho h u, h u, rho k u, k u, eta u)
   {
-    const R sh = (R)s_h, sk = (R)s_k, se = (R)s_eta;
-    const R rsh = (R)(rho * s_h), rsk = (R)(rho * s_k);
+    const R sh = (R)h, sk = (R)kk, se = (R)eta_full;
+    const R rsh = (R)(rho * h), rsk = (R)(rho * kk);
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       buf[(0 + c) * FSTRIDE + s_me] = rsh * uR[c];
@@ -314,13 +250,13 @@ __global__ void __launch_bounds__(64 * EPB) k_rhs_fused(const RhsArgs a) {
   }
   __syncthreads();
 
-  // ---- batch C: tensors q x u and u x u (symmetric) in deviation form
+  // ---- batch C: tensors q x u and u x u (symmetric)
   {
     R sq[3], su[3];
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      sq[c] = (R)(qv[c] - r_q[c]);
-      su[c] = (R)(uv[c] - r_u[c]);
+      sq[c] = (R)qv[c];
+      su[c] = (R)uv[c];
     }
 #pragma unroll
     for (int r = 0; r < 3; ++r)
@@ -660,9 +596,9 @@ __global__ void __launch_bounds__(64 * KV_EPB, SOD_KV_MIN_BLOCKS) k_visc_dt(cons
 // ---------------------------------------------------------------------------------------------
 // Host-side launch helpers
 // ---------------------------------------------------------------------------------------------
-template <typename R, bool DEV, int EPB>
+template <typename R, int EPB>
 static int set_rhs_attr() {
-  SOD_CUDA(cudaFuncSetAttribute(k_rhs_fused<R, DEV, EPB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  SOD_CUDA(cudaFuncSetAttribute(k_rhs_fused<R, EPB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)rhs_smem_bytes<R>(EPB)));
   return SOD_OK;
 }
@@ -670,18 +606,18 @@ static int set_rhs_attr() {
 int init_kernel_attrs() {
   static bool done = false;
   if (done) return SOD_OK;
-  int rc = set_rhs_attr<double, false, 1>() | set_rhs_attr<double, false, 2>() | set_rhs_attr<double, false, 4>() |
+  int rc = set_rhs_attr<double, 1>() | set_rhs_attr<double, 2>() | set_rhs_attr<double, 4>() |
            init_rhs_mixed2_attrs();
   if (rc) return SOD_ERR_CUDA;
   done = true;
   return SOD_OK;
 }
 
-template <typename R, bool DEV, int EPB>
+template <typename R, int EPB>
 static int launch_rhs_t(const RhsArgs& a, cudaStream_t st) {
   const size_t smem = rhs_smem_bytes<R>(EPB);
   const int grid = (a.nelem + EPB - 1) / EPB;
-  k_rhs_fused<R, DEV, EPB><<<grid, 64 * EPB, smem, st>>>(a);
+  k_rhs_fused<R, EPB><<<grid, 64 * EPB, smem, st>>>(a);
   SOD_CHECK_LAUNCH();
   return SOD_OK;
 }
@@ -704,9 +640,9 @@ int launch_rhs(SodMesh* m, bool mixed, int epb, const double* rho, const double*
   a.prm = m->prm;
   if (!mixed) {
     switch (epb) {
-      case 1: return launch_rhs_t<double, false, 1>(a, st);
-      case 4: return launch_rhs_t<double, false, 4>(a, st);
-      default: return launch_rhs_t<double, false, 2>(a, st);
+      case 1: return launch_rhs_t<double, 1>(a, st);
+      case 4: return launch_rhs_t<double, 4>(a, st);
+      default: return launch_rhs_t<double, 2>(a, st);
     }
   } else {
     return launch_rhs_mixed2(a, epb, st);

@@ -1,9 +1,12 @@
 // Mixed-precision fused element RHS with packed FP32 arithmetic (sm_100a FFMA2).
 //
-// Same mathematics as k_rhs_fused<float, true, EPB> in sod_rhs.cu (the reference element loops
-// of full_convec_ijk elem_convec.f90:211-460, full_diffusion_ijk elem_diffu.f90:12-198 and
-// generic_scalar_convec_ijk elem_convec.f90:462-570, FP32 on deviation fields), with the
-// nodal fields staged in shared memory as float2 pairs: one 8-byte shared load and one packed
+// The reference element loops of full_convec_ijk (elem_convec.f90:211-460), full_diffusion_ijk
+// (elem_diffu.f90:12-198) and generic_scalar_convec_ijk (elem_convec.f90:462-570) in FP32 on
+// deviation fields: each element subtracts FP64 references before the FP32 cast (the values of
+// its node 0; for the directly differentiated fields an affine-in-xi reference, see batch A)
+// and every product flux is expanded exactly around them, e.g. div(rho H u) = H_r div q +
+// div(rho (H - H_r) u), so FP32 rounding acts on small deviations.  Assembly, lumped mass, RK
+// state and reductions stay FP64.  The nodal fields are staged in shared memory as float2 pairs: one 8-byte shared load and one packed
 // __ffma2_rn serve two fields, and the xi-lines are read as two 16-byte loads.  The energy
 // convection is linear in (h, k) and every h term has a k twin of the same form (the two
 // skew-symmetric quartets of elem_convec.f90:415-425), so both quartets are evaluated at once
