@@ -242,21 +242,24 @@ int sod_batch_rk4_steps(SodBatch* B, int nsteps, SodPrecision prec, sod_stream_t
 /* ---- Incompressible pressure Poisson (lib_sod2d_incomp) --------------------------------- */
 
 typedef struct SodPoisson SodPoisson;
-/* Assemble the pinned stiffness operator that eval_laplacian_mult (mod_operators.f90:20-128)
- * applies matrix-free, as CSR with FP64 values (plus an FP32 copy) and int32 indices; pinned
- * node = node 0 (lpoin_w(1), mod_operators.f90:46-48,125-127): its row is empty and its
- * column dropped.  Also forms the Jacobi diagonal of eval_laplacian_diag (:417-461). */
+/* Set up the pinned pressure Laplacian that eval_laplacian_mult (mod_operators.f90:20-128)
+ * applies matrix-free: the per-gauss-point metric gpvol He^T He (FP64 and an FP32 copy, 6
+ * values per point) and the Jacobi diagonal of eval_laplacian_diag (:417-461); pinned node =
+ * node 0 (lpoin_w(1), mod_operators.f90:46-48,125-127).  The handle keeps a pointer to the
+ * mesh, which must outlive it. */
 int sod_poisson_create(SodMesh* mesh, SodPoisson** out);
 void sod_poisson_destroy(SodPoisson* P);
-int sod_poisson_nnz(SodPoisson* P, int64_t* nnz);
-/* y = K x through the assembled CSR (device arrays of npoin): eval_laplacian_mult. */
+/* y = K x, matrix-free (device arrays of npoin): eval_laplacian_mult, x(pin) read as 0 and
+ * y(pin) = 0. */
 int sod_poisson_apply(SodPoisson* P, const double* x, double* y, sod_stream_t stream);
 /* Jacobi diagonal (device array of npoin): eval_laplacian_diag. */
 int sod_poisson_diag(SodPoisson* P, double* d, sod_stream_t stream);
 /* conjGrad_pressure_incomp (mod_solver_incomp.f90:247-434): R holds the right-hand side on
  * entry and x0+x on exit; Rp0 is the initial guess; stops at ||r|| < tol ||r0||, with
- * beta = <r, z - z_old>/<r_old, z_old> as the reference.  mixed != 0 runs FP32 Jacobi-PCG
- * sweeps (FP32 values and vectors) inside FP64 residual iterative refinement.  Returns
+ * beta = <r, z - z_old>/<r_old, z_old> as the reference; the stop test runs on the device and
+ * the host reads the scalars every 16 iterations.  mixed != 0 runs FP32 Jacobi-PCG sweeps
+ * (FP32 metric and vectors) inside FP64 residual iterative refinement.  Calls on one handle
+ * must not overlap (its work vectors are shared).  Returns
  * SOD_ERR_NOT_CONVERGED when max_iter is reached first.  iters/final_rel may be null. */
 int sod_conjgrad_pressure(SodPoisson* P, const double* Rp0, double* R, int max_iter, double tol,
                           int mixed, int* iters, double* final_rel, sod_stream_t stream);

@@ -67,7 +67,6 @@ _SIGS = {
     "sod_sutherland_viscosity": (_i, [C.c_int32, _p, _p, _p, _p]),
     "sod_poisson_create": (_i, [_p, _p]),
     "sod_poisson_destroy": (None, [_p]),
-    "sod_poisson_nnz": (_i, [_p, _p]),
     "sod_poisson_apply": (_i, [_p, _p, _p, _p]),
     "sod_poisson_diag": (_i, [_p, _p, _p]),
     "sod_conjgrad_pressure": (_i, [_p, _p, _p, _i, _d, _i, _p, _p, _p]),

@@ -1,90 +1,124 @@
-// Incompressible pressure Poisson: assembled CSR operator and Jacobi PCG (sm_100a).
+// Incompressible pressure Poisson: matrix-free operator and Jacobi PCG (sm_100a).
 //
-// The operator is the pinned stiffness matrix that eval_laplacian_mult (lib_sod2d_incomp
-// mod_operators.f90:20-128) applies matrix-free:
-//   (K p)_a = sum_e sum_dir sum_{q on the dir-line through a} gpvol_q D[q_dir][a_dir]
-//             sum_i He(i,dir,q) (He(q) grad_iso p)_i ,      p(pin) := 0, (K p)(pin) := 0,
-// with pin = lpoin_w(1) = node 0 (mod_operators.f90:46-48,125-127).  Its element matrix is
-//   K^e_ab = sum_q sum_{dir,dir'} M_q(dir,dir') D[q_dir][a_dir] D[q_dir'][b_dir'],
-//   M_q = gpvol_q He_q^T He_q,  a on the dir-line and b on the dir'-line through q,
-// so K couples the nodes of an element that share at least one ijk index.  Rows are assembled
-// by their owner thread in ascending element order (deterministic, no atomics); the pinned row
-// is empty and the pinned column is dropped.  The Jacobi diagonal is the unpinned K_aa, which
-// equals eval_laplacian_diag (mod_operators.f90:417-461).
+// The operator is eval_laplacian_mult (lib_sod2d_incomp mod_operators.f90:20-128), applied
+// matrix-free as the reference does:
+//   (K p)_a = sum_e sum_dir sum_{q on the dir-line through a} D[q_dir][a_dir] F_dir(q),
+//   F(q) = gpvol_q He_q^T He_q grad_iso p(q),          p(pin) := 0, (K p)(pin) := 0,
+// with pin = lpoin_w(1) = node 0 (mod_operators.f90:46-48,125-127).  The symmetric 3x3
+// M_q = gpvol_q He_q^T He_q is formed once per gauss point at setup (6 values: the reference
+// re-reads He and gpvol, 10 values, on every product), in FP64 and in an FP32 copy.
 //
-// conjGrad_pressure_incomp (mod_solver_incomp.f90:247-434) runs as: fused SpMV + <p,Ap>;
-// device scalars alpha; fused x/r/z update with ||r||^2, <r,z-z_old>, <r,z>; device scalars
-// beta; p update.  The host reads ||r||^2 each iteration for the stopping test, as the
-// reference does after its MPI_Allreduce.  mixed != 0 runs FP32 CG sweeps (FP32 values and
-// vectors) inside FP64 residual iterative refinement.
+// One product is two kernels.  k_lap_elem: one thread per gauss point, EPB elements per CTA;
+// the element's p is gathered into shared memory, the three line derivatives and F are formed
+// in registers, F goes back to shared memory and the transposed line sums give the element
+// residual, stored as rel[e*64 + d].  k_lap_gather: one thread per node sums its element
+// residuals through the node->element CSR in ascending element order (deterministic; the
+// reference uses atomics) and adds <p, Kp> to per-block partials.
+//
+// The Jacobi diagonal is eval_laplacian_diag (mod_operators.f90:417-461): the unpinned K_aa.
+//
+// conjGrad_pressure_incomp (mod_solver_incomp.f90:247-434) runs as: product + <p,Ap>; device
+// scalars alpha; fused x/r/z update with ||r||^2, <r,z-z_old>, <r,z>; device scalars beta and
+// the stop test ||r|| < tol ||r0|| (:393); p update.  The stop test, the iteration counter and
+// a done flag live on the device, so iterations are replayed in CUDA-graph batches of kBatch
+// and the host reads the scalars once per batch; every kernel of an iteration after the
+// converged one returns at once, so the iterate and the count are those of a host-tested
+// loop.  mixed != 0 runs FP32 CG sweeps (FP32 metric and vectors) inside FP64 residual
+// iterative refinement.
 #include "sod_internal.cuh"
 #include <algorithm>
 #include <cmath>
 #include <vector>
 
+namespace sod {
+namespace cg {
+
+constexpr int kBlock = 256;
+#ifndef SOD_LAP_EPB
+#define SOD_LAP_EPB 4
+#endif
+#ifndef SOD_LAP_MINB
+#define SOD_LAP_MINB 6
+#endif
+constexpr int EPB = SOD_LAP_EPB;  // elements per CTA of the element kernel
+constexpr int NMET = 6;     // M00, M01, M02, M11, M12, M22
+constexpr int kBatch = 16;  // CG iterations per graph replay
+
+// device scalar slots
+enum {
+  S_Q1 = 0, S_Q2, S_T1, S_NUM, S_ALPHA, S_BETA, S_BNORM2, S_TOL, S_ITER, S_MAXIT, S_DONE, S_COUNT
+};
+
+template <typename T>
+struct DT {
+  T d[NP1][NP1];
+};
+
+}  // namespace cg
+}  // namespace sod
+
 struct SodPoisson {
   SodMesh* mesh = nullptr;
-  int64_t n = 0, nnz = 0;
+  int64_t n = 0, nelem = 0;
   int pin = 0;
-  int32_t* rowptr = nullptr;
-  int32_t* col = nullptr;
-  double* val = nullptr;
-  float* val32 = nullptr;
+  double* met = nullptr;   // [e][6][64]  gpvol He^T He
+  float* met32 = nullptr;
   double* diag = nullptr;
-  // CG work vectors (FP64) and inner FP32 vectors
-  double *x = nullptr, *r = nullptr, *p = nullptr, *q = nullptr, *z = nullptr, *zold = nullptr, *b = nullptr;
-  float *r32 = nullptr, *p32 = nullptr, *q32 = nullptr, *z32 = nullptr, *zold32 = nullptr, *e32 = nullptr;
   float* diag32 = nullptr;
-  double* part = nullptr;   // block partials [4][nblk]
+  void* rel = nullptr;     // element residuals [e*64 + d] (double, or float for the FP32 sweeps)
+  // CG work vectors (FP64) and inner FP32 vectors
+  double *x = nullptr, *r = nullptr, *p = nullptr, *q = nullptr, *z = nullptr, *b = nullptr;
+  float *r32 = nullptr, *p32 = nullptr, *q32 = nullptr, *z32 = nullptr, *e32 = nullptr;
+  double* part = nullptr;  // block partials [3][nblk]
   int nblk = 0;
-  double* scal = nullptr;   // device scalars
-  double* hscal = nullptr;  // pinned host mirror
+  double* scal = nullptr;  // device scalars
+  double* hscal = nullptr; // pinned host mirror
+  sod::cg::DT<double> D64;
+  sod::cg::DT<float> D32;
+  cudaGraphExec_t batch[2] = {nullptr, nullptr};  // kBatch iterations: FP64, FP32
+  int batch_kernels[2] = {0, 0};
 };
 
 namespace sod {
 namespace cg {
 
-constexpr int kRowThreads = 8;  // threads per CSR row in the SpMV
-constexpr int kBlock = 256;
-
-// device scalar slots
-enum { S_Q1 = 0, S_Q2, S_T1, S_NUM, S_ALPHA, S_BETA, S_Q1NEW, S_BNORM2, S_COUNT };
-
-struct AsmArgs {
-  int n, pin;
-  const int32_t* n2e_ptr;
-  const int32_t* n2e;
-  const int32_t* econn;
-  const double* geo;
-  const int32_t* rowptr;
-  const int32_t* col;
-  double* val;
-  double* diag;
-  DMat D;
-};
-
-__device__ __forceinline__ int find_col(const int32_t* c, int lo, int hi, int key) {
-  while (lo < hi) {
-    int mid = (lo + hi) >> 1;
-    if (c[mid] < key) lo = mid + 1; else hi = mid;
+// M_q = gpvol He^T He at every gauss point (He(r,c) = geo[3r+c])
+__global__ void k_metric(int64_t total, const double* __restrict__ geo, double* __restrict__ met,
+                         float* __restrict__ met32) {
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t e = t / NN;
+    const int d = (int)(t % NN);
+    const double* G = geo + e * NGEO * NN;
+    double H[9];
+#pragma unroll
+    for (int c = 0; c < 9; ++c) H[c] = G[c * NN + d];
+    const double gv = G[9 * NN + d];
+    const int rc[NMET][2] = {{0, 0}, {0, 1}, {0, 2}, {1, 1}, {1, 2}, {2, 2}};
+#pragma unroll
+    for (int c = 0; c < NMET; ++c) {
+      const int a = rc[c][0], b = rc[c][1];
+      const double v = gv * (H[a] * H[b] + H[3 + a] * H[3 + b] + H[6 + a] * H[6 + b]);
+      met[(e * NMET + c) * NN + d] = v;
+      met32[(e * NMET + c) * NN + d] = (float)v;
+    }
   }
-  return lo;
 }
 
-__global__ void k_assemble(const AsmArgs a) {
+// Jacobi diagonal K_aa (unpinned), one thread per node over its elements in ascending order
+__global__ void k_diag(int n, const int32_t* __restrict__ n2e_ptr, const int32_t* __restrict__ n2e,
+                       const double* __restrict__ geo, const DMat D, double* __restrict__ diag,
+                       float* __restrict__ diag32) {
   const int row = blockIdx.x * blockDim.x + threadIdx.x;
-  if (row >= a.n) return;
-  const int rb = a.rowptr[row], re = a.rowptr[row + 1];
+  if (row >= n) return;
   double dsum = 0.0;
-  for (int c = a.n2e_ptr[row]; c < a.n2e_ptr[row + 1]; ++c) {
-    const int pk = a.n2e[c];
+  for (int c = n2e_ptr[row]; c < n2e_ptr[row + 1]; ++c) {
+    const int pk = n2e[c];
     const int e = pk >> 6, da = pk & 63;
     const int ac[3] = {da & 3, (da >> 2) & 3, da >> 4};
-    const double* G = a.geo + (size_t)e * NGEO * NN;
-    const int32_t* conn = a.econn + (size_t)e * NN;
+    const double* G = geo + (size_t)e * NGEO * NN;
     for (int dir = 0; dir < 3; ++dir) {
       for (int m = 0; m < NP1; ++m) {
-        const double c1 = a.D.d[m][ac[dir]];
+        const double c1 = D.d[m][ac[dir]];
         if (c1 == 0.0) continue;
         int gc[3] = {ac[0], ac[1], ac[2]};
         gc[dir] = m;
@@ -93,65 +127,72 @@ __global__ void k_assemble(const AsmArgs a) {
         for (int t = 0; t < 9; ++t) H[t] = G[t * NN + g];
         const double gv = G[9 * NN + g];
         for (int dp = 0; dp < 3; ++dp) {
+          // the entry (a, a) needs the dp-line through q to pass through a
+          if (dp != dir && m != ac[dir]) continue;
           const double Mq = gv * (H[0 * 3 + dir] * H[0 * 3 + dp] + H[1 * 3 + dir] * H[1 * 3 + dp] +
                                   H[2 * 3 + dir] * H[2 * 3 + dp]);
-          for (int np = 0; np < NP1; ++np) {
-            const double c2 = a.D.d[gc[dp]][np];
-            const double v = Mq * c1 * c2;
-            int bc[3] = {gc[0], gc[1], gc[2]};
-            bc[dp] = np;
-            const int b = bc[0] + 4 * bc[1] + 16 * bc[2];
-            if (b == da) dsum += v;
-            const int colg = conn[b];
-            if (row != a.pin && colg != a.pin) {
-              const int pos = find_col(a.col, rb, re, colg);
-              a.val[pos] += v;
-            }
-          }
+          dsum += Mq * c1 * D.d[gc[dp]][ac[dp]];
         }
       }
     }
   }
-  a.diag[row] = dsum;
+  diag[row] = dsum;
+  diag32[row] = (float)dsum;
 }
 
+// element residuals of K x (x(pin) read as 0); skipped once the solve is done
 template <typename T>
-__global__ void k_cast(const double* __restrict__ s, T* __restrict__ d, int64_t n) {
-  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x)
-    d[t] = (T)s[t];
-}
-
-// y = A x (kRowThreads threads per row, fixed-order partial sums) fused with <x, y> partials
-template <typename TV, typename TX>
-__global__ void __launch_bounds__(kBlock) k_spmv_dot(int n, const int32_t* __restrict__ rowptr,
-                                                     const int32_t* __restrict__ col, const TV* __restrict__ val,
-                                                     const TX* __restrict__ x, TX* __restrict__ y,
-                                                     double* __restrict__ part) {
-  const int lane = threadIdx.x & (kRowThreads - 1);
-  const int row = (blockIdx.x * blockDim.x + threadIdx.x) / kRowThreads;
-  double dot = 0.0;
-  TX s = (TX)0;
-  if (row < n) {
-    const int b = rowptr[row], e = rowptr[row + 1];
-    for (int c = b + lane; c < e; c += kRowThreads) s += (TX)val[c] * x[col[c]];
-  }
-  // every lane takes part in the shuffles (rows past n carry zero)
+__global__ void __launch_bounds__(64 * EPB, SOD_LAP_MINB * 4 / EPB) k_lap_elem(int nelem, int pin, const int32_t* __restrict__ econn,
+                                                      const T* __restrict__ met, const DT<T> D,
+                                                      const T* __restrict__ x, T* __restrict__ rel,
+                                                      const double* __restrict__ scal) {
+  if (scal && scal[S_DONE] != 0.0) return;
+  __shared__ T pl[EPB][FSTRIDE];
+  __shared__ T fl[EPB][3][FSTRIDE];
+  __shared__ T Ds[NP1][NP1];
+  const int es = threadIdx.x >> 6, d = threadIdx.x & 63;
+  if (threadIdx.x == 0) {  // constant indices: D stays in the parameter bank
 #pragma unroll
-  for (int o = kRowThreads / 2; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o, kRowThreads);
-  if (row < n && lane == 0) {
-    y[row] = s;
-    dot = (double)x[row] * (double)s;
+    for (int a = 0; a < NP1; ++a)
+#pragma unroll
+      for (int b = 0; b < NP1; ++b) Ds[a][b] = D.d[a][b];
   }
-  // block partial of <x, y>
-  for (int o = 16; o > 0; o >>= 1) dot += __shfl_down_sync(0xffffffffu, dot, o);
-  __shared__ double sh[kBlock / 32];
-  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = dot;
+  const int e = blockIdx.x * EPB + es;
+  const bool act = e < nelem;
+  const int ee = act ? e : nelem - 1;
+  const int i = d & 3, j = (d >> 2) & 3, k = d >> 4, s = sidx(i, j, k);
+  const int nd = econn[(size_t)ee * NN + d];
+  pl[es][s] = nd == pin ? (T)0 : x[nd];
+  T M[NMET];
+#pragma unroll
+  for (int c = 0; c < NMET; ++c) M[c] = met[((size_t)ee * NMET + c) * NN + d];
   __syncthreads();
-  if (threadIdx.x == 0) {
-    double t = 0.0;
-    for (int w = 0; w < kBlock / 32; ++w) t += sh[w];
-    part[blockIdx.x] = t;
+  T Dx[NP1], Dy[NP1], Dz[NP1], DTx[NP1], DTy[NP1], DTz[NP1];
+#pragma unroll
+  for (int m = 0; m < NP1; ++m) {
+    Dx[m] = Ds[i][m]; Dy[m] = Ds[j][m]; Dz[m] = Ds[k][m];
+    DTx[m] = Ds[m][i]; DTy[m] = Ds[m][j]; DTz[m] = Ds[m][k];
   }
+  const T* f = pl[es];
+  T g0 = (T)0, g1 = (T)0, g2 = (T)0;
+#pragma unroll
+  for (int m = 0; m < NP1; ++m) {
+    g0 += Dx[m] * f[sidx(m, j, k)];
+    g1 += Dy[m] * f[sidx(i, m, k)];
+    g2 += Dz[m] * f[sidx(i, j, m)];
+  }
+  fl[es][0][s] = M[0] * g0 + M[1] * g1 + M[2] * g2;
+  fl[es][1][s] = M[1] * g0 + M[3] * g1 + M[4] * g2;
+  fl[es][2][s] = M[2] * g0 + M[4] * g1 + M[5] * g2;
+  __syncthreads();
+  T acc = (T)0;
+#pragma unroll
+  for (int m = 0; m < NP1; ++m) {
+    acc += DTx[m] * fl[es][0][sidx(m, j, k)];
+    acc += DTy[m] * fl[es][1][sidx(i, m, k)];
+    acc += DTz[m] * fl[es][2][sidx(i, j, m)];
+  }
+  if (act) rel[(size_t)e * NN + d] = acc;
 }
 
 template <int NP>
@@ -173,7 +214,34 @@ __device__ __forceinline__ void block_partials(double (&v)[NP], double* part, in
     }
 }
 
-// r = b - Ax (ax given), z = r/M, p = z; partials ||r||^2, <r,z>
+// y = sum of the element residuals of each node, y(pin) = 0; partials of <x, y>
+template <typename T>
+__global__ void __launch_bounds__(kBlock) k_lap_gather(int n, int pin, const int32_t* __restrict__ n2e_ptr,
+                                                      const int32_t* __restrict__ n2e, const T* __restrict__ rel,
+                                                      const T* __restrict__ x, T* __restrict__ y,
+                                                      double* __restrict__ part, const double* __restrict__ scal) {
+  if (scal && scal[S_DONE] != 0.0) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double v[1] = {0.0};
+  if (i < n) {
+    T s = (T)0;
+    int c = n2e_ptr[i];
+    const int c1 = n2e_ptr[i + 1];
+    // four independent loads in flight, summed in ascending element order
+    for (; c + 4 <= c1; c += 4) {
+      const int i0 = n2e[c], i1 = n2e[c + 1], i2 = n2e[c + 2], i3 = n2e[c + 3];
+      const T v0 = rel[i0], v1 = rel[i1], v2 = rel[i2], v3 = rel[i3];
+      s += v0; s += v1; s += v2; s += v3;
+    }
+    for (; c < c1; ++c) s += rel[n2e[c]];
+    if (i == pin) s = (T)0;
+    y[i] = s;
+    v[0] = (double)x[i] * (double)s;
+  }
+  block_partials<1>(v, part, 0);
+}
+
+// r = b - Ax (ax may be null), z = r/M, p = z, x = 0 (if given); partials ||r||^2, <r,z>
 template <typename TV>
 __global__ void __launch_bounds__(kBlock) k_cg_init(int n, const TV* __restrict__ b, const TV* __restrict__ ax,
                                                     const TV* __restrict__ M, TV* r, TV* z, TV* p, TV* x,
@@ -196,6 +264,7 @@ template <typename TV>
 __global__ void __launch_bounds__(kBlock) k_cg_update(int n, const double* __restrict__ scal, TV* x, TV* r, TV* z,
                                                       const TV* __restrict__ p, const TV* __restrict__ q,
                                                       const TV* __restrict__ M, double* part, int stride) {
+  if (scal[S_DONE] != 0.0) return;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   double v[3] = {0.0, 0.0, 0.0};
   if (i < n) {
@@ -214,17 +283,28 @@ __global__ void __launch_bounds__(kBlock) k_cg_update(int n, const double* __res
 
 template <typename TV>
 __global__ void k_cg_pupdate(int n, const double* __restrict__ scal, const TV* __restrict__ z, TV* p) {
+  if (scal[S_DONE] != 0.0) return;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) p[i] = z[i] + (TV)scal[S_BETA] * p[i];
 }
 
+__global__ void k_cg_setup(double* scal, double tol, int max_iter) {
+  scal[S_TOL] = tol;
+  scal[S_MAXIT] = (double)max_iter;
+  scal[S_ITER] = 0.0;
+  scal[S_DONE] = 0.0;
+}
+
 // single-block fixed-order reductions of the partials and the CG scalars
-// mode 0: init  (part0 = ||r||^2 -> T1 and BNORM2, part1 = <r,z> -> Q1)
+// mode 0: init  (part0 = ||r||^2 -> T1 and BNORM2, part1 = <r,z> -> Q1; done if ||b|| = 0)
 // mode 1: alpha (part0 = <p,Ap> -> Q2, alpha = Q1/Q2)
-// mode 2: update(part0 -> T1, part1 -> num, part2 -> Q1new; beta = num/Q1; Q1 = Q1new)
+// mode 2: update(part0 -> T1, part1 -> num, part2 -> Q1new; beta = num/Q1; Q1 = Q1new;
+//                iteration += 1; done if ||r|| < tol ||b|| or the iteration limit is reached)
 // mode 3: norm  (part0 -> T1)
+// modes 1 and 2 do nothing once done
 __global__ void __launch_bounds__(1024) k_cg_scalars(int nblk, const double* __restrict__ part, int stride,
                                                      int mode, double* scal) {
+  if ((mode == 1 || mode == 2) && scal[S_DONE] != 0.0) return;
   __shared__ double sh[3][32];
   const int np = mode == 2 ? 3 : (mode == 0 ? 2 : 1);
   double v[3] = {0.0, 0.0, 0.0};
@@ -241,10 +321,13 @@ __global__ void __launch_bounds__(1024) k_cg_scalars(int nblk, const double* __r
       for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t[k] += sh[k][w];
     if (mode == 0) {
       scal[S_T1] = t[0]; scal[S_BNORM2] = t[0]; scal[S_Q1] = t[1];
+      if (t[0] == 0.0) scal[S_DONE] = 1.0;
     } else if (mode == 1) {
       scal[S_Q2] = t[0]; scal[S_ALPHA] = scal[S_Q1] / t[0];
     } else if (mode == 2) {
       scal[S_T1] = t[0]; scal[S_NUM] = t[1]; scal[S_BETA] = t[1] / scal[S_Q1]; scal[S_Q1] = t[2];
+      scal[S_ITER] += 1.0;
+      if (sqrt(t[0]) < scal[S_TOL] * sqrt(scal[S_BNORM2]) || scal[S_ITER] >= scal[S_MAXIT]) scal[S_DONE] = 1.0;
     } else {
       scal[S_T1] = t[0];
     }
@@ -256,6 +339,10 @@ template <typename T>
 __global__ void k_sub_pin(int n, int pin, const T* __restrict__ a, const T* __restrict__ b, T* out) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) out[i] = (i == pin) ? (T)0 : a[i] - (b ? b[i] : (T)0);
+}
+__global__ void k_cast32(int n, const double* __restrict__ s, float* __restrict__ d) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) d[i] = (float)s[i];
 }
 __global__ void k_axpy_cast(int n, const float* __restrict__ e, double* x) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -272,11 +359,25 @@ __global__ void k_add(int n, const double* __restrict__ a, const double* __restr
 using namespace sod;
 using namespace sod::cg;
 
-static int spmv_grid(int64_t n) { return (int)((n * kRowThreads + kBlock - 1) / kBlock); }
+static int node_grid(int64_t n) { return (int)((n + kBlock - 1) / kBlock); }
 
-template <typename TV, typename TX>
-static int spmv(SodPoisson* P, const TV* val, const TX* x, TX* y, cudaStream_t st) {
-  k_spmv_dot<TV, TX><<<spmv_grid(P->n), kBlock, 0, st>>>((int)P->n, P->rowptr, P->col, val, x, y, P->part);
+// y = K x with <x, y> block partials (part[0..node_grid(n))); scal != null skips once done
+template <typename T>
+static int lap_apply(SodPoisson* P, const T* x, T* y, const double* scal, cudaStream_t st) {
+  const SodMesh* m = P->mesh;
+  const int E = (int)P->nelem;
+  const T* met;
+  const DT<T>* D;
+  if constexpr (sizeof(T) == 8) {
+    met = P->met; D = &P->D64;
+  } else {
+    met = P->met32; D = &P->D32;
+  }
+  T* rel = static_cast<T*>(P->rel);
+  k_lap_elem<T><<<(E + EPB - 1) / EPB, 64 * EPB, 0, st>>>(E, P->pin, m->econn, met, *D, x, rel, scal);
+  SOD_CHECK_LAUNCH();
+  k_lap_gather<T><<<node_grid(P->n), kBlock, 0, st>>>((int)P->n, P->pin, m->n2e_ptr, m->n2e, rel, x, y, P->part,
+                                                      scal);
   SOD_CHECK_LAUNCH();
   return SOD_OK;
 }
@@ -287,45 +388,104 @@ static int scalars(SodPoisson* P, int nblk, int mode, cudaStream_t st) {
   return SOD_OK;
 }
 
-static int read_T1(SodPoisson* P, cudaStream_t st, double* T1) {
+static int read_scalars(SodPoisson* P, cudaStream_t st) {
   SOD_CUDA(cudaMemcpyAsync(P->hscal, P->scal, sizeof(double) * S_COUNT, cudaMemcpyDeviceToHost, st));
   SOD_CUDA(cudaStreamSynchronize(st));
-  *T1 = P->hscal[S_T1];
   return SOD_OK;
 }
 
-// Jacobi PCG on A e = rhs (vectors TV, values TM) in the reference's iteration order; e starts
-// at 0.  Stops when ||r|| < tol * ||r0|| or after max_iter; returns the iteration count.
-template <typename TV, typename TM>
-static int pcg(SodPoisson* P, const TM* val, const TV* M, const TV* rhs, TV* e, TV* r, TV* z, TV* p, TV* q,
-               int max_iter, double tol, cudaStream_t st, int* iters, double* rel) {
+template <typename TV>
+struct CgVecs {
+  const TV* M; TV *e, *r, *z, *p, *q;
+};
+
+// FP64: the solve's own vectors; FP32 sweep: its residual overwrites its right-hand side r32
+template <typename TV> static CgVecs<TV> vecs(SodPoisson* P);
+template <> CgVecs<double> vecs<double>(SodPoisson* P) { return {P->diag, P->x, P->r, P->z, P->p, P->q}; }
+template <> CgVecs<float> vecs<float>(SodPoisson* P) { return {P->diag32, P->e32, P->r32, P->z32, P->p32, P->q32}; }
+
+// one CG iteration after the init (matvec, alpha, update, beta + stop test, p update)
+template <typename TV>
+static int cg_iteration(SodPoisson* P, const CgVecs<TV>& v, cudaStream_t st) {
   const int n = (int)P->n;
-  const int gb = (n + kBlock - 1) / kBlock;
-  k_cg_init<TV><<<gb, kBlock, 0, st>>>(n, rhs, (const TV*)nullptr, M, r, z, p, e, P->part, P->nblk);
+  const int gb = node_grid(n);
+  if (int rc = lap_apply<TV>(P, v.p, v.q, P->scal, st)) return rc;
+  if (int rc = scalars(P, gb, 1, st)) return rc;
+  k_cg_update<TV><<<gb, kBlock, 0, st>>>(n, P->scal, v.e, v.r, v.z, v.p, v.q, v.M, P->part, P->nblk);
+  SOD_CHECK_LAUNCH();
+  if (int rc = scalars(P, gb, 2, st)) return rc;
+  k_cg_pupdate<TV><<<gb, kBlock, 0, st>>>(n, P->scal, v.z, v.p);
+  SOD_CHECK_LAUNCH();
+  return SOD_OK;
+}
+
+// the graph of kBatch iterations for vector type TV (built once per handle)
+template <typename TV>
+static int batch_graph(SodPoisson* P, cudaGraphExec_t* exec, int* nkernels) {
+  const int slot = sizeof(TV) == 8 ? 0 : 1;
+  if (!P->batch[slot]) {
+    const CgVecs<TV> v = vecs<TV>(P);
+    cudaStream_t cap;
+    SOD_CUDA(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+    cudaGraph_t graph;
+    const int64_t before = g_launches.load();
+    cudaError_t be = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
+    int rc = SOD_OK;
+    if (be == cudaSuccess)
+      for (int t = 0; t < kBatch && rc == SOD_OK; ++t) rc = cg_iteration<TV>(P, v, cap);
+    cudaError_t ce = be == cudaSuccess ? cudaStreamEndCapture(cap, &graph) : be;
+    cudaStreamDestroy(cap);
+    const int nk = (int)(g_launches.load() - before);
+    g_launches.fetch_sub(nk);
+    if (rc) return rc;
+    if (ce != cudaSuccess) {
+      set_error("CG graph capture failed: %s", cudaGetErrorString(ce));
+      return SOD_ERR_CUDA;
+    }
+    cudaError_t ie = cudaGraphInstantiate(&P->batch[slot], graph, 0);
+    cudaGraphDestroy(graph);
+    if (ie != cudaSuccess) {
+      P->batch[slot] = nullptr;
+      set_error("CG graph instantiate failed: %s", cudaGetErrorString(ie));
+      return SOD_ERR_CUDA;
+    }
+    P->batch_kernels[slot] = nk;
+  }
+  *exec = P->batch[slot];
+  *nkernels = P->batch_kernels[slot];
+  return SOD_OK;
+}
+
+// Jacobi PCG on A e = rhs in the reference's iteration order; e starts at 0.  Stops when
+// ||r|| < tol * ||r0|| or after max_iter; returns the iteration count and ||r|| / ||r0||.
+template <typename TV>
+static int pcg(SodPoisson* P, const CgVecs<TV>& v, const TV* rhs, int max_iter, double tol, cudaStream_t st,
+               int* iters, double* rel) {
+  const int n = (int)P->n;
+  const int gb = node_grid(n);
+  cudaGraphExec_t exec = nullptr;
+  int nk = 0;
+  if (int rc = batch_graph<TV>(P, &exec, &nk)) return rc;
+  k_cg_setup<<<1, 1, 0, st>>>(P->scal, tol, max_iter);
+  SOD_CHECK_LAUNCH();
+  k_cg_init<TV><<<gb, kBlock, 0, st>>>(n, rhs, (const TV*)nullptr, v.M, v.r, v.z, v.p, v.e, P->part, P->nblk);
   SOD_CHECK_LAUNCH();
   if (int rc = scalars(P, gb, 0, st)) return rc;
-  double T1 = 0.0;
-  if (int rc = read_T1(P, st, &T1)) return rc;
+  if (int rc = read_scalars(P, st)) return rc;
   const double auxB = std::sqrt(P->hscal[S_BNORM2]);
-  int it = 0;
   if (auxB == 0.0) {
     *iters = 0;
     *rel = 0.0;
     return SOD_OK;
   }
-  for (it = 1; it <= max_iter; ++it) {
-    if (int rc = spmv<TM, TV>(P, val, p, q, st)) return rc;
-    if (int rc = scalars(P, spmv_grid(n), 1, st)) return rc;
-    k_cg_update<TV><<<gb, kBlock, 0, st>>>(n, P->scal, e, r, z, p, q, M, P->part, P->nblk);
-    SOD_CHECK_LAUNCH();
-    if (int rc = scalars(P, gb, 2, st)) return rc;
-    if (int rc = read_T1(P, st, &T1)) return rc;
-    if (std::sqrt(T1) < tol * auxB) break;
-    k_cg_pupdate<TV><<<gb, kBlock, 0, st>>>(n, P->scal, z, p);
-    SOD_CHECK_LAUNCH();
+  // bounded: every replay advances the counter by kBatch until the limit sets done
+  for (int guard = 0; guard <= max_iter / kBatch + 1 && P->hscal[S_DONE] == 0.0; ++guard) {
+    SOD_CUDA(cudaGraphLaunch(exec, st));
+    g_launches.fetch_add(nk);
+    if (int rc = read_scalars(P, st)) return rc;
   }
-  *iters = it > max_iter ? max_iter : it;
-  *rel = std::sqrt(T1) / auxB;
+  *iters = (int)P->hscal[S_ITER];
+  *rel = std::sqrt(P->hscal[S_T1]) / auxB;
   return SOD_OK;
 }
 
@@ -333,8 +493,10 @@ extern "C" {
 
 void sod_poisson_destroy(SodPoisson* P) {
   if (!P) return;
-  void* ptrs[] = {P->rowptr, P->col, P->val, P->val32, P->diag, P->x, P->r, P->p, P->q, P->z, P->zold, P->b,
-                  P->r32, P->p32, P->q32, P->z32, P->zold32, P->e32, P->diag32, P->part, P->scal};
+  for (cudaGraphExec_t& g : P->batch)
+    if (g) cudaGraphExecDestroy(g);
+  void* ptrs[] = {P->met, P->met32, P->diag, P->diag32, P->rel, P->x, P->r, P->p, P->q, P->z, P->b,
+                  P->r32, P->p32, P->q32, P->z32, P->e32, P->part, P->scal};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (P->hscal) cudaFreeHost(P->hscal);
@@ -344,83 +506,39 @@ void sod_poisson_destroy(SodPoisson* P) {
 int sod_poisson_create(SodMesh* m, SodPoisson** out) {
   SOD_ARG(m && out, "mesh/out null");
   *out = nullptr;
-  const int N = m->npoin, E = m->nelem;
-  const int pin = 0;
-  // host copies of the connectivity and node->element map
-  std::vector<int32_t> econn((size_t)E * NN), nptr(N + 1), nidx((size_t)E * NN);
-  SOD_CUDA(cudaMemcpy(econn.data(), m->econn, sizeof(int32_t) * econn.size(), cudaMemcpyDeviceToHost));
-  SOD_CUDA(cudaMemcpy(nptr.data(), m->n2e_ptr, sizeof(int32_t) * (N + 1), cudaMemcpyDeviceToHost));
-  SOD_CUDA(cudaMemcpy(nidx.data(), m->n2e, sizeof(int32_t) * nidx.size(), cudaMemcpyDeviceToHost));
-  // local pairs sharing at least one ijk index (the structural nonzeros of K^e)
-  std::vector<int> share[NN];
-  for (int a = 0; a < NN; ++a)
-    for (int b = 0; b < NN; ++b)
-      if ((a & 3) == (b & 3) || ((a >> 2) & 3) == ((b >> 2) & 3) || (a >> 4) == (b >> 4)) share[a].push_back(b);
-  std::vector<int32_t> rowptr(N + 1, 0);
-  std::vector<int32_t> tmp;
-  tmp.reserve(1024);
-  auto row_cols = [&](int n) {
-    tmp.clear();
-    if (n == pin) return;
-    for (int c = nptr[n]; c < nptr[n + 1]; ++c) {
-      const int e = nidx[c] >> 6, da = nidx[c] & 63;
-      for (int b : share[da]) {
-        const int32_t cg = econn[(size_t)e * NN + b];
-        if (cg != pin) tmp.push_back(cg);
-      }
-    }
-    std::sort(tmp.begin(), tmp.end());
-    tmp.erase(std::unique(tmp.begin(), tmp.end()), tmp.end());
-  };
-  for (int n = 0; n < N; ++n) {
-    row_cols(n);
-    rowptr[n + 1] = rowptr[n] + (int32_t)tmp.size();
-    if ((int64_t)rowptr[n + 1] > (int64_t)INT32_MAX - 4096) {
-      set_error("Poisson CSR exceeds int32 indices");
-      return SOD_ERR_UNSUPPORTED;
-    }
-  }
-  const int64_t nnz = rowptr[N];
-  std::vector<int32_t> col(nnz);
-  for (int n = 0; n < N; ++n) {
-    row_cols(n);
-    std::copy(tmp.begin(), tmp.end(), col.begin() + rowptr[n]);
-  }
+  const int64_t N = m->npoin, E = m->nelem;
   SodPoisson* P = new SodPoisson();
-  P->mesh = m; P->n = N; P->nnz = nnz; P->pin = pin;
-  P->nblk = std::max(spmv_grid(N), (N + kBlock - 1) / kBlock);
+  P->mesh = m; P->n = N; P->nelem = E; P->pin = 0;
+  P->nblk = node_grid(N);
+  for (int a = 0; a < NP1; ++a)
+    for (int b = 0; b < NP1; ++b) {
+      P->D64.d[a][b] = m->D.d[a][b];
+      P->D32.d[a][b] = (float)m->D.d[a][b];
+    }
   auto fail = [&](const char* what) {
     set_error("sod_poisson_create: %s failed", what);
     sod_poisson_destroy(P);
     return SOD_ERR_NOMEM;
   };
 #define PALLOC(ptr, bytes) if (cudaMalloc(&(ptr), (bytes)) != cudaSuccess) return fail(#ptr)
-  PALLOC(P->rowptr, sizeof(int32_t) * (N + 1));
-  PALLOC(P->col, sizeof(int32_t) * (nnz > 0 ? nnz : 1));
-  PALLOC(P->val, sizeof(double) * (nnz > 0 ? nnz : 1));
-  PALLOC(P->val32, sizeof(float) * (nnz > 0 ? nnz : 1));
+  PALLOC(P->met, sizeof(double) * NMET * NN * E);
+  PALLOC(P->met32, sizeof(float) * NMET * NN * E);
+  PALLOC(P->rel, sizeof(double) * NN * E);
   PALLOC(P->diag, sizeof(double) * N);
   PALLOC(P->diag32, sizeof(float) * N);
-  for (double** v : {&P->x, &P->r, &P->p, &P->q, &P->z, &P->zold, &P->b}) PALLOC(*v, sizeof(double) * N);
-  for (float** v : {&P->r32, &P->p32, &P->q32, &P->z32, &P->zold32, &P->e32}) PALLOC(*v, sizeof(float) * N);
-  PALLOC(P->part, sizeof(double) * 4 * P->nblk);
+  for (double** v : {&P->x, &P->r, &P->p, &P->q, &P->z, &P->b}) PALLOC(*v, sizeof(double) * N);
+  for (float** v : {&P->r32, &P->p32, &P->q32, &P->z32, &P->e32}) PALLOC(*v, sizeof(float) * N);
+  PALLOC(P->part, sizeof(double) * 3 * P->nblk);
   PALLOC(P->scal, sizeof(double) * S_COUNT);
 #undef PALLOC
   if (cudaMallocHost(&P->hscal, sizeof(double) * S_COUNT) != cudaSuccess) return fail("hscal");
-  cudaMemcpy(P->rowptr, rowptr.data(), sizeof(int32_t) * (N + 1), cudaMemcpyHostToDevice);
-  cudaMemcpy(P->col, col.data(), sizeof(int32_t) * nnz, cudaMemcpyHostToDevice);
-  cudaMemset(P->val, 0, sizeof(double) * (nnz > 0 ? nnz : 1));
-  AsmArgs a;
-  a.n = N; a.pin = pin; a.n2e_ptr = m->n2e_ptr; a.n2e = m->n2e; a.econn = m->econn; a.geo = m->geo64;
-  a.rowptr = P->rowptr; a.col = P->col; a.val = P->val; a.diag = P->diag; a.D = m->D;
-  k_assemble<<<(N + 127) / 128, 128>>>(a);
-  g_launches.fetch_add(1);
-  k_cast<float><<<1024, 256>>>(P->val, P->val32, nnz);
-  k_cast<float><<<256, 256>>>(P->diag, P->diag32, N);
+  k_metric<<<1184, 256>>>(E * NN, m->geo64, P->met, P->met32);
+  k_diag<<<node_grid(N), kBlock>>>((int)N, m->n2e_ptr, m->n2e, m->geo64, m->D, P->diag, P->diag32);
   g_launches.fetch_add(2);
   cudaError_t err = cudaDeviceSynchronize();
+  if (err == cudaSuccess) err = cudaGetLastError();
   if (err != cudaSuccess) {
-    set_error("Poisson assembly: %s", cudaGetErrorString(err));
+    set_error("Poisson setup: %s", cudaGetErrorString(err));
     sod_poisson_destroy(P);
     return SOD_ERR_CUDA;
   }
@@ -428,15 +546,9 @@ int sod_poisson_create(SodMesh* m, SodPoisson** out) {
   return SOD_OK;
 }
 
-int sod_poisson_nnz(SodPoisson* P, int64_t* nnz) {
-  SOD_ARG(P && nnz, "null argument");
-  *nnz = P->nnz;
-  return SOD_OK;
-}
-
 int sod_poisson_apply(SodPoisson* P, const double* x, double* y, sod_stream_t stream) {
   SOD_ARG(P && x && y, "null argument");
-  return spmv<double, double>(P, P->val, x, y, (cudaStream_t)stream);
+  return lap_apply<double>(P, x, y, nullptr, (cudaStream_t)stream);
 }
 
 int sod_poisson_diag(SodPoisson* P, double* d, sod_stream_t stream) {
@@ -450,15 +562,15 @@ int sod_conjgrad_pressure(SodPoisson* P, const double* Rp0, double* R, int max_i
   SOD_ARG(P && Rp0 && R && max_iter > 0 && tol > 0.0, "conjgrad arguments");
   cudaStream_t st = (cudaStream_t)stream;
   const int n = (int)P->n;
-  const int gb = (n + kBlock - 1) / kBlock;
+  const int gb = node_grid(n);
   // b = R - A x0, b(pin) = 0 (mod_solver_incomp.f90:307-317)
-  if (int rc = spmv<double, double>(P, P->val, Rp0, P->q, st)) return rc;
+  if (int rc = lap_apply<double>(P, Rp0, P->q, nullptr, st)) return rc;
   k_sub_pin<double><<<gb, kBlock, 0, st>>>(n, P->pin, R, P->q, P->b);
   SOD_CHECK_LAUNCH();
   int iters = 0;
   double rel = 0.0;
   if (!mixed) {
-    int rc = pcg<double, double>(P, P->val, P->diag, P->b, P->x, P->r, P->z, P->p, P->q, max_iter, tol, st, &iters, &rel);
+    int rc = pcg<double>(P, vecs<double>(P), P->b, max_iter, tol, st, &iters, &rel);
     if (rc) return rc;
   } else {
     // FP64 residual iterative refinement around FP32 Jacobi-PCG sweeps
@@ -466,31 +578,29 @@ int sod_conjgrad_pressure(SodPoisson* P, const double* Rp0, double* R, int max_i
                                              P->part, P->nblk);
     SOD_CHECK_LAUNCH();
     if (int rc = scalars(P, gb, 0, st)) return rc;
-    double T1 = 0.0;
-    if (int rc = read_T1(P, st, &T1)) return rc;
+    if (int rc = read_scalars(P, st)) return rc;
     const double bnorm = std::sqrt(P->hscal[S_BNORM2]);
     rel = bnorm > 0.0 ? 1.0 : 0.0;
     for (int outer = 0; outer < 64 && rel >= tol && iters < max_iter; ++outer) {
       // each FP32 sweep is asked for the remaining reduction, but not below what FP32 resolves
       const double inner_tol = std::max(0.5 * tol / rel, 2e-6);
-      k_cast<float><<<gb, kBlock, 0, st>>>(P->r, P->r32, n);
+      k_cast32<<<gb, kBlock, 0, st>>>(n, P->r, P->r32);
       SOD_CHECK_LAUNCH();
       int it_in = 0;
       double rel_in = 0.0;
-      int rc = pcg<float, float>(P, P->val32, P->diag32, P->r32, P->e32, P->zold32, P->z32, P->p32, P->q32,
-                                 max_iter - iters, inner_tol, st, &it_in, &rel_in);
+      int rc = pcg<float>(P, vecs<float>(P), P->r32, max_iter - iters, inner_tol, st, &it_in, &rel_in);
       if (rc) return rc;
       iters += it_in;
       k_axpy_cast<<<gb, kBlock, 0, st>>>(n, P->e32, P->x);
       SOD_CHECK_LAUNCH();
       // r = b - A x in FP64, ||r||^2
-      if (int rc2 = spmv<double, double>(P, P->val, P->x, P->q, st)) return rc2;
+      if (int rc2 = lap_apply<double>(P, P->x, P->q, nullptr, st)) return rc2;
       k_cg_init<double><<<gb, kBlock, 0, st>>>(n, P->b, P->q, P->diag, P->r, P->z, P->p, (double*)nullptr, P->part,
                                                P->nblk);
       SOD_CHECK_LAUNCH();
       if (int rc3 = scalars(P, gb, 3, st)) return rc3;
-      if (int rc4 = read_T1(P, st, &T1)) return rc4;
-      rel = std::sqrt(T1) / bnorm;
+      if (int rc4 = read_scalars(P, st)) return rc4;
+      rel = std::sqrt(P->hscal[S_T1]) / bnorm;
     }
   }
   // R = x0 + x (mod_solver_incomp.f90:428-430)

@@ -341,9 +341,8 @@ class Sod2dPoisson:
         _lib.check(_lib.load().sod_poisson_create(mesh.handle, C.byref(h)))
         self.handle = h
         self.n = mesh.npoin
-        nnz = C.c_int64(0)
-        _lib.check(_lib.load().sod_poisson_nnz(h, C.byref(nnz)))
-        self.nnz = nnz.value
+        self.nelem = mesh.nelem
+        self._mesh = mesh  # the handle points into the mesh
 
     def close(self):
         if getattr(self, "handle", None) and self.handle.value:

@@ -61,3 +61,21 @@ def test_cg_mixed_refinement(penv):
     r = b.clone(); r[0] = 0.0
     res = (r - P.apply(x32)).norm().item() / r.norm().item()
     assert res < 1e-9, res
+
+
+def test_cg_iteration_limit(penv):
+    """The device-side iteration limit ends the batched replays at exactly max_iter (not a
+    multiple of the 16-iteration batch) and the call reports non-convergence."""
+    torch, P, rhs = penv["torch"], penv["P"], penv["rhs"]
+    b = torch.from_numpy(rhs).cuda()
+    with pytest.raises(RuntimeError, match="after 21 iterations"):
+        P.solve(b, tol=1e-10, max_iter=21)
+    # the handle stays usable: the next solve converges as before
+    _, it, rel = P.solve(b, tol=1e-10)
+    assert rel < 1e-10 and it > 21
+
+
+def test_cg_zero_rhs(penv):
+    torch, P = penv["torch"], penv["P"]
+    x, it, rel = P.solve(torch.zeros(P.n, dtype=torch.float64, device="cuda"), tol=1e-10)
+    assert it == 0 and rel == 0.0 and float(x.abs().max()) == 0.0
