@@ -8,12 +8,16 @@
 // M_q = gpvol_q He_q^T He_q is formed once per gauss point at setup (6 values: the reference
 // re-reads He and gpvol, 10 values, on every product), in FP64 and in an FP32 copy.
 //
-// One product is two kernels.  k_lap_elem: one thread per gauss point, EPB elements per CTA;
-// the element's p is gathered into shared memory, the three line derivatives and F are formed
-// in registers, F goes back to shared memory and the transposed line sums give the element
-// residual, stored as rel[e*64 + d].  k_lap_gather: one thread per node sums its element
-// residuals through the node->element CSR in ascending element order (deterministic; the
-// reference uses atomics) and adds <p, Kp> to per-block partials.
+// One product is two kernels.  k_lap_elem_async: one thread per gauss point, EPB elements per
+// group, persistent CTAs (SMs x 3) that stream the metric and connectivity of their next 4
+// groups through a cp.async shared-memory ring and gather the next group's p during the
+// current group's arithmetic; the element's p goes to shared memory, the three line
+// derivatives and F are formed in registers, F goes back to shared memory and the transposed
+// line sums give the element residual, stored as rel[e*64 + d].  The kernel is bound by the
+// bytes it keeps in flight: one group per CTA (k_lap_elem, the fallback when the occupancy
+// query gives no resident CTA) reaches 4.1 TB/s on the same bytes.  k_lap_gather: one thread
+// per node sums its element residuals through the node->element CSR in ascending element
+// order (deterministic; the reference uses atomics) and adds <p, Kp> to per-block partials.
 //
 // The Jacobi diagonal is eval_laplacian_diag (mod_operators.f90:417-461): the unpinned K_aa.
 //
@@ -34,13 +38,10 @@ namespace sod {
 namespace cg {
 
 constexpr int kBlock = 256;
-#ifndef SOD_LAP_EPB
-#define SOD_LAP_EPB 4
-#endif
-#ifndef SOD_LAP_MINB
-#define SOD_LAP_MINB 6
-#endif
-constexpr int EPB = SOD_LAP_EPB;  // elements per CTA of the element kernel
+constexpr int EPB = 4;      // elements per CTA of the element kernels
+constexpr int NSTAGE = 4;   // cp.async ring stages of the streamed element kernel
+constexpr int kRingCtas = 3; // its resident CTAs per SM (3 x 64.6 KB shared memory in FP64)
+constexpr int kGather = 8;   // residual loads in flight per node in the gather
 constexpr int NMET = 6;     // M00, M01, M02, M11, M12, M22
 constexpr int kBatch = 16;  // CG iterations per graph replay
 
@@ -77,6 +78,7 @@ struct SodPoisson {
   sod::cg::DT<float> D32;
   cudaGraphExec_t batch[2] = {nullptr, nullptr};  // kBatch iterations: FP64, FP32
   int batch_kernels[2] = {0, 0};
+  int ring_grid[2] = {0, 0};  // streamed element-kernel grid: FP64, FP32 (SMs x resident CTAs)
 };
 
 namespace sod {
@@ -142,7 +144,7 @@ __global__ void k_diag(int n, const int32_t* __restrict__ n2e_ptr, const int32_t
 
 // element residuals of K x (x(pin) read as 0); skipped once the solve is done
 template <typename T>
-__global__ void __launch_bounds__(64 * EPB, SOD_LAP_MINB * 4 / EPB) k_lap_elem(int nelem, int pin, const int32_t* __restrict__ econn,
+__global__ void __launch_bounds__(64 * EPB) k_lap_elem(int nelem, int pin, const int32_t* __restrict__ econn,
                                                       const T* __restrict__ met, const DT<T> D,
                                                       const T* __restrict__ x, T* __restrict__ rel,
                                                       const double* __restrict__ scal) {
@@ -195,6 +197,125 @@ __global__ void __launch_bounds__(64 * EPB, SOD_LAP_MINB * 4 / EPB) k_lap_elem(i
   if (act) rel[(size_t)e * NN + d] = acc;
 }
 
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+// Streamed form of k_lap_elem: persistent CTAs, the metric and connectivity of the next
+// NSTAGE element groups copied into a shared-memory ring by cp.async (16-byte chunks, L1
+// bypassed), so that several groups' bytes are in flight per CTA, and the p values of the
+// next group gathered during the current group's arithmetic.  Same arithmetic and order as
+// k_lap_elem (bitwise equal results).  Stage layout: metric [EPB][6][64] T, then
+// connectivity [EPB][64] int32.
+template <typename T, int NSTAGE>
+struct LapRing {
+  static constexpr int kMetBytes = EPB * NMET * NN * (int)sizeof(T);
+  static constexpr int kConnBytes = EPB * NN * 4;
+  static constexpr int kStage = kMetBytes + kConnBytes;
+  static constexpr int kBytes = NSTAGE * kStage;
+};
+
+template <typename T, int NSTAGE>
+__global__ void __launch_bounds__(64 * EPB, kRingCtas) k_lap_elem_async(int nelem, int pin, const int32_t* __restrict__ econn,
+                                                            const T* __restrict__ met, const DT<T> D,
+                                                            const T* __restrict__ x, T* __restrict__ rel,
+                                                            const double* __restrict__ scal) {
+  using Ring = LapRing<T, NSTAGE>;
+  if (scal && scal[S_DONE] != 0.0) return;
+  const int ngroups = (nelem + EPB - 1) / EPB;
+  if ((int)blockIdx.x >= ngroups) return;
+  extern __shared__ __align__(16) unsigned char ring[];
+  __shared__ T pl[EPB][FSTRIDE];
+  __shared__ T fl[EPB][3][FSTRIDE];
+  __shared__ T Ds[NP1][NP1];
+  const int tid = threadIdx.x;
+  const int es = tid >> 6, d = tid & 63;
+  if (tid == 0) {  // constant indices: D stays in the parameter bank
+#pragma unroll
+    for (int a = 0; a < NP1; ++a)
+#pragma unroll
+      for (int b = 0; b < NP1; ++b) Ds[a][b] = D.d[a][b];
+  }
+  const int i = d & 3, j = (d >> 2) & 3, k = d >> 4, s = sidx(i, j, k);
+  // copy the metric and connectivity of the t-th group of this CTA into its stage (all threads)
+  auto issue = [&](int t) {
+    const int g = blockIdx.x + t * gridDim.x;
+    if (g < ngroups) {
+      const int nval = min(EPB, nelem - g * EPB);
+      unsigned char* st = ring + (t % NSTAGE) * Ring::kStage;
+      const unsigned char* gm = reinterpret_cast<const unsigned char*>(met) + (size_t)g * Ring::kMetBytes;
+      const int mchunks = nval * NMET * NN * (int)sizeof(T) / 16;
+      for (int q = tid; q < mchunks; q += 64 * EPB) cp_async16(st + 16 * q, gm + 16 * (size_t)q);
+      const unsigned char* gc = reinterpret_cast<const unsigned char*>(econn) + (size_t)g * EPB * NN * 4;
+      const int cchunks = nval * NN * 4 / 16;
+      for (int q = tid; q < cchunks; q += 64 * EPB) cp_async16(st + Ring::kMetBytes + 16 * q, gc + 16 * (size_t)q);
+    }
+    cp_async_commit();
+  };
+  auto node_of = [&](int t) {  // this thread's node in the t-th group (0 past the last element)
+    const int e = (blockIdx.x + t * gridDim.x) * EPB + es;
+    const int32_t* cs = reinterpret_cast<const int32_t*>(ring + (t % NSTAGE) * Ring::kStage + Ring::kMetBytes);
+    return e < nelem ? cs[es * NN + d] : 0;
+  };
+  for (int t = 0; t < NSTAGE; ++t) issue(t);
+  cp_async_wait<NSTAGE - 1>();  // group 0 landed
+  __syncthreads();
+  // this thread's D rows, read once for all its groups
+  T Dx[NP1], Dy[NP1], Dz[NP1], DTx[NP1], DTy[NP1], DTz[NP1];
+#pragma unroll
+  for (int m = 0; m < NP1; ++m) {
+    Dx[m] = Ds[i][m]; Dy[m] = Ds[j][m]; Dz[m] = Ds[k][m];
+    DTx[m] = Ds[m][i]; DTy[m] = Ds[m][j]; DTz[m] = Ds[m][k];
+  }
+  int nd = node_of(0);
+  T xv = nd == pin ? (T)0 : x[nd];
+  for (int t = 0;; ++t) {
+    const int g = blockIdx.x + t * gridDim.x;
+    if (g >= ngroups) break;
+    const T* ms = reinterpret_cast<const T*>(ring + (t % NSTAGE) * Ring::kStage) + es * NMET * NN + d;
+    T M[NMET];
+#pragma unroll
+    for (int c = 0; c < NMET; ++c) M[c] = ms[c * NN];
+    pl[es][s] = xv;
+    cp_async_wait<NSTAGE - 2>();  // this thread's copies of group t + 1 landed
+    __syncthreads();              // everyone's copies of group t + 1 and the p line visible
+    T xv_n = (T)0;
+    if (g + (int)gridDim.x < ngroups) {
+      const int ndn = node_of(t + 1);
+      xv_n = ndn == pin ? (T)0 : x[ndn];
+    }
+    const T* f = pl[es];
+    T g0 = (T)0, g1 = (T)0, g2 = (T)0;
+#pragma unroll
+    for (int m = 0; m < NP1; ++m) {
+      g0 += Dx[m] * f[sidx(m, j, k)];
+      g1 += Dy[m] * f[sidx(i, m, k)];
+      g2 += Dz[m] * f[sidx(i, j, m)];
+    }
+    fl[es][0][s] = M[0] * g0 + M[1] * g1 + M[2] * g2;
+    fl[es][1][s] = M[1] * g0 + M[3] * g1 + M[4] * g2;
+    fl[es][2][s] = M[2] * g0 + M[4] * g1 + M[5] * g2;
+    __syncthreads();  // fluxes visible; stage t no longer read by anyone
+    T acc = (T)0;
+#pragma unroll
+    for (int m = 0; m < NP1; ++m) {
+      acc += DTx[m] * fl[es][0][sidx(m, j, k)];
+      acc += DTy[m] * fl[es][1][sidx(i, m, k)];
+      acc += DTz[m] * fl[es][2][sidx(i, j, m)];
+    }
+    const int e = g * EPB + es;
+    if (e < nelem) rel[(size_t)e * NN + d] = acc;
+    issue(t + NSTAGE);  // refill stage t
+    xv = xv_n;
+  }
+  cp_async_wait<0>();  // no copy outlives the CTA
+}
+
+
 template <int NP>
 __device__ __forceinline__ void block_partials(double (&v)[NP], double* part, int stride) {
   __shared__ double sh[NP][kBlock / 32];
@@ -227,13 +348,19 @@ __global__ void __launch_bounds__(kBlock) k_lap_gather(int n, int pin, const int
     T s = (T)0;
     int c = n2e_ptr[i];
     const int c1 = n2e_ptr[i + 1];
-    // four independent loads in flight, summed in ascending element order
-    for (; c + 4 <= c1; c += 4) {
-      const int i0 = n2e[c], i1 = n2e[c + 1], i2 = n2e[c + 2], i3 = n2e[c + 3];
-      const T v0 = rel[i0], v1 = rel[i1], v2 = rel[i2], v3 = rel[i3];
-      s += v0; s += v1; s += v2; s += v3;
+    // up to kGather independent loads in flight (a hexahedral vertex has 8 elements), summed in
+    // ascending element order
+    for (; c < c1; c += kGather) {
+      int ix[kGather];
+#pragma unroll
+      for (int u = 0; u < kGather; ++u) ix[u] = c + u < c1 ? n2e[c + u] : -1;
+      T v[kGather];
+#pragma unroll
+      for (int u = 0; u < kGather; ++u) v[u] = ix[u] >= 0 ? rel[ix[u]] : (T)0;
+#pragma unroll
+      for (int u = 0; u < kGather; ++u)
+        if (ix[u] >= 0) s += v[u];
     }
-    for (; c < c1; ++c) s += rel[n2e[c]];
     if (i == pin) s = (T)0;
     y[i] = s;
     v[0] = (double)x[i] * (double)s;
@@ -374,7 +501,14 @@ static int lap_apply(SodPoisson* P, const T* x, T* y, const double* scal, cudaSt
     met = P->met32; D = &P->D32;
   }
   T* rel = static_cast<T*>(P->rel);
-  k_lap_elem<T><<<(E + EPB - 1) / EPB, 64 * EPB, 0, st>>>(E, P->pin, m->econn, met, *D, x, rel, scal);
+  const int ngroups = (E + EPB - 1) / EPB;
+  const int pg = P->ring_grid[sizeof(T) == 8 ? 0 : 1];
+  if (pg > 0) {
+    k_lap_elem_async<T, NSTAGE><<<std::min(pg, ngroups), 64 * EPB, LapRing<T, NSTAGE>::kBytes, st>>>(
+        E, P->pin, m->econn, met, *D, x, rel, scal);
+  } else {
+    k_lap_elem<T><<<ngroups, 64 * EPB, 0, st>>>(E, P->pin, m->econn, met, *D, x, rel, scal);
+  }
   SOD_CHECK_LAUNCH();
   k_lap_gather<T><<<node_grid(P->n), kBlock, 0, st>>>((int)P->n, P->pin, m->n2e_ptr, m->n2e, rel, x, y, P->part,
                                                       scal);
@@ -532,6 +666,21 @@ int sod_poisson_create(SodMesh* m, SodPoisson** out) {
   PALLOC(P->scal, sizeof(double) * S_COUNT);
 #undef PALLOC
   if (cudaMallocHost(&P->hscal, sizeof(double) * S_COUNT) != cudaSuccess) return fail("hscal");
+  {
+    int dev = 0, nsm = 0, b64 = 0, b32 = 0;
+    SOD_CUDA(cudaGetDevice(&dev));
+    SOD_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    SOD_CUDA(cudaFuncSetAttribute(k_lap_elem_async<double, NSTAGE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  LapRing<double, NSTAGE>::kBytes));
+    SOD_CUDA(cudaFuncSetAttribute(k_lap_elem_async<float, NSTAGE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  LapRing<float, NSTAGE>::kBytes));
+    SOD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b64, k_lap_elem_async<double, NSTAGE>, 64 * EPB,
+                                                           LapRing<double, NSTAGE>::kBytes));
+    SOD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b32, k_lap_elem_async<float, NSTAGE>, 64 * EPB,
+                                                           LapRing<float, NSTAGE>::kBytes));
+    P->ring_grid[0] = nsm * b64;
+    P->ring_grid[1] = nsm * b32;
+  }
   k_metric<<<1184, 256>>>(E * NN, m->geo64, P->met, P->met32);
   k_diag<<<node_grid(N), kBlock>>>((int)N, m->n2e_ptr, m->n2e, m->geo64, m->D, P->diag, P->diag32);
   g_launches.fetch_add(2);
