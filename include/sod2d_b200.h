@@ -104,6 +104,28 @@ int sod_mesh_get_geometry(SodMesh* mesh, double* He, double* gpvol, double* Ml, 
                           double* helem_l);
 int sod_mesh_set_params(SodMesh* mesh, const SodParams* params);
 
+/* ---- Boundary conditions (non-periodic meshes: rk_4_main with noBoundaries = .false.) ---- */
+
+/* The nscbc_* values read by temporary_bc_routine_dirichlet_prim (mod_bc_routines.f90:17-180). */
+typedef struct {
+  double rho_inf, u_inf, p_inf, c_inf; /* far-field state (bc_type_far_field = 1)          */
+  double gamma_inf, Rgas_inf;          /* nscbc_gamma_inf, nscbc_Rgas_inf                   */
+  double T_H, T_C;                     /* wall temperatures of codes 4 (hot) and 5 (cold)   */
+} SodBcParams;
+
+/* Register the boundary data rk_4_main takes (time_integ.f90:137-141) and switch the mesh's
+ * step to the non-periodic path: host arrays of npoin rows, node ids in the mesh's
+ * index_base.  bou_codes_nodes: a node is on a boundary when its code is below
+ * max_num_bou_codes = 10 (mod_constants.f90:29; codes :41-48); lnbn_nodes: nearBoundaryNode
+ * (mod_geom.f90:101-121), read for boundary nodes only; normalsAtNodes (npoin,3); u_buffer
+ * (npoin,3), may be null (zeros).  Each step then applies temporary_bc_routine_dirichlet_prim
+ * to every stage state and to the updated state, and bc_fix_dirichlet_residual_entropy to the
+ * entropy residual (time_integ.f90:256-259,299-301,434-437,474-477).  bou_codes_nodes = null
+ * removes the boundaries.  Captured step graphs of the mesh are dropped.  The ensemble
+ * (sod_batch_*) and the adjoint entry points reject meshes with boundaries. */
+int sod_mesh_set_boundaries(SodMesh* mesh, const int32_t* bou_codes_nodes, const int32_t* lnbn_nodes,
+                            const double* normalsAtNodes, const double* u_buffer, const SodBcParams* bc);
+
 /* Device-resident solver state in the reference's array layouts (level pos=2 only).
  * Every pointer is a device pointer owned by the caller. */
 typedef struct {
@@ -125,8 +147,10 @@ typedef struct {
                        sgs_visc (mod_sgs_viscosity.f90:13-125); null = no SGS (flag_les off) */
 } SodState;
 
-/* One explicit RK4 step: rk_4_main (time_integ.f90:137-508) on the periodic compressible
- * path (noBoundaries, flag_les=0, flag_total_enthalpy=.false., Sutherland on).  dt is read
+/* One explicit RK4 step: rk_4_main (time_integ.f90:137-508) on the compressible path
+ * (flag_total_enthalpy=.false., Sutherland on; LES when flag_les = 1 and state->mu_sgs is
+ * set; boundary conditions when sod_mesh_set_boundaries registered some, else the periodic
+ * noBoundaries path).  dt is read
  * from dt_dev (device double) so that a captured step needs no host value; when
  * update_dt != 0 the next dt from adapt_dt_cfl (mod_time_ops.f90:11-61) is written back to
  * dt_dev after the step (CFDSolverBase.f90:1592). */
@@ -263,6 +287,19 @@ int sod_poisson_diag(SodPoisson* P, double* d, sod_stream_t stream);
  * SOD_ERR_NOT_CONVERGED when max_iter is reached first.  iters/final_rel may be null. */
 int sod_conjgrad_pressure(SodPoisson* P, const double* Rp0, double* R, int max_iter, double tol,
                           int mixed, int* iters, double* final_rel, sod_stream_t stream);
+
+/* ---- Boundary routines on device arrays (the mesh's registered boundary data) ---------- */
+/* temporary_bc_routine_dirichlet_prim (mod_bc_routines.f90:17-180) in place on rho, q, u, pr,
+ * E (npoin / (npoin,3) device arrays): every boundary node takes the far-field HLL state, the
+ * no-slip wall state or the slip projection of its code, from the state of its lnbn node; u
+ * is read (slip walls) and written, pr written for far-field nodes, as the reference. */
+int sod_bc_dirichlet_prim(SodMesh* mesh, double* rho, double* q, double* u, double* pr, double* E,
+                          sod_stream_t stream);
+/* bc_fix_dirichlet_residual (mod_bc_routines.f90:181-221): zero Rmass, Rmom (and Rener for the
+ * isothermal walls) on no-slip nodes. */
+int sod_bc_fix_dirichlet_residual(SodMesh* mesh, double* Rmass, double* Rmom, double* Rener, sod_stream_t stream);
+/* bc_fix_dirichlet_residual_entropy (mod_bc_routines.f90:265-291): zero R on no-slip nodes. */
+int sod_bc_fix_dirichlet_residual_entropy(SodMesh* mesh, double* R, sod_stream_t stream);
 
 /* ---- Taylor-Green diagnostics ------------------------------------------------------------ */
 /* volAvg_EK and visc_dissipationRate (mod_analysis.f90:10-144), as the time loop calls them

@@ -40,6 +40,25 @@ class StageCapture(C.Structure):
     _fields_ = [("Rmass", _p), ("Rmom", _p), ("Rener", _p), ("Reta", _p), ("stage", C.c_int)]
 
 
+class BcData(C.Structure):
+    _fields_ = [("bou_codes_nodes", _p), ("lnbn_nodes", _p), ("normals", _p), ("u_buffer", _p)] + \
+        [(n, C.c_double) for n in ("rho_inf", "u_inf", "p_inf", "c_inf", "gamma_inf", "Rgas_inf", "T_H", "T_C")]
+
+
+class Boundaries:
+    """Boundary data of a non-periodic mesh for the oracle (arrays kept alive here)."""
+
+    def __init__(self, codes, lnbn, normals, u_buffer, bc: dict):
+        self.codes = np.ascontiguousarray(codes, dtype=np.int32)
+        self.lnbn = np.ascontiguousarray(lnbn, dtype=np.int32)
+        self.normals = np.asfortranarray(normals, dtype=np.float64)
+        self.u_buffer = np.asfortranarray(u_buffer, dtype=np.float64)
+        self.c = BcData(ptr(self.codes).value, ptr(self.lnbn).value, ptr(self.normals).value,
+                        ptr(self.u_buffer).value,
+                        *(float(bc[k]) for k in ("rho_inf", "u_inf", "p_inf", "c_inf", "gamma_inf", "Rgas_inf",
+                                                 "T_H", "T_C")))
+
+
 def build() -> str:
     """Compile the oracle with its Makefile (idempotent)."""
     subprocess.run(["make", "-s", "-C", HERE], check=True)
@@ -59,7 +78,11 @@ def lib():
         L.oracle_set_threads.restype = C.c_int
         L.oracle_conjgrad_pressure.restype = C.c_int
         L.oracle_rk_4_main.argtypes = [C.POINTER(ElemCtx), C.POINTER(Params), _p, _p, _p, _p, _p, _p,
-                                       C.c_double, C.c_int, C.POINTER(State), C.POINTER(StageCapture)]
+                                       C.c_double, C.c_int, C.POINTER(State), C.POINTER(StageCapture),
+                                       C.POINTER(BcData)]
+        L.oracle_bc_dirichlet_prim.argtypes = [C.c_int, C.POINTER(BcData), _p, _p, _p, _p, _p]
+        L.oracle_bc_fix_dirichlet_residual.argtypes = [C.c_int, C.POINTER(BcData), _p, _p, _p]
+        L.oracle_bc_fix_dirichlet_residual_entropy.argtypes = [C.c_int, C.POINTER(BcData), _p]
         L.oracle_adapt_dt_cfl.argtypes = [C.POINTER(ElemCtx), _p, _p, _p, C.c_double, C.c_double, _p, _p, _p]
         L.oracle_conjgrad_pressure.argtypes = [C.POINTER(ElemCtx), _p, _p, _p, C.c_int, C.c_double,
                                                C.POINTER(C.c_double)]
@@ -147,9 +170,10 @@ def adapt_dt(om: OracleMesh, st, prm) -> float:
                                      prm.cfl_diff, ptr(st.mu_fluid), ptr(st.mu_sgs), ptr(st.rho))
 
 
-def rk4(om: OracleMesh, prm, st, dt: float, nsteps: int = 1, capture_stage: int = 0):
+def rk4(om: OracleMesh, prm, st, dt: float, nsteps: int = 1, capture_stage: int = 0,
+        bnd: "Boundaries | None" = None):
     """Runs nsteps rk_4_main steps in place on st (a FlowState).  Returns the stage residuals of
-    capture_stage (1..4) of the first step when requested."""
+    capture_stage (1..4) of the first step when requested.  bnd selects the non-periodic path."""
     P = params_of(prm)
     mue_l = np.zeros((om.nelem, 64), order="F")
     S = State(*(ptr(a).value for a in (st.rho, st.u, st.q, st.pr, st.E, st.Tem, st.e_int, st.eta, st.csound,
@@ -163,8 +187,21 @@ def rk4(om: OracleMesh, prm, st, dt: float, nsteps: int = 1, capture_stage: int 
                            ptr(out["Reta"]).value, int(capture_stage))
     lib().oracle_rk_4_main(C.byref(om.ctx), C.byref(P), ptr(om.Ml), ptr(st.mu_factor), ptr(om.gpvol), ptr(om.wgp),
                            ptr(om.helem), ptr(om.helem_l), float(dt), int(nsteps), C.byref(S),
-                           C.byref(cap) if cap is not None else None)
+                           C.byref(cap) if cap is not None else None, C.byref(bnd.c) if bnd is not None else None)
     return out
+
+
+def bc_dirichlet_prim(bnd: Boundaries, rho, q, u, pr, E):
+    """temporary_bc_routine_dirichlet_prim in place on the given FP64 arrays."""
+    lib().oracle_bc_dirichlet_prim(len(rho), C.byref(bnd.c), ptr(rho), ptr(q), ptr(u), ptr(pr), ptr(E))
+
+
+def bc_fix_residual(bnd: Boundaries, Rmass, Rmom, Rener):
+    lib().oracle_bc_fix_dirichlet_residual(len(Rmass), C.byref(bnd.c), ptr(Rmass), ptr(Rmom), ptr(Rener))
+
+
+def bc_fix_residual_entropy(bnd: Boundaries, R):
+    lib().oracle_bc_fix_dirichlet_residual_entropy(len(R), C.byref(bnd.c), ptr(R))
 
 
 def convec(om: OracleMesh, u, q, rho, pr, E):

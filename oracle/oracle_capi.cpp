@@ -96,13 +96,26 @@ double oracle_adapt_dt_cfl(const ElemCtx* ctx, const double* helem, const double
 
 // Runs nsteps explicit RK4 steps of rk_4_main on the state S (level pos=2 only).  When
 // capture is non-null its arrays receive the residuals (after /Ml) of stage capture->stage of
-// the first step.
+// the first step.  bc non-null selects the non-periodic path with those boundary data.
 void oracle_rk_4_main(const ElemCtx* ctx, const Params* P, const double* Ml, const double* mu_factor,
                       const double* gpvol, const double* wgp, const double* helem, const double* helem_l,
-                      double dt, int nsteps, State* S, StageCapture* capture) {
+                      double dt, int nsteps, State* S, StageCapture* capture, const BcData* bc) {
   Rk4Scratch W(ctx->npoin);
   for (int s = 0; s < nsteps; ++s)
-    rk_4_main(*ctx, *P, Ml, mu_factor, gpvol, wgp, helem, helem_l, dt, *S, W, s == 0 ? capture : nullptr);
+    rk_4_main(*ctx, *P, Ml, mu_factor, gpvol, wgp, helem, helem_l, dt, *S, W, s == 0 ? capture : nullptr, bc);
+}
+
+void oracle_bc_dirichlet_prim(int npoin, const BcData* bc, double* rho, double* q, double* u, double* pr,
+                              double* E) {
+  temporary_bc_routine_dirichlet_prim(npoin, *bc, rho, q, u, pr, E);
+}
+
+void oracle_bc_fix_dirichlet_residual(int npoin, const BcData* bc, double* Rmass, double* Rmom, double* Rener) {
+  bc_fix_dirichlet_residual(npoin, *bc, Rmass, Rmom, Rener);
+}
+
+void oracle_bc_fix_dirichlet_residual_entropy(int npoin, const BcData* bc, double* R) {
+  bc_fix_dirichlet_residual_entropy(npoin, *bc, R);
 }
 
 void oracle_eval_laplacian_mult(const ElemCtx* ctx, const double* p, double* ResP) {

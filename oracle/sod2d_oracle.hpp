@@ -1115,9 +1115,10 @@ inline double adapt_dt_cfl(const ElemCtx& ctx, const double* helem, const double
 }
 
 // ------------------------------------------------------------------------------------------
-// rk_4_main (time_integ.f90:137-508) restricted to the periodic compressible path:
-// noBoundaries, no wall model, no source term, no buffer, flag_les=0, flag_total_enthalpy
-// false, Sutherland on (flag_real_diff=flag_diff_suth=1), RK order 4, single rank.
+// rk_4_main (time_integ.f90:137-508) on the compressible path: periodic (noBoundaries) or
+// with the Dirichlet boundary routines below; no wall model, no source term, no buffer,
+// flag_total_enthalpy false, Sutherland on (flag_real_diff=flag_diff_suth=1), RK order 4,
+// single rank.
 // State arrays hold level pos=2 only (the only level rk_4_main reads and writes).
 // ------------------------------------------------------------------------------------------
 struct State {
@@ -1214,9 +1215,122 @@ inline void sgs_visc(const ElemCtx& ctx, const Params& P, const double* u, doubl
   }
 }
 
+// ------------------------------------------------------------------------------------------
+// Boundary conditions of the non-periodic path (noBoundaries = .false.), mod_bc_routines.f90.
+// Codes from mod_constants.f90:29,41-48; a node is on a boundary when its code is below
+// max_num_bou_codes.  lnbn_nodes is 0-based here.
+// ------------------------------------------------------------------------------------------
+constexpr int kMaxNumBouCodes = 10;
+constexpr int kBcFarField = 1, kBcNonSlipAdiabatic = 3, kBcNonSlipHot = 4, kBcNonSlipCold = 5,
+              kBcSlipAdiabatic = 6, kBcSlipWallModel = 7;
+
+struct BcData {
+  const int32_t* bou_codes_nodes;  // (npoin)
+  const int32_t* lnbn_nodes;       // (npoin), 0-based
+  const double* normals;           // normalsAtNodes (npoin,3)
+  const double* u_buffer;          // (npoin,3)
+  double rho_inf, u_inf, p_inf, c_inf, gamma_inf, Rgas_inf, T_H, T_C;  // nscbc_* values
+};
+
+// temporary_bc_routine_dirichlet_prim (mod_bc_routines.f90:17-180): the first loop copies the
+// state of each boundary node's lnbn node, the second forms its velocity and pressure, the
+// third overwrites the boundary node by code.  u is read (slip walls) and written.
+inline void temporary_bc_routine_dirichlet_prim(int npoin, const BcData& B, double* rho, double* q, double* u,
+                                                double* pr, double* E) {
+  const int64_t N = npoin;
+  std::vector<double> rho2(npoin, 0.0), p2(npoin, 0.0), E2(npoin, 0.0), u2(3 * N, 0.0), q2(3 * N, 0.0);
+  const double gi = B.gamma_inf;
+  for (int n = 0; n < npoin; ++n) {
+    if (B.bou_codes_nodes[n] < kMaxNumBouCodes) {
+      const int64_t s = B.lnbn_nodes[n];
+      q2[n] = q[s];
+      q2[n + N] = q[s + N];
+      q2[n + 2 * N] = q[s + 2 * N];
+      rho2[n] = rho[s];
+      E2[n] = E[s];
+    }
+  }
+  for (int n = 0; n < npoin; ++n) {
+    if (B.bou_codes_nodes[n] < kMaxNumBouCodes) {
+      u2[n] = q2[n] / rho2[n];
+      u2[n + N] = q2[n + N] / rho2[n];
+      u2[n + 2 * N] = q2[n + 2 * N] / rho2[n];
+      p2[n] = rho2[n] * (gi - 1.0) *
+              ((E2[n] / rho2[n]) - 0.5 * ((u2[n] * u2[n]) + (u2[n + N] * u2[n + N]) + (u2[n + 2 * N] * u2[n + 2 * N])));
+    }
+  }
+  for (int n = 0; n < npoin; ++n) {
+    const int bcode = B.bou_codes_nodes[n];
+    if (bcode >= kMaxNumBouCodes) continue;
+    if (bcode == kBcFarField) {
+      const double E_inf = (B.rho_inf * 0.5 * (B.u_inf * B.u_inf) + B.p_inf / (gi - 1.0));
+      const double c2 = std::sqrt(gi * p2[n] / rho2[n]);
+      double sl = std::min(B.u_inf - B.c_inf, u2[n] - c2);
+      double sr = std::max(u2[n] + c2, B.u_inf + B.c_inf);
+      const double rho_hll = (sr * rho2[n] - sl * B.rho_inf + B.rho_inf * B.u_inf - q2[n]) / (sr - sl);
+      const double E_hll = (sr * E2[n] - sl * E_inf + B.u_inf * (E_inf + B.p_inf) - u2[n] * (E2[n] + p2[n])) / (sr - sl);
+      double qh[3];
+      for (int d = 0; d < 3; ++d) {
+        const double ub = B.u_buffer[n + N * d], ud = u2[n + N * d], qd = q2[n + N * d];
+        sl = std::min(ub - B.c_inf, ud - c2);
+        sr = std::max(ud + c2, ub + B.c_inf);
+        qh[d] = (sr * qd - sl * B.rho_inf * ub + B.rho_inf * (ub * ub) - ud * qd) / (sr - sl);
+      }
+      rho[n] = rho_hll;
+      E[n] = E_hll;
+      for (int d = 0; d < 3; ++d) q[n + N * d] = qh[d];
+      for (int d = 0; d < 3; ++d) u[n + N * d] = q[n + N * d] / rho[n];
+      pr[n] = rho[n] * (gi - 1.0) *
+              ((E[n] / rho[n]) - 0.5 * ((u[n] * u[n]) + (u[n + N] * u[n + N]) + (u[n + 2 * N] * u[n + 2 * N])));
+    } else if (bcode == kBcNonSlipAdiabatic) {
+      for (int d = 0; d < 3; ++d) q[n + N * d] = 0.0;
+      for (int d = 0; d < 3; ++d) u[n + N * d] = 0.0;
+      rho[n] = B.rho_inf;
+    } else if (bcode == kBcNonSlipHot || bcode == kBcNonSlipCold) {
+      for (int d = 0; d < 3; ++d) q[n + N * d] = 0.0;
+      for (int d = 0; d < 3; ++d) u[n + N * d] = 0.0;
+      rho[n] = B.p_inf / B.Rgas_inf / (bcode == kBcNonSlipHot ? B.T_H : B.T_C);
+      E[n] = B.p_inf / (gi - 1.0);
+    } else if (bcode == kBcSlipWallModel || bcode == kBcSlipAdiabatic) {
+      E[n] = E[n] - rho[n] * 0.5 * ((u[n] * u[n]) + (u[n + N] * u[n + N]) + (u[n + 2 * N] * u[n + 2 * N]));
+      const double norm = (B.normals[n] * q[n]) + (B.normals[n + N] * q[n + N]) + (B.normals[n + 2 * N] * q[n + 2 * N]);
+      for (int d = 0; d < 3; ++d) q[n + N * d] = q[n + N * d] - norm * B.normals[n + N * d];
+      rho[n] = B.rho_inf;
+      for (int d = 0; d < 3; ++d) u[n + N * d] = q[n + N * d] / rho[n];
+      E[n] = E[n] + rho[n] * 0.5 * ((u[n] * u[n]) + (u[n + N] * u[n + N]) + (u[n + 2 * N] * u[n + 2 * N]));
+    }
+  }
+}
+
+// bc_fix_dirichlet_residual (mod_bc_routines.f90:181-221): no-slip walls keep rho and rho u
+// (and, isothermal, rho E).
+inline void bc_fix_dirichlet_residual(int npoin, const BcData& B, double* Rmass, double* Rmom, double* Rener) {
+  const int64_t N = npoin;
+  for (int n = 0; n < npoin; ++n) {
+    const int bcode = B.bou_codes_nodes[n];
+    if (bcode >= kMaxNumBouCodes) continue;
+    if (bcode == kBcNonSlipAdiabatic || bcode == kBcNonSlipHot || bcode == kBcNonSlipCold) {
+      for (int d = 0; d < 3; ++d) Rmom[n + N * d] = 0.0;
+      Rmass[n] = 0.0;
+      if (bcode != kBcNonSlipAdiabatic) Rener[n] = 0.0;
+    }
+  }
+}
+
+// bc_fix_dirichlet_residual_entropy (mod_bc_routines.f90:265-291)
+inline void bc_fix_dirichlet_residual_entropy(int npoin, const BcData& B, double* R) {
+  for (int n = 0; n < npoin; ++n) {
+    const int bcode = B.bou_codes_nodes[n];
+    if (bcode == kBcNonSlipAdiabatic || bcode == kBcNonSlipHot || bcode == kBcNonSlipCold) R[n] = 0.0;
+  }
+}
+
+// bc != null: the non-periodic path (noBoundaries = .false.): boundary conditions on each stage
+// state and on the updated state, entropy residual zeroed on no-slip walls
+// (time_integ.f90:256-259,299-301,434-437,474-477).
 inline void rk_4_main(const ElemCtx& ctx, const Params& P, const double* Ml, const double* mu_factor,
                       const double* gpvol, const double* wgp, const double* helem, const double* helem_l,
-                      double dt, State& S, Rk4Scratch& W, StageCapture* cap) {
+                      double dt, State& S, Rk4Scratch& W, StageCapture* cap, const BcData* bc = nullptr) {
   const int npoin = ctx.npoin;
   const int64_t n3 = (int64_t)npoin * 3;
   const double a_i[4] = {0.0, 0.5, 0.5, 1.0};
@@ -1230,6 +1344,7 @@ inline void rk_4_main(const ElemCtx& ctx, const Params& P, const double* Ml, con
   std::fill(W.Rener_sum.begin(), W.Rener_sum.end(), 0.0);
   std::fill(W.Reta_sum.begin(), W.Reta_sum.end(), 0.0);
   std::fill(W.Rmom_sum.begin(), W.Rmom_sum.end(), 0.0);
+  std::fill(W.aux_u.begin(), W.aux_u.end(), 0.0);  // time_integ.f90:208
   for (int istep = 0; istep < 4; ++istep) {
     // stage state (time_integ.f90:239-248)
 #pragma omp parallel for schedule(static)
@@ -1239,6 +1354,9 @@ inline void rk_4_main(const ElemCtx& ctx, const Params& P, const double* Ml, con
       for (int d = 0; d < 3; ++d)
         W.aux_q[p + (int64_t)npoin * d] = S.q[p + (int64_t)npoin * d] - dt * a_i[istep] * W.Rmom[p + (int64_t)npoin * d];
     }
+    if (bc)  // time_integ.f90:256-259
+      temporary_bc_routine_dirichlet_prim(npoin, *bc, W.aux_rho.data(), W.aux_q.data(), W.aux_u.data(),
+                                          W.aux_pr.data(), W.aux_E.data());
     // EOS (time_integ.f90:266-285)
 #pragma omp parallel for schedule(static)
     for (int p = 0; p < npoin; ++p) {
@@ -1255,6 +1373,7 @@ inline void rk_4_main(const ElemCtx& ctx, const Params& P, const double* Ml, con
       for (int d = 0; d < 3; ++d) W.f_eta[p + (int64_t)npoin * d] = W.aux_u[p + (int64_t)npoin * d] * W.aux_eta[p];
     }
     generic_scalar_convec_ijk(ctx, W.f_eta.data(), W.aux_eta.data(), W.aux_u.data(), W.Reta.data());
+    if (bc) bc_fix_dirichlet_residual_entropy(npoin, *bc, W.Reta.data());  // time_integ.f90:299-301
     for (int p = 0; p < npoin; ++p) W.Reta[p] = W.Reta[p] / Ml[p];
     sutherland_viscosity(npoin, W.aux_Tem.data(), mu_factor, S.mu_fluid);
     full_diffusion_ijk(ctx, P, W.aux_rho.data(), W.aux_rho.data(), W.aux_u.data(), W.aux_Tem.data(),
@@ -1293,6 +1412,7 @@ inline void rk_4_main(const ElemCtx& ctx, const Params& P, const double* Ml, con
     S.E[p] = S.E[p] - dt * W.Rener_sum[p];
     for (int d = 0; d < 3; ++d) S.q[p + (int64_t)npoin * d] = S.q[p + (int64_t)npoin * d] - dt * W.Rmom_sum[p + (int64_t)npoin * d];
   }
+  if (bc) temporary_bc_routine_dirichlet_prim(npoin, *bc, S.rho, S.q, S.u, S.pr, S.E);  // time_integ.f90:434-437
   // EOS at the new level (time_integ.f90:445-463)
   for (int p = 0; p < npoin; ++p) {
     double umag = 0.0;
@@ -1310,6 +1430,7 @@ inline void rk_4_main(const ElemCtx& ctx, const Params& P, const double* Ml, con
   }
   // Reta = -Reta_sum (time_integ.f90:467-471)
   for (int p = 0; p < npoin; ++p) W.Reta[p] = -W.Reta_sum[p];
+  if (bc) bc_fix_dirichlet_residual_entropy(npoin, *bc, W.Reta.data());  // time_integ.f90:474-477
   sutherland_viscosity(npoin, S.Tem, mu_factor, S.mu_fluid);
   smart_visc_spectral(ctx, P, W.Reta.data(), gpvol, wgp, S.rho, S.u, S.csound, S.Tem, S.eta, helem_l, helem,
                       S.mu_e, S.mue_l);

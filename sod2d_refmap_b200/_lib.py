@@ -34,6 +34,10 @@ class SodParams(C.Structure):
                 ("cfl_diff", _d), ("flag_les", C.c_int32), ("c_sgs", _d)]
 
 
+class SodBcParams(C.Structure):
+    _fields_ = [(n, _d) for n in ("rho_inf", "u_inf", "p_inf", "c_inf", "gamma_inf", "Rgas_inf", "T_H", "T_C")]
+
+
 class SodMeshDesc(C.Structure):
     _fields_ = [("nelem", C.c_int32), ("npoin", C.c_int32), ("npoin_orig", C.c_int32), ("porder", C.c_int32),
                 ("index_base", C.c_int32), ("connec", _p), ("connec_orig", _p), ("coord_orig", _p),
@@ -74,6 +78,10 @@ _SIGS = {
     "sod_rhs_vjp": (_i, [_p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p]),
     "sod_rk4_step_vjp": (_i, [_p] * 15),
     "sod_tgv_diagnostics": (_i, [_p, _p, _p, _p, _p, _d, _d, _p, _p]),
+    "sod_mesh_set_boundaries": (_i, [_p] * 6),
+    "sod_bc_dirichlet_prim": (_i, [_p] * 7),
+    "sod_bc_fix_dirichlet_residual": (_i, [_p] * 5),
+    "sod_bc_fix_dirichlet_residual_entropy": (_i, [_p] * 3),
     "sod_legacy_mass_convec": (_i, [_i] * 5 + [_p] * 7),
     "sod_legacy_generic_scalar_convec": (_i, [_i] * 5 + [_p] * 7),
     "sod_legacy_mom_convec": (_i, [_i] * 5 + [_p] * 9),

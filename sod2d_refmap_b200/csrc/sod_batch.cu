@@ -79,6 +79,11 @@ int sod_batch_create(SodMesh* const* meshes, int nmesh, SodBatch** out) {
   SOD_ARG(meshes && nmesh > 0 && out, "meshes/nmesh/out");
   *out = nullptr;
   for (int i = 0; i < nmesh; ++i) SOD_ARG(meshes[i], "null member mesh");
+  for (int i = 0; i < nmesh; ++i)
+    if (meshes[i]->bc.nb > 0) {
+      set_error("sod_batch_create: members with boundaries are not supported");
+      return SOD_ERR_UNSUPPORTED;
+    }
   const SodMesh* m0 = meshes[0];
   int64_t E = 0, N = 0;
   SodBatch* B = new SodBatch();

@@ -1,0 +1,440 @@
+// Boundary conditions of the non-periodic path (noBoundaries = .false.): the routines of
+// mod_bc_routines.f90 on the device and their place in rk_4_main (time_integ.f90:256-259,
+// 299-301, 434-437, 474-477).
+//
+// The boundary nodes are compacted once (sod_mesh_set_boundaries) into an ascending list with
+// their code, lnbn node, normal and buffer velocity; every kernel here runs one thread per
+// boundary node.  temporary_bc_routine_dirichlet_prim is two kernels: k_bc_gather copies the
+// state of every boundary node's lnbn node first (the reference's first loop), so a boundary
+// node whose lnbn node is itself on a boundary reads the value from before the routine, as
+// there; k_bc_apply forms the lnbn node's velocity and pressure and overwrites the boundary
+// node by code.
+//
+// Inside a step the stage state is formed by the gather kernel of the previous stage (stage
+// 1: a copy of the state) and the routine runs on it before the element kernels evaluate its
+// EOS.  The slip branch reads the velocity left in aux_u by the previous stage's EOS (zero at
+// stage 1, time_integ.f90:208), which for a boundary node is q/rho of its post-boundary stage
+// state: k_bc_apply keeps that per boundary node for the next stage.  After the final update
+// the routine reads u(:,:,pos) from before the update (kept at the start of the step), then
+// the EOS and Sutherland viscosity of the boundary nodes are re-evaluated, the entropy
+// residual is zeroed on no-slip walls and the entropy normalisation (mean and spread of eta,
+// mod_entropy_viscosity.f90:43-66) is recomputed from the post-boundary eta.
+#include "sod_internal.cuh"
+#include <vector>
+
+namespace sod {
+namespace bcd {
+
+constexpr int kMaxNumBouCodes = 10;  // mod_constants.f90:29
+constexpr int kFarField = 1, kNonSlipAdiabatic = 3, kNonSlipHot = 4, kNonSlipCold = 5, kSlipAdiabatic = 6,
+              kSlipWallModel = 7;  // mod_constants.f90:41-48
+constexpr int kBlock = 256;
+
+__device__ __forceinline__ bool no_slip(int c) {
+  return c == kNonSlipAdiabatic || c == kNonSlipHot || c == kNonSlipCold;
+}
+
+// aux2 = (rho, q x3, E) of each boundary node's lnbn node (mod_bc_routines.f90:41-51)
+__global__ void k_bc_gather(int nb, const int32_t* __restrict__ nbr, const double* __restrict__ rho,
+                            const double* __restrict__ q, const double* __restrict__ E, size_t N,
+                            double* __restrict__ aux2) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= nb) return;
+  const size_t s = (size_t)nbr[b];
+  aux2[b] = rho[s];
+  aux2[(size_t)nb + b] = q[s];
+  aux2[2 * (size_t)nb + b] = q[s + N];
+  aux2[3 * (size_t)nb + b] = q[s + 2 * N];
+  aux2[4 * (size_t)nb + b] = E[s];
+}
+
+struct ApplyArgs {
+  int nb;
+  size_t N;
+  const int32_t* node;
+  const int32_t* code;
+  const double* normal;  // [3][nb]
+  const double* ubuf;    // [3][nb]
+  const double* aux2;    // [5][nb]
+  double *rho, *q, *E;   // state updated in place (node-indexed)
+  const double* uold_b;  // slip branch velocity per boundary node [3][nb], or
+  const double* uold_n;  // per node (npoin,3); both null: zero
+  double* u_n;           // aux_u / aux_p outputs of the routine (node-indexed), optional
+  double* pr_n;
+  double* u_post_b;      // q/rho after the routine per boundary node [3][nb], optional
+  int eos;               // 1: EOS + Sutherland of the boundary nodes into the outputs below
+  double *e_int, *csound, *machno, *Tem, *eta, *mu_fluid;
+  const double* mu_factor;
+  double* Reta;          // zeroed on no-slip nodes when set
+  double gamma, Rgas;
+  SodBcParams p;
+};
+
+// mod_bc_routines.f90:55-178 (second and third loops) for one boundary node
+__global__ void __launch_bounds__(kBlock) k_bc_apply(const ApplyArgs a) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= a.nb) return;
+  const size_t nb = (size_t)a.nb, N = a.N;
+  const size_t n = (size_t)a.node[b];
+  const int c = a.code[b];
+  const double gi = a.p.gamma_inf;
+  const double rho2 = a.aux2[b];
+  const double q2[3] = {a.aux2[nb + b], a.aux2[2 * nb + b], a.aux2[3 * nb + b]};
+  const double E2 = a.aux2[4 * nb + b];
+  const double u2[3] = {q2[0] / rho2, q2[1] / rho2, q2[2] / rho2};
+  const double p2 = rho2 * (gi - 1.0) * ((E2 / rho2) - 0.5 * ((u2[0] * u2[0]) + (u2[1] * u2[1]) + (u2[2] * u2[2])));
+  double r = a.rho[n], e = a.E[n];
+  double qq[3] = {a.q[n], a.q[n + N], a.q[n + 2 * N]};
+  double uu[3] = {0.0, 0.0, 0.0}, pp = 0.0;
+  bool set_u = false, set_p = false;
+  if (c == kFarField) {
+    const double E_inf = (a.p.rho_inf * 0.5 * (a.p.u_inf * a.p.u_inf) + a.p.p_inf / (gi - 1.0));
+    const double c2 = sqrt(gi * p2 / rho2);
+    double sl = fmin(a.p.u_inf - a.p.c_inf, u2[0] - c2);
+    double sr = fmax(u2[0] + c2, a.p.u_inf + a.p.c_inf);
+    const double rho_hll = (sr * rho2 - sl * a.p.rho_inf + a.p.rho_inf * a.p.u_inf - q2[0]) / (sr - sl);
+    const double E_hll =
+        (sr * E2 - sl * E_inf + a.p.u_inf * (E_inf + a.p.p_inf) - u2[0] * (E2 + p2)) / (sr - sl);
+    double qh[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const double ub = a.ubuf[d * nb + b];
+      sl = fmin(ub - a.p.c_inf, u2[d] - c2);
+      sr = fmax(u2[d] + c2, ub + a.p.c_inf);
+      qh[d] = (sr * q2[d] - sl * a.p.rho_inf * ub + a.p.rho_inf * (ub * ub) - u2[d] * q2[d]) / (sr - sl);
+    }
+    r = rho_hll;
+    e = E_hll;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) qq[d] = qh[d];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) uu[d] = qq[d] / r;
+    pp = r * (gi - 1.0) * ((e / r) - 0.5 * ((uu[0] * uu[0]) + (uu[1] * uu[1]) + (uu[2] * uu[2])));
+    set_u = set_p = true;
+  } else if (c == kNonSlipAdiabatic) {
+    qq[0] = qq[1] = qq[2] = 0.0;
+    set_u = true;
+    r = a.p.rho_inf;
+  } else if (c == kNonSlipHot || c == kNonSlipCold) {
+    qq[0] = qq[1] = qq[2] = 0.0;
+    set_u = true;
+    r = a.p.p_inf / a.p.Rgas_inf / (c == kNonSlipHot ? a.p.T_H : a.p.T_C);
+    e = a.p.p_inf / (gi - 1.0);
+  } else if (c == kSlipWallModel || c == kSlipAdiabatic) {
+    double uo[3] = {0.0, 0.0, 0.0};
+    if (a.uold_b) {
+#pragma unroll
+      for (int d = 0; d < 3; ++d) uo[d] = a.uold_b[d * nb + b];
+    } else if (a.uold_n) {
+#pragma unroll
+      for (int d = 0; d < 3; ++d) uo[d] = a.uold_n[n + N * d];
+    }
+    e = e - r * 0.5 * ((uo[0] * uo[0]) + (uo[1] * uo[1]) + (uo[2] * uo[2]));
+    const double nx = a.normal[b], ny = a.normal[nb + b], nz = a.normal[2 * nb + b];
+    const double norm = (nx * qq[0]) + (ny * qq[1]) + (nz * qq[2]);
+    qq[0] = qq[0] - norm * nx;
+    qq[1] = qq[1] - norm * ny;
+    qq[2] = qq[2] - norm * nz;
+    r = a.p.rho_inf;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) uu[d] = qq[d] / r;
+    e = e + r * 0.5 * ((uu[0] * uu[0]) + (uu[1] * uu[1]) + (uu[2] * uu[2]));
+    set_u = true;
+  }
+  a.rho[n] = r;
+  a.E[n] = e;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) a.q[n + N * d] = qq[d];
+  if (a.u_post_b) {
+#pragma unroll
+    for (int d = 0; d < 3; ++d) a.u_post_b[d * nb + b] = qq[d] / r;
+  }
+  if (a.eos) {
+    // EOS and Sutherland at the new level (time_integ.f90:445-463, mod_fluid_viscosity.f90:21-41)
+    const double g = a.gamma;
+    const double rho = r;
+    const double u0 = qq[0] / rho, u1 = qq[1] / rho, u2v = qq[2] / rho;
+    double umag = u0 * u0 + u1 * u1 + u2v * u2v;
+    const double ei = (e / rho) - 0.5 * umag;
+    const double pr = rho * (g - 1.0) * ei;
+    const double cs = sqrt(g * pr / rho);
+    umag = sqrt(umag);
+    const double T = pr / (rho * a.Rgas);
+    a.u_n[n] = u0;
+    a.u_n[n + N] = u1;
+    a.u_n[n + 2 * N] = u2v;
+    a.e_int[n] = ei;
+    a.pr_n[n] = pr;
+    a.csound[n] = cs;
+    a.machno[n] = umag / cs;
+    a.Tem[n] = T;
+    a.eta[n] = (rho / (g - 1.0)) * log(pr / pow(rho, g));
+    a.mu_fluid[n] = a.mu_factor[n] * kSuthC1 * (T * sqrt(T)) / (T + kSuthS);
+  } else {
+    if (a.u_n && set_u) {
+#pragma unroll
+      for (int d = 0; d < 3; ++d) a.u_n[n + N * d] = uu[d];
+    }
+    if (a.pr_n && set_p) a.pr_n[n] = pp;
+  }
+  if (a.Reta && no_slip(c)) a.Reta[n] = 0.0;
+}
+
+// bc_fix_dirichlet_residual (mod_bc_routines.f90:181-221) and _entropy (:265-291)
+__global__ void k_bc_fix(int nb, const int32_t* __restrict__ node, const int32_t* __restrict__ code, size_t N,
+                         double* Rmass, double* Rmom, double* Rener, double* R) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= nb) return;
+  const int c = code[b];
+  if (!no_slip(c)) return;
+  const size_t n = (size_t)node[b];
+  if (R) R[n] = 0.0;
+  if (Rmom) {
+    Rmom[n] = 0.0;
+    Rmom[n + N] = 0.0;
+    Rmom[n + 2 * N] = 0.0;
+  }
+  if (Rmass) Rmass[n] = 0.0;
+  if (Rener && c != kNonSlipAdiabatic) Rener[n] = 0.0;
+}
+
+__global__ void k_bc_snapshot(int nb, const int32_t* __restrict__ node, const double* __restrict__ u, size_t N,
+                              double* __restrict__ out) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= nb) return;
+  const size_t n = (size_t)node[b];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) out[(size_t)d * nb + b] = u[n + N * d];
+}
+
+// entropy normalisation from the post-boundary eta: block partials (sum, max, min), then one
+// block in a fixed order (deterministic)
+__device__ __forceinline__ void reduce3(double& s, double& mx, double& mn, double (*sh)[kBlock / 32]) {
+  for (int o = 16; o > 0; o >>= 1) {
+    s += __shfl_down_sync(0xffffffffu, s, o);
+    mx = fmax(mx, __shfl_down_sync(0xffffffffu, mx, o));
+    mn = fmin(mn, __shfl_down_sync(0xffffffffu, mn, o));
+  }
+  const int w = threadIdx.x >> 5;
+  if ((threadIdx.x & 31) == 0) { sh[0][w] = s; sh[1][w] = mx; sh[2][w] = mn; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    s = sh[0][0]; mx = sh[1][0]; mn = sh[2][0];
+    for (int q = 1; q < kBlock / 32; ++q) { s += sh[0][q]; mx = fmax(mx, sh[1][q]); mn = fmin(mn, sh[2][q]); }
+  }
+}
+
+__global__ void __launch_bounds__(kBlock) k_eta_partials(int n, const double* __restrict__ eta, double* red) {
+  __shared__ double sh[3][kBlock / 32];
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double s = 0.0, mx = -1e300, mn = 1e300;
+  if (i < n) s = mx = mn = eta[i];
+  reduce3(s, mx, mn, sh);
+  if (threadIdx.x == 0) {
+    red[3 * blockIdx.x] = s;
+    red[3 * blockIdx.x + 1] = mx;
+    red[3 * blockIdx.x + 2] = mn;
+  }
+}
+
+__global__ void __launch_bounds__(kBlock) k_eta_final(int nblk, int npoin, int normalise,
+                                                      const double* __restrict__ red, double* scal) {
+  __shared__ double sh[3][kBlock / 32];
+  double s = 0.0, mx = -1e300, mn = 1e300;
+  for (int b = threadIdx.x; b < nblk; b += blockDim.x) {
+    s += red[3 * b];
+    mx = fmax(mx, red[3 * b + 1]);
+    mn = fmin(mn, red[3 * b + 2]);
+  }
+  reduce3(s, mx, mn, sh);
+  if (threadIdx.x == 0) {
+    if (normalise) {
+      const double mean = s / (double)npoin;
+      scal[0] = mean;
+      scal[1] = fmax(mx - mean, mean - mn);
+    } else {
+      scal[0] = 0.0;
+      scal[1] = 1.0;
+    }
+  }
+}
+
+static int grid_of(int n) { return (n + kBlock - 1) / kBlock; }
+
+static ApplyArgs base_args(SodMesh* m) {
+  ApplyArgs a{};
+  a.nb = m->bc.nb;
+  a.N = (size_t)m->npoin;
+  a.node = m->bc.node;
+  a.code = m->bc.code;
+  a.normal = m->bc.normal;
+  a.ubuf = m->bc.ubuf;
+  a.aux2 = m->bc.aux2;
+  a.gamma = m->prm.gamma;
+  a.Rgas = m->prm.Rgas;
+  a.p = m->bc.prm;
+  return a;
+}
+
+static int gather(SodMesh* m, const double* rho, const double* q, const double* E, cudaStream_t st) {
+  k_bc_gather<<<grid_of(m->bc.nb), kBlock, 0, st>>>(m->bc.nb, m->bc.nbr, rho, q, E, (size_t)m->npoin, m->bc.aux2);
+  SOD_CHECK_LAUNCH();
+  return SOD_OK;
+}
+
+}  // namespace bcd
+
+void bc_free(SodMesh* m) {
+  BcState& b = m->bc;
+  void* ptrs[] = {b.node, b.code, b.nbr, b.normal, b.ubuf, b.aux2, b.u_stage, b.u_final};
+  for (void* p : ptrs)
+    if (p) cudaFree(p);
+  b = BcState{};
+}
+
+int bc_snapshot_u(SodMesh* m, const double* u, cudaStream_t st) {
+  bcd::k_bc_snapshot<<<bcd::grid_of(m->bc.nb), bcd::kBlock, 0, st>>>(m->bc.nb, m->bc.node, u, (size_t)m->npoin,
+                                                                      m->bc.u_final);
+  SOD_CHECK_LAUNCH();
+  return SOD_OK;
+}
+
+// the routine on stage state ys ([5][npoin]: rho, q x3, E) of stage 1..4
+int bc_stage(SodMesh* m, double* ys, int stage, cudaStream_t st) {
+  const size_t N = m->npoin;
+  if (int rc = bcd::gather(m, ys, ys + N, ys + 4 * N, st)) return rc;
+  bcd::ApplyArgs a = bcd::base_args(m);
+  a.rho = ys;
+  a.q = ys + N;
+  a.E = ys + 4 * N;
+  a.uold_b = stage == 1 ? nullptr : m->bc.u_stage;  // aux_u is zero before the first stage's EOS
+  a.u_post_b = m->bc.u_stage;
+  bcd::k_bc_apply<<<bcd::grid_of(m->bc.nb), bcd::kBlock, 0, st>>>(a);
+  SOD_CHECK_LAUNCH();
+  return SOD_OK;
+}
+
+// the routine on the updated state, boundary-node EOS, entropy residual fix and normalisation
+int bc_final(SodMesh* m, SodState* s, double* Reta, cudaStream_t st) {
+  if (int rc = bcd::gather(m, s->rho, s->q, s->E, st)) return rc;
+  bcd::ApplyArgs a = bcd::base_args(m);
+  a.rho = s->rho;
+  a.q = s->q;
+  a.E = s->E;
+  a.uold_b = m->bc.u_final;
+  a.eos = 1;
+  a.u_n = s->u;
+  a.pr_n = s->pr;
+  a.e_int = s->e_int;
+  a.csound = s->csound;
+  a.machno = s->machno;
+  a.Tem = s->Tem;
+  a.eta = s->eta;
+  a.mu_fluid = s->mu_fluid;
+  a.mu_factor = s->mu_factor;
+  a.Reta = Reta;
+  bcd::k_bc_apply<<<bcd::grid_of(m->bc.nb), bcd::kBlock, 0, st>>>(a);
+  SOD_CHECK_LAUNCH();
+  const int nblk = bcd::grid_of(m->npoin);
+  SOD_ARG(m->buf.red_cap >= 3 * (int64_t)nblk, "reduction scratch too small");
+  bcd::k_eta_partials<<<nblk, bcd::kBlock, 0, st>>>(m->npoin, s->eta, m->buf.red);
+  SOD_CHECK_LAUNCH();
+  bcd::k_eta_final<<<1, bcd::kBlock, 0, st>>>(nblk, m->npoin, m->prm.normalise, m->buf.red, m->buf.scal);
+  SOD_CHECK_LAUNCH();
+  return SOD_OK;
+}
+
+}  // namespace sod
+
+using namespace sod;
+
+extern "C" {
+
+int sod_mesh_set_boundaries(SodMesh* m, const int32_t* codes, const int32_t* lnbn, const double* normals,
+                            const double* u_buffer, const SodBcParams* bc) {
+  SOD_ARG(m, "mesh null");
+  SOD_ARG(m->nmember == 0, "boundaries on an ensemble mesh are not supported");
+  for (auto& kv : m->graphs)
+    if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+  m->graphs.clear();
+  bc_free(m);
+  if (!codes) return SOD_OK;
+  SOD_ARG(lnbn && bc, "lnbn_nodes and bc parameters required");
+  const int N = m->npoin;
+  std::vector<int32_t> node, code, nbr;
+  for (int n = 0; n < N; ++n) {
+    if (codes[n] < bcd::kMaxNumBouCodes) {
+      const int32_t s = lnbn[n] - m->index_base;
+      SOD_ARG(s >= 0 && s < N, "lnbn_nodes entry out of range");
+      node.push_back(n);
+      code.push_back(codes[n]);
+      nbr.push_back(s);
+    }
+  }
+  const int nb = (int)node.size();
+  if (nb == 0) return SOD_OK;
+  std::vector<double> nrm((size_t)3 * nb, 0.0), ub((size_t)3 * nb, 0.0);
+  for (int b = 0; b < nb; ++b)
+    for (int d = 0; d < 3; ++d) {
+      if (normals) nrm[(size_t)d * nb + b] = normals[(size_t)node[b] + (size_t)N * d];
+      if (u_buffer) ub[(size_t)d * nb + b] = u_buffer[(size_t)node[b] + (size_t)N * d];
+    }
+  BcState& B = m->bc;
+  auto alloc = [&](void** p, size_t bytes) { return cudaMalloc(p, bytes) == cudaSuccess; };
+  bool ok = alloc((void**)&B.node, sizeof(int32_t) * nb) && alloc((void**)&B.code, sizeof(int32_t) * nb) &&
+            alloc((void**)&B.nbr, sizeof(int32_t) * nb) && alloc((void**)&B.normal, sizeof(double) * 3 * nb) &&
+            alloc((void**)&B.ubuf, sizeof(double) * 3 * nb) && alloc((void**)&B.aux2, sizeof(double) * 5 * nb) &&
+            alloc((void**)&B.u_stage, sizeof(double) * 3 * nb) && alloc((void**)&B.u_final, sizeof(double) * 3 * nb);
+  if (!ok) {
+    bc_free(m);
+    set_error("sod_mesh_set_boundaries: device allocation failed");
+    return SOD_ERR_NOMEM;
+  }
+  B.nb = nb;
+  B.prm = *bc;
+  SOD_CUDA(cudaMemcpy(B.node, node.data(), sizeof(int32_t) * nb, cudaMemcpyHostToDevice));
+  SOD_CUDA(cudaMemcpy(B.code, code.data(), sizeof(int32_t) * nb, cudaMemcpyHostToDevice));
+  SOD_CUDA(cudaMemcpy(B.nbr, nbr.data(), sizeof(int32_t) * nb, cudaMemcpyHostToDevice));
+  SOD_CUDA(cudaMemcpy(B.normal, nrm.data(), sizeof(double) * 3 * nb, cudaMemcpyHostToDevice));
+  SOD_CUDA(cudaMemcpy(B.ubuf, ub.data(), sizeof(double) * 3 * nb, cudaMemcpyHostToDevice));
+  SOD_CUDA(cudaMemset(B.u_stage, 0, sizeof(double) * 3 * nb));
+  SOD_CUDA(cudaMemset(B.u_final, 0, sizeof(double) * 3 * nb));
+  return SOD_OK;
+}
+
+int sod_bc_dirichlet_prim(SodMesh* m, double* rho, double* q, double* u, double* pr, double* E, sod_stream_t stream) {
+  SOD_ARG(m && rho && q && u && pr && E, "null argument");
+  SOD_ARG(m->bc.nb > 0, "no boundary nodes registered (sod_mesh_set_boundaries)");
+  cudaStream_t st = (cudaStream_t)stream;
+  if (int rc = bcd::gather(m, rho, q, E, st)) return rc;
+  bcd::ApplyArgs a = bcd::base_args(m);
+  a.rho = rho;
+  a.q = q;
+  a.E = E;
+  a.uold_n = u;
+  a.u_n = u;
+  a.pr_n = pr;
+  bcd::k_bc_apply<<<bcd::grid_of(m->bc.nb), bcd::kBlock, 0, st>>>(a);
+  SOD_CHECK_LAUNCH();
+  return SOD_OK;
+}
+
+int sod_bc_fix_dirichlet_residual(SodMesh* m, double* Rmass, double* Rmom, double* Rener, sod_stream_t stream) {
+  SOD_ARG(m && Rmass && Rmom && Rener, "null argument");
+  SOD_ARG(m->bc.nb > 0, "no boundary nodes registered (sod_mesh_set_boundaries)");
+  bcd::k_bc_fix<<<bcd::grid_of(m->bc.nb), bcd::kBlock, 0, (cudaStream_t)stream>>>(
+      m->bc.nb, m->bc.node, m->bc.code, (size_t)m->npoin, Rmass, Rmom, Rener, nullptr);
+  SOD_CHECK_LAUNCH();
+  return SOD_OK;
+}
+
+int sod_bc_fix_dirichlet_residual_entropy(SodMesh* m, double* R, sod_stream_t stream) {
+  SOD_ARG(m && R, "null argument");
+  SOD_ARG(m->bc.nb > 0, "no boundary nodes registered (sod_mesh_set_boundaries)");
+  bcd::k_bc_fix<<<bcd::grid_of(m->bc.nb), bcd::kBlock, 0, (cudaStream_t)stream>>>(
+      m->bc.nb, m->bc.node, m->bc.code, (size_t)m->npoin, nullptr, nullptr, nullptr, R);
+  SOD_CHECK_LAUNCH();
+  return SOD_OK;
+}
+
+}  // extern "C"

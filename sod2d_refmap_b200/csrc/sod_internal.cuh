@@ -27,6 +27,8 @@ constexpr int NP1 = P + 1;
 constexpr int NN = NP1 * NP1 * NP1;   // 64 nodes / gauss points per element
 constexpr int NGEO = 10;              // 9 He entries + gpvol
 constexpr int NRES = 6;               // element residual fields: mass, mom x3, ener, eta
+constexpr double kSuthC1 = 0.000001458;  // sutherland_viscosity (mod_fluid_viscosity.f90:21-41)
+constexpr double kSuthS = 110.4;
 // shared-memory field stride: 4 k-planes of 16 values, plane pitch 22 (bank-conflict free
 // for the xi/eta/zeta line reads of a 4x4x2 warp in FP64)
 constexpr int PLANE = 22;
@@ -139,6 +141,21 @@ struct GraphEntry {
   int nkernels = 0;
 };
 
+// Boundary data of a non-periodic mesh (sod_bc.cu), compacted to the nb boundary nodes in
+// ascending node order; per-boundary-node columns are [field][nb].
+struct BcState {
+  int nb = 0;
+  int32_t* node = nullptr;     // boundary node ids
+  int32_t* code = nullptr;     // bou_codes_nodes of each
+  int32_t* nbr = nullptr;      // lnbn_nodes of each (0-based)
+  double* normal = nullptr;    // [3][nb] normalsAtNodes
+  double* ubuf = nullptr;      // [3][nb] u_buffer
+  double* aux2 = nullptr;      // [5][nb] state of the lnbn node (rho, q x3, E)
+  double* u_stage = nullptr;   // [3][nb] aux_u of the previous stage's EOS
+  double* u_final = nullptr;   // [3][nb] u(:,:,pos) at the start of the step
+  SodBcParams prm{};
+};
+
 }  // namespace sod
 
 struct SodMesh {
@@ -177,6 +194,8 @@ struct SodMesh {
   // adjoint scratch (sod_adjoint.cu): stage states, seeds, accumulators
   double* adj = nullptr;
   size_t adj_len = 0;
+  int index_base = 0;          // of the caller's node ids (SodMeshDesc.index_base)
+  sod::BcState bc;             // boundaries (nb == 0: periodic path, noBoundaries)
 };
 
 namespace sod {
@@ -187,6 +206,11 @@ int mesh_ref_to_internal_elem(SodMesh* m, const double* ref_dev /*(nelem,64) F*/
 int mesh_internal_to_ref_elem(SodMesh* m, const double* int_dev, double* ref_dev, cudaStream_t st);
 int launch_copy_f32(const double* src, float* dst, int64_t n, cudaStream_t st);
 int init_kernel_attrs();
+// boundary conditions (sod_bc.cu), used by the step pipeline when m->bc.nb > 0
+int bc_snapshot_u(SodMesh* m, const double* u, cudaStream_t st);
+int bc_stage(SodMesh* m, double* ys, int stage, cudaStream_t st);
+int bc_final(SodMesh* m, SodState* s, double* Reta, cudaStream_t st);
+void bc_free(SodMesh* m);
 // packed-FP32 (FFMA2) variant of the mixed fused RHS kernel (sod_rhs_mixed.cu)
 int launch_rhs_mixed2(const RhsArgs& a, int epb, cudaStream_t st);
 // LES (sod_les.cu): musgs_int <- sgs_visc of the velocity u (3 columns of npoin)

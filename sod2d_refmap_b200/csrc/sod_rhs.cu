@@ -21,9 +21,6 @@
 
 namespace sod {
 
-constexpr double kSuthC1 = 0.000001458;
-constexpr double kSuthS = 110.4;
-
 template <typename R>
 __device__ __forceinline__ void giso(const R* __restrict__ f, int i, int j, int k, const R* Dx, const R* Dy,
                                      const R* Dz, R& gx, R& gy, R& gz) {
@@ -783,13 +780,28 @@ int run_step(SodMesh* m, SodState* s, const double* dt_dev, double* dt_next, boo
     loc.Reta = reta_tmp;
   }
   int rc;
+  // non-periodic path: boundary routine on every stage state and on the updated state
+  const bool bc = m->bc.nb > 0;
+  if (bc) {
+    rc = bc_snapshot_u(m, s->u, st);  // u(:,:,pos) before the update, read by slip walls
+    if (rc) return rc;
+  }
   for (int stage = 1; stage <= 4; ++stage) {
     double* yin = (stage_store && stage >= 2) ? stage_store + (size_t)(stage - 2) * 5 * N : m->buf.ys;
-    const double* src_rho = stage == 1 ? s->rho : yin;
-    const double* src_q0 = stage == 1 ? s->q : yin + N;
-    const double* src_q1 = stage == 1 ? s->q + N : yin + 2 * N;
-    const double* src_q2 = stage == 1 ? s->q + 2 * N : yin + 3 * N;
-    const double* src_E = stage == 1 ? s->E : yin + 4 * N;
+    if (bc && stage == 1) {
+      // the first stage state is the state itself with the boundary routine applied to a copy
+      SOD_CUDA(cudaMemcpyAsync(yin, s->rho, sizeof(double) * N, cudaMemcpyDeviceToDevice, st));
+      SOD_CUDA(cudaMemcpyAsync(yin + N, s->q, sizeof(double) * 3 * N, cudaMemcpyDeviceToDevice, st));
+      SOD_CUDA(cudaMemcpyAsync(yin + 4 * N, s->E, sizeof(double) * N, cudaMemcpyDeviceToDevice, st));
+      rc = bc_stage(m, yin, 1, st);
+      if (rc) return rc;
+    }
+    const bool from_state = stage == 1 && !bc;
+    const double* src_rho = from_state ? s->rho : yin;
+    const double* src_q0 = from_state ? s->q : yin + N;
+    const double* src_q1 = from_state ? s->q + N : yin + 2 * N;
+    const double* src_q2 = from_state ? s->q + 2 * N : yin + 3 * N;
+    const double* src_E = from_state ? s->E : yin + 4 * N;
     if (ev) cudaEventRecord(ev[2 * (stage - 1)], st);
     rc = launch_rhs(m, mixed, epb, src_rho, src_q0, src_q1, src_q2, src_E, s->mu_factor, les ? m->musgs_int : nullptr,
                     st);
@@ -810,6 +822,15 @@ int run_step(SodMesh* m, SodState* s, const double* dt_dev, double* dt_next, boo
     if (stage == 4 && m->nmember > 0) {
       k_member_eta<<<m->nmember, 512, 0, st>>>(m->member_node_off, s->eta, m->member_scal, m->prm.normalise);
       SOD_CHECK_LAUNCH();
+    }
+    if (bc) {
+      if (stage < 4) {
+        double* ynext = (stage_store && stage < 4) ? stage_store + (size_t)(stage - 1) * 5 * N : m->buf.ys;
+        rc = bc_stage(m, ynext, stage + 1, st);
+      } else {
+        rc = bc_final(m, s, loc.Reta, st);
+      }
+      if (rc) return rc;
     }
     if (ev) cudaEventRecord(ev[2 * (3 + stage) + 1], st);
   }
@@ -870,6 +891,10 @@ int sod_rk4_main_record(SodMesh* m, SodState* s, const double* dt_dev, double* d
   if (rc) return rc;
   SOD_ARG(dt_dev && stages, "dt_dev/stages null");
   SOD_ARG(prec == SOD_FP64 || prec == SOD_MIXED, "precision");
+  if (m->bc.nb > 0) {
+    set_error("sod_rk4_main_record: the adjoint of the boundary routines is not built");
+    return SOD_ERR_UNSUPPORTED;
+  }
   cudaStream_t st = (cudaStream_t)stream;
   const bool mixed = prec == SOD_MIXED;
   rc = ensure_step_buffers(m, mixed);

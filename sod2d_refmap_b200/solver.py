@@ -14,7 +14,7 @@ import ctypes as C
 import numpy as np
 
 from . import _lib
-from .mesh import BoxMesh, FlowState, TGVParams
+from .mesh import BoxMesh, FlowState, TGVParams, bc_params
 
 
 def _torch():
@@ -167,6 +167,41 @@ class Sod2dMesh:
         self.prm = prm
         p = params_struct(prm)
         _lib.check(_lib.load().sod_mesh_set_params(self.handle, C.byref(p)))
+
+    # ---- boundary conditions (non-periodic meshes) -------------------------------------
+    def set_boundaries(self, bou_codes_nodes, lnbn_nodes, normals, u_buffer=None, bc: dict | None = None):
+        """Registers rk_4_main's boundary data (host numpy arrays, 0-based node ids): the step
+        then applies the boundary routines (noBoundaries = .false.).  bou_codes_nodes=None
+        removes them.  bc: the nscbc_* values (mesh.bc_params)."""
+        L = _lib.load()
+        if bou_codes_nodes is None:
+            _lib.check(L.sod_mesh_set_boundaries(self.handle, None, None, None, None, None))
+            self._bnd = None
+            return
+        if bc is None:
+            bc = bc_params(self.prm)
+        arrs = (np.ascontiguousarray(bou_codes_nodes, dtype=np.int32), np.ascontiguousarray(lnbn_nodes, dtype=np.int32),
+                np.asfortranarray(normals, dtype=np.float64),
+                None if u_buffer is None else np.asfortranarray(u_buffer, dtype=np.float64))
+        p = _lib.SodBcParams(*(float(bc[k]) for k in ("rho_inf", "u_inf", "p_inf", "c_inf", "gamma_inf", "Rgas_inf",
+                                                      "T_H", "T_C")))
+        _lib.check(L.sod_mesh_set_boundaries(self.handle, *(_np_ptr(a) if a is not None else None for a in arrs),
+                                             C.byref(p)))
+        self._bnd = arrs
+
+    def bc_dirichlet_prim(self, rho, q, u, pr, E, stream=None):
+        """temporary_bc_routine_dirichlet_prim in place on device tensors ((npoin), q/u (3,npoin)
+        storage = Fortran (npoin,3))."""
+        _lib.check(_lib.load().sod_bc_dirichlet_prim(self.handle, *(C.c_void_p(_ptr(_contig(t))) for t in (
+            rho, q, u, pr, E)), _stream(stream)))
+
+    def bc_fix_residual(self, Rmass, Rmom, Rener, stream=None):
+        _lib.check(_lib.load().sod_bc_fix_dirichlet_residual(self.handle, *(C.c_void_p(_ptr(_contig(t))) for t in (
+            Rmass, Rmom, Rener)), _stream(stream)))
+
+    def bc_fix_residual_entropy(self, R, stream=None):
+        _lib.check(_lib.load().sod_bc_fix_dirichlet_residual_entropy(self.handle, C.c_void_p(_ptr(_contig(R))),
+                                                                      _stream(stream)))
 
     # ---- time integration --------------------------------------------------------------
     def rk_4_main(self, state: Sod2dState, precision: int = FP64, update_dt: bool = True, stream=None):
