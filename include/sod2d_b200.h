@@ -60,6 +60,8 @@ typedef struct {
   double cfl_conv, cfl_diff;    /* CFDSolverBase cfl_conv / cfl_diff                      */
   int32_t flag_les;             /* 1: Vreman sgs_visc after each step (time_integ.f90:498-506) */
   double c_sgs;                 /* mod_numerical_params.f90:15 (0.025)                    */
+  int32_t flag_total_enthalpy;  /* 1: convection by full_convec_ijk_H (time_integ.f90:361-365;
+                                   mod_numerical_params.f90:20, default 0)                 */
 } SodParams;
 
 void sod_params_default(SodParams* p);
@@ -102,6 +104,7 @@ void sod_mesh_destroy(SodMesh* mesh);
 /* Copy the device geometry back in the reference layouts (any pointer may be null). */
 int sod_mesh_get_geometry(SodMesh* mesh, double* He, double* gpvol, double* Ml, double* helem,
                           double* helem_l);
+/* Replace the parameters; step graphs captured with the old ones are dropped. */
 int sod_mesh_set_params(SodMesh* mesh, const SodParams* params);
 
 /* ---- Boundary conditions (non-periodic meshes: rk_4_main with noBoundaries = .false.) ---- */
@@ -148,7 +151,7 @@ typedef struct {
 } SodState;
 
 /* One explicit RK4 step: rk_4_main (time_integ.f90:137-508) on the compressible path
- * (flag_total_enthalpy=.false., Sutherland on; LES when flag_les = 1 and state->mu_sgs is
+ * (either convection routine by flag_total_enthalpy, Sutherland on; LES when flag_les = 1 and state->mu_sgs is
  * set; boundary conditions when sod_mesh_set_boundaries registered some, else the periodic
  * noBoundaries path).  dt is read
  * from dt_dev (device double) so that a captured step needs no host value; when
@@ -203,6 +206,11 @@ int sod_adapt_dt_cfl(SodMesh* mesh, const double* u, const double* csound, const
 int sod_full_convec_ijk(SodMesh* mesh, const double* u, const double* q, const double* rho,
                         const double* pr, const double* E, double* Rmass, double* Rmom,
                         double* Rener, sod_stream_t stream);
+/* full_convec_ijk_H (elem_convec.f90:20-208): the total-enthalpy form, energy flux (E + p) u;
+ * E is the total energy rho E (time_integ.f90:362).  Outputs are overwritten. */
+int sod_full_convec_ijk_H(SodMesh* mesh, const double* u, const double* q, const double* rho,
+                          const double* pr, const double* E, double* Rmass, double* Rmom,
+                          double* Rener, sod_stream_t stream);
 /* generic_scalar_convec_ijk (elem_convec.f90:462-570). */
 int sod_generic_scalar_convec_ijk(SodMesh* mesh, const double* q, const double* eta,
                                   const double* u, double* Rconvec, sod_stream_t stream);

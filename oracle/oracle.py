@@ -28,7 +28,8 @@ class Params(C.Structure):
     _fields_ = [("gamma_gas", C.c_double), ("Rgas", C.c_double), ("Cp", C.c_double), ("Prt", C.c_double),
                 ("ce", C.c_double), ("cmax", C.c_double), ("cglob", C.c_double), ("c_rho", C.c_double),
                 ("c_ener", C.c_double), ("flag_normalise_entropy", C.c_int), ("cfl_conv", C.c_double),
-                ("cfl_diff", C.c_double), ("flag_les", C.c_int), ("c_sgs", C.c_double)]
+                ("cfl_diff", C.c_double), ("flag_les", C.c_int), ("c_sgs", C.c_double),
+                ("flag_total_enthalpy", C.c_int)]
 
 
 class State(C.Structure):
@@ -162,7 +163,8 @@ class OracleMesh:
 def params_of(prm) -> Params:
     return Params(prm.gamma_gas, prm.Rgas, prm.Cp, prm.Prt, prm.ce, prm.cmax, prm.cglob, prm.c_rho,
                   prm.c_ener, int(prm.flag_normalise_entropy), prm.cfl_conv, prm.cfl_diff,
-                  int(getattr(prm, "flag_les", 0)), float(getattr(prm, "c_sgs", 0.025)))
+                  int(getattr(prm, "flag_les", 0)), float(getattr(prm, "c_sgs", 0.025)),
+                  int(getattr(prm, "flag_total_enthalpy", 0)))
 
 
 def adapt_dt(om: OracleMesh, st, prm) -> float:
@@ -207,6 +209,14 @@ def bc_fix_residual_entropy(bnd: Boundaries, R):
 def convec(om: OracleMesh, u, q, rho, pr, E):
     Rm = np.zeros(om.npoin); Rmo = np.zeros((om.npoin, 3), order="F"); Re = np.zeros(om.npoin)
     lib().oracle_full_convec_ijk(C.byref(om.ctx), ptr(u), ptr(q), ptr(rho), ptr(pr), ptr(E), ptr(Rm), ptr(Rmo), ptr(Re))
+    return Rm, Rmo, Re
+
+
+def convec_H(om: OracleMesh, u, q, rho, pr, E):
+    """full_convec_ijk_H (E: total energy rho E)."""
+    Rm = np.zeros(om.npoin); Rmo = np.zeros((om.npoin, 3), order="F"); Re = np.zeros(om.npoin)
+    lib().oracle_full_convec_ijk_H(C.byref(om.ctx), ptr(u), ptr(q), ptr(rho), ptr(pr), ptr(E), ptr(Rm), ptr(Rmo),
+                                   ptr(Re))
     return Rm, Rmo, Re
 
 

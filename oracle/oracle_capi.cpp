@@ -65,6 +65,11 @@ void oracle_full_convec_ijk(const ElemCtx* ctx, const double* u, const double* q
   full_convec_ijk(*ctx, u, q, rho, pr, E, Rmass, Rmom, Rener);
 }
 
+void oracle_full_convec_ijk_H(const ElemCtx* ctx, const double* u, const double* q, const double* rho,
+                              const double* pr, const double* E, double* Rmass, double* Rmom, double* Rener) {
+  full_convec_ijk_H(*ctx, u, q, rho, pr, E, Rmass, Rmom, Rener);
+}
+
 void oracle_generic_scalar_convec_ijk(const ElemCtx* ctx, const double* q, const double* eta,
                                       const double* u, double* R) {
   generic_scalar_convec_ijk(*ctx, q, eta, u, R);

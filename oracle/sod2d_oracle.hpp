@@ -45,6 +45,7 @@ struct Params {
   double cfl_conv, cfl_diff;
   int flag_les;                           // LES (Vreman sgs_visc) after each step (time_integ.f90:498-506)
   double c_sgs;                           // mod_numerical_params.f90:15
+  int flag_total_enthalpy;                // convection by full_convec_ijk_H (time_integ.f90:361-365)
 };
 
 // ------------------------------------------------------------------------------------------
@@ -492,6 +493,111 @@ inline void full_convec_ijk(const ElemCtx& ctx, const double* u, const double* q
         Re_ener[igaus] = Re_ener[igaus] +
                          0.25 * (ql[igaus][id] * gradE[id] + ul[igaus][id] * gradRE[id] + fuel[igaus][id] * gradRho[id]) +
                          0.25 * (ql[igaus][id] * gradk[id] + ul[igaus][id] * gradRk[id] + fukl[igaus][id] * gradRho[id]);
+        for (int jd = 0; jd < 3; ++jd)
+          Re_mom[igaus][id] = Re_mom[igaus][id] + 0.25 * (fuul[igaus][id][jd] * gradRho[jd] +
+                                                          ql[igaus][jd] * gradU[id][jd] + ul[igaus][jd] * gradQ[id][jd]);
+        Re_mom[igaus][id] = SOD_GPVOL(igaus, ielem) * Re_mom[igaus][id];
+      }
+      Re_mass[igaus] = SOD_GPVOL(igaus, ielem) * Re_mass[igaus];
+      Re_ener[igaus] = SOD_GPVOL(igaus, ielem) * Re_ener[igaus];
+    }
+    for (int d = 0; d < 3; ++d)
+      for (int a = 0; a < nnode; ++a) Rmom[ipoin[a] + (int64_t)npoin * d] += Re_mom[a][d];
+    for (int a = 0; a < nnode; ++a) {
+      Rmass[ipoin[a]] += Re_mass[a];
+      Rener[ipoin[a]] += Re_ener[a];
+    }
+  });
+}
+
+// full_convec_ijk_H (elem_convec.f90:20-208): the convective residual with the total-enthalpy
+// energy flux (E + p) u; E is the total energy rho E here (time_integ.f90:362).
+inline void full_convec_ijk_H(const ElemCtx& ctx, const double* u, const double* q, const double* rho,
+                              const double* pr, const double* E, double* Rmass, double* Rmom, double* Rener) {
+  const int nelem = ctx.nelem, npoin = ctx.npoin;
+  for (int64_t p = 0; p < (int64_t)npoin * 3; ++p) Rmom[p] = 0.0;
+  for (int p = 0; p < npoin; ++p) { Rmass[p] = 0.0; Rener[p] = 0.0; }
+  for_each_element_coloured(ctx, [&](int ielem) {
+    int ipoin[nnode];
+    double Re_mom[nnode][3], Re_mass[nnode], Re_ener[nnode];
+    double ul[nnode][3], ql[nnode][3], rhol[nnode], prl[nnode], El[nnode], fel[nnode][3];
+    double fl[nnode][3][3], fuul[nnode][3][3];
+    for (int a = 0; a < nnode; ++a) ipoin[a] = ctx.connec[ielem + (int64_t)nelem * a];
+    for (int d = 0; d < 3; ++d)
+      for (int a = 0; a < nnode; ++a) {
+        ul[a][d] = u[ipoin[a] + (int64_t)npoin * d];
+        ql[a][d] = q[ipoin[a] + (int64_t)npoin * d];
+        fel[a][d] = (E[ipoin[a]] + pr[ipoin[a]]) * u[ipoin[a] + (int64_t)npoin * d];
+      }
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j)
+        for (int a = 0; a < nnode; ++a) {
+          fl[a][i][j] = q[ipoin[a] + (int64_t)npoin * i] * u[ipoin[a] + (int64_t)npoin * j];
+          fuul[a][i][j] = u[ipoin[a] + (int64_t)npoin * i] * u[ipoin[a] + (int64_t)npoin * j];
+        }
+    for (int a = 0; a < nnode; ++a) {
+      rhol[a] = rho[ipoin[a]];
+      El[a] = E[ipoin[a]];
+      prl[a] = pr[ipoin[a]];
+    }
+    for (int igaus = 0; igaus < ngaus; ++igaus) {
+      double dlxi[4], dleta[4], dlzeta[4];
+      for (int ii = 0; ii < 4; ++ii) {
+        dlxi[ii] = SOD_DL(igaus, 0, ii);
+        dleta[ii] = SOD_DL(igaus, 1, ii);
+        dlzeta[ii] = SOD_DL(igaus, 2, ii);
+      }
+      int isoI = ctx.gmshAtoI[igaus], isoJ = ctx.gmshAtoJ[igaus], isoK = ctx.gmshAtoK[igaus];
+      double gIRho[3] = {0, 0, 0}, gIP[3] = {0, 0, 0}, gIE[3] = {0, 0, 0};
+      double gIU[3][3] = {}, gIQ[3][3] = {}, gIFe[3][3] = {}, gIF[3][3][3] = {}, gIFuu[3][3][3] = {};
+      for (int ii = 0; ii < 4; ++ii) {
+        int a1 = SOD_INV(ii, isoJ, isoK), a2 = SOD_INV(isoI, ii, isoK), a3 = SOD_INV(isoI, isoJ, ii);
+        gIRho[0] += dlxi[ii] * rhol[a1]; gIRho[1] += dleta[ii] * rhol[a2]; gIRho[2] += dlzeta[ii] * rhol[a3];
+        gIP[0] += dlxi[ii] * prl[a1];    gIP[1] += dleta[ii] * prl[a2];    gIP[2] += dlzeta[ii] * prl[a3];
+        gIE[0] += dlxi[ii] * (prl[a1] + El[a1]);
+        gIE[1] += dleta[ii] * (prl[a2] + El[a2]);
+        gIE[2] += dlzeta[ii] * (prl[a3] + El[a3]);
+        for (int id = 0; id < 3; ++id) {
+          gIU[id][0] += dlxi[ii] * ul[a1][id];   gIU[id][1] += dleta[ii] * ul[a2][id];   gIU[id][2] += dlzeta[ii] * ul[a3][id];
+          gIQ[id][0] += dlxi[ii] * ql[a1][id];   gIQ[id][1] += dleta[ii] * ql[a2][id];   gIQ[id][2] += dlzeta[ii] * ql[a3][id];
+          gIFe[id][0] += dlxi[ii] * fel[a1][id]; gIFe[id][1] += dleta[ii] * fel[a2][id]; gIFe[id][2] += dlzeta[ii] * fel[a3][id];
+          for (int jd = 0; jd < 3; ++jd) {
+            gIF[id][jd][0] += dlxi[ii] * fl[a1][id][jd];
+            gIF[id][jd][1] += dleta[ii] * fl[a2][id][jd];
+            gIF[id][jd][2] += dlzeta[ii] * fl[a3][id][jd];
+            gIFuu[id][jd][0] += dlxi[ii] * fuul[a1][id][jd];
+            gIFuu[id][jd][1] += dleta[ii] * fuul[a2][id][jd];
+            gIFuu[id][jd][2] += dlzeta[ii] * fuul[a3][id][jd];
+          }
+        }
+      }
+      double gradRho[3] = {0, 0, 0}, gradP[3] = {0, 0, 0}, gradE[3] = {0, 0, 0};
+      double gradU[3][3] = {}, gradQ[3][3] = {}, divF[3] = {0, 0, 0}, divFuu[3] = {0, 0, 0};
+      double divFe = 0.0;
+      for (int id = 0; id < 3; ++id)
+        for (int jd = 0; jd < 3; ++jd) {
+          double h = SOD_HE(id, jd, igaus, ielem);
+          gradRho[id] += h * gIRho[jd];
+          gradP[id] += h * gIP[jd];
+          gradE[id] += h * gIE[jd];
+          divFe += h * gIFe[id][jd];
+          for (int kd = 0; kd < 3; ++kd) {
+            double h2 = SOD_HE(jd, kd, igaus, ielem);
+            gradU[id][jd] += h2 * gIU[id][kd];
+            gradQ[id][jd] += h2 * gIQ[id][kd];
+            divF[id] += h2 * gIF[id][jd][kd];
+            divFuu[id] += h2 * gIFuu[id][jd][kd];
+          }
+        }
+      double divU = gradU[0][0] + gradU[1][1] + gradU[2][2];
+      double divQ = gradQ[0][0] + gradQ[1][1] + gradQ[2][2];
+      Re_mass[igaus] = 0.5 * (divQ + rhol[igaus] * divU);
+      Re_ener[igaus] = 0.5 * (divFe + (El[igaus] + prl[igaus]) * divU);
+      for (int id = 0; id < 3; ++id) {
+        Re_mom[igaus][id] = 0.25 * (divF[id] + ul[igaus][id] * divQ + ql[igaus][id] * divU +
+                                    rhol[igaus] * divFuu[id]) + gradP[id];
+        Re_mass[igaus] = Re_mass[igaus] + 0.5 * (ul[igaus][id] * gradRho[id]);
+        Re_ener[igaus] = Re_ener[igaus] + 0.5 * (ul[igaus][id] * gradE[id]);
         for (int jd = 0; jd < 3; ++jd)
           Re_mom[igaus][id] = Re_mom[igaus][id] + 0.25 * (fuul[igaus][id][jd] * gradRho[jd] +
                                                           ql[igaus][jd] * gradU[id][jd] + ul[igaus][jd] * gradQ[id][jd]);
@@ -1117,8 +1223,8 @@ inline double adapt_dt_cfl(const ElemCtx& ctx, const double* helem, const double
 // ------------------------------------------------------------------------------------------
 // rk_4_main (time_integ.f90:137-508) on the compressible path: periodic (noBoundaries) or
 // with the Dirichlet boundary routines below; no wall model, no source term, no buffer,
-// flag_total_enthalpy false, Sutherland on (flag_real_diff=flag_diff_suth=1), RK order 4,
-// single rank.
+// either convection routine (flag_total_enthalpy), Sutherland on (flag_real_diff =
+// flag_diff_suth = 1), RK order 4, single rank.
 // State arrays hold level pos=2 only (the only level rk_4_main reads and writes).
 // ------------------------------------------------------------------------------------------
 struct State {
@@ -1379,8 +1485,12 @@ inline void rk_4_main(const ElemCtx& ctx, const Params& P, const double* Ml, con
     full_diffusion_ijk(ctx, P, W.aux_rho.data(), W.aux_rho.data(), W.aux_u.data(), W.aux_Tem.data(),
                        S.mu_fluid, S.mu_e, S.mu_sgs, W.Rdiff_mass.data(), W.Rdiff_mom.data(),
                        W.Rdiff_ener.data());
-    full_convec_ijk(ctx, W.aux_u.data(), W.aux_q.data(), W.aux_rho.data(), W.aux_pr.data(), W.aux_h.data(),
-                    W.Rmass.data(), W.Rmom.data(), W.Rener.data());
+    if (P.flag_total_enthalpy)  // time_integ.f90:361-365
+      full_convec_ijk_H(ctx, W.aux_u.data(), W.aux_q.data(), W.aux_rho.data(), W.aux_pr.data(), W.aux_E.data(),
+                        W.Rmass.data(), W.Rmom.data(), W.Rener.data());
+    else
+      full_convec_ijk(ctx, W.aux_u.data(), W.aux_q.data(), W.aux_rho.data(), W.aux_pr.data(), W.aux_h.data(),
+                      W.Rmass.data(), W.Rmom.data(), W.Rener.data());
     for (int p = 0; p < npoin; ++p) {
       W.Rmass[p] = W.Rmass[p] + W.Rdiff_mass[p];
       W.Rener[p] = W.Rener[p] + W.Rdiff_ener[p];

@@ -31,7 +31,7 @@ class SodError(RuntimeError):
 class SodParams(C.Structure):
     _fields_ = [("gamma_gas", _d), ("Rgas", _d), ("Cp", _d), ("Prt", _d), ("ce", _d), ("cmax", _d), ("cglob", _d),
                 ("c_rho", _d), ("c_ener", _d), ("flag_normalise_entropy", C.c_int32), ("cfl_conv", _d),
-                ("cfl_diff", _d), ("flag_les", C.c_int32), ("c_sgs", _d)]
+                ("cfl_diff", _d), ("flag_les", C.c_int32), ("c_sgs", _d), ("flag_total_enthalpy", C.c_int32)]
 
 
 class SodBcParams(C.Structure):
@@ -64,6 +64,7 @@ _SIGS = {
     "sod_smart_visc_spectral": (_i, [_p, _p, _p, _p, _p, _p, _p, _p, _p]),
     "sod_adapt_dt_cfl": (_i, [_p, _p, _p, _p, _p, _p, _p, _p]),
     "sod_full_convec_ijk": (_i, [_p, _p, _p, _p, _p, _p, _p, _p, _p, _p]),
+    "sod_full_convec_ijk_H": (_i, [_p, _p, _p, _p, _p, _p, _p, _p, _p, _p]),
     "sod_full_convec_ijk_noalloc": (_i, [C.c_int32, C.c_int32, C.c_int32] + [_p] * 16),
     "sod_generic_scalar_convec_ijk": (_i, [_p, _p, _p, _p, _p, _p]),
     "sod_full_diffusion_ijk": (_i, [_p, _d, _d, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p]),

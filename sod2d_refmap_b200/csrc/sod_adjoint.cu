@@ -507,6 +507,10 @@ int sod_rhs_vjp(SodMesh* m, const double* rho, const double* q, const double* E,
                 double* grad_rho, double* grad_q, double* grad_E, sod_stream_t stream) {
   SOD_ARG(m && rho && q && E && mu_e && mu_factor, "inputs null");
   SOD_ARG(bar_Rmass && bar_Rmom && bar_Rener && grad_rho && grad_q && grad_E, "adjoint arrays null");
+  if (m->prm.total_enthalpy) {
+    set_error("sod_rhs_vjp: the adjoint of full_convec_ijk_H (flag_total_enthalpy) is not built");
+    return SOD_ERR_UNSUPPORTED;
+  }
   cudaStream_t st = (cudaStream_t)stream;
   int rc = ensure_step_buffers(m, false);
   if (rc) return rc;
@@ -535,8 +539,8 @@ int sod_rk4_step_vjp(SodMesh* m, const double* rho, const double* q, const doubl
                      sod_stream_t stream) {
   SOD_ARG(m && rho && q && E && mu_e && mu_factor && dt_dev, "inputs null");
   SOD_ARG(bar_rho && bar_q && bar_E && out_rho && out_q && out_E, "adjoint arrays null");
-  if (m->bc.nb > 0) {
-    set_error("sod_rk4_step_vjp: the adjoint of the boundary routines is not built");
+  if (m->bc.nb > 0 || m->prm.total_enthalpy) {
+    set_error("sod_rk4_step_vjp: the adjoint of the boundary routines and of full_convec_ijk_H is not built");
     return SOD_ERR_UNSUPPORTED;
   }
   cudaStream_t st = (cudaStream_t)stream;

@@ -74,6 +74,7 @@ struct DevParams {
   float gamma_f, c_rho_f, c_ener_f, CpPr_f, Cp09_f;  // gamma, c_rho, c_ener, Cp/Prt, Cp/0.9
   int flag_les;
   double c_sgs;
+  int total_enthalpy;  // flag_total_enthalpy: energy convection of full_convec_ijk_H
 };
 
 // 1-D derivative matrix in natural order: D[m][n] = l_n'(x_m)

@@ -235,6 +235,7 @@ void sod_params_default(SodParams* p) {
   p->cfl_diff = 0.5;
   p->flag_les = 0;
   p->c_sgs = 0.025;
+  p->flag_total_enthalpy = 0;
 }
 
 static void to_dev_params(const SodParams* s, DevParams* d) {
@@ -248,6 +249,7 @@ static void to_dev_params(const SodParams* s, DevParams* d) {
   d->Cp09 = s->Cp / 0.9;
   d->flag_les = s->flag_les;
   d->c_sgs = s->c_sgs;
+  d->total_enthalpy = s->flag_total_enthalpy != 0;
   d->gamma_f = (float)s->gamma_gas;
   d->c_rho_f = (float)s->c_rho;
   d->c_ener_f = (float)s->c_ener;
@@ -258,6 +260,10 @@ static void to_dev_params(const SodParams* s, DevParams* d) {
 int sod_mesh_set_params(SodMesh* m, const SodParams* p) {
   SOD_ARG(m && p, "mesh/params null");
   to_dev_params(p, &m->prm);
+  // captured step graphs hold the parameters in their kernel arguments
+  for (auto& kv : m->graphs)
+    if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+  m->graphs.clear();
   return SOD_OK;
 }
 

@@ -74,7 +74,8 @@ constexpr size_t rhs_smem_bytes(int epb) {
   return sizeof(R) * (size_t)epb * (NBUF + NP2) * FSTRIDE;
 }
 
-template <typename R, int EPB>
+// TOTH: flag_total_enthalpy (energy convection of full_convec_ijk_H)
+template <typename R, int EPB, bool TOTH>
 __global__ void __launch_bounds__(64 * EPB) k_rhs_fused(const RhsArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   R* buf_all = reinterpret_cast<R*>(smem_raw);
@@ -139,9 +140,12 @@ __global__ void __launch_bounds__(64 * EPB) k_rhs_fused(const RhsArgs a) {
   buf[11 * FSTRIDE + s_me] = (R)(rho * kk);
   buf[12 * FSTRIDE + s_me] = (R)eta_full;
   buf[13 * FSTRIDE + s_me] = (R)T;
+  // flag_total_enthalpy: full_convec_ijk_H differentiates p + E and (E + p) u
+  if constexpr (TOTH) buf[14 * FSTRIDE + s_me] = (R)(p + Et);
   __syncthreads();
 
   R gradRho[3], gradU[3][3], gradQ[3][3], gradP[3], gradH[3], gradRH[3], gradK[3], gradRK[3], gradEta[3], gradT[3];
+  R uGradEp = R(0);  // flag_total_enthalpy: sum_c 0.5 u_c d(p + E)/dx_c
   {
     R gx, gy, gz;
     giso(buf + 0 * FSTRIDE, i, j, k, Dx, Dy, Dz, gx, gy, gz);
@@ -167,6 +171,13 @@ __global__ void __launch_bounds__(64 * EPB) k_rhs_fused(const RhsArgs a) {
     phys(H, gx, gy, gz, gradEta[0], gradEta[1], gradEta[2]);
     giso(buf + 13 * FSTRIDE, i, j, k, Dx, Dy, Dz, gx, gy, gz);
     phys(H, gx, gy, gz, gradT[0], gradT[1], gradT[2]);
+    if constexpr (TOTH) {
+      R gradEp[3];
+      giso(buf + 14 * FSTRIDE, i, j, k, Dx, Dy, Dz, gx, gy, gz);
+      phys(H, gx, gy, gz, gradEp[0], gradEp[1], gradEp[2]);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) uGradEp = uGradEp + R(0.5) * ((R)uv[c] * gradEp[c]);
+    }
   }
   const R divU = gradU[0][0] + gradU[1][1] + gradU[2][2];
   const R divQ = gradQ[0][0] + gradQ[1][1] + gradQ[2][2];
@@ -228,7 +239,7 @@ __global__ void __launch_bounds__(64 * EPB) k_rhs_fused(const RhsArgs a) {
     const R rsh = (R)(rho * h), rsk = (R)(rho * kk);
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      buf[(0 + c) * FSTRIDE + s_me] = rsh * uR[c];
+      buf[(0 + c) * FSTRIDE + s_me] = TOTH ? (R)((Et + p) * uv[c]) : rsh * uR[c];
       buf[(3 + c) * FSTRIDE + s_me] = sh * uR[c];
       buf[(6 + c) * FSTRIDE + s_me] = rsk * uR[c];
       buf[(9 + c) * FSTRIDE + s_me] = sk * uR[c];
@@ -244,6 +255,7 @@ __global__ void __launch_bounds__(64 * EPB) k_rhs_fused(const RhsArgs a) {
     const R divFeta = divv(buf + 12 * FSTRIDE, i, j, k, Dx, Dy, Dz, H);
     Ren += R(0.25) * (divFe + rhoR * divFue) + R(0.25) * (divFk + rhoR * divFuk);
     Ret += R(0.5) * divFeta;
+    if constexpr (TOTH) Ren = R(0.5) * (divFe + (R)(Et + p) * divU) + uGradEp;  // elem_convec.f90:171-177
   }
   __syncthreads();
 
@@ -595,7 +607,9 @@ __global__ void __launch_bounds__(64 * KV_EPB, SOD_KV_MIN_BLOCKS) k_visc_dt(cons
 // ---------------------------------------------------------------------------------------------
 template <typename R, int EPB>
 static int set_rhs_attr() {
-  SOD_CUDA(cudaFuncSetAttribute(k_rhs_fused<R, EPB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  SOD_CUDA(cudaFuncSetAttribute(k_rhs_fused<R, EPB, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)rhs_smem_bytes<R>(EPB)));
+  SOD_CUDA(cudaFuncSetAttribute(k_rhs_fused<R, EPB, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)rhs_smem_bytes<R>(EPB)));
   return SOD_OK;
 }
@@ -614,7 +628,10 @@ template <typename R, int EPB>
 static int launch_rhs_t(const RhsArgs& a, cudaStream_t st) {
   const size_t smem = rhs_smem_bytes<R>(EPB);
   const int grid = (a.nelem + EPB - 1) / EPB;
-  k_rhs_fused<R, EPB><<<grid, 64 * EPB, smem, st>>>(a);
+  if (a.prm.total_enthalpy)
+    k_rhs_fused<R, EPB, true><<<grid, 64 * EPB, smem, st>>>(a);
+  else
+    k_rhs_fused<R, EPB, false><<<grid, 64 * EPB, smem, st>>>(a);
   SOD_CHECK_LAUNCH();
   return SOD_OK;
 }
@@ -891,8 +908,8 @@ int sod_rk4_main_record(SodMesh* m, SodState* s, const double* dt_dev, double* d
   if (rc) return rc;
   SOD_ARG(dt_dev && stages, "dt_dev/stages null");
   SOD_ARG(prec == SOD_FP64 || prec == SOD_MIXED, "precision");
-  if (m->bc.nb > 0) {
-    set_error("sod_rk4_main_record: the adjoint of the boundary routines is not built");
+  if (m->bc.nb > 0 || m->prm.total_enthalpy) {
+    set_error("sod_rk4_main_record: the adjoint of the boundary routines and of full_convec_ijk_H is not built");
     return SOD_ERR_UNSUPPORTED;
   }
   cudaStream_t st = (cudaStream_t)stream;

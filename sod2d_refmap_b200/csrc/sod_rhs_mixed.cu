@@ -84,7 +84,8 @@ __device__ __forceinline__ float2 divT2(const float2* fx, const float2* fy, cons
 #ifndef SOD_MX2_MIN_CTAS
 #define SOD_MX2_MIN_CTAS 10  // resident 64-thread element groups per SM the register budget must allow
 #endif
-template <int EPB>
+// TOTH: flag_total_enthalpy (energy convection of full_convec_ijk_H)
+template <int EPB, bool TOTH>
 __global__ void __launch_bounds__(64 * EPB, (EPB >= SOD_MX2_MIN_CTAS ? 1 : SOD_MX2_MIN_CTAS / EPB))
     k_rhs_mixed2(const RhsArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -352,6 +353,13 @@ __global__ void __launch_bounds__(64 * EPB, (EPB >= SOD_MX2_MIN_CTAS ? 1 : SOD_M
     const float2 dD = div2(6);   // (div F1., div F2.)
     Ren += 0.25f * (dA.x + rhoR * dA.y);
     Ret += 0.5f * dC.x;
+    if constexpr (TOTH) {
+      // full_convec_ijk_H (elem_convec.f90:171-177) with E + p = rho H: div(rho H u) =
+      // H_r div q + div(rho H' u), and grad(rho H) is gradRH
+      Ren = 0.5f * (rf[7] * divQ + dA.x + rHR * divU);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) Ren += 0.5f * (uR[c] * gradRH[c]);
+    }
     // Fuu rows 0,1 from slots 9..11 and row 2 from (Fuu02, Fuu12, Fuu22)
     float2 dE = make_float2(0.f, 0.f);
     float dFuu2 = 0.f;
@@ -398,14 +406,20 @@ __global__ void __launch_bounds__(64 * EPB, (EPB >= SOD_MX2_MIN_CTAS ? 1 : SOD_M
 
 template <int EPB>
 static int set_attr() {
-  SOD_CUDA(cudaFuncSetAttribute(k_rhs_mixed2<EPB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes(EPB)));
+  SOD_CUDA(cudaFuncSetAttribute(k_rhs_mixed2<EPB, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)smem_bytes(EPB)));
+  SOD_CUDA(cudaFuncSetAttribute(k_rhs_mixed2<EPB, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)smem_bytes(EPB)));
   return SOD_OK;
 }
 
 template <int EPB>
 static int launch(const RhsArgs& a, cudaStream_t st) {
   const int grid = (a.nelem + EPB - 1) / EPB;
-  k_rhs_mixed2<EPB><<<grid, 64 * EPB, smem_bytes(EPB), st>>>(a);
+  if (a.prm.total_enthalpy)
+    k_rhs_mixed2<EPB, true><<<grid, 64 * EPB, smem_bytes(EPB), st>>>(a);
+  else
+    k_rhs_mixed2<EPB, false><<<grid, 64 * EPB, smem_bytes(EPB), st>>>(a);
   SOD_CHECK_LAUNCH();
   return SOD_OK;
 }

@@ -42,7 +42,10 @@ struct RefArgs {
   double* rel;                                  // [e][6][64]
 };
 
-// full_convec_ijk (elem_convec.f90:241-435)
+// full_convec_ijk (elem_convec.f90:241-435); TOTH: full_convec_ijk_H (elem_convec.f90:48-187),
+// whose energy residual is 0.5 (div((E + p) u) + (E + p) div u + u . grad(E + p)) with E the
+// total energy; mass and momentum are the same in both
+template <bool TOTH>
 __global__ void __launch_bounds__(64) k_convec_ref(const RefArgs a) {
   __shared__ double f[42][FSTRIDE];
   __shared__ DMat Ds;
@@ -58,10 +61,11 @@ __global__ void __launch_bounds__(64) k_convec_ref(const RefArgs a) {
   for (int c = 0; c < 3; ++c) kl = kl + u[c] * u[c] * 0.5;
   // fields: 0 rho,1 p,2 E,3 rhoE,4 k,5 rhok, 6-8 u, 9-11 q, 12-14 fe, 15-17 fue, 18-20 fk, 21-23 fuk,
   //         24-32 F=q x u, 33-41 Fuu = u x u
-  f[0][s] = rho; f[1][s] = pr; f[2][s] = El; f[3][s] = rho * El; f[4][s] = kl; f[5][s] = rho * kl;
+  // TOTH: field 2 holds p + E and fields 12-14 (E + p) u
+  f[0][s] = rho; f[1][s] = pr; f[2][s] = TOTH ? pr + El : El; f[3][s] = rho * El; f[4][s] = kl; f[5][s] = rho * kl;
   for (int c = 0; c < 3; ++c) {
     f[6 + c][s] = u[c]; f[9 + c][s] = q[c];
-    f[12 + c][s] = rho * El * u[c]; f[15 + c][s] = El * u[c];
+    f[12 + c][s] = TOTH ? (El + pr) * u[c] : rho * El * u[c]; f[15 + c][s] = El * u[c];
     f[18 + c][s] = rho * kl * u[c]; f[21 + c][s] = kl * u[c];
     for (int c2 = 0; c2 < 3; ++c2) { f[24 + 3 * c + c2][s] = q[c] * u[c2]; f[33 + 3 * c + c2][s] = u[c] * u[c2]; }
   }
@@ -89,14 +93,18 @@ __global__ void __launch_bounds__(64) k_convec_ref(const RefArgs a) {
   const double divU = gU[0][0] + gU[1][1] + gU[2][2];
   const double divQ = gQ[0][0] + gQ[1][1] + gQ[2][2];
   double Rm = 0.5 * (divQ + rho * divU);
-  double Re = 0.25 * (divFe + El * divQ + rho * El * divU + rho * divFue) +
-              0.25 * (divFk + kl * divQ + rho * kl * divU + rho * divFuk);
+  double Re = TOTH ? 0.5 * (divFe + (El + pr) * divU)
+                   : 0.25 * (divFe + El * divQ + rho * El * divU + rho * divFue) +
+                         0.25 * (divFk + kl * divQ + rho * kl * divU + rho * divFuk);
   double Rmo[3];
   for (int c = 0; c < 3; ++c) {
     Rmo[c] = 0.25 * (divF[c] + u[c] * divQ + q[c] * divU + rho * divFuu[c]) + gP[c];
     Rm = Rm + 0.5 * (u[c] * gRho[c]);
-    Re = Re + 0.25 * (q[c] * gE[c] + u[c] * gRE[c] + El * u[c] * gRho[c]) +
-         0.25 * (q[c] * gk[c] + u[c] * gRk[c] + kl * u[c] * gRho[c]);
+    if (TOTH)
+      Re = Re + 0.5 * (u[c] * gE[c]);
+    else
+      Re = Re + 0.25 * (q[c] * gE[c] + u[c] * gRE[c] + El * u[c] * gRho[c]) +
+           0.25 * (q[c] * gk[c] + u[c] * gRk[c] + kl * u[c] * gRho[c]);
     for (int c2 = 0; c2 < 3; ++c2) Rmo[c] = Rmo[c] + 0.25 * (u[c] * u[c2] * gRho[c2] + q[c2] * gU[c][c2] + u[c2] * gQ[c][c2]);
   }
   double* out = a.rel + (int64_t)e * NRES * NN + d;
@@ -338,7 +346,21 @@ int sod_full_convec_ijk(SodMesh* m, const double* u, const double* q, const doub
   if (rc) return rc;
   RefArgs a = ref_args(m);
   a.u = u; a.q = q; a.rho = rho; a.pr = pr; a.E = E;
-  k_convec_ref<<<m->nelem, 64, 0, st>>>(a);
+  k_convec_ref<false><<<m->nelem, 64, 0, st>>>(a);
+  SOD_CHECK_LAUNCH();
+  const size_t N = m->npoin;
+  return gather_out(m, nullptr, 0, 5, Rmass, Rmom, Rmom + N, Rmom + 2 * N, Rener, st);
+}
+
+int sod_full_convec_ijk_H(SodMesh* m, const double* u, const double* q, const double* rho, const double* pr,
+                          const double* E, double* Rmass, double* Rmom, double* Rener, sod_stream_t stream) {
+  SOD_ARG(m && u && q && rho && pr && E && Rmass && Rmom && Rener, "null argument");
+  cudaStream_t st = (cudaStream_t)stream;
+  int rc = ensure_step_buffers(m, false);
+  if (rc) return rc;
+  RefArgs a = ref_args(m);
+  a.u = u; a.q = q; a.rho = rho; a.pr = pr; a.E = E;
+  k_convec_ref<true><<<m->nelem, 64, 0, st>>>(a);
   SOD_CHECK_LAUNCH();
   const size_t N = m->npoin;
   return gather_out(m, nullptr, 0, 5, Rmass, Rmom, Rmom + N, Rmom + 2 * N, Rener, st);

@@ -49,7 +49,8 @@ def _stream(stream=None) -> C.c_void_p:
 
 def params_struct(prm: TGVParams) -> _lib.SodParams:
     return _lib.SodParams(prm.gamma_gas, prm.Rgas, prm.Cp, prm.Prt, prm.ce, prm.cmax, prm.cglob, prm.c_rho, prm.c_ener,
-                          int(prm.flag_normalise_entropy), prm.cfl_conv, prm.cfl_diff, int(prm.flag_les), prm.c_sgs)
+                          int(prm.flag_normalise_entropy), prm.cfl_conv, prm.cfl_diff, int(prm.flag_les), prm.c_sgs,
+                          int(getattr(prm, "flag_total_enthalpy", 0)))
 
 
 FP64 = _lib.SOD_FP64
@@ -315,6 +316,17 @@ class Sod2dMesh:
         Rmo = torch.empty(3, N, dtype=torch.float64, device="cuda")
         Re = torch.empty(N, dtype=torch.float64, device="cuda")
         _lib.check(_lib.load().sod_full_convec_ijk(self.handle, *(C.c_void_p(_ptr(t)) for t in (
+            u, q, rho, pr, E, Rm, Rmo, Re)), _stream(stream)))
+        return Rm, Rmo, Re
+
+    def full_convec_ijk_H(self, u, q, rho, pr, E, stream=None):
+        """full_convec_ijk_H: E is the total energy rho E."""
+        torch = _torch()
+        N = self.npoin
+        Rm = torch.empty(N, dtype=torch.float64, device="cuda")
+        Rmo = torch.empty(3, N, dtype=torch.float64, device="cuda")
+        Re = torch.empty(N, dtype=torch.float64, device="cuda")
+        _lib.check(_lib.load().sod_full_convec_ijk_H(self.handle, *(C.c_void_p(_ptr(t)) for t in (
             u, q, rho, pr, E, Rm, Rmo, Re)), _stream(stream)))
         return Rm, Rmo, Re
 
