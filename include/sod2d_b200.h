@@ -386,6 +386,15 @@ const char* sod_last_error(void);
 const char* sod_version(void);
 /* Number of kernels this library enqueued since load (for launch accounting). */
 int64_t sod_launch_count(void);
+/* Failure detection.  Every step checks its new rho, q and E on the device (one predicate per
+ * node in the update kernel) and raises a flag on a NaN/Inf; sod_check_finite waits for the
+ * stream's work, returns SOD_ERR_NONFINITE when the flag is up (steps since the last check) and
+ * clears it.  sod_rk4_main_host checks after its own step. */
+int sod_check_finite(SodMesh* mesh, sod_stream_t stream);
+/* Limit (seconds, 0 = none, the default) on the library's host waits for device work (the
+ * synchronous entry points: sod_rk4_main_host, sod_conjgrad_pressure, sod_check_finite);
+ * past it they return SOD_ERR_TIMEOUT and leave the queued work to complete on its own. */
+void sod_set_wait_timeout(double seconds);
 
 #ifdef __cplusplus
 }

@@ -103,6 +103,8 @@ _SIGS = {
     "sod_last_error": (C.c_char_p, []),
     "sod_version": (C.c_char_p, []),
     "sod_launch_count": (C.c_int64, []),
+    "sod_check_finite": (_i, [_p, _p]),
+    "sod_set_wait_timeout": (None, [_d]),
 }
 
 _lib = None

@@ -524,8 +524,7 @@ static int scalars(SodPoisson* P, int nblk, int mode, cudaStream_t st) {
 
 static int read_scalars(SodPoisson* P, cudaStream_t st) {
   SOD_CUDA(cudaMemcpyAsync(P->hscal, P->scal, sizeof(double) * S_COUNT, cudaMemcpyDeviceToHost, st));
-  SOD_CUDA(cudaStreamSynchronize(st));
-  return SOD_OK;
+  return sync_stream(st);
 }
 
 template <typename TV>

@@ -207,6 +207,10 @@ int mesh_ref_to_internal_elem(SodMesh* m, const double* ref_dev /*(nelem,64) F*/
 int mesh_internal_to_ref_elem(SodMesh* m, const double* int_dev, double* ref_dev, cudaStream_t st);
 int launch_copy_f32(const double* src, float* dst, int64_t n, cudaStream_t st);
 int init_kernel_attrs();
+// bounded host wait (sod_set_wait_timeout) and the non-finite flag of the stage-4 gather
+constexpr int kNonfiniteCounter = 1;  // index in StepBuffers::counters
+int sync_stream(cudaStream_t st);
+int take_nonfinite(SodMesh* m, cudaStream_t st, bool* flagged);
 // boundary conditions (sod_bc.cu), used by the step pipeline when m->bc.nb > 0
 int bc_snapshot_u(SodMesh* m, const double* u, cudaStream_t st);
 int bc_stage(SodMesh* m, double* ys, int stage, cudaStream_t st);

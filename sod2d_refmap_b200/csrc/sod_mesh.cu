@@ -11,11 +11,53 @@
 #include <cstring>
 #include <cmath>
 #include <algorithm>
+#include <chrono>
+#include <thread>
 
 namespace sod {
 
 static thread_local std::string g_err;
 std::atomic<int64_t> g_launches{0};
+static std::atomic<double> g_wait_timeout_s{0.0};
+
+// Host wait on a stream, given up after the sod_set_wait_timeout limit (0: no limit).  Giving
+// up leaves the device work queued; it completes on its own.
+int sync_stream(cudaStream_t st) {
+  const double lim = g_wait_timeout_s.load();
+  if (lim <= 0.0) {
+    SOD_CUDA(cudaStreamSynchronize(st));
+    return SOD_OK;
+  }
+  const auto t0 = std::chrono::steady_clock::now();
+  for (;;) {
+    const cudaError_t e = cudaStreamQuery(st);
+    if (e == cudaSuccess) return SOD_OK;
+    if (e != cudaErrorNotReady) {
+      set_error("stream wait: %s", cudaGetErrorString(e));
+      return SOD_ERR_CUDA;
+    }
+    if (std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count() > lim) {
+      set_error("host wait on device work exceeded %.3g s (sod_set_wait_timeout)", lim);
+      return SOD_ERR_TIMEOUT;
+    }
+    std::this_thread::yield();
+  }
+}
+
+// Reads and clears the non-finite flag the stage-4 gather sets (after the stream's work).
+int take_nonfinite(SodMesh* m, cudaStream_t st, bool* flagged) {
+  *flagged = false;
+  if (!m->buf.counters) return SOD_OK;
+  unsigned int h = 0;
+  SOD_CUDA(cudaMemcpyAsync(&h, m->buf.counters + kNonfiniteCounter, sizeof(unsigned int), cudaMemcpyDeviceToHost,
+                           st));
+  if (int rc = sync_stream(st)) return rc;
+  if (h) {
+    SOD_CUDA(cudaMemsetAsync(m->buf.counters + kNonfiniteCounter, 0, sizeof(unsigned int), st));
+    *flagged = true;
+  }
+  return SOD_OK;
+}
 
 void set_error(const char* fmt, ...) {
   char buf[1024];
@@ -218,6 +260,19 @@ extern "C" {
 const char* sod_last_error(void) { return sod::g_err.c_str(); }
 const char* sod_version(void) { return "sod2d_b200 0.1 (sm_100a)"; }
 int64_t sod_launch_count(void) { return sod::g_launches.load(); }
+
+void sod_set_wait_timeout(double seconds) { sod::g_wait_timeout_s.store(seconds > 0.0 ? seconds : 0.0); }
+
+int sod_check_finite(SodMesh* m, sod_stream_t stream) {
+  SOD_ARG(m, "mesh null");
+  bool bad = false;
+  if (int rc = take_nonfinite(m, (cudaStream_t)stream, &bad)) return rc;
+  if (bad) {
+    set_error("a non-finite value (NaN/Inf) appeared in rho, q or E during a step");
+    return SOD_ERR_NONFINITE;
+  }
+  return SOD_OK;
+}
 
 void sod_params_default(SodParams* p) {
   if (!p) return;

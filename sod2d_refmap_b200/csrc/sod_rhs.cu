@@ -343,6 +343,7 @@ struct GatherArgs {
   double gamma, Rgas;
   double* red;              // partials [3*nblocks]
   unsigned int* counter;
+  unsigned int* nonfinite;  // raised by stage 4 on a NaN/Inf in the new rho, q, E
   double* scal;             // [0] eta mean, [1] eta norm
   int normalise;
 };
@@ -420,6 +421,8 @@ __global__ void __launch_bounds__(256, SOD_KG_MIN_BLOCKS) k_gather_rk(const Gath
           y[f] = a.y[f][n] - dt * rs[f];
           a.y[f][n] = y[f];
         }
+        if (!(isfinite(y[0]) && isfinite(y[1]) && isfinite(y[2]) && isfinite(y[3]) && isfinite(y[4])))
+          atomicOr(a.nonfinite, 1u);
         const double g = a.gamma;
         const double rho = y[0];
         const double u0 = y[1] / rho, u1 = y[2] / rho, u2 = y[3] / rho;
@@ -693,6 +696,7 @@ int launch_gather(SodMesh* m, bool mixed, int stage, GatherArgs& a, cudaStream_t
   a.rsum = m->buf.rsum;
   a.red = m->buf.red;
   a.counter = m->buf.counters + 0;
+  a.nonfinite = m->buf.counters + kNonfiniteCounter;
   a.scal = m->buf.scal;
   if (stage >= 1) {
     a.b_cur = kB[stage - 1];
@@ -1148,7 +1152,13 @@ int sod_rk4_main_host(SodMesh* m, SodState* h, double dt_host, double* dt_next_h
   for (auto& o : outs)
     if (o.hst) SOD_CUDA(cudaMemcpyAsync(o.hst, o.dev, o.n * 8, cudaMemcpyDeviceToHost, st));
   if (dt_next_host) SOD_CUDA(cudaMemcpyAsync(dt_next_host, ddt, 8, cudaMemcpyDeviceToHost, st));
-  SOD_CUDA(cudaStreamSynchronize(st));
+  if (int rc2 = sync_stream(st)) return rc2;
+  bool bad = false;
+  if (int rc3 = take_nonfinite(m, st, &bad)) return rc3;
+  if (bad) {
+    set_error("a non-finite value (NaN/Inf) appeared in rho, q or E during the step");
+    return SOD_ERR_NONFINITE;
+  }
   return SOD_OK;
 }
 

@@ -53,6 +53,11 @@ def params_struct(prm: TGVParams) -> _lib.SodParams:
                           int(getattr(prm, "flag_total_enthalpy", 0)))
 
 
+def set_wait_timeout(seconds: float):
+    """Limit on the library's host waits (0 = none); past it calls raise SOD_ERR_TIMEOUT."""
+    _lib.load().sod_set_wait_timeout(C.c_double(float(seconds)))
+
+
 FP64 = _lib.SOD_FP64
 MIXED = _lib.SOD_MIXED
 
@@ -168,6 +173,11 @@ class Sod2dMesh:
         self.prm = prm
         p = params_struct(prm)
         _lib.check(_lib.load().sod_mesh_set_params(self.handle, C.byref(p)))
+
+    def check_finite(self, stream=None):
+        """Raises SodError(SOD_ERR_NONFINITE) when a step since the last check produced a NaN/Inf
+        in rho, q or E (waits for the stream's work; clears the flag)."""
+        _lib.check(_lib.load().sod_check_finite(self.handle, _stream(stream)))
 
     # ---- boundary conditions (non-periodic meshes) -------------------------------------
     def set_boundaries(self, bou_codes_nodes, lnbn_nodes, normals, u_buffer=None, bc: dict | None = None):
