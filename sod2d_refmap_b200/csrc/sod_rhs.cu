@@ -366,7 +366,9 @@ __device__ __forceinline__ void block_reduce3(double& s, double& mx, double& mn,
 }
 
 #ifndef SOD_KG_MIN_BLOCKS
-#define SOD_KG_MIN_BLOCKS 7  // resident 256-thread blocks per SM the register budget must allow
+// resident 256-thread blocks per SM the register budget must allow: 4 leaves 64 registers, no
+// spills (7 blocks capped the kernel at 32 registers and spilled 140-244 bytes per thread)
+#define SOD_KG_MIN_BLOCKS 4
 #endif
 template <typename R, int STAGE>
 __global__ void __launch_bounds__(256, SOD_KG_MIN_BLOCKS) k_gather_rk(const GatherArgs a) {
@@ -375,6 +377,16 @@ __global__ void __launch_bounds__(256, SOD_KG_MIN_BLOCKS) k_gather_rk(const Gath
   double eta_n = 0.0;
   if (act) {
     const R* rel = reinterpret_cast<const R*>(a.rel);
+    const size_t N = (size_t)a.npoin;
+    // node data independent of the gather, loaded first so their latency overlaps it
+    double yv[5], rsv[6];
+    if constexpr (STAGE >= 1) {
+#pragma unroll
+      for (int f = 0; f < 5; ++f) yv[f] = a.y[f][n];
+#pragma unroll
+      for (int f = 0; f < 6; ++f) rsv[f] = STAGE == 1 ? 0.0 : a.rsum[f * N + n];
+    }
+    const double ml = a.Ml[n];
     double r[6] = {0, 0, 0, 0, 0, 0};
     const int beg = a.ptr[n], end = a.ptr[n + 1];
     int c = beg;
@@ -394,10 +406,8 @@ __global__ void __launch_bounds__(256, SOD_KG_MIN_BLOCKS) k_gather_rk(const Gath
 #pragma unroll
       for (int f = 0; f < 6; ++f) r[f] += (double)v[f];
     }
-    const double ml = a.Ml[n];
 #pragma unroll
     for (int f = 0; f < 6; ++f) r[f] = r[f] / ml;
-    const size_t N = (size_t)a.npoin;
     if constexpr (STAGE == 0) {
 #pragma unroll
       for (int f = 0; f < 6; ++f)
@@ -406,19 +416,19 @@ __global__ void __launch_bounds__(256, SOD_KG_MIN_BLOCKS) k_gather_rk(const Gath
       const double dt = a.node_member ? a.dt[a.node_member[n]] : *a.dt;
       double rs[6];
 #pragma unroll
-      for (int f = 0; f < 6; ++f) rs[f] = (STAGE == 1 ? 0.0 : a.rsum[f * N + n]) + a.b_cur * r[f];
+      for (int f = 0; f < 6; ++f) rs[f] = rsv[f] + a.b_cur * r[f];
       if constexpr (STAGE < 4) {
 #pragma unroll
         for (int f = 0; f < 6; ++f) a.rsum[f * N + n] = rs[f];
         const double da = dt * a.a_next;
 #pragma unroll
-        for (int f = 0; f < 5; ++f) a.ys[f * N + n] = a.y[f][n] - da * r[f];
+        for (int f = 0; f < 5; ++f) a.ys[f * N + n] = yv[f] - da * r[f];
       } else {
         // RK update (time_integ.f90:417-426) and EOS at the new level (:445-463)
         double y[5];
 #pragma unroll
         for (int f = 0; f < 5; ++f) {
-          y[f] = a.y[f][n] - dt * rs[f];
+          y[f] = yv[f] - dt * rs[f];
           a.y[f][n] = y[f];
         }
         if (!(isfinite(y[0]) && isfinite(y[1]) && isfinite(y[2]) && isfinite(y[3]) && isfinite(y[4])))
