@@ -545,6 +545,9 @@ __global__ void __launch_bounds__(64 * KV_EPB, SOD_KV_MIN_BLOCKS) k_visc_dt(cons
   const int ee = act ? e : a.nelem - 1;
   const int n = a.econn[(size_t)ee * NN + d];
   const double rho = a.rho[n], u0 = a.u0[n], u1 = a.u1[n], u2 = a.u2[n], cs = a.csound[n], T = a.Tem[n];
+  // inputs of the second half, loaded before the element reductions so their latency overlaps them
+  const double reta_n = a.Reta[n];
+  const double hl = a.helem_l[(size_t)ee * NN + d];
   const double vmag = sqrt(u0 * u0 + u1 * u1 + u2 * u2);
   const double he = a.helem[ee];
   // betae node term (mod_entropy_viscosity.f90:90-95)
@@ -586,8 +589,7 @@ __global__ void __launch_bounds__(64 * KV_EPB, SOD_KV_MIN_BLOCKS) k_visc_dt(cons
   mB = fmax(wm[es][0][2], wm[es][1][2]);
   const int mem = a.elem_member ? a.elem_member[ee] : 0;
   const double norm = a.elem_member ? a.member_scal[2 * mem + 1] : a.scal[1];
-  const double R1 = (norm > 0.0) ? rho * fabs(a.Reta[n]) / norm : 0.0;
-  const double hl = a.helem_l[(size_t)ee * NN + d];
+  const double R1 = (norm > 0.0) ? rho * fabs(reta_n) / norm : 0.0;
   const double Ve = ced * R1 * hl * hl;
   ml[es][d] = a.prm.cglob * fmin(Ve, mB);
   __syncthreads();
