@@ -539,8 +539,9 @@ int sod_rk4_step_vjp(SodMesh* m, const double* rho, const double* q, const doubl
                      sod_stream_t stream) {
   SOD_ARG(m && rho && q && E && mu_e && mu_factor && dt_dev, "inputs null");
   SOD_ARG(bar_rho && bar_q && bar_E && out_rho && out_q && out_E, "adjoint arrays null");
-  if (m->bc.nb > 0 || m->prm.total_enthalpy) {
-    set_error("sod_rk4_step_vjp: the adjoint of the boundary routines and of full_convec_ijk_H is not built");
+  if (m->bc.nb > 0 || m->prm.total_enthalpy || m->prm.flag_les) {
+    set_error("sod_rk4_step_vjp: the adjoint of the boundary routines, of full_convec_ijk_H and of the LES "
+              "viscosity is not built");
     return SOD_ERR_UNSUPPORTED;
   }
   cudaStream_t st = (cudaStream_t)stream;

@@ -70,3 +70,17 @@ def test_les_graph_matches_eager_and_mixed_close(env):
         assert torch.equal(getattr(a, k), getattr(b, k)), k
     for k in ("rho", "q", "E"):
         assert float((getattr(c, k) - getattr(a, k)).norm() / getattr(a, k).norm()) < 1e-7, k
+
+
+def test_les_step_adjoint_rejected(env):
+    """The step adjoint does not differentiate the SGS viscosity: it refuses LES steps."""
+    from sod2d_refmap_b200 import _lib
+    S, gm, torch = env["S"], env["gm"], env["torch"]
+    s = S.Sod2dState.from_host(env["st0"], gm.nelem)
+    s.dt.fill_(env["dt"])
+    stages = torch.zeros(15 * env["m"].npoin, dtype=torch.float64, device="cuda")
+    with pytest.raises(_lib.SodError, match="SOD_ERR_UNSUPPORTED"):
+        gm.rk_4_main_record(s, stages, update_dt=False)
+    with pytest.raises(_lib.SodError, match="SOD_ERR_UNSUPPORTED"):
+        gm.rk4_step_vjp(s.rho, s.q, s.E, s.mu_e, s.mu_factor, s.dt, s.rho.clone(), s.q.clone(), s.E.clone(),
+                        stages=stages)
