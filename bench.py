@@ -597,6 +597,17 @@ def run_ours(args):
             roof["traffic"] = float(per_elem) * gm.nelem
             roof["traffic_note"] = ("ncu DRAM bytes per element on the 32^3 profile case, scaled by the "
                                     "element count: " + kv.get("source", ""))
+        wf = kv.get("k_rhs_mixed2_shared_wavefronts_per_element")
+        if wf:
+            # the binding resource of the kernel: one 128-byte shared-memory wavefront per SM clock
+            clk = (clocks or {}).get("sm_mhz") or 1965.0
+            per_s = float(wf) * gm.nelem / (kr_ms / 1e3)
+            peak = 148 * clk * 1e6
+            roof["shared_memory"] = {"achieved_Gwavefronts_per_s": per_s / 1e9, "peak_Gwavefronts_per_s": peak / 1e9,
+                                     "frac": per_s / peak, "achieved_TBs": per_s * 128 / 1e12,
+                                     "note": "ncu shared-memory wavefronts per element (32^3 profile case) x elements "
+                                             "over the measured launch time, against 1 wavefront (128 B) per SM "
+                                             "clock at the sampled SM clock"}
     cg = None if args.no_cg else bench_cg(args.cg_n)
     batch = None if args.no_batch else bench_batch(args.batch_members, args.batch_steps)
     adjoint = None if args.no_adjoint else bench_adjoint(args.adj_n, args.adj_steps, args.adj_every)
