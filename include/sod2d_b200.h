@@ -321,8 +321,8 @@ int sod_tgv_diagnostics(SodMesh* mesh, const double* rho, const double* u, const
 
 /* ---- Adjoint (reverse mode) of the RHS and of one RK4 step ------------------------------ */
 /* No counterpart in the reference (SOD2D has no adjoint); these differentiate the FP64 path of
- * sod_rhs / sod_rk4_main with the entropy viscosity mu_e (and dt) frozen at the given values,
- * Sutherland's law differentiated, no SGS viscosity.  All arrays are device arrays in the
+ * sod_rhs / sod_rk4_main with the entropy viscosity mu_e (and dt, and the LES mu_sgs of the
+ * step) frozen at the given values, Sutherland's law differentiated.  All arrays are device arrays in the
  * SodState layouts (q and its adjoints: 3 columns of npoin). */
 
 /* VJP of the stage RHS of sod_rhs (Rmass, Rmom, Rener, already divided by Ml): given seeds
@@ -336,13 +336,15 @@ int sod_rhs_vjp(SodMesh* mesh, const double* rho, const double* q, const double*
 int sod_rk4_main_record(SodMesh* mesh, SodState* state, const double* dt_dev, double* dt_next_dev,
                         double* stages, SodPrecision prec, sod_stream_t stream);
 /* VJP of one RK4 step y_{n+1} = y_n - dt sum_s b_s R(Y_s) (rk_4_main, time_integ.f90:288-426)
- * at the state (rho, q, E) with mu_e and dt_dev frozen: out = (dy_{n+1}/dy_n)^T bar.  stages
+ * at the state (rho, q, E) with mu_e, mu_sgs and dt_dev frozen: out = (dy_{n+1}/dy_n)^T bar.
+ * mu_sgs (nelem,64): the step's SGS viscosity when flag_les = 1 (rho mu_sgs in the stress and
+ * Cp/0.9 rho mu_sgs in the heat flux, differentiated through rho), null otherwise.  stages
  * from sod_rk4_main_record, or null to recompute them; out may alias bar. */
 int sod_rk4_step_vjp(SodMesh* mesh, const double* rho, const double* q, const double* E,
-                     const double* mu_e, const double* mu_factor, const double* dt_dev,
-                     const double* stages, const double* bar_rho, const double* bar_q,
-                     const double* bar_E, double* out_rho, double* out_q, double* out_E,
-                     sod_stream_t stream);
+                     const double* mu_e, const double* mu_sgs, const double* mu_factor,
+                     const double* dt_dev, const double* stages, const double* bar_rho,
+                     const double* bar_q, const double* bar_E, double* out_rho, double* out_q,
+                     double* out_E, sod_stream_t stream);
 
 /* ---- Legacy unit-test API ----------------------------------------------------------- */
 

@@ -77,7 +77,7 @@ _SIGS = {
     "sod_conjgrad_pressure": (_i, [_p, _p, _p, _i, _d, _i, _p, _p, _p]),
     "sod_csr_spmv_scal": (_i, [C.c_int32, C.c_int32, _p, _p, _p, _p, _p, _p]),
     "sod_rhs_vjp": (_i, [_p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p]),
-    "sod_rk4_step_vjp": (_i, [_p] * 15),
+    "sod_rk4_step_vjp": (_i, [_p] * 16),
     "sod_tgv_diagnostics": (_i, [_p, _p, _p, _p, _p, _d, _d, _p, _p]),
     "sod_mesh_set_boundaries": (_i, [_p] * 6),
     "sod_bc_dirichlet_prim": (_i, [_p] * 7),

@@ -3,7 +3,8 @@
 The forward model is the FP64 ``rk_4_main`` time loop (time_integ.f90:137-493) with the entropy
 viscosity mu_e and the time step dt *frozen* along the trajectory: each step n uses the mu_e_n
 and dt_n that the undifferentiated solver produced for it (smart_visc_spectral and adapt_dt_cfl
-run in the forward pass, but their outputs are treated as constants).  The gradient therefore
+run in the forward pass, but their outputs are treated as constants).  With LES (flag_les = 1)
+the step's SGS viscosity mu_sgs_n (sgs_visc after the previous step) is frozen the same way.  The gradient therefore
 is the exact gradient of ``replay`` (the frozen-coefficient map), which is what the dot-product
 and finite-difference checks compare against.
 
@@ -31,6 +32,7 @@ class _Ckpt:
     E: object
     mu_e: object
     dt: object
+    mu_sgs: object = None  # LES: the step's frozen SGS viscosity
 
 
 def _clone_state(src: Sod2dState) -> Sod2dState:
@@ -41,8 +43,13 @@ def _clone_state(src: Sod2dState) -> Sod2dState:
     return dst
 
 
-def _ckpt(s: Sod2dState) -> _Ckpt:
-    return _Ckpt(s.rho.clone(), s.q.clone(), s.E.clone(), s.mu_e.clone(), s.dt.clone())
+def _les(mesh: Sod2dMesh) -> bool:
+    return int(getattr(mesh.prm, "flag_les", 0)) == 1
+
+
+def _ckpt(s: Sod2dState, les: bool = False) -> _Ckpt:
+    return _Ckpt(s.rho.clone(), s.q.clone(), s.E.clone(), s.mu_e.clone(), s.dt.clone(),
+                 s.mu_sgs.clone() if les else None)
 
 
 def _load(s: Sod2dState, c: _Ckpt):
@@ -51,37 +58,46 @@ def _load(s: Sod2dState, c: _Ckpt):
     s.E.copy_(c.E)
     s.mu_e.copy_(c.mu_e)
     s.dt.copy_(c.dt)
+    if c.mu_sgs is not None:
+        s.mu_sgs.copy_(c.mu_sgs)
 
 
 def rollout(mesh: Sod2dMesh, state: Sod2dState, nsteps: int, checkpoint_every: int = 10, precision: int = FP64):
     """Run nsteps steps in place (dt from the CFL condition after every step, as rk_4_main)
     and return the checkpoints [(step index, _Ckpt)] at multiples of checkpoint_every."""
     ck = []
+    les = _les(mesh)
     for n in range(nsteps):
         if n % checkpoint_every == 0:
-            ck.append((n, _ckpt(state)))
+            ck.append((n, _ckpt(state, les)))
         mesh.rk_4_main(state, precision, update_dt=True)
     return ck
 
 
-def replay(mesh: Sod2dMesh, state: Sod2dState, mu_e_seq, dt_seq, precision: int = FP64):
-    """The frozen-coefficient forward map: step n with mu_e_seq[n] and dt_seq[n] (device (1,))."""
-    for mu_e, dt in zip(mu_e_seq, dt_seq):
+def replay(mesh: Sod2dMesh, state: Sod2dState, mu_e_seq, dt_seq, precision: int = FP64, mu_sgs_seq=None):
+    """The frozen-coefficient forward map: step n with mu_e_seq[n], dt_seq[n] (device (1,)) and,
+    with LES, mu_sgs_seq[n]."""
+    for n, (mu_e, dt) in enumerate(zip(mu_e_seq, dt_seq)):
         state.mu_e.copy_(mu_e)
         state.dt.copy_(dt)
+        if mu_sgs_seq is not None:
+            state.mu_sgs.copy_(mu_sgs_seq[n])
         mesh.rk_4_main(state, precision, update_dt=False)
     return state
 
 
-def trajectory_coefficients(mesh: Sod2dMesh, state: Sod2dState, nsteps: int, precision: int = FP64):
-    """(mu_e_n, dt_n) of each step of the unfrozen forward run from a copy of state."""
+def trajectory_coefficients(mesh: Sod2dMesh, state: Sod2dState, nsteps: int, precision: int = FP64,
+                            with_sgs: bool = False):
+    """(mu_e_n, dt_n) of each step of the unfrozen forward run from a copy of state, and the
+    steps' mu_sgs_n as a third list when with_sgs."""
     s = _clone_state(state)
-    mus, dts = [], []
+    mus, dts, sgs = [], [], []
     for _ in range(nsteps):
         mus.append(s.mu_e.clone())
         dts.append(s.dt.clone())
+        sgs.append(s.mu_sgs.clone())
         mesh.rk_4_main(s, precision, update_dt=True)
-    return mus, dts
+    return (mus, dts, sgs) if with_sgs else (mus, dts)
 
 
 def backward_through(mesh: Sod2dMesh, template: Sod2dState, ckpts, nsteps: int, bar_rho, bar_q, bar_E,
@@ -99,8 +115,9 @@ def backward_through(mesh: Sod2dMesh, template: Sod2dState, ckpts, nsteps: int, 
         n1 = bounds[seg + 1]
         _load(s, c)
         stack = []
+        les = c.mu_sgs is not None
         for t in range(n1 - n0):
-            stack.append(_ckpt(s))
+            stack.append(_ckpt(s, les))
             if store_stages:
                 mesh.rk_4_main_record(s, stages[t], update_dt=True, precision=precision)
             else:
@@ -108,7 +125,8 @@ def backward_through(mesh: Sod2dMesh, template: Sod2dState, ckpts, nsteps: int, 
         for t in range(n1 - n0 - 1, -1, -1):
             cs = stack[t]
             mesh.rk4_step_vjp(cs.rho, cs.q, cs.E, cs.mu_e, template.mu_factor, cs.dt, bar_rho, bar_q, bar_E,
-                              out=(bar_rho, bar_q, bar_E), stages=stages[t] if store_stages else None)
+                              out=(bar_rho, bar_q, bar_E), stages=stages[t] if store_stages else None,
+                              mu_sgs=cs.mu_sgs)
     return bar_rho, bar_q, bar_E
 
 

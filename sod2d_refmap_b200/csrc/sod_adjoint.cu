@@ -25,6 +25,7 @@
 
 namespace sod {
 int ensure_step_buffers(SodMesh* m, bool mixed);
+int les_in(SodMesh* m, const SodState* s, cudaStream_t st);
 int launch_rhs(SodMesh* m, bool mixed, int epb, const double* rho, const double* q0, const double* q1,
                const double* q2, const double* E, const double* mu_factor, const double* musgs_int, cudaStream_t st);
 
@@ -50,6 +51,7 @@ struct VjpArgs {
   const int32_t* __restrict__ econn;
   const double* __restrict__ geo;
   const double* __restrict__ mue;        // internal [e][64]
+  const double* __restrict__ musgs;      // internal [e][64] frozen SGS viscosity, or null
   const double* __restrict__ rho;
   const double* __restrict__ q0;
   const double* __restrict__ q1;
@@ -114,6 +116,10 @@ __global__ void __launch_bounds__(64, SOD_VJP_MIN_BLOCKS) k_rhs_vjp(const VjpArg
   const double muf = mf * kC1 * (T * sqrt(T)) / (T + kS);
   const double dmuf_dT = mf * kC1 * (1.5 * sqrt(T) * (T + kS) - T * sqrt(T)) / ((T + kS) * (T + kS));
   const double mue = a.mue[(size_t)e * NN + d];
+  const double musgs = a.musgs ? a.musgs[(size_t)e * NN + d] : 0.0;
+  // elem_diffu.f90: the molecular part of the stress carries rho mu_sgs (mu_fgp), the heat flux
+  // Cp/0.9 rho mu_sgs; both enter the reverse sweep through rho
+  const double mufgp = muf + rho * musgs;
 
   // ---------------- forward recompute of the derivative quantities ----------------
   double* Fw = sm;
@@ -154,14 +160,14 @@ __global__ void __launch_bounds__(64, SOD_VJP_MIN_BLOCKS) k_rhs_vjp(const VjpArg
   const double divU = gU[0][0] + gU[1][1] + gU[2][2];
   const double divQ = gQ[0][0] + gQ[1][1] + gQ[2][2];
   // diffusion pass 1 (stresses) and the contravariant gradRho / gradT fluxes for pass 2
-  const double mut = muf + mue;
+  const double mut = mufgp + mue;
   double tau[3][3];
 #pragma unroll
   for (int r = 0; r < 3; ++r)
 #pragma unroll
     for (int c = 0; c < 3; ++c) tau[r][c] = mut * (gU[r][c] + gU[c][r]);
 #pragma unroll
-  for (int r = 0; r < 3; ++r) tau[r][r] -= muf * (2.0 / 3.0) * divU;
+  for (int r = 0; r < 3; ++r) tau[r][r] -= mufgp * (2.0 / 3.0) * divU;
   double* V6 = sm + NF_FWD * FSTRIDE;  // does not overlap the forward fields
 #pragma unroll
   for (int dir = 0; dir < 3; ++dir) {
@@ -187,9 +193,10 @@ __global__ void __launch_bounds__(64, SOD_VJP_MIN_BLOCKS) k_rhs_vjp(const VjpArg
   // divD(tau row r); nu_e and kappa belong to the output node
   const double CpPr = a.prm.Cp / a.prm.Prt;
   const double nu_e = a.prm.c_rho * mue / rho;
-  const double kappa = muf * CpPr + a.prm.c_ener * mue * CpPr;
+  const double kappa = muf * CpPr + a.prm.c_ener * mue * CpPr + a.prm.Cp09 * rho * musgs;
   rb += wm * divDr * (-a.prm.c_rho * mue / (rho * rho));
   mufb += we * divDgT * CpPr;
+  rb += we * divDgT * a.prm.Cp09 * musgs;
   double* S6 = sm;  // overlaps forward fields only (read before the last barrier), not V6
   S6[0 * FSTRIDE + s] = nu_e * wm;
   S6[1 * FSTRIDE + s] = we;
@@ -225,20 +232,23 @@ __global__ void __launch_bounds__(64, SOD_VJP_MIN_BLOCKS) k_rhs_vjp(const VjpArg
         for (int c = 0; c < 3; ++c) taub[v - 3][c] += Vb[c];
       }
     }
-    // tau_rc = (muf+mue)(du_r/dx_c + du_c/dx_r) - delta_rc muf 2/3 div u
+    // tau_rc = (mu_fgp+mue)(du_r/dx_c + du_c/dx_r) - delta_rc mu_fgp 2/3 div u, mu_fgp = muf + rho musgs
+    double mufgpb = 0.0;
 #pragma unroll
     for (int r = 0; r < 3; ++r)
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
         gUb[r][c] += mut * taub[r][c];
         gUb[c][r] += mut * taub[r][c];
-        mufb += taub[r][c] * (gU[r][c] + gU[c][r]);
+        mufgpb += taub[r][c] * (gU[r][c] + gU[c][r]);
       }
 #pragma unroll
     for (int r = 0; r < 3; ++r) {
-      mufb += -taub[r][r] * (2.0 / 3.0) * divU;
-      divUb += -muf * (2.0 / 3.0) * taub[r][r];
+      mufgpb += -taub[r][r] * (2.0 / 3.0) * divU;
+      divUb += -mufgp * (2.0 / 3.0) * taub[r][r];
     }
+    mufb += mufgpb;
+    rb += mufgpb * musgs;
   }
 
   // convection (elem_convec.f90:412-434), seeds times gpvol; energy through H = h + k
@@ -464,12 +474,13 @@ __global__ void __launch_bounds__(256) k_stage_state(int64_t N, const int32_t* _
 }
 
 static int launch_vjp(SodMesh* m, const double* rho, const double* q0, const double* q1, const double* q2,
-                      const double* E, const double* mu_factor, const double* w, cudaStream_t st) {
+                      const double* E, const double* mu_factor, const double* musgs, const double* w, cudaStream_t st) {
   VjpArgs a;
   a.nelem = m->nelem;
   a.econn = m->econn;
   a.geo = m->geo64;
   a.mue = m->mue_int;
+  a.musgs = musgs;
   a.rho = rho; a.q0 = q0; a.q1 = q1; a.q2 = q2; a.E = E;
   a.mu_factor = mu_factor;
   a.w = w;
@@ -524,7 +535,7 @@ int sod_rhs_vjp(SodMesh* m, const double* rho, const double* q, const double* E,
   MCols5 none{{nullptr, nullptr, nullptr, nullptr, nullptr}};
   k_seed<<<nblk(N), 256, 0, st>>>(N, src, m->Ml, nullptr, 1.0, w, none);
   SOD_CHECK_LAUNCH();
-  rc = launch_vjp(m, rho, q, q + N, q + 2 * N, E, mu_factor, w, st);
+  rc = launch_vjp(m, rho, q, q + N, q + 2 * N, E, mu_factor, nullptr, w, st);
   if (rc) return rc;
   MCols5 out{{grad_rho, grad_q, grad_q + N, grad_q + 2 * N, grad_E}};
   k_gather_vjp<<<nblk(N), 256, 0, st>>>(N, m->n2e_ptr, m->n2e, reinterpret_cast<const double*>(m->buf.rel), out, 0,
@@ -534,19 +545,27 @@ int sod_rhs_vjp(SodMesh* m, const double* rho, const double* q, const double* E,
 }
 
 int sod_rk4_step_vjp(SodMesh* m, const double* rho, const double* q, const double* E, const double* mu_e,
-                     const double* mu_factor, const double* dt_dev, const double* stages, const double* bar_rho,
-                     const double* bar_q, const double* bar_E, double* out_rho, double* out_q, double* out_E,
-                     sod_stream_t stream) {
+                     const double* mu_sgs, const double* mu_factor, const double* dt_dev, const double* stages,
+                     const double* bar_rho, const double* bar_q, const double* bar_E, double* out_rho, double* out_q,
+                     double* out_E, sod_stream_t stream) {
   SOD_ARG(m && rho && q && E && mu_e && mu_factor && dt_dev, "inputs null");
   SOD_ARG(bar_rho && bar_q && bar_E && out_rho && out_q && out_E, "adjoint arrays null");
-  if (m->bc.nb > 0 || m->prm.total_enthalpy || m->prm.flag_les) {
-    set_error("sod_rk4_step_vjp: the adjoint of the boundary routines, of full_convec_ijk_H and of the LES "
-              "viscosity is not built");
+  if (m->bc.nb > 0 || m->prm.total_enthalpy) {
+    set_error("sod_rk4_step_vjp: the adjoint of the boundary routines and of full_convec_ijk_H is not built");
     return SOD_ERR_UNSUPPORTED;
   }
   cudaStream_t st = (cudaStream_t)stream;
   int rc = ensure_step_buffers(m, false);
   if (rc) return rc;
+  // LES: the step's frozen mu_sgs in the internal layout (the forward re-derives it per step)
+  const double* musgs = nullptr;
+  if (m->prm.flag_les == 1 && mu_sgs) {
+    SodState tmp{};
+    tmp.mu_sgs = const_cast<double*>(mu_sgs);
+    rc = les_in(m, &tmp, st);
+    if (rc) return rc;
+    musgs = m->musgs_int;
+  }
   const int64_t N = m->npoin;
   // scratch: ybar copy | w | (ys2 ys3 ys4 when the stages are not given)   (5 columns each)
   rc = ensure_adj(m, (stages ? 10 : 25) * (size_t)N);
@@ -567,7 +586,7 @@ int sod_rk4_step_vjp(SodMesh* m, const double* rho, const double* q, const doubl
     Cols5 cur = y0;
     for (int t = 0; t < 3; ++t) {
       double* b = m->adj + (size_t)(10 + 5 * t) * N;
-      rc = launch_rhs(m, false, epb, cur.c[0], cur.c[1], cur.c[2], cur.c[3], cur.c[4], mu_factor, nullptr, st);
+      rc = launch_rhs(m, false, epb, cur.c[0], cur.c[1], cur.c[2], cur.c[3], cur.c[4], mu_factor, musgs, st);
       if (rc) return rc;
       k_stage_state<<<nblk(N), 256, 0, st>>>(N, m->n2e_ptr, m->n2e, rel, m->Ml, dt_dev, acoef[t], y0, b);
       SOD_CHECK_LAUNCH();
@@ -590,7 +609,7 @@ int sod_rk4_step_vjp(SodMesh* m, const double* rho, const double* q, const doubl
     const Cols5 ysrc = stage == 1 ? y0
                                   : Cols5{{ys[stage - 2], ys[stage - 2] + N, ys[stage - 2] + 2 * N,
                                            ys[stage - 2] + 3 * N, ys[stage - 2] + 4 * N}};
-    rc = launch_vjp(m, ysrc.c[0], ysrc.c[1], ysrc.c[2], ysrc.c[3], ysrc.c[4], mu_factor, w, st);
+    rc = launch_vjp(m, ysrc.c[0], ysrc.c[1], ysrc.c[2], ysrc.c[3], ysrc.c[4], mu_factor, musgs, w, st);
     if (rc) return rc;
     const int t = 4 - stage;
     k_gather_vjp<<<nblk(N), 256, 0, st>>>(N, m->n2e_ptr, m->n2e, rel, acc, 1, yb, m->Ml, dt_dev, cb[t], ca[t],

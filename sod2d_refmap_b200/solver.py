@@ -296,16 +296,18 @@ class Sod2dMesh:
                                                   _stream(stream)))
 
     def rk4_step_vjp(self, rho, q, E, mu_e, mu_factor, dt, bar_rho, bar_q, bar_E, out=None, stages=None,
-                     stream=None):
-        """Adjoint of one FP64 RK4 step from (rho, q, E) with mu_e and dt (device (1,)) frozen;
-        stages from rk_4_main_record of the same step (recomputed when None)."""
+                     mu_sgs=None, stream=None):
+        """Adjoint of one FP64 RK4 step from (rho, q, E) with mu_e, mu_sgs (LES, or None) and dt
+        (device (1,)) frozen; stages from rk_4_main_record of the same step (recomputed when None)."""
         torch = _torch()
         N = self.npoin
         if out is None:
             out = (torch.empty(N, dtype=torch.float64, device="cuda"),
                    torch.empty(3, N, dtype=torch.float64, device="cuda"),
                    torch.empty(N, dtype=torch.float64, device="cuda"))
-        args = [_contig(t) for t in (rho, q, E, mu_e, mu_factor, dt)]
+        args = [_contig(t) for t in (rho, q, E, mu_e)]
+        args += [None if mu_sgs is None else _contig(mu_sgs)]
+        args += [_contig(t) for t in (mu_factor, dt)]
         args += [None if stages is None else _contig(stages)]
         args += [_contig(t) for t in (bar_rho, bar_q, bar_E)]
         _lib.check(_lib.load().sod_rk4_step_vjp(self.handle, *(C.c_void_p(_ptr(t)) for t in args + list(out)),
