@@ -512,16 +512,18 @@ inline void full_convec_ijk(const ElemCtx& ctx, const double* u, const double* q
 
 // full_convec_ijk_H (elem_convec.f90:20-208): the convective residual with the total-enthalpy
 // energy flux (E + p) u; E is the total energy rho E here (time_integ.f90:362).
-inline void full_convec_ijk_H(const ElemCtx& ctx, const double* u, const double* q, const double* rho,
-                              const double* pr, const double* E, double* Rmass, double* Rmom, double* Rener) {
+// Templated on the scalar type (double, and the dual numbers of the forward-mode JVP).
+template <class T>
+inline void full_convec_ijk_H(const ElemCtx& ctx, const T* u, const T* q, const T* rho, const T* pr, const T* E,
+                              T* Rmass, T* Rmom, T* Rener) {
   const int nelem = ctx.nelem, npoin = ctx.npoin;
   for (int64_t p = 0; p < (int64_t)npoin * 3; ++p) Rmom[p] = 0.0;
   for (int p = 0; p < npoin; ++p) { Rmass[p] = 0.0; Rener[p] = 0.0; }
   for_each_element_coloured(ctx, [&](int ielem) {
     int ipoin[nnode];
-    double Re_mom[nnode][3], Re_mass[nnode], Re_ener[nnode];
-    double ul[nnode][3], ql[nnode][3], rhol[nnode], prl[nnode], El[nnode], fel[nnode][3];
-    double fl[nnode][3][3], fuul[nnode][3][3];
+    T Re_mom[nnode][3], Re_mass[nnode], Re_ener[nnode];
+    T ul[nnode][3], ql[nnode][3], rhol[nnode], prl[nnode], El[nnode], fel[nnode][3];
+    T fl[nnode][3][3], fuul[nnode][3][3];
     for (int a = 0; a < nnode; ++a) ipoin[a] = ctx.connec[ielem + (int64_t)nelem * a];
     for (int d = 0; d < 3; ++d)
       for (int a = 0; a < nnode; ++a) {
@@ -548,8 +550,8 @@ inline void full_convec_ijk_H(const ElemCtx& ctx, const double* u, const double*
         dlzeta[ii] = SOD_DL(igaus, 2, ii);
       }
       int isoI = ctx.gmshAtoI[igaus], isoJ = ctx.gmshAtoJ[igaus], isoK = ctx.gmshAtoK[igaus];
-      double gIRho[3] = {0, 0, 0}, gIP[3] = {0, 0, 0}, gIE[3] = {0, 0, 0};
-      double gIU[3][3] = {}, gIQ[3][3] = {}, gIFe[3][3] = {}, gIF[3][3][3] = {}, gIFuu[3][3][3] = {};
+      T gIRho[3] = {0, 0, 0}, gIP[3] = {0, 0, 0}, gIE[3] = {0, 0, 0};
+      T gIU[3][3] = {}, gIQ[3][3] = {}, gIFe[3][3] = {}, gIF[3][3][3] = {}, gIFuu[3][3][3] = {};
       for (int ii = 0; ii < 4; ++ii) {
         int a1 = SOD_INV(ii, isoJ, isoK), a2 = SOD_INV(isoI, ii, isoK), a3 = SOD_INV(isoI, isoJ, ii);
         gIRho[0] += dlxi[ii] * rhol[a1]; gIRho[1] += dleta[ii] * rhol[a2]; gIRho[2] += dlzeta[ii] * rhol[a3];
@@ -571,9 +573,9 @@ inline void full_convec_ijk_H(const ElemCtx& ctx, const double* u, const double*
           }
         }
       }
-      double gradRho[3] = {0, 0, 0}, gradP[3] = {0, 0, 0}, gradE[3] = {0, 0, 0};
-      double gradU[3][3] = {}, gradQ[3][3] = {}, divF[3] = {0, 0, 0}, divFuu[3] = {0, 0, 0};
-      double divFe = 0.0;
+      T gradRho[3] = {0, 0, 0}, gradP[3] = {0, 0, 0}, gradE[3] = {0, 0, 0};
+      T gradU[3][3] = {}, gradQ[3][3] = {}, divF[3] = {0, 0, 0}, divFuu[3] = {0, 0, 0};
+      T divFe = 0.0;
       for (int id = 0; id < 3; ++id)
         for (int jd = 0; jd < 3; ++jd) {
           double h = SOD_HE(id, jd, igaus, ielem);
@@ -589,8 +591,8 @@ inline void full_convec_ijk_H(const ElemCtx& ctx, const double* u, const double*
             divFuu[id] += h2 * gIFuu[id][jd][kd];
           }
         }
-      double divU = gradU[0][0] + gradU[1][1] + gradU[2][2];
-      double divQ = gradQ[0][0] + gradQ[1][1] + gradQ[2][2];
+      T divU = gradU[0][0] + gradU[1][1] + gradU[2][2];
+      T divQ = gradQ[0][0] + gradQ[1][1] + gradQ[2][2];
       Re_mass[igaus] = 0.5 * (divQ + rhol[igaus] * divU);
       Re_ener[igaus] = 0.5 * (divFe + (El[igaus] + prl[igaus]) * divU);
       for (int id = 0; id < 3; ++id) {
@@ -1077,7 +1079,8 @@ inline void full_diffusion_ijk_t(const ElemCtx& ctx, const Params& P, const T* r
 }
 
 // The stage RHS of rk_4_main without the entropy residual (time_integ.f90:266-393): EOS,
-// Sutherland, full_diffusion_ijk + full_convec_ijk (energy with h), sum, /Ml.  State in
+// Sutherland, full_diffusion_ijk + full_convec_ijk (energy with h; full_convec_ijk_H with the
+// total-enthalpy flag), sum, /Ml.  State in
 // (rho, q(npoin,3), E); R is 5 columns of npoin: mass, mom x3, energy.  mu_e frozen.
 template <class T>
 inline void rhs_stage_t(const ElemCtx& ctx, const Params& P, const double* Ml, const double* mu_factor,
@@ -1100,7 +1103,10 @@ inline void rhs_stage_t(const ElemCtx& ctx, const Params& P, const double* Ml, c
   }
   full_diffusion_ijk_t<T>(ctx, P, rho, rho, u.data(), Tem.data(), muf.data(), mu_e, mu_sgs, Dm.data(), Dmo.data(),
                           De.data());
-  full_convec_ijk_t<T>(ctx, u.data(), q, rho, pr.data(), h.data(), Rm.data(), Rmo.data(), Re.data());
+  if (P.flag_total_enthalpy)  // time_integ.f90:361-365
+    full_convec_ijk_H<T>(ctx, u.data(), q, rho, pr.data(), E, Rm.data(), Rmo.data(), Re.data());
+  else
+    full_convec_ijk_t<T>(ctx, u.data(), q, rho, pr.data(), h.data(), Rm.data(), Rmo.data(), Re.data());
   for (int p = 0; p < npoin; ++p) {
     R[p] = (Rm[p] + Dm[p]) / Ml[p];
     for (int d = 0; d < 3; ++d) R[p + N * (1 + d)] = (Rmo[p + N * d] + Dmo[p + N * d]) / Ml[p];

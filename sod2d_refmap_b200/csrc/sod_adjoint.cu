@@ -89,6 +89,8 @@ __device__ constexpr int sym_j(int t) { return t < 3 ? t : (t < 5 ? t - 2 : 2); 
 #ifndef SOD_VJP_MIN_BLOCKS
 #define SOD_VJP_MIN_BLOCKS 1  // CTAs per SM the register allocation must allow
 #endif
+// TOTH: flag_total_enthalpy (energy convection of full_convec_ijk_H)
+template <bool TOTH>
 __global__ void __launch_bounds__(64, SOD_VJP_MIN_BLOCKS) k_rhs_vjp(const VjpArgs a) {
   __shared__ __align__(16) double sm[kArrays * FSTRIDE];
   __shared__ DMat Ds;
@@ -259,17 +261,26 @@ __global__ void __launch_bounds__(64, SOD_VJP_MIN_BLOCKS) k_rhs_vjp(const VjpArg
     divQb += 0.5 * mm; rb += 0.5 * divU * mm; divUb += 0.5 * rho * mm;
 #pragma unroll
     for (int c = 0; c < 3; ++c) { ub[c] += 0.5 * gRho[c] * mm; gRhob[c] += 0.5 * uv[c] * mm; }
-    // energy: 1/4 (H div q + rho H div u + q.grad H + u.grad(rho H) + H u.grad rho
-    //              + div(rho H u) + rho div(H u))
-    dFeb += 0.25 * me;
-    Hb += 0.25 * divQ * me; divQb += 0.25 * Ht * me;
-    rb += 0.25 * Ht * divU * me; Hb += 0.25 * rho * divU * me; divUb += 0.25 * rho * Ht * me;
-    rb += 0.25 * divHu * me; dFueb += 0.25 * rho * me;
+    if constexpr (TOTH) {
+      // full_convec_ijk_H (elem_convec.f90:171-177): 1/2 (div((E + p) u) + (E + p) div u
+      // + u.grad(E + p)) with E + p = rho H (the same function of rho, q, E)
+      dFeb += 0.5 * me;
+      rb += 0.5 * Ht * divU * me; Hb += 0.5 * rho * divU * me; divUb += 0.5 * rho * Ht * me;
 #pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      qb[c] += 0.25 * gH[c] * me; gHb[c] += 0.25 * qv[c] * me;
-      ub[c] += 0.25 * gRH[c] * me; gRHb[c] += 0.25 * uv[c] * me;
-      Hb += 0.25 * uv[c] * gRho[c] * me; ub[c] += 0.25 * Ht * gRho[c] * me; gRhob[c] += 0.25 * Ht * uv[c] * me;
+      for (int c = 0; c < 3; ++c) { ub[c] += 0.5 * gRH[c] * me; gRHb[c] += 0.5 * uv[c] * me; }
+    } else {
+      // energy: 1/4 (H div q + rho H div u + q.grad H + u.grad(rho H) + H u.grad rho
+      //              + div(rho H u) + rho div(H u))
+      dFeb += 0.25 * me;
+      Hb += 0.25 * divQ * me; divQb += 0.25 * Ht * me;
+      rb += 0.25 * Ht * divU * me; Hb += 0.25 * rho * divU * me; divUb += 0.25 * rho * Ht * me;
+      rb += 0.25 * divHu * me; dFueb += 0.25 * rho * me;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        qb[c] += 0.25 * gH[c] * me; gHb[c] += 0.25 * qv[c] * me;
+        ub[c] += 0.25 * gRH[c] * me; gRHb[c] += 0.25 * uv[c] * me;
+        Hb += 0.25 * uv[c] * gRho[c] * me; ub[c] += 0.25 * Ht * gRho[c] * me; gRhob[c] += 0.25 * Ht * uv[c] * me;
+      }
     }
     // momentum: 1/4 (div(q u) + u div q + q div u + rho div(u u) + u u.grad rho + q.grad u + u.grad q)
     //           + grad p
@@ -488,7 +499,10 @@ static int launch_vjp(SodMesh* m, const double* rho, const double* q0, const dou
   a.out = reinterpret_cast<double*>(m->buf.rel);
   a.D = m->D;
   a.prm = m->prm;
-  k_rhs_vjp<<<m->nelem, NN, 0, st>>>(a);
+  if (m->prm.total_enthalpy)
+    k_rhs_vjp<true><<<m->nelem, NN, 0, st>>>(a);
+  else
+    k_rhs_vjp<false><<<m->nelem, NN, 0, st>>>(a);
   SOD_CHECK_LAUNCH();
   return SOD_OK;
 }
@@ -518,10 +532,6 @@ int sod_rhs_vjp(SodMesh* m, const double* rho, const double* q, const double* E,
                 double* grad_rho, double* grad_q, double* grad_E, sod_stream_t stream) {
   SOD_ARG(m && rho && q && E && mu_e && mu_factor, "inputs null");
   SOD_ARG(bar_Rmass && bar_Rmom && bar_Rener && grad_rho && grad_q && grad_E, "adjoint arrays null");
-  if (m->prm.total_enthalpy) {
-    set_error("sod_rhs_vjp: the adjoint of full_convec_ijk_H (flag_total_enthalpy) is not built");
-    return SOD_ERR_UNSUPPORTED;
-  }
   cudaStream_t st = (cudaStream_t)stream;
   int rc = ensure_step_buffers(m, false);
   if (rc) return rc;
@@ -550,8 +560,8 @@ int sod_rk4_step_vjp(SodMesh* m, const double* rho, const double* q, const doubl
                      double* out_E, sod_stream_t stream) {
   SOD_ARG(m && rho && q && E && mu_e && mu_factor && dt_dev, "inputs null");
   SOD_ARG(bar_rho && bar_q && bar_E && out_rho && out_q && out_E, "adjoint arrays null");
-  if (m->bc.nb > 0 || m->prm.total_enthalpy) {
-    set_error("sod_rk4_step_vjp: the adjoint of the boundary routines and of full_convec_ijk_H is not built");
+  if (m->bc.nb > 0) {
+    set_error("sod_rk4_step_vjp: the adjoint of the boundary routines is not built");
     return SOD_ERR_UNSUPPORTED;
   }
   cudaStream_t st = (cudaStream_t)stream;

@@ -924,8 +924,8 @@ int sod_rk4_main_record(SodMesh* m, SodState* s, const double* dt_dev, double* d
   if (rc) return rc;
   SOD_ARG(dt_dev && stages, "dt_dev/stages null");
   SOD_ARG(prec == SOD_FP64 || prec == SOD_MIXED, "precision");
-  if (m->bc.nb > 0 || m->prm.total_enthalpy) {
-    set_error("sod_rk4_main_record: the adjoint of the boundary routines and of full_convec_ijk_H is not built");
+  if (m->bc.nb > 0) {
+    set_error("sod_rk4_main_record: the adjoint of the boundary routines is not built");
     return SOD_ERR_UNSUPPORTED;
   }
   cudaStream_t st = (cudaStream_t)stream;

@@ -12,3 +12,30 @@ def t2n(t):
     """torch tensor in the (3,npoin)/(64,nelem) storage -> numpy in the reference Fortran shape."""
     a = t.detach().cpu().numpy()
     return np.asfortranarray(a.T) if a.ndim == 2 else a
+
+
+def oracle_step_jvp(oracle, om, prm, st, dt, v, mu_sgs=None):
+    """One rk_4_main step (time_integ.f90:288-426) from the FlowState st and its JVP along
+    v = (drho, dq (npoin,3), dE), composed from the oracle's dual-number stage JVPs with mu_e
+    (and mu_sgs) frozen."""
+    def with_state(rho, q, E):
+        s = st.copy()
+        s.rho = np.ascontiguousarray(rho); s.q = np.asfortranarray(q); s.E = np.ascontiguousarray(E)
+        return s
+    y0 = (st.rho, st.q, st.E)
+    acc_y = [a.copy() for a in y0]
+    acc_v = [a.copy() for a in v]
+    ys, vs = y0, v
+    a_next = [0.5, 0.5, 1.0, None]
+    b = [1 / 6, 1 / 3, 1 / 3, 1 / 6]
+    for s in range(4):
+        R, dR = oracle.rhs_jvp(om, prm, with_state(*ys), vs[0], vs[1], vs[2], mu_sgs=mu_sgs)
+        Rc = (R[0], np.asfortranarray(R[1:4].T), R[4])
+        dRc = (dR[0], np.asfortranarray(dR[1:4].T), dR[4])
+        for f in range(3):
+            acc_y[f] = acc_y[f] - dt * b[s] * Rc[f]
+            acc_v[f] = acc_v[f] - dt * b[s] * dRc[f]
+        if a_next[s] is not None:
+            ys = tuple(y0[f] - dt * a_next[s] * Rc[f] for f in range(3))
+            vs = tuple(v[f] - dt * a_next[s] * dRc[f] for f in range(3))
+    return acc_y, acc_v

@@ -1,7 +1,8 @@
 """flag_total_enthalpy: convection by full_convec_ijk_H (elem_convec.f90:20-208) as rk_4_main
 selects it (time_integ.f90:361-365), against the oracle.  FP64 bound 1e-12 relative per field
 (the rest of the FP64 path); the mixed path against FP64 with the bounds of the enthalpy path's
-mixed test on the same 4^3 mesh (stage RHS 1e-3, state after 10 steps 1e-6)."""
+mixed test on the same 4^3 mesh (stage RHS 1e-3, state after 10 steps 1e-6); the adjoints by
+dot-product tests against the oracle's dual-number JVP (1e-11)."""
 import dataclasses
 
 import numpy as np
@@ -88,14 +89,36 @@ def test_mixed_and_graph(env):
         assert rel_l2(t2n(getattr(c, k)), t2n(getattr(a, k))) < 1e-6, k
 
 
-def test_adjoint_rejects_total_enthalpy(env):
-    from sod2d_refmap_b200 import _lib
-    S, gm, torch = env["S"], env["gm"], env["torch"]
-    s = S.Sod2dState.from_host(env["st0"], gm.nelem)
-    s.dt.fill_(env["dt"])
-    stages = torch.zeros(15 * env["m"].npoin, dtype=torch.float64, device="cuda")
-    with pytest.raises(_lib.SodError, match="SOD_ERR_UNSUPPORTED"):
-        gm.rk_4_main_record(s, stages, update_dt=False)
+def test_adjoint_total_enthalpy(env, oracle):
+    """The RHS and step adjoints of the total-enthalpy path: dot-product tests against the
+    oracle's dual-number JVP of the same map (bound 1e-11 relative to sum |w_i (J v)_i|)."""
+    from _util import oracle_step_jvp
+    S, gm, om, prm, torch, dt = env["S"], env["gm"], env["om"], env["prm"], env["torch"], env["dt"]
+    st = env["st1"]
+    rng = np.random.default_rng(41)
+    rnd = lambda a: rng.standard_normal(a.shape) * np.abs(a).mean()
+    dev = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    v = (rnd(st.rho), np.asfortranarray(rnd(st.q)), rnd(st.E))
+    # stage RHS
+    _, dR = oracle.rhs_jvp(om, prm, st, *v)
+    w = np.stack([rnd(st.rho) for _ in range(5)])
+    g = gm.rhs_vjp(dev(st.rho), dev(st.q.T), dev(st.E), dev(st.mu_e.T), dev(st.mu_factor), dev(w[0]), dev(w[1:4]),
+                   dev(w[4]))
+    lhs = float((w * dR).sum())
+    rhs = sum(float((gi.cpu().numpy() * vi).sum()) for gi, vi in zip(g, (v[0], v[1].T, v[2])))
+    assert abs(lhs - rhs) <= 1e-11 * float(np.abs(w * dR).sum()), (lhs, rhs)
+    # one RK4 step
+    y1, dy1 = oracle_step_jvp(oracle, om, prm, st, dt, v)
+    wb = (rnd(st.rho), np.asfortranarray(rnd(st.q)), rnd(st.E))
+    dtd = torch.full((1,), dt, dtype=torch.float64, device="cuda")
+    out = gm.rk4_step_vjp(dev(st.rho), dev(st.q.T), dev(st.E), dev(st.mu_e.T), dev(st.mu_factor), dtd,
+                          dev(wb[0]), dev(wb[1].T), dev(wb[2]))
+    gs = [o.cpu().numpy() for o in out]
+    gs[1] = gs[1].T
+    terms = [wb[f] * dy1[f] for f in range(3)]
+    lhs = sum(t.sum() for t in terms)
+    rhs = sum((gs[f] * v[f]).sum() for f in range(3))
+    assert abs(lhs - rhs) <= 1e-11 * sum(np.abs(t).sum() for t in terms), (lhs, rhs)
 
 
 def test_set_params_drops_captured_graphs(env):
