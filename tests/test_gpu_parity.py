@@ -164,3 +164,26 @@ def test_mixed_precision_error(env, oracle):
     print("mixed state rel L2 after 10 steps:", serr)
     for k, e in serr.items():
         assert e < 1e-6, (k, e)
+
+
+def test_step_capturable_in_caller_graph(env):
+    """sod_rk4_main allocates and synchronizes nothing after its first call, so a caller can
+    capture it in its own CUDA graph; replays equal eager steps bit for bit (mixed, dt updated)."""
+    S, gm, torch = env["S"], env["gm"], env["torch"]
+    a = S.Sod2dState.from_host(env["st0"], gm.nelem); a.dt.fill_(env["dt"])
+    b = S.Sod2dState.from_host(env["st0"], gm.nelem); b.dt.fill_(env["dt"])
+    warm = S.Sod2dState.from_host(env["st0"], gm.nelem); warm.dt.fill_(env["dt"])
+    side = torch.cuda.Stream()
+    side.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(side):
+        gm.rk_4_main(warm, precision=S.MIXED, update_dt=True)  # first call: buffers allocated here
+    torch.cuda.current_stream().wait_stream(side)
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        gm.rk_4_main(a, precision=S.MIXED, update_dt=True)
+    for _ in range(3):
+        g.replay()
+        gm.rk_4_main(b, precision=S.MIXED, update_dt=True)
+    torch.cuda.synchronize()
+    for k in ("rho", "q", "E", "mu_e", "dt"):
+        assert torch.equal(getattr(a, k), getattr(b, k)), k
