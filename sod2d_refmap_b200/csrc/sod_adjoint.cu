@@ -564,6 +564,7 @@ int sod_rk4_step_vjp(SodMesh* m, const double* rho, const double* q, const doubl
     set_error("sod_rk4_step_vjp: the adjoint of the boundary routines is not built");
     return SOD_ERR_UNSUPPORTED;
   }
+  NvtxRange range("sod rk4 step vjp");
   cudaStream_t st = (cudaStream_t)stream;
   int rc = ensure_step_buffers(m, false);
   if (rc) return rc;

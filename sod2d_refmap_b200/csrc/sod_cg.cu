@@ -708,6 +708,7 @@ int sod_poisson_diag(SodPoisson* P, double* d, sod_stream_t stream) {
 int sod_conjgrad_pressure(SodPoisson* P, const double* Rp0, double* R, int max_iter, double tol, int mixed,
                           int* iters_out, double* rel_out, sod_stream_t stream) {
   SOD_ARG(P && Rp0 && R && max_iter > 0 && tol > 0.0, "conjgrad arguments");
+  NvtxRange range("sod conjgrad pressure");
   cudaStream_t st = (cudaStream_t)stream;
   const int n = (int)P->n;
   const int gb = node_grid(n);

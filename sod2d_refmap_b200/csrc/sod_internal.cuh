@@ -19,6 +19,7 @@
 #include <unordered_map>
 #include <vector>
 #include "../../include/sod2d_b200.h"
+#include <nvtx3/nvToolsExt.h>
 
 namespace sod {
 
@@ -36,6 +37,15 @@ constexpr int FSTRIDE = 4 * PLANE;    // 88
 __host__ __device__ constexpr int sidx(int i, int j, int k) { return i + 4 * j + PLANE * k; }
 
 void set_error(const char* fmt, ...);
+
+// Host-side NVTX range for the duration of a scope (no device synchronisation; visible to
+// Nsight tools, free otherwise).
+struct NvtxRange {
+  explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange&) = delete;
+  NvtxRange& operator=(const NvtxRange&) = delete;
+};
 extern std::atomic<int64_t> g_launches;
 
 #define SOD_CUDA(call)                                                                  \

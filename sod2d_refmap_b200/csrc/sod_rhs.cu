@@ -802,6 +802,7 @@ static double* reta_scratch(SodMesh* m) {
 // written there instead of the internal stage buffer (for the adjoint's reverse sweep).
 int run_step(SodMesh* m, SodState* s, const double* dt_dev, double* dt_next, bool mixed, cudaStream_t st,
              cudaEvent_t* ev = nullptr, double* stage_store = nullptr) {
+  NvtxRange range(mixed ? "sod rk4 step (mixed)" : "sod rk4 step (fp64)");
   const size_t N = m->npoin;
   const int epb = m->tuned_epb[mixed ? 1 : 0] ? m->tuned_epb[mixed ? 1 : 0] : (mixed ? 4 : 2);
   SodState loc = *s;
