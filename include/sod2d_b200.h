@@ -125,7 +125,8 @@ typedef struct {
  * to every stage state and to the updated state, and bc_fix_dirichlet_residual_entropy to the
  * entropy residual (time_integ.f90:256-259,299-301,434-437,474-477).  bou_codes_nodes = null
  * removes the boundaries.  Captured step graphs of the mesh are dropped.  The ensemble
- * (sod_batch_*) and the adjoint entry points reject meshes with boundaries. */
+ * (sod_batch_*) rejects meshes with boundaries; sod_rk4_step_vjp differentiates through the
+ * routines of codes 2-5 and 8 and rejects meshes holding codes 1, 6 or 7. */
 int sod_mesh_set_boundaries(SodMesh* mesh, const int32_t* bou_codes_nodes, const int32_t* lnbn_nodes,
                             const double* normalsAtNodes, const double* u_buffer, const SodBcParams* bc);
 
@@ -339,7 +340,12 @@ int sod_rk4_main_record(SodMesh* mesh, SodState* state, const double* dt_dev, do
  * at the state (rho, q, E) with mu_e, mu_sgs and dt_dev frozen: out = (dy_{n+1}/dy_n)^T bar.
  * mu_sgs (nelem,64): the step's SGS viscosity when flag_les = 1 (rho mu_sgs in the stress and
  * Cp/0.9 rho mu_sgs in the heat flux, differentiated through rho), null otherwise.  stages
- * from sod_rk4_main_record, or null to recompute them; out may alias bar. */
+ * from sod_rk4_main_record, or null to recompute them; out may alias bar.  On a mesh with
+ * boundaries the map includes temporary_bc_routine_dirichlet_prim on every stage state and on
+ * the update; for the no-slip codes 3-5 the routine is affine (constants on rho, q and, for
+ * 4 and 5, E) and the outlet / ABL-top codes 2 and 8 leave the node alone, so its adjoint is a
+ * constant mask of the wall rows.  Codes 1 (far field), 6 and 7 (slip walls, which read the
+ * previous velocity) give SOD_ERR_UNSUPPORTED. */
 int sod_rk4_step_vjp(SodMesh* mesh, const double* rho, const double* q, const double* E,
                      const double* mu_e, const double* mu_sgs, const double* mu_factor,
                      const double* dt_dev, const double* stages, const double* bar_rho,

@@ -462,6 +462,27 @@ __global__ void __launch_bounds__(256) k_gather_vjp(int64_t N, const int32_t* __
   }
 }
 
+// acc += Ybar (the adjoint of a stage state after the boundary routine's adjoint); when wnext
+// is set: wnext = -dt (cb * ybar + ca * Ybar) / Ml
+__global__ void __launch_bounds__(256) k_accum_seed(int64_t N, const double* __restrict__ Yb, MCols5 acc,
+                                                    const double* __restrict__ ybar, const double* __restrict__ Ml,
+                                                    const double* __restrict__ dt, double cb, double ca,
+                                                    double* __restrict__ wnext) {
+  const int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= N) return;
+  double r[5];
+#pragma unroll
+  for (int f = 0; f < 5; ++f) {
+    r[f] = Yb[f * N + n];
+    acc.c[f][n] += r[f];
+  }
+  if (wnext) {
+    const double sc = -(*dt) / Ml[n];
+#pragma unroll
+    for (int f = 0; f < 5; ++f) wnext[f * N + n] = sc * (cb * ybar[f * N + n] + ca * r[f]);
+  }
+}
+
 // stage state: ys = y - coef * dt * gather(rel)/Ml   (time_integ.f90:301-318)
 __global__ void __launch_bounds__(256) k_stage_state(int64_t N, const int32_t* __restrict__ ptr,
                                                      const int32_t* __restrict__ idx, const double* __restrict__ el,
@@ -560,8 +581,11 @@ int sod_rk4_step_vjp(SodMesh* m, const double* rho, const double* q, const doubl
                      double* out_E, sod_stream_t stream) {
   SOD_ARG(m && rho && q && E && mu_e && mu_factor && dt_dev, "inputs null");
   SOD_ARG(bar_rho && bar_q && bar_E && out_rho && out_q && out_E, "adjoint arrays null");
-  if (m->bc.nb > 0) {
-    set_error("sod_rk4_step_vjp: the adjoint of the boundary routines is not built");
+  // boundaries: the routine's adjoint after every stage VJP and on the seed (walls and passive
+  // codes; far-field and slip codes are refused)
+  const bool bc = m->bc.nb > 0;
+  if (bc && m->bc.has_state_dependent) {
+    set_error("sod_rk4_step_vjp: the adjoint of the far-field and slip-wall boundary codes is not built");
     return SOD_ERR_UNSUPPORTED;
   }
   NvtxRange range("sod rk4 step vjp");
@@ -578,38 +602,64 @@ int sod_rk4_step_vjp(SodMesh* m, const double* rho, const double* q, const doubl
     musgs = m->musgs_int;
   }
   const int64_t N = m->npoin;
-  // scratch: ybar copy | w | (ys2 ys3 ys4 when the stages are not given)   (5 columns each)
-  rc = ensure_adj(m, (stages ? 10 : 25) * (size_t)N);
+  // scratch: ybar copy | w | (with boundaries: Y1 | Ybar of a stage) | (ys2 ys3 ys4 when the
+  // stages are not given)   (5 columns each)
+  const size_t base = bc ? 20 : 10;
+  rc = ensure_adj(m, (base + (stages ? 0 : 15)) * (size_t)N);
   if (rc) return rc;
   rc = mesh_ref_to_internal_elem(m, mu_e, m->mue_int, st);
   if (rc) return rc;
   double* yb = m->adj;
   double* w = m->adj + 5 * N;
+  double* y1s = bc ? m->adj + 10 * N : nullptr;   // first stage state B(y0)
+  double* Ybs = bc ? m->adj + 15 * N : nullptr;   // adjoint of one stage state
   const double* ys[3];
   const double* rel = reinterpret_cast<const double*>(m->buf.rel);
   Cols5 y0{{rho, q, q + N, q + 2 * N, E}};
+  Cols5 Y1 = y0;
+  if (bc) {
+    for (int f = 0; f < 5; ++f)
+      SOD_CUDA(cudaMemcpyAsync(y1s + f * N, y0.c[f], N * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    rc = bc_stage(m, y1s, 1, st);
+    if (rc) return rc;
+    Y1 = Cols5{{y1s, y1s + N, y1s + 2 * N, y1s + 3 * N, y1s + 4 * N}};
+  }
   if (stages) {
     for (int t = 0; t < 3; ++t) ys[t] = stages + (size_t)t * 5 * N;
   } else {
     // forward recompute of the stage states (mu_e and dt frozen)
     const int epb = m->tuned_epb[0] ? m->tuned_epb[0] : 2;
     const double acoef[3] = {0.5, 0.5, 1.0};
-    Cols5 cur = y0;
+    Cols5 cur = Y1;
     for (int t = 0; t < 3; ++t) {
-      double* b = m->adj + (size_t)(10 + 5 * t) * N;
+      double* b = m->adj + (base + 5 * t) * N;
       rc = launch_rhs(m, false, epb, cur.c[0], cur.c[1], cur.c[2], cur.c[3], cur.c[4], mu_factor, musgs, st);
       if (rc) return rc;
       k_stage_state<<<nblk(N), 256, 0, st>>>(N, m->n2e_ptr, m->n2e, rel, m->Ml, dt_dev, acoef[t], y0, b);
       SOD_CHECK_LAUNCH();
+      if (bc) {
+        rc = bc_stage(m, b, t + 2, st);
+        if (rc) return rc;
+      }
       ys[t] = b;
       cur = Cols5{{b, b + N, b + 2 * N, b + 3 * N, b + 4 * N}};
     }
   }
   // reverse sweep: kbar4 = -dt/6 ybar, Ybar4 = J4^T kbar4, kbar3 = -dt (ybar/3 + Ybar4), ...
+  // (with boundaries ybar is first mapped through the final routine's adjoint)
   Cols5 src{{bar_rho, bar_q, bar_q + N, bar_q + 2 * N, bar_E}};
   MCols5 keep{{yb, yb + N, yb + 2 * N, yb + 3 * N, yb + 4 * N}};
+  if (bc) {
+    for (int f = 0; f < 5; ++f)
+      SOD_CUDA(cudaMemcpyAsync(keep.c[f], src.c[f], N * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    rc = bc_adjoint(m, yb, st);
+    if (rc) return rc;
+    src = Cols5{{yb, yb + N, yb + 2 * N, yb + 3 * N, yb + 4 * N}};
+    keep = MCols5{{nullptr, nullptr, nullptr, nullptr, nullptr}};
+  }
   k_seed<<<nblk(N), 256, 0, st>>>(N, src, m->Ml, dt_dev, 1.0 / 6.0, w, keep);
   SOD_CHECK_LAUNCH();
+  keep = MCols5{{yb, yb + N, yb + 2 * N, yb + 3 * N, yb + 4 * N}};
   MCols5 acc{{out_rho, out_q, out_q + N, out_q + 2 * N, out_E}};
   // acc = ybar (copied from the kept columns, so out may alias bar)
   for (int f = 0; f < 5; ++f)
@@ -617,15 +667,27 @@ int sod_rk4_step_vjp(SodMesh* m, const double* rho, const double* q, const doubl
   const double cb[4] = {1.0 / 3.0, 1.0 / 3.0, 1.0 / 6.0, 0.0};
   const double ca[4] = {1.0, 0.5, 0.5, 0.0};
   for (int stage = 4; stage >= 1; --stage) {
-    const Cols5 ysrc = stage == 1 ? y0
+    const Cols5 ysrc = stage == 1 ? Y1
                                   : Cols5{{ys[stage - 2], ys[stage - 2] + N, ys[stage - 2] + 2 * N,
                                            ys[stage - 2] + 3 * N, ys[stage - 2] + 4 * N}};
     rc = launch_vjp(m, ysrc.c[0], ysrc.c[1], ysrc.c[2], ysrc.c[3], ysrc.c[4], mu_factor, musgs, w, st);
     if (rc) return rc;
     const int t = 4 - stage;
-    k_gather_vjp<<<nblk(N), 256, 0, st>>>(N, m->n2e_ptr, m->n2e, rel, acc, 1, yb, m->Ml, dt_dev, cb[t], ca[t],
-                                           stage > 1 ? w : nullptr);
-    SOD_CHECK_LAUNCH();
+    if (!bc) {
+      k_gather_vjp<<<nblk(N), 256, 0, st>>>(N, m->n2e_ptr, m->n2e, rel, acc, 1, yb, m->Ml, dt_dev, cb[t], ca[t],
+                                             stage > 1 ? w : nullptr);
+      SOD_CHECK_LAUNCH();
+    } else {
+      // Ybar of the post-routine stage state, through the stage routine's adjoint, then accumulated
+      MCols5 yc{{Ybs, Ybs + N, Ybs + 2 * N, Ybs + 3 * N, Ybs + 4 * N}};
+      k_gather_vjp<<<nblk(N), 256, 0, st>>>(N, m->n2e_ptr, m->n2e, rel, yc, 0, nullptr, nullptr, nullptr, 0.0, 0.0,
+                                             nullptr);
+      SOD_CHECK_LAUNCH();
+      rc = bc_adjoint(m, Ybs, st);
+      if (rc) return rc;
+      k_accum_seed<<<nblk(N), 256, 0, st>>>(N, Ybs, acc, yb, m->Ml, dt_dev, cb[t], ca[t], stage > 1 ? w : nullptr);
+      SOD_CHECK_LAUNCH();
+    }
   }
   return SOD_OK;
 }

@@ -70,38 +70,44 @@ struct ApplyArgs {
   SodBcParams p;
 };
 
-// mod_bc_routines.f90:55-178 (second and third loops) for one boundary node
-__global__ void __launch_bounds__(kBlock) k_bc_apply(const ApplyArgs a) {
-  const int b = blockIdx.x * blockDim.x + threadIdx.x;
-  if (b >= a.nb) return;
-  const size_t nb = (size_t)a.nb, N = a.N;
-  const size_t n = (size_t)a.node[b];
-  const int c = a.code[b];
-  const double gi = a.p.gamma_inf;
-  const double rho2 = a.aux2[b];
-  const double q2[3] = {a.aux2[nb + b], a.aux2[2 * nb + b], a.aux2[3 * nb + b]};
-  const double E2 = a.aux2[4 * nb + b];
-  const double u2[3] = {q2[0] / rho2, q2[1] / rho2, q2[2] / rho2};
-  const double p2 = rho2 * (gi - 1.0) * ((E2 / rho2) - 0.5 * ((u2[0] * u2[0]) + (u2[1] * u2[1]) + (u2[2] * u2[2])));
-  double r = a.rho[n], e = a.E[n];
-  double qq[3] = {a.q[n], a.q[n + N], a.q[n + 2 * N]};
-  double uu[3] = {0.0, 0.0, 0.0}, pp = 0.0;
-  bool set_u = false, set_p = false;
+// mod_bc_routines.f90:55-178 (second and third loops) for one boundary node of code c: own =
+// (rho, q x3, E) of the node, nb = the same of its lnbn node (copied by the first loop), uo the
+// velocity the slip branch reads.  Writes the node's new (rho, q x3, E) to out; uu / pp receive
+// the routine's aux_u / aux_p where it sets them (set_u / set_p).
+template <typename T> __device__ __forceinline__ T cst(double v);
+template <> __device__ __forceinline__ double cst<double>(double v) { return v; }
+
+template <typename T>
+__device__ __forceinline__ void bc_point(int c, const T (&own)[5], const T (&nb)[5], const double (&uo)[3],
+                                         const double (&nrm)[3], const double (&ub)[3], const SodBcParams& p,
+                                         T (&out)[5], T (&uu)[3], T& pp, bool& set_u, bool& set_p) {
+  const double gi = p.gamma_inf;
+  const T rho2 = nb[0];
+  const T q2[3] = {nb[1], nb[2], nb[3]};
+  const T E2 = nb[4];
+  const T u2[3] = {q2[0] / rho2, q2[1] / rho2, q2[2] / rho2};
+  const T p2 = rho2 * cst<T>(gi - 1.0) *
+               ((E2 / rho2) - cst<T>(0.5) * ((u2[0] * u2[0]) + (u2[1] * u2[1]) + (u2[2] * u2[2])));
+  T r = own[0], e = own[4];
+  T qq[3] = {own[1], own[2], own[3]};
+  uu[0] = uu[1] = uu[2] = cst<T>(0.0);
+  pp = cst<T>(0.0);
+  set_u = set_p = false;
   if (c == kFarField) {
-    const double E_inf = (a.p.rho_inf * 0.5 * (a.p.u_inf * a.p.u_inf) + a.p.p_inf / (gi - 1.0));
-    const double c2 = sqrt(gi * p2 / rho2);
-    double sl = fmin(a.p.u_inf - a.p.c_inf, u2[0] - c2);
-    double sr = fmax(u2[0] + c2, a.p.u_inf + a.p.c_inf);
-    const double rho_hll = (sr * rho2 - sl * a.p.rho_inf + a.p.rho_inf * a.p.u_inf - q2[0]) / (sr - sl);
-    const double E_hll =
-        (sr * E2 - sl * E_inf + a.p.u_inf * (E_inf + a.p.p_inf) - u2[0] * (E2 + p2)) / (sr - sl);
-    double qh[3];
+    const double E_inf = (p.rho_inf * 0.5 * (p.u_inf * p.u_inf) + p.p_inf / (gi - 1.0));
+    const T c2 = ::sqrt(cst<T>(gi) * p2 / rho2);
+    T sl = ::fmin(cst<T>(p.u_inf - p.c_inf), u2[0] - c2);
+    T sr = ::fmax(u2[0] + c2, cst<T>(p.u_inf + p.c_inf));
+    const T rho_hll = (sr * rho2 - sl * cst<T>(p.rho_inf) + cst<T>(p.rho_inf * p.u_inf) - q2[0]) / (sr - sl);
+    const T E_hll = (sr * E2 - sl * cst<T>(E_inf) + cst<T>(p.u_inf * (E_inf + p.p_inf)) - u2[0] * (E2 + p2)) /
+                    (sr - sl);
+    T qh[3];
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
-      const double ub = a.ubuf[d * nb + b];
-      sl = fmin(ub - a.p.c_inf, u2[d] - c2);
-      sr = fmax(u2[d] + c2, ub + a.p.c_inf);
-      qh[d] = (sr * q2[d] - sl * a.p.rho_inf * ub + a.p.rho_inf * (ub * ub) - u2[d] * q2[d]) / (sr - sl);
+      sl = ::fmin(cst<T>(ub[d] - p.c_inf), u2[d] - c2);
+      sr = ::fmax(u2[d] + c2, cst<T>(ub[d] + p.c_inf));
+      qh[d] = (sr * q2[d] - sl * cst<T>(p.rho_inf) * cst<T>(ub[d]) + cst<T>(p.rho_inf * (ub[d] * ub[d])) -
+               u2[d] * q2[d]) / (sr - sl);
     }
     r = rho_hll;
     e = E_hll;
@@ -109,38 +115,60 @@ __global__ void __launch_bounds__(kBlock) k_bc_apply(const ApplyArgs a) {
     for (int d = 0; d < 3; ++d) qq[d] = qh[d];
 #pragma unroll
     for (int d = 0; d < 3; ++d) uu[d] = qq[d] / r;
-    pp = r * (gi - 1.0) * ((e / r) - 0.5 * ((uu[0] * uu[0]) + (uu[1] * uu[1]) + (uu[2] * uu[2])));
+    pp = r * cst<T>(gi - 1.0) * ((e / r) - cst<T>(0.5) * ((uu[0] * uu[0]) + (uu[1] * uu[1]) + (uu[2] * uu[2])));
     set_u = set_p = true;
   } else if (c == kNonSlipAdiabatic) {
-    qq[0] = qq[1] = qq[2] = 0.0;
+    qq[0] = qq[1] = qq[2] = cst<T>(0.0);
     set_u = true;
-    r = a.p.rho_inf;
+    r = cst<T>(p.rho_inf);
   } else if (c == kNonSlipHot || c == kNonSlipCold) {
-    qq[0] = qq[1] = qq[2] = 0.0;
+    qq[0] = qq[1] = qq[2] = cst<T>(0.0);
     set_u = true;
-    r = a.p.p_inf / a.p.Rgas_inf / (c == kNonSlipHot ? a.p.T_H : a.p.T_C);
-    e = a.p.p_inf / (gi - 1.0);
+    r = cst<T>(p.p_inf / p.Rgas_inf / (c == kNonSlipHot ? p.T_H : p.T_C));
+    e = cst<T>(p.p_inf / (gi - 1.0));
   } else if (c == kSlipWallModel || c == kSlipAdiabatic) {
-    double uo[3] = {0.0, 0.0, 0.0};
-    if (a.uold_b) {
+    e = e - r * cst<T>(0.5) * cst<T>((uo[0] * uo[0]) + (uo[1] * uo[1]) + (uo[2] * uo[2]));
+    const T norm = (cst<T>(nrm[0]) * qq[0]) + (cst<T>(nrm[1]) * qq[1]) + (cst<T>(nrm[2]) * qq[2]);
 #pragma unroll
-      for (int d = 0; d < 3; ++d) uo[d] = a.uold_b[d * nb + b];
-    } else if (a.uold_n) {
-#pragma unroll
-      for (int d = 0; d < 3; ++d) uo[d] = a.uold_n[n + N * d];
-    }
-    e = e - r * 0.5 * ((uo[0] * uo[0]) + (uo[1] * uo[1]) + (uo[2] * uo[2]));
-    const double nx = a.normal[b], ny = a.normal[nb + b], nz = a.normal[2 * nb + b];
-    const double norm = (nx * qq[0]) + (ny * qq[1]) + (nz * qq[2]);
-    qq[0] = qq[0] - norm * nx;
-    qq[1] = qq[1] - norm * ny;
-    qq[2] = qq[2] - norm * nz;
-    r = a.p.rho_inf;
+    for (int d = 0; d < 3; ++d) qq[d] = qq[d] - norm * cst<T>(nrm[d]);
+    r = cst<T>(p.rho_inf);
 #pragma unroll
     for (int d = 0; d < 3; ++d) uu[d] = qq[d] / r;
-    e = e + r * 0.5 * ((uu[0] * uu[0]) + (uu[1] * uu[1]) + (uu[2] * uu[2]));
+    e = e + r * cst<T>(0.5) * ((uu[0] * uu[0]) + (uu[1] * uu[1]) + (uu[2] * uu[2]));
     set_u = true;
   }
+  out[0] = r;
+  out[1] = qq[0];
+  out[2] = qq[1];
+  out[3] = qq[2];
+  out[4] = e;
+}
+
+__global__ void __launch_bounds__(kBlock) k_bc_apply(const ApplyArgs a) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= a.nb) return;
+  const size_t nb = (size_t)a.nb, N = a.N;
+  const size_t n = (size_t)a.node[b];
+  const int c = a.code[b];
+  double own[5] = {a.rho[n], a.q[n], a.q[n + N], a.q[n + 2 * N], a.E[n]};
+  double nbv[5];
+#pragma unroll
+  for (int f = 0; f < 5; ++f) nbv[f] = a.aux2[f * nb + b];
+  double uo[3] = {0.0, 0.0, 0.0};
+  if (a.uold_b) {
+#pragma unroll
+    for (int d = 0; d < 3; ++d) uo[d] = a.uold_b[d * nb + b];
+  } else if (a.uold_n) {
+#pragma unroll
+    for (int d = 0; d < 3; ++d) uo[d] = a.uold_n[n + N * d];
+  }
+  const double nrm[3] = {a.normal[b], a.normal[nb + b], a.normal[2 * nb + b]};
+  const double ubv[3] = {a.ubuf[b], a.ubuf[nb + b], a.ubuf[2 * nb + b]};
+  double out[5], uu[3], pp;
+  bool set_u, set_p;
+  bc_point<double>(c, own, nbv, uo, nrm, ubv, a.p, out, uu, pp, set_u, set_p);
+  const double r = out[0], e = out[4];
+  const double qq[3] = {out[1], out[2], out[3]};
   a.rho[n] = r;
   a.E[n] = e;
 #pragma unroll
@@ -157,8 +185,8 @@ __global__ void __launch_bounds__(kBlock) k_bc_apply(const ApplyArgs a) {
     double umag = u0 * u0 + u1 * u1 + u2v * u2v;
     const double ei = (e / rho) - 0.5 * umag;
     const double pr = rho * (g - 1.0) * ei;
-    const double cs = sqrt(g * pr / rho);
-    umag = sqrt(umag);
+    const double cs = ::sqrt(g * pr / rho);
+    umag = ::sqrt(umag);
     const double T = pr / (rho * a.Rgas);
     a.u_n[n] = u0;
     a.u_n[n + N] = u1;
@@ -169,7 +197,7 @@ __global__ void __launch_bounds__(kBlock) k_bc_apply(const ApplyArgs a) {
     a.machno[n] = umag / cs;
     a.Tem[n] = T;
     a.eta[n] = (rho / (g - 1.0)) * log(pr / pow(rho, g));
-    a.mu_fluid[n] = a.mu_factor[n] * kSuthC1 * (T * sqrt(T)) / (T + kSuthS);
+    a.mu_fluid[n] = a.mu_factor[n] * kSuthC1 * (T * ::sqrt(T)) / (T + kSuthS);
   } else {
     if (a.u_n && set_u) {
 #pragma unroll
@@ -178,6 +206,22 @@ __global__ void __launch_bounds__(kBlock) k_bc_apply(const ApplyArgs a) {
     if (a.pr_n && set_p) a.pr_n[n] = pp;
   }
   if (a.Reta && no_slip(c)) a.Reta[n] = 0.0;
+}
+
+// Adjoint of the routine for the codes whose new state does not depend on the old one except
+// through the identity: no-slip adiabatic keeps E (rho and q are constants), the isothermal
+// walls set every field to a constant, outlet / ABL-top codes leave the node alone.  vbar is the
+// adjoint of the new state ([5][npoin] columns), mapped in place to that of the old state.
+__global__ void k_bc_adjoint_mask(int nb, const int32_t* __restrict__ node, const int32_t* __restrict__ code,
+                                  size_t N, double* __restrict__ vbar) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= nb) return;
+  const int c = code[b];
+  if (!no_slip(c)) return;
+  const size_t n = (size_t)node[b];
+#pragma unroll
+  for (int f = 0; f < 4; ++f) vbar[f * N + n] = 0.0;
+  if (c != kNonSlipAdiabatic) vbar[4 * N + n] = 0.0;
 }
 
 // bc_fix_dirichlet_residual (mod_bc_routines.f90:181-221) and _entropy (:265-291)
@@ -283,6 +327,19 @@ static int gather(SodMesh* m, const double* rho, const double* q, const double* 
 }
 
 }  // namespace bcd
+
+// adjoint of the routine in place on vbar ([5][npoin]); SOD_ERR_UNSUPPORTED when a boundary
+// node has a code whose new state depends on the old state (far-field, slip walls)
+int bc_adjoint(SodMesh* m, double* vbar, cudaStream_t st) {
+  if (m->bc.has_state_dependent) {
+    set_error("the adjoint of the far-field and slip-wall boundary codes is not built");
+    return SOD_ERR_UNSUPPORTED;
+  }
+  bcd::k_bc_adjoint_mask<<<bcd::grid_of(m->bc.nb), bcd::kBlock, 0, st>>>(m->bc.nb, m->bc.node, m->bc.code,
+                                                                         (size_t)m->npoin, vbar);
+  SOD_CHECK_LAUNCH();
+  return SOD_OK;
+}
 
 void bc_free(SodMesh* m) {
   BcState& b = m->bc;
@@ -392,6 +449,8 @@ int sod_mesh_set_boundaries(SodMesh* m, const int32_t* codes, const int32_t* lnb
   }
   B.nb = nb;
   B.prm = *bc;
+  for (int c : code)
+    if (c == bcd::kFarField || c == bcd::kSlipAdiabatic || c == bcd::kSlipWallModel) B.has_state_dependent = true;
   SOD_CUDA(cudaMemcpy(B.node, node.data(), sizeof(int32_t) * nb, cudaMemcpyHostToDevice));
   SOD_CUDA(cudaMemcpy(B.code, code.data(), sizeof(int32_t) * nb, cudaMemcpyHostToDevice));
   SOD_CUDA(cudaMemcpy(B.nbr, nbr.data(), sizeof(int32_t) * nb, cudaMemcpyHostToDevice));

@@ -164,6 +164,7 @@ struct BcState {
   double* aux2 = nullptr;      // [5][nb] state of the lnbn node (rho, q x3, E)
   double* u_stage = nullptr;   // [3][nb] aux_u of the previous stage's EOS
   double* u_final = nullptr;   // [3][nb] u(:,:,pos) at the start of the step
+  bool has_state_dependent = false;  // a far-field or slip code: no adjoint
   SodBcParams prm{};
 };
 
@@ -225,6 +226,7 @@ int take_nonfinite(SodMesh* m, cudaStream_t st, bool* flagged);
 int bc_snapshot_u(SodMesh* m, const double* u, cudaStream_t st);
 int bc_stage(SodMesh* m, double* ys, int stage, cudaStream_t st);
 int bc_final(SodMesh* m, SodState* s, double* Reta, cudaStream_t st);
+int bc_adjoint(SodMesh* m, double* vbar, cudaStream_t st);
 void bc_free(SodMesh* m);
 // packed-FP32 (FFMA2) variant of the mixed fused RHS kernel (sod_rhs_mixed.cu)
 int launch_rhs_mixed2(const RhsArgs& a, int epb, cudaStream_t st);

@@ -925,10 +925,6 @@ int sod_rk4_main_record(SodMesh* m, SodState* s, const double* dt_dev, double* d
   if (rc) return rc;
   SOD_ARG(dt_dev && stages, "dt_dev/stages null");
   SOD_ARG(prec == SOD_FP64 || prec == SOD_MIXED, "precision");
-  if (m->bc.nb > 0) {
-    set_error("sod_rk4_main_record: the adjoint of the boundary routines is not built");
-    return SOD_ERR_UNSUPPORTED;
-  }
   cudaStream_t st = (cudaStream_t)stream;
   const bool mixed = prec == SOD_MIXED;
   rc = ensure_step_buffers(m, mixed);

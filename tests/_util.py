@@ -14,18 +14,41 @@ def t2n(t):
     return np.asfortranarray(a.T) if a.ndim == 2 else a
 
 
-def oracle_step_jvp(oracle, om, prm, st, dt, v, mu_sgs=None):
+def oracle_bc_map(oracle, bnd):
+    """(rho, q, E) -> the same after temporary_bc_routine_dirichlet_prim (mod_bc_routines.f90),
+    on copies; the routine's aux_u / aux_p outputs are dropped."""
+    def B(rho, q, E):
+        r = np.array(rho, dtype=np.float64, copy=True)
+        qq = np.array(q, dtype=np.float64, order="F", copy=True)
+        e = np.array(E, dtype=np.float64, copy=True)
+        u = np.zeros((len(r), 3), order="F")
+        pr = np.zeros(len(r))
+        oracle.bc_dirichlet_prim(bnd, r, qq, u, pr, e)
+        return r, qq, e
+    return B
+
+
+def oracle_step_jvp(oracle, om, prm, st, dt, v, mu_sgs=None, bc=None):
     """One rk_4_main step (time_integ.f90:288-426) from the FlowState st and its JVP along
     v = (drho, dq (npoin,3), dE), composed from the oracle's dual-number stage JVPs with mu_e
-    (and mu_sgs) frozen."""
+    (and mu_sgs) frozen.  bc (oracle_bc_map) selects the non-periodic path: the routine on every
+    stage state (time_integ.f90:255-259) and on the update (:434-438); its tangent is B(y + v) - B(y), exact up to rounding for the affine routines of
+    the wall and passive codes."""
     def with_state(rho, q, E):
         s = st.copy()
         s.rho = np.ascontiguousarray(rho); s.q = np.asfortranarray(q); s.E = np.ascontiguousarray(E)
         return s
+
+    def bmap(y, w):
+        if bc is None:
+            return tuple(y), tuple(w)
+        by = bc(*y)
+        byw = bc(*(y[f] + w[f] for f in range(3)))
+        return by, tuple(byw[f] - by[f] for f in range(3))
     y0 = (st.rho, st.q, st.E)
     acc_y = [a.copy() for a in y0]
     acc_v = [a.copy() for a in v]
-    ys, vs = y0, v
+    ys, vs = bmap(y0, v)
     a_next = [0.5, 0.5, 1.0, None]
     b = [1 / 6, 1 / 3, 1 / 3, 1 / 6]
     for s in range(4):
@@ -36,6 +59,8 @@ def oracle_step_jvp(oracle, om, prm, st, dt, v, mu_sgs=None):
             acc_y[f] = acc_y[f] - dt * b[s] * Rc[f]
             acc_v[f] = acc_v[f] - dt * b[s] * dRc[f]
         if a_next[s] is not None:
-            ys = tuple(y0[f] - dt * a_next[s] * Rc[f] for f in range(3))
-            vs = tuple(v[f] - dt * a_next[s] * dRc[f] for f in range(3))
+            ys, vs = bmap(tuple(y0[f] - dt * a_next[s] * Rc[f] for f in range(3)),
+                          tuple(v[f] - dt * a_next[s] * dRc[f] for f in range(3)))
+    if bc is not None:
+        acc_y, acc_v = (list(t) for t in bmap(acc_y, acc_v))
     return acc_y, acc_v

@@ -137,6 +137,8 @@ def test_channel_dt_graph_mixed(torch_mod, oracle):
 
 
 def test_boundaries_removed_and_adjoint_rejected(torch_mod, oracle):
+    """A slip wall (code 6) makes the routine depend on the old velocity: the step adjoint is
+    refused, the recording step still runs; removing the boundaries gives the periodic step."""
     from sod2d_refmap_b200 import _lib, mesh as M, solver as S
     torch = torch_mod
     m, prm, st0, ub = channel((3, 6), seed=9, n=2)
@@ -147,8 +149,13 @@ def test_boundaries_removed_and_adjoint_rejected(torch_mod, oracle):
     dt = oracle.adapt_dt(om, st0, prm)
     s.dt.fill_(dt)
     stages = torch.zeros(15 * m.npoin, dtype=torch.float64, device="cuda")
+    y0 = (s.rho.clone(), s.q.clone(), s.E.clone(), s.mu_e.clone())
+    gm.rk_4_main_record(s, stages, update_dt=False)
     with pytest.raises(_lib.SodError, match="SOD_ERR_UNSUPPORTED"):
-        gm.rk_4_main_record(s, stages, update_dt=False)
+        gm.rk4_step_vjp(*y0, s.mu_factor, s.dt, s.rho, s.q, s.E, stages=stages)
+    fresh = S.Sod2dState.from_host(st0, gm.nelem)
+    for f in S.Sod2dState.FIELDS:
+        getattr(s, f).copy_(getattr(fresh, f))
     # without boundaries the step is the periodic-path step of the same mesh
     gm.set_boundaries(None, None, None)
     ref = st0.copy()
@@ -157,4 +164,96 @@ def test_boundaries_removed_and_adjoint_rejected(torch_mod, oracle):
     h = s.to_host()
     for k in ("rho", "q", "E", "mu_e"):
         assert rel_l2(h[k], getattr(ref, k)) < TOL64, k
+    gm.close()
+
+
+@pytest.mark.parametrize("codes", [(3, 4), (5, 3), (4, 2)])
+def test_channel_step_vjp_walls(torch_mod, oracle, codes):
+    """Step adjoint on wall channels (no-slip adiabatic / isothermal, outlet): the routine is
+    affine there, so its adjoint is a constant mask after every stage VJP and on the seed.
+    <w, J v> with J v from the oracle's dual-number stage JVPs through its own boundary routine
+    equals <J^T w, v>, bound 1e-11 relative to sum |w_i (J v)_i|, with recorded and with
+    recomputed stage states; the device step matches the oracle step (1e-12)."""
+    from _util import oracle_bc_map, oracle_step_jvp
+    from sod2d_refmap_b200 import mesh as M, solver as S
+    torch = torch_mod
+    m, prm, st0, ub = channel(codes, seed=21)
+    bc = M.bc_params(prm)
+    om = oracle.OracleMesh(m)
+    bnd = oracle.Boundaries(m.extra["bou_codes_nodes"], m.extra["lnbn_nodes"], m.extra["normals"], ub, bc)
+    dt = oracle.adapt_dt(om, st0, prm)
+    st = st0.copy()
+    oracle.rk4(om, prm, st, dt, nsteps=1, bnd=bnd)  # mu_e > 0, wall nodes at their wall values
+    rng = np.random.default_rng(17)
+    rnd = lambda a: rng.standard_normal(a.shape) * np.abs(a).mean()
+    v = (rnd(st.rho), np.asfortranarray(rnd(st.q)), rnd(st.E))
+    y1, dy1 = oracle_step_jvp(oracle, om, prm, st, dt, v, bc=oracle_bc_map(oracle, bnd))
+    gm = S.Sod2dMesh(m, prm)
+    gm.set_boundaries(m.extra["bou_codes_nodes"], m.extra["lnbn_nodes"], m.extra["normals"], ub, bc)
+    s = S.Sod2dState.from_host(st, gm.nelem)
+    s.dt.fill_(dt)
+    stages = torch.zeros(15 * m.npoin, dtype=torch.float64, device="cuda")
+    y0 = (s.rho.clone(), s.q.clone(), s.E.clone(), s.mu_e.clone())
+    gm.rk_4_main_record(s, stages, update_dt=False)
+    h = s.to_host()
+    for got, ref in ((h["rho"], y1[0]), (h["q"], y1[1]), (h["E"], y1[2])):
+        assert rel_l2(got, ref) < TOL64
+    wb = (rnd(st.rho), np.asfortranarray(rnd(st.q)), rnd(st.E))
+    bars = (dev(torch, wb[0]), dev(torch, wb[1]), dev(torch, wb[2]))
+    terms = [wb[f] * dy1[f] for f in range(3)]
+    lhs = sum(t.sum() for t in terms)
+    scale = sum(np.abs(t).sum() for t in terms)
+    outs = []
+    for stg in (stages, None):
+        out = gm.rk4_step_vjp(*y0, s.mu_factor, s.dt, *bars, stages=stg)
+        g = [host(o) for o in out]
+        rhs = sum((g[f] * v[f]).sum() for f in range(3))
+        assert abs(lhs - rhs) <= 1e-11 * scale, (stg is None, lhs, rhs)
+        outs.append(out)
+    for a, b in zip(*outs):
+        assert float((a - b).norm() / b.norm()) < 1e-13
+    # the seed's wall rows are masked: a cotangent only on the wall nodes' rho and q gives none
+    nodes = np.flatnonzero(np.isin(m.extra["bou_codes_nodes"], codes[:1]))
+    wr = np.zeros(m.npoin); wr[nodes] = 1.0
+    wq = np.zeros((m.npoin, 3), order="F"); wq[nodes, :] = 1.0
+    z = gm.rk4_step_vjp(*y0, s.mu_factor, s.dt, dev(torch, wr), dev(torch, wq), dev(torch, np.zeros(m.npoin)),
+                        stages=stages)
+    assert all(float(t.abs().max()) == 0.0 for t in z)
+    gm.close()
+
+
+def test_channel_rollout_gradient_fd(torch_mod, oracle):
+    """Loss 1/2 sum |q_K|^2 after K = 4 steps of a no-slip channel (codes 3 and 5), checkpoints
+    every 2, against central differences of the frozen-coefficient map (mu_e, dt frozen),
+    h = 1e-4 and 1e-6, bound 1e-6 relative."""
+    from sod2d_refmap_b200 import mesh as M, solver as S
+    from sod2d_refmap_b200.adjoint import Sod2dRollout, replay, trajectory_coefficients, _clone_state
+    torch = torch_mod
+    m, prm, st0, ub = channel((3, 5), seed=23)
+    om = oracle.OracleMesh(m)
+    dt = oracle.adapt_dt(om, st0, prm)
+    gm = S.Sod2dMesh(m, prm)
+    gm.set_boundaries(m.extra["bou_codes_nodes"], m.extra["lnbn_nodes"], m.extra["normals"], ub, M.bc_params(prm))
+    s = S.Sod2dState.from_host(st0, gm.nelem)
+    s.dt.fill_(dt)
+    gm.rk_4_main(s, precision=S.FP64, update_dt=True)
+    K = 4
+    rho = s.rho.clone().requires_grad_(True)
+    q = s.q.clone().requires_grad_(True)
+    E = s.E.clone().requires_grad_(True)
+    rK, qK, EK = Sod2dRollout.apply(gm, s, rho, q, E, K, 2)
+    (0.5 * (qK * qK).sum()).backward()
+    rng = np.random.default_rng(29)
+    v = [torch.from_numpy(rng.standard_normal(t.shape)).cuda() * t.abs().mean() for t in (s.rho, s.q, s.E)]
+    dL = float(sum((g * d).sum() for g, d in zip((rho.grad, q.grad, E.grad), v)).item())
+    mus, dts = trajectory_coefficients(gm, s, K)
+
+    def L_at(h):
+        t = _clone_state(s)
+        t.rho.add_(h * v[0]); t.q.add_(h * v[1]); t.E.add_(h * v[2])
+        replay(gm, t, mus, dts)
+        return 0.5 * float((t.q * t.q).sum().item())
+    for h in (1e-4, 1e-6):
+        fd = (L_at(h) - L_at(-h)) / (2 * h)
+        assert abs(fd - dL) <= 1e-6 * abs(dL), (h, fd, dL)
     gm.close()
