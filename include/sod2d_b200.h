@@ -130,6 +130,28 @@ typedef struct {
 int sod_mesh_set_boundaries(SodMesh* mesh, const int32_t* bou_codes_nodes, const int32_t* lnbn_nodes,
                             const double* normalsAtNodes, const double* u_buffer, const SodBcParams* bc);
 
+/* Penalisation buffer zone of rk_4_main (flag_buffer_on and flag_buffer_*,
+ * mod_numerical_params.f90:50-74): a zone is enabled by its on_* flag; east/west act on x,
+ * north/south on y, top/bottom on z; east, north and top cover coordinates above their minimum,
+ * west, south and bottom those below it.  The state is relaxed towards (nscbc_rho_inf,
+ * u_buffer rho, E_inf), E_inf = rho_inf u_inf^2 / 2 + p_inf / (gamma_inf - 1). */
+typedef struct {
+  int32_t on_east, on_west, on_north, on_south, on_top, on_bottom;
+  double e_min, e_size, w_min, w_size, n_min, n_size, s_min, s_size, t_min, t_size, b_min, b_size;
+  double rho_inf, u_inf, p_inf, gamma_inf;
+} SodBufferParams;
+
+/* flag_buffer_on = .true.: registers the zone (coord (npoin,3) and u_buffer (npoin,3) host
+ * arrays in Fortran order; u_buffer may be null: zeros).  Each step then applies updateBuffer
+ * (time_integ.f90:510-589) to every stage state (:251) and to the updated state (:429), before
+ * the boundary routine; sod_rk4_step_vjp differentiates through it.  The zone factor of each
+ * node is formed here once.  p = null removes the zone.  Captured step graphs of the mesh are
+ * dropped; ensemble meshes (sod_batch_*) reject it. */
+int sod_mesh_set_buffer(SodMesh* mesh, const SodBufferParams* p, const double* coord, const double* u_buffer);
+/* updateBuffer on device arrays rho (npoin), q (npoin,3), E (npoin) with the registered zone
+ * (no-op without one). */
+int sod_update_buffer(SodMesh* mesh, double* rho, double* q, double* E, sod_stream_t stream);
+
 /* Device-resident solver state in the reference's array layouts (level pos=2 only).
  * Every pointer is a device pointer owned by the caller. */
 typedef struct {

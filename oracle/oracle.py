@@ -46,6 +46,28 @@ class BcData(C.Structure):
         [(n, C.c_double) for n in ("rho_inf", "u_inf", "p_inf", "c_inf", "gamma_inf", "Rgas_inf", "T_H", "T_C")]
 
 
+class BufferData(C.Structure):
+    _fields_ = [("coord", _p), ("u_buffer", _p), ("on", C.c_int32 * 6), ("mn", C.c_double * 6),
+                ("sz", C.c_double * 6)] + [(n, C.c_double) for n in ("rho_inf", "u_inf", "p_inf", "gamma_inf")]
+
+
+BUFFER_SIDES = ("east", "west", "north", "south", "top", "bottom")
+
+
+class BufferZone:
+    """Buffer-zone data (flag_buffer_on) for the oracle: prm is the flat dict of
+    sod2d_refmap_b200.mesh.buffer_params (on_*, *_min, *_size per side, nscbc_* values)."""
+
+    def __init__(self, coord, u_buffer, prm: dict):
+        self.coord = np.asfortranarray(coord, dtype=np.float64)
+        self.u_buffer = np.asfortranarray(u_buffer, dtype=np.float64)
+        on = (C.c_int32 * 6)(*(int(prm["on_" + s]) for s in BUFFER_SIDES))
+        mn = (C.c_double * 6)(*(float(prm[s[0] + "_min"]) for s in BUFFER_SIDES))
+        sz = (C.c_double * 6)(*(float(prm[s[0] + "_size"]) for s in BUFFER_SIDES))
+        self.c = BufferData(ptr(self.coord).value, ptr(self.u_buffer).value, on, mn, sz,
+                            *(float(prm[k]) for k in ("rho_inf", "u_inf", "p_inf", "gamma_inf")))
+
+
 class Boundaries:
     """Boundary data of a non-periodic mesh for the oracle (arrays kept alive here)."""
 
@@ -80,7 +102,8 @@ def lib():
         L.oracle_conjgrad_pressure.restype = C.c_int
         L.oracle_rk_4_main.argtypes = [C.POINTER(ElemCtx), C.POINTER(Params), _p, _p, _p, _p, _p, _p,
                                        C.c_double, C.c_int, C.POINTER(State), C.POINTER(StageCapture),
-                                       C.POINTER(BcData)]
+                                       C.POINTER(BcData), C.POINTER(BufferData)]
+        L.oracle_update_buffer.argtypes = [C.c_int, C.POINTER(BufferData), _p, _p, _p]
         L.oracle_bc_dirichlet_prim.argtypes = [C.c_int, C.POINTER(BcData), _p, _p, _p, _p, _p]
         L.oracle_bc_fix_dirichlet_residual.argtypes = [C.c_int, C.POINTER(BcData), _p, _p, _p]
         L.oracle_bc_fix_dirichlet_residual_entropy.argtypes = [C.c_int, C.POINTER(BcData), _p]
@@ -173,9 +196,10 @@ def adapt_dt(om: OracleMesh, st, prm) -> float:
 
 
 def rk4(om: OracleMesh, prm, st, dt: float, nsteps: int = 1, capture_stage: int = 0,
-        bnd: "Boundaries | None" = None):
+        bnd: "Boundaries | None" = None, buf: "BufferZone | None" = None):
     """Runs nsteps rk_4_main steps in place on st (a FlowState).  Returns the stage residuals of
-    capture_stage (1..4) of the first step when requested.  bnd selects the non-periodic path."""
+    capture_stage (1..4) of the first step when requested.  bnd selects the non-periodic path,
+    buf the buffer zone (flag_buffer_on)."""
     P = params_of(prm)
     mue_l = np.zeros((om.nelem, 64), order="F")
     S = State(*(ptr(a).value for a in (st.rho, st.u, st.q, st.pr, st.E, st.Tem, st.e_int, st.eta, st.csound,
@@ -189,8 +213,14 @@ def rk4(om: OracleMesh, prm, st, dt: float, nsteps: int = 1, capture_stage: int 
                            ptr(out["Reta"]).value, int(capture_stage))
     lib().oracle_rk_4_main(C.byref(om.ctx), C.byref(P), ptr(om.Ml), ptr(st.mu_factor), ptr(om.gpvol), ptr(om.wgp),
                            ptr(om.helem), ptr(om.helem_l), float(dt), int(nsteps), C.byref(S),
-                           C.byref(cap) if cap is not None else None, C.byref(bnd.c) if bnd is not None else None)
+                           C.byref(cap) if cap is not None else None, C.byref(bnd.c) if bnd is not None else None,
+                           C.byref(buf.c) if buf is not None else None)
     return out
+
+
+def update_buffer(buf: BufferZone, rho, q, E):
+    """updateBuffer in place on FP64 arrays rho (npoin), q (npoin,3) Fortran order, E."""
+    lib().oracle_update_buffer(len(rho), C.byref(buf.c), ptr(rho), ptr(q), ptr(E))
 
 
 def bc_dirichlet_prim(bnd: Boundaries, rho, q, u, pr, E):

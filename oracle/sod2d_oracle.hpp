@@ -1344,6 +1344,45 @@ struct BcData {
   double rho_inf, u_inf, p_inf, c_inf, gamma_inf, Rgas_inf, T_H, T_C;  // nscbc_* values
 };
 
+// Penalisation buffer zone (flag_buffer_on, mod_numerical_params.f90:50-74): on[6] =
+// flag_buffer_on_east/west/north/south/top/bottom, mn/sz the zones' minimum and size in the same
+// order; rho_inf, u_inf, p_inf, gamma_inf the nscbc_* values.
+struct BufferData {
+  const double* coord;     // (npoin,3)
+  const double* u_buffer;  // (npoin,3)
+  int32_t on[6];
+  double mn[6], sz[6];
+  double rho_inf, u_inf, p_inf, gamma_inf;
+};
+
+// updateBuffer (time_integ.f90:510-589) over every node: xi = 1, lowered by each enabled zone
+// that holds the node, then q, E and rho relaxed towards their free-stream values
+inline void update_buffer(int npoin, const BufferData& B, double* rho, double* q, double* E) {
+  const int64_t N = npoin;
+  const double c1 = 0.01, c2 = 10.0;
+  const double E_inf = (B.rho_inf * 0.5 * (B.u_inf * B.u_inf) + B.p_inf / (B.gamma_inf - 1.0));
+  for (int64_t p = 0; p < N; ++p) {
+    double xi = 1.0;
+    for (int f = 0; f < 6; ++f) {
+      if (!B.on[f]) continue;
+      const double xs = B.coord[p + N * (f / 2)];
+      double xb;
+      if (f % 2 == 0) {  // east, north, top
+        if (!(xs > B.mn[f])) continue;
+        xb = (xs - B.mn[f]) / B.sz[f];
+      } else {           // west, south, bottom
+        if (!(xs < B.mn[f])) continue;
+        xb = (B.mn[f] - xs) / B.sz[f];
+      }
+      xi = std::min((1.0 - c1 * xb * xb) * (1.0 - (1.0 - std::exp(c2 * xb * xb)) / (1.0 - std::exp(c2))), xi);
+    }
+    for (int d = 0; d < 3; ++d)
+      q[p + N * d] = B.u_buffer[p + N * d] * rho[p] + xi * (q[p + N * d] - B.u_buffer[p + N * d] * rho[p]);
+    E[p] = E_inf + xi * (E[p] - E_inf);
+    rho[p] = B.rho_inf + xi * (rho[p] - B.rho_inf);
+  }
+}
+
 // temporary_bc_routine_dirichlet_prim (mod_bc_routines.f90:17-180): the first loop copies the
 // state of each boundary node's lnbn node, the second forms its velocity and pressure, the
 // third overwrites the boundary node by code.  u is read (slip walls) and written.
@@ -1442,7 +1481,8 @@ inline void bc_fix_dirichlet_residual_entropy(int npoin, const BcData& B, double
 // (time_integ.f90:256-259,299-301,434-437,474-477).
 inline void rk_4_main(const ElemCtx& ctx, const Params& P, const double* Ml, const double* mu_factor,
                       const double* gpvol, const double* wgp, const double* helem, const double* helem_l,
-                      double dt, State& S, Rk4Scratch& W, StageCapture* cap, const BcData* bc = nullptr) {
+                      double dt, State& S, Rk4Scratch& W, StageCapture* cap, const BcData* bc = nullptr,
+                      const BufferData* buf = nullptr) {
   const int npoin = ctx.npoin;
   const int64_t n3 = (int64_t)npoin * 3;
   const double a_i[4] = {0.0, 0.5, 0.5, 1.0};
@@ -1466,6 +1506,7 @@ inline void rk_4_main(const ElemCtx& ctx, const Params& P, const double* Ml, con
       for (int d = 0; d < 3; ++d)
         W.aux_q[p + (int64_t)npoin * d] = S.q[p + (int64_t)npoin * d] - dt * a_i[istep] * W.Rmom[p + (int64_t)npoin * d];
     }
+    if (buf) update_buffer(npoin, *buf, W.aux_rho.data(), W.aux_q.data(), W.aux_E.data());  // time_integ.f90:251
     if (bc)  // time_integ.f90:256-259
       temporary_bc_routine_dirichlet_prim(npoin, *bc, W.aux_rho.data(), W.aux_q.data(), W.aux_u.data(),
                                           W.aux_pr.data(), W.aux_E.data());
@@ -1528,6 +1569,7 @@ inline void rk_4_main(const ElemCtx& ctx, const Params& P, const double* Ml, con
     S.E[p] = S.E[p] - dt * W.Rener_sum[p];
     for (int d = 0; d < 3; ++d) S.q[p + (int64_t)npoin * d] = S.q[p + (int64_t)npoin * d] - dt * W.Rmom_sum[p + (int64_t)npoin * d];
   }
+  if (buf) update_buffer(npoin, *buf, S.rho, S.q, S.E);  // time_integ.f90:429
   if (bc) temporary_bc_routine_dirichlet_prim(npoin, *bc, S.rho, S.q, S.u, S.pr, S.E);  // time_integ.f90:434-437
   // EOS at the new level (time_integ.f90:445-463)
   for (int p = 0; p < npoin; ++p) {

@@ -38,6 +38,12 @@ class SodBcParams(C.Structure):
     _fields_ = [(n, _d) for n in ("rho_inf", "u_inf", "p_inf", "c_inf", "gamma_inf", "Rgas_inf", "T_H", "T_C")]
 
 
+class SodBufferParams(C.Structure):
+    _fields_ = [("on_" + s, C.c_int32) for s in ("east", "west", "north", "south", "top", "bottom")] + \
+        [(n, _d) for s in "ewnstb" for n in (s + "_min", s + "_size")] + \
+        [(n, _d) for n in ("rho_inf", "u_inf", "p_inf", "gamma_inf")]
+
+
 class SodMeshDesc(C.Structure):
     _fields_ = [("nelem", C.c_int32), ("npoin", C.c_int32), ("npoin_orig", C.c_int32), ("porder", C.c_int32),
                 ("index_base", C.c_int32), ("connec", _p), ("connec_orig", _p), ("coord_orig", _p),
@@ -80,6 +86,8 @@ _SIGS = {
     "sod_rk4_step_vjp": (_i, [_p] * 16),
     "sod_tgv_diagnostics": (_i, [_p, _p, _p, _p, _p, _d, _d, _p, _p]),
     "sod_mesh_set_boundaries": (_i, [_p] * 6),
+    "sod_mesh_set_buffer": (_i, [_p] * 4),
+    "sod_update_buffer": (_i, [_p] * 5),
     "sod_bc_dirichlet_prim": (_i, [_p] * 7),
     "sod_bc_fix_dirichlet_residual": (_i, [_p] * 5),
     "sod_bc_fix_dirichlet_residual_entropy": (_i, [_p] * 3),

@@ -581,10 +581,11 @@ int sod_rk4_step_vjp(SodMesh* m, const double* rho, const double* q, const doubl
                      double* out_E, sod_stream_t stream) {
   SOD_ARG(m && rho && q && E && mu_e && mu_factor && dt_dev, "inputs null");
   SOD_ARG(bar_rho && bar_q && bar_E && out_rho && out_q && out_E, "adjoint arrays null");
-  // boundaries: the routine's adjoint after every stage VJP and on the seed (walls and passive
-  // codes; far-field and slip codes are refused)
-  const bool bc = m->bc.nb > 0;
-  if (bc && m->bc.has_state_dependent) {
+  // boundaries and buffer zone: the routines' adjoints after every stage VJP and on the seed
+  // (walls and passive boundary codes; far-field and slip codes are refused)
+  const bool has_bc = m->bc.nb > 0, has_zone = m->zone.nb > 0;
+  const bool bc = has_bc || has_zone;
+  if (has_bc && m->bc.has_state_dependent) {
     set_error("sod_rk4_step_vjp: the adjoint of the far-field and slip-wall boundary codes is not built");
     return SOD_ERR_UNSUPPORTED;
   }
@@ -602,6 +603,17 @@ int sod_rk4_step_vjp(SodMesh* m, const double* rho, const double* q, const doubl
     musgs = m->musgs_int;
   }
   const int64_t N = m->npoin;
+  // Y = B(Z(y)) for the buffer zone Z and the boundary routine B; adjoint Z^T B^T
+  auto pre_stage = [&](double* ys, int stage_of) -> int {
+    if (has_zone)
+      if (int r = zone_stage(m, ys, st)) return r;
+    return has_bc ? bc_stage(m, ys, stage_of, st) : SOD_OK;
+  };
+  auto pre_adjoint = [&](double* vbar) -> int {
+    if (has_bc)
+      if (int r = bc_adjoint(m, vbar, st)) return r;
+    return has_zone ? zone_adjoint(m, vbar, st) : SOD_OK;
+  };
   // scratch: ybar copy | w | (with boundaries: Y1 | Ybar of a stage) | (ys2 ys3 ys4 when the
   // stages are not given)   (5 columns each)
   const size_t base = bc ? 20 : 10;
@@ -620,7 +632,7 @@ int sod_rk4_step_vjp(SodMesh* m, const double* rho, const double* q, const doubl
   if (bc) {
     for (int f = 0; f < 5; ++f)
       SOD_CUDA(cudaMemcpyAsync(y1s + f * N, y0.c[f], N * sizeof(double), cudaMemcpyDeviceToDevice, st));
-    rc = bc_stage(m, y1s, 1, st);
+    rc = pre_stage(y1s, 1);
     if (rc) return rc;
     Y1 = Cols5{{y1s, y1s + N, y1s + 2 * N, y1s + 3 * N, y1s + 4 * N}};
   }
@@ -638,7 +650,7 @@ int sod_rk4_step_vjp(SodMesh* m, const double* rho, const double* q, const doubl
       k_stage_state<<<nblk(N), 256, 0, st>>>(N, m->n2e_ptr, m->n2e, rel, m->Ml, dt_dev, acoef[t], y0, b);
       SOD_CHECK_LAUNCH();
       if (bc) {
-        rc = bc_stage(m, b, t + 2, st);
+        rc = pre_stage(b, t + 2);
         if (rc) return rc;
       }
       ys[t] = b;
@@ -652,7 +664,7 @@ int sod_rk4_step_vjp(SodMesh* m, const double* rho, const double* q, const doubl
   if (bc) {
     for (int f = 0; f < 5; ++f)
       SOD_CUDA(cudaMemcpyAsync(keep.c[f], src.c[f], N * sizeof(double), cudaMemcpyDeviceToDevice, st));
-    rc = bc_adjoint(m, yb, st);
+    rc = pre_adjoint(yb);
     if (rc) return rc;
     src = Cols5{{yb, yb + N, yb + 2 * N, yb + 3 * N, yb + 4 * N}};
     keep = MCols5{{nullptr, nullptr, nullptr, nullptr, nullptr}};
@@ -683,7 +695,7 @@ int sod_rk4_step_vjp(SodMesh* m, const double* rho, const double* q, const doubl
       k_gather_vjp<<<nblk(N), 256, 0, st>>>(N, m->n2e_ptr, m->n2e, rel, yc, 0, nullptr, nullptr, nullptr, 0.0, 0.0,
                                              nullptr);
       SOD_CHECK_LAUNCH();
-      rc = bc_adjoint(m, Ybs, st);
+      rc = pre_adjoint(Ybs);
       if (rc) return rc;
       k_accum_seed<<<nblk(N), 256, 0, st>>>(N, Ybs, acc, yb, m->Ml, dt_dev, cb[t], ca[t], stage > 1 ? w : nullptr);
       SOD_CHECK_LAUNCH();

@@ -178,26 +178,8 @@ __global__ void __launch_bounds__(kBlock) k_bc_apply(const ApplyArgs a) {
     for (int d = 0; d < 3; ++d) a.u_post_b[d * nb + b] = qq[d] / r;
   }
   if (a.eos) {
-    // EOS and Sutherland at the new level (time_integ.f90:445-463, mod_fluid_viscosity.f90:21-41)
-    const double g = a.gamma;
-    const double rho = r;
-    const double u0 = qq[0] / rho, u1 = qq[1] / rho, u2v = qq[2] / rho;
-    double umag = u0 * u0 + u1 * u1 + u2v * u2v;
-    const double ei = (e / rho) - 0.5 * umag;
-    const double pr = rho * (g - 1.0) * ei;
-    const double cs = ::sqrt(g * pr / rho);
-    umag = ::sqrt(umag);
-    const double T = pr / (rho * a.Rgas);
-    a.u_n[n] = u0;
-    a.u_n[n + N] = u1;
-    a.u_n[n + 2 * N] = u2v;
-    a.e_int[n] = ei;
-    a.pr_n[n] = pr;
-    a.csound[n] = cs;
-    a.machno[n] = umag / cs;
-    a.Tem[n] = T;
-    a.eta[n] = (rho / (g - 1.0)) * log(pr / pow(rho, g));
-    a.mu_fluid[n] = a.mu_factor[n] * kSuthC1 * (T * ::sqrt(T)) / (T + kSuthS);
+    eos_store(n, N, r, qq, e, a.gamma, a.Rgas, a.u_n, a.pr_n, a.e_int, a.csound, a.machno, a.Tem, a.eta, a.mu_fluid,
+              a.mu_factor);
   } else {
     if (a.u_n && set_u) {
 #pragma unroll
@@ -392,9 +374,13 @@ int bc_final(SodMesh* m, SodState* s, double* Reta, cudaStream_t st) {
   a.Reta = Reta;
   bcd::k_bc_apply<<<bcd::grid_of(m->bc.nb), bcd::kBlock, 0, st>>>(a);
   SOD_CHECK_LAUNCH();
+  return eta_stats(m, s->eta, st);
+}
+
+int eta_stats(SodMesh* m, const double* eta, cudaStream_t st) {
   const int nblk = bcd::grid_of(m->npoin);
   SOD_ARG(m->buf.red_cap >= 3 * (int64_t)nblk, "reduction scratch too small");
-  bcd::k_eta_partials<<<nblk, bcd::kBlock, 0, st>>>(m->npoin, s->eta, m->buf.red);
+  bcd::k_eta_partials<<<nblk, bcd::kBlock, 0, st>>>(m->npoin, eta, m->buf.red);
   SOD_CHECK_LAUNCH();
   bcd::k_eta_final<<<1, bcd::kBlock, 0, st>>>(nblk, m->npoin, m->prm.normalise, m->buf.red, m->buf.scal);
   SOD_CHECK_LAUNCH();

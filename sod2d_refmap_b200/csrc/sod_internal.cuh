@@ -168,6 +168,41 @@ struct BcState {
   SodBcParams prm{};
 };
 
+// Penalisation buffer zone (sod_buffer.cu): the nodes inside an enabled zone in ascending
+// order with their relaxation factor xi and u_buffer ([3][nb]).
+struct ZoneState {
+  int nb = 0;
+  int32_t* node = nullptr;
+  double* xi = nullptr;
+  double* ub = nullptr;
+  double rho_inf = 0.0, E_inf = 0.0;
+};
+
+// EOS and Sutherland viscosity of node n at the new level (time_integ.f90:445-463,
+// mod_fluid_viscosity.f90:21-41) from its conserved values
+__device__ __forceinline__ void eos_store(size_t n, size_t N, double rho, const double (&qq)[3], double e, double g,
+                                          double Rgas, double* u_n, double* pr_n, double* e_int, double* csound,
+                                          double* machno, double* Tem, double* eta, double* mu_fluid,
+                                          const double* mu_factor) {
+  const double u0 = qq[0] / rho, u1 = qq[1] / rho, u2 = qq[2] / rho;
+  double umag = u0 * u0 + u1 * u1 + u2 * u2;
+  const double ei = (e / rho) - 0.5 * umag;
+  const double pr = rho * (g - 1.0) * ei;
+  const double cs = ::sqrt(g * pr / rho);
+  umag = ::sqrt(umag);
+  const double T = pr / (rho * Rgas);
+  u_n[n] = u0;
+  u_n[n + N] = u1;
+  u_n[n + 2 * N] = u2;
+  e_int[n] = ei;
+  pr_n[n] = pr;
+  csound[n] = cs;
+  machno[n] = umag / cs;
+  Tem[n] = T;
+  eta[n] = (rho / (g - 1.0)) * log(pr / pow(rho, g));
+  mu_fluid[n] = mu_factor[n] * kSuthC1 * (T * ::sqrt(T)) / (T + kSuthS);
+}
+
 }  // namespace sod
 
 struct SodMesh {
@@ -208,6 +243,7 @@ struct SodMesh {
   size_t adj_len = 0;
   int index_base = 0;          // of the caller's node ids (SodMeshDesc.index_base)
   sod::BcState bc;             // boundaries (nb == 0: periodic path, noBoundaries)
+  sod::ZoneState zone;         // buffer zone (nb == 0: flag_buffer_on = .false.)
 };
 
 namespace sod {
@@ -228,6 +264,16 @@ int bc_stage(SodMesh* m, double* ys, int stage, cudaStream_t st);
 int bc_final(SodMesh* m, SodState* s, double* Reta, cudaStream_t st);
 int bc_adjoint(SodMesh* m, double* vbar, cudaStream_t st);
 void bc_free(SodMesh* m);
+// entropy normalisation (mean and spread of eta) recomputed into buf.scal after a routine that
+// changed eta
+int eta_stats(SodMesh* m, const double* eta, cudaStream_t st);
+// buffer zone (sod_buffer.cu), used by the step pipeline when m->zone.nb > 0: updateBuffer on a
+// stage state ([5][npoin]), on the updated state (with the EOS of the zone nodes), and its
+// adjoint in place on vbar ([5][npoin])
+int zone_stage(SodMesh* m, double* ys, cudaStream_t st);
+int zone_final(SodMesh* m, SodState* s, cudaStream_t st);
+int zone_adjoint(SodMesh* m, double* vbar, cudaStream_t st);
+void zone_free(SodMesh* m);
 // packed-FP32 (FFMA2) variant of the mixed fused RHS kernel (sod_rhs_mixed.cu)
 int launch_rhs_mixed2(const RhsArgs& a, int epb, cudaStream_t st);
 // LES (sod_les.cu): musgs_int <- sgs_visc of the velocity u (3 columns of npoin)

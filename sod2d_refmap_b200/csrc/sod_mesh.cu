@@ -325,6 +325,7 @@ int sod_mesh_set_params(SodMesh* m, const SodParams* p) {
 void sod_mesh_destroy(SodMesh* m) {
   if (!m) return;
   bc_free(m);
+  zone_free(m);
   for (auto& kv : m->graphs)
     if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
   void* ptrs[] = {m->econn, m->geo64, m->geo32, m->Ml, m->helem, m->helem_l, m->jratio, m->n2e_ptr, m->n2e,

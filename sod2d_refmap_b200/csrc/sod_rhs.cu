@@ -814,23 +814,31 @@ int run_step(SodMesh* m, SodState* s, const double* dt_dev, double* dt_next, boo
     loc.Reta = reta_tmp;
   }
   int rc;
-  // non-periodic path: boundary routine on every stage state and on the updated state
+  // non-periodic path / buffer zone: updateBuffer, then the boundary routine, on every stage
+  // state and on the updated state
   const bool bc = m->bc.nb > 0;
+  const bool zone = m->zone.nb > 0;
+  const bool pre = bc || zone;
+  auto pre_stage = [&](double* ys, int stage_of) -> int {
+    if (zone)
+      if (int r = zone_stage(m, ys, st)) return r;
+    return bc ? bc_stage(m, ys, stage_of, st) : SOD_OK;
+  };
   if (bc) {
     rc = bc_snapshot_u(m, s->u, st);  // u(:,:,pos) before the update, read by slip walls
     if (rc) return rc;
   }
   for (int stage = 1; stage <= 4; ++stage) {
     double* yin = (stage_store && stage >= 2) ? stage_store + (size_t)(stage - 2) * 5 * N : m->buf.ys;
-    if (bc && stage == 1) {
-      // the first stage state is the state itself with the boundary routine applied to a copy
+    if (pre && stage == 1) {
+      // the first stage state is the state itself with the routines applied to a copy
       SOD_CUDA(cudaMemcpyAsync(yin, s->rho, sizeof(double) * N, cudaMemcpyDeviceToDevice, st));
       SOD_CUDA(cudaMemcpyAsync(yin + N, s->q, sizeof(double) * 3 * N, cudaMemcpyDeviceToDevice, st));
       SOD_CUDA(cudaMemcpyAsync(yin + 4 * N, s->E, sizeof(double) * N, cudaMemcpyDeviceToDevice, st));
-      rc = bc_stage(m, yin, 1, st);
+      rc = pre_stage(yin, 1);
       if (rc) return rc;
     }
-    const bool from_state = stage == 1 && !bc;
+    const bool from_state = stage == 1 && !pre;
     const double* src_rho = from_state ? s->rho : yin;
     const double* src_q0 = from_state ? s->q : yin + N;
     const double* src_q1 = from_state ? s->q + N : yin + 2 * N;
@@ -857,12 +865,13 @@ int run_step(SodMesh* m, SodState* s, const double* dt_dev, double* dt_next, boo
       k_member_eta<<<m->nmember, 512, 0, st>>>(m->member_node_off, s->eta, m->member_scal, m->prm.normalise);
       SOD_CHECK_LAUNCH();
     }
-    if (bc) {
+    if (pre) {
       if (stage < 4) {
         double* ynext = (stage_store && stage < 4) ? stage_store + (size_t)(stage - 1) * 5 * N : m->buf.ys;
-        rc = bc_stage(m, ynext, stage + 1, st);
+        rc = pre_stage(ynext, stage + 1);
       } else {
-        rc = bc_final(m, s, loc.Reta, st);
+        rc = zone ? zone_final(m, s, st) : SOD_OK;
+        if (!rc && bc) rc = bc_final(m, s, loc.Reta, st);
       }
       if (rc) return rc;
     }

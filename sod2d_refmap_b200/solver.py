@@ -200,6 +200,28 @@ class Sod2dMesh:
                                              C.byref(p)))
         self._bnd = arrs
 
+    def set_buffer(self, prm: dict | None, coord=None, u_buffer=None):
+        """Registers the buffer zone of rk_4_main (flag_buffer_on = .true.): prm is the flat dict
+        of mesh.buffer_params, coord (npoin,3) and u_buffer (npoin,3) host arrays (u_buffer None:
+        zeros).  prm=None removes it."""
+        L = _lib.load()
+        if prm is None:
+            _lib.check(L.sod_mesh_set_buffer(self.handle, None, None, None))
+            return
+        sides = ("east", "west", "north", "south", "top", "bottom")
+        p = _lib.SodBufferParams(*(int(prm["on_" + s]) for s in sides),
+                                 *(float(prm[s + k]) for s in "ewnstb" for k in ("_min", "_size")),
+                                 *(float(prm[k]) for k in ("rho_inf", "u_inf", "p_inf", "gamma_inf")))
+        c = np.asfortranarray(coord, dtype=np.float64)
+        ub = None if u_buffer is None else np.asfortranarray(u_buffer, dtype=np.float64)
+        _lib.check(L.sod_mesh_set_buffer(self.handle, C.byref(p), _np_ptr(c), _np_ptr(ub) if ub is not None else None))
+
+    def update_buffer(self, rho, q, E, stream=None):
+        """updateBuffer in place on device tensors rho (npoin), q (3,npoin) storage = Fortran
+        (npoin,3), E (npoin)."""
+        _lib.check(_lib.load().sod_update_buffer(self.handle, *(C.c_void_p(_ptr(_contig(t))) for t in (rho, q, E)),
+                                                 _stream(stream)))
+
     def bc_dirichlet_prim(self, rho, q, u, pr, E, stream=None):
         """temporary_bc_routine_dirichlet_prim in place on device tensors ((npoin), q/u (3,npoin)
         storage = Fortran (npoin,3))."""
