@@ -152,6 +152,15 @@ int sod_mesh_set_buffer(SodMesh* mesh, const SodBufferParams* p, const double* c
  * (no-op without one). */
 int sod_update_buffer(SodMesh* mesh, double* rho, double* q, double* E, sod_stream_t stream);
 
+/* The optional source_term argument of rk_4_main (time_integ.f90:187,326-330): a device array
+ * (npoin,3) the mesh keeps a pointer to (caller-owned; its values may change between steps,
+ * the pointer may not be freed while registered).  Every stage then adds
+ * mom_source_const_vect (elem_source.f90:20-55), - sum over the node's elements of gpvol s =
+ * - Ml s, to the momentum residual, inside the ordered node gather in FP64 (both precisions),
+ * and so does sod_rhs.  null removes it.  A source term is constant in the state: the step
+ * adjoint only sees it through the stage states.  Ensemble meshes reject it. */
+int sod_mesh_set_source_term(SodMesh* mesh, const double* source_term);
+
 /* Device-resident solver state in the reference's array layouts (level pos=2 only).
  * Every pointer is a device pointer owned by the caller. */
 typedef struct {

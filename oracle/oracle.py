@@ -102,7 +102,7 @@ def lib():
         L.oracle_conjgrad_pressure.restype = C.c_int
         L.oracle_rk_4_main.argtypes = [C.POINTER(ElemCtx), C.POINTER(Params), _p, _p, _p, _p, _p, _p,
                                        C.c_double, C.c_int, C.POINTER(State), C.POINTER(StageCapture),
-                                       C.POINTER(BcData), C.POINTER(BufferData)]
+                                       C.POINTER(BcData), C.POINTER(BufferData), _p]
         L.oracle_update_buffer.argtypes = [C.c_int, C.POINTER(BufferData), _p, _p, _p]
         L.oracle_bc_dirichlet_prim.argtypes = [C.c_int, C.POINTER(BcData), _p, _p, _p, _p, _p]
         L.oracle_bc_fix_dirichlet_residual.argtypes = [C.c_int, C.POINTER(BcData), _p, _p, _p]
@@ -196,10 +196,11 @@ def adapt_dt(om: OracleMesh, st, prm) -> float:
 
 
 def rk4(om: OracleMesh, prm, st, dt: float, nsteps: int = 1, capture_stage: int = 0,
-        bnd: "Boundaries | None" = None, buf: "BufferZone | None" = None):
+        bnd: "Boundaries | None" = None, buf: "BufferZone | None" = None, source=None):
     """Runs nsteps rk_4_main steps in place on st (a FlowState).  Returns the stage residuals of
     capture_stage (1..4) of the first step when requested.  bnd selects the non-periodic path,
-    buf the buffer zone (flag_buffer_on)."""
+    buf the buffer zone (flag_buffer_on), source (npoin,3) the constant momentum source term."""
+    src = None if source is None else np.asfortranarray(source, dtype=np.float64)
     P = params_of(prm)
     mue_l = np.zeros((om.nelem, 64), order="F")
     S = State(*(ptr(a).value for a in (st.rho, st.u, st.q, st.pr, st.E, st.Tem, st.e_int, st.eta, st.csound,
@@ -214,7 +215,7 @@ def rk4(om: OracleMesh, prm, st, dt: float, nsteps: int = 1, capture_stage: int 
     lib().oracle_rk_4_main(C.byref(om.ctx), C.byref(P), ptr(om.Ml), ptr(st.mu_factor), ptr(om.gpvol), ptr(om.wgp),
                            ptr(om.helem), ptr(om.helem_l), float(dt), int(nsteps), C.byref(S),
                            C.byref(cap) if cap is not None else None, C.byref(bnd.c) if bnd is not None else None,
-                           C.byref(buf.c) if buf is not None else None)
+                           C.byref(buf.c) if buf is not None else None, ptr(src) if src is not None else None)
     return out
 
 

@@ -105,10 +105,11 @@ double oracle_adapt_dt_cfl(const ElemCtx* ctx, const double* helem, const double
 void oracle_rk_4_main(const ElemCtx* ctx, const Params* P, const double* Ml, const double* mu_factor,
                       const double* gpvol, const double* wgp, const double* helem, const double* helem_l,
                       double dt, int nsteps, State* S, StageCapture* capture, const BcData* bc,
-                      const BufferData* buf) {
+                      const BufferData* buf, const double* source) {
   Rk4Scratch W(ctx->npoin);
   for (int s = 0; s < nsteps; ++s)
-    rk_4_main(*ctx, *P, Ml, mu_factor, gpvol, wgp, helem, helem_l, dt, *S, W, s == 0 ? capture : nullptr, bc, buf);
+    rk_4_main(*ctx, *P, Ml, mu_factor, gpvol, wgp, helem, helem_l, dt, *S, W, s == 0 ? capture : nullptr, bc, buf,
+              source);
 }
 
 void oracle_update_buffer(int npoin, const BufferData* buf, double* rho, double* q, double* E) {

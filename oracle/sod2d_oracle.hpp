@@ -1344,6 +1344,19 @@ struct BcData {
   double rho_inf, u_inf, p_inf, c_inf, gamma_inf, Rgas_inf, T_H, T_C;  // nscbc_* values
 };
 
+// mom_source_const_vect (elem_source.f90:20-55): Rmom(node) -= gpvol(a, e) s(node) over every
+// element node, in element order (the reference's atomics)
+inline void mom_source_const_vect(const ElemCtx& ctx, const double* s, double* Rmom) {
+  const int nelem = ctx.nelem;
+  const int64_t npoin = ctx.npoin;
+  for (int ielem = 0; ielem < nelem; ++ielem)
+    for (int d = 0; d < 3; ++d)
+      for (int a = 0; a < nnode; ++a) {
+        const int64_t p = ctx.connec[ielem + (int64_t)nelem * a];
+        Rmom[p + npoin * d] = Rmom[p + npoin * d] - SOD_GPVOL(a, ielem) * s[p + npoin * d];
+      }
+}
+
 // Penalisation buffer zone (flag_buffer_on, mod_numerical_params.f90:50-74): on[6] =
 // flag_buffer_on_east/west/north/south/top/bottom, mn/sz the zones' minimum and size in the same
 // order; rho_inf, u_inf, p_inf, gamma_inf the nscbc_* values.
@@ -1482,7 +1495,7 @@ inline void bc_fix_dirichlet_residual_entropy(int npoin, const BcData& B, double
 inline void rk_4_main(const ElemCtx& ctx, const Params& P, const double* Ml, const double* mu_factor,
                       const double* gpvol, const double* wgp, const double* helem, const double* helem_l,
                       double dt, State& S, Rk4Scratch& W, StageCapture* cap, const BcData* bc = nullptr,
-                      const BufferData* buf = nullptr) {
+                      const BufferData* buf = nullptr, const double* source = nullptr) {
   const int npoin = ctx.npoin;
   const int64_t n3 = (int64_t)npoin * 3;
   const double a_i[4] = {0.0, 0.5, 0.5, 1.0};
@@ -1532,6 +1545,7 @@ inline void rk_4_main(const ElemCtx& ctx, const Params& P, const double* Ml, con
     full_diffusion_ijk(ctx, P, W.aux_rho.data(), W.aux_rho.data(), W.aux_u.data(), W.aux_Tem.data(),
                        S.mu_fluid, S.mu_e, S.mu_sgs, W.Rdiff_mass.data(), W.Rdiff_mom.data(),
                        W.Rdiff_ener.data());
+    if (source) mom_source_const_vect(ctx, source, W.Rdiff_mom.data());  // time_integ.f90:326-330
     if (P.flag_total_enthalpy)  // time_integ.f90:361-365
       full_convec_ijk_H(ctx, W.aux_u.data(), W.aux_q.data(), W.aux_rho.data(), W.aux_pr.data(), W.aux_E.data(),
                         W.Rmass.data(), W.Rmom.data(), W.Rener.data());

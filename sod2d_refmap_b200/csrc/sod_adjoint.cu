@@ -487,7 +487,8 @@ __global__ void __launch_bounds__(256) k_accum_seed(int64_t N, const double* __r
 __global__ void __launch_bounds__(256) k_stage_state(int64_t N, const int32_t* __restrict__ ptr,
                                                      const int32_t* __restrict__ idx, const double* __restrict__ el,
                                                      const double* __restrict__ Ml, const double* __restrict__ dt,
-                                                     double coef, Cols5 y, double* __restrict__ ys) {
+                                                     double coef, Cols5 y, const double* __restrict__ src,
+                                                     double* __restrict__ ys) {
   const int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (n >= N) return;
   double r[5] = {0, 0, 0, 0, 0};
@@ -500,6 +501,10 @@ __global__ void __launch_bounds__(256) k_stage_state(int64_t N, const int32_t* _
   }
   // same operation order as the forward stage gather, so the stage states match it bit for bit
   const double ml = Ml[n];
+  if (src) {
+#pragma unroll
+    for (int d = 0; d < 3; ++d) r[1 + d] -= ml * src[d * N + n];
+  }
   const double da = (*dt) * coef;
 #pragma unroll
   for (int f = 0; f < 5; ++f) ys[f * N + n] = y.c[f][n] - da * (r[f] / ml);
@@ -647,7 +652,7 @@ int sod_rk4_step_vjp(SodMesh* m, const double* rho, const double* q, const doubl
       double* b = m->adj + (base + 5 * t) * N;
       rc = launch_rhs(m, false, epb, cur.c[0], cur.c[1], cur.c[2], cur.c[3], cur.c[4], mu_factor, musgs, st);
       if (rc) return rc;
-      k_stage_state<<<nblk(N), 256, 0, st>>>(N, m->n2e_ptr, m->n2e, rel, m->Ml, dt_dev, acoef[t], y0, b);
+      k_stage_state<<<nblk(N), 256, 0, st>>>(N, m->n2e_ptr, m->n2e, rel, m->Ml, dt_dev, acoef[t], y0, m->source, b);
       SOD_CHECK_LAUNCH();
       if (bc) {
         rc = pre_stage(b, t + 2);

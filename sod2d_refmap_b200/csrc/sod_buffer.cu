@@ -11,6 +11,9 @@
 // final pass recomputes it otherwise).  The update is affine in the state with a constant
 // Jacobian (rho' = xi rho + c, q' = xi q + (1 - xi) u_b rho + ..., E' = xi E + c), so its
 // adjoint is a fixed per-node map.
+//
+// The other optional per-node input of rk_4_main, the constant momentum source term, is
+// registered here too (sod_mesh_set_source_term); the node gather applies it.
 #include "sod_internal.cuh"
 #include <cmath>
 #include <vector>
@@ -180,6 +183,18 @@ int sod_mesh_set_buffer(SodMesh* m, const SodBufferParams* p, const double* coor
   SOD_CUDA(cudaMemcpy(z.node, node.data(), sizeof(int32_t) * nb, cudaMemcpyHostToDevice));
   SOD_CUDA(cudaMemcpy(z.xi, xi.data(), sizeof(double) * nb, cudaMemcpyHostToDevice));
   SOD_CUDA(cudaMemcpy(z.ub, ub.data(), sizeof(double) * 3 * nb, cudaMemcpyHostToDevice));
+  return SOD_OK;
+}
+
+int sod_mesh_set_source_term(SodMesh* m, const double* source_term) {
+  SOD_ARG(m, "mesh null");
+  SOD_ARG(m->nmember == 0 || !source_term, "a source term on an ensemble mesh is not supported");
+  if (m->source != source_term) {
+    for (auto& kv : m->graphs)
+      if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+    m->graphs.clear();
+  }
+  m->source = source_term;
   return SOD_OK;
 }
 

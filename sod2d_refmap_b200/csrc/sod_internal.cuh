@@ -244,6 +244,7 @@ struct SodMesh {
   int index_base = 0;          // of the caller's node ids (SodMeshDesc.index_base)
   sod::BcState bc;             // boundaries (nb == 0: periodic path, noBoundaries)
   sod::ZoneState zone;         // buffer zone (nb == 0: flag_buffer_on = .false.)
+  const double* source = nullptr;  // caller's constant momentum source term (npoin,3), or null
 };
 
 namespace sod {

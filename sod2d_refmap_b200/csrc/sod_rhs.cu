@@ -346,6 +346,7 @@ struct GatherArgs {
   unsigned int* nonfinite;  // raised by stage 4 on a NaN/Inf in the new rho, q, E
   double* scal;             // [0] eta mean, [1] eta norm
   int normalise;
+  const double* src;        // momentum source term (npoin,3) or null
 };
 
 __device__ __forceinline__ void block_reduce3(double& s, double& mx, double& mn, double* sh) {
@@ -405,6 +406,11 @@ __global__ void __launch_bounds__(256, SOD_KG_MIN_BLOCKS) k_gather_rk(const Gath
       load_res6<R>(rel, (size_t)a.idx[c], v);
 #pragma unroll
       for (int f = 0; f < 6; ++f) r[f] += (double)v[f];
+    }
+    if (a.src) {
+      // mom_source_const_vect (elem_source.f90:20-55): - sum_e gpvol s = - Ml s on the momentum
+#pragma unroll
+      for (int d = 0; d < 3; ++d) r[1 + d] -= ml * a.src[d * N + n];
     }
 #pragma unroll
     for (int f = 0; f < 6; ++f) r[f] = r[f] / ml;
@@ -710,6 +716,7 @@ int launch_gather(SodMesh* m, bool mixed, int stage, GatherArgs& a, cudaStream_t
   a.counter = m->buf.counters + 0;
   a.nonfinite = m->buf.counters + kNonfiniteCounter;
   a.scal = m->buf.scal;
+  a.src = m->nmember > 0 ? nullptr : m->source;
   if (stage >= 1) {
     a.b_cur = kB[stage - 1];
     a.a_next = stage < 4 ? kA[stage] : 0.0;

@@ -216,6 +216,18 @@ class Sod2dMesh:
         ub = None if u_buffer is None else np.asfortranarray(u_buffer, dtype=np.float64)
         _lib.check(L.sod_mesh_set_buffer(self.handle, C.byref(p), _np_ptr(c), _np_ptr(ub) if ub is not None else None))
 
+    def set_source_term(self, source):
+        """The source_term of rk_4_main (mom_source_const_vect): a device tensor (3, npoin) =
+        Fortran (npoin,3) that the mesh keeps (and this object references) until replaced;
+        None removes it."""
+        if source is None:
+            _lib.check(_lib.load().sod_mesh_set_source_term(self.handle, None))
+            self._source = None
+            return
+        src = _contig(source)
+        _lib.check(_lib.load().sod_mesh_set_source_term(self.handle, C.c_void_p(_ptr(src))))
+        self._source = src
+
     def update_buffer(self, rho, q, E, stream=None):
         """updateBuffer in place on device tensors rho (npoin), q (3,npoin) storage = Fortran
         (npoin,3), E (npoin)."""
