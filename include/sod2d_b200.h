@@ -207,6 +207,9 @@ int sod_step_profile(SodMesh* mesh, SodState* state, double* dt_dev, int nsteps,
  * {1,2,4,8} mixed) on the given state and keeps the fastest for this mesh and precision. */
 int sod_autotune(SodMesh* mesh, SodState* state, SodPrecision prec, int* best_epb, float* best_ms,
                  sod_stream_t stream);
+/* Pins the fused-RHS elements per CTA of a precision (one of the autotuner's candidates; 0: the
+ * default).  Captured step graphs are dropped when it changes. */
+int sod_set_rhs_config(SodMesh* mesh, SodPrecision prec, int config);
 
 /* Host-buffer variant of sod_rk4_main for the CPU-side drop-in (the reference's CPU build
  * calls rk_4_main on host arrays): copies rho,q,E,mu_e,mu_factor in, runs one step and copies

@@ -87,6 +87,7 @@ _SIGS = {
     "sod_tgv_diagnostics": (_i, [_p, _p, _p, _p, _p, _d, _d, _p, _p]),
     "sod_mesh_set_boundaries": (_i, [_p] * 6),
     "sod_mesh_set_buffer": (_i, [_p] * 4),
+    "sod_set_rhs_config": (_i, [_p, _i, _i]),
     "sod_mesh_set_source_term": (_i, [_p] * 2),
     "sod_update_buffer": (_i, [_p] * 5),
     "sod_bc_dirichlet_prim": (_i, [_p] * 7),

@@ -1062,6 +1062,21 @@ int sod_step_profile(SodMesh* m, SodState* s, double* dt_dev, int nsteps, SodPre
 // Elements-per-CTA autotuner for the fused RHS kernel: times every candidate on the caller's
 // state (3 warm-up + 10 timed launches each, CUDA events on the stream) and keeps the fastest
 // for this mesh and precision; later steps and newly captured graphs use it.
+int sod_set_rhs_config(SodMesh* m, SodPrecision prec, int config) {
+  SOD_ARG(m, "mesh null");
+  SOD_ARG(prec == SOD_FP64 || prec == SOD_MIXED, "precision");
+  const bool mixed = prec == SOD_MIXED;
+  const bool ok = (config == 1 || config == 2 || config == 4 || (mixed && config == 8));
+  SOD_ARG(ok || config == 0, "unknown fused-RHS configuration");
+  if (m->tuned_epb[mixed ? 1 : 0] != config) {
+    for (auto& kv : m->graphs)
+      if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+    m->graphs.clear();
+  }
+  m->tuned_epb[mixed ? 1 : 0] = config;
+  return SOD_OK;
+}
+
 int sod_autotune(SodMesh* m, SodState* s, SodPrecision prec, int* best_epb, float* best_ms, sod_stream_t stream) {
   int rc = check_state(m, s);
   if (rc) return rc;

@@ -284,6 +284,10 @@ class Sod2dMesh:
                                            _stream(stream)))
         return best.value, ms.value
 
+    def set_rhs_config(self, precision: int, config: int):
+        """Pins the fused-RHS configuration of a precision (sod_set_rhs_config)."""
+        _lib.check(_lib.load().sod_set_rhs_config(self.handle, int(precision), int(config)))
+
     def rhs(self, state: Sod2dState, precision: int = FP64, stream=None):
         torch = _torch()
         N = self.npoin
