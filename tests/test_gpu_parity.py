@@ -90,6 +90,25 @@ def test_graph_steps_bitwise_match_eager(env):
         assert env["torch"].equal(getattr(a, k), getattr(b, k)), k
 
 
+def test_rhs_configs_bitwise_equal(env):
+    """Every elements-per-CTA configuration of the fused RHS computes each element with the same
+    operations: outputs bit for bit equal; unknown configurations are refused."""
+    from sod2d_refmap_b200 import _lib
+    S, gm, st1, torch = env["S"], env["gm"], env["st1"], env["torch"]
+    for prec, cfgs in ((S.FP64, (1, 2, 4)), (S.MIXED, (1, 2, 4, 8))):
+        outs = []
+        for c in cfgs:
+            gm.set_rhs_config(prec, c)
+            s = S.Sod2dState.from_host(st1, gm.nelem)
+            outs.append({k: v.clone() for k, v in gm.rhs(s, precision=prec).items()})
+        for o in outs[1:]:
+            for k in o:
+                assert torch.equal(o[k], outs[0][k]), (prec, k)
+        with pytest.raises(_lib.SodError, match="SOD_ERR_ARG"):
+            gm.set_rhs_config(prec, 3)
+        gm.set_rhs_config(prec, 0)
+
+
 def test_deterministic(env):
     S, gm, st1 = env["S"], env["gm"], env["st1"]
     outs = []
