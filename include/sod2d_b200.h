@@ -211,6 +211,14 @@ int sod_autotune(SodMesh* mesh, SodState* state, SodPrecision prec, int* best_ep
  * default).  Captured step graphs are dropped when it changes. */
 int sod_set_rhs_config(SodMesh* mesh, SodPrecision prec, int config);
 
+/* compute_fieldDerivs (mod_postpro.f90:12-139) on device arrays rho (npoin) and u (npoin,3):
+ * gradRho (npoin,3), curlU (npoin,3) = sum_jk leviCivi(i,j,k) du_j/dx_k, divU (npoin) =
+ * (div(rho u) + rho div u) / 2 and Qcrit (npoin) = -1/2 du_i/dx_j du_j/dx_i, each averaged over
+ * the elements holding the node (lelpn).  leviCivi: host (3,3,3) Fortran array, or null for the
+ * symbol CFDSolverBase sets (CFDSolverBase.f90:1248-1253). */
+int sod_compute_field_derivs(SodMesh* mesh, const double* rho, const double* u, const double* leviCivi,
+                             double* gradRho, double* curlU, double* divU, double* Qcrit, sod_stream_t stream);
+
 /* Host-buffer variant of sod_rk4_main for the CPU-side drop-in (the reference's CPU build
  * calls rk_4_main on host arrays): copies rho,q,E,mu_e,mu_factor in, runs one step and copies
  * rho,q,E,u,pr,Tem,e_int,eta,csound,machno,mu_fluid,mu_e back.  dt_host in, dt_next_host out. */

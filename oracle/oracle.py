@@ -103,6 +103,7 @@ def lib():
         L.oracle_rk_4_main.argtypes = [C.POINTER(ElemCtx), C.POINTER(Params), _p, _p, _p, _p, _p, _p,
                                        C.c_double, C.c_int, C.POINTER(State), C.POINTER(StageCapture),
                                        C.POINTER(BcData), C.POINTER(BufferData), _p]
+        L.oracle_compute_field_derivs.argtypes = [C.POINTER(ElemCtx), _p, _p, _p, _p, _p, _p, _p]
         L.oracle_update_buffer.argtypes = [C.c_int, C.POINTER(BufferData), _p, _p, _p]
         L.oracle_bc_dirichlet_prim.argtypes = [C.c_int, C.POINTER(BcData), _p, _p, _p, _p, _p]
         L.oracle_bc_fix_dirichlet_residual.argtypes = [C.c_int, C.POINTER(BcData), _p, _p, _p]
@@ -217,6 +218,24 @@ def rk4(om: OracleMesh, prm, st, dt: float, nsteps: int = 1, capture_stage: int 
                            C.byref(cap) if cap is not None else None, C.byref(bnd.c) if bnd is not None else None,
                            C.byref(buf.c) if buf is not None else None, ptr(src) if src is not None else None)
     return out
+
+
+def levi_civita() -> np.ndarray:
+    """The (3,3,3) symbol CFDSolverBase sets (CFDSolverBase.f90:1248-1253)."""
+    e = np.zeros((3, 3, 3), order="F")
+    e[1, 2, 0] = 1.0; e[2, 1, 0] = -1.0; e[0, 2, 1] = -1.0; e[2, 0, 1] = 1.0; e[0, 1, 2] = 1.0; e[1, 0, 2] = -1.0
+    return e
+
+
+def compute_field_derivs(om: OracleMesh, rho, u, levi=None):
+    """compute_fieldDerivs: (gradRho (npoin,3), curlU (npoin,3), divU, Qcrit)."""
+    N = om.npoin
+    lv = np.asfortranarray(levi_civita() if levi is None else levi, dtype=np.float64)
+    r = np.ascontiguousarray(rho, dtype=np.float64)
+    uu = np.asfortranarray(u, dtype=np.float64)
+    g = np.zeros((N, 3), order="F"); c = np.zeros((N, 3), order="F"); dv = np.zeros(N); qc = np.zeros(N)
+    lib().oracle_compute_field_derivs(C.byref(om.ctx), ptr(lv), ptr(r), ptr(uu), ptr(g), ptr(c), ptr(dv), ptr(qc))
+    return g, c, dv, qc
 
 
 def update_buffer(buf: BufferZone, rho, q, E):

@@ -112,6 +112,11 @@ void oracle_rk_4_main(const ElemCtx* ctx, const Params* P, const double* Ml, con
               source);
 }
 
+void oracle_compute_field_derivs(const ElemCtx* ctx, const double* levi, const double* rho, const double* u,
+                                 double* gradRho, double* curlU, double* divU, double* Qcrit) {
+  compute_field_derivs(*ctx, levi, rho, u, gradRho, curlU, divU, Qcrit);
+}
+
 void oracle_update_buffer(int npoin, const BufferData* buf, double* rho, double* q, double* E) {
   update_buffer(npoin, *buf, rho, q, E);
 }

@@ -1327,6 +1327,77 @@ inline void sgs_visc(const ElemCtx& ctx, const Params& P, const double* u, doubl
   }
 }
 
+// compute_fieldDerivs (mod_postpro.f90:12-139): per element and gauss point the iso gradients
+// of rho, u and rho u, their physical forms with He, the element's contributions to gradRho,
+// divU = (div(rho u) + rho div u)/2, curlU = leviCivi(i,j,k) du_j/dx_k and
+// Qcrit = -1/2 du_i/dx_j du_j/dx_i added to the node (the reference's atomics, here in element
+// order), then each node divided by lelpn, the number of elements holding it.  levi (3,3,3)
+// Fortran order.
+inline void compute_field_derivs(const ElemCtx& ctx, const double* levi, const double* rho, const double* u,
+                                 double* gradRho, double* curlU, double* divU, double* Qcrit) {
+  const int nelem = ctx.nelem, npoin = ctx.npoin;
+  const int64_t N = npoin;
+  std::fill(divU, divU + N, 0.0);
+  std::fill(gradRho, gradRho + 3 * N, 0.0);
+  std::fill(curlU, curlU + 3 * N, 0.0);
+  std::fill(Qcrit, Qcrit + N, 0.0);
+  std::vector<int> lelpn(npoin, 0);
+  for (int ielem = 0; ielem < nelem; ++ielem) {
+    double rho_e[nnode], u_e[nnode][3], ru_e[nnode][3];
+    for (int a = 0; a < nnode; ++a) {
+      const int64_t p = ctx.connec[ielem + (int64_t)nelem * a];
+      rho_e[a] = rho[p];
+      for (int d = 0; d < 3; ++d) {
+        u_e[a][d] = u[p + N * d];
+        ru_e[a][d] = rho[p] * u[p + N * d];
+      }
+    }
+    for (int igaus = 0; igaus < ngaus; ++igaus) {
+      const int isoI = ctx.gmshAtoI[igaus], isoJ = ctx.gmshAtoJ[igaus], isoK = ctx.gmshAtoK[igaus];
+      double gIR[3] = {}, gIU[3][3] = {}, gIRU[3][3] = {};
+      for (int ii = 0; ii < 4; ++ii) {
+        gIR[0] += SOD_DL(igaus, 0, ii) * rho_e[SOD_INV(ii, isoJ, isoK)];
+        gIR[1] += SOD_DL(igaus, 1, ii) * rho_e[SOD_INV(isoI, ii, isoK)];
+        gIR[2] += SOD_DL(igaus, 2, ii) * rho_e[SOD_INV(isoI, isoJ, ii)];
+        for (int id = 0; id < 3; ++id) {
+          gIU[id][0] += SOD_DL(igaus, 0, ii) * u_e[SOD_INV(ii, isoJ, isoK)][id];
+          gIU[id][1] += SOD_DL(igaus, 1, ii) * u_e[SOD_INV(isoI, ii, isoK)][id];
+          gIU[id][2] += SOD_DL(igaus, 2, ii) * u_e[SOD_INV(isoI, isoJ, ii)][id];
+          gIRU[id][0] += SOD_DL(igaus, 0, ii) * ru_e[SOD_INV(ii, isoJ, isoK)][id];
+          gIRU[id][1] += SOD_DL(igaus, 1, ii) * ru_e[SOD_INV(isoI, ii, isoK)][id];
+          gIRU[id][2] += SOD_DL(igaus, 2, ii) * ru_e[SOD_INV(isoI, isoJ, ii)][id];
+        }
+      }
+      const int64_t p = ctx.connec[ielem + (int64_t)nelem * igaus];
+      double gu[3][3] = {}, divql = 0.0;
+      for (int id = 0; id < 3; ++id)
+        for (int jd = 0; jd < 3; ++jd) {
+          gradRho[p + N * id] = gradRho[p + N * id] + SOD_HE(id, jd, igaus, ielem) * gIR[jd];
+          divql = divql + SOD_HE(id, jd, igaus, ielem) * gIRU[id][jd];
+          for (int kd = 0; kd < 3; ++kd) gu[id][jd] = gu[id][jd] + SOD_HE(jd, kd, igaus, ielem) * gIU[id][kd];
+        }
+      const double divul = gu[0][0] + gu[1][1] + gu[2][2];
+      divU[p] = divU[p] + 0.5 * (divql + rho[p] * divul);
+      for (int id = 0; id < 3; ++id)
+        for (int jd = 0; jd < 3; ++jd) {
+          for (int kd = 0; kd < 3; ++kd)
+            curlU[p + N * id] = curlU[p + N * id] + levi[id + 3 * (jd + 3 * kd)] * gu[jd][kd];
+          Qcrit[p] = Qcrit[p] - 0.5 * (gu[id][jd] * gu[jd][id]);
+        }
+      lelpn[p] += 1;
+    }
+  }
+  for (int64_t p = 0; p < N; ++p) {
+    const double c = (double)lelpn[p];
+    for (int d = 0; d < 3; ++d) {
+      gradRho[p + N * d] = gradRho[p + N * d] / c;
+      curlU[p + N * d] = curlU[p + N * d] / c;
+    }
+    divU[p] = divU[p] / c;
+    Qcrit[p] = Qcrit[p] / c;
+  }
+}
+
 // ------------------------------------------------------------------------------------------
 // Boundary conditions of the non-periodic path (noBoundaries = .false.), mod_bc_routines.f90.
 // Codes from mod_constants.f90:29,41-48; a node is on a boundary when its code is below

@@ -108,6 +108,107 @@ __global__ void k_diag_final(int nblk, const double* __restrict__ partial, doubl
   }
 }
 
+// compute_fieldDerivs (mod_postpro.f90:12-139), element part: per gauss point the physical
+// gradient of rho, the reference's curl sum_jk leviCivi(i,j,k) du_j/dx_k, the split divergence
+// (div(rho u) + rho div u) / 2 and Q = -1/2 du_i/dx_j du_j/dx_i, written per element node
+// [(e*64 + d)*8]: grad rho x3, curl x3, div, Q.  The nodal average over the elements holding a
+// node (the reference's atomics, then / lelpn) is the ordered gather below.
+struct Levi {
+  double e[27];  // leviCivi(i,j,k) at i + 3j + 9k
+};
+
+__global__ void __launch_bounds__(64 * EPB) k_fderiv_elem(int nelem, const int32_t* __restrict__ econn,
+                                                         const double* __restrict__ geo, const double* __restrict__ rho,
+                                                         const double* __restrict__ u0, const double* __restrict__ u1,
+                                                         const double* __restrict__ u2, const DMat D, const Levi L,
+                                                         double* __restrict__ out) {
+  __shared__ double fs[EPB][7][FSTRIDE];  // rho, u x3, rho u x3
+  const int es = threadIdx.x >> 6, d = threadIdx.x & 63;
+  const int e = blockIdx.x * EPB + es;
+  const bool act = e < nelem;
+  const int ee = act ? e : nelem - 1;
+  const int i = d & 3, j = (d >> 2) & 3, k = d >> 4, s = sidx(i, j, k);
+  const int n = econn[(size_t)ee * NN + d];
+  const double r = rho[n];
+  const double uv[3] = {u0[n], u1[n], u2[n]};
+  fs[es][0][s] = r;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    fs[es][1 + c][s] = uv[c];
+    fs[es][4 + c][s] = r * uv[c];
+  }
+  const double* G = geo + (size_t)ee * NGEO * NN;
+  double H[9];
+#pragma unroll
+  for (int c = 0; c < 9; ++c) H[c] = G[c * NN + d];
+  __syncthreads();
+  double ph[7][3];  // physical gradient of each staged field: ph[f][r] = d f / d x_r
+#pragma unroll
+  for (int f = 0; f < 7; ++f) {
+    const double* v = fs[es][f];
+    double gx = 0.0, gy = 0.0, gz = 0.0;
+#pragma unroll
+    for (int m = 0; m < NP1; ++m) {
+      gx += D.d[i][m] * v[sidx(m, j, k)];
+      gy += D.d[j][m] * v[sidx(i, m, k)];
+      gz += D.d[k][m] * v[sidx(i, j, m)];
+    }
+#pragma unroll
+    for (int q = 0; q < 3; ++q) ph[f][q] = H[3 * q] * gx + H[3 * q + 1] * gy + H[3 * q + 2] * gz;
+  }
+  if (!act) return;
+  double o[8];
+#pragma unroll
+  for (int q = 0; q < 3; ++q) o[q] = ph[0][q];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    double c = 0.0;
+#pragma unroll
+    for (int b = 0; b < 3; ++b)
+#pragma unroll
+      for (int cc = 0; cc < 3; ++cc) c += L.e[a + 3 * b + 9 * cc] * ph[1 + b][cc];
+    o[3 + a] = c;
+  }
+  const double divq = ph[4][0] + ph[5][1] + ph[6][2];
+  const double divu = ph[1][0] + ph[2][1] + ph[3][2];
+  o[6] = 0.5 * (divq + r * divu);
+  double qc = 0.0;
+#pragma unroll
+  for (int a = 0; a < 3; ++a)
+#pragma unroll
+    for (int b = 0; b < 3; ++b) qc -= 0.5 * (ph[1 + a][b] * ph[1 + b][a]);
+  o[7] = qc;
+  double4* dst = reinterpret_cast<double4*>(out + ((size_t)e * NN + d) * 8);
+  dst[0] = make_double4(o[0], o[1], o[2], o[3]);
+  dst[1] = make_double4(o[4], o[5], o[6], o[7]);
+}
+
+// nodal average of the element values in ascending element order (deterministic)
+__global__ void __launch_bounds__(256) k_fderiv_gather(int npoin, const int32_t* __restrict__ ptr,
+                                                       const int32_t* __restrict__ idx, const double* __restrict__ el,
+                                                       double* __restrict__ gradRho, double* __restrict__ curlU,
+                                                       double* __restrict__ divU, double* __restrict__ Qcrit) {
+  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= npoin) return;
+  double a[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  const int beg = ptr[n], end = ptr[n + 1];
+  for (int c = beg; c < end; ++c) {
+    const double4* v = reinterpret_cast<const double4*>(el + (size_t)idx[c] * 8);
+    const double4 x = v[0], y = v[1];
+    a[0] += x.x; a[1] += x.y; a[2] += x.z; a[3] += x.w;
+    a[4] += y.x; a[5] += y.y; a[6] += y.z; a[7] += y.w;
+  }
+  const double cnt = (double)(end - beg);  // lelpn
+  const size_t N = (size_t)npoin;
+#pragma unroll
+  for (int q = 0; q < 3; ++q) {
+    gradRho[n + N * q] = a[q] / cnt;
+    curlU[n + N * q] = a[3 + q] / cnt;
+  }
+  divU[n] = a[6] / cnt;
+  Qcrit[n] = a[7] / cnt;
+}
+
 }  // namespace diag
 }  // namespace sod
 
@@ -133,6 +234,41 @@ int sod_tgv_diagnostics(SodMesh* m, const double* rho, const double* u, const do
   const double two_pi = 2.0 * 3.14159;  // the reference's constant (mod_analysis.f90:36)
   const double ek_scale = 1.0 / (rho0 * (two_pi * two_pi * two_pi));
   diag::k_diag_final<<<1, 256, 0, st>>>(nblk, m->buf.red, ek_scale, rho0, volT, out_dev);
+  SOD_CHECK_LAUNCH();
+  return SOD_OK;
+}
+
+int sod_compute_field_derivs(SodMesh* m, const double* rho, const double* u, const double* leviCivi,
+                             double* gradRho, double* curlU, double* divU, double* Qcrit, sod_stream_t stream) {
+  SOD_ARG(m && rho && u && gradRho && curlU && divU && Qcrit, "null argument");
+  SOD_ARG(m->nmember == 0, "field derivatives of an ensemble mesh are not supported");
+  cudaStream_t st = (cudaStream_t)stream;
+  diag::Levi L{};
+  if (leviCivi) {
+    for (int q = 0; q < 27; ++q) L.e[q] = leviCivi[q];
+  } else {  // CFDSolverBase.f90:1248-1253
+    L.e[1 + 3 * 2 + 9 * 0] = 1.0;  L.e[2 + 3 * 1 + 9 * 0] = -1.0;
+    L.e[0 + 3 * 2 + 9 * 1] = -1.0; L.e[2 + 3 * 0 + 9 * 1] = 1.0;
+    L.e[0 + 3 * 1 + 9 * 2] = 1.0;  L.e[1 + 3 * 0 + 9 * 2] = -1.0;
+  }
+  const size_t need = (size_t)m->nelem * NN * 8;
+  if (m->postpro_len < need) {
+    if (m->postpro) cudaFree(m->postpro);
+    m->postpro = nullptr;
+    m->postpro_len = 0;
+    if (cudaMalloc(&m->postpro, need * sizeof(double)) != cudaSuccess) {
+      set_error("sod_compute_field_derivs: device allocation failed");
+      return SOD_ERR_NOMEM;
+    }
+    m->postpro_len = need;
+  }
+  const size_t N = m->npoin;
+  const int nblk = (m->nelem + diag::EPB - 1) / diag::EPB;
+  diag::k_fderiv_elem<<<nblk, 64 * diag::EPB, 0, st>>>(m->nelem, m->econn, m->geo64, rho, u, u + N, u + 2 * N, m->D,
+                                                      L, m->postpro);
+  SOD_CHECK_LAUNCH();
+  diag::k_fderiv_gather<<<(m->npoin + 255) / 256, 256, 0, st>>>(m->npoin, m->n2e_ptr, m->n2e, m->postpro, gradRho,
+                                                                curlU, divU, Qcrit);
   SOD_CHECK_LAUNCH();
   return SOD_OK;
 }

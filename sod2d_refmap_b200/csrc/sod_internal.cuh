@@ -245,6 +245,8 @@ struct SodMesh {
   sod::BcState bc;             // boundaries (nb == 0: periodic path, noBoundaries)
   sod::ZoneState zone;         // buffer zone (nb == 0: flag_buffer_on = .false.)
   const double* source = nullptr;  // caller's constant momentum source term (npoin,3), or null
+  double* postpro = nullptr;       // element-node scratch of sod_compute_field_derivs
+  size_t postpro_len = 0;
 };
 
 namespace sod {

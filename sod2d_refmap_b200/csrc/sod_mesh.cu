@@ -326,6 +326,7 @@ void sod_mesh_destroy(SodMesh* m) {
   if (!m) return;
   bc_free(m);
   zone_free(m);
+  if (m->postpro) cudaFree(m->postpro);
   for (auto& kv : m->graphs)
     if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
   void* ptrs[] = {m->econn, m->geo64, m->geo32, m->Ml, m->helem, m->helem_l, m->jratio, m->n2e_ptr, m->n2e,

@@ -284,6 +284,22 @@ class Sod2dMesh:
                                            _stream(stream)))
         return best.value, ms.value
 
+    def compute_field_derivs(self, rho, u, leviCivi=None, stream=None):
+        """compute_fieldDerivs on device tensors rho (npoin) and u (3, npoin) = Fortran (npoin,3):
+        returns (gradRho (3,npoin), curlU (3,npoin), divU, Qcrit).  leviCivi: (3,3,3) array
+        or None for the reference's symbol."""
+        torch = _torch()
+        N = self.npoin
+        g = torch.empty(3, N, dtype=torch.float64, device="cuda")
+        c = torch.empty(3, N, dtype=torch.float64, device="cuda")
+        dv = torch.empty(N, dtype=torch.float64, device="cuda")
+        qc = torch.empty(N, dtype=torch.float64, device="cuda")
+        lv = None if leviCivi is None else np.asfortranarray(leviCivi, dtype=np.float64).ravel(order="F")
+        _lib.check(_lib.load().sod_compute_field_derivs(
+            self.handle, C.c_void_p(_ptr(_contig(rho))), C.c_void_p(_ptr(_contig(u))),
+            _np_ptr(lv) if lv is not None else None, *(C.c_void_p(_ptr(t)) for t in (g, c, dv, qc)), _stream(stream)))
+        return g, c, dv, qc
+
     def set_rhs_config(self, precision: int, config: int):
         """Pins the fused-RHS configuration of a precision (sod_set_rhs_config)."""
         _lib.check(_lib.load().sod_set_rhs_config(self.handle, int(precision), int(config)))
