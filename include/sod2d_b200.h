@@ -126,7 +126,7 @@ typedef struct {
  * entropy residual (time_integ.f90:256-259,299-301,434-437,474-477).  bou_codes_nodes = null
  * removes the boundaries.  Captured step graphs of the mesh are dropped.  The ensemble
  * (sod_batch_*) rejects meshes with boundaries; sod_rk4_step_vjp differentiates through the
- * routines of codes 2-5 and 8 and rejects meshes holding codes 1, 6 or 7. */
+ * routines of codes 1-5 and 8 and rejects meshes holding codes 6 or 7. */
 int sod_mesh_set_boundaries(SodMesh* mesh, const int32_t* bou_codes_nodes, const int32_t* lnbn_nodes,
                             const double* normalsAtNodes, const double* u_buffer, const SodBcParams* bc);
 
@@ -160,6 +160,16 @@ int sod_update_buffer(SodMesh* mesh, double* rho, double* q, double* E, sod_stre
  * and so does sod_rhs.  null removes it.  A source term is constant in the state: the step
  * adjoint only sees it through the stage states.  Ensemble meshes reject it. */
 int sod_mesh_set_source_term(SodMesh* mesh, const double* source_term);
+
+/* Adjoint of temporary_bc_routine_dirichlet_prim in (rho, q, E): bar (the adjoint of the new
+ * state, device rho (npoin), q (npoin,3), E (npoin)) is replaced in place by the adjoint of the
+ * old state.  (rho, q, E) is the state the routine read (used by far-field nodes, whose new
+ * state is the HLL state of their lnbn node; may be null without them).  No-slip walls zero the
+ * rows they overwrite, outlet / ABL-top nodes pass through.  SOD_ERR_UNSUPPORTED for slip walls
+ * (their new state reads the previous stage's velocity) and for a far-field node whose lnbn node
+ * lies on a boundary. */
+int sod_bc_dirichlet_prim_vjp(SodMesh* mesh, const double* rho, const double* q, const double* E,
+                              double* bar_rho, double* bar_q, double* bar_E, sod_stream_t stream);
 
 /* Device-resident solver state in the reference's array layouts (level pos=2 only).
  * Every pointer is a device pointer owned by the caller. */
@@ -386,8 +396,10 @@ int sod_rk4_main_record(SodMesh* mesh, SodState* state, const double* dt_dev, do
  * boundaries the map includes temporary_bc_routine_dirichlet_prim on every stage state and on
  * the update; for the no-slip codes 3-5 the routine is affine (constants on rho, q and, for
  * 4 and 5, E) and the outlet / ABL-top codes 2 and 8 leave the node alone, so its adjoint is a
- * constant mask of the wall rows.  Codes 1 (far field), 6 and 7 (slip walls, which read the
- * previous velocity) give SOD_ERR_UNSUPPORTED. */
+ * constant mask of the wall rows; far-field nodes (code 1) take the HLL state of their lnbn
+ * node, whose Jacobian is evaluated at the stage states and at the updated state (one more RHS
+ * evaluation at the last stage state).  Codes 6 and 7 (slip walls, which read the previous
+ * velocity), and far-field nodes together with a buffer zone, give SOD_ERR_UNSUPPORTED. */
 int sod_rk4_step_vjp(SodMesh* mesh, const double* rho, const double* q, const double* E,
                      const double* mu_e, const double* mu_sgs, const double* mu_factor,
                      const double* dt_dev, const double* stages, const double* bar_rho,

@@ -106,6 +106,7 @@ def lib():
         L.oracle_compute_field_derivs.argtypes = [C.POINTER(ElemCtx), _p, _p, _p, _p, _p, _p, _p]
         L.oracle_update_buffer.argtypes = [C.c_int, C.POINTER(BufferData), _p, _p, _p]
         L.oracle_bc_dirichlet_prim.argtypes = [C.c_int, C.POINTER(BcData), _p, _p, _p, _p, _p]
+        L.oracle_bc_jvp.argtypes = [C.c_int, C.POINTER(BcData)] + [_p] * 13
         L.oracle_bc_fix_dirichlet_residual.argtypes = [C.c_int, C.POINTER(BcData), _p, _p, _p]
         L.oracle_bc_fix_dirichlet_residual_entropy.argtypes = [C.c_int, C.POINTER(BcData), _p]
         L.oracle_adapt_dt_cfl.argtypes = [C.POINTER(ElemCtx), _p, _p, _p, C.c_double, C.c_double, _p, _p, _p]
@@ -246,6 +247,20 @@ def update_buffer(buf: BufferZone, rho, q, E):
 def bc_dirichlet_prim(bnd: Boundaries, rho, q, u, pr, E):
     """temporary_bc_routine_dirichlet_prim in place on the given FP64 arrays."""
     lib().oracle_bc_dirichlet_prim(len(rho), C.byref(bnd.c), ptr(rho), ptr(q), ptr(u), ptr(pr), ptr(E))
+
+
+def bc_jvp(bnd: Boundaries, rho, q, E, drho, dq, dE, u=None):
+    """The routine's new (rho, q, E) and its tangent along (drho, dq, dE) (dual numbers);
+    u: the aux_u the slip branch reads (zeros when None)."""
+    N = len(rho)
+    ins = [np.ascontiguousarray(rho, dtype=np.float64), np.asfortranarray(q, dtype=np.float64),
+           np.zeros((N, 3), order="F") if u is None else np.asfortranarray(u, dtype=np.float64),
+           np.ascontiguousarray(E, dtype=np.float64), np.ascontiguousarray(drho, dtype=np.float64),
+           np.asfortranarray(dq, dtype=np.float64), np.ascontiguousarray(dE, dtype=np.float64)]
+    outs = [np.zeros(N), np.zeros((N, 3), order="F"), np.zeros(N), np.zeros(N), np.zeros((N, 3), order="F"),
+            np.zeros(N)]
+    lib().oracle_bc_jvp(N, C.byref(bnd.c), *(ptr(a) for a in ins), *(ptr(a) for a in outs))
+    return (outs[0], outs[1], outs[2]), (outs[3], outs[4], outs[5])
 
 
 def bc_fix_residual(bnd: Boundaries, Rmass, Rmom, Rener):

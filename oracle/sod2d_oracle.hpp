@@ -1470,10 +1470,16 @@ inline void update_buffer(int npoin, const BufferData& B, double* rho, double* q
 // temporary_bc_routine_dirichlet_prim (mod_bc_routines.f90:17-180): the first loop copies the
 // state of each boundary node's lnbn node, the second forms its velocity and pressure, the
 // third overwrites the boundary node by code.  u is read (slip walls) and written.
-inline void temporary_bc_routine_dirichlet_prim(int npoin, const BcData& B, double* rho, double* q, double* u,
-                                                double* pr, double* E) {
+inline double bc_min(double a, double b) { return std::min(a, b); }
+inline double bc_max(double a, double b) { return std::max(a, b); }
+inline Dual bc_min(Dual a, Dual b) { return a.v <= b.v ? a : b; }
+inline Dual bc_max(Dual a, Dual b) { return a.v >= b.v ? a : b; }
+
+template <class T>
+inline void temporary_bc_routine_dirichlet_prim_t(int npoin, const BcData& B, T* rho, T* q, T* u, T* pr, T* E) {
+  using std::sqrt;
   const int64_t N = npoin;
-  std::vector<double> rho2(npoin, 0.0), p2(npoin, 0.0), E2(npoin, 0.0), u2(3 * N, 0.0), q2(3 * N, 0.0);
+  std::vector<T> rho2(npoin, T(0.0)), p2(npoin, T(0.0)), E2(npoin, T(0.0)), u2(3 * N, T(0.0)), q2(3 * N, T(0.0));
   const double gi = B.gamma_inf;
   for (int n = 0; n < npoin; ++n) {
     if (B.bou_codes_nodes[n] < kMaxNumBouCodes) {
@@ -1499,16 +1505,17 @@ inline void temporary_bc_routine_dirichlet_prim(int npoin, const BcData& B, doub
     if (bcode >= kMaxNumBouCodes) continue;
     if (bcode == kBcFarField) {
       const double E_inf = (B.rho_inf * 0.5 * (B.u_inf * B.u_inf) + B.p_inf / (gi - 1.0));
-      const double c2 = std::sqrt(gi * p2[n] / rho2[n]);
-      double sl = std::min(B.u_inf - B.c_inf, u2[n] - c2);
-      double sr = std::max(u2[n] + c2, B.u_inf + B.c_inf);
-      const double rho_hll = (sr * rho2[n] - sl * B.rho_inf + B.rho_inf * B.u_inf - q2[n]) / (sr - sl);
-      const double E_hll = (sr * E2[n] - sl * E_inf + B.u_inf * (E_inf + B.p_inf) - u2[n] * (E2[n] + p2[n])) / (sr - sl);
-      double qh[3];
+      const T c2 = sqrt(gi * p2[n] / rho2[n]);
+      T sl = bc_min(T(B.u_inf - B.c_inf), u2[n] - c2);
+      T sr = bc_max(u2[n] + c2, T(B.u_inf + B.c_inf));
+      const T rho_hll = (sr * rho2[n] - sl * B.rho_inf + B.rho_inf * B.u_inf - q2[n]) / (sr - sl);
+      const T E_hll = (sr * E2[n] - sl * E_inf + B.u_inf * (E_inf + B.p_inf) - u2[n] * (E2[n] + p2[n])) / (sr - sl);
+      T qh[3];
       for (int d = 0; d < 3; ++d) {
-        const double ub = B.u_buffer[n + N * d], ud = u2[n + N * d], qd = q2[n + N * d];
-        sl = std::min(ub - B.c_inf, ud - c2);
-        sr = std::max(ud + c2, ub + B.c_inf);
+        const double ub = B.u_buffer[n + N * d];
+        const T ud = u2[n + N * d], qd = q2[n + N * d];
+        sl = bc_min(T(ub - B.c_inf), ud - c2);
+        sr = bc_max(ud + c2, T(ub + B.c_inf));
         qh[d] = (sr * qd - sl * B.rho_inf * ub + B.rho_inf * (ub * ub) - ud * qd) / (sr - sl);
       }
       rho[n] = rho_hll;
@@ -1518,23 +1525,28 @@ inline void temporary_bc_routine_dirichlet_prim(int npoin, const BcData& B, doub
       pr[n] = rho[n] * (gi - 1.0) *
               ((E[n] / rho[n]) - 0.5 * ((u[n] * u[n]) + (u[n + N] * u[n + N]) + (u[n + 2 * N] * u[n + 2 * N])));
     } else if (bcode == kBcNonSlipAdiabatic) {
-      for (int d = 0; d < 3; ++d) q[n + N * d] = 0.0;
-      for (int d = 0; d < 3; ++d) u[n + N * d] = 0.0;
-      rho[n] = B.rho_inf;
+      for (int d = 0; d < 3; ++d) q[n + N * d] = T(0.0);
+      for (int d = 0; d < 3; ++d) u[n + N * d] = T(0.0);
+      rho[n] = T(B.rho_inf);
     } else if (bcode == kBcNonSlipHot || bcode == kBcNonSlipCold) {
-      for (int d = 0; d < 3; ++d) q[n + N * d] = 0.0;
-      for (int d = 0; d < 3; ++d) u[n + N * d] = 0.0;
-      rho[n] = B.p_inf / B.Rgas_inf / (bcode == kBcNonSlipHot ? B.T_H : B.T_C);
-      E[n] = B.p_inf / (gi - 1.0);
+      for (int d = 0; d < 3; ++d) q[n + N * d] = T(0.0);
+      for (int d = 0; d < 3; ++d) u[n + N * d] = T(0.0);
+      rho[n] = T(B.p_inf / B.Rgas_inf / (bcode == kBcNonSlipHot ? B.T_H : B.T_C));
+      E[n] = T(B.p_inf / (gi - 1.0));
     } else if (bcode == kBcSlipWallModel || bcode == kBcSlipAdiabatic) {
       E[n] = E[n] - rho[n] * 0.5 * ((u[n] * u[n]) + (u[n + N] * u[n + N]) + (u[n + 2 * N] * u[n + 2 * N]));
-      const double norm = (B.normals[n] * q[n]) + (B.normals[n + N] * q[n + N]) + (B.normals[n + 2 * N] * q[n + 2 * N]);
+      const T norm = (B.normals[n] * q[n]) + (B.normals[n + N] * q[n + N]) + (B.normals[n + 2 * N] * q[n + 2 * N]);
       for (int d = 0; d < 3; ++d) q[n + N * d] = q[n + N * d] - norm * B.normals[n + N * d];
-      rho[n] = B.rho_inf;
+      rho[n] = T(B.rho_inf);
       for (int d = 0; d < 3; ++d) u[n + N * d] = q[n + N * d] / rho[n];
       E[n] = E[n] + rho[n] * 0.5 * ((u[n] * u[n]) + (u[n + N] * u[n + N]) + (u[n + 2 * N] * u[n + 2 * N]));
     }
   }
+}
+
+inline void temporary_bc_routine_dirichlet_prim(int npoin, const BcData& B, double* rho, double* q, double* u,
+                                                double* pr, double* E) {
+  temporary_bc_routine_dirichlet_prim_t<double>(npoin, B, rho, q, u, pr, E);
 }
 
 // bc_fix_dirichlet_residual (mod_bc_routines.f90:181-221): no-slip walls keep rho and rho u

@@ -89,6 +89,7 @@ _SIGS = {
     "sod_mesh_set_buffer": (_i, [_p] * 4),
     "sod_set_rhs_config": (_i, [_p, _i, _i]),
     "sod_compute_field_derivs": (_i, [_p] * 9),
+    "sod_bc_dirichlet_prim_vjp": (_i, [_p] * 8),
     "sod_mesh_set_source_term": (_i, [_p] * 2),
     "sod_update_buffer": (_i, [_p] * 5),
     "sod_bc_dirichlet_prim": (_i, [_p] * 7),

@@ -510,6 +510,39 @@ __global__ void __launch_bounds__(256) k_stage_state(int64_t N, const int32_t* _
   for (int f = 0; f < 5; ++f) ys[f * N + n] = y.c[f][n] - da * (r[f] / ml);
 }
 
+// y0 - dt sum_s b_s R_s from the stage states (dt R_1 = 2 (y0 - Y2), dt R_2 = 2 (y0 - Y3),
+// dt R_3 = y0 - Y4) and R_4 = gather(rel)/Ml (+ the source term): the forward's updated state at
+// nodes the routines do not modify
+__global__ void __launch_bounds__(256) k_final_pre(int64_t N, const int32_t* __restrict__ ptr,
+                                                   const int32_t* __restrict__ idx, const double* __restrict__ el,
+                                                   const double* __restrict__ Ml, const double* __restrict__ dt,
+                                                   Cols5 y, const double* __restrict__ Y2,
+                                                   const double* __restrict__ Y3, const double* __restrict__ Y4,
+                                                   const double* __restrict__ src, double* __restrict__ zf) {
+  const int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= N) return;
+  double r[5] = {0, 0, 0, 0, 0};
+  const int beg = ptr[n], end = ptr[n + 1];
+  for (int c = beg; c < end; ++c) {
+    double v[6];
+    load_res6<double>(el, (size_t)idx[c], v);
+#pragma unroll
+    for (int f = 0; f < 5; ++f) r[f] += v[f];
+  }
+  const double ml = Ml[n];
+  if (src) {
+#pragma unroll
+    for (int d = 0; d < 3; ++d) r[1 + d] -= ml * src[d * N + n];
+  }
+  const double h = (*dt) / 6.0;
+#pragma unroll
+  for (int f = 0; f < 5; ++f) {
+    const double y0 = y.c[f][n];
+    const double acc = (y0 - Y2[f * N + n]) / 3.0 + 2.0 * (y0 - Y3[f * N + n]) / 3.0 + (y0 - Y4[f * N + n]) / 3.0;
+    zf[f * N + n] = y0 - acc - h * (r[f] / ml);
+  }
+}
+
 static int launch_vjp(SodMesh* m, const double* rho, const double* q0, const double* q1, const double* q2,
                       const double* E, const double* mu_factor, const double* musgs, const double* w, cudaStream_t st) {
   VjpArgs a;
@@ -587,11 +620,16 @@ int sod_rk4_step_vjp(SodMesh* m, const double* rho, const double* q, const doubl
   SOD_ARG(m && rho && q && E && mu_e && mu_factor && dt_dev, "inputs null");
   SOD_ARG(bar_rho && bar_q && bar_E && out_rho && out_q && out_E, "adjoint arrays null");
   // boundaries and buffer zone: the routines' adjoints after every stage VJP and on the seed
-  // (walls and passive boundary codes; far-field and slip codes are refused)
+  // (wall, passive and far-field boundary codes; slip codes are refused)
   const bool has_bc = m->bc.nb > 0, has_zone = m->zone.nb > 0;
   const bool bc = has_bc || has_zone;
-  if (has_bc && m->bc.has_state_dependent) {
-    set_error("sod_rk4_step_vjp: the adjoint of the far-field and slip-wall boundary codes is not built");
+  const bool ff = has_bc && m->bc.nff > 0;
+  if (has_bc && m->bc.has_slip) {
+    set_error("sod_rk4_step_vjp: the adjoint of the slip-wall boundary codes is not built");
+    return SOD_ERR_UNSUPPORTED;
+  }
+  if (ff && has_zone) {
+    set_error("sod_rk4_step_vjp: far-field boundaries together with a buffer zone are not differentiated");
     return SOD_ERR_UNSUPPORTED;
   }
   NvtxRange range("sod rk4 step vjp");
@@ -614,14 +652,15 @@ int sod_rk4_step_vjp(SodMesh* m, const double* rho, const double* q, const doubl
       if (int r = zone_stage(m, ys, st)) return r;
     return has_bc ? bc_stage(m, ys, stage_of, st) : SOD_OK;
   };
-  auto pre_adjoint = [&](double* vbar) -> int {
+  // y: the state the boundary routine read (its far-field nodes' lnbn rows)
+  auto pre_adjoint = [&](double* vbar, const double* y) -> int {
     if (has_bc)
-      if (int r = bc_adjoint(m, vbar, st)) return r;
+      if (int r = bc_adjoint(m, vbar, y, st)) return r;
     return has_zone ? zone_adjoint(m, vbar, st) : SOD_OK;
   };
-  // scratch: ybar copy | w | (with boundaries: Y1 | Ybar of a stage) | (ys2 ys3 ys4 when the
-  // stages are not given)   (5 columns each)
-  const size_t base = bc ? 20 : 10;
+  // scratch: ybar copy | w | (with boundaries: Y1 | Ybar of a stage) | (far-field: the updated
+  // state before the routine) | (ys2 ys3 ys4 when the stages are not given)   (5 columns each)
+  const size_t base = bc ? (ff ? 25 : 20) : 10;
   rc = ensure_adj(m, (base + (stages ? 0 : 15)) * (size_t)N);
   if (rc) return rc;
   rc = mesh_ref_to_internal_elem(m, mu_e, m->mue_int, st);
@@ -630,6 +669,7 @@ int sod_rk4_step_vjp(SodMesh* m, const double* rho, const double* q, const doubl
   double* w = m->adj + 5 * N;
   double* y1s = bc ? m->adj + 10 * N : nullptr;   // first stage state B(y0)
   double* Ybs = bc ? m->adj + 15 * N : nullptr;   // adjoint of one stage state
+  double* zf = ff ? m->adj + 20 * N : nullptr;     // y0 - dt sum b_s R_s, before the final routine
   const double* ys[3];
   const double* rel = reinterpret_cast<const double*>(m->buf.rel);
   Cols5 y0{{rho, q, q + N, q + 2 * N, E}};
@@ -662,6 +702,18 @@ int sod_rk4_step_vjp(SodMesh* m, const double* rho, const double* q, const doubl
       cur = Cols5{{b, b + N, b + 2 * N, b + 3 * N, b + 4 * N}};
     }
   }
+  if (ff) {
+    // the updated state the final routine reads, at the far-field nodes' lnbn nodes (interior:
+    // there the stage states equal their pre-routine values, so dt R_s = (y0 - Y_{s+1}) / a_{s+1}
+    // for s = 1..3); R_4 from one more RHS evaluation at Y4
+    const int epb = m->tuned_epb[0] ? m->tuned_epb[0] : 2;
+    const double* y4 = ys[2];
+    rc = launch_rhs(m, false, epb, y4, y4 + N, y4 + 2 * N, y4 + 3 * N, y4 + 4 * N, mu_factor, musgs, st);
+    if (rc) return rc;
+    k_final_pre<<<nblk(N), 256, 0, st>>>(N, m->n2e_ptr, m->n2e, rel, m->Ml, dt_dev, y0, ys[0], ys[1], ys[2],
+                                         m->source, zf);
+    SOD_CHECK_LAUNCH();
+  }
   // reverse sweep: kbar4 = -dt/6 ybar, Ybar4 = J4^T kbar4, kbar3 = -dt (ybar/3 + Ybar4), ...
   // (with boundaries ybar is first mapped through the final routine's adjoint)
   Cols5 src{{bar_rho, bar_q, bar_q + N, bar_q + 2 * N, bar_E}};
@@ -669,7 +721,7 @@ int sod_rk4_step_vjp(SodMesh* m, const double* rho, const double* q, const doubl
   if (bc) {
     for (int f = 0; f < 5; ++f)
       SOD_CUDA(cudaMemcpyAsync(keep.c[f], src.c[f], N * sizeof(double), cudaMemcpyDeviceToDevice, st));
-    rc = pre_adjoint(yb);
+    rc = pre_adjoint(yb, zf);
     if (rc) return rc;
     src = Cols5{{yb, yb + N, yb + 2 * N, yb + 3 * N, yb + 4 * N}};
     keep = MCols5{{nullptr, nullptr, nullptr, nullptr, nullptr}};
@@ -700,12 +752,40 @@ int sod_rk4_step_vjp(SodMesh* m, const double* rho, const double* q, const doubl
       k_gather_vjp<<<nblk(N), 256, 0, st>>>(N, m->n2e_ptr, m->n2e, rel, yc, 0, nullptr, nullptr, nullptr, 0.0, 0.0,
                                              nullptr);
       SOD_CHECK_LAUNCH();
-      rc = pre_adjoint(Ybs);
+      rc = pre_adjoint(Ybs, stage == 1 ? y1s : ys[stage - 2]);
       if (rc) return rc;
       k_accum_seed<<<nblk(N), 256, 0, st>>>(N, Ybs, acc, yb, m->Ml, dt_dev, cb[t], ca[t], stage > 1 ? w : nullptr);
       SOD_CHECK_LAUNCH();
     }
   }
+  return SOD_OK;
+}
+
+int sod_bc_dirichlet_prim_vjp(SodMesh* m, const double* rho, const double* q, const double* E, double* bar_rho,
+                              double* bar_q, double* bar_E, sod_stream_t stream) {
+  SOD_ARG(m && bar_rho && bar_q && bar_E, "null argument");
+  SOD_ARG(m->bc.nb > 0, "no boundary nodes registered (sod_mesh_set_boundaries)");
+  SOD_ARG(m->bc.nff == 0 || (rho && q && E), "far-field adjoint needs the state the routine read");
+  cudaStream_t st = (cudaStream_t)stream;
+  const size_t N = m->npoin;
+  int rc = ensure_adj(m, 10 * N);
+  if (rc) return rc;
+  double* v = m->adj;
+  double* y = m->adj + 5 * N;
+  const double* bars[3] = {bar_rho, bar_q, bar_E};
+  const size_t cnt[3] = {N, 3 * N, N}, off[3] = {0, N, 4 * N};
+  for (int t = 0; t < 3; ++t) {
+    SOD_CUDA(cudaMemcpyAsync(v + off[t], bars[t], cnt[t] * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    if (m->bc.nff > 0) {
+      const double* ys[3] = {rho, q, E};
+      SOD_CUDA(cudaMemcpyAsync(y + off[t], ys[t], cnt[t] * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    }
+  }
+  rc = bc_adjoint(m, v, m->bc.nff > 0 ? y : nullptr, st);
+  if (rc) return rc;
+  double* outs[3] = {bar_rho, bar_q, bar_E};
+  for (int t = 0; t < 3; ++t)
+    SOD_CUDA(cudaMemcpyAsync(outs[t], v + off[t], cnt[t] * sizeof(double), cudaMemcpyDeviceToDevice, st));
   return SOD_OK;
 }
 

@@ -20,6 +20,8 @@
 // residual is zeroed on no-slip walls and the entropy normalisation (mean and spread of eta,
 // mod_entropy_viscosity.f90:43-66) is recomputed from the post-boundary eta.
 #include "sod_internal.cuh"
+#include <algorithm>
+#include <utility>
 #include <vector>
 
 namespace sod {
@@ -76,6 +78,27 @@ struct ApplyArgs {
 // the routine's aux_u / aux_p where it sets them (set_u / set_p).
 template <typename T> __device__ __forceinline__ T cst(double v);
 template <> __device__ __forceinline__ double cst<double>(double v) { return v; }
+__device__ __forceinline__ double bsqrt(double a) { return ::sqrt(a); }
+__device__ __forceinline__ double bmin(double a, double b) { return ::fmin(a, b); }
+__device__ __forceinline__ double bmax(double a, double b) { return ::fmax(a, b); }
+
+// forward-mode dual numbers: the directional derivative of the far-field state (the adjoint)
+struct Dual {
+  double v, d;
+};
+__device__ __forceinline__ Dual operator+(Dual a, Dual b) { return {a.v + b.v, a.d + b.d}; }
+__device__ __forceinline__ Dual operator-(Dual a, Dual b) { return {a.v - b.v, a.d - b.d}; }
+__device__ __forceinline__ Dual operator*(Dual a, Dual b) { return {a.v * b.v, a.d * b.v + a.v * b.d}; }
+__device__ __forceinline__ Dual operator/(Dual a, Dual b) {
+  return {a.v / b.v, (a.d * b.v - a.v * b.d) / (b.v * b.v)};
+}
+template <> __device__ __forceinline__ Dual cst<Dual>(double v) { return {v, 0.0}; }
+__device__ __forceinline__ Dual bsqrt(Dual a) {
+  const double s = ::sqrt(a.v);
+  return {s, a.d / (2.0 * s)};
+}
+__device__ __forceinline__ Dual bmin(Dual a, Dual b) { return a.v <= b.v ? a : b; }
+__device__ __forceinline__ Dual bmax(Dual a, Dual b) { return a.v >= b.v ? a : b; }
 
 template <typename T>
 __device__ __forceinline__ void bc_point(int c, const T (&own)[5], const T (&nb)[5], const double (&uo)[3],
@@ -95,17 +118,17 @@ __device__ __forceinline__ void bc_point(int c, const T (&own)[5], const T (&nb)
   set_u = set_p = false;
   if (c == kFarField) {
     const double E_inf = (p.rho_inf * 0.5 * (p.u_inf * p.u_inf) + p.p_inf / (gi - 1.0));
-    const T c2 = ::sqrt(cst<T>(gi) * p2 / rho2);
-    T sl = ::fmin(cst<T>(p.u_inf - p.c_inf), u2[0] - c2);
-    T sr = ::fmax(u2[0] + c2, cst<T>(p.u_inf + p.c_inf));
+    const T c2 = bsqrt(cst<T>(gi) * p2 / rho2);
+    T sl = bmin(cst<T>(p.u_inf - p.c_inf), u2[0] - c2);
+    T sr = bmax(u2[0] + c2, cst<T>(p.u_inf + p.c_inf));
     const T rho_hll = (sr * rho2 - sl * cst<T>(p.rho_inf) + cst<T>(p.rho_inf * p.u_inf) - q2[0]) / (sr - sl);
     const T E_hll = (sr * E2 - sl * cst<T>(E_inf) + cst<T>(p.u_inf * (E_inf + p.p_inf)) - u2[0] * (E2 + p2)) /
                     (sr - sl);
     T qh[3];
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
-      sl = ::fmin(cst<T>(ub[d] - p.c_inf), u2[d] - c2);
-      sr = ::fmax(u2[d] + c2, cst<T>(ub[d] + p.c_inf));
+      sl = bmin(cst<T>(ub[d] - p.c_inf), u2[d] - c2);
+      sr = bmax(u2[d] + c2, cst<T>(ub[d] + p.c_inf));
       qh[d] = (sr * q2[d] - sl * cst<T>(p.rho_inf) * cst<T>(ub[d]) + cst<T>(p.rho_inf * (ub[d] * ub[d])) -
                u2[d] * q2[d]) / (sr - sl);
     }
@@ -190,20 +213,79 @@ __global__ void __launch_bounds__(kBlock) k_bc_apply(const ApplyArgs a) {
   if (a.Reta && no_slip(c)) a.Reta[n] = 0.0;
 }
 
-// Adjoint of the routine for the codes whose new state does not depend on the old one except
-// through the identity: no-slip adiabatic keeps E (rho and q are constants), the isothermal
-// walls set every field to a constant, outlet / ABL-top codes leave the node alone.  vbar is the
-// adjoint of the new state ([5][npoin] columns), mapped in place to that of the old state.
+// Adjoint of the routine, in three steps on vbar, the adjoint of the new state ([5][npoin]
+// columns), mapped in place to that of the old state.  (1) Far-field nodes: the new state is
+// the HLL state of the lnbn node's old state, so J^T vbar(node) is formed with dual numbers
+// (5 directions through bc_point<Dual>) into per-node contributions.  (2) The rows the routine
+// overwrites are zeroed: far-field nodes entirely, no-slip nodes in rho and q (adiabatic walls
+// keep E, isothermal walls set it), outlet / ABL-top nodes are left alone.  (3) Each lnbn node
+// of a far-field node adds the contributions of the far-field nodes that read it, in ascending
+// order (deterministic).
+__global__ void __launch_bounds__(kBlock) k_bc_ff_adjoint(int nb, const int32_t* __restrict__ node,
+                                                          const int32_t* __restrict__ code,
+                                                          const int32_t* __restrict__ nbr, size_t N,
+                                                          const double* __restrict__ y,
+                                                          const double* __restrict__ vbar,
+                                                          const double* __restrict__ normal,
+                                                          const double* __restrict__ ubuf, const SodBcParams p,
+                                                          double* __restrict__ contrib) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= nb || code[b] != kFarField) return;
+  const size_t n = (size_t)node[b], s = (size_t)nbr[b];
+  double w[5];
+#pragma unroll
+  for (int f = 0; f < 5; ++f) w[f] = vbar[f * N + n];
+  const double uo[3] = {0.0, 0.0, 0.0};
+  const double nrm[3] = {normal[b], normal[(size_t)nb + b], normal[2 * (size_t)nb + b]};
+  const double ubv[3] = {ubuf[b], ubuf[(size_t)nb + b], ubuf[2 * (size_t)nb + b]};
+  for (int dir = 0; dir < 5; ++dir) {
+    Dual own[5], nbd[5], out[5], uu[3], pp;
+#pragma unroll
+    for (int f = 0; f < 5; ++f) {
+      own[f] = Dual{0.0, 0.0};
+      nbd[f] = Dual{y[f * N + s], f == dir ? 1.0 : 0.0};
+    }
+    bool su, sp;
+    bc_point<Dual>(kFarField, own, nbd, uo, nrm, ubv, p, out, uu, pp, su, sp);
+    double c = 0.0;
+#pragma unroll
+    for (int f = 0; f < 5; ++f) c += out[f].d * w[f];
+    contrib[(size_t)dir * nb + b] = c;
+  }
+}
+
 __global__ void k_bc_adjoint_mask(int nb, const int32_t* __restrict__ node, const int32_t* __restrict__ code,
                                   size_t N, double* __restrict__ vbar) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= nb) return;
   const int c = code[b];
-  if (!no_slip(c)) return;
   const size_t n = (size_t)node[b];
+  if (c == kFarField) {
+#pragma unroll
+    for (int f = 0; f < 5; ++f) vbar[f * N + n] = 0.0;
+    return;
+  }
+  if (!no_slip(c)) return;
 #pragma unroll
   for (int f = 0; f < 4; ++f) vbar[f * N + n] = 0.0;
   if (c != kNonSlipAdiabatic) vbar[4 * N + n] = 0.0;
+}
+
+__global__ void __launch_bounds__(kBlock) k_bc_ff_scatter(int nu, const int32_t* __restrict__ ptr,
+                                                          const int32_t* __restrict__ target,
+                                                          const int32_t* __restrict__ bidx, int nb, size_t N,
+                                                          const double* __restrict__ contrib,
+                                                          double* __restrict__ vbar) {
+  const int u = blockIdx.x * blockDim.x + threadIdx.x;
+  if (u >= nu) return;
+  const size_t s = (size_t)target[u];
+  const int beg = ptr[u], end = ptr[u + 1];
+#pragma unroll
+  for (int f = 0; f < 5; ++f) {
+    double a = 0.0;
+    for (int k = beg; k < end; ++k) a += contrib[(size_t)f * nb + bidx[k]];
+    vbar[f * N + s] += a;
+  }
 }
 
 // bc_fix_dirichlet_residual (mod_bc_routines.f90:181-221) and _entropy (:265-291)
@@ -310,22 +392,39 @@ static int gather(SodMesh* m, const double* rho, const double* q, const double* 
 
 }  // namespace bcd
 
-// adjoint of the routine in place on vbar ([5][npoin]); SOD_ERR_UNSUPPORTED when a boundary
-// node has a code whose new state depends on the old state (far-field, slip walls)
-int bc_adjoint(SodMesh* m, double* vbar, cudaStream_t st) {
-  if (m->bc.has_state_dependent) {
-    set_error("the adjoint of the far-field and slip-wall boundary codes is not built");
+// SOD_ERR_UNSUPPORTED for slip walls (their new state reads the velocity of the previous
+// stage) and for far-field nodes whose lnbn node is itself a boundary node
+int bc_adjoint(SodMesh* m, double* vbar, const double* y, cudaStream_t st) {
+  const BcState& B = m->bc;
+  if (B.has_slip) {
+    set_error("the adjoint of the slip-wall boundary codes is not built");
     return SOD_ERR_UNSUPPORTED;
   }
-  bcd::k_bc_adjoint_mask<<<bcd::grid_of(m->bc.nb), bcd::kBlock, 0, st>>>(m->bc.nb, m->bc.node, m->bc.code,
-                                                                         (size_t)m->npoin, vbar);
+  if (B.nff > 0 && B.ff_nbr_on_boundary) {
+    set_error("far-field adjoint: an lnbn node of a far-field node lies on a boundary");
+    return SOD_ERR_UNSUPPORTED;
+  }
+  const size_t N = m->npoin;
+  if (B.nff > 0) {
+    SOD_ARG(y, "far-field adjoint needs the state the routine read");
+    bcd::k_bc_ff_adjoint<<<bcd::grid_of(B.nb), bcd::kBlock, 0, st>>>(B.nb, B.node, B.code, B.nbr, N, y, vbar,
+                                                                     B.normal, B.ubuf, B.prm, B.ff_contrib);
+    SOD_CHECK_LAUNCH();
+  }
+  bcd::k_bc_adjoint_mask<<<bcd::grid_of(B.nb), bcd::kBlock, 0, st>>>(B.nb, B.node, B.code, N, vbar);
   SOD_CHECK_LAUNCH();
+  if (B.nff > 0) {
+    bcd::k_bc_ff_scatter<<<bcd::grid_of(B.ff_nu), bcd::kBlock, 0, st>>>(B.ff_nu, B.ff_ptr, B.ff_target, B.ff_b,
+                                                                         B.nb, N, B.ff_contrib, vbar);
+    SOD_CHECK_LAUNCH();
+  }
   return SOD_OK;
 }
 
 void bc_free(SodMesh* m) {
   BcState& b = m->bc;
-  void* ptrs[] = {b.node, b.code, b.nbr, b.normal, b.ubuf, b.aux2, b.u_stage, b.u_final};
+  void* ptrs[] = {b.node, b.code, b.nbr, b.normal, b.ubuf, b.aux2, b.u_stage, b.u_final,
+                  b.ff_ptr, b.ff_target, b.ff_b, b.ff_contrib};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   b = BcState{};
@@ -436,7 +535,41 @@ int sod_mesh_set_boundaries(SodMesh* m, const int32_t* codes, const int32_t* lnb
   B.nb = nb;
   B.prm = *bc;
   for (int c : code)
-    if (c == bcd::kFarField || c == bcd::kSlipAdiabatic || c == bcd::kSlipWallModel) B.has_state_dependent = true;
+    if (c == bcd::kSlipAdiabatic || c == bcd::kSlipWallModel) B.has_slip = true;
+  // far-field adjoint scatter: lnbn targets in ascending node order, readers in ascending order
+  {
+    std::vector<std::pair<int32_t, int32_t>> tb;  // (target node, boundary index)
+    for (int b = 0; b < nb; ++b)
+      if (code[b] == bcd::kFarField) {
+        tb.emplace_back(nbr[b], b);
+        if (codes[nbr[b]] < bcd::kMaxNumBouCodes) B.ff_nbr_on_boundary = true;
+      }
+    std::sort(tb.begin(), tb.end());
+    std::vector<int32_t> ptr{0}, target, bidx;
+    for (size_t k = 0; k < tb.size(); ++k) {
+      if (k == 0 || tb[k].first != tb[k - 1].first) {
+        if (k > 0) ptr.push_back((int32_t)k);
+        target.push_back(tb[k].first);
+      }
+      bidx.push_back(tb[k].second);
+    }
+    ptr.push_back((int32_t)tb.size());
+    B.nff = (int)tb.size();
+    B.ff_nu = (int)target.size();
+    if (B.nff > 0) {
+      if (!(alloc((void**)&B.ff_ptr, sizeof(int32_t) * ptr.size()) &&
+            alloc((void**)&B.ff_target, sizeof(int32_t) * target.size()) &&
+            alloc((void**)&B.ff_b, sizeof(int32_t) * bidx.size()) &&
+            alloc((void**)&B.ff_contrib, sizeof(double) * 5 * (size_t)nb))) {
+        bc_free(m);
+        set_error("sod_mesh_set_boundaries: device allocation failed");
+        return SOD_ERR_NOMEM;
+      }
+      SOD_CUDA(cudaMemcpy(B.ff_ptr, ptr.data(), sizeof(int32_t) * ptr.size(), cudaMemcpyHostToDevice));
+      SOD_CUDA(cudaMemcpy(B.ff_target, target.data(), sizeof(int32_t) * target.size(), cudaMemcpyHostToDevice));
+      SOD_CUDA(cudaMemcpy(B.ff_b, bidx.data(), sizeof(int32_t) * bidx.size(), cudaMemcpyHostToDevice));
+    }
+  }
   SOD_CUDA(cudaMemcpy(B.node, node.data(), sizeof(int32_t) * nb, cudaMemcpyHostToDevice));
   SOD_CUDA(cudaMemcpy(B.code, code.data(), sizeof(int32_t) * nb, cudaMemcpyHostToDevice));
   SOD_CUDA(cudaMemcpy(B.nbr, nbr.data(), sizeof(int32_t) * nb, cudaMemcpyHostToDevice));

@@ -164,7 +164,16 @@ struct BcState {
   double* aux2 = nullptr;      // [5][nb] state of the lnbn node (rho, q x3, E)
   double* u_stage = nullptr;   // [3][nb] aux_u of the previous stage's EOS
   double* u_final = nullptr;   // [3][nb] u(:,:,pos) at the start of the step
-  bool has_state_dependent = false;  // a far-field or slip code: no adjoint
+  bool has_slip = false;       // a slip code (6, 7): reads the previous velocity, no adjoint
+  // far-field nodes (code 1): their lnbn nodes, each with the far-field nodes that read it in
+  // ascending order (CSR), for the ordered scatter of the adjoint; the adjoint's per-node
+  // contributions [5][nb]
+  int nff = 0, ff_nu = 0;
+  bool ff_nbr_on_boundary = false;  // an lnbn node of a far-field node is a boundary node
+  int32_t* ff_ptr = nullptr;
+  int32_t* ff_target = nullptr;
+  int32_t* ff_b = nullptr;
+  double* ff_contrib = nullptr;
   SodBcParams prm{};
 };
 
@@ -265,7 +274,9 @@ int take_nonfinite(SodMesh* m, cudaStream_t st, bool* flagged);
 int bc_snapshot_u(SodMesh* m, const double* u, cudaStream_t st);
 int bc_stage(SodMesh* m, double* ys, int stage, cudaStream_t st);
 int bc_final(SodMesh* m, SodState* s, double* Reta, cudaStream_t st);
-int bc_adjoint(SodMesh* m, double* vbar, cudaStream_t st);
+// adjoint of the routine in place on vbar ([5][npoin]); y ([5][npoin]) is the state the routine
+// read (only its far-field nodes' lnbn rows are used; may be null without far-field nodes)
+int bc_adjoint(SodMesh* m, double* vbar, const double* y, cudaStream_t st);
 void bc_free(SodMesh* m);
 // entropy normalisation (mean and spread of eta) recomputed into buf.scal after a routine that
 // changed eta

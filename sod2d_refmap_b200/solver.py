@@ -240,6 +240,12 @@ class Sod2dMesh:
         _lib.check(_lib.load().sod_bc_dirichlet_prim(self.handle, *(C.c_void_p(_ptr(_contig(t))) for t in (
             rho, q, u, pr, E)), _stream(stream)))
 
+    def bc_dirichlet_prim_vjp(self, rho, q, E, bar_rho, bar_q, bar_E, stream=None):
+        """Adjoint of temporary_bc_routine_dirichlet_prim in place on (bar_rho, bar_q (3,npoin),
+        bar_E); (rho, q, E) the state the routine read."""
+        _lib.check(_lib.load().sod_bc_dirichlet_prim_vjp(self.handle, *(C.c_void_p(_ptr(_contig(t))) for t in (
+            rho, q, E, bar_rho, bar_q, bar_E)), _stream(stream)))
+
     def bc_fix_residual(self, Rmass, Rmom, Rener, stream=None):
         _lib.check(_lib.load().sod_bc_fix_dirichlet_residual(self.handle, *(C.c_void_p(_ptr(_contig(t))) for t in (
             Rmass, Rmom, Rener)), _stream(stream)))

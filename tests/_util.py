@@ -28,7 +28,15 @@ def oracle_bc_map(oracle, bnd):
     return B
 
 
-def oracle_step_jvp(oracle, om, prm, st, dt, v, mu_sgs=None, bc=None):
+def oracle_bc_jvp_map(oracle, bnd):
+    """(y, v) -> (B(y), J_B(y) v) for the routine in dual numbers (exact for every code that does
+    not read aux_u)."""
+    def J(y, v):
+        return oracle.bc_jvp(bnd, y[0], y[1], y[2], v[0], v[1], v[2])
+    return J
+
+
+def oracle_step_jvp(oracle, om, prm, st, dt, v, mu_sgs=None, bc=None, bc_jvp=None):
     """One rk_4_main step (time_integ.f90:288-426) from the FlowState st and its JVP along
     v = (drho, dq (npoin,3), dE), composed from the oracle's dual-number stage JVPs with mu_e
     (and mu_sgs) frozen.  bc (oracle_bc_map) selects the non-periodic path: the routine on every
@@ -40,6 +48,8 @@ def oracle_step_jvp(oracle, om, prm, st, dt, v, mu_sgs=None, bc=None):
         return s
 
     def bmap(y, w):
+        if bc_jvp is not None:
+            return bc_jvp(tuple(y), tuple(w))
         if bc is None:
             return tuple(y), tuple(w)
         by = bc(*y)
@@ -61,6 +71,6 @@ def oracle_step_jvp(oracle, om, prm, st, dt, v, mu_sgs=None, bc=None):
         if a_next[s] is not None:
             ys, vs = bmap(tuple(y0[f] - dt * a_next[s] * Rc[f] for f in range(3)),
                           tuple(v[f] - dt * a_next[s] * dRc[f] for f in range(3)))
-    if bc is not None:
+    if bc is not None or bc_jvp is not None:
         acc_y, acc_v = (list(t) for t in bmap(acc_y, acc_v))
     return acc_y, acc_v

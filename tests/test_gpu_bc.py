@@ -257,3 +257,109 @@ def test_channel_rollout_gradient_fd(torch_mod, oracle):
         fd = (L_at(h) - L_at(-h)) / (2 * h)
         assert abs(fd - dL) <= 1e-6 * abs(dL), (h, fd, dL)
     gm.close()
+
+
+@pytest.mark.parametrize("codes", [(1, 3), (3, 1), (1, 1)])
+def test_channel_step_vjp_far_field(torch_mod, oracle, codes):
+    """Step adjoint through far-field nodes (the HLL state of the lnbn node): <w, J v> with J v
+    from the oracle's dual-number stage JVPs composed with its boundary routine in dual numbers
+    equals <J^T w, v>, bound 1e-11 relative to sum |w_i (J v)_i|, recorded and recomputed stage
+    states; the routine's own adjoint (sod_bc_dirichlet_prim_vjp) against the oracle's JVP of it
+    (1e-12)."""
+    from _util import oracle_bc_jvp_map, oracle_step_jvp
+    from sod2d_refmap_b200 import mesh as M, solver as S
+    torch = torch_mod
+    m, prm, st0, ub = channel(codes, seed=31)
+    bc = M.bc_params(prm)
+    om = oracle.OracleMesh(m)
+    bnd = oracle.Boundaries(m.extra["bou_codes_nodes"], m.extra["lnbn_nodes"], m.extra["normals"], ub, bc)
+    dt = oracle.adapt_dt(om, st0, prm)
+    st = st0.copy()
+    oracle.rk4(om, prm, st, dt, nsteps=1, bnd=bnd)
+    rng = np.random.default_rng(23)
+    rnd = lambda a: rng.standard_normal(a.shape) * np.abs(a).mean()
+    gm = S.Sod2dMesh(m, prm)
+    gm.set_boundaries(m.extra["bou_codes_nodes"], m.extra["lnbn_nodes"], m.extra["normals"], ub, bc)
+    # the routine alone
+    v = (rnd(st.rho), np.asfortranarray(rnd(st.q)), rnd(st.E))
+    w = (rnd(st.rho), np.asfortranarray(rnd(st.q)), rnd(st.E))
+    _, Jv = oracle.bc_jvp(bnd, st.rho, st.q, st.E, *v)
+    bars = [dev(torch, a) for a in w]
+    gm.bc_dirichlet_prim_vjp(dev(torch, st.rho), dev(torch, st.q), dev(torch, st.E), *bars)
+    g = [host(t) for t in bars]
+    terms = [w[f] * Jv[f] for f in range(3)]
+    lhs = sum(t.sum() for t in terms)
+    rhs = sum((g[f] * v[f]).sum() for f in range(3))
+    assert abs(lhs - rhs) <= 1e-12 * sum(np.abs(t).sum() for t in terms), (lhs, rhs)
+    # one step
+    y1, dy1 = oracle_step_jvp(oracle, om, prm, st, dt, v, bc_jvp=oracle_bc_jvp_map(oracle, bnd))
+    s = S.Sod2dState.from_host(st, gm.nelem)
+    s.dt.fill_(dt)
+    stages = torch.zeros(15 * m.npoin, dtype=torch.float64, device="cuda")
+    y0 = (s.rho.clone(), s.q.clone(), s.E.clone(), s.mu_e.clone())
+    gm.rk_4_main_record(s, stages, update_dt=False)
+    h = s.to_host()
+    for got, ref in ((h["rho"], y1[0]), (h["q"], y1[1]), (h["E"], y1[2])):
+        assert rel_l2(got, ref) < TOL64
+    terms = [w[f] * dy1[f] for f in range(3)]
+    lhs = sum(t.sum() for t in terms)
+    scale = sum(np.abs(t).sum() for t in terms)
+    outs = []
+    for stg in (stages, None):
+        out = gm.rk4_step_vjp(*y0, s.mu_factor, s.dt, *(dev(torch, a) for a in w), stages=stg)
+        g = [host(o) for o in out]
+        rhs = sum((g[f] * v[f]).sum() for f in range(3))
+        assert abs(lhs - rhs) <= 1e-11 * scale, (stg is None, lhs, rhs)
+        outs.append(out)
+    for a, b in zip(*outs):
+        assert float((a - b).norm() / b.norm()) < 1e-13
+    gm.close()
+
+
+def test_far_field_rollout_fd_and_refusals(torch_mod, oracle):
+    """4-step rollout with a far-field side (codes 1 and 3) against central differences
+    (h = 1e-5, 1e-6; 1e-6 relative); far-field with a buffer zone and slip walls are refused."""
+    from sod2d_refmap_b200 import _lib, mesh as M, solver as S
+    from sod2d_refmap_b200.adjoint import Sod2dRollout, replay, trajectory_coefficients, _clone_state
+    torch = torch_mod
+    m, prm, st0, ub = channel((1, 3), seed=33)
+    om = oracle.OracleMesh(m)
+    dt = oracle.adapt_dt(om, st0, prm)
+    gm = S.Sod2dMesh(m, prm)
+    gm.set_boundaries(m.extra["bou_codes_nodes"], m.extra["lnbn_nodes"], m.extra["normals"], ub, M.bc_params(prm))
+    s = S.Sod2dState.from_host(st0, gm.nelem)
+    s.dt.fill_(dt)
+    gm.rk_4_main(s, precision=S.FP64, update_dt=True)
+    K = 4
+    rho = s.rho.clone().requires_grad_(True)
+    q = s.q.clone().requires_grad_(True)
+    E = s.E.clone().requires_grad_(True)
+    rK, qK, EK = Sod2dRollout.apply(gm, s, rho, q, E, K, 2)
+    (0.5 * (qK * qK).sum()).backward()
+    rng = np.random.default_rng(37)
+    v = [torch.from_numpy(rng.standard_normal(t.shape)).cuda() * t.abs().mean() for t in (s.rho, s.q, s.E)]
+    dL = float(sum((g * d).sum() for g, d in zip((rho.grad, q.grad, E.grad), v)).item())
+    mus, dts = trajectory_coefficients(gm, s, K)
+
+    def L_at(h):
+        t = _clone_state(s)
+        t.rho.add_(h * v[0]); t.q.add_(h * v[1]); t.E.add_(h * v[2])
+        replay(gm, t, mus, dts)
+        return 0.5 * float((t.q * t.q).sum().item())
+    for h in (1e-5, 1e-6):
+        fd = (L_at(h) - L_at(-h)) / (2 * h)
+        assert abs(fd - dL) <= 1e-6 * abs(dL), (h, fd, dL)
+    # refusals
+    bars = (s.rho.clone(), s.q.clone(), s.E.clone())
+    L = 2.0 * np.pi
+    gm.set_buffer(M.buffer_params(prm, east=(0.8 * L, 0.3 * L)), m.coord, ub)
+    with pytest.raises(_lib.SodError, match="SOD_ERR_UNSUPPORTED"):
+        gm.rk4_step_vjp(s.rho, s.q, s.E, s.mu_e, s.mu_factor, s.dt, *bars)
+    gm.set_buffer(None)
+    m6, prm6, _, ub6 = channel((1, 6), seed=33)
+    gm6 = S.Sod2dMesh(m6, prm6)
+    gm6.set_boundaries(m6.extra["bou_codes_nodes"], m6.extra["lnbn_nodes"], m6.extra["normals"], ub6)
+    with pytest.raises(_lib.SodError, match="SOD_ERR_UNSUPPORTED"):
+        gm6.bc_dirichlet_prim_vjp(s.rho, s.q, s.E, *bars)
+    gm6.close()
+    gm.close()
