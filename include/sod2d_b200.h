@@ -126,7 +126,7 @@ typedef struct {
  * entropy residual (time_integ.f90:256-259,299-301,434-437,474-477).  bou_codes_nodes = null
  * removes the boundaries.  Captured step graphs of the mesh are dropped.  The ensemble
  * (sod_batch_*) rejects meshes with boundaries; sod_rk4_step_vjp differentiates through the
- * routines of codes 1-5 and 8 and rejects meshes holding codes 6 or 7. */
+ * routines of every code. */
 int sod_mesh_set_boundaries(SodMesh* mesh, const int32_t* bou_codes_nodes, const int32_t* lnbn_nodes,
                             const double* normalsAtNodes, const double* u_buffer, const SodBcParams* bc);
 
@@ -166,8 +166,8 @@ int sod_mesh_set_source_term(SodMesh* mesh, const double* source_term);
  * old state.  (rho, q, E) is the state the routine read (used by far-field nodes, whose new
  * state is the HLL state of their lnbn node; may be null without them).  No-slip walls zero the
  * rows they overwrite, outlet / ABL-top nodes pass through.  SOD_ERR_UNSUPPORTED for slip walls
- * (their new state reads the previous stage's velocity) and for a far-field node whose lnbn node
- * lies on a boundary. */
+ * (their new state reads a velocity this entry point is not given; sod_rk4_step_vjp handles
+ * them) and for a far-field node whose lnbn node lies on a boundary. */
 int sod_bc_dirichlet_prim_vjp(SodMesh* mesh, const double* rho, const double* q, const double* E,
                               double* bar_rho, double* bar_q, double* bar_E, sod_stream_t stream);
 
@@ -398,8 +398,11 @@ int sod_rk4_main_record(SodMesh* mesh, SodState* state, const double* dt_dev, do
  * 4 and 5, E) and the outlet / ABL-top codes 2 and 8 leave the node alone, so its adjoint is a
  * constant mask of the wall rows; far-field nodes (code 1) take the HLL state of their lnbn
  * node, whose Jacobian is evaluated at the stage states and at the updated state (one more RHS
- * evaluation at the last stage state).  Codes 6 and 7 (slip walls, which read the previous
- * velocity), and far-field nodes together with a buffer zone, give SOD_ERR_UNSUPPORTED. */
+ * evaluation at the last stage state); slip walls (codes 6, 7) also read a velocity: zero at
+ * stage 1, q/rho of the previous post-routine stage state at stages 2-4, and u(pos) of the input
+ * state at the update, which the map takes as q/rho of (rho, q, E) (its value in every state a
+ * step produces).  Far-field or slip nodes together with a buffer zone give
+ * SOD_ERR_UNSUPPORTED. */
 int sod_rk4_step_vjp(SodMesh* mesh, const double* rho, const double* q, const double* E,
                      const double* mu_e, const double* mu_sgs, const double* mu_factor,
                      const double* dt_dev, const double* stages, const double* bar_rho,

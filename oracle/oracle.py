@@ -106,7 +106,7 @@ def lib():
         L.oracle_compute_field_derivs.argtypes = [C.POINTER(ElemCtx), _p, _p, _p, _p, _p, _p, _p]
         L.oracle_update_buffer.argtypes = [C.c_int, C.POINTER(BufferData), _p, _p, _p]
         L.oracle_bc_dirichlet_prim.argtypes = [C.c_int, C.POINTER(BcData), _p, _p, _p, _p, _p]
-        L.oracle_bc_jvp.argtypes = [C.c_int, C.POINTER(BcData)] + [_p] * 13
+        L.oracle_bc_jvp.argtypes = [C.c_int, C.POINTER(BcData)] + [_p] * 14
         L.oracle_bc_fix_dirichlet_residual.argtypes = [C.c_int, C.POINTER(BcData), _p, _p, _p]
         L.oracle_bc_fix_dirichlet_residual_entropy.argtypes = [C.c_int, C.POINTER(BcData), _p]
         L.oracle_adapt_dt_cfl.argtypes = [C.POINTER(ElemCtx), _p, _p, _p, C.c_double, C.c_double, _p, _p, _p]
@@ -249,14 +249,16 @@ def bc_dirichlet_prim(bnd: Boundaries, rho, q, u, pr, E):
     lib().oracle_bc_dirichlet_prim(len(rho), C.byref(bnd.c), ptr(rho), ptr(q), ptr(u), ptr(pr), ptr(E))
 
 
-def bc_jvp(bnd: Boundaries, rho, q, E, drho, dq, dE, u=None):
-    """The routine's new (rho, q, E) and its tangent along (drho, dq, dE) (dual numbers);
-    u: the aux_u the slip branch reads (zeros when None)."""
+def bc_jvp(bnd: Boundaries, rho, q, E, drho, dq, dE, u=None, du=None):
+    """The routine's new (rho, q, E) and its tangent along (drho, dq, dE, du) (dual numbers);
+    u: the aux_u the slip branch reads (zeros when None), du its tangent (zeros when None)."""
     N = len(rho)
+    z = np.zeros((N, 3), order="F")
     ins = [np.ascontiguousarray(rho, dtype=np.float64), np.asfortranarray(q, dtype=np.float64),
-           np.zeros((N, 3), order="F") if u is None else np.asfortranarray(u, dtype=np.float64),
+           z if u is None else np.asfortranarray(u, dtype=np.float64),
            np.ascontiguousarray(E, dtype=np.float64), np.ascontiguousarray(drho, dtype=np.float64),
-           np.asfortranarray(dq, dtype=np.float64), np.ascontiguousarray(dE, dtype=np.float64)]
+           np.asfortranarray(dq, dtype=np.float64), np.ascontiguousarray(dE, dtype=np.float64),
+           z if du is None else np.asfortranarray(du, dtype=np.float64)]
     outs = [np.zeros(N), np.zeros((N, 3), order="F"), np.zeros(N), np.zeros(N), np.zeros((N, 3), order="F"),
             np.zeros(N)]
     lib().oracle_bc_jvp(N, C.byref(bnd.c), *(ptr(a) for a in ins), *(ptr(a) for a in outs))

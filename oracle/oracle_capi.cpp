@@ -126,15 +126,17 @@ void oracle_bc_dirichlet_prim(int npoin, const BcData* bc, double* rho, double* 
   temporary_bc_routine_dirichlet_prim(npoin, *bc, rho, q, u, pr, E);
 }
 
-// JVP of temporary_bc_routine_dirichlet_prim in (rho, q, E) along (drho, dq, dE); u is the
-// aux_u the slip branch reads (held fixed).  Outputs the new state and its tangent.
+// JVP of temporary_bc_routine_dirichlet_prim in (rho, q, E, u) along (drho, dq, dE, du); u is
+// the aux_u the slip branch reads (du may be null: held fixed).  Outputs the new state and its
+// tangent.
 void oracle_bc_jvp(int npoin, const BcData* bc, const double* rho, const double* q, const double* u,
-                   const double* E, const double* drho, const double* dq, const double* dE, double* rho_out,
-                   double* q_out, double* E_out, double* drho_out, double* dq_out, double* dE_out) {
+                   const double* E, const double* drho, const double* dq, const double* dE, const double* du,
+                   double* rho_out, double* q_out, double* E_out, double* drho_out, double* dq_out,
+                   double* dE_out) {
   const int64_t N = npoin;
   std::vector<Dual> r(N), qq(3 * N), uu(3 * N), pp(N), e(N);
   for (int64_t p = 0; p < N; ++p) { r[p] = Dual(rho[p], drho[p]); e[p] = Dual(E[p], dE[p]); }
-  for (int64_t p = 0; p < 3 * N; ++p) { qq[p] = Dual(q[p], dq[p]); uu[p] = Dual(u[p], 0.0); }
+  for (int64_t p = 0; p < 3 * N; ++p) { qq[p] = Dual(q[p], dq[p]); uu[p] = Dual(u[p], du ? du[p] : 0.0); }
   temporary_bc_routine_dirichlet_prim_t<Dual>(npoin, *bc, r.data(), qq.data(), uu.data(), pp.data(), e.data());
   for (int64_t p = 0; p < N; ++p) {
     rho_out[p] = r[p].v; drho_out[p] = r[p].d; E_out[p] = e[p].v; dE_out[p] = e[p].d;

@@ -146,6 +146,7 @@ class Sod2dRollout:
                 s.rho.copy_(rho_)
                 s.q.copy_(q_)
                 s.E.copy_(E_)
+                s.u.copy_(s.q / s.rho)  # u(pos) of the state (read by slip walls) is q / rho
                 ck = rollout(mesh, s, nsteps, checkpoint_every, precision)
                 ctx.ck = ck
                 ctx.template = state

@@ -620,16 +620,12 @@ int sod_rk4_step_vjp(SodMesh* m, const double* rho, const double* q, const doubl
   SOD_ARG(m && rho && q && E && mu_e && mu_factor && dt_dev, "inputs null");
   SOD_ARG(bar_rho && bar_q && bar_E && out_rho && out_q && out_E, "adjoint arrays null");
   // boundaries and buffer zone: the routines' adjoints after every stage VJP and on the seed
-  // (wall, passive and far-field boundary codes; slip codes are refused)
   const bool has_bc = m->bc.nb > 0, has_zone = m->zone.nb > 0;
   const bool bc = has_bc || has_zone;
   const bool ff = has_bc && m->bc.nff > 0;
-  if (has_bc && m->bc.has_slip) {
-    set_error("sod_rk4_step_vjp: the adjoint of the slip-wall boundary codes is not built");
-    return SOD_ERR_UNSUPPORTED;
-  }
-  if (ff && has_zone) {
-    set_error("sod_rk4_step_vjp: far-field boundaries together with a buffer zone are not differentiated");
+  const bool slip = has_bc && m->bc.has_slip;
+  if ((ff || slip) && has_zone) {
+    set_error("sod_rk4_step_vjp: far-field or slip boundaries together with a buffer zone are not differentiated");
     return SOD_ERR_UNSUPPORTED;
   }
   NvtxRange range("sod rk4 step vjp");
@@ -652,10 +648,11 @@ int sod_rk4_step_vjp(SodMesh* m, const double* rho, const double* q, const doubl
       if (int r = zone_stage(m, ys, st)) return r;
     return has_bc ? bc_stage(m, ys, stage_of, st) : SOD_OK;
   };
-  // y: the state the boundary routine read (its far-field nodes' lnbn rows)
-  auto pre_adjoint = [&](double* vbar, const double* y) -> int {
+  // y: the state the boundary routine read (its far-field nodes' lnbn rows); app: which of the
+  // step's five applications (stages 1-4, the update) for the slip walls
+  auto pre_adjoint = [&](double* vbar, const double* y, int app) -> int {
     if (has_bc)
-      if (int r = bc_adjoint(m, vbar, y, st)) return r;
+      if (int r = bc_adjoint(m, vbar, y, app, st)) return r;
     return has_zone ? zone_adjoint(m, vbar, st) : SOD_OK;
   };
   // scratch: ybar copy | w | (with boundaries: Y1 | Ybar of a stage) | (far-field: the updated
@@ -692,6 +689,10 @@ int sod_rk4_step_vjp(SodMesh* m, const double* rho, const double* q, const doubl
       double* b = m->adj + (base + 5 * t) * N;
       rc = launch_rhs(m, false, epb, cur.c[0], cur.c[1], cur.c[2], cur.c[3], cur.c[4], mu_factor, musgs, st);
       if (rc) return rc;
+      if (slip) {
+        rc = bc_slip_residuals(m, t + 1, rel, st);
+        if (rc) return rc;
+      }
       k_stage_state<<<nblk(N), 256, 0, st>>>(N, m->n2e_ptr, m->n2e, rel, m->Ml, dt_dev, acoef[t], y0, m->source, b);
       SOD_CHECK_LAUNCH();
       if (bc) {
@@ -702,17 +703,36 @@ int sod_rk4_step_vjp(SodMesh* m, const double* rho, const double* q, const doubl
       cur = Cols5{{b, b + N, b + 2 * N, b + 3 * N, b + 4 * N}};
     }
   }
-  if (ff) {
+  if (ff || slip) {
+    const int epb = m->tuned_epb[0] ? m->tuned_epb[0] : 2;
+    if (slip && stages) {
+      // the stage residuals at the slip nodes (the recompute above gathered them already)
+      for (int t = 0; t < 3; ++t) {
+        const double* yt = t == 0 ? y1s : ys[t - 1];
+        rc = launch_rhs(m, false, epb, yt, yt + N, yt + 2 * N, yt + 3 * N, yt + 4 * N, mu_factor, musgs, st);
+        if (rc) return rc;
+        rc = bc_slip_residuals(m, t + 1, rel, st);
+        if (rc) return rc;
+      }
+    }
     // the updated state the final routine reads, at the far-field nodes' lnbn nodes (interior:
     // there the stage states equal their pre-routine values, so dt R_s = (y0 - Y_{s+1}) / a_{s+1}
     // for s = 1..3); R_4 from one more RHS evaluation at Y4
-    const int epb = m->tuned_epb[0] ? m->tuned_epb[0] : 2;
     const double* y4 = ys[2];
     rc = launch_rhs(m, false, epb, y4, y4 + N, y4 + 2 * N, y4 + 3 * N, y4 + 4 * N, mu_factor, musgs, st);
     if (rc) return rc;
-    k_final_pre<<<nblk(N), 256, 0, st>>>(N, m->n2e_ptr, m->n2e, rel, m->Ml, dt_dev, y0, ys[0], ys[1], ys[2],
-                                         m->source, zf);
-    SOD_CHECK_LAUNCH();
+    if (ff) {
+      k_final_pre<<<nblk(N), 256, 0, st>>>(N, m->n2e_ptr, m->n2e, rel, m->Ml, dt_dev, y0, ys[0], ys[1], ys[2],
+                                           m->source, zf);
+      SOD_CHECK_LAUNCH();
+    }
+    if (slip) {
+      // slip walls: pre-routine rho, q of the five applications and the velocities they read
+      rc = bc_slip_residuals(m, 4, rel, st);
+      if (rc) return rc;
+      rc = bc_slip_prepare(m, rho, q, y1s, ys[0], ys[1], dt_dev, st);
+      if (rc) return rc;
+    }
   }
   // reverse sweep: kbar4 = -dt/6 ybar, Ybar4 = J4^T kbar4, kbar3 = -dt (ybar/3 + Ybar4), ...
   // (with boundaries ybar is first mapped through the final routine's adjoint)
@@ -721,7 +741,7 @@ int sod_rk4_step_vjp(SodMesh* m, const double* rho, const double* q, const doubl
   if (bc) {
     for (int f = 0; f < 5; ++f)
       SOD_CUDA(cudaMemcpyAsync(keep.c[f], src.c[f], N * sizeof(double), cudaMemcpyDeviceToDevice, st));
-    rc = pre_adjoint(yb, zf);
+    rc = pre_adjoint(yb, zf, 4);
     if (rc) return rc;
     src = Cols5{{yb, yb + N, yb + 2 * N, yb + 3 * N, yb + 4 * N}};
     keep = MCols5{{nullptr, nullptr, nullptr, nullptr, nullptr}};
@@ -733,6 +753,11 @@ int sod_rk4_step_vjp(SodMesh* m, const double* rho, const double* q, const doubl
   // acc = ybar (copied from the kept columns, so out may alias bar)
   for (int f = 0; f < 5; ++f)
     SOD_CUDA(cudaMemcpyAsync(acc.c[f], keep.c[f], N * sizeof(double), cudaMemcpyDeviceToDevice, st));
+  if (slip) {
+    // the update's slip walls read the velocity q/rho of y0 itself
+    rc = bc_slip_push(m, rho, q, out_rho, out_q, st);
+    if (rc) return rc;
+  }
   const double cb[4] = {1.0 / 3.0, 1.0 / 3.0, 1.0 / 6.0, 0.0};
   const double ca[4] = {1.0, 0.5, 0.5, 0.0};
   for (int stage = 4; stage >= 1; --stage) {
@@ -752,7 +777,13 @@ int sod_rk4_step_vjp(SodMesh* m, const double* rho, const double* q, const doubl
       k_gather_vjp<<<nblk(N), 256, 0, st>>>(N, m->n2e_ptr, m->n2e, rel, yc, 0, nullptr, nullptr, nullptr, 0.0, 0.0,
                                              nullptr);
       SOD_CHECK_LAUNCH();
-      rc = pre_adjoint(Ybs, stage == 1 ? y1s : ys[stage - 2]);
+      const double* Ysv = stage == 1 ? y1s : ys[stage - 2];
+      if (slip && stage < 4) {
+        // stage s + 1's slip walls read the velocity of this stage's post-routine state
+        rc = bc_slip_push(m, Ysv, Ysv + N, Ybs, Ybs + N, st);
+        if (rc) return rc;
+      }
+      rc = pre_adjoint(Ybs, Ysv, stage - 1);
       if (rc) return rc;
       k_accum_seed<<<nblk(N), 256, 0, st>>>(N, Ybs, acc, yb, m->Ml, dt_dev, cb[t], ca[t], stage > 1 ? w : nullptr);
       SOD_CHECK_LAUNCH();
@@ -781,7 +812,7 @@ int sod_bc_dirichlet_prim_vjp(SodMesh* m, const double* rho, const double* q, co
       SOD_CUDA(cudaMemcpyAsync(y + off[t], ys[t], cnt[t] * sizeof(double), cudaMemcpyDeviceToDevice, st));
     }
   }
-  rc = bc_adjoint(m, v, m->bc.nff > 0 ? y : nullptr, st);
+  rc = bc_adjoint(m, v, m->bc.nff > 0 ? y : nullptr, -1, st);
   if (rc) return rc;
   double* outs[3] = {bar_rho, bar_q, bar_E};
   for (int t = 0; t < 3; ++t)

@@ -254,6 +254,137 @@ __global__ void __launch_bounds__(kBlock) k_bc_ff_adjoint(int nb, const int32_t*
   }
 }
 
+// Slip walls: new state (rho_inf, P q, e - rho |uo|^2 / 2 + |P q|^2 / (2 rho_inf)), P = I - n n^T,
+// rho, q, e the node's pre-routine values and uo the velocity it read.  Adjoint of the own
+// node (rows replaced in place) and of uo (left in ubar for the state uo was read from).
+__global__ void __launch_bounds__(kBlock) k_bc_slip_adjoint(int nb, const int32_t* __restrict__ node,
+                                                            const int32_t* __restrict__ code,
+                                                            const double* __restrict__ normal, size_t N,
+                                                            const double* __restrict__ pre,  // [4][nb] rho, q
+                                                            const double* __restrict__ uo,   // [3][nb]
+                                                            double rho_inf, double* __restrict__ vbar,
+                                                            double* __restrict__ ubar) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= nb) return;
+  const int c = code[b];
+  if (c != kSlipAdiabatic && c != kSlipWallModel) return;
+  const size_t n = (size_t)node[b], B = (size_t)nb;
+  const double nv[3] = {normal[b], normal[B + b], normal[2 * B + b]};
+  const double r = pre[b];
+  const double q[3] = {pre[B + b], pre[2 * B + b], pre[3 * B + b]};
+  const double u[3] = {uo[b], uo[B + b], uo[2 * B + b]};
+  const double qn = nv[0] * q[0] + nv[1] * q[1] + nv[2] * q[2];
+  double qp[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) qp[d] = q[d] - qn * nv[d];
+  const double eb = vbar[4 * N + n];
+  double qb[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) qb[d] = vbar[(1 + d) * N + n];
+  const double qbn = nv[0] * qb[0] + nv[1] * qb[1] + nv[2] * qb[2];
+  vbar[n] = -0.5 * (u[0] * u[0] + u[1] * u[1] + u[2] * u[2]) * eb;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) vbar[(1 + d) * N + n] = (qb[d] - qbn * nv[d]) + (qp[d] / rho_inf) * eb;
+  // vbar[4N + n] stays eb
+#pragma unroll
+  for (int d = 0; d < 3; ++d) ubar[(size_t)d * nb + b] = -r * u[d] * eb;
+}
+
+// rho and q residuals (gather / Ml, with the source term on q) of one stage at the slip nodes
+__global__ void __launch_bounds__(kBlock) k_bc_slip_res(int nb, const int32_t* __restrict__ node,
+                                                        const int32_t* __restrict__ code,
+                                                        const int32_t* __restrict__ ptr,
+                                                        const int32_t* __restrict__ idx,
+                                                        const double* __restrict__ el, const double* __restrict__ Ml,
+                                                        const double* __restrict__ src, size_t N,
+                                                        double* __restrict__ res /*[4][nb]*/) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= nb) return;
+  const int c = code[b];
+  if (c != kSlipAdiabatic && c != kSlipWallModel) return;
+  const size_t n = (size_t)node[b];
+  double r[4] = {0.0, 0.0, 0.0, 0.0};
+  const int beg = ptr[n], end = ptr[n + 1];
+  for (int k = beg; k < end; ++k) {
+    const double* v = el + (size_t)idx[k] * NRES;
+#pragma unroll
+    for (int f = 0; f < 4; ++f) r[f] += v[f];
+  }
+  const double ml = Ml[n];
+  if (src) {
+#pragma unroll
+    for (int d = 0; d < 3; ++d) r[1 + d] -= ml * src[d * N + n];
+  }
+#pragma unroll
+  for (int f = 0; f < 4; ++f) res[(size_t)f * nb + b] = r[f] / ml;
+}
+
+// pre-routine rho and q of the five applications (stages 1-4: y0 - a_s dt R_{s-1}; the update:
+// y0 - dt sum_s b_s R_s, accumulated in the forward's order) and the velocity each reads
+// (stage 1: zero; stage s: q/rho of the post-routine stage state s - 1; the update: q/rho of y0)
+__global__ void __launch_bounds__(kBlock) k_bc_slip_prepare(int nb, const int32_t* __restrict__ node,
+                                                            const int32_t* __restrict__ code, size_t N,
+                                                            const double* __restrict__ rho0,
+                                                            const double* __restrict__ q0,
+                                                            const double* __restrict__ Y1,
+                                                            const double* __restrict__ Y2,
+                                                            const double* __restrict__ Y3,
+                                                            const double* __restrict__ dt,
+                                                            const double* __restrict__ res,
+                                                            double* __restrict__ pre, double* __restrict__ uo) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= nb) return;
+  const int c = code[b];
+  if (c != kSlipAdiabatic && c != kSlipWallModel) return;
+  const size_t n = (size_t)node[b], B = (size_t)nb;
+  const double h = *dt;
+  const double a_s[4] = {0.0, 0.5, 0.5, 1.0};
+  const double b_s[4] = {1.0 / 6.0, 1.0 / 3.0, 1.0 / 3.0, 1.0 / 6.0};
+#pragma unroll
+  for (int f = 0; f < 4; ++f) {
+    const double y = f == 0 ? rho0[n] : q0[(f - 1) * N + n];
+    pre[(0 * 4 + f) * B + b] = y;
+    double rs = 0.0;
+#pragma unroll
+    for (int s = 1; s < 4; ++s) pre[((size_t)s * 4 + f) * B + b] = y - h * a_s[s] * res[((size_t)(s - 1) * 4 + f) * B + b];
+#pragma unroll
+    for (int s = 0; s < 4; ++s) rs = rs + b_s[s] * res[((size_t)s * 4 + f) * B + b];
+    pre[((size_t)4 * 4 + f) * B + b] = y - h * rs;
+  }
+  const double* from[4] = {nullptr, Y1, Y2, Y3};
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+      uo[((size_t)a * 3 + d) * B + b] = from[a] ? from[a][(1 + d) * N + n] / from[a][n] : 0.0;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) uo[((size_t)4 * 3 + d) * B + b] = q0[d * N + n] / rho0[n];
+}
+
+// the velocity adjoint ubar of a slip node into the adjoint (vrho, vq) of the state (rho, q) it
+// was read from (uo = q / rho at the node)
+__global__ void __launch_bounds__(kBlock) k_bc_slip_push(int nb, const int32_t* __restrict__ node,
+                                                         const int32_t* __restrict__ code, size_t N,
+                                                         const double* __restrict__ rho,
+                                                         const double* __restrict__ q,
+                                                         const double* __restrict__ ubar, double* __restrict__ vrho,
+                                                         double* __restrict__ vq) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= nb) return;
+  const int c = code[b];
+  if (c != kSlipAdiabatic && c != kSlipWallModel) return;
+  const size_t n = (size_t)node[b], B = (size_t)nb;
+  const double r = rho[n];
+  double s = 0.0;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const double ub = ubar[d * B + b];
+    s += (q[d * N + n] / r) * ub;
+    vq[d * N + n] += ub / r;
+  }
+  vrho[n] -= s / r;
+}
+
 __global__ void k_bc_adjoint_mask(int nb, const int32_t* __restrict__ node, const int32_t* __restrict__ code,
                                   size_t N, double* __restrict__ vbar) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
@@ -392,12 +523,12 @@ static int gather(SodMesh* m, const double* rho, const double* q, const double* 
 
 }  // namespace bcd
 
-// SOD_ERR_UNSUPPORTED for slip walls (their new state reads the velocity of the previous
-// stage) and for far-field nodes whose lnbn node is itself a boundary node
-int bc_adjoint(SodMesh* m, double* vbar, const double* y, cudaStream_t st) {
+// SOD_ERR_UNSUPPORTED for slip walls without the data of a step application (app < 0) and for
+// far-field nodes whose lnbn node is itself a boundary node
+int bc_adjoint(SodMesh* m, double* vbar, const double* y, int app, cudaStream_t st) {
   const BcState& B = m->bc;
-  if (B.has_slip) {
-    set_error("the adjoint of the slip-wall boundary codes is not built");
+  if (B.has_slip && (app < 0 || app > 4)) {
+    set_error("the slip-wall adjoint needs the velocity the routine read (step adjoint only)");
     return SOD_ERR_UNSUPPORTED;
   }
   if (B.nff > 0 && B.ff_nbr_on_boundary) {
@@ -405,6 +536,12 @@ int bc_adjoint(SodMesh* m, double* vbar, const double* y, cudaStream_t st) {
     return SOD_ERR_UNSUPPORTED;
   }
   const size_t N = m->npoin;
+  if (B.has_slip) {
+    bcd::k_bc_slip_adjoint<<<bcd::grid_of(B.nb), bcd::kBlock, 0, st>>>(
+        B.nb, B.node, B.code, B.normal, N, B.sl_pre + (size_t)app * 4 * B.nb, B.sl_uo + (size_t)app * 3 * B.nb,
+        B.prm.rho_inf, vbar, B.sl_ubar);
+    SOD_CHECK_LAUNCH();
+  }
   if (B.nff > 0) {
     SOD_ARG(y, "far-field adjoint needs the state the routine read");
     bcd::k_bc_ff_adjoint<<<bcd::grid_of(B.nb), bcd::kBlock, 0, st>>>(B.nb, B.node, B.code, B.nbr, N, y, vbar,
@@ -421,10 +558,37 @@ int bc_adjoint(SodMesh* m, double* vbar, const double* y, cudaStream_t st) {
   return SOD_OK;
 }
 
+int bc_slip_residuals(SodMesh* m, int stage, const void* rel, cudaStream_t st) {
+  const BcState& B = m->bc;
+  bcd::k_bc_slip_res<<<bcd::grid_of(B.nb), bcd::kBlock, 0, st>>>(
+      B.nb, B.node, B.code, m->n2e_ptr, m->n2e, reinterpret_cast<const double*>(rel), m->Ml, m->source,
+      (size_t)m->npoin, B.sl_res + (size_t)(stage - 1) * 4 * B.nb);
+  SOD_CHECK_LAUNCH();
+  return SOD_OK;
+}
+
+int bc_slip_prepare(SodMesh* m, const double* rho0, const double* q0, const double* Y1, const double* Y2,
+                    const double* Y3, const double* dt_dev, cudaStream_t st) {
+  const BcState& B = m->bc;
+  bcd::k_bc_slip_prepare<<<bcd::grid_of(B.nb), bcd::kBlock, 0, st>>>(B.nb, B.node, B.code, (size_t)m->npoin, rho0,
+                                                                     q0, Y1, Y2, Y3, dt_dev, B.sl_res, B.sl_pre,
+                                                                     B.sl_uo);
+  SOD_CHECK_LAUNCH();
+  return SOD_OK;
+}
+
+int bc_slip_push(SodMesh* m, const double* rho, const double* q, double* vrho, double* vq, cudaStream_t st) {
+  const BcState& B = m->bc;
+  bcd::k_bc_slip_push<<<bcd::grid_of(B.nb), bcd::kBlock, 0, st>>>(B.nb, B.node, B.code, (size_t)m->npoin, rho, q,
+                                                                  B.sl_ubar, vrho, vq);
+  SOD_CHECK_LAUNCH();
+  return SOD_OK;
+}
+
 void bc_free(SodMesh* m) {
   BcState& b = m->bc;
   void* ptrs[] = {b.node, b.code, b.nbr, b.normal, b.ubuf, b.aux2, b.u_stage, b.u_final,
-                  b.ff_ptr, b.ff_target, b.ff_b, b.ff_contrib};
+                  b.ff_ptr, b.ff_target, b.ff_b, b.ff_contrib, b.slip};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   b = BcState{};
@@ -536,6 +700,19 @@ int sod_mesh_set_boundaries(SodMesh* m, const int32_t* codes, const int32_t* lnb
   B.prm = *bc;
   for (int c : code)
     if (c == bcd::kSlipAdiabatic || c == bcd::kSlipWallModel) B.has_slip = true;
+  if (B.has_slip) {
+    const size_t nbs = (size_t)nb;
+    if (!alloc((void**)&B.slip, sizeof(double) * (16 + 20 + 15 + 3) * nbs)) {
+      bc_free(m);
+      set_error("sod_mesh_set_boundaries: device allocation failed");
+      return SOD_ERR_NOMEM;
+    }
+    B.sl_res = B.slip;
+    B.sl_pre = B.sl_res + 16 * nbs;
+    B.sl_uo = B.sl_pre + 20 * nbs;
+    B.sl_ubar = B.sl_uo + 15 * nbs;
+    SOD_CUDA(cudaMemset(B.slip, 0, sizeof(double) * (16 + 20 + 15 + 3) * nbs));
+  }
   // far-field adjoint scatter: lnbn targets in ascending node order, readers in ascending order
   {
     std::vector<std::pair<int32_t, int32_t>> tb;  // (target node, boundary index)

@@ -164,7 +164,13 @@ struct BcState {
   double* aux2 = nullptr;      // [5][nb] state of the lnbn node (rho, q x3, E)
   double* u_stage = nullptr;   // [3][nb] aux_u of the previous stage's EOS
   double* u_final = nullptr;   // [3][nb] u(:,:,pos) at the start of the step
-  bool has_slip = false;       // a slip code (6, 7): reads the previous velocity, no adjoint
+  bool has_slip = false;       // a slip code (6, 7): its new state reads the previous velocity
+  // slip-wall adjoint data per boundary node ([..][nb] columns, one allocation): the stage
+  // residuals of rho and q (sl_res [4 stages][4]), the pre-routine rho and q of the five
+  // applications of a step (sl_pre [5][4]: stages 1-4, then the update), the velocity each one
+  // reads (sl_uo [5][3]) and the adjoint of that velocity (sl_ubar [3])
+  double* slip = nullptr;
+  double *sl_res = nullptr, *sl_pre = nullptr, *sl_uo = nullptr, *sl_ubar = nullptr;
   // far-field nodes (code 1): their lnbn nodes, each with the far-field nodes that read it in
   // ascending order (CSR), for the ordered scatter of the adjoint; the adjoint's per-node
   // contributions [5][nb]
@@ -275,8 +281,18 @@ int bc_snapshot_u(SodMesh* m, const double* u, cudaStream_t st);
 int bc_stage(SodMesh* m, double* ys, int stage, cudaStream_t st);
 int bc_final(SodMesh* m, SodState* s, double* Reta, cudaStream_t st);
 // adjoint of the routine in place on vbar ([5][npoin]); y ([5][npoin]) is the state the routine
-// read (only its far-field nodes' lnbn rows are used; may be null without far-field nodes)
-int bc_adjoint(SodMesh* m, double* vbar, const double* y, cudaStream_t st);
+// read (only its far-field nodes' lnbn rows are used; may be null without far-field nodes);
+// app (0-3: stage 1-4, 4: the update) selects the slip-wall data of that application of the
+// step (-1: none; slip walls are then refused); the adjoint of the velocity a slip wall read is
+// left in bc.sl_ubar
+int bc_adjoint(SodMesh* m, double* vbar, const double* y, int app, cudaStream_t st);
+// slip-wall adjoint helpers (sod_bc.cu): the rho and q residuals of stage s at the slip nodes
+// from the element residuals; the pre-routine states and read velocities of the five
+// applications; the velocity adjoint pushed into the adjoint of the state it was read from
+int bc_slip_residuals(SodMesh* m, int stage, const void* rel, cudaStream_t st);
+int bc_slip_prepare(SodMesh* m, const double* rho0, const double* q0, const double* Y1, const double* Y2,
+                    const double* Y3, const double* dt_dev, cudaStream_t st);
+int bc_slip_push(SodMesh* m, const double* rho, const double* q, double* vrho, double* vq, cudaStream_t st);
 void bc_free(SodMesh* m);
 // entropy normalisation (mean and spread of eta) recomputed into buf.scal after a routine that
 // changed eta

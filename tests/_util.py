@@ -29,10 +29,10 @@ def oracle_bc_map(oracle, bnd):
 
 
 def oracle_bc_jvp_map(oracle, bnd):
-    """(y, v) -> (B(y), J_B(y) v) for the routine in dual numbers (exact for every code that does
-    not read aux_u)."""
-    def J(y, v):
-        return oracle.bc_jvp(bnd, y[0], y[1], y[2], v[0], v[1], v[2])
+    """(y, v, u, du) -> (B(y), J_B v) for the routine in dual numbers, u / du the aux_u the slip
+    branch reads and its tangent."""
+    def J(y, v, u=None, du=None):
+        return oracle.bc_jvp(bnd, y[0], y[1], y[2], v[0], v[1], v[2], u=u, du=du)
     return J
 
 
@@ -40,16 +40,29 @@ def oracle_step_jvp(oracle, om, prm, st, dt, v, mu_sgs=None, bc=None, bc_jvp=Non
     """One rk_4_main step (time_integ.f90:288-426) from the FlowState st and its JVP along
     v = (drho, dq (npoin,3), dE), composed from the oracle's dual-number stage JVPs with mu_e
     (and mu_sgs) frozen.  bc (oracle_bc_map) selects the non-periodic path: the routine on every
-    stage state (time_integ.f90:255-259) and on the update (:434-438); its tangent is B(y + v) - B(y), exact up to rounding for the affine routines of
-    the wall and passive codes."""
+    stage state (time_integ.f90:255-259) and on the update (:434-438), with the tangent
+    B(y + v) - B(y), exact up to rounding for the affine routines of the wall and passive codes;
+    bc_jvp (oracle_bc_jvp_map) takes the routine's tangent from dual numbers instead, with the
+    velocity the slip branch reads carried along."""
     def with_state(rho, q, E):
         s = st.copy()
         s.rho = np.ascontiguousarray(rho); s.q = np.asfortranarray(q); s.E = np.ascontiguousarray(E)
         return s
 
+    # the velocity the slip branch reads: zero at stage 1, then q/rho of the previous post-routine
+    # stage state, and q/rho of y0 for the update (time_integ.f90:208, 266-285)
+    uread = [None, None]
+
+    def vel(y, w):
+        u = np.asfortranarray(y[1] / y[0][:, None])
+        du = np.asfortranarray((w[1] - u * w[0][:, None]) / y[0][:, None])
+        return u, du
+
     def bmap(y, w):
         if bc_jvp is not None:
-            return bc_jvp(tuple(y), tuple(w))
+            out = bc_jvp(tuple(y), tuple(w), uread[0], uread[1])
+            uread[0], uread[1] = vel(*out)
+            return out
         if bc is None:
             return tuple(y), tuple(w)
         by = bc(*y)
@@ -72,5 +85,6 @@ def oracle_step_jvp(oracle, om, prm, st, dt, v, mu_sgs=None, bc=None, bc_jvp=Non
             ys, vs = bmap(tuple(y0[f] - dt * a_next[s] * Rc[f] for f in range(3)),
                           tuple(v[f] - dt * a_next[s] * dRc[f] for f in range(3)))
     if bc is not None or bc_jvp is not None:
+        uread[0], uread[1] = vel(y0, v)
         acc_y, acc_v = (list(t) for t in bmap(acc_y, acc_v))
     return acc_y, acc_v

@@ -137,8 +137,8 @@ def test_channel_dt_graph_mixed(torch_mod, oracle):
 
 
 def test_boundaries_removed_and_adjoint_rejected(torch_mod, oracle):
-    """A slip wall (code 6) makes the routine depend on the old velocity: the step adjoint is
-    refused, the recording step still runs; removing the boundaries gives the periodic step."""
+    """A slip wall (code 6) together with a buffer zone: the step adjoint is refused, the
+    recording step still runs; removing the boundaries gives the periodic step."""
     from sod2d_refmap_b200 import _lib, mesh as M, solver as S
     torch = torch_mod
     m, prm, st0, ub = channel((3, 6), seed=9, n=2)
@@ -150,9 +150,12 @@ def test_boundaries_removed_and_adjoint_rejected(torch_mod, oracle):
     s.dt.fill_(dt)
     stages = torch.zeros(15 * m.npoin, dtype=torch.float64, device="cuda")
     y0 = (s.rho.clone(), s.q.clone(), s.E.clone(), s.mu_e.clone())
+    L = 2.0 * np.pi
+    gm.set_buffer(M.buffer_params(prm, east=(0.8 * L, 0.3 * L)), m.coord, ub)
     gm.rk_4_main_record(s, stages, update_dt=False)
     with pytest.raises(_lib.SodError, match="SOD_ERR_UNSUPPORTED"):
         gm.rk4_step_vjp(*y0, s.mu_factor, s.dt, s.rho, s.q, s.E, stages=stages)
+    gm.set_buffer(None)
     fresh = S.Sod2dState.from_host(st0, gm.nelem)
     for f in S.Sod2dState.FIELDS:
         getattr(s, f).copy_(getattr(fresh, f))
@@ -259,13 +262,15 @@ def test_channel_rollout_gradient_fd(torch_mod, oracle):
     gm.close()
 
 
-@pytest.mark.parametrize("codes", [(1, 3), (3, 1), (1, 1)])
+@pytest.mark.parametrize("codes", [(1, 3), (3, 1), (1, 1), (1, 6), (6, 3), (7, 1)])
 def test_channel_step_vjp_far_field(torch_mod, oracle, codes):
-    """Step adjoint through far-field nodes (the HLL state of the lnbn node): <w, J v> with J v
-    from the oracle's dual-number stage JVPs composed with its boundary routine in dual numbers
-    equals <J^T w, v>, bound 1e-11 relative to sum |w_i (J v)_i|, recorded and recomputed stage
-    states; the routine's own adjoint (sod_bc_dirichlet_prim_vjp) against the oracle's JVP of it
-    (1e-12)."""
+    """Step adjoint through far-field nodes (the HLL state of the lnbn node) and slip walls (which
+    read the velocity of the previous post-routine stage state, and for the update q/rho of the
+    step's own input): <w, J v> with J v from the oracle's dual-number stage JVPs composed with
+    its boundary routine in dual numbers (the read velocity's tangent carried along) equals
+    <J^T w, v>, bound 1e-11 relative to sum |w_i (J v)_i|, recorded and recomputed stage states;
+    without slip walls, the routine's own adjoint (sod_bc_dirichlet_prim_vjp) against the
+    oracle's JVP of it (1e-12)."""
     from _util import oracle_bc_jvp_map, oracle_step_jvp
     from sod2d_refmap_b200 import mesh as M, solver as S
     torch = torch_mod
@@ -280,17 +285,18 @@ def test_channel_step_vjp_far_field(torch_mod, oracle, codes):
     rnd = lambda a: rng.standard_normal(a.shape) * np.abs(a).mean()
     gm = S.Sod2dMesh(m, prm)
     gm.set_boundaries(m.extra["bou_codes_nodes"], m.extra["lnbn_nodes"], m.extra["normals"], ub, bc)
-    # the routine alone
     v = (rnd(st.rho), np.asfortranarray(rnd(st.q)), rnd(st.E))
     w = (rnd(st.rho), np.asfortranarray(rnd(st.q)), rnd(st.E))
-    _, Jv = oracle.bc_jvp(bnd, st.rho, st.q, st.E, *v)
-    bars = [dev(torch, a) for a in w]
-    gm.bc_dirichlet_prim_vjp(dev(torch, st.rho), dev(torch, st.q), dev(torch, st.E), *bars)
-    g = [host(t) for t in bars]
-    terms = [w[f] * Jv[f] for f in range(3)]
-    lhs = sum(t.sum() for t in terms)
-    rhs = sum((g[f] * v[f]).sum() for f in range(3))
-    assert abs(lhs - rhs) <= 1e-12 * sum(np.abs(t).sum() for t in terms), (lhs, rhs)
+    if not {6, 7} & set(codes):
+        # the routine alone
+        _, Jv = oracle.bc_jvp(bnd, st.rho, st.q, st.E, *v)
+        bars = [dev(torch, a) for a in w]
+        gm.bc_dirichlet_prim_vjp(dev(torch, st.rho), dev(torch, st.q), dev(torch, st.E), *bars)
+        g = [host(t) for t in bars]
+        terms = [w[f] * Jv[f] for f in range(3)]
+        lhs = sum(t.sum() for t in terms)
+        rhs = sum((g[f] * v[f]).sum() for f in range(3))
+        assert abs(lhs - rhs) <= 1e-12 * sum(np.abs(t).sum() for t in terms), (lhs, rhs)
     # one step
     y1, dy1 = oracle_step_jvp(oracle, om, prm, st, dt, v, bc_jvp=oracle_bc_jvp_map(oracle, bnd))
     s = S.Sod2dState.from_host(st, gm.nelem)
@@ -316,13 +322,16 @@ def test_channel_step_vjp_far_field(torch_mod, oracle, codes):
     gm.close()
 
 
-def test_far_field_rollout_fd_and_refusals(torch_mod, oracle):
-    """4-step rollout with a far-field side (codes 1 and 3) against central differences
-    (h = 1e-5, 1e-6; 1e-6 relative); far-field with a buffer zone and slip walls are refused."""
+@pytest.mark.parametrize("codes", [(1, 3), (6, 1)])
+def test_far_field_rollout_fd_and_refusals(torch_mod, oracle, codes):
+    """4-step rollouts with a far-field side (codes 1 and 3) and with a slip wall and a far-field
+    side (6 and 1) against central differences of the frozen-coefficient map with u = q/rho in
+    the perturbed initial state (h = 1e-5, 1e-6; 1e-6 relative); far-field with a buffer zone,
+    and the standalone routine adjoint with slip walls, are refused."""
     from sod2d_refmap_b200 import _lib, mesh as M, solver as S
     from sod2d_refmap_b200.adjoint import Sod2dRollout, replay, trajectory_coefficients, _clone_state
     torch = torch_mod
-    m, prm, st0, ub = channel((1, 3), seed=33)
+    m, prm, st0, ub = channel(codes, seed=33)
     om = oracle.OracleMesh(m)
     dt = oracle.adapt_dt(om, st0, prm)
     gm = S.Sod2dMesh(m, prm)
@@ -344,6 +353,7 @@ def test_far_field_rollout_fd_and_refusals(torch_mod, oracle):
     def L_at(h):
         t = _clone_state(s)
         t.rho.add_(h * v[0]); t.q.add_(h * v[1]); t.E.add_(h * v[2])
+        t.u.copy_(t.q / t.rho)
         replay(gm, t, mus, dts)
         return 0.5 * float((t.q * t.q).sum().item())
     for h in (1e-5, 1e-6):
