@@ -306,14 +306,14 @@ def bench_adjoint(n: int, steps: int, every: int):
     v = [torch.randn(x.shape, dtype=torch.float64, device="cuda", generator=g) * x.abs().mean()
          for x in (s.rho, s.q, s.E)]
 
-    def run(K, prec):
+    def run(K, prec, keep=False):
         rho = s.rho.clone().requires_grad_(True)
         q = s.q.clone().requires_grad_(True)
         E = s.E.clone().requires_grad_(True)
         ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
         torch.cuda.synchronize()
         ev[0].record()
-        _, qK, _ = Sod2dRollout.apply(gm, s, rho, q, E, K, every, True, prec)
+        _, qK, _ = Sod2dRollout.apply(gm, s, rho, q, E, K, every, True, prec, keep)
         loss = 0.5 * (qK * qK).sum()
         ev[1].record()
         loss.backward()
@@ -325,9 +325,13 @@ def bench_adjoint(n: int, steps: int, every: int):
     dls = {}
     for prec, name in ((S.FP64, "fp64"), (S.MIXED, "mixed")):
         run(2, prec)  # warm-up
+        run(2, prec, True)
         grads, loss, t_fwd, t_bwd = run(steps, prec)
+        # the forward keeps every step's stage states in HBM: the backward is the VJPs alone
+        grads_k, _, t_fwd_k, t_bwd_k = run(steps, prec, True)
+        keep_equal = all(bool(torch.equal(a, b)) for a, b in zip(grads, grads_k))
         t = _clone_state(s)
-        gm.rk4_steps(t, 1, precision=prec)
+        gm.rk4_steps(t, steps, precision=prec)  # captures the graph of this step count
         t = _clone_state(s)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         torch.cuda.synchronize()
@@ -350,9 +354,14 @@ def bench_adjoint(n: int, steps: int, every: int):
             d = (L_at(h) - L_at(-h)) / (2 * h)
             fd[f"{h:g}"] = {"fd": d, "rel_err": abs(d - dL) / abs(dL)}
         out[name] = {"loss": loss, "directional_derivative": dL, "finite_differences": fd,
-                     "ms": {"forward_with_checkpoints": t_fwd, "backward": t_bwd, "forward_plain_graph": t_graph},
+                     "ms": {"forward_with_checkpoints": t_fwd, "backward": t_bwd, "forward_plain_graph": t_graph,
+                            "forward_keeping_trajectory": t_fwd_k, "backward_from_kept_trajectory": t_bwd_k},
                      "adjoint_over_forward": {"backward/forward_with_checkpoints": t_bwd / t_fwd,
-                                              "backward/forward_plain_graph": t_bwd / t_graph}}
+                                              "backward/forward_plain_graph": t_bwd / t_graph,
+                                              "kept_trajectory_backward/forward": t_bwd_k / t_fwd_k,
+                                              "kept_trajectory_backward/forward_plain_graph": t_bwd_k / t_graph},
+                     "kept_trajectory_gradient_bitwise_equal": keep_equal,
+                     "kept_trajectory_bytes": steps * (20 * m.npoin + 64 * m.nelem) * 8}
     out["mixed"]["directional_derivative_rel_diff_vs_fp64"] = abs(dls["mixed"] - dls["fp64"]) / abs(dls["fp64"])
     out["note"] = ("step VJPs are FP64 in both; the mixed row differentiates the FP64 map along the mixed "
                    "trajectory, and FP32 rounding noise of the mixed map limits its finite differences")

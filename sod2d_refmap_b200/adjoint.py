@@ -10,7 +10,10 @@ and finite-difference checks compare against.
 
 Memory: states (rho, q, E, mu_e, dt) are kept every ``checkpoint_every`` steps; the backward
 pass re-runs each segment from its checkpoint (bitwise identical, the solver is deterministic)
-and applies the hand-written step VJP (sod_rk4_step_vjp) in reverse.
+and applies the hand-written step VJP (sod_rk4_step_vjp) in reverse.  With
+``keep_trajectory=True`` the forward pass instead keeps every step's state and its three RK
+stage states (22.4 doubles per node and step: 160 MB per step at 32^3, 1.3 GB at 64^3, so
+tens of steps fit in the GPU's HBM) and the backward pass is the step VJPs alone.
 
 Precision: the trajectory (forward and re-run) can be the FP64 or the mixed path; the step
 VJPs are always the FP64 Jacobian-transpose evaluated at the stored stage states.  For the
@@ -62,15 +65,20 @@ def _load(s: Sod2dState, c: _Ckpt):
         s.mu_sgs.copy_(c.mu_sgs)
 
 
-def rollout(mesh: Sod2dMesh, state: Sod2dState, nsteps: int, checkpoint_every: int = 10, precision: int = FP64):
+def rollout(mesh: Sod2dMesh, state: Sod2dState, nsteps: int, checkpoint_every: int = 10, precision: int = FP64,
+            stages=None):
     """Run nsteps steps in place (dt from the CFL condition after every step, as rk_4_main)
-    and return the checkpoints [(step index, _Ckpt)] at multiples of checkpoint_every."""
+    and return the checkpoints [(step index, _Ckpt)] at multiples of checkpoint_every.  With
+    stages (nsteps, 15*npoin) every step is a checkpoint and records its stage states there."""
     ck = []
     les = _les(mesh)
     for n in range(nsteps):
-        if n % checkpoint_every == 0:
+        if stages is not None or n % checkpoint_every == 0:
             ck.append((n, _ckpt(state, les)))
-        mesh.rk_4_main(state, precision, update_dt=True)
+        if stages is not None:
+            mesh.rk_4_main_record(state, stages[n], update_dt=True, precision=precision)
+        else:
+            mesh.rk_4_main(state, precision, update_dt=True)
     return ck
 
 
@@ -101,11 +109,18 @@ def trajectory_coefficients(mesh: Sod2dMesh, state: Sod2dState, nsteps: int, pre
 
 
 def backward_through(mesh: Sod2dMesh, template: Sod2dState, ckpts, nsteps: int, bar_rho, bar_q, bar_E,
-                     store_stages: bool = True, precision: int = FP64):
+                     store_stages: bool = True, precision: int = FP64, trajectory=None):
     """Adjoint of nsteps steps: (bar_rho, bar_q, bar_E) at step nsteps -> at step 0, in place.
     Each segment is re-run from its checkpoint; with store_stages the re-run keeps the RK stage
-    states (15*npoin doubles per step) so that the step VJPs need no second recompute."""
+    states (15*npoin doubles per step) so that the step VJPs need no second recompute.  With
+    trajectory (the forward's per-step stage states, every step a checkpoint) nothing is re-run."""
     torch = _torch()
+    if trajectory is not None:
+        for t in range(nsteps - 1, -1, -1):
+            cs = ckpts[t][1]
+            mesh.rk4_step_vjp(cs.rho, cs.q, cs.E, cs.mu_e, template.mu_factor, cs.dt, bar_rho, bar_q, bar_E,
+                              out=(bar_rho, bar_q, bar_E), stages=trajectory[t], mu_sgs=cs.mu_sgs)
+        return bar_rho, bar_q, bar_E
     s = _clone_state(template)
     bounds = [c[0] for c in ckpts] + [nsteps]
     longest = max(bounds[i + 1] - bounds[i] for i in range(len(ckpts)))
@@ -132,11 +147,13 @@ def backward_through(mesh: Sod2dMesh, template: Sod2dState, ckpts, nsteps: int, 
 
 class Sod2dRollout:
     """``Sod2dRollout.apply(mesh, state, rho, q, E, nsteps, checkpoint_every)`` -> (rho_K, q_K, E_K)
-    as a differentiable torch function of the initial conserved fields (rho, q, E)."""
+    as a differentiable torch function of the initial conserved fields (rho, q, E).
+    keep_trajectory: keep every step's stage states from the forward pass (no re-run in the
+    backward pass; checkpoint_every and store_stages are then unused)."""
 
     @staticmethod
     def apply(mesh: Sod2dMesh, state: Sod2dState, rho, q, E, nsteps: int, checkpoint_every: int = 10,
-              store_stages: bool = True, precision: int = FP64):
+              store_stages: bool = True, precision: int = FP64, keep_trajectory: bool = False):
         torch = _torch()
 
         class _Fn(torch.autograd.Function):
@@ -147,8 +164,11 @@ class Sod2dRollout:
                 s.q.copy_(q_)
                 s.E.copy_(E_)
                 s.u.copy_(s.q / s.rho)  # u(pos) of the state (read by slip walls) is q / rho
-                ck = rollout(mesh, s, nsteps, checkpoint_every, precision)
+                traj = (torch.empty(nsteps, 15 * s.npoin, dtype=torch.float64, device="cuda")
+                        if keep_trajectory else None)
+                ck = rollout(mesh, s, nsteps, checkpoint_every, precision, stages=traj)
                 ctx.ck = ck
+                ctx.traj = traj
                 ctx.template = state
                 return s.rho.clone(), s.q.clone(), s.E.clone()
 
@@ -156,7 +176,9 @@ class Sod2dRollout:
             def backward(ctx, g_rho, g_q, g_E):
                 z = lambda g, like: torch.zeros_like(like) if g is None else g.contiguous().clone()
                 br, bq, bE = z(g_rho, rho), z(g_q, q), z(g_E, E)
-                backward_through(mesh, ctx.template, ctx.ck, nsteps, br, bq, bE, store_stages, precision)
+                backward_through(mesh, ctx.template, ctx.ck, nsteps, br, bq, bE, store_stages, precision,
+                                 trajectory=ctx.traj)
+                ctx.traj = None
                 return br, bq, bE
 
         return _Fn.apply(rho, q, E)

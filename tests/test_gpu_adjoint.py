@@ -257,17 +257,19 @@ def test_stored_stages_match_recompute(env):
 
 
 def test_rollout_checkpoint_spacing_invariant(env):
-    """The gradient does not depend on the checkpoint spacing nor on stored vs recomputed
-    stage states (bitwise: the re-forward is deterministic)."""
+    """The gradient does not depend on the checkpoint spacing, on stored vs recomputed stage
+    states, nor on keeping the forward's trajectory (bitwise: the re-forward is
+    deterministic)."""
     from sod2d_refmap_b200.adjoint import Sod2dRollout
-    torch, gm = env["torch"], env["gm"]
+    torch, gm, S = env["torch"], env["gm"], env["S"]
     grads = []
-    for every, store in ((1, True), (2, True), (5, True), (2, False)):
+    for every, store, keep in ((1, True, False), (2, True, False), (5, True, False), (2, False, False),
+                               (2, True, True)):
         s = _rollout_env(env, 5)
         rho = s.rho.clone().requires_grad_(True)
         q = s.q.clone().requires_grad_(True)
         E = s.E.clone().requires_grad_(True)
-        _, qK, _ = Sod2dRollout.apply(gm, s, rho, q, E, 5, every, store)
+        _, qK, _ = Sod2dRollout.apply(gm, s, rho, q, E, 5, every, store, S.FP64, keep)
         (0.5 * (qK * qK).sum()).backward()
         grads.append((rho.grad.clone(), q.grad.clone(), E.grad.clone()))
     for other in grads[1:]:
