@@ -171,6 +171,27 @@ int sod_mesh_set_source_term(SodMesh* mesh, const double* source_term);
 int sod_bc_dirichlet_prim_vjp(SodMesh* mesh, const double* rho, const double* q, const double* E,
                               double* bar_rho, double* bar_q, double* bar_E, sod_stream_t stream);
 
+/* Wall model of rk_4_main (isWallModelOn, time_integ.f90:334-357): type 1 Reichardt
+ * (evalWallModelReichardt, mod_wall_model.f90:12-175), 2 ABL (evalWallModelABL, :177-300; needs
+ * walave_u, as the reference, and zo).  Host arrays in the reference layouts and the mesh's
+ * index_base: bound (nboun,npbou=16), bounorm (nboun,3*npbou), wgp_b (npbou), listBoundsWM
+ * (numBoundsWM faces), point2elem (npoin), coord (npoin,3), normalsAtNodes (npoin,3), zo (npoin)
+ * or null; walave_u: a device (npoin,3) array the mesh keeps a pointer to (flag_walave), or null
+ * for the stage velocity.  Each stage then adds the modelled wall shear to the momentum
+ * residual of the wall nodes.  numBoundsWM = 0 removes the model.  The step adjoint and the
+ * ensemble reject meshes with a wall model. */
+int sod_mesh_set_wall_model(SodMesh* mesh, int32_t type, int32_t nboun, int32_t npbou, const int32_t* bound,
+                            const double* bounorm, const double* wgp_b, int32_t numBoundsWM,
+                            const int32_t* listBoundsWM, const int32_t* point2elem, const double* coord,
+                            const double* normalsAtNodes, const double* zo, const double* walave_u);
+/* The registered wall model as the reference routine: Rdiff (npoin,3) += the wall shear terms from
+ * device rho (npoin), u (npoin,3) (the exchange velocity: aux_u or walave_u) and mu_fluid
+ * (npoin); tauw (npoin,3) receives tmag * tvelo, or may be null. */
+int sod_wall_model(SodMesh* mesh, const double* rho, const double* u, const double* mu_fluid, double* Rdiff,
+                   double* tauw, sod_stream_t stream);
+/* tauw of the last stage the step evaluated the wall model on (device (npoin,3)). */
+int sod_wall_model_tauw(SodMesh* mesh, double* tauw, sod_stream_t stream);
+
 /* Device-resident solver state in the reference's array layouts (level pos=2 only).
  * Every pointer is a device pointer owned by the caller. */
 typedef struct {

@@ -46,6 +46,33 @@ class BcData(C.Structure):
         [(n, C.c_double) for n in ("rho_inf", "u_inf", "p_inf", "c_inf", "gamma_inf", "Rgas_inf", "T_H", "T_C")]
 
 
+class WallModelData(C.Structure):
+    _fields_ = [("type", C.c_int), ("nboun", C.c_int), ("npbou", C.c_int), ("numBoundsWM", C.c_int)] + \
+        [(n, _p) for n in ("bound", "bounorm", "wgp_b", "listBoundsWM", "point2elem", "coord", "normals", "zo",
+                           "walave", "tauw")]
+
+
+class WallModel:
+    """Wall-model data for the oracle (0-based ids; arrays kept alive here); tauw receives the
+    wall shear of the last evaluation."""
+
+    def __init__(self, wtype, bound, bounorm, wgp_b, list_wm, point2elem, coord, normals, zo=None, walave=None):
+        self.bound = np.asfortranarray(bound, dtype=np.int32)
+        self.bounorm = np.asfortranarray(bounorm, dtype=np.float64)
+        self.wgp_b = np.ascontiguousarray(wgp_b, dtype=np.float64)
+        self.list_wm = np.ascontiguousarray(list_wm, dtype=np.int32)
+        self.point2elem = np.ascontiguousarray(point2elem, dtype=np.int32)
+        self.coord = np.asfortranarray(coord, dtype=np.float64)
+        self.normals = np.asfortranarray(normals, dtype=np.float64)
+        self.zo = None if zo is None else np.ascontiguousarray(zo, dtype=np.float64)
+        self.walave = None if walave is None else np.asfortranarray(walave, dtype=np.float64)
+        self.tauw = np.zeros((len(self.point2elem), 3), order="F")
+        pz = lambda a: ptr(a).value if a is not None else None
+        self.c = WallModelData(int(wtype), self.bound.shape[0], self.bound.shape[1], len(self.list_wm),
+                               pz(self.bound), pz(self.bounorm), pz(self.wgp_b), pz(self.list_wm), pz(self.point2elem),
+                               pz(self.coord), pz(self.normals), pz(self.zo), pz(self.walave), pz(self.tauw))
+
+
 class BufferData(C.Structure):
     _fields_ = [("coord", _p), ("u_buffer", _p), ("on", C.c_int32 * 6), ("mn", C.c_double * 6),
                 ("sz", C.c_double * 6)] + [(n, C.c_double) for n in ("rho_inf", "u_inf", "p_inf", "gamma_inf")]
@@ -102,7 +129,8 @@ def lib():
         L.oracle_conjgrad_pressure.restype = C.c_int
         L.oracle_rk_4_main.argtypes = [C.POINTER(ElemCtx), C.POINTER(Params), _p, _p, _p, _p, _p, _p,
                                        C.c_double, C.c_int, C.POINTER(State), C.POINTER(StageCapture),
-                                       C.POINTER(BcData), C.POINTER(BufferData), _p]
+                                       C.POINTER(BcData), C.POINTER(BufferData), _p, C.POINTER(WallModelData)]
+        L.oracle_wall_model.argtypes = [C.POINTER(ElemCtx), C.POINTER(WallModelData), _p, _p, _p, _p]
         L.oracle_compute_field_derivs.argtypes = [C.POINTER(ElemCtx), _p, _p, _p, _p, _p, _p, _p]
         L.oracle_update_buffer.argtypes = [C.c_int, C.POINTER(BufferData), _p, _p, _p]
         L.oracle_bc_dirichlet_prim.argtypes = [C.c_int, C.POINTER(BcData), _p, _p, _p, _p, _p]
@@ -198,7 +226,8 @@ def adapt_dt(om: OracleMesh, st, prm) -> float:
 
 
 def rk4(om: OracleMesh, prm, st, dt: float, nsteps: int = 1, capture_stage: int = 0,
-        bnd: "Boundaries | None" = None, buf: "BufferZone | None" = None, source=None):
+        bnd: "Boundaries | None" = None, buf: "BufferZone | None" = None, source=None,
+        wall: "WallModel | None" = None):
     """Runs nsteps rk_4_main steps in place on st (a FlowState).  Returns the stage residuals of
     capture_stage (1..4) of the first step when requested.  bnd selects the non-periodic path,
     buf the buffer zone (flag_buffer_on), source (npoin,3) the constant momentum source term."""
@@ -217,8 +246,14 @@ def rk4(om: OracleMesh, prm, st, dt: float, nsteps: int = 1, capture_stage: int 
     lib().oracle_rk_4_main(C.byref(om.ctx), C.byref(P), ptr(om.Ml), ptr(st.mu_factor), ptr(om.gpvol), ptr(om.wgp),
                            ptr(om.helem), ptr(om.helem_l), float(dt), int(nsteps), C.byref(S),
                            C.byref(cap) if cap is not None else None, C.byref(bnd.c) if bnd is not None else None,
-                           C.byref(buf.c) if buf is not None else None, ptr(src) if src is not None else None)
+                           C.byref(buf.c) if buf is not None else None, ptr(src) if src is not None else None,
+                           C.byref(wall.c) if wall is not None else None)
     return out
+
+
+def wall_model(om: OracleMesh, wall: WallModel, rho, ui, mu_fluid, Rdiff):
+    """evalWallModel* in place on Rdiff (npoin,3) Fortran order; wall.tauw receives tauw."""
+    lib().oracle_wall_model(C.byref(om.ctx), C.byref(wall.c), ptr(rho), ptr(ui), ptr(mu_fluid), ptr(Rdiff))
 
 
 def levi_civita() -> np.ndarray:

@@ -105,11 +105,16 @@ double oracle_adapt_dt_cfl(const ElemCtx* ctx, const double* helem, const double
 void oracle_rk_4_main(const ElemCtx* ctx, const Params* P, const double* Ml, const double* mu_factor,
                       const double* gpvol, const double* wgp, const double* helem, const double* helem_l,
                       double dt, int nsteps, State* S, StageCapture* capture, const BcData* bc,
-                      const BufferData* buf, const double* source) {
+                      const BufferData* buf, const double* source, const WallModelData* wmd) {
   Rk4Scratch W(ctx->npoin);
   for (int s = 0; s < nsteps; ++s)
     rk_4_main(*ctx, *P, Ml, mu_factor, gpvol, wgp, helem, helem_l, dt, *S, W, s == 0 ? capture : nullptr, bc, buf,
-              source);
+              source, wmd);
+}
+
+void oracle_wall_model(const ElemCtx* ctx, const WallModelData* wmd, const double* rho, const double* ui,
+                       const double* mu_fluid, double* Rdiff) {
+  eval_wall_model(*ctx, *wmd, rho, ui, mu_fluid, Rdiff);
 }
 
 void oracle_compute_field_derivs(const ElemCtx* ctx, const double* levi, const double* rho, const double* u,

@@ -1415,6 +1415,111 @@ struct BcData {
   double rho_inf, u_inf, p_inf, c_inf, gamma_inf, Rgas_inf, T_H, T_C;  // nscbc_* values
 };
 
+// Wall model data (isWallModelOn): reference arrays with 0-based ids; type 1 Reichardt, 2 ABL;
+// walave (npoin,3) replaces the stage velocity when set (flag_walave).
+struct WallModelData {
+  int type, nboun, npbou, numBoundsWM;
+  const int32_t* bound;         // (nboun,npbou)
+  const double* bounorm;        // (nboun,3*npbou)
+  const double* wgp_b;          // (npbou)
+  const int32_t* listBoundsWM;  // (numBoundsWM)
+  const int32_t* point2elem;    // (npoin)
+  const double* coord;          // (npoin,3)
+  const double* normals;        // (npoin,3)
+  const double* zo;             // (npoin) or null
+  const double* walave;         // (npoin,3) or null
+  double* tauw;                 // (npoin,3) output or null
+};
+
+// evalWallModelReichardt / evalWallModelABL (mod_wall_model.f90:12-300): per wall-model face,
+// the element of an interior face node and the face's normal iso direction; per face node the
+// exchange node on the element's opposite face, the tangential velocity there, the law's wall
+// shear and Rdiff(node) += |bounorm| wgp_b tmag tvelo (the reference's atomics, in face order),
+// tauw(node) = tmag tvelo (the last face wins).
+inline void eval_wall_model(const ElemCtx& ctx, const WallModelData& W, const double* rho, const double* ui,
+                            const double* mu_fluid, double* Rdiff) {
+  const int64_t N = ctx.npoin, NB = W.nboun;
+  const int nelem = ctx.nelem;
+  auto local_of = [&](int e, int64_t node) {
+    for (int a = 0; a < nnode; ++a)
+      if (ctx.connec[e + (int64_t)nelem * a] == node) return a;
+    return -1;
+  };
+  for (int f = 0; f < W.numBoundsWM; ++f) {
+    const int64_t ib = W.listBoundsWM[f];
+    int iElem = -1, type_ijk = -1, isoF = -1;
+    for (int a = 0; a < W.npbou && iElem < 0; ++a) {  // an interior face node (reference: atoIJ(npbou))
+      const int64_t nd = W.bound[ib + NB * a];
+      const int e = W.point2elem[nd];
+      const int jg = local_of(e, nd);
+      const int iso[3] = {ctx.gmshAtoI[jg], ctx.gmshAtoJ[jg], ctx.gmshAtoK[jg]};
+      int nend = 0, dd = -1;
+      for (int r = 0; r < 3; ++r)
+        if (iso[r] <= 1) { ++nend; dd = r; }
+      if (nend == 1) { iElem = e; type_ijk = dd; isoF = iso[dd] == 0 ? 1 : 0; }
+    }
+    for (int a = 0; a < W.npbou; ++a) {
+      const int64_t nd = W.bound[ib + NB * a];
+      const int jg = local_of(iElem, nd);
+      int iso[3] = {ctx.gmshAtoI[jg], ctx.gmshAtoJ[jg], ctx.gmshAtoK[jg]};
+      iso[type_ijk] = isoF;
+      const int64_t x = ctx.connec[iElem + (int64_t)nelem * SOD_INV(iso[0], iso[1], iso[2])];
+      double uiex[3], point[3], pointF[3], normalF[3];
+      for (int d = 0; d < 3; ++d) {
+        point[d] = W.coord[x + N * d];
+        uiex[d] = ui[x + N * d];
+        pointF[d] = W.coord[nd + N * d];
+        normalF[d] = W.normals[nd + N * d];
+      }
+      const double rhol = rho[nd], nul = mu_fluid[nd] / rhol;
+      const double y = std::fabs(normalF[0] * (point[0] - pointF[0]) + normalF[1] * (point[1] - pointF[1]) +
+                                 normalF[2] * (point[2] - pointF[2]));
+      const double auxvn = normalF[0] * uiex[0] + normalF[1] * uiex[1] + normalF[2] * uiex[2];
+      double tvelo[3];
+      for (int d = 0; d < 3; ++d) tvelo[d] = uiex[d] - auxvn * normalF[d];
+      const double ul = std::sqrt(tvelo[0] * tvelo[0] + tvelo[1] * tvelo[1] + tvelo[2] * tvelo[2]);
+      double tmag;
+      if (W.type == 2) {
+        const double uistar = ul * 0.41 / std::log(1.0 + y / W.zo[nd]);
+        tmag = rhol * uistar * uistar / ul;
+      } else {
+        double uistar;
+        if (y > 0.0 && ul > 1.0e-10) {
+          uistar = std::sqrt(ul * nul / y);
+          if (uistar * y / nul > 5.0) {
+            const double vkinv = 1.0 / 0.41, onovu = 1.0 / ul, xmuit = y / nul, oneoe = 1.0 / 11.0;
+            int itera = 0;
+            double parco = 1.0;
+            while (parco >= 1.0e-6 && itera < 100) {
+              itera = itera + 1;
+              uistar = std::max(uistar, 0.0);
+              const double yplus = uistar * xmuit, ypele = yplus * oneoe, ypel2 = std::min(ypele, 20.0);
+              const double expye = std::exp(-ypel2), yplu2 = std::min(yplus, 70.0);
+              const double expyt = std::exp(-yplu2 * 0.33), firsl = vkinv * std::log(1.0 + 0.4 * yplus);
+              const double fdvfr = uistar * (firsl + 7.8 * (1.0 - expye - ypele * expyt)) - ul;
+              const double diffd = firsl + vkinv * 0.4 * yplus / (1.0 + 0.4 * yplus) +
+                                   7.8 * (1.0 - expye * (1.0 - ypele) - ypele * expyt * (2.0 - yplus * 0.33));
+              const double devfr = -fdvfr / diffd;
+              parco = std::fabs(devfr * onovu);
+              uistar = uistar + devfr;
+            }
+          }
+        } else {
+          uistar = 0.0;
+        }
+        tmag = (y * uistar / nul < 5.0) ? rhol * nul / y : rhol * uistar * uistar / ul;
+      }
+      double am = 0.0;
+      for (int d = 0; d < 3; ++d) am += W.bounorm[ib + NB * (3 * a + d)] * W.bounorm[ib + NB * (3 * a + d)];
+      am = std::sqrt(am);
+      for (int d = 0; d < 3; ++d) {
+        Rdiff[nd + N * d] = Rdiff[nd + N * d] + am * W.wgp_b[a] * tmag * tvelo[d];
+        if (W.tauw) W.tauw[nd + N * d] = tmag * tvelo[d];
+      }
+    }
+  }
+}
+
 // mom_source_const_vect (elem_source.f90:20-55): Rmom(node) -= gpvol(a, e) s(node) over every
 // element node, in element order (the reference's atomics)
 inline void mom_source_const_vect(const ElemCtx& ctx, const double* s, double* Rmom) {
@@ -1578,7 +1683,8 @@ inline void bc_fix_dirichlet_residual_entropy(int npoin, const BcData& B, double
 inline void rk_4_main(const ElemCtx& ctx, const Params& P, const double* Ml, const double* mu_factor,
                       const double* gpvol, const double* wgp, const double* helem, const double* helem_l,
                       double dt, State& S, Rk4Scratch& W, StageCapture* cap, const BcData* bc = nullptr,
-                      const BufferData* buf = nullptr, const double* source = nullptr) {
+                      const BufferData* buf = nullptr, const double* source = nullptr,
+                      const WallModelData* wmd = nullptr) {
   const int npoin = ctx.npoin;
   const int64_t n3 = (int64_t)npoin * 3;
   const double a_i[4] = {0.0, 0.5, 0.5, 1.0};
@@ -1629,6 +1735,9 @@ inline void rk_4_main(const ElemCtx& ctx, const Params& P, const double* Ml, con
                        S.mu_fluid, S.mu_e, S.mu_sgs, W.Rdiff_mass.data(), W.Rdiff_mom.data(),
                        W.Rdiff_ener.data());
     if (source) mom_source_const_vect(ctx, source, W.Rdiff_mom.data());  // time_integ.f90:326-330
+    if (wmd)  // time_integ.f90:334-357
+      eval_wall_model(ctx, *wmd, W.aux_rho.data(), wmd->walave ? wmd->walave : W.aux_u.data(), S.mu_fluid,
+                      W.Rdiff_mom.data());
     if (P.flag_total_enthalpy)  // time_integ.f90:361-365
       full_convec_ijk_H(ctx, W.aux_u.data(), W.aux_q.data(), W.aux_rho.data(), W.aux_pr.data(), W.aux_E.data(),
                         W.Rmass.data(), W.Rmom.data(), W.Rener.data());

@@ -90,6 +90,9 @@ _SIGS = {
     "sod_set_rhs_config": (_i, [_p, _i, _i]),
     "sod_compute_field_derivs": (_i, [_p] * 9),
     "sod_bc_dirichlet_prim_vjp": (_i, [_p] * 8),
+    "sod_mesh_set_wall_model": (_i, [_p, _i, _i, _i, _p, _p, _p, _i, _p, _p, _p, _p, _p, _p]),
+    "sod_wall_model": (_i, [_p] * 7),
+    "sod_wall_model_tauw": (_i, [_p] * 3),
     "sod_mesh_set_source_term": (_i, [_p] * 2),
     "sod_update_buffer": (_i, [_p] * 5),
     "sod_bc_dirichlet_prim": (_i, [_p] * 7),

@@ -624,6 +624,10 @@ int sod_rk4_step_vjp(SodMesh* m, const double* rho, const double* q, const doubl
   const bool bc = has_bc || has_zone;
   const bool ff = has_bc && m->bc.nff > 0;
   const bool slip = has_bc && m->bc.has_slip;
+  if (m->wmodel.nw > 0) {
+    set_error("sod_rk4_step_vjp: the wall model is not differentiated");
+    return SOD_ERR_UNSUPPORTED;
+  }
   if ((ff || slip) && has_zone) {
     set_error("sod_rk4_step_vjp: far-field or slip boundaries together with a buffer zone are not differentiated");
     return SOD_ERR_UNSUPPORTED;

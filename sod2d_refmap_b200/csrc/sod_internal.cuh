@@ -193,6 +193,17 @@ struct ZoneState {
   double rho_inf = 0.0, E_inf = 0.0;
 };
 
+// Wall model (sod_wallmodel.cu): wall nodes, their (face, node) entries grouped by node with
+// the exchange node, weight |bounorm| wgp_b, node normal, wall distance and roughness; the
+// per-node contribution to the momentum residual [3][npoin] (zero off the walls) and tauw.
+struct WallModelState {
+  int nw = 0, nent = 0, type = 0;
+  int32_t *wnode = nullptr, *wptr = nullptr, *ex = nullptr;
+  double *w = nullptr, *nrm = nullptr, *y = nullptr, *zo = nullptr;
+  double *contrib = nullptr, *tauw = nullptr;
+  const double* walave = nullptr;  // caller's time-averaged velocity (flag_walave), or null
+};
+
 // EOS and Sutherland viscosity of node n at the new level (time_integ.f90:445-463,
 // mod_fluid_viscosity.f90:21-41) from its conserved values
 __device__ __forceinline__ void eos_store(size_t n, size_t N, double rho, const double (&qq)[3], double e, double g,
@@ -260,6 +271,7 @@ struct SodMesh {
   sod::BcState bc;             // boundaries (nb == 0: periodic path, noBoundaries)
   sod::ZoneState zone;         // buffer zone (nb == 0: flag_buffer_on = .false.)
   const double* source = nullptr;  // caller's constant momentum source term (npoin,3), or null
+  sod::WallModelState wmodel;      // wall model (nw == 0: isWallModelOn = .false.)
   double* postpro = nullptr;       // element-node scratch of sod_compute_field_derivs
   size_t postpro_len = 0;
 };
@@ -304,6 +316,10 @@ int zone_stage(SodMesh* m, double* ys, cudaStream_t st);
 int zone_final(SodMesh* m, SodState* s, cudaStream_t st);
 int zone_adjoint(SodMesh* m, double* vbar, cudaStream_t st);
 void zone_free(SodMesh* m);
+// wall model (sod_wallmodel.cu) on a stage state: wmodel.contrib <- the wall shear terms
+int wall_model_stage(SodMesh* m, const double* rho, const double* q0, const double* E, const double* mu_factor,
+                     cudaStream_t st);
+void wall_model_free(SodMesh* m);
 // packed-FP32 (FFMA2) variant of the mixed fused RHS kernel (sod_rhs_mixed.cu)
 int launch_rhs_mixed2(const RhsArgs& a, int epb, cudaStream_t st);
 // LES (sod_les.cu): musgs_int <- sgs_visc of the velocity u (3 columns of npoin)

@@ -326,6 +326,7 @@ void sod_mesh_destroy(SodMesh* m) {
   if (!m) return;
   bc_free(m);
   zone_free(m);
+  wall_model_free(m);
   if (m->postpro) cudaFree(m->postpro);
   for (auto& kv : m->graphs)
     if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);

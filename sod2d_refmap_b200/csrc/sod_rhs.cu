@@ -347,6 +347,7 @@ struct GatherArgs {
   double* scal;             // [0] eta mean, [1] eta norm
   int normalise;
   const double* src;        // momentum source term (npoin,3) or null
+  const double* wm;         // wall-model momentum terms (npoin,3) or null
 };
 
 __device__ __forceinline__ void block_reduce3(double& s, double& mx, double& mn, double* sh) {
@@ -411,6 +412,11 @@ __global__ void __launch_bounds__(256, SOD_KG_MIN_BLOCKS) k_gather_rk(const Gath
       // mom_source_const_vect (elem_source.f90:20-55): - sum_e gpvol s = - Ml s on the momentum
 #pragma unroll
       for (int d = 0; d < 3; ++d) r[1 + d] -= ml * a.src[d * N + n];
+    }
+    if (a.wm) {
+      // wall model: the modelled shear added to Rdiff_mom (time_integ.f90:334-357)
+#pragma unroll
+      for (int d = 0; d < 3; ++d) r[1 + d] += a.wm[d * N + n];
     }
 #pragma unroll
     for (int f = 0; f < 6; ++f) r[f] = r[f] / ml;
@@ -717,6 +723,7 @@ int launch_gather(SodMesh* m, bool mixed, int stage, GatherArgs& a, cudaStream_t
   a.nonfinite = m->buf.counters + kNonfiniteCounter;
   a.scal = m->buf.scal;
   a.src = m->nmember > 0 ? nullptr : m->source;
+  a.wm = (m->nmember > 0 || m->wmodel.nw == 0) ? nullptr : m->wmodel.contrib;
   if (stage >= 1) {
     a.b_cur = kB[stage - 1];
     a.a_next = stage < 4 ? kA[stage] : 0.0;
@@ -851,6 +858,10 @@ int run_step(SodMesh* m, SodState* s, const double* dt_dev, double* dt_next, boo
     const double* src_q1 = from_state ? s->q + N : yin + 2 * N;
     const double* src_q2 = from_state ? s->q + 2 * N : yin + 3 * N;
     const double* src_E = from_state ? s->E : yin + 4 * N;
+    if (m->wmodel.nw > 0) {
+      rc = wall_model_stage(m, src_rho, src_q0, src_E, s->mu_factor, st);
+      if (rc) return rc;
+    }
     if (ev) cudaEventRecord(ev[2 * (stage - 1)], st);
     rc = launch_rhs(m, mixed, epb, src_rho, src_q0, src_q1, src_q2, src_E, s->mu_factor, les ? m->musgs_int : nullptr,
                     st);

@@ -228,6 +228,42 @@ class Sod2dMesh:
         _lib.check(_lib.load().sod_mesh_set_source_term(self.handle, C.c_void_p(_ptr(src))))
         self._source = src
 
+    def set_wall_model(self, wtype: int, bound, bounorm, wgp_b, list_wm, point2elem, coord, normals, zo=None,
+                       walave_u=None):
+        """Registers the wall model (isWallModelOn): wtype 1 Reichardt, 2 ABL; host arrays with
+        0-based ids (mesh.wall_faces); list_wm the wall-model faces; walave_u a device tensor
+        (3, npoin) kept by the mesh, or None.  list_wm empty/None removes it."""
+        L = _lib.load()
+        if list_wm is None or len(list_wm) == 0:
+            _lib.check(L.sod_mesh_set_wall_model(self.handle, 1, 0, 0, *([None] * 3), 0, *([None] * 6)))
+            self._walave = None
+            return
+        b = np.asfortranarray(bound, dtype=np.int32)
+        bn = np.asfortranarray(bounorm, dtype=np.float64)
+        wg = np.ascontiguousarray(wgp_b, dtype=np.float64)
+        lw = np.ascontiguousarray(list_wm, dtype=np.int32)
+        pe = np.ascontiguousarray(point2elem, dtype=np.int32)
+        co = np.asfortranarray(coord, dtype=np.float64)
+        nr = np.asfortranarray(normals, dtype=np.float64)
+        z = None if zo is None else np.ascontiguousarray(zo, dtype=np.float64)
+        wa = None if walave_u is None else _contig(walave_u)
+        _lib.check(L.sod_mesh_set_wall_model(
+            self.handle, int(wtype), b.shape[0], b.shape[1], _np_ptr(b), _np_ptr(bn), _np_ptr(wg), len(lw),
+            _np_ptr(lw), _np_ptr(pe), _np_ptr(co), _np_ptr(nr), _np_ptr(z) if z is not None else None,
+            C.c_void_p(_ptr(wa)) if wa is not None else None))
+        self._walave = wa
+
+    def wall_model(self, rho, u, mu_fluid, Rdiff, tauw=None, stream=None):
+        """The registered wall model as the reference routine: Rdiff (3, npoin) += the wall terms."""
+        _lib.check(_lib.load().sod_wall_model(self.handle, *(C.c_void_p(_ptr(_contig(t))) for t in (
+            rho, u, mu_fluid, Rdiff)), C.c_void_p(_ptr(tauw)) if tauw is not None else None, _stream(stream)))
+
+    def wall_model_tauw(self, stream=None):
+        torch = _torch()
+        t = torch.empty(3, self.npoin, dtype=torch.float64, device="cuda")
+        _lib.check(_lib.load().sod_wall_model_tauw(self.handle, C.c_void_p(_ptr(t)), _stream(stream)))
+        return t
+
     def update_buffer(self, rho, q, E, stream=None):
         """updateBuffer in place on device tensors rho (npoin), q (3,npoin) storage = Fortran
         (npoin,3), E (npoin)."""
