@@ -422,8 +422,7 @@ int sod_rk4_main_record(SodMesh* mesh, SodState* state, const double* dt_dev, do
  * evaluation at the last stage state); slip walls (codes 6, 7) also read a velocity: zero at
  * stage 1, q/rho of the previous post-routine stage state at stages 2-4, and u(pos) of the input
  * state at the update, which the map takes as q/rho of (rho, q, E) (its value in every state a
- * step produces).  Far-field or slip nodes together with a buffer zone give
- * SOD_ERR_UNSUPPORTED. */
+ * step produces).  A registered wall model gives SOD_ERR_UNSUPPORTED. */
 int sod_rk4_step_vjp(SodMesh* mesh, const double* rho, const double* q, const double* E,
                      const double* mu_e, const double* mu_sgs, const double* mu_factor,
                      const double* dt_dev, const double* stages, const double* bar_rho,

@@ -628,10 +628,9 @@ int sod_rk4_step_vjp(SodMesh* m, const double* rho, const double* q, const doubl
     set_error("sod_rk4_step_vjp: the wall model is not differentiated");
     return SOD_ERR_UNSUPPORTED;
   }
-  if ((ff || slip) && has_zone) {
-    set_error("sod_rk4_step_vjp: far-field or slip boundaries together with a buffer zone are not differentiated");
-    return SOD_ERR_UNSUPPORTED;
-  }
+  // far-field nodes with a buffer zone: the final routine's input at the lnbn targets from the
+  // stage residuals gathered there (the zone changes the stage states the reconstruction uses)
+  const bool ffz = ff && has_zone;
   NvtxRange range("sod rk4 step vjp");
   cudaStream_t st = (cudaStream_t)stream;
   int rc = ensure_step_buffers(m, false);
@@ -697,6 +696,10 @@ int sod_rk4_step_vjp(SodMesh* m, const double* rho, const double* q, const doubl
         rc = bc_slip_residuals(m, t + 1, rel, st);
         if (rc) return rc;
       }
+      if (ffz) {
+        rc = bc_ff_residuals(m, t + 1, rel, st);
+        if (rc) return rc;
+      }
       k_stage_state<<<nblk(N), 256, 0, st>>>(N, m->n2e_ptr, m->n2e, rel, m->Ml, dt_dev, acoef[t], y0, m->source, b);
       SOD_CHECK_LAUNCH();
       if (bc) {
@@ -709,14 +712,20 @@ int sod_rk4_step_vjp(SodMesh* m, const double* rho, const double* q, const doubl
   }
   if (ff || slip) {
     const int epb = m->tuned_epb[0] ? m->tuned_epb[0] : 2;
-    if (slip && stages) {
-      // the stage residuals at the slip nodes (the recompute above gathered them already)
+    if ((slip || ffz) && stages) {
+      // the stage residuals at the slip nodes / lnbn targets (the recompute gathered them already)
       for (int t = 0; t < 3; ++t) {
         const double* yt = t == 0 ? y1s : ys[t - 1];
         rc = launch_rhs(m, false, epb, yt, yt + N, yt + 2 * N, yt + 3 * N, yt + 4 * N, mu_factor, musgs, st);
         if (rc) return rc;
-        rc = bc_slip_residuals(m, t + 1, rel, st);
-        if (rc) return rc;
+        if (slip) {
+          rc = bc_slip_residuals(m, t + 1, rel, st);
+          if (rc) return rc;
+        }
+        if (ffz) {
+          rc = bc_ff_residuals(m, t + 1, rel, st);
+          if (rc) return rc;
+        }
       }
     }
     // the updated state the final routine reads, at the far-field nodes' lnbn nodes (interior:
@@ -725,7 +734,12 @@ int sod_rk4_step_vjp(SodMesh* m, const double* rho, const double* q, const doubl
     const double* y4 = ys[2];
     rc = launch_rhs(m, false, epb, y4, y4 + N, y4 + 2 * N, y4 + 3 * N, y4 + 4 * N, mu_factor, musgs, st);
     if (rc) return rc;
-    if (ff) {
+    if (ffz) {
+      rc = bc_ff_residuals(m, 4, rel, st);
+      if (rc) return rc;
+      rc = bc_ff_final(m, rho, q, E, dt_dev, zf, st);
+      if (rc) return rc;
+    } else if (ff) {
       k_final_pre<<<nblk(N), 256, 0, st>>>(N, m->n2e_ptr, m->n2e, rel, m->Ml, dt_dev, y0, ys[0], ys[1], ys[2],
                                            m->source, zf);
       SOD_CHECK_LAUNCH();

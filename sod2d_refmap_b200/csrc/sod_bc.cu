@@ -331,7 +331,11 @@ __global__ void __launch_bounds__(kBlock) k_bc_slip_prepare(int nb, const int32_
                                                             const double* __restrict__ Y3,
                                                             const double* __restrict__ dt,
                                                             const double* __restrict__ res,
-                                                            double* __restrict__ pre, double* __restrict__ uo) {
+                                                            const int32_t* __restrict__ zmap,
+                                                            const double* __restrict__ zxi,
+                                                            const double* __restrict__ zub, int znb,
+                                                            double rho_inf, double* __restrict__ pre,
+                                                            double* __restrict__ uo) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= nb) return;
   const int c = code[b];
@@ -350,6 +354,19 @@ __global__ void __launch_bounds__(kBlock) k_bc_slip_prepare(int nb, const int32_
 #pragma unroll
     for (int s = 0; s < 4; ++s) rs = rs + b_s[s] * res[((size_t)s * 4 + f) * B + b];
     pre[((size_t)4 * 4 + f) * B + b] = y - h * rs;
+  }
+  // with a buffer zone the routine reads the zone-updated state (E is not needed here)
+  const int zi = zmap ? zmap[n] : -1;
+  if (zi >= 0) {
+    for (int a = 0; a < 5; ++a) {
+      double r = pre[((size_t)a * 4) * B + b], e = 0.0;
+      double qq[3] = {pre[((size_t)a * 4 + 1) * B + b], pre[((size_t)a * 4 + 2) * B + b],
+                      pre[((size_t)a * 4 + 3) * B + b]};
+      zone_point(zxi, zub, znb, zi, rho_inf, 0.0, r, qq, e);
+      pre[((size_t)a * 4) * B + b] = r;
+#pragma unroll
+      for (int d = 0; d < 3; ++d) pre[((size_t)a * 4 + 1 + d) * B + b] = qq[d];
+    }
   }
   const double* from[4] = {nullptr, Y1, Y2, Y3};
 #pragma unroll
@@ -383,6 +400,65 @@ __global__ void __launch_bounds__(kBlock) k_bc_slip_push(int nb, const int32_t* 
     vq[d * N + n] += ub / r;
   }
   vrho[n] -= s / r;
+}
+
+// residuals (gather / Ml, with the source term on q) of one stage at the far-field lnbn targets
+__global__ void __launch_bounds__(kBlock) k_bc_ff_res(int nu, const int32_t* __restrict__ target,
+                                                      const int32_t* __restrict__ ptr, const int32_t* __restrict__ idx,
+                                                      const double* __restrict__ el, const double* __restrict__ Ml,
+                                                      const double* __restrict__ src, size_t N,
+                                                      double* __restrict__ res /*[5][nu]*/) {
+  const int u = blockIdx.x * blockDim.x + threadIdx.x;
+  if (u >= nu) return;
+  const size_t n = (size_t)target[u];
+  double r[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+  for (int k = ptr[n]; k < ptr[n + 1]; ++k) {
+    const double* v = el + (size_t)idx[k] * NRES;
+#pragma unroll
+    for (int f = 0; f < 5; ++f) r[f] += v[f];
+  }
+  const double ml = Ml[n];
+  if (src) {
+#pragma unroll
+    for (int d = 0; d < 3; ++d) r[1 + d] -= ml * src[d * N + n];
+  }
+#pragma unroll
+  for (int f = 0; f < 5; ++f) res[(size_t)f * nu + u] = r[f] / ml;
+}
+
+// the state the final routine reads at the far-field lnbn targets: y0 - dt sum_s b_s R_s
+// (accumulated in the forward's order), then updateBuffer where the target is in a zone
+__global__ void __launch_bounds__(kBlock) k_bc_ff_final(int nu, const int32_t* __restrict__ target, size_t N,
+                                                        const double* __restrict__ rho0,
+                                                        const double* __restrict__ q0,
+                                                        const double* __restrict__ E0,
+                                                        const double* __restrict__ dt,
+                                                        const double* __restrict__ res,
+                                                        const int32_t* __restrict__ zmap,
+                                                        const double* __restrict__ zxi,
+                                                        const double* __restrict__ zub, int znb, double rho_inf,
+                                                        double E_inf, double* __restrict__ zf) {
+  const int u = blockIdx.x * blockDim.x + threadIdx.x;
+  if (u >= nu) return;
+  const size_t n = (size_t)target[u], U = (size_t)nu;
+  const double b_s[4] = {1.0 / 6.0, 1.0 / 3.0, 1.0 / 3.0, 1.0 / 6.0};
+  double y[5];
+#pragma unroll
+  for (int f = 0; f < 5; ++f) {
+    double rs = 0.0;
+#pragma unroll
+    for (int s = 0; s < 4; ++s) rs = rs + b_s[s] * res[((size_t)s * 5 + f) * U + u];
+    const double y0 = f == 0 ? rho0[n] : (f == 4 ? E0[n] : q0[(f - 1) * N + n]);
+    y[f] = y0 - (*dt) * rs;
+  }
+  const int zi = zmap ? zmap[n] : -1;
+  if (zi >= 0) {
+    double qq[3] = {y[1], y[2], y[3]};
+    zone_point(zxi, zub, znb, zi, rho_inf, E_inf, y[0], qq, y[4]);
+    y[1] = qq[0]; y[2] = qq[1]; y[3] = qq[2];
+  }
+#pragma unroll
+  for (int f = 0; f < 5; ++f) zf[f * N + n] = y[f];
 }
 
 __global__ void k_bc_adjoint_mask(int nb, const int32_t* __restrict__ node, const int32_t* __restrict__ code,
@@ -570,9 +646,30 @@ int bc_slip_residuals(SodMesh* m, int stage, const void* rel, cudaStream_t st) {
 int bc_slip_prepare(SodMesh* m, const double* rho0, const double* q0, const double* Y1, const double* Y2,
                     const double* Y3, const double* dt_dev, cudaStream_t st) {
   const BcState& B = m->bc;
-  bcd::k_bc_slip_prepare<<<bcd::grid_of(B.nb), bcd::kBlock, 0, st>>>(B.nb, B.node, B.code, (size_t)m->npoin, rho0,
-                                                                     q0, Y1, Y2, Y3, dt_dev, B.sl_res, B.sl_pre,
-                                                                     B.sl_uo);
+  const ZoneState& Z = m->zone;
+  bcd::k_bc_slip_prepare<<<bcd::grid_of(B.nb), bcd::kBlock, 0, st>>>(
+      B.nb, B.node, B.code, (size_t)m->npoin, rho0, q0, Y1, Y2, Y3, dt_dev, B.sl_res, Z.nb > 0 ? Z.zmap : nullptr,
+      Z.xi, Z.ub, Z.nb, Z.rho_inf, B.sl_pre, B.sl_uo);
+  SOD_CHECK_LAUNCH();
+  return SOD_OK;
+}
+
+int bc_ff_residuals(SodMesh* m, int stage, const void* rel, cudaStream_t st) {
+  const BcState& B = m->bc;
+  bcd::k_bc_ff_res<<<bcd::grid_of(B.ff_nu), bcd::kBlock, 0, st>>>(
+      B.ff_nu, B.ff_target, m->n2e_ptr, m->n2e, reinterpret_cast<const double*>(rel), m->Ml, m->source,
+      (size_t)m->npoin, B.ff_res + (size_t)(stage - 1) * 5 * B.ff_nu);
+  SOD_CHECK_LAUNCH();
+  return SOD_OK;
+}
+
+int bc_ff_final(SodMesh* m, const double* rho0, const double* q0, const double* E0, const double* dt_dev, double* zf,
+                cudaStream_t st) {
+  const BcState& B = m->bc;
+  const ZoneState& Z = m->zone;
+  bcd::k_bc_ff_final<<<bcd::grid_of(B.ff_nu), bcd::kBlock, 0, st>>>(
+      B.ff_nu, B.ff_target, (size_t)m->npoin, rho0, q0, E0, dt_dev, B.ff_res, Z.nb > 0 ? Z.zmap : nullptr, Z.xi,
+      Z.ub, Z.nb, Z.rho_inf, Z.E_inf, zf);
   SOD_CHECK_LAUNCH();
   return SOD_OK;
 }
@@ -588,7 +685,7 @@ int bc_slip_push(SodMesh* m, const double* rho, const double* q, double* vrho, d
 void bc_free(SodMesh* m) {
   BcState& b = m->bc;
   void* ptrs[] = {b.node, b.code, b.nbr, b.normal, b.ubuf, b.aux2, b.u_stage, b.u_final,
-                  b.ff_ptr, b.ff_target, b.ff_b, b.ff_contrib, b.slip};
+                  b.ff_ptr, b.ff_target, b.ff_b, b.ff_contrib, b.ff_res, b.slip};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   b = BcState{};
@@ -737,7 +834,8 @@ int sod_mesh_set_boundaries(SodMesh* m, const int32_t* codes, const int32_t* lnb
       if (!(alloc((void**)&B.ff_ptr, sizeof(int32_t) * ptr.size()) &&
             alloc((void**)&B.ff_target, sizeof(int32_t) * target.size()) &&
             alloc((void**)&B.ff_b, sizeof(int32_t) * bidx.size()) &&
-            alloc((void**)&B.ff_contrib, sizeof(double) * 5 * (size_t)nb))) {
+            alloc((void**)&B.ff_contrib, sizeof(double) * 5 * (size_t)nb) &&
+            alloc((void**)&B.ff_res, sizeof(double) * 20 * target.size()))) {
         bc_free(m);
         set_error("sod_mesh_set_boundaries: device allocation failed");
         return SOD_ERR_NOMEM;

@@ -116,7 +116,7 @@ int zone_adjoint(SodMesh* m, double* vbar, cudaStream_t st) {
 
 void zone_free(SodMesh* m) {
   ZoneState& z = m->zone;
-  void* ptrs[] = {z.node, z.xi, z.ub};
+  void* ptrs[] = {z.node, z.xi, z.ub, z.zmap};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   z = ZoneState{};
@@ -172,7 +172,7 @@ int sod_mesh_set_buffer(SodMesh* m, const SodBufferParams* p, const double* coor
   ZoneState& z = m->zone;
   auto alloc = [&](void** q, size_t bytes) { return cudaMalloc(q, bytes) == cudaSuccess; };
   if (!(alloc((void**)&z.node, sizeof(int32_t) * nb) && alloc((void**)&z.xi, sizeof(double) * nb) &&
-        alloc((void**)&z.ub, sizeof(double) * 3 * nb))) {
+        alloc((void**)&z.ub, sizeof(double) * 3 * nb) && alloc((void**)&z.zmap, sizeof(int32_t) * N))) {
     zone_free(m);
     set_error("sod_mesh_set_buffer: device allocation failed");
     return SOD_ERR_NOMEM;
@@ -183,6 +183,11 @@ int sod_mesh_set_buffer(SodMesh* m, const SodBufferParams* p, const double* coor
   SOD_CUDA(cudaMemcpy(z.node, node.data(), sizeof(int32_t) * nb, cudaMemcpyHostToDevice));
   SOD_CUDA(cudaMemcpy(z.xi, xi.data(), sizeof(double) * nb, cudaMemcpyHostToDevice));
   SOD_CUDA(cudaMemcpy(z.ub, ub.data(), sizeof(double) * 3 * nb, cudaMemcpyHostToDevice));
+  {
+    std::vector<int32_t> zmap(N, -1);
+    for (int b = 0; b < nb; ++b) zmap[node[b]] = b;
+    SOD_CUDA(cudaMemcpy(z.zmap, zmap.data(), sizeof(int32_t) * N, cudaMemcpyHostToDevice));
+  }
   return SOD_OK;
 }
 

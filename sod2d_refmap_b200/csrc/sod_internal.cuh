@@ -180,6 +180,7 @@ struct BcState {
   int32_t* ff_target = nullptr;
   int32_t* ff_b = nullptr;
   double* ff_contrib = nullptr;
+  double* ff_res = nullptr;  // [4 stages][5][ff_nu] residuals at the lnbn targets (with a buffer zone)
   SodBcParams prm{};
 };
 
@@ -190,8 +191,22 @@ struct ZoneState {
   int32_t* node = nullptr;
   double* xi = nullptr;
   double* ub = nullptr;
+  int32_t* zmap = nullptr;  // [npoin] zone entry of a node, -1 outside every zone
   double rho_inf = 0.0, E_inf = 0.0;
 };
+
+// updateBuffer on one node's (rho, q, E) given its zone entry (time_integ.f90:580-585)
+__device__ __forceinline__ void zone_point(const double* xi, const double* ub, int znb, int idx, double rho_inf,
+                                           double E_inf, double& rho, double (&q)[3], double& E) {
+  const double x = xi[idx];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const double ur = ub[(size_t)d * znb + idx] * rho;
+    q[d] = ur + x * (q[d] - ur);
+  }
+  E = E_inf + x * (E - E_inf);
+  rho = rho_inf + x * (rho - rho_inf);
+}
 
 // Wall model (sod_wallmodel.cu): wall nodes, their (face, node) entries grouped by node with
 // the exchange node, weight |bounorm| wgp_b, node normal, wall distance and roughness; the
@@ -305,6 +320,11 @@ int bc_slip_residuals(SodMesh* m, int stage, const void* rel, cudaStream_t st);
 int bc_slip_prepare(SodMesh* m, const double* rho0, const double* q0, const double* Y1, const double* Y2,
                     const double* Y3, const double* dt_dev, cudaStream_t st);
 int bc_slip_push(SodMesh* m, const double* rho, const double* q, double* vrho, double* vq, cudaStream_t st);
+// far-field with a buffer zone: the stage residuals at the lnbn targets, and the updated state
+// the final routine reads there (y0 - dt sum b_s R_s, then updateBuffer) into the rows of zf
+int bc_ff_residuals(SodMesh* m, int stage, const void* rel, cudaStream_t st);
+int bc_ff_final(SodMesh* m, const double* rho0, const double* q0, const double* E0, const double* dt_dev, double* zf,
+                cudaStream_t st);
 void bc_free(SodMesh* m);
 // entropy normalisation (mean and spread of eta) recomputed into buf.scal after a routine that
 // changed eta

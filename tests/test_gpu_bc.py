@@ -136,9 +136,9 @@ def test_channel_dt_graph_mixed(torch_mod, oracle):
     gm.close()
 
 
-def test_boundaries_removed_and_adjoint_rejected(torch_mod, oracle):
-    """A slip wall (code 6) together with a buffer zone: the step adjoint is refused, the
-    recording step still runs; removing the boundaries gives the periodic step."""
+def test_boundaries_removed(torch_mod, oracle):
+    """The recording step runs with a slip wall (code 6) and a buffer zone; removing the
+    boundaries and the zone gives the periodic step."""
     from sod2d_refmap_b200 import _lib, mesh as M, solver as S
     torch = torch_mod
     m, prm, st0, ub = channel((3, 6), seed=9, n=2)
@@ -153,8 +153,6 @@ def test_boundaries_removed_and_adjoint_rejected(torch_mod, oracle):
     L = 2.0 * np.pi
     gm.set_buffer(M.buffer_params(prm, east=(0.8 * L, 0.3 * L)), m.coord, ub)
     gm.rk_4_main_record(s, stages, update_dt=False)
-    with pytest.raises(_lib.SodError, match="SOD_ERR_UNSUPPORTED"):
-        gm.rk4_step_vjp(*y0, s.mu_factor, s.dt, s.rho, s.q, s.E, stages=stages)
     gm.set_buffer(None)
     fresh = S.Sod2dState.from_host(st0, gm.nelem)
     for f in S.Sod2dState.FIELDS:
@@ -326,8 +324,8 @@ def test_channel_step_vjp_far_field(torch_mod, oracle, codes):
 def test_far_field_rollout_fd_and_refusals(torch_mod, oracle, codes):
     """4-step rollouts with a far-field side (codes 1 and 3) and with a slip wall and a far-field
     side (6 and 1) against central differences of the frozen-coefficient map with u = q/rho in
-    the perturbed initial state (h = 1e-5, 1e-6; 1e-6 relative); far-field with a buffer zone,
-    and the standalone routine adjoint with slip walls, are refused."""
+    the perturbed initial state (h = 1e-5, 1e-6; 1e-6 relative); the standalone routine adjoint
+    with slip walls is refused."""
     from sod2d_refmap_b200 import _lib, mesh as M, solver as S
     from sod2d_refmap_b200.adjoint import Sod2dRollout, replay, trajectory_coefficients, _clone_state
     torch = torch_mod
@@ -359,17 +357,69 @@ def test_far_field_rollout_fd_and_refusals(torch_mod, oracle, codes):
     for h in (1e-5, 1e-6):
         fd = (L_at(h) - L_at(-h)) / (2 * h)
         assert abs(fd - dL) <= 1e-6 * abs(dL), (h, fd, dL)
-    # refusals
+    # refusal: the standalone routine adjoint does not get the velocity slip walls read
     bars = (s.rho.clone(), s.q.clone(), s.E.clone())
-    L = 2.0 * np.pi
-    gm.set_buffer(M.buffer_params(prm, east=(0.8 * L, 0.3 * L)), m.coord, ub)
-    with pytest.raises(_lib.SodError, match="SOD_ERR_UNSUPPORTED"):
-        gm.rk4_step_vjp(s.rho, s.q, s.E, s.mu_e, s.mu_factor, s.dt, *bars)
-    gm.set_buffer(None)
     m6, prm6, _, ub6 = channel((1, 6), seed=33)
     gm6 = S.Sod2dMesh(m6, prm6)
     gm6.set_boundaries(m6.extra["bou_codes_nodes"], m6.extra["lnbn_nodes"], m6.extra["normals"], ub6)
     with pytest.raises(_lib.SodError, match="SOD_ERR_UNSUPPORTED"):
         gm6.bc_dirichlet_prim_vjp(s.rho, s.q, s.E, *bars)
     gm6.close()
+    gm.close()
+
+
+@pytest.mark.parametrize("codes", [(1, 3), (6, 1)])
+def test_step_vjp_far_field_slip_with_buffer_zone(torch_mod, oracle, codes):
+    """Far-field and slip boundaries together with a buffer zone reaching both walls: the step
+    adjoint against the oracle's dual-number JVP of B(Z(.)) per stage (1e-11), recorded and
+    recomputed stage states."""
+    from _util import oracle_bc_jvp_map, oracle_step_jvp
+    from sod2d_refmap_b200 import mesh as M, solver as S
+    torch = torch_mod
+    m, prm, st0, ub = channel(codes, seed=41)
+    bc = M.bc_params(prm)
+    L = 2.0 * np.pi
+    lo, hi = m.coord.min(axis=0), m.coord.max(axis=0)
+    bp = M.buffer_params(prm, u_inf=0.5, south=(0.3 * L, (0.3 * L - lo[1]) / 0.995),
+                         north=(0.7 * L, (hi[1] - 0.7 * L) / 0.995))
+    om = oracle.OracleMesh(m)
+    bnd = oracle.Boundaries(m.extra["bou_codes_nodes"], m.extra["lnbn_nodes"], m.extra["normals"], ub, bc)
+    buf = oracle.BufferZone(m.coord, ub, bp)
+    dt = oracle.adapt_dt(om, st0, prm)
+    st = st0.copy()
+    oracle.rk4(om, prm, st, dt, nsteps=1, bnd=bnd, buf=buf)
+    J = oracle_bc_jvp_map(oracle, bnd)
+
+    def ZJ(y, v, u=None, du=None):
+        def Z(r, q, E):
+            r = np.array(r, copy=True); q = np.array(q, order="F", copy=True); E = np.array(E, copy=True)
+            oracle.update_buffer(buf, r, q, E)
+            return r, q, E
+        zy = Z(*y)
+        zyv = Z(*(y[f] + v[f] for f in range(3)))
+        return J(zy, tuple(zyv[f] - zy[f] for f in range(3)), u, du)
+    rng = np.random.default_rng(43)
+    rnd = lambda a: rng.standard_normal(a.shape) * np.abs(a).mean()
+    v = (rnd(st.rho), np.asfortranarray(rnd(st.q)), rnd(st.E))
+    w = (rnd(st.rho), np.asfortranarray(rnd(st.q)), rnd(st.E))
+    y1, dy1 = oracle_step_jvp(oracle, om, prm, st, dt, v, bc_jvp=ZJ)
+    gm = S.Sod2dMesh(m, prm)
+    gm.set_boundaries(m.extra["bou_codes_nodes"], m.extra["lnbn_nodes"], m.extra["normals"], ub, bc)
+    gm.set_buffer(bp, m.coord, ub)
+    s = S.Sod2dState.from_host(st, gm.nelem)
+    s.dt.fill_(dt)
+    stages = torch.zeros(15 * m.npoin, dtype=torch.float64, device="cuda")
+    y0 = (s.rho.clone(), s.q.clone(), s.E.clone(), s.mu_e.clone())
+    gm.rk_4_main_record(s, stages, update_dt=False)
+    h = s.to_host()
+    for got, ref in ((h["rho"], y1[0]), (h["q"], y1[1]), (h["E"], y1[2])):
+        assert rel_l2(got, ref) < TOL64
+    terms = [w[f] * dy1[f] for f in range(3)]
+    lhs = sum(t.sum() for t in terms)
+    scale = sum(np.abs(t).sum() for t in terms)
+    for stg in (stages, None):
+        out = gm.rk4_step_vjp(*y0, s.mu_factor, s.dt, *(dev(torch, a) for a in w), stages=stg)
+        g = [host(o) for o in out]
+        rhs = sum((g[f] * v[f]).sum() for f in range(3))
+        assert abs(lhs - rhs) <= 1e-11 * scale, (stg is None, lhs, rhs)
     gm.close()
