@@ -178,8 +178,8 @@ int sod_bc_dirichlet_prim_vjp(SodMesh* mesh, const double* rho, const double* q,
  * (numBoundsWM faces), point2elem (npoin), coord (npoin,3), normalsAtNodes (npoin,3), zo (npoin)
  * or null; walave_u: a device (npoin,3) array the mesh keeps a pointer to (flag_walave), or null
  * for the stage velocity.  Each stage then adds the modelled wall shear to the momentum
- * residual of the wall nodes.  numBoundsWM = 0 removes the model.  The step adjoint and the
- * ensemble reject meshes with a wall model. */
+ * residual of the wall nodes.  numBoundsWM = 0 removes the model.  The RHS and step adjoints
+ * include it; the ensemble rejects meshes with a wall model. */
 int sod_mesh_set_wall_model(SodMesh* mesh, int32_t type, int32_t nboun, int32_t npbou, const int32_t* bound,
                             const double* bounorm, const double* wgp_b, int32_t numBoundsWM,
                             const int32_t* listBoundsWM, const int32_t* point2elem, const double* coord,
@@ -422,7 +422,7 @@ int sod_rk4_main_record(SodMesh* mesh, SodState* state, const double* dt_dev, do
  * evaluation at the last stage state); slip walls (codes 6, 7) also read a velocity: zero at
  * stage 1, q/rho of the previous post-routine stage state at stages 2-4, and u(pos) of the input
  * state at the update, which the map takes as q/rho of (rho, q, E) (its value in every state a
- * step produces).  A registered wall model gives SOD_ERR_UNSUPPORTED. */
+ * step produces).  A registered wall model is differentiated too (its law by dual numbers). */
 int sod_rk4_step_vjp(SodMesh* mesh, const double* rho, const double* q, const double* E,
                      const double* mu_e, const double* mu_sgs, const double* mu_factor,
                      const double* dt_dev, const double* stages, const double* bar_rho,

@@ -395,9 +395,10 @@ def rhs_opcount(om: OracleMesh, prm, st, mu_e=None) -> float:
                    ptr(np.asfortranarray(st.q)), ptr(st.E)))
 
 
-def rhs_jvp(om: OracleMesh, prm, st, drho, dq, dE, mu_e=None, mu_sgs=None):
+def rhs_jvp(om: OracleMesh, prm, st, drho, dq, dE, mu_e=None, mu_sgs=None, wall: "WallModel | None" = None):
     """Exact JVP of rhs_stage along (drho, dq(npoin,3), dE): returns (R, dR) as (5, npoin).
-    mu_sgs (nelem,64): a frozen SGS viscosity in the diffusion (LES), None for none."""
+    mu_sgs (nelem,64): a frozen SGS viscosity in the diffusion (LES), None for none; wall: the
+    wall model's term in the momentum residual."""
     P = params_of(prm)
     R = np.zeros(5 * om.npoin); dR = np.zeros(5 * om.npoin)
     mue = np.asfortranarray(st.mu_e if mu_e is None else mu_e)
@@ -405,7 +406,8 @@ def rhs_jvp(om: OracleMesh, prm, st, drho, dq, dE, mu_e=None, mu_sgs=None):
     lib().oracle_rhs_jvp(C.byref(om.ctx), C.byref(P), ptr(om.Ml), ptr(st.mu_factor), ptr(mue),
                          ptr(sgs) if sgs is not None else None, ptr(st.rho),
                          ptr(np.asfortranarray(st.q)), ptr(st.E), ptr(np.ascontiguousarray(drho)),
-                         ptr(np.asfortranarray(dq)), ptr(np.ascontiguousarray(dE)), ptr(R), ptr(dR))
+                         ptr(np.asfortranarray(dq)), ptr(np.ascontiguousarray(dE)), ptr(R), ptr(dR),
+                         C.byref(wall.c) if wall is not None else None)
     return R.reshape(5, om.npoin), dR.reshape(5, om.npoin)
 
 

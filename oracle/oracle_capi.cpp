@@ -200,14 +200,15 @@ void oracle_rhs_stage(const ElemCtx* ctx, const Params* P, const double* Ml, con
 // Exact JVP of oracle_rhs_stage by forward-mode dual numbers: dR = (dR/dU) dU, U = (rho,q,E).
 void oracle_rhs_jvp(const ElemCtx* ctx, const Params* P, const double* Ml, const double* mu_factor,
                     const double* mu_e, const double* mu_sgs, const double* rho, const double* q, const double* E,
-                    const double* drho, const double* dq, const double* dE, double* R, double* dR) {
+                    const double* drho, const double* dq, const double* dE, double* R, double* dR,
+                    const WallModelData* wmd) {
   const int64_t N = ctx->npoin;
   std::vector<double> zeros;
   if (!mu_sgs) { zeros.assign((size_t)ctx->nelem * nnode, 0.0); mu_sgs = zeros.data(); }
   std::vector<Dual> r(N), qq(3 * N), e(N), out(5 * N);
   for (int64_t p = 0; p < N; ++p) { r[p] = Dual(rho[p], drho[p]); e[p] = Dual(E[p], dE[p]); }
   for (int64_t p = 0; p < 3 * N; ++p) qq[p] = Dual(q[p], dq[p]);
-  rhs_stage_t<Dual>(*ctx, *P, Ml, mu_factor, mu_e, mu_sgs, r.data(), qq.data(), e.data(), out.data());
+  rhs_stage_t<Dual>(*ctx, *P, Ml, mu_factor, mu_e, mu_sgs, r.data(), qq.data(), e.data(), out.data(), wmd);
   for (int64_t p = 0; p < 5 * N; ++p) { if (R) R[p] = out[p].v; dR[p] = out[p].d; }
 }
 

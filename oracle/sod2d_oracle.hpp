@@ -21,6 +21,7 @@
 #include <cstring>
 #include <vector>
 #include <algorithm>
+#include <type_traits>
 #ifdef _OPENMP
 #include <omp.h>
 #endif
@@ -797,6 +798,19 @@ inline Dual operator/(double a, Dual b) { return {a / b.v, -a * b.d / (b.v * b.v
 inline Dual& operator+=(Dual& a, Dual b) { a = a + b; return a; }
 inline Dual& operator-=(Dual& a, Dual b) { a = a - b; return a; }
 inline Dual sqrt(Dual a) { double s = std::sqrt(a.v); return {s, a.d / (2.0 * s)}; }
+inline Dual exp(Dual a) { double e = std::exp(a.v); return {e, e * a.d}; }
+inline Dual log(Dual a) { return {std::log(a.v), a.d / a.v}; }
+inline Dual fabs(Dual a) { return a.v < 0.0 ? Dual{-a.v, -a.d} : a; }
+inline Dual wm_min(Dual a, Dual b) { return a.v <= b.v ? a : b; }
+inline Dual wm_max(Dual a, Dual b) { return a.v >= b.v ? a : b; }
+inline double exp(double a) { return std::exp(a); }
+inline double log(double a) { return std::log(a); }
+inline double fabs(double a) { return std::fabs(a); }
+inline double wm_min(double a, double b) { return std::min(a, b); }
+inline double wm_max(double a, double b) { return std::max(a, b); }
+inline bool operator<(Dual a, double b) { return a.v < b; }
+inline bool operator>(Dual a, double b) { return a.v > b; }
+inline bool operator>=(Dual a, double b) { return a.v >= b; }
 inline Dual pow(Dual a, double e) { double p = std::pow(a.v, e); return {p, e * std::pow(a.v, e - 1.0) * a.d}; }
 inline double sqrt(double a) { return std::sqrt(a); }
 inline double pow(double a, double e) { return std::pow(a, e); }
@@ -1078,13 +1092,122 @@ inline void full_diffusion_ijk_t(const ElemCtx& ctx, const Params& P, const T* r
   });
 }
 
+// Wall model data (isWallModelOn): reference arrays with 0-based ids; type 1 Reichardt, 2 ABL;
+// walave (npoin,3) replaces the stage velocity when set (flag_walave).
+struct WallModelData {
+  int type, nboun, npbou, numBoundsWM;
+  const int32_t* bound;         // (nboun,npbou)
+  const double* bounorm;        // (nboun,3*npbou)
+  const double* wgp_b;          // (npbou)
+  const int32_t* listBoundsWM;  // (numBoundsWM)
+  const int32_t* point2elem;    // (npoin)
+  const double* coord;          // (npoin,3)
+  const double* normals;        // (npoin,3)
+  const double* zo;             // (npoin) or null
+  const double* walave;         // (npoin,3) or null
+  double* tauw;                 // (npoin,3) output or null
+};
+
+// evalWallModelReichardt / evalWallModelABL (mod_wall_model.f90:12-300): per wall-model face,
+// the element of an interior face node and the face's normal iso direction; per face node the
+// exchange node on the element's opposite face, the tangential velocity there, the law's wall
+// shear and Rdiff(node) += |bounorm| wgp_b tmag tvelo (the reference's atomics, in face order),
+// tauw(node) = tmag tvelo (the last face wins).
+template <class T>
+inline void eval_wall_model(const ElemCtx& ctx, const WallModelData& W, const T* rho, const T* ui, const T* mu_fluid,
+                            T* Rdiff) {
+  const int64_t N = ctx.npoin, NB = W.nboun;
+  const int nelem = ctx.nelem;
+  auto local_of = [&](int e, int64_t node) {
+    for (int a = 0; a < nnode; ++a)
+      if (ctx.connec[e + (int64_t)nelem * a] == node) return a;
+    return -1;
+  };
+  for (int f = 0; f < W.numBoundsWM; ++f) {
+    const int64_t ib = W.listBoundsWM[f];
+    int iElem = -1, type_ijk = -1, isoF = -1;
+    for (int a = 0; a < W.npbou && iElem < 0; ++a) {  // an interior face node (reference: atoIJ(npbou))
+      const int64_t nd = W.bound[ib + NB * a];
+      const int e = W.point2elem[nd];
+      const int jg = local_of(e, nd);
+      const int iso[3] = {ctx.gmshAtoI[jg], ctx.gmshAtoJ[jg], ctx.gmshAtoK[jg]};
+      int nend = 0, dd = -1;
+      for (int r = 0; r < 3; ++r)
+        if (iso[r] <= 1) { ++nend; dd = r; }
+      if (nend == 1) { iElem = e; type_ijk = dd; isoF = iso[dd] == 0 ? 1 : 0; }
+    }
+    for (int a = 0; a < W.npbou; ++a) {
+      const int64_t nd = W.bound[ib + NB * a];
+      const int jg = local_of(iElem, nd);
+      int iso[3] = {ctx.gmshAtoI[jg], ctx.gmshAtoJ[jg], ctx.gmshAtoK[jg]};
+      iso[type_ijk] = isoF;
+      const int64_t x = ctx.connec[iElem + (int64_t)nelem * SOD_INV(iso[0], iso[1], iso[2])];
+      T uiex[3];
+      double point[3], pointF[3], normalF[3];
+      for (int d = 0; d < 3; ++d) {
+        point[d] = W.coord[x + N * d];
+        uiex[d] = ui[x + N * d];
+        pointF[d] = W.coord[nd + N * d];
+        normalF[d] = W.normals[nd + N * d];
+      }
+      const T rhol = rho[nd], nul = mu_fluid[nd] / rhol;
+      const double y = std::fabs(normalF[0] * (point[0] - pointF[0]) + normalF[1] * (point[1] - pointF[1]) +
+                                 normalF[2] * (point[2] - pointF[2]));
+      const T auxvn = normalF[0] * uiex[0] + normalF[1] * uiex[1] + normalF[2] * uiex[2];
+      T tvelo[3];
+      for (int d = 0; d < 3; ++d) tvelo[d] = uiex[d] - auxvn * normalF[d];
+      const T ul = sqrt(tvelo[0] * tvelo[0] + tvelo[1] * tvelo[1] + tvelo[2] * tvelo[2]);
+      T tmag;
+      if (W.type == 2) {
+        const T uistar = ul * 0.41 / log(1.0 + y / W.zo[nd]);
+        tmag = rhol * uistar * uistar / ul;
+      } else {
+        T uistar;
+        if (y > 0.0 && ul > 1.0e-10) {
+          uistar = sqrt(ul * nul / y);
+          if (uistar * y / nul > 5.0) {
+            const double vkinv = 1.0 / 0.41, oneoe = 1.0 / 11.0;
+            const T onovu = 1.0 / ul, xmuit = y / nul;
+            int itera = 0;
+            T parco = T(1.0);
+            while (parco >= 1.0e-6 && itera < 100) {
+              itera = itera + 1;
+              uistar = wm_max(uistar, T(0.0));
+              const T yplus = uistar * xmuit, ypele = yplus * oneoe, ypel2 = wm_min(ypele, T(20.0));
+              const T expye = exp(-ypel2), yplu2 = wm_min(yplus, T(70.0));
+              const T expyt = exp(-yplu2 * 0.33), firsl = vkinv * log(1.0 + 0.4 * yplus);
+              const T fdvfr = uistar * (firsl + 7.8 * (1.0 - expye - ypele * expyt)) - ul;
+              const T diffd = firsl + vkinv * 0.4 * yplus / (1.0 + 0.4 * yplus) +
+                              7.8 * (1.0 - expye * (1.0 - ypele) - ypele * expyt * (2.0 - yplus * 0.33));
+              const T devfr = -fdvfr / diffd;
+              parco = fabs(devfr * onovu);
+              uistar = uistar + devfr;
+            }
+          }
+        } else {
+          uistar = T(0.0);
+        }
+        tmag = (y * uistar / nul < 5.0) ? rhol * nul / y : rhol * uistar * uistar / ul;
+      }
+      double am = 0.0;
+      for (int d = 0; d < 3; ++d) am += W.bounorm[ib + NB * (3 * a + d)] * W.bounorm[ib + NB * (3 * a + d)];
+      am = std::sqrt(am);
+      for (int d = 0; d < 3; ++d) {
+        Rdiff[nd + N * d] = Rdiff[nd + N * d] + am * W.wgp_b[a] * tmag * tvelo[d];
+        if (W.tauw) W.tauw[nd + N * d] = value(tmag * tvelo[d]);
+      }
+    }
+  }
+}
+
 // The stage RHS of rk_4_main without the entropy residual (time_integ.f90:266-393): EOS,
 // Sutherland, full_diffusion_ijk + full_convec_ijk (energy with h; full_convec_ijk_H with the
 // total-enthalpy flag), sum, /Ml.  State in
 // (rho, q(npoin,3), E); R is 5 columns of npoin: mass, mom x3, energy.  mu_e frozen.
 template <class T>
 inline void rhs_stage_t(const ElemCtx& ctx, const Params& P, const double* Ml, const double* mu_factor,
-                        const double* mu_e, const double* mu_sgs, const T* rho, const T* q, const T* E, T* R) {
+                        const double* mu_e, const double* mu_sgs, const T* rho, const T* q, const T* E, T* R,
+                        const WallModelData* wmd = nullptr) {
   const int npoin = ctx.npoin;
   const int64_t N = npoin;
   const double g = P.gamma_gas, Rgas = P.Rgas;
@@ -1103,6 +1226,13 @@ inline void rhs_stage_t(const ElemCtx& ctx, const Params& P, const double* Ml, c
   }
   full_diffusion_ijk_t<T>(ctx, P, rho, rho, u.data(), Tem.data(), muf.data(), mu_e, mu_sgs, Dm.data(), Dmo.data(),
                           De.data());
+  if constexpr (std::is_same_v<T, double> || std::is_same_v<T, Dual>) {  // not in the operation count
+    if (wmd) {  // time_integ.f90:334-357
+      std::vector<T> wav;
+      if (wmd->walave) wav.assign(wmd->walave, wmd->walave + 3 * N);
+      eval_wall_model<T>(ctx, *wmd, rho, wmd->walave ? wav.data() : u.data(), muf.data(), Dmo.data());
+    }
+  }
   if (P.flag_total_enthalpy)  // time_integ.f90:361-365
     full_convec_ijk_H<T>(ctx, u.data(), q, rho, pr.data(), E, Rm.data(), Rmo.data(), Re.data());
   else
@@ -1414,111 +1544,6 @@ struct BcData {
   const double* u_buffer;          // (npoin,3)
   double rho_inf, u_inf, p_inf, c_inf, gamma_inf, Rgas_inf, T_H, T_C;  // nscbc_* values
 };
-
-// Wall model data (isWallModelOn): reference arrays with 0-based ids; type 1 Reichardt, 2 ABL;
-// walave (npoin,3) replaces the stage velocity when set (flag_walave).
-struct WallModelData {
-  int type, nboun, npbou, numBoundsWM;
-  const int32_t* bound;         // (nboun,npbou)
-  const double* bounorm;        // (nboun,3*npbou)
-  const double* wgp_b;          // (npbou)
-  const int32_t* listBoundsWM;  // (numBoundsWM)
-  const int32_t* point2elem;    // (npoin)
-  const double* coord;          // (npoin,3)
-  const double* normals;        // (npoin,3)
-  const double* zo;             // (npoin) or null
-  const double* walave;         // (npoin,3) or null
-  double* tauw;                 // (npoin,3) output or null
-};
-
-// evalWallModelReichardt / evalWallModelABL (mod_wall_model.f90:12-300): per wall-model face,
-// the element of an interior face node and the face's normal iso direction; per face node the
-// exchange node on the element's opposite face, the tangential velocity there, the law's wall
-// shear and Rdiff(node) += |bounorm| wgp_b tmag tvelo (the reference's atomics, in face order),
-// tauw(node) = tmag tvelo (the last face wins).
-inline void eval_wall_model(const ElemCtx& ctx, const WallModelData& W, const double* rho, const double* ui,
-                            const double* mu_fluid, double* Rdiff) {
-  const int64_t N = ctx.npoin, NB = W.nboun;
-  const int nelem = ctx.nelem;
-  auto local_of = [&](int e, int64_t node) {
-    for (int a = 0; a < nnode; ++a)
-      if (ctx.connec[e + (int64_t)nelem * a] == node) return a;
-    return -1;
-  };
-  for (int f = 0; f < W.numBoundsWM; ++f) {
-    const int64_t ib = W.listBoundsWM[f];
-    int iElem = -1, type_ijk = -1, isoF = -1;
-    for (int a = 0; a < W.npbou && iElem < 0; ++a) {  // an interior face node (reference: atoIJ(npbou))
-      const int64_t nd = W.bound[ib + NB * a];
-      const int e = W.point2elem[nd];
-      const int jg = local_of(e, nd);
-      const int iso[3] = {ctx.gmshAtoI[jg], ctx.gmshAtoJ[jg], ctx.gmshAtoK[jg]};
-      int nend = 0, dd = -1;
-      for (int r = 0; r < 3; ++r)
-        if (iso[r] <= 1) { ++nend; dd = r; }
-      if (nend == 1) { iElem = e; type_ijk = dd; isoF = iso[dd] == 0 ? 1 : 0; }
-    }
-    for (int a = 0; a < W.npbou; ++a) {
-      const int64_t nd = W.bound[ib + NB * a];
-      const int jg = local_of(iElem, nd);
-      int iso[3] = {ctx.gmshAtoI[jg], ctx.gmshAtoJ[jg], ctx.gmshAtoK[jg]};
-      iso[type_ijk] = isoF;
-      const int64_t x = ctx.connec[iElem + (int64_t)nelem * SOD_INV(iso[0], iso[1], iso[2])];
-      double uiex[3], point[3], pointF[3], normalF[3];
-      for (int d = 0; d < 3; ++d) {
-        point[d] = W.coord[x + N * d];
-        uiex[d] = ui[x + N * d];
-        pointF[d] = W.coord[nd + N * d];
-        normalF[d] = W.normals[nd + N * d];
-      }
-      const double rhol = rho[nd], nul = mu_fluid[nd] / rhol;
-      const double y = std::fabs(normalF[0] * (point[0] - pointF[0]) + normalF[1] * (point[1] - pointF[1]) +
-                                 normalF[2] * (point[2] - pointF[2]));
-      const double auxvn = normalF[0] * uiex[0] + normalF[1] * uiex[1] + normalF[2] * uiex[2];
-      double tvelo[3];
-      for (int d = 0; d < 3; ++d) tvelo[d] = uiex[d] - auxvn * normalF[d];
-      const double ul = std::sqrt(tvelo[0] * tvelo[0] + tvelo[1] * tvelo[1] + tvelo[2] * tvelo[2]);
-      double tmag;
-      if (W.type == 2) {
-        const double uistar = ul * 0.41 / std::log(1.0 + y / W.zo[nd]);
-        tmag = rhol * uistar * uistar / ul;
-      } else {
-        double uistar;
-        if (y > 0.0 && ul > 1.0e-10) {
-          uistar = std::sqrt(ul * nul / y);
-          if (uistar * y / nul > 5.0) {
-            const double vkinv = 1.0 / 0.41, onovu = 1.0 / ul, xmuit = y / nul, oneoe = 1.0 / 11.0;
-            int itera = 0;
-            double parco = 1.0;
-            while (parco >= 1.0e-6 && itera < 100) {
-              itera = itera + 1;
-              uistar = std::max(uistar, 0.0);
-              const double yplus = uistar * xmuit, ypele = yplus * oneoe, ypel2 = std::min(ypele, 20.0);
-              const double expye = std::exp(-ypel2), yplu2 = std::min(yplus, 70.0);
-              const double expyt = std::exp(-yplu2 * 0.33), firsl = vkinv * std::log(1.0 + 0.4 * yplus);
-              const double fdvfr = uistar * (firsl + 7.8 * (1.0 - expye - ypele * expyt)) - ul;
-              const double diffd = firsl + vkinv * 0.4 * yplus / (1.0 + 0.4 * yplus) +
-                                   7.8 * (1.0 - expye * (1.0 - ypele) - ypele * expyt * (2.0 - yplus * 0.33));
-              const double devfr = -fdvfr / diffd;
-              parco = std::fabs(devfr * onovu);
-              uistar = uistar + devfr;
-            }
-          }
-        } else {
-          uistar = 0.0;
-        }
-        tmag = (y * uistar / nul < 5.0) ? rhol * nul / y : rhol * uistar * uistar / ul;
-      }
-      double am = 0.0;
-      for (int d = 0; d < 3; ++d) am += W.bounorm[ib + NB * (3 * a + d)] * W.bounorm[ib + NB * (3 * a + d)];
-      am = std::sqrt(am);
-      for (int d = 0; d < 3; ++d) {
-        Rdiff[nd + N * d] = Rdiff[nd + N * d] + am * W.wgp_b[a] * tmag * tvelo[d];
-        if (W.tauw) W.tauw[nd + N * d] = tmag * tvelo[d];
-      }
-    }
-  }
-}
 
 // mom_source_const_vect (elem_source.f90:20-55): Rmom(node) -= gpvol(a, e) s(node) over every
 // element node, in element order (the reference's atomics)

@@ -433,13 +433,14 @@ __global__ void k_seed(int64_t N, Cols5 src, const double* __restrict__ Ml, cons
 }
 
 // Ordered gather of the element-node adjoints [e][6][64] (ascending element order, like the
-// forward assembly).  Ybar = sum; out = Ybar (mode 0) or acc += Ybar (mode 1, acc = out);
-// when wnext is set: wnext = -dt (cb * ybar + ca * Ybar) / Ml.
+// forward assembly), plus extra ([5][npoin], or null); Ybar = sum; out = Ybar (mode 0) or
+// acc += Ybar (mode 1, acc = out); when wnext is set: wnext = -dt (cb * ybar + ca * Ybar) / Ml.
 __global__ void __launch_bounds__(256) k_gather_vjp(int64_t N, const int32_t* __restrict__ ptr,
                                                     const int32_t* __restrict__ idx, const double* __restrict__ el,
                                                     MCols5 out, int mode, const double* __restrict__ ybar,
                                                     const double* __restrict__ Ml, const double* __restrict__ dt,
-                                                    double cb, double ca, double* __restrict__ wnext) {
+                                                    double cb, double ca, double* __restrict__ wnext,
+                                                    const double* __restrict__ extra) {
   const int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (n >= N) return;
   double r[5] = {0, 0, 0, 0, 0};
@@ -449,6 +450,10 @@ __global__ void __launch_bounds__(256) k_gather_vjp(int64_t N, const int32_t* __
     load_res6<double>(el, (size_t)idx[c], v);
 #pragma unroll
     for (int f = 0; f < 5; ++f) r[f] += v[f];
+  }
+  if (extra) {  // the wall model's node-level adjoint
+#pragma unroll
+    for (int f = 0; f < 5; ++f) r[f] += extra[f * N + n];
   }
 #pragma unroll
   for (int f = 0; f < 5; ++f) {
@@ -488,7 +493,7 @@ __global__ void __launch_bounds__(256) k_stage_state(int64_t N, const int32_t* _
                                                      const int32_t* __restrict__ idx, const double* __restrict__ el,
                                                      const double* __restrict__ Ml, const double* __restrict__ dt,
                                                      double coef, Cols5 y, const double* __restrict__ src,
-                                                     double* __restrict__ ys) {
+                                                     const double* __restrict__ wmc, double* __restrict__ ys) {
   const int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (n >= N) return;
   double r[5] = {0, 0, 0, 0, 0};
@@ -505,6 +510,10 @@ __global__ void __launch_bounds__(256) k_stage_state(int64_t N, const int32_t* _
 #pragma unroll
     for (int d = 0; d < 3; ++d) r[1 + d] -= ml * src[d * N + n];
   }
+  if (wmc) {
+#pragma unroll
+    for (int d = 0; d < 3; ++d) r[1 + d] += wmc[d * N + n];
+  }
   const double da = (*dt) * coef;
 #pragma unroll
   for (int f = 0; f < 5; ++f) ys[f * N + n] = y.c[f][n] - da * (r[f] / ml);
@@ -518,7 +527,8 @@ __global__ void __launch_bounds__(256) k_final_pre(int64_t N, const int32_t* __r
                                                    const double* __restrict__ Ml, const double* __restrict__ dt,
                                                    Cols5 y, const double* __restrict__ Y2,
                                                    const double* __restrict__ Y3, const double* __restrict__ Y4,
-                                                   const double* __restrict__ src, double* __restrict__ zf) {
+                                                   const double* __restrict__ src, const double* __restrict__ wmc,
+                                                   double* __restrict__ zf) {
   const int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (n >= N) return;
   double r[5] = {0, 0, 0, 0, 0};
@@ -533,6 +543,10 @@ __global__ void __launch_bounds__(256) k_final_pre(int64_t N, const int32_t* __r
   if (src) {
 #pragma unroll
     for (int d = 0; d < 3; ++d) r[1 + d] -= ml * src[d * N + n];
+  }
+  if (wmc) {
+#pragma unroll
+    for (int d = 0; d < 3; ++d) r[1 + d] += wmc[d * N + n];
   }
   const double h = (*dt) / 6.0;
 #pragma unroll
@@ -606,9 +620,15 @@ int sod_rhs_vjp(SodMesh* m, const double* rho, const double* q, const double* E,
   SOD_CHECK_LAUNCH();
   rc = launch_vjp(m, rho, q, q + N, q + 2 * N, E, mu_factor, nullptr, w, st);
   if (rc) return rc;
+  const double* wmb = nullptr;
+  if (m->wmodel.nw > 0) {
+    rc = wall_model_vjp(m, rho, q, E, mu_factor, w, st);
+    if (rc) return rc;
+    wmb = m->wmodel.wmbar;
+  }
   MCols5 out{{grad_rho, grad_q, grad_q + N, grad_q + 2 * N, grad_E}};
   k_gather_vjp<<<nblk(N), 256, 0, st>>>(N, m->n2e_ptr, m->n2e, reinterpret_cast<const double*>(m->buf.rel), out, 0,
-                                         nullptr, nullptr, nullptr, 0.0, 0.0, nullptr);
+                                         nullptr, nullptr, nullptr, 0.0, 0.0, nullptr, wmb);
   SOD_CHECK_LAUNCH();
   return SOD_OK;
 }
@@ -624,10 +644,9 @@ int sod_rk4_step_vjp(SodMesh* m, const double* rho, const double* q, const doubl
   const bool bc = has_bc || has_zone;
   const bool ff = has_bc && m->bc.nff > 0;
   const bool slip = has_bc && m->bc.has_slip;
-  if (m->wmodel.nw > 0) {
-    set_error("sod_rk4_step_vjp: the wall model is not differentiated");
-    return SOD_ERR_UNSUPPORTED;
-  }
+  // wall model: its forward term in the stage residuals the adjoint rebuilds, its own adjoint in
+  // every stage's gather
+  const double* wmc = m->wmodel.nw > 0 ? m->wmodel.contrib : nullptr;
   // far-field nodes with a buffer zone: the final routine's input at the lnbn targets from the
   // stage residuals gathered there (the zone changes the stage states the reconstruction uses)
   const bool ffz = ff && has_zone;
@@ -690,6 +709,10 @@ int sod_rk4_step_vjp(SodMesh* m, const double* rho, const double* q, const doubl
     Cols5 cur = Y1;
     for (int t = 0; t < 3; ++t) {
       double* b = m->adj + (base + 5 * t) * N;
+      if (wmc) {
+        rc = wall_model_stage(m, cur.c[0], cur.c[1], cur.c[4], mu_factor, st);
+        if (rc) return rc;
+      }
       rc = launch_rhs(m, false, epb, cur.c[0], cur.c[1], cur.c[2], cur.c[3], cur.c[4], mu_factor, musgs, st);
       if (rc) return rc;
       if (slip) {
@@ -700,7 +723,8 @@ int sod_rk4_step_vjp(SodMesh* m, const double* rho, const double* q, const doubl
         rc = bc_ff_residuals(m, t + 1, rel, st);
         if (rc) return rc;
       }
-      k_stage_state<<<nblk(N), 256, 0, st>>>(N, m->n2e_ptr, m->n2e, rel, m->Ml, dt_dev, acoef[t], y0, m->source, b);
+      k_stage_state<<<nblk(N), 256, 0, st>>>(N, m->n2e_ptr, m->n2e, rel, m->Ml, dt_dev, acoef[t], y0, m->source, wmc,
+                                             b);
       SOD_CHECK_LAUNCH();
       if (bc) {
         rc = pre_stage(b, t + 2);
@@ -716,6 +740,10 @@ int sod_rk4_step_vjp(SodMesh* m, const double* rho, const double* q, const doubl
       // the stage residuals at the slip nodes / lnbn targets (the recompute gathered them already)
       for (int t = 0; t < 3; ++t) {
         const double* yt = t == 0 ? y1s : ys[t - 1];
+        if (wmc) {
+          rc = wall_model_stage(m, yt, yt + N, yt + 4 * N, mu_factor, st);
+          if (rc) return rc;
+        }
         rc = launch_rhs(m, false, epb, yt, yt + N, yt + 2 * N, yt + 3 * N, yt + 4 * N, mu_factor, musgs, st);
         if (rc) return rc;
         if (slip) {
@@ -732,6 +760,10 @@ int sod_rk4_step_vjp(SodMesh* m, const double* rho, const double* q, const doubl
     // there the stage states equal their pre-routine values, so dt R_s = (y0 - Y_{s+1}) / a_{s+1}
     // for s = 1..3); R_4 from one more RHS evaluation at Y4
     const double* y4 = ys[2];
+    if (wmc) {
+      rc = wall_model_stage(m, y4, y4 + N, y4 + 4 * N, mu_factor, st);
+      if (rc) return rc;
+    }
     rc = launch_rhs(m, false, epb, y4, y4 + N, y4 + 2 * N, y4 + 3 * N, y4 + 4 * N, mu_factor, musgs, st);
     if (rc) return rc;
     if (ffz) {
@@ -741,7 +773,7 @@ int sod_rk4_step_vjp(SodMesh* m, const double* rho, const double* q, const doubl
       if (rc) return rc;
     } else if (ff) {
       k_final_pre<<<nblk(N), 256, 0, st>>>(N, m->n2e_ptr, m->n2e, rel, m->Ml, dt_dev, y0, ys[0], ys[1], ys[2],
-                                           m->source, zf);
+                                           m->source, wmc, zf);
       SOD_CHECK_LAUNCH();
     }
     if (slip) {
@@ -784,16 +816,22 @@ int sod_rk4_step_vjp(SodMesh* m, const double* rho, const double* q, const doubl
                                            ys[stage - 2] + 3 * N, ys[stage - 2] + 4 * N}};
     rc = launch_vjp(m, ysrc.c[0], ysrc.c[1], ysrc.c[2], ysrc.c[3], ysrc.c[4], mu_factor, musgs, w, st);
     if (rc) return rc;
+    const double* wmb = nullptr;
+    if (wmc) {
+      rc = wall_model_vjp(m, ysrc.c[0], ysrc.c[1], ysrc.c[4], mu_factor, w, st);
+      if (rc) return rc;
+      wmb = m->wmodel.wmbar;
+    }
     const int t = 4 - stage;
     if (!bc) {
       k_gather_vjp<<<nblk(N), 256, 0, st>>>(N, m->n2e_ptr, m->n2e, rel, acc, 1, yb, m->Ml, dt_dev, cb[t], ca[t],
-                                             stage > 1 ? w : nullptr);
+                                             stage > 1 ? w : nullptr, wmb);
       SOD_CHECK_LAUNCH();
     } else {
       // Ybar of the post-routine stage state, through the stage routine's adjoint, then accumulated
       MCols5 yc{{Ybs, Ybs + N, Ybs + 2 * N, Ybs + 3 * N, Ybs + 4 * N}};
       k_gather_vjp<<<nblk(N), 256, 0, st>>>(N, m->n2e_ptr, m->n2e, rel, yc, 0, nullptr, nullptr, nullptr, 0.0, 0.0,
-                                             nullptr);
+                                             nullptr, wmb);
       SOD_CHECK_LAUNCH();
       const double* Ysv = stage == 1 ? y1s : ys[stage - 2];
       if (slip && stage < 4) {

@@ -296,7 +296,8 @@ __global__ void __launch_bounds__(kBlock) k_bc_slip_res(int nb, const int32_t* _
                                                         const int32_t* __restrict__ ptr,
                                                         const int32_t* __restrict__ idx,
                                                         const double* __restrict__ el, const double* __restrict__ Ml,
-                                                        const double* __restrict__ src, size_t N,
+                                                        const double* __restrict__ src,
+                                                        const double* __restrict__ wmc, size_t N,
                                                         double* __restrict__ res /*[4][nb]*/) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= nb) return;
@@ -314,6 +315,10 @@ __global__ void __launch_bounds__(kBlock) k_bc_slip_res(int nb, const int32_t* _
   if (src) {
 #pragma unroll
     for (int d = 0; d < 3; ++d) r[1 + d] -= ml * src[d * N + n];
+  }
+  if (wmc) {
+#pragma unroll
+    for (int d = 0; d < 3; ++d) r[1 + d] += wmc[d * N + n];
   }
 #pragma unroll
   for (int f = 0; f < 4; ++f) res[(size_t)f * nb + b] = r[f] / ml;
@@ -406,7 +411,8 @@ __global__ void __launch_bounds__(kBlock) k_bc_slip_push(int nb, const int32_t* 
 __global__ void __launch_bounds__(kBlock) k_bc_ff_res(int nu, const int32_t* __restrict__ target,
                                                       const int32_t* __restrict__ ptr, const int32_t* __restrict__ idx,
                                                       const double* __restrict__ el, const double* __restrict__ Ml,
-                                                      const double* __restrict__ src, size_t N,
+                                                      const double* __restrict__ src,
+                                                      const double* __restrict__ wmc, size_t N,
                                                       double* __restrict__ res /*[5][nu]*/) {
   const int u = blockIdx.x * blockDim.x + threadIdx.x;
   if (u >= nu) return;
@@ -421,6 +427,10 @@ __global__ void __launch_bounds__(kBlock) k_bc_ff_res(int nu, const int32_t* __r
   if (src) {
 #pragma unroll
     for (int d = 0; d < 3; ++d) r[1 + d] -= ml * src[d * N + n];
+  }
+  if (wmc) {
+#pragma unroll
+    for (int d = 0; d < 3; ++d) r[1 + d] += wmc[d * N + n];
   }
 #pragma unroll
   for (int f = 0; f < 5; ++f) res[(size_t)f * nu + u] = r[f] / ml;
@@ -638,7 +648,7 @@ int bc_slip_residuals(SodMesh* m, int stage, const void* rel, cudaStream_t st) {
   const BcState& B = m->bc;
   bcd::k_bc_slip_res<<<bcd::grid_of(B.nb), bcd::kBlock, 0, st>>>(
       B.nb, B.node, B.code, m->n2e_ptr, m->n2e, reinterpret_cast<const double*>(rel), m->Ml, m->source,
-      (size_t)m->npoin, B.sl_res + (size_t)(stage - 1) * 4 * B.nb);
+      m->wmodel.nw > 0 ? m->wmodel.contrib : nullptr, (size_t)m->npoin, B.sl_res + (size_t)(stage - 1) * 4 * B.nb);
   SOD_CHECK_LAUNCH();
   return SOD_OK;
 }
@@ -658,7 +668,7 @@ int bc_ff_residuals(SodMesh* m, int stage, const void* rel, cudaStream_t st) {
   const BcState& B = m->bc;
   bcd::k_bc_ff_res<<<bcd::grid_of(B.ff_nu), bcd::kBlock, 0, st>>>(
       B.ff_nu, B.ff_target, m->n2e_ptr, m->n2e, reinterpret_cast<const double*>(rel), m->Ml, m->source,
-      (size_t)m->npoin, B.ff_res + (size_t)(stage - 1) * 5 * B.ff_nu);
+      m->wmodel.nw > 0 ? m->wmodel.contrib : nullptr, (size_t)m->npoin, B.ff_res + (size_t)(stage - 1) * 5 * B.ff_nu);
   SOD_CHECK_LAUNCH();
   return SOD_OK;
 }

@@ -217,6 +217,11 @@ struct WallModelState {
   double *w = nullptr, *nrm = nullptr, *y = nullptr, *zo = nullptr;
   double *contrib = nullptr, *tauw = nullptr;
   const double* walave = nullptr;  // caller's time-averaged velocity (flag_walave), or null
+  // adjoint: targets (wall and exchange nodes) with their wall index and reading entries, the
+  // per-wall-node and per-entry contributions, and the per-node result [5][npoin] (zero elsewhere)
+  int nt = 0;
+  int32_t *tnode = nullptr, *twall = nullptr, *tptr = nullptr, *tent = nullptr;
+  double *own_bar = nullptr, *ex_bar = nullptr, *wmbar = nullptr;
 };
 
 // EOS and Sutherland viscosity of node n at the new level (time_integ.f90:445-463,
@@ -340,6 +345,9 @@ void zone_free(SodMesh* m);
 int wall_model_stage(SodMesh* m, const double* rho, const double* q0, const double* E, const double* mu_factor,
                      cudaStream_t st);
 void wall_model_free(SodMesh* m);
+// adjoint of the stage's wall-model term for seeds w ([5][npoin]) into wmodel.wmbar
+int wall_model_vjp(SodMesh* m, const double* rho, const double* q0, const double* E, const double* mu_factor,
+                   const double* w, cudaStream_t st);
 // packed-FP32 (FFMA2) variant of the mixed fused RHS kernel (sod_rhs_mixed.cu)
 int launch_rhs_mixed2(const RhsArgs& a, int epb, cudaStream_t st);
 // LES (sod_les.cu): musgs_int <- sgs_visc of the velocity u (3 columns of npoin)

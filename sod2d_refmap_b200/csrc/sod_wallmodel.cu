@@ -38,41 +38,76 @@ struct Args {
   size_t N;
 };
 
+// forward-mode dual numbers: the law's derivatives for the adjoint (through the executed
+// Newton iterations)
+struct Dual {
+  double v, d;
+};
+__device__ __forceinline__ Dual operator+(Dual a, Dual b) { return {a.v + b.v, a.d + b.d}; }
+__device__ __forceinline__ Dual operator-(Dual a, Dual b) { return {a.v - b.v, a.d - b.d}; }
+__device__ __forceinline__ Dual operator-(Dual a) { return {-a.v, -a.d}; }
+__device__ __forceinline__ Dual operator*(Dual a, Dual b) { return {a.v * b.v, a.d * b.v + a.v * b.d}; }
+__device__ __forceinline__ Dual operator/(Dual a, Dual b) { return {a.v / b.v, (a.d * b.v - a.v * b.d) / (b.v * b.v)}; }
+__device__ __forceinline__ Dual operator+(Dual a, double b) { return {a.v + b, a.d}; }
+__device__ __forceinline__ Dual operator+(double a, Dual b) { return {a + b.v, b.d}; }
+__device__ __forceinline__ Dual operator-(Dual a, double b) { return {a.v - b, a.d}; }
+__device__ __forceinline__ Dual operator-(double a, Dual b) { return {a - b.v, -b.d}; }
+__device__ __forceinline__ Dual operator*(Dual a, double b) { return {a.v * b, a.d * b}; }
+__device__ __forceinline__ Dual operator*(double a, Dual b) { return {a * b.v, a * b.d}; }
+__device__ __forceinline__ Dual operator/(Dual a, double b) { return {a.v / b, a.d / b}; }
+__device__ __forceinline__ Dual operator/(double a, Dual b) { return {a / b.v, -a * b.d / (b.v * b.v)}; }
+__device__ __forceinline__ Dual dexp(Dual a) { const double e = exp(a.v); return {e, e * a.d}; }
+__device__ __forceinline__ Dual dlog(Dual a) { return {log(a.v), a.d / a.v}; }
+__device__ __forceinline__ Dual dsqrt(Dual a) { const double s = sqrt(a.v); return {s, a.d / (2.0 * s)}; }
+__device__ __forceinline__ Dual dabs(Dual a) { return a.v < 0.0 ? -a : a; }
+__device__ __forceinline__ Dual dmin(Dual a, Dual b) { return a.v <= b.v ? a : b; }
+__device__ __forceinline__ Dual dmax(Dual a, Dual b) { return a.v >= b.v ? a : b; }
+__device__ __forceinline__ double dexp(double a) { return exp(a); }
+__device__ __forceinline__ double dlog(double a) { return log(a); }
+__device__ __forceinline__ double dsqrt(double a) { return sqrt(a); }
+__device__ __forceinline__ double dabs(double a) { return fabs(a); }
+__device__ __forceinline__ double dmin(double a, double b) { return fmin(a, b); }
+__device__ __forceinline__ double dmax(double a, double b) { return fmax(a, b); }
+__device__ __forceinline__ double val(double a) { return a; }
+__device__ __forceinline__ double val(Dual a) { return a.v; }
+
 // the wall shear magnitude of one entry (the two laws of mod_wall_model.f90)
-__device__ double shear(int type, double ul, double y, double nul, double rhol, double zo) {
+template <typename T>
+__device__ T shear(int type, T ul, double y, T nul, T rhol, double zo) {
   if (type == kABL) {
-    const double uistar = ul * 0.41 / log(1.0 + y / zo);
+    const T uistar = ul * 0.41 / dlog(T{1.0 + y / zo});
     return rhol * uistar * uistar / ul;
   }
-  double uistar;
-  if (y > 0.0 && ul > 1.0e-10) {
-    uistar = sqrt(ul * nul / y);
-    if (uistar * y / nul > 5.0) {
-      const double vkinv = 1.0 / 0.41, onovu = 1.0 / ul, xmuit = y / nul, oneoe = 1.0 / 11.0;
+  T uistar;
+  if (y > 0.0 && val(ul) > 1.0e-10) {
+    uistar = dsqrt(ul * nul / y);
+    if (val(uistar * y / nul) > 5.0) {
+      const double vkinv = 1.0 / 0.41, oneoe = 1.0 / 11.0;
+      const T onovu = 1.0 / ul, xmuit = y / nul;
       int itera = 0;
       double parco = 1.0;
       while (parco >= 1.0e-6 && itera < 100) {  // bounded: at most 100 iterations
         itera = itera + 1;
-        uistar = fmax(uistar, 0.0);
-        const double yplus = uistar * xmuit;
-        const double ypele = yplus * oneoe;
-        const double ypel2 = fmin(ypele, 20.0);
-        const double expye = exp(-ypel2);
-        const double yplu2 = fmin(yplus, 70.0);
-        const double expyt = exp(-yplu2 * 0.33);
-        const double firsl = vkinv * log(1.0 + 0.4 * yplus);
-        const double fdvfr = uistar * (firsl + 7.8 * (1.0 - expye - ypele * expyt)) - ul;
-        const double diffd = firsl + vkinv * 0.4 * yplus / (1.0 + 0.4 * yplus) +
-                             7.8 * (1.0 - expye * (1.0 - ypele) - ypele * expyt * (2.0 - yplus * 0.33));
-        const double devfr = -fdvfr / diffd;
-        parco = fabs(devfr * onovu);
+        uistar = dmax(uistar, T{0.0});
+        const T yplus = uistar * xmuit;
+        const T ypele = yplus * oneoe;
+        const T ypel2 = dmin(ypele, T{20.0});
+        const T expye = dexp(-ypel2);
+        const T yplu2 = dmin(yplus, T{70.0});
+        const T expyt = dexp(-yplu2 * 0.33);
+        const T firsl = vkinv * dlog(1.0 + 0.4 * yplus);
+        const T fdvfr = uistar * (firsl + 7.8 * (1.0 - expye - ypele * expyt)) - ul;
+        const T diffd = firsl + vkinv * 0.4 * yplus / (1.0 + 0.4 * yplus) +
+                        7.8 * (1.0 - expye * (1.0 - ypele) - ypele * expyt * (2.0 - yplus * 0.33));
+        const T devfr = -fdvfr / diffd;
+        parco = val(dabs(devfr * onovu));
         uistar = uistar + devfr;
       }
     }
   } else {
-    uistar = 0.0;
+    uistar = T{0.0};
   }
-  return (y * uistar / nul < 5.0) ? rhol * nul / y : rhol * uistar * uistar / ul;
+  return (val(y * uistar / nul) < 5.0) ? rhol * nul / y : rhol * uistar * uistar / ul;
 }
 
 // STATE: rho, q, E are a state's columns (velocity q/rho, viscosity from the EOS + Sutherland);
@@ -121,7 +156,7 @@ __global__ void __launch_bounds__(kBlock) k_wall_model(const Args a, const doubl
 #pragma unroll
     for (int d = 0; d < 3; ++d) tv[d] = uiex[d] - auxvn * nF[d];
     const double ul = sqrt(tv[0] * tv[0] + tv[1] * tv[1] + tv[2] * tv[2]);
-    const double tmag = shear(a.type, ul, a.y[k], nul, rhol, a.zo ? a.zo[k] : 1.0);
+    const double tmag = shear<double>(a.type, ul, a.y[k], nul, rhol, a.zo ? a.zo[k] : 1.0);
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
       acc[d] += a.w[k] * tmag * tv[d];
@@ -133,6 +168,112 @@ __global__ void __launch_bounds__(kBlock) k_wall_model(const Args a, const doubl
     out[n + N * d] = accumulate ? out[n + N * d] + acc[d] : acc[d];
     if (tauw) tauw[n + N * d] = last[d];
   }
+}
+
+// Adjoint of the stage's wall-model term: given the seeds w ([5][npoin], rows 1-3 weigh the
+// momentum residual), the transposed Jacobian of sum_k W_k tmag_k tv_k at wall node n with
+// respect to the stage state (rho, q, E): the node's own rows (rho through rho_l and nu_l, q and
+// E through the EOS temperature of the Sutherland viscosity) into own [5][nw], and the exchange
+// velocity q/rho of each entry into ex [4][nent] (rho, q x3; zero with walave_u).  The law's
+// derivatives with respect to ul, nu_l and rho_l come from dual numbers through its executed
+// iterations.
+__global__ void __launch_bounds__(kBlock) k_wall_model_vjp(const Args a, const double* __restrict__ rho,
+                                                           const double* __restrict__ q,
+                                                           const double* __restrict__ E,
+                                                           const double* __restrict__ mu_factor,
+                                                           const double* __restrict__ ui,
+                                                           const double* __restrict__ w, double gamma, double Rgas,
+                                                           double* __restrict__ own, double* __restrict__ ex) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= a.nw) return;
+  const size_t N = a.N, n = (size_t)a.wnode[t], NE = (size_t)a.nent, NW = (size_t)a.nw;
+  const double rhol = rho[n];
+  const double ir = 1.0 / rhol;
+  const double qn[3] = {q[n], q[n + N], q[n + 2 * N]};
+  const double q2 = qn[0] * qn[0] + qn[1] * qn[1] + qn[2] * qn[2];
+  const double u0 = qn[0] * ir, u1 = qn[1] * ir, u2 = qn[2] * ir;
+  const double p = rhol * (gamma - 1.0) * (E[n] * ir - 0.5 * (u0 * u0 + u1 * u1 + u2 * u2));
+  const double T = p / (rhol * Rgas);
+  const double mf = mu_factor[n];
+  const double mu = mf * kSuthC1 * (T * sqrt(T)) / (T + kSuthS);
+  const double dmu = mf * kSuthC1 * (1.5 * sqrt(T) * (T + kSuthS) - T * sqrt(T)) / ((T + kSuthS) * (T + kSuthS));
+  const double nul = mu / rhol;
+  const double g[3] = {w[N + n], w[2 * N + n], w[3 * N + n]};
+  double nul_b = 0.0, rhol_b = 0.0;
+  for (int k = a.wptr[t]; k < a.wptr[t + 1]; ++k) {
+    const size_t x = (size_t)a.ex[k];
+    double uiex[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) uiex[d] = ui ? ui[x + N * d] : q[x + N * d] / rho[x];
+    const double nF[3] = {a.nrm[k], a.nrm[NE + k], a.nrm[2 * NE + k]};
+    const double auxvn = nF[0] * uiex[0] + nF[1] * uiex[1] + nF[2] * uiex[2];
+    double tv[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) tv[d] = uiex[d] - auxvn * nF[d];
+    const double ul = sqrt(tv[0] * tv[0] + tv[1] * tv[1] + tv[2] * tv[2]);
+    const double zo = a.zo ? a.zo[k] : 1.0, yk = a.y[k];
+    const Dual t_ul = shear<Dual>(a.type, Dual{ul, 1.0}, yk, Dual{nul, 0.0}, Dual{rhol, 0.0}, zo);
+    const Dual t_nu = shear<Dual>(a.type, Dual{ul, 0.0}, yk, Dual{nul, 1.0}, Dual{rhol, 0.0}, zo);
+    const Dual t_rh = shear<Dual>(a.type, Dual{ul, 0.0}, yk, Dual{nul, 0.0}, Dual{rhol, 1.0}, zo);
+    const double tmag = t_ul.v;
+    const double gt = g[0] * tv[0] + g[1] * tv[1] + g[2] * tv[2];
+    const double W = a.w[k];
+    nul_b += W * gt * t_nu.d;
+    rhol_b += W * gt * t_rh.d;
+    double exb[4] = {0.0, 0.0, 0.0, 0.0};
+    if (!ui) {
+      const double gn = nF[0] * g[0] + nF[1] * g[1] + nF[2] * g[2];
+      const double c = ul > 0.0 ? t_ul.d * gt / ul : 0.0;
+      double ub[3];
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        // W P (c tv + tmag g), P = I - n n^T (P tv = tv)
+        ub[d] = W * (c * tv[d] + tmag * (g[d] - gn * nF[d]));
+      }
+      const double rx = rho[x];
+      exb[0] = -(uiex[0] * ub[0] + uiex[1] * ub[1] + uiex[2] * ub[2]) / rx;
+#pragma unroll
+      for (int d = 0; d < 3; ++d) exb[1 + d] = ub[d] / rx;
+    }
+#pragma unroll
+    for (int f = 0; f < 4; ++f) ex[(size_t)f * NE + k] = exb[f];
+  }
+  // own node: rho_l directly and through nu_l = mu(T)/rho; T = (g-1)/R (E/rho - |q|^2/(2 rho^2))
+  const double mu_b = nul_b / rhol;
+  double rho_b = rhol_b - nul_b * mu / (rhol * rhol);
+  const double T_b = mu_b * dmu;
+  const double cT = (gamma - 1.0) / Rgas;
+  const double E_b = T_b * cT / rhol;
+  rho_b += T_b * cT * (-E[n] / (rhol * rhol) + q2 / (rhol * rhol * rhol));
+  own[t] = rho_b;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) own[(1 + d) * NW + t] = -T_b * cT * qn[d] / (rhol * rhol);
+  own[4 * NW + t] = E_b;
+}
+
+// the adjoint contributions per node in a fixed order: each target (wall node or exchange node)
+// sums its own rows and the entries that read it as exchange node; wmbar is [5][npoin]
+__global__ void __launch_bounds__(kBlock) k_wall_model_bar(int nt, const int32_t* __restrict__ tnode,
+                                                           const int32_t* __restrict__ twall,
+                                                           const int32_t* __restrict__ tptr,
+                                                           const int32_t* __restrict__ tent, int nw, int nent,
+                                                           size_t N, const double* __restrict__ own,
+                                                           const double* __restrict__ ex,
+                                                           double* __restrict__ wmbar) {
+  const int u = blockIdx.x * blockDim.x + threadIdx.x;
+  if (u >= nt) return;
+  const size_t n = (size_t)tnode[u];
+  const int wi = twall[u];
+  double acc[5];
+#pragma unroll
+  for (int f = 0; f < 5; ++f) acc[f] = wi >= 0 ? own[(size_t)f * nw + wi] : 0.0;
+  for (int e = tptr[u]; e < tptr[u + 1]; ++e) {
+    const size_t k = (size_t)tent[e];
+#pragma unroll
+    for (int f = 0; f < 4; ++f) acc[f] += ex[(size_t)f * nent + k];
+  }
+#pragma unroll
+  for (int f = 0; f < 5; ++f) wmbar[f * N + n] = acc[f];
 }
 
 static Args args_of(const SodMesh* m) {
@@ -163,9 +304,22 @@ int wall_model_stage(SodMesh* m, const double* rho, const double* q0, const doub
   return SOD_OK;
 }
 
+int wall_model_vjp(SodMesh* m, const double* rho, const double* q0, const double* E, const double* mu_factor,
+                   const double* w, cudaStream_t st) {
+  const WallModelState& W = m->wmodel;
+  wm::k_wall_model_vjp<<<(W.nw + wm::kBlock - 1) / wm::kBlock, wm::kBlock, 0, st>>>(
+      wm::args_of(m), rho, q0, E, mu_factor, W.walave, w, m->prm.gamma, m->prm.Rgas, W.own_bar, W.ex_bar);
+  SOD_CHECK_LAUNCH();
+  wm::k_wall_model_bar<<<(W.nt + wm::kBlock - 1) / wm::kBlock, wm::kBlock, 0, st>>>(
+      W.nt, W.tnode, W.twall, W.tptr, W.tent, W.nw, W.nent, (size_t)m->npoin, W.own_bar, W.ex_bar, W.wmbar);
+  SOD_CHECK_LAUNCH();
+  return SOD_OK;
+}
+
 void wall_model_free(SodMesh* m) {
   WallModelState& W = m->wmodel;
-  void* ptrs[] = {W.wnode, W.wptr, W.ex, W.w, W.nrm, W.y, W.zo, W.contrib, W.tauw};
+  void* ptrs[] = {W.wnode, W.wptr, W.ex, W.w, W.nrm, W.y, W.zo, W.contrib, W.tauw,
+                  W.tnode, W.twall, W.tptr, W.tent, W.own_bar, W.ex_bar, W.wmbar};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   W = WallModelState{};
@@ -283,6 +437,42 @@ int sod_mesh_set_wall_model(SodMesh* m, int32_t type, int32_t nboun, int32_t npb
     set_error("sod_mesh_set_wall_model: device allocation failed");
     return SOD_ERR_NOMEM;
   }
+  // adjoint targets: wall nodes and exchange nodes (ascending), with the entries reading each
+  // target as exchange node
+  std::vector<int32_t> tnode, twall, tptr, tent;
+  {
+    std::vector<std::pair<int32_t, int32_t>> xe;  // (exchange node, entry)
+    for (size_t k = 0; k < ne; ++k) xe.emplace_back(ex[k], (int32_t)k);
+    std::sort(xe.begin(), xe.end());
+    std::vector<int32_t> all(wnode.begin(), wnode.end());
+    for (auto& p : xe) all.push_back(p.first);
+    std::sort(all.begin(), all.end());
+    all.erase(std::unique(all.begin(), all.end()), all.end());
+    size_t xi = 0;
+    for (int32_t nd : all) {
+      auto it = std::lower_bound(wnode.begin(), wnode.end(), nd);
+      tnode.push_back(nd);
+      twall.push_back(it != wnode.end() && *it == nd ? (int32_t)(it - wnode.begin()) : -1);
+      tptr.push_back((int32_t)tent.size());
+      while (xi < xe.size() && xe[xi].first == nd) tent.push_back(xe[xi++].second);
+    }
+    tptr.push_back((int32_t)tent.size());
+  }
+  const size_t nt = tnode.size();
+  if (!(alloc((void**)&W.tnode, sizeof(int32_t) * nt) && alloc((void**)&W.twall, sizeof(int32_t) * nt) &&
+        alloc((void**)&W.tptr, sizeof(int32_t) * (nt + 1)) && alloc((void**)&W.tent, sizeof(int32_t) * (ne + 1)) &&
+        alloc((void**)&W.own_bar, sizeof(double) * 5 * nw) && alloc((void**)&W.ex_bar, sizeof(double) * 4 * ne) &&
+        alloc((void**)&W.wmbar, sizeof(double) * 5 * (size_t)N))) {
+    wall_model_free(m);
+    set_error("sod_mesh_set_wall_model: device allocation failed");
+    return SOD_ERR_NOMEM;
+  }
+  SOD_CUDA(cudaMemcpy(W.tnode, tnode.data(), sizeof(int32_t) * nt, cudaMemcpyHostToDevice));
+  SOD_CUDA(cudaMemcpy(W.twall, twall.data(), sizeof(int32_t) * nt, cudaMemcpyHostToDevice));
+  SOD_CUDA(cudaMemcpy(W.tptr, tptr.data(), sizeof(int32_t) * (nt + 1), cudaMemcpyHostToDevice));
+  if (!tent.empty()) SOD_CUDA(cudaMemcpy(W.tent, tent.data(), sizeof(int32_t) * tent.size(), cudaMemcpyHostToDevice));
+  SOD_CUDA(cudaMemset(W.wmbar, 0, sizeof(double) * 5 * (size_t)N));
+  W.nt = (int)nt;
   W.nw = (int)nw;
   W.nent = (int)ne;
   W.type = type;

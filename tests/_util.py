@@ -36,7 +36,7 @@ def oracle_bc_jvp_map(oracle, bnd):
     return J
 
 
-def oracle_step_jvp(oracle, om, prm, st, dt, v, mu_sgs=None, bc=None, bc_jvp=None):
+def oracle_step_jvp(oracle, om, prm, st, dt, v, mu_sgs=None, bc=None, bc_jvp=None, wall=None):
     """One rk_4_main step (time_integ.f90:288-426) from the FlowState st and its JVP along
     v = (drho, dq (npoin,3), dE), composed from the oracle's dual-number stage JVPs with mu_e
     (and mu_sgs) frozen.  bc (oracle_bc_map) selects the non-periodic path: the routine on every
@@ -75,7 +75,7 @@ def oracle_step_jvp(oracle, om, prm, st, dt, v, mu_sgs=None, bc=None, bc_jvp=Non
     a_next = [0.5, 0.5, 1.0, None]
     b = [1 / 6, 1 / 3, 1 / 3, 1 / 6]
     for s in range(4):
-        R, dR = oracle.rhs_jvp(om, prm, with_state(*ys), vs[0], vs[1], vs[2], mu_sgs=mu_sgs)
+        R, dR = oracle.rhs_jvp(om, prm, with_state(*ys), vs[0], vs[1], vs[2], mu_sgs=mu_sgs, wall=wall)
         Rc = (R[0], np.asfortranarray(R[1:4].T), R[4])
         dRc = (dR[0], np.asfortranarray(dR[1:4].T), dR[4])
         for f in range(3):
