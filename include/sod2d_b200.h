@@ -189,7 +189,8 @@ int sod_mesh_set_wall_model(SodMesh* mesh, int32_t type, int32_t nboun, int32_t 
  * (npoin); tauw (npoin,3) receives tmag * tvelo, or may be null. */
 int sod_wall_model(SodMesh* mesh, const double* rho, const double* u, const double* mu_fluid, double* Rdiff,
                    double* tauw, sod_stream_t stream);
-/* tauw of the last stage the step evaluated the wall model on (device (npoin,3)). */
+/* tauw of the last evaluation of the wall model inside the library: a step's last stage, or the
+ * forward recompute of a step adjoint (device (npoin,3)). */
 int sod_wall_model_tauw(SodMesh* mesh, double* tauw, sod_stream_t stream);
 
 /* Device-resident solver state in the reference's array layouts (level pos=2 only).
