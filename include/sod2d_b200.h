@@ -312,7 +312,9 @@ int sod_sutherland_viscosity(int32_t npoin, const double* Tem, const double* mu_
  * SOD_NOALLOC_MAX_ELEM elements and 64*SOD_NOALLOC_MAX_ELEM nodes (larger: SOD_ERR_ARG).
  * All calls share that array: calls that overlap on the GPU race.  The first call on a
  * device looks up the array's address; make it before any stream capture.  The call waits
- * for its stream to finish so it can report bad node ids. */
+ * for its stream to finish (bounded by sod_set_wait_timeout) so it can report bad node ids
+ * (SOD_ERR_ARG); on a stream that is capturing it enqueues nothing and returns
+ * SOD_ERR_UNSUPPORTED, since that wait is not allowed there. */
 #define SOD_NOALLOC_MAX_ELEM 4096
 int sod_full_convec_ijk_noalloc(int32_t nelem, int32_t npoin, int32_t index_base, const int32_t* connec,
                                 const double* He, const double* gpvol, const double* dlxigp_ip,

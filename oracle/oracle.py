@@ -385,6 +385,17 @@ def rhs_stage(om: OracleMesh, prm, st, mu_e=None):
     return R.reshape(5, om.npoin)
 
 
+def rhs_stage_ld(om: OracleMesh, prm, st, mu_e=None):
+    """rhs_stage evaluated in x87 extended precision (64-bit significand), rounded to FP64:
+    the reference value against which FP64 rounding is measured."""
+    P = params_of(prm)
+    R = np.zeros(5 * om.npoin)
+    mue = np.asfortranarray(st.mu_e if mu_e is None else mu_e)
+    lib().oracle_rhs_stage_ld(C.byref(om.ctx), C.byref(P), ptr(om.Ml), ptr(st.mu_factor), ptr(mue), None,
+                              ptr(st.rho), ptr(np.asfortranarray(st.q)), ptr(st.E), ptr(R))
+    return R.reshape(5, om.npoin)
+
+
 def rhs_opcount(om: OracleMesh, prm, st, mu_e=None) -> float:
     """Arithmetic operations of one stage RHS evaluation (reference formulation, whole mesh)."""
     P = params_of(prm)

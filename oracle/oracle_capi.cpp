@@ -197,6 +197,19 @@ void oracle_rhs_stage(const ElemCtx* ctx, const Params* P, const double* Ml, con
   rhs_stage_t<double>(*ctx, *P, Ml, mu_factor, mu_e, mu_sgs, rho, q, E, R);
 }
 
+// oracle_rhs_stage evaluated in x87 extended precision (inputs and outputs FP64): the rounding
+// floor against which the FP64 evaluations are measured on ill-conditioned residuals.
+void oracle_rhs_stage_ld(const ElemCtx* ctx, const Params* P, const double* Ml, const double* mu_factor,
+                         const double* mu_e, const double* mu_sgs, const double* rho, const double* q,
+                         const double* E, double* R) {
+  const int64_t N = ctx->npoin;
+  std::vector<double> zeros;
+  if (!mu_sgs) { zeros.assign((size_t)ctx->nelem * nnode, 0.0); mu_sgs = zeros.data(); }
+  std::vector<long double> r(rho, rho + N), qq(q, q + 3 * N), e(E, E + N), out(5 * N);
+  rhs_stage_t<long double>(*ctx, *P, Ml, mu_factor, mu_e, mu_sgs, r.data(), qq.data(), e.data(), out.data());
+  for (int64_t p = 0; p < 5 * N; ++p) R[p] = (double)out[p];
+}
+
 // Exact JVP of oracle_rhs_stage by forward-mode dual numbers: dR = (dR/dU) dU, U = (rho,q,E).
 void oracle_rhs_jvp(const ElemCtx* ctx, const Params* P, const double* Ml, const double* mu_factor,
                     const double* mu_e, const double* mu_sgs, const double* rho, const double* q, const double* E,

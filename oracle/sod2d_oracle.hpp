@@ -816,6 +816,14 @@ inline double sqrt(double a) { return std::sqrt(a); }
 inline double pow(double a, double e) { return std::pow(a, e); }
 inline double value(double a) { return a; }
 inline double value(Dual a) { return a.v; }
+// x87 extended precision (64-bit significand): a reference evaluation of the same formulas
+// whose own rounding is 2^11 times below FP64's, to measure FP64 rounding of a result
+inline long double sqrt(long double a) { return std::sqrt(a); }
+inline long double pow(long double a, double e) { return std::pow(a, (long double)e); }
+inline long double log(long double a) { return std::log(a); }
+inline long double exp(long double a) { return std::exp(a); }
+inline long double fabs(long double a) { return std::fabs(a); }
+inline double value(long double a) { return (double)a; }
 
 // Operation counter: a double that counts every +, -, *, / (and sqrt, pow as one operation
 // each) applied to it, to give the reference formulation's algorithmic operation count.

@@ -16,7 +16,9 @@
 //     streams or host threads at the same time) race on it and give wrong results;
 //   * the first call on a device looks up the array's device address (cudaGetSymbolAddress) with
 //     that device current and caches it; make that first call before any stream capture;
-//   * the call waits for its own stream to finish so that it can report out-of-range node ids.
+//   * the call waits for its own stream to finish (within sod_set_wait_timeout's limit) so that it
+//     can report out-of-range node ids; a wait is not allowed on a stream that is capturing, so on
+//     such a stream the call returns SOD_ERR_UNSUPPORTED before it enqueues anything.
 #include "sod_internal.cuh"
 #include <mutex>
 
@@ -287,10 +289,17 @@ extern "C" int sod_full_convec_ijk_noalloc(int32_t nelem, int32_t npoin, int32_t
               kMaxElem, kMaxPoin, nelem, npoin);
     return SOD_ERR_ARG;
   }
+  cudaStream_t st = (cudaStream_t)stream;
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  SOD_CUDA(cudaStreamIsCapturing(st, &cap));
+  if (cap != cudaStreamCaptureStatusNone) {
+    set_error("sod_full_convec_ijk_noalloc waits for its stream to report bad node ids, which a capturing "
+              "stream does not allow");
+    return SOD_ERR_UNSUPPORTED;
+  }
   unsigned char* base = nullptr;
   int rc = scratch_address(&base);
   if (rc) return rc;
-  cudaStream_t st = (cudaStream_t)stream;
   View v = carve(base);
   const int64_t nen = (int64_t)nelem * NN;
   const int gb = (int)((nen + 255) / 256);
@@ -312,9 +321,10 @@ extern "C" int sod_full_convec_ijk_noalloc(int32_t nelem, int32_t npoin, int32_t
   SOD_CHECK_LAUNCH();
   k_gather<<<(npoin + 255) / 256, 256, 0, st>>>(v, npoin, Rmass, Rmom, Rener);
   SOD_CHECK_LAUNCH();
+  // bounded wait (sod_set_wait_timeout), then a plain read of the flag once the work is done
+  if ((rc = sync_stream(st))) return rc;
   int32_t hflag = 0;
-  SOD_CUDA(cudaMemcpyAsync(&hflag, v.flag, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
-  SOD_CUDA(cudaStreamSynchronize(st));
+  SOD_CUDA(cudaMemcpy(&hflag, v.flag, sizeof(int32_t), cudaMemcpyDeviceToHost));
   if (hflag & 1) {
     set_error("invalid argument: connec holds node ids outside [%d, %d)", index_base, index_base + npoin);
     return SOD_ERR_ARG;

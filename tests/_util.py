@@ -88,3 +88,41 @@ def oracle_step_jvp(oracle, om, prm, st, dt, v, mu_sgs=None, bc=None, bc_jvp=Non
         uread[0], uread[1] = vel(y0, v)
         acc_y, acc_v = (list(t) for t in bmap(acc_y, acc_v))
     return acc_y, acc_v
+
+
+def slab_oracle(oracle, M, m, layers):
+    """The oracle on the first `layers` element layers in z of the periodic box m: returns the
+    oracle mesh, the slab's global node ids (slab-local id -> global id), its element count and
+    the slab-local ids of the nodes whose elements all lie in the slab."""
+    n = m.n
+    E = n * n * layers
+    conn = np.asarray(m.connec[:E], dtype=np.int64)
+    nodes, inv = np.unique(conn, return_inverse=True)
+    sub = M.BoxMesh(n=n, L=m.L, nelem=E, npoin=len(nodes), npoin_orig=m.npoin_orig,
+                    connec=np.asfortranarray(inv.reshape(E, 64).astype(np.int32)),
+                    connec_orig=np.asfortranarray(m.connec_orig[:E]), coord=np.asfortranarray(m.coord[nodes]),
+                    coord_orig=m.coord_orig, master=m.master, tables=m.tables)
+    om = oracle.OracleMesh(sub, colour=False)
+    # race-free parallel scatter: colour classes by element parity in x, y, z
+    e = np.arange(E)
+    col = (e % n % 2) + 2 * ((e // n) % n % 2) + 4 * ((e // (n * n)) % 2)
+    om.cptr = np.concatenate([[0], np.cumsum(np.bincount(col, minlength=8))]).astype(np.int32)
+    om.celems = np.argsort(col, kind="stable").astype(np.int32)
+    om.ctx.ncolors = 8
+    om.ctx.color_ptr = oracle.ptr(om.cptr).value
+    om.ctx.color_elems = oracle.ptr(om.celems).value
+    mm = 3 * n
+    kplane = nodes // (mm * mm)
+    interior = np.flatnonzero((kplane >= 1) & (kplane <= 3 * layers - 1))
+    return om, nodes, E, interior
+
+
+def slab_state(st, nodes, E, mu_e=None):
+    s = st.copy()
+    for k in ("rho", "E", "pr", "Tem", "e_int", "eta", "csound", "machno", "mu_fluid", "mu_factor"):
+        setattr(s, k, np.ascontiguousarray(getattr(st, k)[nodes]))
+    s.u = np.asfortranarray(st.u[nodes])
+    s.q = np.asfortranarray(st.q[nodes])
+    s.mu_e = np.asfortranarray(np.zeros((E, 64)) if mu_e is None else mu_e[:E])
+    s.mu_sgs = np.zeros((E, 64), order="F")
+    return s

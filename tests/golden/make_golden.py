@@ -1,7 +1,8 @@
 """Extract the known-answer data of the reference's own unit tests into reference_kats.json.
 
-Run in a checkout that has the SOD2D sources (default path below or $SOD2D_REF); the JSON it
-writes is committed so the tests need no reference tree at run time.
+Run with the SOD2D source tree as the argument (or in $SOD2D_REF):
+    python tests/golden/make_golden.py <path to the SOD2D checkout>
+The JSON it writes is committed so the tests need no reference tree at run time.
 
   unitt/unitt_CSR_SPMV_scal/unitt_CSR_SPMV_scal.f90:14-52      CSR matrix, vector, sum(u) = 252
   unitt/unitt_3d_jacobian_inverse/unitt_3d_jacobian_inverse.f90:11-38  TET4 elcod/dN, det(He)=0.0625
@@ -19,7 +20,7 @@ import os
 import re
 import sys
 
-REF = os.environ.get("SOD2D_REF", "/root/reference")
+REF = ""  # the SOD2D checkout, set by main() from argv[1] or $SOD2D_REF
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "reference_kats.json")
 
 
@@ -104,6 +105,11 @@ def legacy_expected(name, case):
 
 
 def main():
+    global REF
+    REF = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("SOD2D_REF", "")
+    if not REF or not os.path.isdir(os.path.join(REF, "unitt")):
+        sys.stderr.write("usage: make_golden.py <SOD2D checkout with unitt/> (or set SOD2D_REF)\n")
+        return 2
     rd = lambda p: open(os.path.join(REF, p)).read()
     kats = {}
     s = rd("unitt/unitt_CSR_SPMV_scal/unitt_CSR_SPMV_scal.f90")

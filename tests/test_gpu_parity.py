@@ -173,8 +173,11 @@ def test_mixed_precision_error(env, oracle):
     r32 = gm.rhs(s, precision=S.MIXED)
     errs = {k: rel_l2(t2n(r32[k]), t2n(r64[k])) for k in r64}
     print("mixed RHS rel L2:", errs)
+    # 5e-6 on this 4^3 box (measured <= 2.2e-6): an element spans 1.6 rad of the vortex, so the
+    # second-order remainder the mixed kernel rounds to FP32 is far larger relative to the fields
+    # than on the 64^3 benchmark mesh, where the 1e-6 bound is checked (test_gpu_configs.py)
     for k, e in errs.items():
-        assert e < 1e-3, (k, e)
+        assert e < 5e-6, (k, e)
     a = S.Sod2dState.from_host(env["st0"], gm.nelem); a.dt.fill_(env["dt"])
     b = S.Sod2dState.from_host(env["st0"], gm.nelem); b.dt.fill_(env["dt"])
     gm.rk4_steps(a, 10, precision=S.FP64)
