@@ -73,7 +73,8 @@ void sod_params_default(SodParams* p);
  * char_length mod_geom.f90:13-37, char_length_spectral mod_geom.f90:39-66). */
 typedef struct {
   int32_t nelem;             /* elements                                                 */
-  int32_t npoin;             /* working (unique) nodes: rows of the state arrays         */
+  int32_t npoin;             /* rows of the state arrays (unique nodes, or every lattice
+                                point with periodic slave rows when lpoin_w is given)    */
   int32_t npoin_orig;        /* rows of coord_orig (nodes incl. periodic images)         */
   int32_t porder;            /* must be 3                                                */
   int32_t index_base;        /* 0 or 1                                                   */
@@ -91,6 +92,15 @@ typedef struct {
   const double* Ml;          /* (npoin)        optional                                  */
   const double* helem;       /* (nelem)        optional                                  */
   const double* helem_l;     /* (nelem,64)     optional                                  */
+  /* Working nodes of rk_4_main's node loops (npoin_w, lpoin_w(npoin_w): workingNodesPar,
+   * mod_mpi_mesh.f90:25-28; time_integ.f90:147,267-285,445-471).  lpoin_w = null: every row
+   * works.  Otherwise the rows not listed are periodic slaves, as in SOD2D's mesh arrays
+   * (coordPar with every lattice point, connecParWork with each image replaced by its master):
+   * connec must reference exactly the listed rows, every step leaves the slave rows of the
+   * state untouched (their mu_fluid is re-evaluated from their Tem, as sutherland_viscosity
+   * runs over all npoin), and the entropy normalisation averages over the listed rows. */
+  int32_t npoin_w;
+  const int32_t* lpoin_w;    /* (npoin_w) index_base applies                             */
 } SodMeshDesc;
 
 typedef struct SodMesh SodMesh;
@@ -253,7 +263,9 @@ int sod_compute_field_derivs(SodMesh* mesh, const double* rho, const double* u, 
 
 /* Host-buffer variant of sod_rk4_main for the CPU-side drop-in (the reference's CPU build
  * calls rk_4_main on host arrays): copies rho,q,E,mu_e,mu_factor in, runs one step and copies
- * rho,q,E,u,pr,Tem,e_int,eta,csound,machno,mu_fluid,mu_e back.  dt_host in, dt_next_host out. */
+ * rho,q,E,u,pr,Tem,e_int,eta,csound,machno,mu_fluid,mu_e back.  dt_host in, dt_next_host out.
+ * On a mesh with periodic slave rows (lpoin_w) the fields it copies back are also copied in, so
+ * that their slave rows come back as they were. */
 int sod_rk4_main_host(SodMesh* mesh, SodState* host_state, double dt_host, double* dt_next_host,
                       SodPrecision prec, sod_stream_t stream);
 
@@ -299,6 +311,57 @@ int sod_lumped_solver(SodMesh* mesh, double* R, int ncomp, sod_stream_t stream);
 /* sutherland_viscosity (mod_fluid_viscosity.f90:21-41). */
 int sod_sutherland_viscosity(int32_t npoin, const double* Tem, const double* mu_factor,
                              double* mu_fluid, sod_stream_t stream);
+
+/* ---- The same routines with the reference's complete argument lists ---------------------
+ * full_convec_ijk (elem_convec.f90:211-224), full_convec_ijk_H (:20-33),
+ * generic_scalar_convec_ijk (:462-476), full_diffusion_ijk (elem_diffu.f90:12-25) and
+ * smart_visc_spectral (mod_entropy_viscosity.f90:14-28): every argument of the Fortran
+ * subroutine, in its order and layout, as a device pointer (the arrays SOD2D keeps resident),
+ * with one addition, index_base, after npoin (1 for Fortran callers).  The mesh travels with
+ * each call, as in the reference: the call builds a transient device view of it (element-major
+ * connectivity and geometry, the ordered node->element gather map sorted on the device), runs
+ * the handle-based routine's kernels on it (the results equal those of the entry points above
+ * bit for bit), waits for the stream and releases the view.  It allocates per call; a time loop
+ * creates a SodMesh once instead.  Arguments the routine does not read (Ngp, dNgp, xgp; Ml in
+ * full_diffusion_ijk; Ngp, coord, dNgp, Ml and the scratch mue_l in smart_visc_spectral) are
+ * accepted and ignored.  invAtoIJK, when given, must invert gmshAtoI/J/K (SOD_ERR_ARG otherwise);
+ * node ids outside [index_base, index_base + npoin) give SOD_ERR_ARG.  smart_visc_spectral reads
+ * the module variables of mod_numerical_params (ce, cmax, cglob, c_rho, c_ener,
+ * flag_normalise_entropy) and nscbc_Rgas_inf from params (null: defaults); its lpoin_w must
+ * list exactly the nodes connec references. */
+int sod_full_convec_ijk_ref(int32_t nelem, int32_t npoin, int32_t index_base, const int32_t* connec,
+                            const double* Ngp, const double* dNgp, const double* He, const double* gpvol,
+                            const double* dlxigp_ip, const double* xgp, const int32_t* invAtoIJK,
+                            const int32_t* gmshAtoI, const int32_t* gmshAtoJ, const int32_t* gmshAtoK,
+                            const double* u, const double* q, const double* rho, const double* pr, const double* E,
+                            double* Rmass, double* Rmom, double* Rener, sod_stream_t stream);
+int sod_full_convec_ijk_H_ref(int32_t nelem, int32_t npoin, int32_t index_base, const int32_t* connec,
+                              const double* Ngp, const double* dNgp, const double* He, const double* gpvol,
+                              const double* dlxigp_ip, const double* xgp, const int32_t* invAtoIJK,
+                              const int32_t* gmshAtoI, const int32_t* gmshAtoJ, const int32_t* gmshAtoK,
+                              const double* u, const double* q, const double* rho, const double* pr, const double* E,
+                              double* Rmass, double* Rmom, double* Rener, sod_stream_t stream);
+int sod_generic_scalar_convec_ijk_ref(int32_t nelem, int32_t npoin, int32_t index_base, const int32_t* connec,
+                                      const double* Ngp, const double* dNgp, const double* He, const double* gpvol,
+                                      const double* dlxigp_ip, const double* xgp, const int32_t* invAtoIJK,
+                                      const int32_t* gmshAtoI, const int32_t* gmshAtoJ, const int32_t* gmshAtoK,
+                                      const double* q, const double* eta, const double* u, double* Rconvec,
+                                      sod_stream_t stream);
+int sod_full_diffusion_ijk_ref(int32_t nelem, int32_t npoin, int32_t index_base, const int32_t* connec,
+                               const double* Ngp, const double* He, const double* gpvol, const double* dlxigp_ip,
+                               const int32_t* invAtoIJK, const int32_t* gmshAtoI, const int32_t* gmshAtoJ,
+                               const int32_t* gmshAtoK, double Cp, double Pr, const double* rho_n, const double* rho,
+                               const double* u, const double* Tem, const double* mu_fluid, const double* mu_e,
+                               const double* mu_sgs, const double* Ml, double* Rmass, double* Rmom, double* Rener,
+                               sod_stream_t stream);
+int sod_smart_visc_spectral_ref(int32_t nelem, int32_t npoin, int32_t npoin_w, int32_t index_base,
+                                const int32_t* connec, const int32_t* lpoin_w, const double* Reta, const double* Ngp,
+                                const double* coord, const double* dNgp, const double* gpvol, const double* wgp,
+                                double gamma_gas, const double* rho, const double* u, const double* csound,
+                                const double* Tem, const double* eta, const double* helem_l, const double* helem,
+                                const double* Ml, double* mu_e, const int32_t* invAtoIJK, const int32_t* gmshAtoI,
+                                const int32_t* gmshAtoJ, const int32_t* gmshAtoK, double* mue_l,
+                                const SodParams* params, sod_stream_t stream);
 
 /* Allocation-free full_convec_ijk, for callers that cannot allocate device memory: host codes
  * whose device memory is owned by the OpenACC runtime or by their own fixed pool (as SOD2D's

@@ -21,7 +21,8 @@ _i32p = C.POINTER(C.c_int32)
 class ElemCtx(C.Structure):
     _fields_ = [("nelem", C.c_int), ("npoin", C.c_int), ("connec", _p), ("He", _p), ("gpvol", _p),
                 ("dlxigp_ip", _p), ("invAtoIJK", _p), ("gmshAtoI", _p), ("gmshAtoJ", _p),
-                ("gmshAtoK", _p), ("ncolors", C.c_int), ("color_ptr", _p), ("color_elems", _p)]
+                ("gmshAtoK", _p), ("ncolors", C.c_int), ("color_ptr", _p), ("color_elems", _p),
+                ("npoin_w", C.c_int), ("lpoin_w", _p)]
 
 
 class Params(C.Structure):
@@ -207,10 +208,13 @@ class OracleMesh:
         else:
             self.cptr, self.celems = np.zeros(1, np.int32), np.zeros(1, np.int32)
             ncol = 0
+        lw = mesh.extra.get("lpoin_w") if getattr(mesh, "extra", None) else None
+        self.lpoin_w = None if lw is None else np.ascontiguousarray(lw, dtype=np.int32)
         self.ctx = ElemCtx(self.nelem, self.npoin, ptr(self.connec).value, ptr(self.He).value,
                            ptr(self.gpvol).value, ptr(self.dlxigp_ip).value, ptr(self.invAtoIJK).value,
                            ptr(self.gI).value, ptr(self.gJ).value, ptr(self.gK).value, ncol,
-                           ptr(self.cptr).value, ptr(self.celems).value)
+                           ptr(self.cptr).value, ptr(self.celems).value,
+                           0 if lw is None else len(self.lpoin_w), 0 if lw is None else ptr(self.lpoin_w).value)
 
 
 def params_of(prm) -> Params:

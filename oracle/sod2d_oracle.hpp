@@ -357,7 +357,16 @@ struct ElemCtx {
   int ncolors;
   const int32_t* color_ptr;
   const int32_t* color_elems;
+  // working nodes lpoin_w(npoin_w) (workingNodesPar, mod_mpi_mesh.f90:25-28), 0-based; null:
+  // every node works.  Rows outside the list are periodic slaves: rk_4_main's node loops over
+  // lpoin_w (EOS, lumped solve, entropy residual, normalisation) never touch them.
+  int npoin_w;
+  const int32_t* lpoin_w;
 };
+
+// number of working nodes and the w-th of them
+inline int n_working(const ElemCtx& c) { return c.lpoin_w ? c.npoin_w : c.npoin; }
+inline int working(const ElemCtx& c, int w) { return c.lpoin_w ? c.lpoin_w[w] : w; }
 
 #define SOD_INV(i, j, k) (ctx.invAtoIJK[(i) + 4 * ((j) + 4 * (k))])
 #define SOD_DL(g, d, ii) (ctx.dlxigp_ip[(g) + ngaus * ((d) + 3 * (ii))])
@@ -1220,7 +1229,8 @@ inline void rhs_stage_t(const ElemCtx& ctx, const Params& P, const double* Ml, c
   const int64_t N = npoin;
   const double g = P.gamma_gas, Rgas = P.Rgas;
   std::vector<T> u(3 * N), pr(N), h(N), Tem(N), muf(N), Rm(N), Rmo(3 * N), Re(N), Dm(N), Dmo(3 * N), De(N);
-  for (int p = 0; p < npoin; ++p) {
+  for (int w = 0; w < n_working(ctx); ++w) {  // EOS over lpoin_w (time_integ.f90:267-285)
+    const int p = working(ctx, w);
     T umag = T(0.0);
     for (int d = 0; d < 3; ++d) {
       u[p + N * d] = q[p + N * d] / rho[p];
@@ -1245,7 +1255,9 @@ inline void rhs_stage_t(const ElemCtx& ctx, const Params& P, const double* Ml, c
     full_convec_ijk_H<T>(ctx, u.data(), q, rho, pr.data(), E, Rm.data(), Rmo.data(), Re.data());
   else
     full_convec_ijk_t<T>(ctx, u.data(), q, rho, pr.data(), h.data(), Rm.data(), Rmo.data(), Re.data());
-  for (int p = 0; p < npoin; ++p) {
+  for (int64_t p = 0; p < 5 * N; ++p) R[p] = 0.0;
+  for (int w = 0; w < n_working(ctx); ++w) {  // lumped_solver over lpoin_w (mod_solver.f90:23-58)
+    const int p = working(ctx, w);
     R[p] = (Rm[p] + Dm[p]) / Ml[p];
     for (int d = 0; d < 3; ++d) R[p + N * (1 + d)] = (Rmo[p + N * d] + Dmo[p + N * d]) / Ml[p];
     R[p + N * 4] = (Re[p] + De[p]) / Ml[p];
@@ -1265,12 +1277,13 @@ inline void smart_visc_spectral(const ElemCtx& ctx, const Params& P, const doubl
   const double v_pi = 2.0 * std::asin(1.0);
   for (int64_t q = 0; q < (int64_t)nelem * nnode; ++q) mue_l[q] = mu_e[q];
   double norm;
-  if (P.flag_normalise_entropy == 1) {
+  if (P.flag_normalise_entropy == 1) {  // over lpoin_w (mod_entropy_viscosity.f90:43-62)
+    const int nw = n_working(ctx);
     double maxEta_r = 0.0;
-    for (int p = 0; p < npoin; ++p) maxEta_r = maxEta_r + eta[p];
-    double maxEta = maxEta_r / (double)npoin;
+    for (int w = 0; w < nw; ++w) maxEta_r = maxEta_r + eta[working(ctx, w)];
+    double maxEta = maxEta_r / (double)nw;
     double norm_r = 0.0;
-    for (int p = 0; p < npoin; ++p) norm_r = std::max(norm_r, std::fabs(eta[p] - maxEta));
+    for (int w = 0; w < nw; ++w) norm_r = std::max(norm_r, std::fabs(eta[working(ctx, w)] - maxEta));
     norm = norm_r;
   } else {
     norm = 1.0;
@@ -1579,11 +1592,14 @@ struct BufferData {
 
 // updateBuffer (time_integ.f90:510-589) over every node: xi = 1, lowered by each enabled zone
 // that holds the node, then q, E and rho relaxed towards their free-stream values
-inline void update_buffer(int npoin, const BufferData& B, double* rho, double* q, double* E) {
+inline void update_buffer(int npoin, const BufferData& B, double* rho, double* q, double* E, int npoin_w = -1,
+                          const int32_t* lpoin_w = nullptr) {
   const int64_t N = npoin;
   const double c1 = 0.01, c2 = 10.0;
   const double E_inf = (B.rho_inf * 0.5 * (B.u_inf * B.u_inf) + B.p_inf / (B.gamma_inf - 1.0));
-  for (int64_t p = 0; p < N; ++p) {
+  const int64_t nw = lpoin_w ? npoin_w : N;
+  for (int64_t w = 0; w < nw; ++w) {  // over lpoin_w (time_integ.f90:529)
+    const int64_t p = lpoin_w ? lpoin_w[w] : w;
     double xi = 1.0;
     for (int f = 0; f < 6; ++f) {
       if (!B.on[f]) continue;
@@ -1741,13 +1757,15 @@ inline void rk_4_main(const ElemCtx& ctx, const Params& P, const double* Ml, con
       for (int d = 0; d < 3; ++d)
         W.aux_q[p + (int64_t)npoin * d] = S.q[p + (int64_t)npoin * d] - dt * a_i[istep] * W.Rmom[p + (int64_t)npoin * d];
     }
-    if (buf) update_buffer(npoin, *buf, W.aux_rho.data(), W.aux_q.data(), W.aux_E.data());  // time_integ.f90:251
+    if (buf)  // time_integ.f90:251
+      update_buffer(npoin, *buf, W.aux_rho.data(), W.aux_q.data(), W.aux_E.data(), ctx.npoin_w, ctx.lpoin_w);
     if (bc)  // time_integ.f90:256-259
       temporary_bc_routine_dirichlet_prim(npoin, *bc, W.aux_rho.data(), W.aux_q.data(), W.aux_u.data(),
                                           W.aux_pr.data(), W.aux_E.data());
-    // EOS (time_integ.f90:266-285)
+    // EOS over lpoin_w (time_integ.f90:266-285)
 #pragma omp parallel for schedule(static)
-    for (int p = 0; p < npoin; ++p) {
+    for (int w = 0; w < n_working(ctx); ++w) {
+      const int p = working(ctx, w);
       double umag = 0.0;
       for (int d = 0; d < 3; ++d) {
         W.aux_u[p + (int64_t)npoin * d] = W.aux_q[p + (int64_t)npoin * d] / W.aux_rho[p];
@@ -1762,7 +1780,7 @@ inline void rk_4_main(const ElemCtx& ctx, const Params& P, const double* Ml, con
     }
     generic_scalar_convec_ijk(ctx, W.f_eta.data(), W.aux_eta.data(), W.aux_u.data(), W.Reta.data());
     if (bc) bc_fix_dirichlet_residual_entropy(npoin, *bc, W.Reta.data());  // time_integ.f90:299-301
-    for (int p = 0; p < npoin; ++p) W.Reta[p] = W.Reta[p] / Ml[p];
+    for (int w = 0; w < n_working(ctx); ++w) W.Reta[working(ctx, w)] /= Ml[working(ctx, w)];  // mod_solver.f90:23-38
     sutherland_viscosity(npoin, W.aux_Tem.data(), mu_factor, S.mu_fluid);
     full_diffusion_ijk(ctx, P, W.aux_rho.data(), W.aux_rho.data(), W.aux_u.data(), W.aux_Tem.data(),
                        S.mu_fluid, S.mu_e, S.mu_sgs, W.Rdiff_mass.data(), W.Rdiff_mom.data(),
@@ -1782,12 +1800,12 @@ inline void rk_4_main(const ElemCtx& ctx, const Params& P, const double* Ml, con
       W.Rener[p] = W.Rener[p] + W.Rdiff_ener[p];
     }
     for (int64_t p = 0; p < n3; ++p) W.Rmom[p] = W.Rmom[p] + W.Rdiff_mom[p];
-    for (int p = 0; p < npoin; ++p) {
+    for (int w = 0; w < n_working(ctx); ++w) {  // lumped_solver_scal/vect over lpoin_w (mod_solver.f90:23-58)
+      const int p = working(ctx, w);
       W.Rmass[p] = W.Rmass[p] / Ml[p];
       W.Rener[p] = W.Rener[p] / Ml[p];
+      for (int d = 0; d < 3; ++d) W.Rmom[p + (int64_t)npoin * d] = W.Rmom[p + (int64_t)npoin * d] / Ml[p];
     }
-    for (int d = 0; d < 3; ++d)
-      for (int p = 0; p < npoin; ++p) W.Rmom[p + (int64_t)npoin * d] = W.Rmom[p + (int64_t)npoin * d] / Ml[p];
     if (cap && cap->stage == istep + 1) {
       if (cap->Rmass) std::memcpy(cap->Rmass, W.Rmass.data(), sizeof(double) * npoin);
       if (cap->Rener) std::memcpy(cap->Rener, W.Rener.data(), sizeof(double) * npoin);
@@ -1808,10 +1826,11 @@ inline void rk_4_main(const ElemCtx& ctx, const Params& P, const double* Ml, con
     S.E[p] = S.E[p] - dt * W.Rener_sum[p];
     for (int d = 0; d < 3; ++d) S.q[p + (int64_t)npoin * d] = S.q[p + (int64_t)npoin * d] - dt * W.Rmom_sum[p + (int64_t)npoin * d];
   }
-  if (buf) update_buffer(npoin, *buf, S.rho, S.q, S.E);  // time_integ.f90:429
+  if (buf) update_buffer(npoin, *buf, S.rho, S.q, S.E, ctx.npoin_w, ctx.lpoin_w);  // time_integ.f90:429
   if (bc) temporary_bc_routine_dirichlet_prim(npoin, *bc, S.rho, S.q, S.u, S.pr, S.E);  // time_integ.f90:434-437
-  // EOS at the new level (time_integ.f90:445-463)
-  for (int p = 0; p < npoin; ++p) {
+  // EOS at the new level over lpoin_w (time_integ.f90:445-463)
+  for (int w = 0; w < n_working(ctx); ++w) {
+    const int p = working(ctx, w);
     double umag = 0.0;
     for (int d = 0; d < 3; ++d) {
       S.u[p + (int64_t)npoin * d] = S.q[p + (int64_t)npoin * d] / S.rho[p];
@@ -1825,8 +1844,8 @@ inline void rk_4_main(const ElemCtx& ctx, const Params& P, const double* Ml, con
     S.Tem[p] = S.pr[p] / (S.rho[p] * Rgas);
     S.eta[p] = (S.rho[p] / (g - 1.0)) * std::log(S.pr[p] / std::pow(S.rho[p], g));
   }
-  // Reta = -Reta_sum (time_integ.f90:467-471)
-  for (int p = 0; p < npoin; ++p) W.Reta[p] = -W.Reta_sum[p];
+  // Reta = -Reta_sum over lpoin_w (time_integ.f90:467-471)
+  for (int w = 0; w < n_working(ctx); ++w) W.Reta[working(ctx, w)] = -W.Reta_sum[working(ctx, w)];
   if (bc) bc_fix_dirichlet_residual_entropy(npoin, *bc, W.Reta.data());  // time_integ.f90:474-477
   sutherland_viscosity(npoin, S.Tem, mu_factor, S.mu_fluid);
   smart_visc_spectral(ctx, P, W.Reta.data(), gpvol, wgp, S.rho, S.u, S.csound, S.Tem, S.eta, helem_l, helem,

@@ -48,7 +48,8 @@ class SodMeshDesc(C.Structure):
     _fields_ = [("nelem", C.c_int32), ("npoin", C.c_int32), ("npoin_orig", C.c_int32), ("porder", C.c_int32),
                 ("index_base", C.c_int32), ("connec", _p), ("connec_orig", _p), ("coord_orig", _p),
                 ("dlxigp_ip", _p), ("wgp", _p), ("invAtoIJK", _p), ("gmshAtoI", _p), ("gmshAtoJ", _p),
-                ("gmshAtoK", _p), ("He", _p), ("gpvol", _p), ("Ml", _p), ("helem", _p), ("helem_l", _p)]
+                ("gmshAtoK", _p), ("He", _p), ("gpvol", _p), ("Ml", _p), ("helem", _p), ("helem_l", _p),
+                ("npoin_w", C.c_int32), ("lpoin_w", _p)]
 
 
 class SodState(C.Structure):
@@ -73,6 +74,11 @@ _SIGS = {
     "sod_full_convec_ijk_H": (_i, [_p, _p, _p, _p, _p, _p, _p, _p, _p, _p]),
     "sod_full_convec_ijk_noalloc": (_i, [C.c_int32, C.c_int32, C.c_int32] + [_p] * 16),
     "sod_generic_scalar_convec_ijk": (_i, [_p, _p, _p, _p, _p, _p]),
+    "sod_full_convec_ijk_ref": (_i, [C.c_int32] * 3 + [_p] * 20),
+    "sod_full_convec_ijk_H_ref": (_i, [C.c_int32] * 3 + [_p] * 20),
+    "sod_generic_scalar_convec_ijk_ref": (_i, [C.c_int32] * 3 + [_p] * 16),
+    "sod_full_diffusion_ijk_ref": (_i, [C.c_int32] * 3 + [_p] * 9 + [_d, _d] + [_p] * 12),
+    "sod_smart_visc_spectral_ref": (_i, [C.c_int32] * 4 + [_p] * 8 + [_d] + [_p] * 16),
     "sod_full_diffusion_ijk": (_i, [_p, _d, _d, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p]),
     "sod_lumped_solver": (_i, [_p, _p, _i, _p]),
     "sod_sutherland_viscosity": (_i, [C.c_int32, _p, _p, _p, _p]),

@@ -605,6 +605,10 @@ int sod_rhs_vjp(SodMesh* m, const double* rho, const double* q, const double* E,
                 double* grad_rho, double* grad_q, double* grad_E, sod_stream_t stream) {
   SOD_ARG(m && rho && q && E && mu_e && mu_factor, "inputs null");
   SOD_ARG(bar_Rmass && bar_Rmom && bar_Rener && grad_rho && grad_q && grad_E, "adjoint arrays null");
+  if (m->has_slaves) {
+    set_error("sod_rhs_vjp on a mesh with periodic slave rows (lpoin_w) is not supported");
+    return SOD_ERR_UNSUPPORTED;
+  }
   cudaStream_t st = (cudaStream_t)stream;
   int rc = ensure_step_buffers(m, false);
   if (rc) return rc;
@@ -639,6 +643,10 @@ int sod_rk4_step_vjp(SodMesh* m, const double* rho, const double* q, const doubl
                      double* out_E, sod_stream_t stream) {
   SOD_ARG(m && rho && q && E && mu_e && mu_factor && dt_dev, "inputs null");
   SOD_ARG(bar_rho && bar_q && bar_E && out_rho && out_q && out_E, "adjoint arrays null");
+  if (m->has_slaves) {
+    set_error("sod_rk4_step_vjp on a mesh with periodic slave rows (lpoin_w) is not supported");
+    return SOD_ERR_UNSUPPORTED;
+  }
   // boundaries and buffer zone: the routines' adjoints after every stage VJP and on the seed
   const bool has_bc = m->bc.nb > 0, has_zone = m->zone.nb > 0;
   const bool bc = has_bc || has_zone;
@@ -852,6 +860,10 @@ int sod_bc_dirichlet_prim_vjp(SodMesh* m, const double* rho, const double* q, co
                               double* bar_q, double* bar_E, sod_stream_t stream) {
   SOD_ARG(m && bar_rho && bar_q && bar_E, "null argument");
   SOD_ARG(m->bc.nb > 0, "no boundary nodes registered (sod_mesh_set_boundaries)");
+  if (m->has_slaves) {
+    set_error("sod_bc_dirichlet_prim_vjp on a mesh with periodic slave rows (lpoin_w) is not supported");
+    return SOD_ERR_UNSUPPORTED;
+  }
   SOD_ARG(m->bc.nff == 0 || (rho && q && E), "far-field adjoint needs the state the routine read");
   cudaStream_t st = (cudaStream_t)stream;
   const size_t N = m->npoin;

@@ -80,6 +80,11 @@ int sod_batch_create(SodMesh* const* meshes, int nmesh, SodBatch** out) {
   *out = nullptr;
   for (int i = 0; i < nmesh; ++i) SOD_ARG(meshes[i], "null member mesh");
   for (int i = 0; i < nmesh; ++i)
+    if (meshes[i]->has_slaves) {
+      set_error("sod_batch_create: members with periodic slave rows (lpoin_w) are not supported");
+      return SOD_ERR_UNSUPPORTED;
+    }
+  for (int i = 0; i < nmesh; ++i)
     if (meshes[i]->bc.nb > 0 || meshes[i]->zone.nb > 0 || meshes[i]->source || meshes[i]->wmodel.nw > 0) {
       set_error("sod_batch_create: members with boundaries, a buffer zone, a source term or a wall model are not supported");
       return SOD_ERR_UNSUPPORTED;

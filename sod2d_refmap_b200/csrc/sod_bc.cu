@@ -549,11 +549,12 @@ __device__ __forceinline__ void reduce3(double& s, double& mx, double& mn, doubl
   }
 }
 
-__global__ void __launch_bounds__(kBlock) k_eta_partials(int n, const double* __restrict__ eta, double* red) {
+__global__ void __launch_bounds__(kBlock) k_eta_partials(int n, const int32_t* __restrict__ ptr,
+                                                         const double* __restrict__ eta, double* red) {
   __shared__ double sh[3][kBlock / 32];
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   double s = 0.0, mx = -1e300, mn = 1e300;
-  if (i < n) s = mx = mn = eta[i];
+  if (i < n && ptr[i + 1] > ptr[i]) s = mx = mn = eta[i];  // working nodes only
   reduce3(s, mx, mn, sh);
   if (threadIdx.x == 0) {
     red[3 * blockIdx.x] = s;
@@ -750,9 +751,9 @@ int bc_final(SodMesh* m, SodState* s, double* Reta, cudaStream_t st) {
 int eta_stats(SodMesh* m, const double* eta, cudaStream_t st) {
   const int nblk = bcd::grid_of(m->npoin);
   SOD_ARG(m->buf.red_cap >= 3 * (int64_t)nblk, "reduction scratch too small");
-  bcd::k_eta_partials<<<nblk, bcd::kBlock, 0, st>>>(m->npoin, eta, m->buf.red);
+  bcd::k_eta_partials<<<nblk, bcd::kBlock, 0, st>>>(m->npoin, m->n2e_ptr, eta, m->buf.red);
   SOD_CHECK_LAUNCH();
-  bcd::k_eta_final<<<1, bcd::kBlock, 0, st>>>(nblk, m->npoin, m->prm.normalise, m->buf.red, m->buf.scal);
+  bcd::k_eta_final<<<1, bcd::kBlock, 0, st>>>(nblk, m->npoin_w, m->prm.normalise, m->buf.red, m->buf.scal);
   SOD_CHECK_LAUNCH();
   return SOD_OK;
 }
@@ -777,6 +778,11 @@ int sod_mesh_set_boundaries(SodMesh* m, const int32_t* codes, const int32_t* lnb
   std::vector<int32_t> node, code, nbr;
   for (int n = 0; n < N; ++n) {
     if (codes[n] < bcd::kMaxNumBouCodes) {
+      if (m->has_slaves && m->slave_host[n]) {
+        set_error("sod_mesh_set_boundaries: boundary code on periodic slave row %d is not supported",
+                  n + m->index_base);
+        return SOD_ERR_UNSUPPORTED;
+      }
       const int32_t s = lnbn[n] - m->index_base;
       SOD_ARG(s >= 0 && s < N, "lnbn_nodes entry out of range");
       node.push_back(n);

@@ -146,6 +146,7 @@ int sod_mesh_set_buffer(SodMesh* m, const SodBufferParams* p, const double* coor
   std::vector<int32_t> node;
   std::vector<double> xi;
   for (size_t n = 0; n < N; ++n) {
+    if (m->has_slaves && m->slave_host[n]) continue;  // updateBuffer runs over lpoin_w (time_integ.f90:529)
     double x = 1.0;
     bool in = false;
     for (int f = 0; f < 6; ++f) {

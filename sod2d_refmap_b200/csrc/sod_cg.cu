@@ -639,6 +639,10 @@ void sod_poisson_destroy(SodPoisson* P) {
 int sod_poisson_create(SodMesh* m, SodPoisson** out) {
   SOD_ARG(m && out, "mesh/out null");
   *out = nullptr;
+  if (m->has_slaves) {
+    set_error("sod_poisson_create on a mesh with periodic slave rows (lpoin_w) is not supported");
+    return SOD_ERR_UNSUPPORTED;
+  }
   const int64_t N = m->npoin, E = m->nelem;
   SodPoisson* P = new SodPoisson();
   P->mesh = m; P->n = N; P->nelem = E; P->pin = 0;

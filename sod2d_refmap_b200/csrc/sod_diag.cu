@@ -198,7 +198,9 @@ __global__ void __launch_bounds__(256) k_fderiv_gather(int npoin, const int32_t*
     a[0] += x.x; a[1] += x.y; a[2] += x.z; a[3] += x.w;
     a[4] += y.x; a[5] += y.y; a[6] += y.z; a[7] += y.w;
   }
-  const double cnt = (double)(end - beg);  // lelpn
+  // lelpn; a row without elements (a periodic slave, outside lpoin_w) keeps the zero the
+  // reference's outputs start from (mod_postpro.f90:28-32,127-136)
+  const double cnt = end > beg ? (double)(end - beg) : 1.0;
   const size_t N = (size_t)npoin;
 #pragma unroll
   for (int q = 0; q < 3; ++q) {

@@ -253,6 +253,11 @@ __device__ __forceinline__ void eos_store(size_t n, size_t N, double rho, const 
 
 struct SodMesh {
   int32_t nelem = 0, npoin = 0;
+  // working nodes (lpoin_w): rows with elements; the others are periodic slave rows that the
+  // node kernels skip (a row works iff n2e_ptr[n+1] > n2e_ptr[n])
+  int32_t npoin_w = 0;
+  bool has_slaves = false;
+  std::vector<uint8_t> slave_host;  // [npoin] 1 on slave rows (only kept when has_slaves)
   int device = 0;
   sod::DevParams prm{};
   sod::DMat D{};
@@ -299,6 +304,16 @@ struct SodMesh {
 namespace sod {
 // helpers implemented in sod_mesh.cu
 int ensure_step_buffers(SodMesh* m, bool mixed);
+int mesh_set_local_tables(SodMesh* m, const int32_t* gI, const int32_t* gJ, const int32_t* gK,
+                          const double* dlxigp_ip, const double* wgp, int base);
+// a SodMesh built on the device from reference-layout device arrays (sod_refargs.cu): He may be
+// null (geometry then holds gpvol only), wgp null (no jratio), helem/helem_l null, lpoin_w null
+// (every node works); the caller destroys it with sod_mesh_destroy
+int mesh_from_device_ref(int nelem, int npoin, int base, const int32_t* connec, const double* He,
+                         const double* gpvol, const double* dlxigp_ip, const int32_t* invAtoIJK,
+                         const int32_t* gI, const int32_t* gJ, const int32_t* gK, const double* wgp,
+                         const double* helem_l, const double* helem, int npoin_w, const int32_t* lpoin_w,
+                         const SodParams* params, cudaStream_t st, SodMesh** out);
 int mesh_ref_to_internal_elem(SodMesh* m, const double* ref_dev /*(nelem,64) F*/, double* int_dev,
                               cudaStream_t st);
 int mesh_internal_to_ref_elem(SodMesh* m, const double* int_dev, double* ref_dev, cudaStream_t st);

@@ -216,6 +216,37 @@ int mesh_internal_to_ref_elem(SodMesh* m, const double* in, double* ref, cudaStr
   return SOD_OK;
 }
 
+// Local node order of the library (natural d = i + 4j + 16k) from the reference's gmshAtoI/J/K
+// maps (host arrays, index_base-based), the 1-D derivative matrix from dlxigp_ip and, when given,
+// the GLL weights in that order.
+int mesh_set_local_tables(SodMesh* m, const int32_t* gI, const int32_t* gJ, const int32_t* gK,
+                          const double* dlxigp_ip, const double* wgp, int base) {
+  bool seen[NN] = {false};
+  for (int a = 0; a < NN; ++a) {
+    int si = gI[a] - base, sj = gJ[a] - base, sk = gK[a] - base;
+    if (si < 0 || si > 3 || sj < 0 || sj > 3 || sk < 0 || sk > 3) {
+      set_error("invalid argument: gmshAto* out of range at local node %d", a);
+      return SOD_ERR_ARG;
+    }
+    int d = kSodToNat[si] + 4 * kSodToNat[sj] + 16 * kSodToNat[sk];
+    if (seen[d]) {
+      set_error("invalid argument: gmshAto* maps two local nodes to one ijk");
+      return SOD_ERR_ARG;
+    }
+    seen[d] = true;
+    m->perm_a_of_d[d] = a;
+    m->perm_d_of_a[a] = d;
+  }
+  // D[mpt][nb] = l'_nb(x_mpt): dlxigp_ip(g, 0, ii) for a gauss point g with natural i = mpt
+  for (int mpt = 0; mpt < NP1; ++mpt) {
+    int g = m->perm_a_of_d[mpt];  // natural (mpt, 0, 0)
+    for (int ii = 0; ii < NP1; ++ii) m->D.d[mpt][kSodToNat[ii]] = dlxigp_ip[g + NN * (0 + 3 * ii)];
+  }
+  if (wgp)
+    for (int d = 0; d < NN; ++d) m->wgp_nat[d] = wgp[m->perm_a_of_d[d]];
+  return SOD_OK;
+}
+
 int ensure_step_buffers(SodMesh* m, bool mixed) {
   if (int rc = init_kernel_attrs()) return rc;
   StepBuffers& b = m->buf;
@@ -362,31 +393,14 @@ int sod_mesh_create(const SodMeshDesc* desc, const SodParams* params, SodMesh** 
   SodParams dp;
   sod_params_default(&dp);
   to_dev_params(params ? params : &dp, &m->prm);
-  // local node permutation from the reference's ijk maps
-  bool seen[NN] = {false};
-  for (int a = 0; a < NN; ++a) {
-    int si = desc->gmshAtoI[a] - base, sj = desc->gmshAtoJ[a] - base, sk = desc->gmshAtoK[a] - base;
-    if (si < 0 || si > 3 || sj < 0 || sj > 3 || sk < 0 || sk > 3) {
+  {
+    const int rc = mesh_set_local_tables(m, desc->gmshAtoI, desc->gmshAtoJ, desc->gmshAtoK, desc->dlxigp_ip, desc->wgp,
+                                         base);
+    if (rc) {
       delete m;
-      set_error("invalid argument: gmshAto* out of range at local node %d", a);
-      return SOD_ERR_ARG;
+      return rc;
     }
-    int d = kSodToNat[si] + 4 * kSodToNat[sj] + 16 * kSodToNat[sk];
-    if (seen[d]) {
-      delete m;
-      set_error("invalid argument: gmshAto* maps two local nodes to one ijk");
-      return SOD_ERR_ARG;
-    }
-    seen[d] = true;
-    m->perm_a_of_d[d] = a;
-    m->perm_d_of_a[a] = d;
   }
-  // D[mpt][nb] = l'_nb(x_mpt): dlxigp_ip(g, 0, ii) for a gauss point g with natural i = mpt
-  for (int mpt = 0; mpt < NP1; ++mpt) {
-    int g = m->perm_a_of_d[mpt];  // natural (mpt, 0, 0)
-    for (int ii = 0; ii < NP1; ++ii) m->D.d[mpt][kSodToNat[ii]] = desc->dlxigp_ip[g + NN * (0 + 3 * ii)];
-  }
-  for (int d = 0; d < NN; ++d) m->wgp_nat[d] = desc->wgp[m->perm_a_of_d[d]];
 
   auto fail = [&](int rc) { sod_mesh_destroy(m); return rc; };
   // connectivity in internal layout
@@ -412,11 +426,41 @@ int sod_mesh_create(const SodMeshDesc* desc, const SodParams* params, SodMesh** 
         idx[fillp[v]++] = e * NN + d;
       }
   }
-  for (int n = 0; n < N; ++n)
-    if (ptr[n + 1] == ptr[n]) {
-      set_error("invalid argument: node %d is not referenced by any element", n + base);
+  // working nodes: lpoin_w when given (rows it does not list are periodic slaves), else all;
+  // connec (connecParWork) must reference exactly the working rows
+  std::vector<uint8_t> work((size_t)N, desc->lpoin_w ? 0 : 1);
+  if (desc->lpoin_w) {
+    if (desc->npoin_w <= 0 || desc->npoin_w > N) {
+      set_error("invalid argument: npoin_w=%d must be in 1..npoin=%d", desc->npoin_w, N);
       return fail(SOD_ERR_ARG);
     }
+    for (int w = 0; w < desc->npoin_w; ++w) {
+      const int v = desc->lpoin_w[w] - base;
+      if (v < 0 || v >= N || work[v]) {
+        set_error("invalid argument: lpoin_w(%d)=%d is out of range or listed twice", w + base, v + base);
+        return fail(SOD_ERR_ARG);
+      }
+      work[v] = 1;
+    }
+  }
+  m->npoin_w = desc->lpoin_w ? desc->npoin_w : N;
+  m->has_slaves = m->npoin_w < N;
+  if (m->has_slaves) {
+    m->slave_host.assign((size_t)N, 0);
+    for (int n = 0; n < N; ++n) m->slave_host[n] = work[n] ? 0 : 1;
+  }
+  for (int n = 0; n < N; ++n) {
+    const bool has = ptr[n + 1] > ptr[n];
+    if (work[n] && !has) {
+      set_error("invalid argument: working node %d is not referenced by any element", n + base);
+      return fail(SOD_ERR_ARG);
+    }
+    if (!work[n] && has) {
+      set_error("invalid argument: connec references node %d, which lpoin_w does not list (connec must be "
+                "connecParWork: every periodic image replaced by its master)", n + base);
+      return fail(SOD_ERR_ARG);
+    }
+  }
 #define ALLOC(p, bytes)                                        \
   do {                                                         \
     if (cudaMalloc(&(p), (bytes)) != cudaSuccess) {            \

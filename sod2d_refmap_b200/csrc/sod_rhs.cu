@@ -323,6 +323,7 @@ __global__ void __launch_bounds__(64 * EPB) k_rhs_fused(const RhsArgs a) {
 // ---------------------------------------------------------------------------------------------
 struct GatherArgs {
   int npoin;
+  int nwork;                      // working nodes (rows with elements): the entropy mean's count
   const int32_t* __restrict__ ptr;
   const int32_t* __restrict__ idx;
   const void* rel;
@@ -375,7 +376,22 @@ __device__ __forceinline__ void block_reduce3(double& s, double& mx, double& mn,
 template <typename R, int STAGE>
 __global__ void __launch_bounds__(256, SOD_KG_MIN_BLOCKS) k_gather_rk(const GatherArgs a) {
   const int n = blockIdx.x * blockDim.x + threadIdx.x;
-  const bool act = n < a.npoin;
+  // a row without elements is a periodic slave (not in lpoin_w): rk_4_main's node loops
+  // (time_integ.f90:267-285,445-471) and the lumped solve (mod_solver.f90:23-58) skip it, its
+  // residual stays zero and its state untouched; only sutherland_viscosity, which runs over all
+  // npoin (time_integ.f90:483-487), re-evaluates its mu_fluid from its own Tem
+  const bool inrange = n < a.npoin;
+  const bool act = inrange && a.ptr[n + 1] > a.ptr[n];
+  if (inrange && !act) {
+    if constexpr (STAGE == 0) {
+#pragma unroll
+      for (int f = 0; f < 6; ++f)
+        if (a.out[f]) a.out[f][n] = 0.0;
+    } else if constexpr (STAGE == 4) {
+      const double T = a.Tem[n];
+      a.mu_fluid[n] = a.mu_factor[n] * kSuthC1 * (T * sqrt(T)) / (T + kSuthS);
+    }
+  }
   double eta_n = 0.0;
   if (act) {
     const R* rel = reinterpret_cast<const R*>(a.rel);
@@ -494,7 +510,7 @@ __global__ void __launch_bounds__(256, SOD_KG_MIN_BLOCKS) k_gather_rk(const Gath
       block_reduce3(ts, tmx, tmn, sh);
       if (threadIdx.x == 0) {
         if (a.normalise) {
-          const double mean = ts / (double)a.npoin;
+          const double mean = ts / (double)a.nwork;
           a.scal[0] = mean;
           a.scal[1] = fmax(tmx - mean, mean - tmn);
         } else {
@@ -710,6 +726,7 @@ static int launch_gather_t(int stage, const GatherArgs& a, cudaStream_t st) {
 
 int launch_gather(SodMesh* m, bool mixed, int stage, GatherArgs& a, cudaStream_t st) {
   a.npoin = m->npoin;
+  a.nwork = m->npoin_w;
   a.ptr = m->n2e_ptr;
   a.idx = m->n2e;
   a.rel = m->buf.rel;
@@ -1194,13 +1211,17 @@ int sod_rk4_main_host(SodMesh* m, SodState* h, double dt_host, double* dt_next_h
   SOD_CUDA(cudaMemcpyAsync(d.mu_factor, h->mu_factor, N * 8, cudaMemcpyHostToDevice, st));
   SOD_CUDA(cudaMemcpyAsync(ddt, &dt_host, 8, cudaMemcpyHostToDevice, st));
   if (les_h) SOD_CUDA(cudaMemcpyAsync(d.mu_sgs, h->mu_sgs, EN * 8, cudaMemcpyHostToDevice, st));
-  int rc = sod_rk4_main(m, &d, ddt, ddt, prec, stream);
-  if (rc) return rc;
   struct Pair { double* hst; double* dev; size_t n; };
   Pair outs[] = {{h->rho, d.rho, N}, {h->q, d.q, 3 * N}, {h->E, d.E, N}, {h->u, d.u, 3 * N}, {h->pr, d.pr, N},
                  {h->Tem, d.Tem, N}, {h->e_int, d.e_int, N}, {h->eta, d.eta, N}, {h->csound, d.csound, N},
                  {h->machno, d.machno, N}, {h->mu_fluid, d.mu_fluid, N}, {h->mu_e, d.mu_e, EN},
                  {h->Reta, d.Reta, N}, {les_h ? h->mu_sgs : nullptr, d.mu_sgs, EN}};
+  if (m->has_slaves)  // the step leaves slave rows as they are: bring in the rows it will copy back
+    for (int i = 3; i < 11; ++i)
+      if (outs[i].hst) SOD_CUDA(cudaMemcpyAsync(outs[i].dev, outs[i].hst, outs[i].n * 8, cudaMemcpyHostToDevice, st));
+  if (m->has_slaves && h->Reta) SOD_CUDA(cudaMemcpyAsync(d.Reta, h->Reta, N * 8, cudaMemcpyHostToDevice, st));
+  int rc = sod_rk4_main(m, &d, ddt, ddt, prec, stream);
+  if (rc) return rc;
   for (auto& o : outs)
     if (o.hst) SOD_CUDA(cudaMemcpyAsync(o.hst, o.dev, o.n * 8, cudaMemcpyDeviceToHost, st));
   if (dt_next_host) SOD_CUDA(cudaMemcpyAsync(dt_next_host, ddt, 8, cudaMemcpyDeviceToHost, st));

@@ -224,10 +224,14 @@ __global__ void k_gather_plain(int npoin, const int32_t* __restrict__ ptr, const
   }
 }
 
-__global__ void k_lumped(int64_t npoin, int ncomp, const double* __restrict__ Ml, double* R) {
+// lumped_solver_scal/vect over the working nodes (mod_solver.f90:23-58): rows without elements
+// (periodic slaves, absent from lpoin_w) are left as they are
+__global__ void k_lumped(int64_t npoin, int ncomp, const double* __restrict__ Ml, const int32_t* __restrict__ ptr,
+                         double* R) {
   int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= npoin * ncomp) return;
-  R[t] = R[t] / Ml[t % npoin];
+  const int64_t n = t % npoin;
+  if (ptr[n + 1] > ptr[n]) R[t] = R[t] / Ml[n];
 }
 
 __global__ void k_sutherland(int64_t npoin, const double* __restrict__ Tem, const double* __restrict__ mf,
@@ -239,11 +243,12 @@ __global__ void k_sutherland(int64_t npoin, const double* __restrict__ Tem, cons
 }
 
 // eta sum/max/min -> scal[0] mean, scal[1] norm (single-block deterministic reduction)
-__global__ void __launch_bounds__(1024) k_eta_norm(int64_t npoin, const double* __restrict__ eta, double* scal,
-                                                   int normalise) {
+__global__ void __launch_bounds__(1024) k_eta_norm(int64_t npoin, int64_t nwork, const int32_t* __restrict__ ptr,
+                                                   const double* __restrict__ eta, double* scal, int normalise) {
   __shared__ double sh[3][32];
   double s = 0.0, mx = -1e300, mn = 1e300;
   for (int64_t t = threadIdx.x; t < npoin; t += blockDim.x) {
+    if (ptr[t + 1] == ptr[t]) continue;  // over lpoin_w only (mod_entropy_viscosity.f90:43-62)
     const double v = eta[t];
     s += v; mx = fmax(mx, v); mn = fmin(mn, v);
   }
@@ -258,7 +263,7 @@ __global__ void __launch_bounds__(1024) k_eta_norm(int64_t npoin, const double* 
     s = sh[0][0]; mx = sh[1][0]; mn = sh[2][0];
     for (int w = 1; w < (int)(blockDim.x >> 5); ++w) { s += sh[0][w]; mx = fmax(mx, sh[1][w]); mn = fmin(mn, sh[2][w]); }
     if (normalise) {
-      const double mean = s / (double)npoin;
+      const double mean = s / (double)nwork;
       scal[0] = mean;
       scal[1] = fmax(mx - mean, mean - mn);
     } else {
@@ -408,7 +413,7 @@ int sod_full_diffusion_ijk(SodMesh* m, double Cp, double Pr, const double* rho_n
 int sod_lumped_solver(SodMesh* m, double* R, int ncomp, sod_stream_t stream) {
   SOD_ARG(m && R && (ncomp == 1 || ncomp == 3), "lumped solver args");
   int64_t n = (int64_t)m->npoin * ncomp;
-  k_lumped<<<(unsigned)((n + 255) / 256), 256, 0, (cudaStream_t)stream>>>(m->npoin, ncomp, m->Ml, R);
+  k_lumped<<<(unsigned)((n + 255) / 256), 256, 0, (cudaStream_t)stream>>>(m->npoin, ncomp, m->Ml, m->n2e_ptr, R);
   SOD_CHECK_LAUNCH();
   return SOD_OK;
 }
@@ -427,7 +432,7 @@ int sod_smart_visc_spectral(SodMesh* m, const double* Reta, const double* rho, c
   cudaStream_t st = (cudaStream_t)stream;
   int rc = ensure_step_buffers(m, false);
   if (rc) return rc;
-  k_eta_norm<<<1, 1024, 0, st>>>(m->npoin, eta, m->buf.scal, m->prm.normalise);
+  k_eta_norm<<<1, 1024, 0, st>>>(m->npoin, m->npoin_w, m->n2e_ptr, eta, m->buf.scal, m->prm.normalise);
   SOD_CHECK_LAUNCH();
   SodState s{};
   s.Reta = const_cast<double*>(Reta);

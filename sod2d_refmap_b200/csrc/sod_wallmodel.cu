@@ -337,6 +337,10 @@ int sod_mesh_set_wall_model(SodMesh* m, int32_t type, int32_t nboun, int32_t npb
                             const double* normalsAtNodes, const double* zo, const double* walave_u) {
   SOD_ARG(m, "mesh null");
   SOD_ARG(m->nmember == 0, "a wall model on an ensemble mesh is not supported");
+  if (m->has_slaves && numBoundsWM > 0) {
+    set_error("sod_mesh_set_wall_model on a mesh with periodic slave rows (lpoin_w) is not supported");
+    return SOD_ERR_UNSUPPORTED;
+  }
   for (auto& kv : m->graphs)
     if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
   m->graphs.clear();

@@ -139,6 +139,10 @@ class Sod2dMesh:
         desc.gmshAtoI = keep(np.ascontiguousarray(T.gmshAtoI, dtype=np.int32))
         desc.gmshAtoJ = keep(np.ascontiguousarray(T.gmshAtoJ, dtype=np.int32))
         desc.gmshAtoK = keep(np.ascontiguousarray(T.gmshAtoK, dtype=np.int32))
+        lw = mesh.extra.get("lpoin_w") if getattr(mesh, "extra", None) else None
+        if lw is not None:  # SOD2D's array form: rows outside lpoin_w are periodic slaves
+            desc.npoin_w = len(lw)
+            desc.lpoin_w = keep(np.ascontiguousarray(lw, dtype=np.int32))
         if geometry:
             for k in ("He", "gpvol", "Ml", "helem", "helem_l"):
                 if geometry.get(k) is not None:
@@ -639,3 +643,66 @@ def legacy_ener_convec(connec, Ngp, gpcar, gpvol, u, pr, E):
 
 def legacy_mom_diffusion(connec, Ngp, gpcar, gpvol, u, mu_e):
     return _legacy_call("sod_legacy_mom_diffusion", connec, Ngp, gpcar, gpvol, [u, mu_e], np.shape(u))
+
+
+# ---- the reference's subroutines with their complete argument lists (device arrays) ----------
+def _ptrs(*ts):
+    return [C.c_void_p(_ptr(t)) for t in ts]
+
+
+def full_convec_ijk_ref(nelem, npoin, connec, Ngp, dNgp, He, gpvol, dlxigp_ip, xgp, invAtoIJK, gmshAtoI, gmshAtoJ,
+                        gmshAtoK, u, q, rho, pr, E, index_base: int = 1, total_enthalpy: bool = False, stream=None):
+    """full_convec_ijk (elem_convec.f90:211-224) or, with total_enthalpy, full_convec_ijk_H
+    (:20-33), called as the reference calls it: every argument a CUDA tensor holding the Fortran
+    array's memory (connec (nelem,64) column-major, ids index_base-based; u, q (npoin,3) ...).
+    Returns (Rmass, Rmom, Rener) with Rmom in (npoin,3) memory order."""
+    torch = _torch()
+    f64 = dict(dtype=torch.float64, device="cuda")
+    Rm, Rmo, Re = torch.empty(npoin, **f64), torch.empty(3 * npoin, **f64), torch.empty(npoin, **f64)
+    fn = _lib.load().sod_full_convec_ijk_H_ref if total_enthalpy else _lib.load().sod_full_convec_ijk_ref
+    _lib.check(fn(int(nelem), int(npoin), int(index_base), *_ptrs(connec, Ngp, dNgp, He, gpvol, dlxigp_ip, xgp,
+                                                                   invAtoIJK, gmshAtoI, gmshAtoJ, gmshAtoK, u, q, rho,
+                                                                   pr, E, Rm, Rmo, Re), _stream(stream)))
+    return Rm, Rmo, Re
+
+
+def generic_scalar_convec_ijk_ref(nelem, npoin, connec, Ngp, dNgp, He, gpvol, dlxigp_ip, xgp, invAtoIJK, gmshAtoI,
+                                  gmshAtoJ, gmshAtoK, q, eta, u, index_base: int = 1, stream=None):
+    """generic_scalar_convec_ijk (elem_convec.f90:462-476) with its argument list; returns Rconvec."""
+    torch = _torch()
+    R = torch.empty(npoin, dtype=torch.float64, device="cuda")
+    _lib.check(_lib.load().sod_generic_scalar_convec_ijk_ref(
+        int(nelem), int(npoin), int(index_base), *_ptrs(connec, Ngp, dNgp, He, gpvol, dlxigp_ip, xgp, invAtoIJK,
+                                                        gmshAtoI, gmshAtoJ, gmshAtoK, q, eta, u, R), _stream(stream)))
+    return R
+
+
+def full_diffusion_ijk_ref(nelem, npoin, connec, Ngp, He, gpvol, dlxigp_ip, invAtoIJK, gmshAtoI, gmshAtoJ, gmshAtoK,
+                           Cp, Pr, rho_n, rho, u, Tem, mu_fluid, mu_e, mu_sgs, Ml, index_base: int = 1, stream=None):
+    """full_diffusion_ijk (elem_diffu.f90:12-25) with its argument list; returns (Rmass, Rmom, Rener)."""
+    torch = _torch()
+    f64 = dict(dtype=torch.float64, device="cuda")
+    Rm, Rmo, Re = torch.empty(npoin, **f64), torch.empty(3 * npoin, **f64), torch.empty(npoin, **f64)
+    L = _lib.load()
+    _lib.check(L.sod_full_diffusion_ijk_ref(
+        int(nelem), int(npoin), int(index_base), *_ptrs(connec, Ngp, He, gpvol, dlxigp_ip, invAtoIJK, gmshAtoI,
+                                                        gmshAtoJ, gmshAtoK), C.c_double(Cp), C.c_double(Pr),
+        *_ptrs(rho_n, rho, u, Tem, mu_fluid, mu_e, mu_sgs, Ml, Rm, Rmo, Re), _stream(stream)))
+    return Rm, Rmo, Re
+
+
+def smart_visc_spectral_ref(nelem, npoin, npoin_w, connec, lpoin_w, Reta, Ngp, coord, dNgp, gpvol, wgp, gamma_gas,
+                            rho, u, csound, Tem, eta, helem_l, helem, Ml, invAtoIJK, gmshAtoI, gmshAtoJ, gmshAtoK,
+                            prm: TGVParams | None = None, index_base: int = 1, stream=None):
+    """smart_visc_spectral (mod_entropy_viscosity.f90:14-28) with its argument list (helem_l is
+    the dummy named helem, helem the one named helem_k); prm gives the mod_numerical_params
+    values and nscbc_Rgas_inf.  Returns mu_e in (nelem,64) memory order."""
+    torch = _torch()
+    mu_e = torch.empty(64 * nelem, dtype=torch.float64, device="cuda")
+    p = params_struct(prm or TGVParams())
+    _lib.check(_lib.load().sod_smart_visc_spectral_ref(
+        int(nelem), int(npoin), int(npoin_w), int(index_base), *_ptrs(connec, lpoin_w, Reta, Ngp, coord, dNgp, gpvol,
+                                                                      wgp), C.c_double(gamma_gas),
+        *_ptrs(rho, u, csound, Tem, eta, helem_l, helem, Ml, mu_e, invAtoIJK, gmshAtoI, gmshAtoJ, gmshAtoK),
+        C.c_void_p(0), C.byref(p), _stream(stream)))
+    return mu_e
