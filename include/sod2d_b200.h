@@ -245,13 +245,28 @@ int sod_rk4_steps(SodMesh* mesh, SodState* state, double* dt_dev, int nsteps, So
 int sod_step_profile(SodMesh* mesh, SodState* state, double* dt_dev, int nsteps, SodPrecision prec,
                      sod_stream_t stream, float* ms_out);
 
-/* Autotuner of the fused RHS kernel: times elements-per-CTA candidates ({1,2,4} FP64,
- * {1,2,4,8} mixed) on the given state and keeps the fastest for this mesh and precision. */
+/* Autotuner of the RK stage (no reference counterpart): times, on the given state, one RK stage
+ * (fused RHS + gather / stage update into the library's stage buffers; the caller's arrays are
+ * only read) for every configuration of two dimensions - elements per CTA {1,2,4,8} and the
+ * launch shape: two launches per stage, or (on the periodic path) one cooperative launch per
+ * stage with 1/2, 3/4 or all of the CTAs per SM that fit - 3 warm-up + 10 timed stages each, and
+ * keeps the fastest for this mesh and precision; captured step graphs use it.  best_ms receives
+ * the fastest fused-RHS launch alone; sod_autotune_table returns the whole sweep. */
 int sod_autotune(SodMesh* mesh, SodState* state, SodPrecision prec, int* best_epb, float* best_ms,
                  sod_stream_t stream);
-/* Pins the fused-RHS elements per CTA of a precision (one of the autotuner's candidates; 0: the
- * default).  Captured step graphs are dropped when it changes. */
+/* The last sweep of sod_autotune for a precision: up to cap rows of (elements per CTA, CTAs per
+ * SM of the one-launch stage or 0 for two launches, ms per stage); returns the number of rows. */
+int sod_autotune_table(SodMesh* mesh, SodPrecision prec, int cap, int32_t* epb, int32_t* ctas_per_sm,
+                       float* ms_per_stage);
+/* Pins the fused-RHS elements per CTA of a precision (1, 2, 4 or 8; 0: the default).  Captured
+ * step graphs are dropped when it changes. */
 int sod_set_rhs_config(SodMesh* mesh, SodPrecision prec, int config);
+/* Pins the launch shape of an RK stage: 0 = two launches (fused RHS, then the gather); n > 0 =
+ * one cooperative launch of min(n, what fits) resident CTAs per SM that runs the fused RHS over
+ * element tiles, a grid barrier and the gather (and, at stage 4, the entropy viscosity and dt):
+ * four launches per step.  Used on the periodic path only (without boundaries, buffer zone,
+ * wall model, source term or LES the step falls back to two launches per stage). */
+int sod_set_stage_launch(SodMesh* mesh, SodPrecision prec, int ctas_per_sm);
 
 /* compute_fieldDerivs (mod_postpro.f90:12-139) on device arrays rho (npoin) and u (npoin,3):
  * gradRho (npoin,3), curlU (npoin,3) = sum_jk leviCivi(i,j,k) du_j/dx_k, divU (npoin) =

@@ -121,6 +121,8 @@ _SIGS = {
     "sod_batch_autotune": (_i, [_p, _i, _p, _p, _p]),
     "sod_batch_rk4_steps": (_i, [_p, _i, _i, _p]),
     "sod_autotune": (_i, [_p, _p, _i, _p, _p, _p]),
+    "sod_autotune_table": (_i, [_p, _i, _i, _p, _p, _p]),
+    "sod_set_stage_launch": (_i, [_p, _i, _i]),
     "sod_last_error": (C.c_char_p, []),
     "sod_version": (C.c_char_p, []),
     "sod_launch_count": (C.c_int64, []),

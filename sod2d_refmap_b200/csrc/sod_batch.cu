@@ -271,7 +271,8 @@ int sod_batch_rk4_steps(SodBatch* B, int nsteps, SodPrecision prec, sod_stream_t
     if (rc) return rc;
   }
   if (nsteps > 0) {
-    const uint64_t key = ((uint64_t)mixed << 40) ^ (uint64_t)m->tuned_epb[mixed ? 1 : 0];
+    const uint64_t key = ((uint64_t)mixed << 40) ^ ((uint64_t)m->persist_ctas[mixed ? 1 : 0] << 16) ^
+                         (uint64_t)m->tuned_epb[mixed ? 1 : 0];
     auto it = B->graphs.find(key);
     if (it == B->graphs.end()) {
       cudaStream_t cap;

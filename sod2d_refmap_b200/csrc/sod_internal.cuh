@@ -280,6 +280,11 @@ struct SodMesh {
   sod::StepBuffers buf;
   std::unordered_map<uint64_t, sod::GraphEntry> graphs;
   int tuned_epb[2] = {0, 0};
+  // per precision: 0 runs a stage as two launches (fused RHS, gather); n > 0 as one cooperative
+  // launch of n resident blocks per SM (the autotuner's choice, or sod_set_rhs_config)
+  int persist_ctas[2] = {0, 0};
+  struct TuneEntry { int epb, ctas; float ms; };
+  std::vector<TuneEntry> tune_table[2];  // the last sod_autotune sweep per precision
   std::vector<double*> host_mirror;  // device buffers of sod_rk4_main_host
   // ensemble members (a SodBatch's concatenated mesh); nmember == 0 for a single mesh
   int nmember = 0;

@@ -16,6 +16,7 @@
 // This is the FP64 parity path: the reference's formulas in FP64 (R = double).  The mixed
 // path (FP32 element arithmetic on deviation fields) is k_rhs_mixed2 in sod_rhs_mixed.cu.
 #include "sod_internal.cuh"
+#include "sod_step_kernels.cuh"
 #include <cmath>
 #include <algorithm>
 
@@ -74,16 +75,17 @@ constexpr size_t rhs_smem_bytes(int epb) {
   return sizeof(R) * (size_t)epb * (NBUF + NP2) * FSTRIDE;
 }
 
+// One tile of EPB elements (64 threads each) of the fused RHS; smem_raw holds
+// rhs_smem_bytes<R>(EPB).  Every thread of the block calls it (it holds block barriers).
 // TOTH: flag_total_enthalpy (energy convection of full_convec_ijk_H)
 template <typename R, int EPB, bool TOTH>
-__global__ void __launch_bounds__(64 * EPB) k_rhs_fused(const RhsArgs a) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+__device__ __forceinline__ void rhs_fused_tile(const RhsArgs& a, int tile, unsigned char* smem_raw) {
   R* buf_all = reinterpret_cast<R*>(smem_raw);
   const int tid = threadIdx.x;
   const int es = tid >> 6;
   const int d = tid & 63;
   const int i = d & 3, j = (d >> 2) & 3, k = d >> 4;
-  const int e = blockIdx.x * EPB + es;
+  const int e = tile * EPB + es;
   const bool active = e < a.nelem;
   const int ee = active ? e : a.nelem - 1;
   R* buf = buf_all + (size_t)es * (NBUF + NP2) * FSTRIDE;
@@ -317,55 +319,24 @@ __global__ void __launch_bounds__(64 * EPB) k_rhs_fused(const RhsArgs a) {
   }
 }
 
-// ---------------------------------------------------------------------------------------------
-// KG: ordered CSR gather of the element residuals, /Ml, RK accumulate and next stage state.
-// STAGE 0 = plain RHS (gather + /Ml into output arrays).  STAGE 4 = final update + EOS.
-// ---------------------------------------------------------------------------------------------
-struct GatherArgs {
-  int npoin;
-  int nwork;                      // working nodes (rows with elements): the entropy mean's count
-  const int32_t* __restrict__ ptr;
-  const int32_t* __restrict__ idx;
-  const void* rel;
-  const double* __restrict__ Ml;
-  const double* __restrict__ dt;  // device scalar, or per-member array when node_member is set
-  const int32_t* __restrict__ node_member;
-  int member_reduce;              // stage 4: eta sums done by the per-member kernel instead
-  double a_next, b_cur;
-  // state (level pos=2) columns
-  double* y[5];
-  double* ys;    // stage state 5*N
-  double* rsum;  // 6*N
-  // stage-0 outputs
-  double* out[6];
-  // stage-4 EOS outputs
-  double *u0, *u1, *u2, *pr, *Tem, *e_int, *eta, *csound, *machno, *mu_fluid, *Reta;
-  const double* mu_factor;
-  double gamma, Rgas;
-  double* red;              // partials [3*nblocks]
-  unsigned int* counter;
-  unsigned int* nonfinite;  // raised by stage 4 on a NaN/Inf in the new rho, q, E
-  double* scal;             // [0] eta mean, [1] eta norm
-  int normalise;
-  const double* src;        // momentum source term (npoin,3) or null
-  const double* wm;         // wall-model momentum terms (npoin,3) or null
-};
+template <typename R, int EPB, bool TOTH>
+__global__ void __launch_bounds__(64 * EPB) k_rhs_fused(const RhsArgs a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  rhs_fused_tile<R, EPB, TOTH>(a, blockIdx.x, smem_raw);
+}
 
-__device__ __forceinline__ void block_reduce3(double& s, double& mx, double& mn, double* sh) {
-  // warp reduce then smem
-  for (int o = 16; o > 0; o >>= 1) {
-    s += __shfl_down_sync(0xffffffffu, s, o);
-    mx = fmax(mx, __shfl_down_sync(0xffffffffu, mx, o));
-    mn = fmin(mn, __shfl_down_sync(0xffffffffu, mn, o));
+// One RK stage of the FP64 path in one cooperative launch (persistent blocks): the fused RHS
+// over element tiles, then persist_stage_tail (gather / stage update; at stage 4 the entropy
+// viscosity and dt).
+template <int EPB, bool TOTH>
+__global__ void __launch_bounds__(64 * EPB) k_stage_fused(const StageArgs p) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int ntiles = (p.r.nelem + EPB - 1) / EPB;
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    rhs_fused_tile<double, EPB, TOTH>(p.r, t, smem_raw);
+    __syncthreads();  // the next tile reuses the shared memory
   }
-  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-  if (l == 0) { sh[3 * w] = s; sh[3 * w + 1] = mx; sh[3 * w + 2] = mn; }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    const int nw = blockDim.x >> 5;
-    s = sh[0]; mx = sh[1]; mn = sh[2];
-    for (int q = 1; q < nw; ++q) { s += sh[3 * q]; mx = fmax(mx, sh[3 * q + 1]); mn = fmin(mn, sh[3 * q + 2]); }
-  }
+  persist_stage_tail<double, EPB>(p, smem_raw);
 }
 
 #ifndef SOD_KG_MIN_BLOCKS
@@ -376,274 +347,22 @@ __device__ __forceinline__ void block_reduce3(double& s, double& mx, double& mn,
 template <typename R, int STAGE>
 __global__ void __launch_bounds__(256, SOD_KG_MIN_BLOCKS) k_gather_rk(const GatherArgs a) {
   const int n = blockIdx.x * blockDim.x + threadIdx.x;
-  // a row without elements is a periodic slave (not in lpoin_w): rk_4_main's node loops
-  // (time_integ.f90:267-285,445-471) and the lumped solve (mod_solver.f90:23-58) skip it, its
-  // residual stays zero and its state untouched; only sutherland_viscosity, which runs over all
-  // npoin (time_integ.f90:483-487), re-evaluates its mu_fluid from its own Tem
-  const bool inrange = n < a.npoin;
-  const bool act = inrange && a.ptr[n + 1] > a.ptr[n];
-  if (inrange && !act) {
-    if constexpr (STAGE == 0) {
-#pragma unroll
-      for (int f = 0; f < 6; ++f)
-        if (a.out[f]) a.out[f][n] = 0.0;
-    } else if constexpr (STAGE == 4) {
-      const double T = a.Tem[n];
-      a.mu_fluid[n] = a.mu_factor[n] * kSuthC1 * (T * sqrt(T)) / (T + kSuthS);
-    }
-  }
   double eta_n = 0.0;
-  if (act) {
-    const R* rel = reinterpret_cast<const R*>(a.rel);
-    const size_t N = (size_t)a.npoin;
-    // node data independent of the gather, loaded first so their latency overlaps it
-    double yv[5], rsv[6];
-    if constexpr (STAGE >= 1) {
-#pragma unroll
-      for (int f = 0; f < 5; ++f) yv[f] = a.y[f][n];
-#pragma unroll
-      for (int f = 0; f < 6; ++f) rsv[f] = STAGE == 1 ? 0.0 : a.rsum[f * N + n];
-    }
-    const double ml = a.Ml[n];
-    double r[6] = {0, 0, 0, 0, 0, 0};
-    const int beg = a.ptr[n], end = a.ptr[n + 1];
-    int c = beg;
-    // groups of 4 contributions: all loads issued before the (ascending, fixed-order) sums
-    for (; c + 4 <= end; c += 4) {
-      R v[4][6];
-#pragma unroll
-      for (int q = 0; q < 4; ++q) load_res6<R>(rel, (size_t)a.idx[c + q], v[q]);
-#pragma unroll
-      for (int q = 0; q < 4; ++q)
-#pragma unroll
-        for (int f = 0; f < 6; ++f) r[f] += (double)v[q][f];
-    }
-    for (; c < end; ++c) {
-      R v[6];
-      load_res6<R>(rel, (size_t)a.idx[c], v);
-#pragma unroll
-      for (int f = 0; f < 6; ++f) r[f] += (double)v[f];
-    }
-    if (a.src) {
-      // mom_source_const_vect (elem_source.f90:20-55): - sum_e gpvol s = - Ml s on the momentum
-#pragma unroll
-      for (int d = 0; d < 3; ++d) r[1 + d] -= ml * a.src[d * N + n];
-    }
-    if (a.wm) {
-      // wall model: the modelled shear added to Rdiff_mom (time_integ.f90:334-357)
-#pragma unroll
-      for (int d = 0; d < 3; ++d) r[1 + d] += a.wm[d * N + n];
-    }
-#pragma unroll
-    for (int f = 0; f < 6; ++f) r[f] = r[f] / ml;
-    if constexpr (STAGE == 0) {
-#pragma unroll
-      for (int f = 0; f < 6; ++f)
-        if (a.out[f]) a.out[f][n] = r[f];
-    } else {
-      const double dt = a.node_member ? a.dt[a.node_member[n]] : *a.dt;
-      double rs[6];
-#pragma unroll
-      for (int f = 0; f < 6; ++f) rs[f] = rsv[f] + a.b_cur * r[f];
-      if constexpr (STAGE < 4) {
-#pragma unroll
-        for (int f = 0; f < 6; ++f) a.rsum[f * N + n] = rs[f];
-        const double da = dt * a.a_next;
-#pragma unroll
-        for (int f = 0; f < 5; ++f) a.ys[f * N + n] = yv[f] - da * r[f];
-      } else {
-        // RK update (time_integ.f90:417-426) and EOS at the new level (:445-463)
-        double y[5];
-#pragma unroll
-        for (int f = 0; f < 5; ++f) {
-          y[f] = yv[f] - dt * rs[f];
-          a.y[f][n] = y[f];
-        }
-        if (!(isfinite(y[0]) && isfinite(y[1]) && isfinite(y[2]) && isfinite(y[3]) && isfinite(y[4])))
-          atomicOr(a.nonfinite, 1u);
-        const double g = a.gamma;
-        const double rho = y[0];
-        const double u0 = y[1] / rho, u1 = y[2] / rho, u2 = y[3] / rho;
-        double umag = u0 * u0 + u1 * u1 + u2 * u2;
-        const double ei = (y[4] / rho) - 0.5 * umag;
-        const double pr = rho * (g - 1.0) * ei;
-        const double cs = sqrt(g * pr / rho);
-        umag = sqrt(umag);
-        const double T = pr / (rho * a.Rgas);
-        const double eta = (rho / (g - 1.0)) * log(pr / pow(rho, g));
-        a.u0[n] = u0; a.u1[n] = u1; a.u2[n] = u2;
-        a.e_int[n] = ei; a.pr[n] = pr; a.csound[n] = cs; a.machno[n] = umag / cs;
-        a.Tem[n] = T; a.eta[n] = eta;
-        a.mu_fluid[n] = a.mu_factor[n] * kSuthC1 * (T * sqrt(T)) / (T + kSuthS);
-        if (a.Reta) a.Reta[n] = -rs[5];
-        eta_n = eta;
-      }
-    }
-  }
+  const bool act = gather_rk_node<R, STAGE>(a, n, eta_n);
   if constexpr (STAGE == 4) {
     if (a.member_reduce) return;  // uniform across the grid
-    // entropy normalisation (mod_entropy_viscosity.f90:43-66): sum, max, min of eta
     __shared__ double sh[3 * 8];
-    __shared__ bool last;
-    double s = act ? eta_n : 0.0, mx = act ? eta_n : -1e300, mn = act ? eta_n : 1e300;
-    block_reduce3(s, mx, mn, sh);
-    if (threadIdx.x == 0) {
-      a.red[3 * blockIdx.x] = s;
-      a.red[3 * blockIdx.x + 1] = mx;
-      a.red[3 * blockIdx.x + 2] = mn;
-      __threadfence();
-      unsigned int done = atomicAdd(a.counter, 1u);
-      last = (done == gridDim.x - 1);
-    }
-    __syncthreads();
-    if (last) {
-      __threadfence();
-      // fixed-order final reduction by the last block (deterministic)
-      double ts = 0.0, tmx = -1e300, tmn = 1e300;
-#pragma unroll 4
-      for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x) {
-        ts += __ldcg(a.red + 3 * b);
-        tmx = fmax(tmx, __ldcg(a.red + 3 * b + 1));
-        tmn = fmin(tmn, __ldcg(a.red + 3 * b + 2));
-      }
-      __syncthreads();
-      block_reduce3(ts, tmx, tmn, sh);
-      if (threadIdx.x == 0) {
-        if (a.normalise) {
-          const double mean = ts / (double)a.nwork;
-          a.scal[0] = mean;
-          a.scal[1] = fmax(tmx - mean, mean - tmn);
-        } else {
-          a.scal[0] = 0.0;
-          a.scal[1] = 1.0;
-        }
-        *a.counter = 0u;
-      }
-    }
+    gather_eta_reduce(a, act ? eta_n : 0.0, act ? eta_n : -1e300, act ? eta_n : 1e300, sh);
   }
 }
-
-// ---------------------------------------------------------------------------------------------
-// KV: smart_visc_spectral (mod_entropy_viscosity.f90:68-121) per element with the convertIJK
-// filter (mod_filters.f90:42-51), fused with the per-element CFL limits of adapt_dt_cfl
-// (mod_time_ops.f90:31-56) and a deterministic min reduction to the next dt.
-// ---------------------------------------------------------------------------------------------
-struct ViscArgs {
-  int nelem;
-  const int32_t* __restrict__ econn;
-  const double* __restrict__ Reta;
-  const double* __restrict__ rho;
-  const double* __restrict__ u0;
-  const double* __restrict__ u1;
-  const double* __restrict__ u2;
-  const double* __restrict__ csound;
-  const double* __restrict__ Tem;
-  const double* __restrict__ mu_fluid;
-  const double* __restrict__ musgs;  // [e][64] or null
-  const double* __restrict__ helem_l;
-  const double* __restrict__ helem;
-  const double* __restrict__ jratio;
-  const double* __restrict__ scal;   // [0] mean, [1] norm
-  double* mue;                       // out FP64 [e][64]
-  float* mue32;                      // optional FP32 copy
-  double* dt_bits;                   // scratch scalar(s) receiving the min dt (bits, pre-set large)
-  const int32_t* __restrict__ elem_member;  // ensemble: member of each element (null = one mesh)
-  const double* __restrict__ member_scal;   // ensemble: [member][2] eta mean, norm
-  double* dt_out;                    // device scalar (may be null)
-  DevParams prm;
-};
-
-__device__ __forceinline__ int nb_filter(int x) {
-  // natural index of convertIJK(x+1): x=-1 -> 1, 0..3 -> x, 4 -> 1 (reference quirk)
-  return (x < 0) ? 1 : ((x > 3) ? 1 : x);
-}
-
-constexpr int KV_EPB = 4;
 
 #ifndef SOD_KV_MIN_BLOCKS
 #define SOD_KV_MIN_BLOCKS 8  // resident blocks per SM the register budget must allow
 #endif
 __global__ void __launch_bounds__(64 * KV_EPB, SOD_KV_MIN_BLOCKS) k_visc_dt(const ViscArgs a) {
-  __shared__ double ml[KV_EPB][NN];
-  __shared__ double fl[KV_EPB][NN];  // filter pass buffer
-  __shared__ double wm[KV_EPB][2][5];
-  __shared__ double elem_s[KV_EPB][2];  // ced, dt limit of the element
-  const int es = threadIdx.x >> 6, d = threadIdx.x & 63;
-  const int e = blockIdx.x * KV_EPB + es;
-  const bool act = e < a.nelem;
-  const int ee = act ? e : a.nelem - 1;
-  const int n = a.econn[(size_t)ee * NN + d];
-  const double rho = a.rho[n], u0 = a.u0[n], u1 = a.u1[n], u2 = a.u2[n], cs = a.csound[n], T = a.Tem[n];
-  // inputs of the second half, loaded before the element reductions so their latency overlaps them
-  const double reta_n = a.Reta[n];
-  const double hl = a.helem_l[(size_t)ee * NN + d];
-  const double vmag = sqrt(u0 * u0 + u1 * u1 + u2 * u2);
-  const double he = a.helem[ee];
-  // betae node term (mod_entropy_viscosity.f90:90-95)
-  const double beta_n = (rho * he) * (a.prm.cmax / (double)P) * (vmag + sqrt(a.prm.Rgas * a.prm.gamma * T));
-  // CFL node terms (mod_time_ops.f90:36-50)
-  const double umax = fmax(fmax(fabs(u0), fabs(u1)), fabs(u2));
-  const double L3n = umax + cs;
-  const double musgs = a.musgs ? a.musgs[(size_t)ee * NN + d] : 0.0;
-  const double mun = (rho * musgs + a.mu_fluid[n]) / rho;
-  // element maxima over the 64 nodes (two warps per element)
-  double mV = vmag, mC = cs, mB = beta_n, mL = L3n, mM = mun;
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    mV = fmax(mV, __shfl_xor_sync(0xffffffffu, mV, o));
-    mC = fmax(mC, __shfl_xor_sync(0xffffffffu, mC, o));
-    mB = fmax(mB, __shfl_xor_sync(0xffffffffu, mB, o));
-    mL = fmax(mL, __shfl_xor_sync(0xffffffffu, mL, o));
-    mM = fmax(mM, __shfl_xor_sync(0xffffffffu, mM, o));
-  }
-  const int wi = d >> 5;
-  if ((d & 31) == 0) { wm[es][wi][0] = mV; wm[es][wi][1] = mC; wm[es][wi][2] = mB; wm[es][wi][3] = mL; wm[es][wi][4] = mM; }
-  __syncthreads();
-  if (d == 0) {
-    // shock sensor and cap, once per element (mod_entropy_viscosity.f90:81-84); M**15 as an
-    // integer power like the reference
-    const double M = fmax(wm[es][0][0], wm[es][1][0]) / fmax(wm[es][0][1], wm[es][1][1]);
-    const double M2 = M * M, M4 = M2 * M2, M8 = M4 * M4;
-    const double M15 = M8 * M4 * M2 * M;
-    const double ceM = fmax(tanh(M15 * 3.141592653589793), a.prm.ce);
-    double ced = fmax(1.0 - a.jratio[ee], a.prm.ce);
-    elem_s[es][0] = fmax(ced, ceM);
-    const double hh = he / (double)(2.0 * P + 1);
-    const double L3 = fmax(wm[es][0][3], wm[es][1][3]);
-    const double maxMU = fmax(wm[es][0][4], wm[es][1][4]);
-    elem_s[es][1] = fmin(a.prm.cfl_conv * hh / L3, a.prm.cfl_diff * (hh * hh) / maxMU);
-  }
-  __syncthreads();
-  const double ced = elem_s[es][0];
-  mB = fmax(wm[es][0][2], wm[es][1][2]);
-  const int mem = a.elem_member ? a.elem_member[ee] : 0;
-  const double norm = a.elem_member ? a.member_scal[2 * mem + 1] : a.scal[1];
-  const double R1 = (norm > 0.0) ? rho * fabs(reta_n) / norm : 0.0;
-  const double Ve = ced * R1 * hl * hl;
-  ml[es][d] = a.prm.cglob * fmin(Ve, mB);
-  __syncthreads();
-  // 3x3x3 filter with weights (1/4,1/2,1/4) through convertIJK (mod_entropy_viscosity.f90:102-120):
-  // the weights and the index map are separable, so it runs as three 3-point passes (xi, eta,
-  // zeta) through shared memory, 9 reads per node instead of 27
-  const int i = d & 3, j = (d >> 2) & 3, k = d >> 4;
-  const int ix[3] = {nb_filter(i - 1), i, nb_filter(i + 1)};
-  const int jx[3] = {nb_filter(j - 1), j, nb_filter(j + 1)};
-  const int kx[3] = {nb_filter(k - 1), k, nb_filter(k + 1)};
-  const double w[3] = {0.25, 0.5, 0.25};
-  fl[es][d] = w[0] * ml[es][ix[0] + 4 * j + 16 * k] + w[1] * ml[es][d] + w[2] * ml[es][ix[2] + 4 * j + 16 * k];
-  __syncthreads();
-  // ml's first-pass reads all happened before the barrier above, so it takes the second pass
-  ml[es][d] = w[0] * fl[es][i + 4 * jx[0] + 16 * k] + w[1] * fl[es][d] + w[2] * fl[es][i + 4 * jx[2] + 16 * k];
-  __syncthreads();
-  const double acc = w[0] * ml[es][i + 4 * j + 16 * kx[0]] + w[1] * ml[es][d] + w[2] * ml[es][i + 4 * j + 16 * kx[2]];
-  if (act) {
-    a.mue[(size_t)e * NN + d] = acc;
-    if (a.mue32) a.mue32[(size_t)e * NN + d] = (float)acc;
-    // next dt: order-independent min over elements on the bit pattern of a positive double
-    if (a.dt_out && d == 0)
-      atomicMin(reinterpret_cast<unsigned long long*>(a.dt_bits) + mem,
-                (unsigned long long)__double_as_longlong(elem_s[es][1]));
-  }
+  __shared__ double sm[KV_EPB][KV_SMEM];
+  const int es = threadIdx.x >> 6;
+  visc_dt_elem(a, blockIdx.x * KV_EPB + es, threadIdx.x & 63, sm[es]);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -655,13 +374,81 @@ static int set_rhs_attr() {
                                 (int)rhs_smem_bytes<R>(EPB)));
   SOD_CUDA(cudaFuncSetAttribute(k_rhs_fused<R, EPB, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)rhs_smem_bytes<R>(EPB)));
+  SOD_CUDA(cudaFuncSetAttribute(k_stage_fused<EPB, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)rhs_smem_bytes<double>(EPB)));
+  SOD_CUDA(cudaFuncSetAttribute(k_stage_fused<EPB, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)rhs_smem_bytes<double>(EPB)));
   return SOD_OK;
+}
+
+// Cooperative launch of one persistent FP64 stage; ctas_per_sm <= 0 asks for the most that fit.
+template <int EPB>
+static int launch_stage_fused_t(const StageArgs& p, int ctas_per_sm, int* grid_out, cudaStream_t st) {
+  const bool toth = p.r.prm.total_enthalpy != 0;
+  const void* fn = toth ? (const void*)k_stage_fused<EPB, true> : (const void*)k_stage_fused<EPB, false>;
+  const size_t smem = rhs_smem_bytes<double>(EPB);
+  int occ = 0, dev = 0, nsm = 0;
+  SOD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, 64 * EPB, smem));
+  SOD_CUDA(cudaGetDevice(&dev));
+  SOD_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  if (occ <= 0) {
+    set_error("persistent stage kernel: no resident block fits (EPB %d)", EPB);
+    return SOD_ERR_UNSUPPORTED;
+  }
+  const int per = (ctas_per_sm > 0 && ctas_per_sm < occ) ? ctas_per_sm : occ;
+  const int ntiles = (p.r.nelem + EPB - 1) / EPB;
+  const int grid = std::min(per * nsm, ntiles);
+  if (grid_out) *grid_out = grid;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(64 * EPB);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  void* args[] = {const_cast<StageArgs*>(&p)};
+  SOD_CUDA(cudaLaunchKernelExC(&cfg, fn, args));
+  SOD_CHECK_LAUNCH();
+  return SOD_OK;
+}
+
+int launch_stage_mixed2(const StageArgs& p, int epb, int ctas_per_sm, int* grid_out, cudaStream_t st);
+void stage_mixed2_info(int epb, bool toth, const void** fn, size_t* smem);
+
+// the persistent stage kernel of a configuration and its dynamic shared memory
+void persist_kernel_info(bool mixed, int epb, bool toth, const void** fn, size_t* smem) {
+  if (mixed) {
+    stage_mixed2_info(epb, toth, fn, smem);
+    return;
+  }
+  switch (epb) {
+    case 1: *fn = toth ? (const void*)k_stage_fused<1, true> : (const void*)k_stage_fused<1, false>; break;
+    case 4: *fn = toth ? (const void*)k_stage_fused<4, true> : (const void*)k_stage_fused<4, false>; break;
+    case 8: *fn = toth ? (const void*)k_stage_fused<8, true> : (const void*)k_stage_fused<8, false>; break;
+    default: *fn = toth ? (const void*)k_stage_fused<2, true> : (const void*)k_stage_fused<2, false>; epb = 2;
+  }
+  *smem = rhs_smem_bytes<double>(epb);
+}
+
+// One persistent stage launch of either precision
+int launch_stage(const StageArgs& p, bool mixed, int epb, int ctas_per_sm, int* grid_out, cudaStream_t st) {
+  if (mixed) return launch_stage_mixed2(p, epb, ctas_per_sm, grid_out, st);
+  switch (epb) {
+    case 1: return launch_stage_fused_t<1>(p, ctas_per_sm, grid_out, st);
+    case 4: return launch_stage_fused_t<4>(p, ctas_per_sm, grid_out, st);
+    case 8: return launch_stage_fused_t<8>(p, ctas_per_sm, grid_out, st);
+    default: return launch_stage_fused_t<2>(p, ctas_per_sm, grid_out, st);
+  }
 }
 
 int init_kernel_attrs() {
   static bool done = false;
   if (done) return SOD_OK;
   int rc = set_rhs_attr<double, 1>() | set_rhs_attr<double, 2>() | set_rhs_attr<double, 4>() |
+           set_rhs_attr<double, 8>() |
            init_rhs_mixed2_attrs();
   if (rc) return SOD_ERR_CUDA;
   done = true;
@@ -680,9 +467,8 @@ static int launch_rhs_t(const RhsArgs& a, cudaStream_t st) {
   return SOD_OK;
 }
 
-int launch_rhs(SodMesh* m, bool mixed, int epb, const double* rho, const double* q0, const double* q1,
-               const double* q2, const double* E, const double* mu_factor, const double* musgs_int,
-               cudaStream_t st) {
+static RhsArgs make_rhs_args(SodMesh* m, bool mixed, const double* rho, const double* q0, const double* q1,
+                             const double* q2, const double* E, const double* mu_factor, const double* musgs_int) {
   RhsArgs a;
   a.nelem = m->nelem;
   a.econn = m->econn;
@@ -696,10 +482,18 @@ int launch_rhs(SodMesh* m, bool mixed, int epb, const double* rho, const double*
   for (int r = 0; r < NP1; ++r)
     for (int c = 0; c < NP1; ++c) a.Df[r][c] = (float)m->D.d[r][c];
   a.prm = m->prm;
+  return a;
+}
+
+int launch_rhs(SodMesh* m, bool mixed, int epb, const double* rho, const double* q0, const double* q1,
+               const double* q2, const double* E, const double* mu_factor, const double* musgs_int,
+               cudaStream_t st) {
+  const RhsArgs a = make_rhs_args(m, mixed, rho, q0, q1, q2, E, mu_factor, musgs_int);
   if (!mixed) {
     switch (epb) {
       case 1: return launch_rhs_t<double, 1>(a, st);
       case 4: return launch_rhs_t<double, 4>(a, st);
+      case 8: return launch_rhs_t<double, 8>(a, st);
       default: return launch_rhs_t<double, 2>(a, st);
     }
   } else {
@@ -724,9 +518,10 @@ static int launch_gather_t(int stage, const GatherArgs& a, cudaStream_t st) {
   return SOD_OK;
 }
 
-int launch_gather(SodMesh* m, bool mixed, int stage, GatherArgs& a, cudaStream_t st) {
+static void fill_gather_args(SodMesh* m, int stage, GatherArgs& a) {
   a.npoin = m->npoin;
   a.nwork = m->npoin_w;
+  a.slaves = m->has_slaves ? 1 : 0;
   a.ptr = m->n2e_ptr;
   a.idx = m->n2e;
   a.rel = m->buf.rel;
@@ -746,6 +541,10 @@ int launch_gather(SodMesh* m, bool mixed, int stage, GatherArgs& a, cudaStream_t
     a.b_cur = kB[stage - 1];
     a.a_next = stage < 4 ? kA[stage] : 0.0;
   }
+}
+
+int launch_gather(SodMesh* m, bool mixed, int stage, GatherArgs& a, cudaStream_t st) {
+  fill_gather_args(m, stage, a);
   return mixed ? launch_gather_t<float>(stage, a, st) : launch_gather_t<double>(stage, a, st);
 }
 
@@ -766,7 +565,7 @@ int les_out(SodMesh* m, const SodState* s, cudaStream_t st) {
   return mesh_internal_to_ref_elem(m, m->musgs_int, s->mu_sgs, st);
 }
 
-int launch_visc_dt(SodMesh* m, const SodState* s, double* dt_out, float* mue32, cudaStream_t st) {
+static ViscArgs make_visc_args(SodMesh* m, const SodState* s, double* dt_out, float* mue32) {
   ViscArgs v;
   v.nelem = m->nelem;
   v.econn = m->econn;
@@ -785,12 +584,17 @@ int launch_visc_dt(SodMesh* m, const SodState* s, double* dt_out, float* mue32, 
   v.scal = m->buf.scal;
   v.mue = m->mue_int;
   v.mue32 = mue32;
-  const int nm = m->nmember > 0 ? m->nmember : 1;
   v.dt_bits = m->nmember > 0 ? m->member_dt_bits : m->buf.scal + 3;
   v.elem_member = m->nmember > 0 ? m->elem_member : nullptr;
   v.member_scal = m->member_scal;
   v.dt_out = dt_out;
   v.prm = m->prm;
+  return v;
+}
+
+int launch_visc_dt(SodMesh* m, const SodState* s, double* dt_out, float* mue32, cudaStream_t st) {
+  const ViscArgs v = make_visc_args(m, s, dt_out, mue32);
+  const int nm = m->nmember > 0 ? m->nmember : 1;
   if (dt_out) SOD_CUDA(cudaMemsetAsync(v.dt_bits, 0x7F, sizeof(double) * nm, st));  // 1.38e306 each
   const int grid = (m->nelem + KV_EPB - 1) / KV_EPB;
   k_visc_dt<<<grid, 64 * KV_EPB, 0, st>>>(v);
@@ -828,6 +632,45 @@ static double* reta_scratch(SodMesh* m) {
   return m->buf.rsum + 5 * (size_t)m->npoin;  // rsum eta column is dead after stage 4 reads it
 }
 
+// The periodic step (no boundaries, buffer zone, wall model, source term or LES) as four
+// cooperative launches, one per RK stage: fused RHS, grid barrier, gather / stage update; the
+// last one also forms the entropy viscosity and the next dt.  Same arithmetic per element and
+// per node as the two-launch path; the entropy sums are blocked by the persistent grid instead,
+// so the normalisation can differ from that path's in the last bits.
+static int run_step_persist(SodMesh* m, SodState* s, SodState& loc, const double* dt_dev, double* dt_next,
+                            bool mixed, int epb, int ctas_per_sm, cudaStream_t st) {
+  NvtxRange range(mixed ? "sod rk4 step persistent (mixed)" : "sod rk4 step persistent (fp64)");
+  const size_t N = m->npoin;
+  StageArgs p{};
+  p.g.dt = dt_dev;
+  p.g.y[0] = s->rho; p.g.y[1] = s->q; p.g.y[2] = s->q + N; p.g.y[3] = s->q + 2 * N; p.g.y[4] = s->E;
+  p.g.u0 = s->u; p.g.u1 = s->u + N; p.g.u2 = s->u + 2 * N;
+  p.g.pr = s->pr; p.g.Tem = s->Tem; p.g.e_int = s->e_int; p.g.eta = s->eta; p.g.csound = s->csound;
+  p.g.machno = s->machno; p.g.mu_fluid = s->mu_fluid; p.g.Reta = loc.Reta; p.g.mu_factor = s->mu_factor;
+  p.g.node_member = m->nmember > 0 ? m->node_member : nullptr;
+  p.g.member_reduce = m->nmember > 0 ? 1 : 0;
+  p.nmember = m->nmember;
+  p.member_node_off = m->member_node_off;
+  p.member_scal = m->member_scal;
+  p.v = make_visc_args(m, &loc, dt_next, mixed ? m->mue32 : nullptr);
+  const int nm = m->nmember > 0 ? m->nmember : 1;
+  for (int stage = 1; stage <= 4; ++stage) {
+    const double* y = m->buf.ys;
+    if (stage == 1)
+      p.r = make_rhs_args(m, mixed, s->rho, s->q, s->q + N, s->q + 2 * N, s->E, s->mu_factor, nullptr);
+    else
+      p.r = make_rhs_args(m, mixed, y, y + N, y + 2 * N, y + 3 * N, y + 4 * N, s->mu_factor, nullptr);
+    p.g.ys = nullptr;
+    fill_gather_args(m, stage, p.g);
+    p.stage = stage;
+    if (stage == 4 && dt_next) SOD_CUDA(cudaMemsetAsync(p.v.dt_bits, 0x7F, sizeof(double) * nm, st));
+    if (int rc = launch_stage(p, mixed, epb, ctas_per_sm, nullptr, st)) return rc;
+    if (stage == 4 && dt_next)
+      SOD_CUDA(cudaMemcpyAsync(dt_next, p.v.dt_bits, sizeof(double) * nm, cudaMemcpyDeviceToDevice, st));
+  }
+  return SOD_OK;
+}
+
 // One RK4 step on device state (mu_e already in m->mue_int / mue32).  When ev is non-null,
 // ev[2*slot] / ev[2*slot+1] bracket each kernel: slots 0-3 KR stages, 4-7 KG stages, 8 KV.
 // When stage_store is non-null the stage states Y2, Y3, Y4 (5 columns of npoin each) are
@@ -851,6 +694,9 @@ int run_step(SodMesh* m, SodState* s, const double* dt_dev, double* dt_next, boo
   const bool bc = m->bc.nb > 0;
   const bool zone = m->zone.nb > 0;
   const bool pre = bc || zone;
+  const int pctas = m->persist_ctas[mixed ? 1 : 0];
+  if (pctas > 0 && !pre && !les && m->wmodel.nw == 0 && !m->source && !ev && !stage_store)
+    return run_step_persist(m, s, loc, dt_dev, dt_next, mixed, epb, pctas, st);
   auto pre_stage = [&](double* ys, int stage_of) -> int {
     if (zone)
       if (int r = zone_stage(m, ys, st)) return r;
@@ -1095,7 +941,7 @@ int sod_set_rhs_config(SodMesh* m, SodPrecision prec, int config) {
   SOD_ARG(m, "mesh null");
   SOD_ARG(prec == SOD_FP64 || prec == SOD_MIXED, "precision");
   const bool mixed = prec == SOD_MIXED;
-  const bool ok = (config == 1 || config == 2 || config == 4 || (mixed && config == 8));
+  const bool ok = (config == 1 || config == 2 || config == 4 || config == 8);
   SOD_ARG(ok || config == 0, "unknown fused-RHS configuration");
   if (m->tuned_epb[mixed ? 1 : 0] != config) {
     for (auto& kv : m->graphs)
@@ -1104,6 +950,34 @@ int sod_set_rhs_config(SodMesh* m, SodPrecision prec, int config) {
   }
   m->tuned_epb[mixed ? 1 : 0] = config;
   return SOD_OK;
+}
+
+int sod_set_stage_launch(SodMesh* m, SodPrecision prec, int ctas_per_sm) {
+  SOD_ARG(m, "mesh null");
+  SOD_ARG(prec == SOD_FP64 || prec == SOD_MIXED, "precision");
+  SOD_ARG(ctas_per_sm >= 0 && ctas_per_sm <= 32, "ctas_per_sm must be in 0..32");
+  const int i = prec == SOD_MIXED ? 1 : 0;
+  if (m->persist_ctas[i] != ctas_per_sm) {
+    for (auto& kv : m->graphs)
+      if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+    m->graphs.clear();
+  }
+  m->persist_ctas[i] = ctas_per_sm;
+  return SOD_OK;
+}
+
+int sod_autotune_table(SodMesh* m, SodPrecision prec, int cap, int32_t* epb, int32_t* ctas_per_sm,
+                       float* ms_per_stage) {
+  SOD_ARG(m, "mesh null");
+  SOD_ARG(prec == SOD_FP64 || prec == SOD_MIXED, "precision");
+  const auto& t = m->tune_table[prec == SOD_MIXED ? 1 : 0];
+  const int n = (int)t.size();
+  for (int q = 0; q < n && q < cap; ++q) {
+    if (epb) epb[q] = t[q].epb;
+    if (ctas_per_sm) ctas_per_sm[q] = t[q].ctas;
+    if (ms_per_stage) ms_per_stage[q] = t[q].ms;
+  }
+  return n;
 }
 
 int sod_autotune(SodMesh* m, SodState* s, SodPrecision prec, int* best_epb, float* best_ms, sod_stream_t stream) {
@@ -1123,35 +997,103 @@ int sod_autotune(SodMesh* m, SodState* s, SodPrecision prec, int* best_epb, floa
     if (rc) return rc;
   }
   const size_t N = m->npoin;
-  const int fp64_cand[] = {1, 2, 4};
-  const int mixed_cand[] = {1, 2, 4, 8};
-  const int* cand = mixed ? mixed_cand : fp64_cand;
-  const int nc = mixed ? 4 : 3;
+  const int cand[] = {1, 2, 4, 8};
   cudaEvent_t e0, e1;
   SOD_CUDA(cudaEventCreate(&e0));
   SOD_CUDA(cudaEventCreate(&e1));
-  int best = 0;
-  float bms = 1e30f;
-  for (int c = 0; c < nc && rc == SOD_OK; ++c) {
-    for (int r = 0; r < 3 && rc == SOD_OK; ++r)
-      rc = launch_rhs(m, mixed, cand[c], s->rho, s->q, s->q + N, s->q + 2 * N, s->E, s->mu_factor, nullptr, st);
+  // One RK stage 1 per trial (fused RHS + gather / stage update into the internal stage buffers;
+  // the caller's state is only read).  Two dimensions: elements per CTA, and the launch shape -
+  // two launches per stage (ctas 0) or one cooperative launch of c resident CTAs per SM.
+  const bool plain = m->bc.nb == 0 && m->zone.nb == 0 && m->wmodel.nw == 0 && !m->source && !les_active(m, s);
+  auto& table = m->tune_table[mixed ? 1 : 0];
+  table.clear();
+  GatherArgs g{};
+  g.dt = m->buf.scal + 4;  // any finite scalar: stage 1 scales its stage-state update by it
+  SOD_CUDA(cudaMemsetAsync(m->buf.scal + 4, 0, sizeof(double), st));
+  g.y[0] = s->rho; g.y[1] = s->q; g.y[2] = s->q + N; g.y[3] = s->q + 2 * N; g.y[4] = s->E;
+  g.mu_factor = s->mu_factor;
+  g.node_member = nullptr;  // one dt scalar for the timing (an ensemble's per-member dt is not needed)
+  auto trial = [&](int epb, int ctas, float* ms_out) -> int {
+    int r2 = SOD_OK;
+    auto once = [&]() -> int {
+      if (ctas == 0) {
+        int r3 = launch_rhs(m, mixed, epb, s->rho, s->q, s->q + N, s->q + 2 * N, s->E, s->mu_factor, nullptr, st);
+        if (r3) return r3;
+        GatherArgs gg = g;
+        return launch_gather(m, mixed, 1, gg, st);
+      }
+      StageArgs p{};
+      p.r = make_rhs_args(m, mixed, s->rho, s->q, s->q + N, s->q + 2 * N, s->E, s->mu_factor, nullptr);
+      p.g = g;
+      fill_gather_args(m, 1, p.g);
+      p.stage = 1;
+      return launch_stage(p, mixed, epb, ctas, nullptr, st);
+    };
+    for (int r = 0; r < 3 && r2 == SOD_OK; ++r) r2 = once();
     cudaEventRecord(e0, st);
-    for (int r = 0; r < 10 && rc == SOD_OK; ++r)
-      rc = launch_rhs(m, mixed, cand[c], s->rho, s->q, s->q + N, s->q + 2 * N, s->E, s->mu_factor, nullptr, st);
+    for (int r = 0; r < 10 && r2 == SOD_OK; ++r) r2 = once();
     cudaEventRecord(e1, st);
-    if (rc) break;
-    if (cudaEventSynchronize(e1) != cudaSuccess) { rc = SOD_ERR_CUDA; break; }
-    float ms = 0.f;
-    cudaEventElapsedTime(&ms, e0, e1);
-    ms /= 10.f;
-    if (ms < bms) { bms = ms; best = cand[c]; }
+    if (r2) return r2;
+    if (cudaEventSynchronize(e1) != cudaSuccess) return SOD_ERR_CUDA;
+    cudaEventElapsedTime(ms_out, e0, e1);
+    *ms_out /= 10.f;
+    return SOD_OK;
+  };
+  int best = 0, best_ctas = 0;
+  float bms = 1e30f, bms_rhs = 1e30f;
+  for (int c = 0; c < 4 && rc == SOD_OK; ++c) {
+    const int epb = cand[c];
+    // the fused RHS alone (reported as best_ms, as before)
+    {
+      for (int r = 0; r < 3 && rc == SOD_OK; ++r)
+        rc = launch_rhs(m, mixed, epb, s->rho, s->q, s->q + N, s->q + 2 * N, s->E, s->mu_factor, nullptr, st);
+      cudaEventRecord(e0, st);
+      for (int r = 0; r < 10 && rc == SOD_OK; ++r)
+        rc = launch_rhs(m, mixed, epb, s->rho, s->q, s->q + N, s->q + 2 * N, s->E, s->mu_factor, nullptr, st);
+      cudaEventRecord(e1, st);
+      if (rc) break;
+      if (cudaEventSynchronize(e1) != cudaSuccess) { rc = SOD_ERR_CUDA; break; }
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      bms_rhs = std::min(bms_rhs, ms / 10.f);
+    }
+    // launch shapes: two launches, then persistent grids of occ, 3/4 occ and 1/2 occ CTAs per SM
+    int shapes[4] = {0, 0, 0, 0}, ns = 1;
+    if (plain) {
+      const void* fn = nullptr;
+      size_t smem = 0;
+      persist_kernel_info(mixed, epb, m->prm.total_enthalpy != 0, &fn, &smem);
+      int occ = 0;
+      if (fn && cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, 64 * epb, smem) == cudaSuccess && occ > 0) {
+        const int opts[3] = {occ, std::max(1, (3 * occ) / 4), std::max(1, occ / 2)};
+        for (int o : opts) {
+          bool dup = false;
+          for (int q = 1; q < ns; ++q) dup |= shapes[q] == o;
+          if (!dup) shapes[ns++] = o;
+        }
+      }
+    }
+    for (int q = 0; q < ns && rc == SOD_OK; ++q) {
+      float ms = 0.f;
+      rc = trial(epb, shapes[q], &ms);
+      if (rc) break;
+      table.push_back(SodMesh::TuneEntry{epb, shapes[q], ms});
+      if (ms < bms) { bms = ms; best = epb; best_ctas = shapes[q]; }
+    }
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   if (rc) return rc;
-  m->tuned_epb[mixed ? 1 : 0] = best;
+  const int i = mixed ? 1 : 0;
+  if (m->tuned_epb[i] != best || m->persist_ctas[i] != best_ctas) {
+    for (auto& kv : m->graphs)
+      if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+    m->graphs.clear();
+  }
+  m->tuned_epb[i] = best;
+  m->persist_ctas[i] = best_ctas;
   if (best_epb) *best_epb = best;
-  if (best_ms) *best_ms = bms;
+  if (best_ms) *best_ms = bms_rhs;
   return SOD_OK;
 }
 

@@ -17,7 +17,9 @@
 // where fe = rho H' u, fue = H' u, F = (q-q_r) x (u-u_r), Fuu = (u-u_r) x (u-u_r) and ^ marks
 // contravariant fluxes.
 #include "sod_internal.cuh"
+#include "sod_step_kernels.cuh"
 #include <cmath>
+#include <algorithm>
 
 namespace sod {
 namespace mx2 {
@@ -84,18 +86,18 @@ __device__ __forceinline__ float2 divT2(const float2* fx, const float2* fy, cons
 #ifndef SOD_MX2_MIN_CTAS
 #define SOD_MX2_MIN_CTAS 10  // resident 64-thread element groups per SM the register budget must allow
 #endif
+// One tile of EPB elements (64 threads each); smem_raw holds smem_bytes(EPB).  Every thread of
+// the block calls it (it holds block barriers).
 // TOTH: flag_total_enthalpy (energy convection of full_convec_ijk_H)
 template <int EPB, bool TOTH>
-__global__ void __launch_bounds__(64 * EPB, (EPB >= SOD_MX2_MIN_CTAS ? 1 : SOD_MX2_MIN_CTAS / EPB))
-    k_rhs_mixed2(const RhsArgs a) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+__device__ __forceinline__ void rhs_mixed2_tile(const RhsArgs& a, int tile, unsigned char* smem_raw) {
   double* refs_all = reinterpret_cast<double*>(smem_raw);
   float2* buf_all = reinterpret_cast<float2*>(smem_raw + sizeof(double) * EPB * NREF);
   const int tid = threadIdx.x;
   const int es = tid >> 6;
   const int d = tid & 63;
   const int i = d & 3, j = (d >> 2) & 3, k = d >> 4;
-  const int e = blockIdx.x * EPB + es;
+  const int e = tile * EPB + es;
   const bool active = e < a.nelem;
   const int ee = active ? e : a.nelem - 1;
   double* refs = refs_all + es * NREF;
@@ -404,12 +406,71 @@ __global__ void __launch_bounds__(64 * EPB, (EPB >= SOD_MX2_MIN_CTAS ? 1 : SOD_M
   }
 }
 
+template <int EPB, bool TOTH>
+__global__ void __launch_bounds__(64 * EPB, (EPB >= SOD_MX2_MIN_CTAS ? 1 : SOD_MX2_MIN_CTAS / EPB))
+    k_rhs_mixed2(const RhsArgs a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  rhs_mixed2_tile<EPB, TOTH>(a, blockIdx.x, smem_raw);
+}
+
+// One RK stage of the mixed path in one cooperative launch (persistent blocks): the fused RHS
+// over element tiles, then persist_stage_tail (gather / stage update; at stage 4 the entropy
+// viscosity and dt).
+template <int EPB, bool TOTH>
+__global__ void __launch_bounds__(64 * EPB, (EPB >= SOD_MX2_MIN_CTAS ? 1 : SOD_MX2_MIN_CTAS / EPB))
+    k_stage_mixed2(const StageArgs p) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int ntiles = (p.r.nelem + EPB - 1) / EPB;
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    rhs_mixed2_tile<EPB, TOTH>(p.r, t, smem_raw);
+    __syncthreads();  // the next tile reuses the shared memory
+  }
+  persist_stage_tail<float, EPB>(p, smem_raw);
+}
+
 template <int EPB>
 static int set_attr() {
   SOD_CUDA(cudaFuncSetAttribute(k_rhs_mixed2<EPB, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)smem_bytes(EPB)));
   SOD_CUDA(cudaFuncSetAttribute(k_rhs_mixed2<EPB, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)smem_bytes(EPB)));
+  SOD_CUDA(cudaFuncSetAttribute(k_stage_mixed2<EPB, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)smem_bytes(EPB)));
+  SOD_CUDA(cudaFuncSetAttribute(k_stage_mixed2<EPB, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)smem_bytes(EPB)));
+  return SOD_OK;
+}
+
+// Cooperative launch of one persistent stage; ctas_per_sm <= 0 asks for the most that fit.
+template <int EPB>
+static int launch_stage(const StageArgs& p, int ctas_per_sm, int* grid_out, cudaStream_t st) {
+  const bool toth = p.r.prm.total_enthalpy != 0;
+  const void* fn = toth ? (const void*)k_stage_mixed2<EPB, true> : (const void*)k_stage_mixed2<EPB, false>;
+  int occ = 0, dev = 0, nsm = 0;
+  SOD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, 64 * EPB, smem_bytes(EPB)));
+  SOD_CUDA(cudaGetDevice(&dev));
+  SOD_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  if (occ <= 0) {
+    set_error("persistent stage kernel: no resident block fits (EPB %d)", EPB);
+    return SOD_ERR_UNSUPPORTED;
+  }
+  const int per = (ctas_per_sm > 0 && ctas_per_sm < occ) ? ctas_per_sm : occ;
+  const int ntiles = (p.r.nelem + EPB - 1) / EPB;
+  const int grid = std::min(per * nsm, ntiles);
+  if (grid_out) *grid_out = grid;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(64 * EPB);
+  cfg.dynamicSmemBytes = smem_bytes(EPB);
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  void* args[] = {const_cast<StageArgs*>(&p)};
+  SOD_CUDA(cudaLaunchKernelExC(&cfg, fn, args));
+  SOD_CHECK_LAUNCH();
   return SOD_OK;
 }
 
@@ -432,6 +493,25 @@ int init_rhs_mixed2_attrs() {
   if (mx2::set_attr<1>() || mx2::set_attr<2>() || mx2::set_attr<4>() || mx2::set_attr<8>()) return SOD_ERR_CUDA;
   done = true;
   return SOD_OK;
+}
+
+void stage_mixed2_info(int epb, bool toth, const void** fn, size_t* smem) {
+  switch (epb) {
+    case 1: *fn = toth ? (const void*)mx2::k_stage_mixed2<1, true> : (const void*)mx2::k_stage_mixed2<1, false>; break;
+    case 2: *fn = toth ? (const void*)mx2::k_stage_mixed2<2, true> : (const void*)mx2::k_stage_mixed2<2, false>; break;
+    case 8: *fn = toth ? (const void*)mx2::k_stage_mixed2<8, true> : (const void*)mx2::k_stage_mixed2<8, false>; break;
+    default: *fn = toth ? (const void*)mx2::k_stage_mixed2<4, true> : (const void*)mx2::k_stage_mixed2<4, false>; epb = 4;
+  }
+  *smem = mx2::smem_bytes(epb);
+}
+
+int launch_stage_mixed2(const StageArgs& p, int epb, int ctas_per_sm, int* grid_out, cudaStream_t st) {
+  switch (epb) {
+    case 1: return mx2::launch_stage<1>(p, ctas_per_sm, grid_out, st);
+    case 2: return mx2::launch_stage<2>(p, ctas_per_sm, grid_out, st);
+    case 8: return mx2::launch_stage<8>(p, ctas_per_sm, grid_out, st);
+    default: return mx2::launch_stage<4>(p, ctas_per_sm, grid_out, st);
+  }
 }
 
 int launch_rhs_mixed2(const RhsArgs& a, int epb, cudaStream_t st) {

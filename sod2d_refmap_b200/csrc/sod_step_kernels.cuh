@@ -1,0 +1,418 @@
+// Device bodies of the node gather / RK stage update (KG) and of the entropy viscosity + CFL dt
+// (KV), shared by their stand-alone kernels (sod_rhs.cu) and by the persistent one-launch-per-
+// stage kernels (sod_rhs.cu for FP64, sod_rhs_mixed.cu for the mixed path).  Not part of the ABI.
+#pragma once
+#include "sod_internal.cuh"
+#include <cooperative_groups.h>
+
+namespace sod {
+
+// ---------------------------------------------------------------------------------------------
+// KG: ordered CSR gather of the element residuals, /Ml, RK accumulate and next stage state.
+// STAGE 0 = plain RHS (gather + /Ml into output arrays).  STAGE 4 = final update + EOS.
+// ---------------------------------------------------------------------------------------------
+struct GatherArgs {
+  int npoin;
+  int nwork;                      // working nodes (rows with elements): the entropy mean's count
+  int slaves;                     // 1 when some rows have no elements (periodic slave rows)
+  const int32_t* __restrict__ ptr;
+  const int32_t* __restrict__ idx;
+  const void* rel;
+  const double* __restrict__ Ml;
+  const double* __restrict__ dt;  // device scalar, or per-member array when node_member is set
+  const int32_t* __restrict__ node_member;
+  int member_reduce;              // stage 4: eta sums done by the per-member kernel instead
+  double a_next, b_cur;
+  // state (level pos=2) columns
+  double* y[5];
+  double* ys;    // stage state 5*N
+  double* rsum;  // 6*N
+  // stage-0 outputs
+  double* out[6];
+  // stage-4 EOS outputs
+  double *u0, *u1, *u2, *pr, *Tem, *e_int, *eta, *csound, *machno, *mu_fluid, *Reta;
+  const double* mu_factor;
+  double gamma, Rgas;
+  double* red;              // partials [3*nblocks]
+  unsigned int* counter;
+  unsigned int* nonfinite;  // raised by stage 4 on a NaN/Inf in the new rho, q, E
+  double* scal;             // [0] eta mean, [1] eta norm
+  int normalise;
+  const double* src;        // momentum source term (npoin,3) or null
+  const double* wm;         // wall-model momentum terms (npoin,3) or null
+};
+
+// sh: 3 doubles per warp of the block
+__device__ __forceinline__ void block_reduce3(double& s, double& mx, double& mn, double* sh) {
+  // warp reduce then smem
+  for (int o = 16; o > 0; o >>= 1) {
+    s += __shfl_down_sync(0xffffffffu, s, o);
+    mx = fmax(mx, __shfl_down_sync(0xffffffffu, mx, o));
+    mn = fmin(mn, __shfl_down_sync(0xffffffffu, mn, o));
+  }
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0) { sh[3 * w] = s; sh[3 * w + 1] = mx; sh[3 * w + 2] = mn; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const int nw = blockDim.x >> 5;
+    s = sh[0]; mx = sh[1]; mn = sh[2];
+    for (int q = 1; q < nw; ++q) { s += sh[3 * q]; mx = fmax(mx, sh[3 * q + 1]); mn = fmin(mn, sh[3 * q + 2]); }
+  }
+}
+
+// One node of KG (n may be past npoin: nothing happens).  Returns whether the node is a working
+// node that was updated; at STAGE 4 eta_n receives its new entropy for the normalisation sums.
+template <typename R, int STAGE>
+__device__ __forceinline__ bool gather_rk_node(const GatherArgs& a, int n, double& eta_n) {
+  // a row without elements is a periodic slave (not in lpoin_w): rk_4_main's node loops
+  // (time_integ.f90:267-285,445-471) and the lumped solve (mod_solver.f90:23-58) skip it, its
+  // residual stays zero and its state untouched; only sutherland_viscosity, which runs over all
+  // npoin (time_integ.f90:483-487), re-evaluates its mu_fluid from its own Tem
+  const bool inrange = n < a.npoin;
+  const bool act = inrange && (!a.slaves || a.ptr[n + 1] > a.ptr[n]);
+  if (inrange && !act) {
+    if constexpr (STAGE == 0) {
+#pragma unroll
+      for (int f = 0; f < 6; ++f)
+        if (a.out[f]) a.out[f][n] = 0.0;
+    } else if constexpr (STAGE == 4) {
+      const double T = a.Tem[n];
+      a.mu_fluid[n] = a.mu_factor[n] * kSuthC1 * (T * sqrt(T)) / (T + kSuthS);
+    }
+  }
+  if (act) {
+    const R* rel = reinterpret_cast<const R*>(a.rel);
+    const size_t N = (size_t)a.npoin;
+    // node data independent of the gather, loaded first so their latency overlaps it
+    double yv[5], rsv[6];
+    if constexpr (STAGE >= 1) {
+#pragma unroll
+      for (int f = 0; f < 5; ++f) yv[f] = a.y[f][n];
+#pragma unroll
+      for (int f = 0; f < 6; ++f) rsv[f] = STAGE == 1 ? 0.0 : a.rsum[f * N + n];
+    }
+    const double ml = a.Ml[n];
+    double r[6] = {0, 0, 0, 0, 0, 0};
+    const int beg = a.ptr[n], end = a.ptr[n + 1];
+    int c = beg;
+    // groups of 4 contributions: all loads issued before the (ascending, fixed-order) sums
+    for (; c + 4 <= end; c += 4) {
+      R v[4][6];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) load_res6<R>(rel, (size_t)a.idx[c + q], v[q]);
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
+#pragma unroll
+        for (int f = 0; f < 6; ++f) r[f] += (double)v[q][f];
+    }
+    for (; c < end; ++c) {
+      R v[6];
+      load_res6<R>(rel, (size_t)a.idx[c], v);
+#pragma unroll
+      for (int f = 0; f < 6; ++f) r[f] += (double)v[f];
+    }
+    if (a.src) {
+      // mom_source_const_vect (elem_source.f90:20-55): - sum_e gpvol s = - Ml s on the momentum
+#pragma unroll
+      for (int d = 0; d < 3; ++d) r[1 + d] -= ml * a.src[d * N + n];
+    }
+    if (a.wm) {
+      // wall model: the modelled shear added to Rdiff_mom (time_integ.f90:334-357)
+#pragma unroll
+      for (int d = 0; d < 3; ++d) r[1 + d] += a.wm[d * N + n];
+    }
+#pragma unroll
+    for (int f = 0; f < 6; ++f) r[f] = r[f] / ml;
+    if constexpr (STAGE == 0) {
+#pragma unroll
+      for (int f = 0; f < 6; ++f)
+        if (a.out[f]) a.out[f][n] = r[f];
+    } else {
+      const double dt = a.node_member ? a.dt[a.node_member[n]] : *a.dt;
+      double rs[6];
+#pragma unroll
+      for (int f = 0; f < 6; ++f) rs[f] = rsv[f] + a.b_cur * r[f];
+      if constexpr (STAGE < 4) {
+#pragma unroll
+        for (int f = 0; f < 6; ++f) a.rsum[f * N + n] = rs[f];
+        const double da = dt * a.a_next;
+#pragma unroll
+        for (int f = 0; f < 5; ++f) a.ys[f * N + n] = yv[f] - da * r[f];
+      } else {
+        // RK update (time_integ.f90:417-426) and EOS at the new level (:445-463)
+        double y[5];
+#pragma unroll
+        for (int f = 0; f < 5; ++f) {
+          y[f] = yv[f] - dt * rs[f];
+          a.y[f][n] = y[f];
+        }
+        if (!(isfinite(y[0]) && isfinite(y[1]) && isfinite(y[2]) && isfinite(y[3]) && isfinite(y[4])))
+          atomicOr(a.nonfinite, 1u);
+        const double g = a.gamma;
+        const double rho = y[0];
+        const double u0 = y[1] / rho, u1 = y[2] / rho, u2 = y[3] / rho;
+        double umag = u0 * u0 + u1 * u1 + u2 * u2;
+        const double ei = (y[4] / rho) - 0.5 * umag;
+        const double pr = rho * (g - 1.0) * ei;
+        const double cs = sqrt(g * pr / rho);
+        umag = sqrt(umag);
+        const double T = pr / (rho * a.Rgas);
+        const double eta = (rho / (g - 1.0)) * log(pr / pow(rho, g));
+        a.u0[n] = u0; a.u1[n] = u1; a.u2[n] = u2;
+        a.e_int[n] = ei; a.pr[n] = pr; a.csound[n] = cs; a.machno[n] = umag / cs;
+        a.Tem[n] = T; a.eta[n] = eta;
+        a.mu_fluid[n] = a.mu_factor[n] * kSuthC1 * (T * sqrt(T)) / (T + kSuthS);
+        if (a.Reta) a.Reta[n] = -rs[5];
+        eta_n = eta;
+      }
+    }
+  }
+  return act;
+}
+
+// The STAGE 4 entropy normalisation (mod_entropy_viscosity.f90:43-66) over the grid: block sums
+// of (eta, max, min) into red[blockIdx.x], then the last block to finish reduces them in a fixed
+// order into scal[0] (mean) and scal[1] (max deviation).  Every thread of the block calls it.
+// sh: 3 doubles per warp.
+__device__ __forceinline__ void gather_eta_reduce(const GatherArgs& a, double s, double mx, double mn, double* sh) {
+  __shared__ bool last;
+  // entropy normalisation (mod_entropy_viscosity.f90:43-66): sum, max, min of eta
+  block_reduce3(s, mx, mn, sh);
+  if (threadIdx.x == 0) {
+    a.red[3 * blockIdx.x] = s;
+    a.red[3 * blockIdx.x + 1] = mx;
+    a.red[3 * blockIdx.x + 2] = mn;
+    __threadfence();
+    unsigned int done = atomicAdd(a.counter, 1u);
+    last = (done == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (last) {
+    __threadfence();
+    // fixed-order final reduction by the last block (deterministic)
+    double ts = 0.0, tmx = -1e300, tmn = 1e300;
+#pragma unroll 4
+    for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x) {
+      ts += __ldcg(a.red + 3 * b);
+      tmx = fmax(tmx, __ldcg(a.red + 3 * b + 1));
+      tmn = fmin(tmn, __ldcg(a.red + 3 * b + 2));
+    }
+    __syncthreads();
+    block_reduce3(ts, tmx, tmn, sh);
+    if (threadIdx.x == 0) {
+      if (a.normalise) {
+        const double mean = ts / (double)a.nwork;
+        a.scal[0] = mean;
+        a.scal[1] = fmax(tmx - mean, mean - tmn);
+      } else {
+        a.scal[0] = 0.0;
+        a.scal[1] = 1.0;
+      }
+      *a.counter = 0u;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
+// KV: smart_visc_spectral (mod_entropy_viscosity.f90:68-121) per element with the convertIJK
+// filter (mod_filters.f90:42-51), fused with the per-element CFL limits of adapt_dt_cfl
+// (mod_time_ops.f90:31-56) and a deterministic min reduction to the next dt.
+// ---------------------------------------------------------------------------------------------
+struct ViscArgs {
+  int nelem;
+  const int32_t* __restrict__ econn;
+  const double* __restrict__ Reta;
+  const double* __restrict__ rho;
+  const double* __restrict__ u0;
+  const double* __restrict__ u1;
+  const double* __restrict__ u2;
+  const double* __restrict__ csound;
+  const double* __restrict__ Tem;
+  const double* __restrict__ mu_fluid;
+  const double* __restrict__ musgs;  // [e][64] or null
+  const double* __restrict__ helem_l;
+  const double* __restrict__ helem;
+  const double* __restrict__ jratio;
+  const double* __restrict__ scal;   // [0] mean, [1] norm
+  double* mue;                       // out FP64 [e][64]
+  float* mue32;                      // optional FP32 copy
+  double* dt_bits;                   // scratch scalar(s) receiving the min dt (bits, pre-set large)
+  const int32_t* __restrict__ elem_member;  // ensemble: member of each element (null = one mesh)
+  const double* __restrict__ member_scal;   // ensemble: [member][2] eta mean, norm
+  double* dt_out;                    // device scalar (may be null)
+  DevParams prm;
+};
+
+__device__ __forceinline__ int nb_filter(int x) {
+  // natural index of convertIJK(x+1): x=-1 -> 1, 0..3 -> x, 4 -> 1 (reference quirk)
+  return (x < 0) ? 1 : ((x > 3) ? 1 : x);
+}
+
+constexpr int KV_EPB = 4;
+
+// One element per 64 threads (d = the element node); sm holds the element's KV_SMEM doubles of
+// shared memory: ml[64], fl[64] (filter passes), wm[2][5] (per-warp maxima), elem_s[2] (ced and
+// the element's dt limit).  Every thread of the block calls it (it holds block barriers).
+constexpr int KV_SMEM = 2 * NN + 10 + 2;
+__device__ __forceinline__ void visc_dt_elem(const ViscArgs& a, int e, int d, double* sm) {
+  double* ml = sm;
+  double* fl = sm + NN;
+  double* wm = sm + 2 * NN;          // [warp][5]
+  double* elem_s = sm + 2 * NN + 10;
+  const bool act = e < a.nelem;
+  const int ee = act ? e : a.nelem - 1;
+  const int n = a.econn[(size_t)ee * NN + d];
+  const double rho = a.rho[n], u0 = a.u0[n], u1 = a.u1[n], u2 = a.u2[n], cs = a.csound[n], T = a.Tem[n];
+  // inputs of the second half, loaded before the element reductions so their latency overlaps them
+  const double reta_n = a.Reta[n];
+  const double hl = a.helem_l[(size_t)ee * NN + d];
+  const double vmag = sqrt(u0 * u0 + u1 * u1 + u2 * u2);
+  const double he = a.helem[ee];
+  // betae node term (mod_entropy_viscosity.f90:90-95)
+  const double beta_n = (rho * he) * (a.prm.cmax / (double)P) * (vmag + sqrt(a.prm.Rgas * a.prm.gamma * T));
+  // CFL node terms (mod_time_ops.f90:36-50)
+  const double umax = fmax(fmax(fabs(u0), fabs(u1)), fabs(u2));
+  const double L3n = umax + cs;
+  const double musgs = a.musgs ? a.musgs[(size_t)ee * NN + d] : 0.0;
+  const double mun = (rho * musgs + a.mu_fluid[n]) / rho;
+  // element maxima over the 64 nodes (two warps per element)
+  double mV = vmag, mC = cs, mB = beta_n, mL = L3n, mM = mun;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    mV = fmax(mV, __shfl_xor_sync(0xffffffffu, mV, o));
+    mC = fmax(mC, __shfl_xor_sync(0xffffffffu, mC, o));
+    mB = fmax(mB, __shfl_xor_sync(0xffffffffu, mB, o));
+    mL = fmax(mL, __shfl_xor_sync(0xffffffffu, mL, o));
+    mM = fmax(mM, __shfl_xor_sync(0xffffffffu, mM, o));
+  }
+  const int wi = d >> 5;
+  if ((d & 31) == 0) { wm[5 * wi + 0] = mV; wm[5 * wi + 1] = mC; wm[5 * wi + 2] = mB; wm[5 * wi + 3] = mL; wm[5 * wi + 4] = mM; }
+  __syncthreads();
+  if (d == 0) {
+    // shock sensor and cap, once per element (mod_entropy_viscosity.f90:81-84); M**15 as an
+    // integer power like the reference
+    const double M = fmax(wm[0], wm[5]) / fmax(wm[1], wm[6]);
+    const double M2 = M * M, M4 = M2 * M2, M8 = M4 * M4;
+    const double M15 = M8 * M4 * M2 * M;
+    const double ceM = fmax(tanh(M15 * 3.141592653589793), a.prm.ce);
+    double ced = fmax(1.0 - a.jratio[ee], a.prm.ce);
+    elem_s[0] = fmax(ced, ceM);
+    const double hh = he / (double)(2.0 * P + 1);
+    const double L3 = fmax(wm[3], wm[8]);
+    const double maxMU = fmax(wm[4], wm[9]);
+    elem_s[1] = fmin(a.prm.cfl_conv * hh / L3, a.prm.cfl_diff * (hh * hh) / maxMU);
+  }
+  __syncthreads();
+  const double ced = elem_s[0];
+  mB = fmax(wm[2], wm[7]);
+  const int mem = a.elem_member ? a.elem_member[ee] : 0;
+  const double norm = a.elem_member ? a.member_scal[2 * mem + 1] : a.scal[1];
+  const double R1 = (norm > 0.0) ? rho * fabs(reta_n) / norm : 0.0;
+  const double Ve = ced * R1 * hl * hl;
+  ml[d] = a.prm.cglob * fmin(Ve, mB);
+  __syncthreads();
+  // 3x3x3 filter with weights (1/4,1/2,1/4) through convertIJK (mod_entropy_viscosity.f90:102-120):
+  // the weights and the index map are separable, so it runs as three 3-point passes (xi, eta,
+  // zeta) through shared memory, 9 reads per node instead of 27
+  const int i = d & 3, j = (d >> 2) & 3, k = d >> 4;
+  const int ix[3] = {nb_filter(i - 1), i, nb_filter(i + 1)};
+  const int jx[3] = {nb_filter(j - 1), j, nb_filter(j + 1)};
+  const int kx[3] = {nb_filter(k - 1), k, nb_filter(k + 1)};
+  const double w[3] = {0.25, 0.5, 0.25};
+  fl[d] = w[0] * ml[ix[0] + 4 * j + 16 * k] + w[1] * ml[d] + w[2] * ml[ix[2] + 4 * j + 16 * k];
+  __syncthreads();
+  // ml's first-pass reads all happened before the barrier above, so it takes the second pass
+  ml[d] = w[0] * fl[i + 4 * jx[0] + 16 * k] + w[1] * fl[d] + w[2] * fl[i + 4 * jx[2] + 16 * k];
+  __syncthreads();
+  const double acc = w[0] * ml[i + 4 * j + 16 * kx[0]] + w[1] * ml[d] + w[2] * ml[i + 4 * j + 16 * kx[2]];
+  if (act) {
+    a.mue[(size_t)e * NN + d] = acc;
+    if (a.mue32) a.mue32[(size_t)e * NN + d] = (float)acc;
+    // next dt: order-independent min over elements on the bit pattern of a positive double
+    if (a.dt_out && d == 0)
+      atomicMin(reinterpret_cast<unsigned long long*>(a.dt_bits) + mem,
+                (unsigned long long)__double_as_longlong(elem_s[1]));
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
+// One RK stage in one cooperative launch: the element RHS over element tiles, a grid barrier,
+// the node gather / stage update over all nodes (grid-stride), and at stage 4 a grid barrier,
+// the per-member entropy statistics of an ensemble, another barrier and the entropy viscosity
+// + CFL dt over element tiles.  The element-RHS phase is the caller's (it differs by precision).
+// ---------------------------------------------------------------------------------------------
+struct StageArgs {
+  RhsArgs r;
+  GatherArgs g;
+  ViscArgs v;
+  int stage;                           // 1..4
+  int nmember;                         // ensemble members (0: one mesh)
+  const int32_t* __restrict__ member_node_off;  // [nmember+1]
+  double* member_scal;                 // [nmember][2]
+};
+
+template <typename R, int STAGE>
+__device__ __forceinline__ void persist_gather_loop(const GatherArgs& g, double& s, double& mx, double& mn) {
+  const int stride = gridDim.x * blockDim.x;
+  for (int n0 = blockIdx.x * blockDim.x; n0 < g.npoin; n0 += stride) {
+    double eta_n = 0.0;
+    if (gather_rk_node<R, STAGE>(g, n0 + threadIdx.x, eta_n) && STAGE == 4) {
+      s += eta_n;
+      mx = fmax(mx, eta_n);
+      mn = fmin(mn, eta_n);
+    }
+  }
+}
+
+// Everything of a stage after its element-RHS phase; EPB elements (64 threads each) per block.
+template <typename R, int EPB>
+__device__ __forceinline__ void persist_stage_tail(const StageArgs& p, unsigned char* smem_raw) {
+  __shared__ double sh[3 * 32];
+  cooperative_groups::grid_group grid = cooperative_groups::this_grid();
+  grid.sync();  // every element residual of the stage is written
+  double s = 0.0, mx = -1e300, mn = 1e300;
+  switch (p.stage) {
+    case 1: persist_gather_loop<R, 1>(p.g, s, mx, mn); break;
+    case 2: persist_gather_loop<R, 2>(p.g, s, mx, mn); break;
+    case 3: persist_gather_loop<R, 3>(p.g, s, mx, mn); break;
+    default: persist_gather_loop<R, 4>(p.g, s, mx, mn); break;
+  }
+  if (p.stage != 4) return;
+  if (p.nmember == 0) {
+    gather_eta_reduce(p.g, s, mx, mn, sh);
+    grid.sync();  // the new state and the entropy statistics are visible
+  } else {
+    grid.sync();  // the new state is visible
+    // per-member entropy statistics over each member's contiguous node range
+    for (int mbr = blockIdx.x; mbr < p.nmember; mbr += gridDim.x) {
+      const int b = p.member_node_off[mbr], e = p.member_node_off[mbr + 1];
+      double ts = 0.0, tmx = -1e300, tmn = 1e300;
+      for (int t = b + threadIdx.x; t < e; t += blockDim.x) {
+        const double v = p.g.eta[t];
+        ts += v; tmx = fmax(tmx, v); tmn = fmin(tmn, v);
+      }
+      block_reduce3(ts, tmx, tmn, sh);
+      if (threadIdx.x == 0) {
+        if (p.g.normalise) {
+          const double mean = ts / (double)(e - b);
+          p.member_scal[2 * mbr] = mean;
+          p.member_scal[2 * mbr + 1] = fmax(tmx - mean, mean - tmn);
+        } else {
+          p.member_scal[2 * mbr] = 0.0;
+          p.member_scal[2 * mbr + 1] = 1.0;
+        }
+      }
+      __syncthreads();
+    }
+    grid.sync();
+  }
+  // entropy viscosity and the CFL limits, EPB elements per block at a time
+  double* sm = reinterpret_cast<double*>(smem_raw) + (threadIdx.x >> 6) * KV_SMEM;
+  const int ntiles = (p.v.nelem + EPB - 1) / EPB;
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    visc_dt_elem(p.v, t * EPB + (threadIdx.x >> 6), threadIdx.x & 63, sm);
+    __syncthreads();
+  }
+}
+
+}  // namespace sod

@@ -323,12 +323,27 @@ class Sod2dMesh:
         return dtn.value
 
     def autotune(self, state: Sod2dState, precision: int = FP64, stream=None):
-        """Pick elements-per-CTA of the fused RHS kernel by timing the candidates."""
+        """Pick elements per CTA and the stage launch shape by timing the candidates; returns
+        (elements per CTA, fastest fused-RHS ms)."""
         best = C.c_int(0); ms = C.c_float(0.0)
         st = state.struct()
         _lib.check(_lib.load().sod_autotune(self.handle, C.byref(st), int(precision), C.byref(best), C.byref(ms),
                                            _stream(stream)))
         return best.value, ms.value
+
+    def autotune_table(self, precision: int = FP64):
+        """The last autotuner sweep: [(elements per CTA, CTAs per SM of the one-launch stage or 0 for
+        two launches, ms per stage)]."""
+        cap = 64
+        e = (C.c_int32 * cap)(); c = (C.c_int32 * cap)(); t = (C.c_float * cap)()
+        n = _lib.load().sod_autotune_table(self.handle, int(precision), cap, e, c, t)
+        if n < 0:
+            _lib.check(n)
+        return [(int(e[q]), int(c[q]), float(t[q])) for q in range(min(n, cap))]
+
+    def set_stage_launch(self, precision: int, ctas_per_sm: int):
+        """0: two launches per RK stage; n > 0: one cooperative launch with n CTAs per SM."""
+        _lib.check(_lib.load().sod_set_stage_launch(self.handle, int(precision), int(ctas_per_sm)))
 
     def compute_field_derivs(self, rho, u, leviCivi=None, stream=None):
         """compute_fieldDerivs on device tensors rho (npoin) and u (3, npoin) = Fortran (npoin,3):
@@ -601,11 +616,32 @@ class Sod2dBatch:
         _lib.check(_lib.load().sod_batch_rk4_steps(self.handle, int(nsteps), int(precision), _stream(stream)))
 
     def autotune(self, precision: int = FP64, stream=None):
-        """Tune elements-per-CTA of the fused RHS kernel on the concatenated ensemble mesh."""
+        """Tune elements per CTA and the stage launch shape on the concatenated ensemble mesh."""
         best = C.c_int(0); ms = C.c_float(0.0)
         _lib.check(_lib.load().sod_batch_autotune(self.handle, int(precision), C.byref(best), C.byref(ms),
                                                  _stream(stream)))
         return best.value, ms.value
+
+    def _mesh(self) -> C.c_void_p:
+        h = C.c_void_p(0)
+        _lib.check(_lib.load().sod_batch_mesh(self.handle, C.byref(h)))
+        return h
+
+    def autotune_table(self, precision: int = FP64):
+        """The last autotuner sweep of the ensemble: [(elements per CTA, CTAs per SM or 0, ms per stage)]."""
+        cap = 64
+        e = (C.c_int32 * cap)(); c = (C.c_int32 * cap)(); t = (C.c_float * cap)()
+        n = _lib.load().sod_autotune_table(self._mesh(), int(precision), cap, e, c, t)
+        if n < 0:
+            _lib.check(n)
+        return [(int(e[q]), int(c[q]), float(t[q])) for q in range(min(n, cap))]
+
+    def set_stage_launch(self, precision: int, ctas_per_sm: int):
+        """0: two launches per RK stage; n > 0: one cooperative launch with n CTAs per SM."""
+        _lib.check(_lib.load().sod_set_stage_launch(self._mesh(), int(precision), int(ctas_per_sm)))
+
+    def set_rhs_config(self, precision: int, config: int):
+        _lib.check(_lib.load().sod_set_rhs_config(self._mesh(), int(precision), int(config)))
 
 
 # ---- legacy element-loop API of the unit tests (host numpy in, host numpy out) ----------------
