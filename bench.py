@@ -390,7 +390,8 @@ def bench_cg(n: int):
     rhs -= rhs.mean()
     b = torch.from_numpy(rhs).cuda()
     out = {"mesh": f"{n}^3 HEX64 jittered periodic", "nodes": m.npoin, "elements": m.nelem, "tol": 1e-10}
-    P.solve(b, tol=1e-6)  # warm-up
+    P.solve(b, tol=1e-6)              # warm-up: both paths build their iteration graphs here
+    P.solve(b, tol=1e-6, mixed=True)
     sols = {}
     for mixed, name in ((False, "fp64"), (True, "mixed")):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)

@@ -21,9 +21,9 @@
 //
 // The Jacobi diagonal is eval_laplacian_diag (mod_operators.f90:417-461): the unpinned K_aa.
 //
-// conjGrad_pressure_incomp (mod_solver_incomp.f90:247-434) runs as: product + <p,Ap>; device
-// scalars alpha; fused x/r/z update with ||r||^2, <r,z-z_old>, <r,z>; device scalars beta and
-// the stop test ||r|| < tol ||r0|| (:393); p update.  The stop test, the iteration counter and
+// conjGrad_pressure_incomp (mod_solver_incomp.f90:247-434) runs as: product + <p,Ap>, whose
+// last block forms alpha; fused x/r/z update with ||r||^2, <r,z-z_old>, <r,z>, whose last block
+// forms beta and the stop test ||r|| < tol ||r0|| (:393); p update: four launches per iteration.  The stop test, the iteration counter and
 // a done flag live on the device, so iterations are replayed in CUDA-graph batches of kBatch
 // and the host reads the scalars once per batch; every kernel of an iteration after the
 // converged one returns at once, so the iterate and the count are those of a host-tested
@@ -71,6 +71,8 @@ struct SodPoisson {
   double *x = nullptr, *r = nullptr, *p = nullptr, *q = nullptr, *z = nullptr, *b = nullptr;
   float *r32 = nullptr, *p32 = nullptr, *q32 = nullptr, *z32 = nullptr, *e32 = nullptr;
   double* part = nullptr;  // block partials [3][nblk]
+  unsigned int* counter = nullptr;  // blocks done, for the last-block scalar reductions
+  int red_blocks = 0;               // grid of the node kernels that reduce (8 CTAs per SM)
   int nblk = 0;
   double* scal = nullptr;  // device scalars
   double* hscal = nullptr; // pinned host mirror
@@ -316,6 +318,68 @@ __global__ void __launch_bounds__(64 * EPB, kRingCtas) k_lap_elem_async(int nele
 }
 
 
+// single-block fixed-order reductions of the partials and the CG scalars
+// mode 0: init  (part0 = ||r||^2 -> T1 and BNORM2, part1 = <r,z> -> Q1; done if ||b|| = 0)
+// mode 1: alpha (part0 = <p,Ap> -> Q2, alpha = Q1/Q2)
+// mode 2: update(part0 -> T1, part1 -> num, part2 -> Q1new; beta = num/Q1; Q1 = Q1new;
+//                iteration += 1; done if ||r|| < tol ||b|| or the iteration limit is reached)
+// mode 3: norm  (part0 -> T1)
+// modes 1 and 2 do nothing once done
+// Any block size up to 1024 threads; every thread of the block calls it.
+__device__ __forceinline__ void cg_scalars_block(int nblk, const double* __restrict__ part, int stride, int mode,
+                                                 double* scal) {
+  __shared__ double sh[3][32];
+  const int np = mode == 2 ? 3 : (mode == 0 ? 2 : 1);
+  double v[3] = {0.0, 0.0, 0.0};
+  for (int b = threadIdx.x; b < nblk; b += blockDim.x)
+    for (int k = 0; k < np; ++k) v[k] += __ldcg(part + k * stride + b);
+  for (int k = 0; k < 3; ++k)
+    for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_down_sync(0xffffffffu, v[k], o);
+  if ((threadIdx.x & 31) == 0)
+    for (int k = 0; k < 3; ++k) sh[k][threadIdx.x >> 5] = v[k];
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t[3] = {0.0, 0.0, 0.0};
+    for (int k = 0; k < 3; ++k)
+      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t[k] += sh[k][w];
+    if (mode == 0) {
+      scal[S_T1] = t[0]; scal[S_BNORM2] = t[0]; scal[S_Q1] = t[1];
+      if (t[0] == 0.0) scal[S_DONE] = 1.0;
+    } else if (mode == 1) {
+      scal[S_Q2] = t[0]; scal[S_ALPHA] = scal[S_Q1] / t[0];
+    } else if (mode == 2) {
+      scal[S_T1] = t[0]; scal[S_NUM] = t[1]; scal[S_BETA] = t[1] / scal[S_Q1]; scal[S_Q1] = t[2];
+      scal[S_ITER] += 1.0;
+      if (sqrt(t[0]) < scal[S_TOL] * sqrt(scal[S_BNORM2]) || scal[S_ITER] >= scal[S_MAXIT]) scal[S_DONE] = 1.0;
+    } else {
+      scal[S_T1] = t[0];
+    }
+  }
+}
+
+__global__ void __launch_bounds__(1024) k_cg_scalars(int nblk, const double* __restrict__ part, int stride,
+                                                     int mode, double* scal) {
+  if ((mode == 1 || mode == 2) && scal[S_DONE] != 0.0) return;
+  cg_scalars_block(nblk, part, stride, mode, scal);
+}
+
+// After a kernel's block partials: the last block to finish reduces them (cg_scalars_block in
+// the given mode) in a fixed order, so the CG scalars need no launch of their own.
+__device__ __forceinline__ void last_block_scalars(unsigned int* counter, const double* part, int stride, int mode,
+                                                   double* scal) {
+  __shared__ bool last;
+  if (threadIdx.x == 0) {
+    __threadfence();
+    last = atomicAdd(counter, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (last) {
+    __threadfence();
+    cg_scalars_block(gridDim.x, part, stride, mode, scal);
+    if (threadIdx.x == 0) *counter = 0u;
+  }
+}
+
 template <int NP>
 __device__ __forceinline__ void block_partials(double (&v)[NP], double* part, int stride) {
   __shared__ double sh[NP][kBlock / 32];
@@ -340,11 +404,12 @@ template <typename T>
 __global__ void __launch_bounds__(kBlock) k_lap_gather(int n, int pin, const int32_t* __restrict__ n2e_ptr,
                                                       const int32_t* __restrict__ n2e, const T* __restrict__ rel,
                                                       const T* __restrict__ x, T* __restrict__ y,
-                                                      double* __restrict__ part, const double* __restrict__ scal) {
+                                                      double* __restrict__ part, double* scal, unsigned int* counter) {
   if (scal && scal[S_DONE] != 0.0) return;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
   double v[1] = {0.0};
-  if (i < n) {
+  // grid-stride over the nodes: a grid of a few CTAs per SM keeps the partials (and the last
+  // block's reduction of them) short
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     T s = (T)0;
     int c = n2e_ptr[i];
     const int c1 = n2e_ptr[i + 1];
@@ -363,9 +428,11 @@ __global__ void __launch_bounds__(kBlock) k_lap_gather(int n, int pin, const int
     }
     if (i == pin) s = (T)0;
     y[i] = s;
-    v[0] = (double)x[i] * (double)s;
+    v[0] += (double)x[i] * (double)s;
   }
   block_partials<1>(v, part, 0);
+  // inside CG (counter given): <p,Ap> and alpha = <r,z>/<p,Ap> by the last block (mode 1)
+  if (counter) last_block_scalars(counter, part, 0, 1, scal);
 }
 
 // r = b - Ax (ax may be null), z = r/M, p = z, x = 0 (if given); partials ||r||^2, <r,z>
@@ -388,31 +455,77 @@ __global__ void __launch_bounds__(kBlock) k_cg_init(int n, const TV* __restrict_
 
 // x += alpha p; r -= alpha q; z_old = z; z = r/M; partials ||r||^2, <r, z - z_old>, <r, z>
 template <typename TV>
-__global__ void __launch_bounds__(kBlock) k_cg_update(int n, const double* __restrict__ scal, TV* x, TV* r, TV* z,
+__global__ void __launch_bounds__(kBlock) k_cg_update(int n, double* scal, TV* x, TV* r, TV* z,
                                                       const TV* __restrict__ p, const TV* __restrict__ q,
-                                                      const TV* __restrict__ M, double* part, int stride) {
+                                                      const TV* __restrict__ M, double* part, int stride,
+                                                      unsigned int* counter) {
   if (scal[S_DONE] != 0.0) return;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
   double v[3] = {0.0, 0.0, 0.0};
-  if (i < n) {
-    const TV alpha = (TV)scal[S_ALPHA];
+  const TV alpha = (TV)scal[S_ALPHA];
+  auto one = [&](int i) {
     x[i] = x[i] + alpha * p[i];
     const TV ri = r[i] - alpha * q[i];
     const TV zo = z[i];
     const TV zi = ri / M[i];
     r[i] = ri; z[i] = zi;
-    v[0] = (double)ri * (double)ri;
-    v[1] = (double)ri * ((double)zi - (double)zo);
-    v[2] = (double)ri * (double)zi;
+    v[0] += (double)ri * (double)ri;
+    v[1] += (double)ri * ((double)zi - (double)zo);
+    v[2] += (double)ri * (double)zi;
+  };
+  const int gstride = gridDim.x * blockDim.x;
+  int i0 = 0;
+  if constexpr (sizeof(TV) == 4) {
+    // FP32 sweeps: four nodes per thread through 16-byte accesses (a 4-byte load per node keeps
+    // too few bytes in flight to reach the HBM rate)
+    const int n4 = n >> 2;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n4; t += gstride) {
+      float4 xv = reinterpret_cast<const float4*>(x)[t], pv = reinterpret_cast<const float4*>(p)[t];
+      float4 rv = reinterpret_cast<const float4*>(r)[t], qv = reinterpret_cast<const float4*>(q)[t];
+      float4 zv = reinterpret_cast<const float4*>(z)[t], mv = reinterpret_cast<const float4*>(M)[t];
+      float xa[4] = {xv.x, xv.y, xv.z, xv.w}, pa[4] = {pv.x, pv.y, pv.z, pv.w}, ra[4] = {rv.x, rv.y, rv.z, rv.w};
+      float qa[4] = {qv.x, qv.y, qv.z, qv.w}, za[4] = {zv.x, zv.y, zv.z, zv.w}, ma[4] = {mv.x, mv.y, mv.z, mv.w};
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        xa[c] = xa[c] + alpha * pa[c];
+        const float ri = ra[c] - alpha * qa[c];
+        const float zo = za[c];
+        const float zi = ri / ma[c];
+        ra[c] = ri; za[c] = zi;
+        v[0] += (double)ri * (double)ri;
+        v[1] += (double)ri * ((double)zi - (double)zo);
+        v[2] += (double)ri * (double)zi;
+      }
+      reinterpret_cast<float4*>(x)[t] = make_float4(xa[0], xa[1], xa[2], xa[3]);
+      reinterpret_cast<float4*>(r)[t] = make_float4(ra[0], ra[1], ra[2], ra[3]);
+      reinterpret_cast<float4*>(z)[t] = make_float4(za[0], za[1], za[2], za[3]);
+    }
+    i0 = n4 << 2;
   }
+  for (int i = i0 + blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gstride) one(i);
   block_partials<3>(v, part, stride);
+  // beta, the iteration count and the stop test by the last block (mode 2)
+  last_block_scalars(counter, part, stride, 2, scal);
 }
 
 template <typename TV>
 __global__ void k_cg_pupdate(int n, const double* __restrict__ scal, const TV* __restrict__ z, TV* p) {
   if (scal[S_DONE] != 0.0) return;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n) p[i] = z[i] + (TV)scal[S_BETA] * p[i];
+  const TV beta = (TV)scal[S_BETA];
+  if constexpr (sizeof(TV) == 4) {  // four nodes per thread, 16-byte accesses
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int n4 = n >> 2;
+    if (t < n4) {
+      const float4 zv = reinterpret_cast<const float4*>(z)[t];
+      float4 pv = reinterpret_cast<float4*>(p)[t];
+      pv.x = zv.x + beta * pv.x; pv.y = zv.y + beta * pv.y; pv.z = zv.z + beta * pv.z; pv.w = zv.w + beta * pv.w;
+      reinterpret_cast<float4*>(p)[t] = pv;
+    }
+    const int i = (n4 << 2) + t;
+    if (t < (n & 3)) p[i] = z[i] + beta * p[i];
+  } else {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) p[i] = z[i] + beta * p[i];
+  }
 }
 
 __global__ void k_cg_setup(double* scal, double tol, int max_iter) {
@@ -420,45 +533,6 @@ __global__ void k_cg_setup(double* scal, double tol, int max_iter) {
   scal[S_MAXIT] = (double)max_iter;
   scal[S_ITER] = 0.0;
   scal[S_DONE] = 0.0;
-}
-
-// single-block fixed-order reductions of the partials and the CG scalars
-// mode 0: init  (part0 = ||r||^2 -> T1 and BNORM2, part1 = <r,z> -> Q1; done if ||b|| = 0)
-// mode 1: alpha (part0 = <p,Ap> -> Q2, alpha = Q1/Q2)
-// mode 2: update(part0 -> T1, part1 -> num, part2 -> Q1new; beta = num/Q1; Q1 = Q1new;
-//                iteration += 1; done if ||r|| < tol ||b|| or the iteration limit is reached)
-// mode 3: norm  (part0 -> T1)
-// modes 1 and 2 do nothing once done
-__global__ void __launch_bounds__(1024) k_cg_scalars(int nblk, const double* __restrict__ part, int stride,
-                                                     int mode, double* scal) {
-  if ((mode == 1 || mode == 2) && scal[S_DONE] != 0.0) return;
-  __shared__ double sh[3][32];
-  const int np = mode == 2 ? 3 : (mode == 0 ? 2 : 1);
-  double v[3] = {0.0, 0.0, 0.0};
-  for (int b = threadIdx.x; b < nblk; b += blockDim.x)
-    for (int k = 0; k < np; ++k) v[k] += part[k * stride + b];
-  for (int k = 0; k < 3; ++k)
-    for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_down_sync(0xffffffffu, v[k], o);
-  if ((threadIdx.x & 31) == 0)
-    for (int k = 0; k < 3; ++k) sh[k][threadIdx.x >> 5] = v[k];
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double t[3] = {0.0, 0.0, 0.0};
-    for (int k = 0; k < 3; ++k)
-      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t[k] += sh[k][w];
-    if (mode == 0) {
-      scal[S_T1] = t[0]; scal[S_BNORM2] = t[0]; scal[S_Q1] = t[1];
-      if (t[0] == 0.0) scal[S_DONE] = 1.0;
-    } else if (mode == 1) {
-      scal[S_Q2] = t[0]; scal[S_ALPHA] = scal[S_Q1] / t[0];
-    } else if (mode == 2) {
-      scal[S_T1] = t[0]; scal[S_NUM] = t[1]; scal[S_BETA] = t[1] / scal[S_Q1]; scal[S_Q1] = t[2];
-      scal[S_ITER] += 1.0;
-      if (sqrt(t[0]) < scal[S_TOL] * sqrt(scal[S_BNORM2]) || scal[S_ITER] >= scal[S_MAXIT]) scal[S_DONE] = 1.0;
-    } else {
-      scal[S_T1] = t[0];
-    }
-  }
 }
 
 // out = a - b with out[pin] = 0 (b may be null)
@@ -487,10 +561,13 @@ using namespace sod;
 using namespace sod::cg;
 
 static int node_grid(int64_t n) { return (int)((n + kBlock - 1) / kBlock); }
+// grid of the node kernels with reductions (grid-stride loops): a few CTAs per SM
+static int red_grid(const SodPoisson* P) { return std::min(P->nblk, P->red_blocks); }
 
-// y = K x with <x, y> block partials (part[0..node_grid(n))); scal != null skips once done
+// y = K x with <x, y> block partials (part[0..node_grid(n))); scal != null skips once done and
+// then also forms alpha (the CG iteration's scalars) in the gather's last block
 template <typename T>
-static int lap_apply(SodPoisson* P, const T* x, T* y, const double* scal, cudaStream_t st) {
+static int lap_apply(SodPoisson* P, const T* x, T* y, double* scal, cudaStream_t st) {
   const SodMesh* m = P->mesh;
   const int E = (int)P->nelem;
   const T* met;
@@ -510,8 +587,8 @@ static int lap_apply(SodPoisson* P, const T* x, T* y, const double* scal, cudaSt
     k_lap_elem<T><<<ngroups, 64 * EPB, 0, st>>>(E, P->pin, m->econn, met, *D, x, rel, scal);
   }
   SOD_CHECK_LAUNCH();
-  k_lap_gather<T><<<node_grid(P->n), kBlock, 0, st>>>((int)P->n, P->pin, m->n2e_ptr, m->n2e, rel, x, y, P->part,
-                                                      scal);
+  k_lap_gather<T><<<red_grid(P), kBlock, 0, st>>>((int)P->n, P->pin, m->n2e_ptr, m->n2e, rel, x, y, P->part, scal,
+                                                  scal ? P->counter : nullptr);
   SOD_CHECK_LAUNCH();
   return SOD_OK;
 }
@@ -542,12 +619,11 @@ template <typename TV>
 static int cg_iteration(SodPoisson* P, const CgVecs<TV>& v, cudaStream_t st) {
   const int n = (int)P->n;
   const int gb = node_grid(n);
-  if (int rc = lap_apply<TV>(P, v.p, v.q, P->scal, st)) return rc;
-  if (int rc = scalars(P, gb, 1, st)) return rc;
-  k_cg_update<TV><<<gb, kBlock, 0, st>>>(n, P->scal, v.e, v.r, v.z, v.p, v.q, v.M, P->part, P->nblk);
+  if (int rc = lap_apply<TV>(P, v.p, v.q, P->scal, st)) return rc;  // + alpha
+  k_cg_update<TV><<<red_grid(P), kBlock, 0, st>>>(n, P->scal, v.e, v.r, v.z, v.p, v.q, v.M, P->part, P->nblk,
+                                                  P->counter);  // + beta and the stop test
   SOD_CHECK_LAUNCH();
-  if (int rc = scalars(P, gb, 2, st)) return rc;
-  k_cg_pupdate<TV><<<gb, kBlock, 0, st>>>(n, P->scal, v.z, v.p);
+  k_cg_pupdate<TV><<<sizeof(TV) == 4 ? node_grid((n + 3) / 4) : gb, kBlock, 0, st>>>(n, P->scal, v.z, v.p);
   SOD_CHECK_LAUNCH();
   return SOD_OK;
 }
@@ -629,7 +705,7 @@ void sod_poisson_destroy(SodPoisson* P) {
   for (cudaGraphExec_t& g : P->batch)
     if (g) cudaGraphExecDestroy(g);
   void* ptrs[] = {P->met, P->met32, P->diag, P->diag32, P->rel, P->x, P->r, P->p, P->q, P->z, P->b,
-                  P->r32, P->p32, P->q32, P->z32, P->e32, P->part, P->scal};
+                  P->r32, P->p32, P->q32, P->z32, P->e32, P->part, P->scal, P->counter};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (P->hscal) cudaFreeHost(P->hscal);
@@ -667,6 +743,8 @@ int sod_poisson_create(SodMesh* m, SodPoisson** out) {
   for (float** v : {&P->r32, &P->p32, &P->q32, &P->z32, &P->e32}) PALLOC(*v, sizeof(float) * N);
   PALLOC(P->part, sizeof(double) * 3 * P->nblk);
   PALLOC(P->scal, sizeof(double) * S_COUNT);
+  PALLOC(P->counter, sizeof(unsigned int));
+  if (cudaMemset(P->counter, 0, sizeof(unsigned int)) != cudaSuccess) return fail("counter");
 #undef PALLOC
   if (cudaMallocHost(&P->hscal, sizeof(double) * S_COUNT) != cudaSuccess) return fail("hscal");
   {
@@ -683,6 +761,7 @@ int sod_poisson_create(SodMesh* m, SodPoisson** out) {
                                                            LapRing<float, NSTAGE>::kBytes));
     P->ring_grid[0] = nsm * b64;
     P->ring_grid[1] = nsm * b32;
+    P->red_blocks = 8 * nsm;
   }
   k_metric<<<1184, 256>>>(E * NN, m->geo64, P->met, P->met32);
   k_diag<<<node_grid(N), kBlock>>>((int)N, m->n2e_ptr, m->n2e, m->geo64, m->D, P->diag, P->diag32);
