@@ -228,6 +228,15 @@ def kr_bytes_per_launch(nelem: int, npoin: int, mixed: bool) -> float:
     return per_elem * nelem + per_node * npoin
 
 
+def _tune_summary(table):
+    """The autotuner's sweep as rows of (elements per CTA, CTAs per SM of the one-launch stage
+    or 0 for two launches, ms per stage) and its choice (the fastest row)."""
+    best = min(table, key=lambda r: r[2]) if table else None
+    return {"columns": ["elements_per_cta", "ctas_per_sm (0: two launches per stage)", "ms_per_stage"],
+            "rows": [list(r) for r in table],
+            "chosen": None if best is None else {"elements_per_cta": best[0], "ctas_per_sm": best[1]}}
+
+
 def bench_batch(nmember: int, steps: int):
     """Ensemble of periodic HEX64 boxes, n per side log-uniform in [4, 24]
     (seed 4), Re uniform in [400, 3200] (seed 5), own TGV state and dt; `steps` RK4 steps of
@@ -250,6 +259,7 @@ def bench_batch(nmember: int, steps: int):
     out = {"members": nmember, "elements": E, "nodes": N, "steps": steps,
            "n_per_side": {"min": int(ns.min()), "max": int(ns.max()), "mean": float(ns.mean())}}
     out["elements_per_cta"] = {"mixed": B.autotune(S.MIXED)[0], "fp64": B.autotune(S.FP64)[0]}
+    out["autotune"] = {name: _tune_summary(B.autotune_table(p)) for p, name in ((S.MIXED, "mixed"), (S.FP64, "fp64"))}
     for prec, name in ((S.MIXED, "mixed"), (S.FP64, "fp64")):
         B.set_dt(dt0)
         B.rk4_steps(3, precision=prec)
@@ -344,15 +354,22 @@ def bench_adjoint(n: int, steps: int, every: int):
         dL = float(sum((gi * vi).sum() for gi, vi in zip(grads, v)).item())
         dls[name] = dL
 
-        def L_at(h):
+        def L_at(h, p_map=prec):
             u = _clone_state(s)
             u.rho.add_(h * v[0]); u.q.add_(h * v[1]); u.E.add_(h * v[2])
-            replay(gm, u, mus, dts, prec)
+            replay(gm, u, mus, dts, p_map)
             return 0.5 * float((u.q * u.q).sum().item())
         fd = {}
         for h in (1e-4, 1e-6):
             d = (L_at(h) - L_at(-h)) / (2 * h)
             fd[f"{h:g}"] = {"fd": d, "rel_err": abs(d - dL) / abs(dL)}
+        if prec == S.MIXED:
+            # the mixed gradient is the FP64 map's gradient along the mixed trajectory: central
+            # differences of the FP64 map with the mixed run's frozen mu_e and dt carry no FP32
+            # rounding noise, so they test it below the mixed map's noise floor
+            for h in (1e-4, 1e-6):
+                d = (L_at(h, S.FP64) - L_at(-h, S.FP64)) / (2 * h)
+                fd[f"fp64_map_{h:g}"] = {"fd": d, "rel_err": abs(d - dL) / abs(dL)}
         out[name] = {"loss": loss, "directional_derivative": dL, "finite_differences": fd,
                      "ms": {"forward_with_checkpoints": t_fwd, "backward": t_bwd, "forward_plain_graph": t_graph,
                             "forward_keeping_trajectory": t_fwd_k, "backward_from_kept_trajectory": t_bwd_k},
@@ -417,11 +434,13 @@ def bench_cg(n: int):
     return out
 
 
-def run_profile_case(n: int):
+def run_profile_case(n: int, pin: str = ""):
     """A short, bounded launch sequence for ncu captures: on an n^3 jittered periodic mesh, per
-    precision the elements-per-CTA autotuner (13 launches per candidate) and 3 RK4 steps (fused
-    RHS, stage gather, entropy viscosity + dt kernels), one RK4-step VJP (adjoint kernels) and
-    5 matrix-free Poisson products (element + gather kernels); inputs exceed L2 from n = 24 up."""
+    precision the configuration (pin "EPB:CTAS", or else the autotuner) and 3 RK4 steps (fused
+    RHS, stage gather, entropy viscosity + dt kernels; or the one-launch stage kernel), one
+    RK4-step VJP (adjoint kernels) and 5 matrix-free Poisson products (element + gather kernels);
+    inputs exceed L2 from n = 24 up.  With a pin, the first launches of each precision are its
+    three steps' kernels (the fused RHS of stage 1 is the second launch after the mu_e copy)."""
     import torch
     from sod2d_refmap_b200 import solver as S
     M, m, prm, st = _workload(n)
@@ -429,7 +448,12 @@ def run_profile_case(n: int):
     for prec in (S.FP64, S.MIXED):
         s = S.Sod2dState.from_host(st, gm.nelem)
         gm.adapt_dt(s)
-        gm.autotune(s, precision=prec)   # elements per CTA as the benchmark picks them
+        if pin:
+            epb, ctas = (int(x) for x in pin.split(":"))
+            gm.set_rhs_config(prec, epb)
+            gm.set_stage_launch(prec, ctas)
+        else:
+            gm.autotune(s, precision=prec)   # the configuration as the benchmark picks it
         for _ in range(3):
             gm.rk_4_main(s, prec, update_dt=True)
     s = S.Sod2dState.from_host(st, gm.nelem)
@@ -495,9 +519,20 @@ def run_ours(args):
             dist.barrier()
 
     tuned = {}
+    tune_tables = {}
     for prec, name in ((S.FP64, "fp64"), (S.MIXED, "mixed")):
+        if args.pin_config:
+            # a fixed configuration instead of the autotuner (for profiler runs, whose serialised
+            # timing would make the tuner choose differently from a live run)
+            epb, ctas = (int(x) for x in args.pin_config.split(":"))
+            gm.set_rhs_config(prec, epb)
+            gm.set_stage_launch(prec, ctas)
+            tuned[name] = (epb, float("nan"))
+            tune_tables[name] = {"pinned": True, "rows": [], "chosen": {"elements_per_cta": epb, "ctas_per_sm": ctas}}
+            continue
         s = fresh()
         tuned[name] = gm.autotune(s, precision=prec)
+        tune_tables[name] = _tune_summary(gm.autotune_table(prec))
     results = {}
     states = {}
     clocks = None
@@ -631,7 +666,9 @@ def run_ours(args):
                 "ms_per_step": results["mixed"]["ms"] / K, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32-element/f64-assembly",
                 "data": "synthetic (seeded TGV on a generated periodic HEX64 mesh)",
-                "config": _config(args.n, m, {"dt0": dt0, "elements_per_cta": {k: v[0] for k, v in tuned.items()}}),
+                "config": _config(args.n, m, {"dt0": dt0, "elements_per_cta": {k: v[0] for k, v in tuned.items()},
+                                              "stage_launch": {k: v["chosen"] for k, v in tune_tables.items()}}),
+                "autotune": tune_tables,
                 "fp64": {"value": value64, "ms_per_step": results["fp64"]["ms"] / K, "dtype": "f64",
                          "speedup_mixed_over_fp64": value / value64},
                 "mixed_rel_l2_vs_fp64": {"state_after_steps": acc, "rhs_stage": acc_rhs},
@@ -660,6 +697,8 @@ def main():
     ap.add_argument("--cpu-reps", type=int, default=10)
     ap.add_argument("--ref-layers", type=int, default=1)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--pin-config", default="", help="EPB:CTAS - elements per CTA and stage launch shape "
+                                                     "(CTAS 0: two launches per stage) instead of the autotuner")
     ap.add_argument("--no-cg", action="store_true")
     ap.add_argument("--cg-n", type=int, default=48)
     ap.add_argument("--no-batch", action="store_true")
@@ -674,7 +713,7 @@ def main():
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.profile_case:
-        return run_profile_case(args.profile_case)
+        return run_profile_case(args.profile_case, args.pin_config)
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)

@@ -353,13 +353,16 @@ struct StageArgs {
 
 template <typename R, int STAGE>
 __device__ __forceinline__ void persist_gather_loop(const GatherArgs& g, double& s, double& mx, double& mn) {
+  // two nodes per trip: the persistent grid holds fewer threads than the stand-alone gather, so
+  // each thread keeps two independent gathers in flight
   const int stride = gridDim.x * blockDim.x;
-  for (int n0 = blockIdx.x * blockDim.x; n0 < g.npoin; n0 += stride) {
-    double eta_n = 0.0;
-    if (gather_rk_node<R, STAGE>(g, n0 + threadIdx.x, eta_n) && STAGE == 4) {
-      s += eta_n;
-      mx = fmax(mx, eta_n);
-      mn = fmin(mn, eta_n);
+  for (int n0 = blockIdx.x * blockDim.x + threadIdx.x; n0 < g.npoin; n0 += 2 * stride) {
+    double e0 = 0.0, e1 = 0.0;
+    const bool a0 = gather_rk_node<R, STAGE>(g, n0, e0);
+    const bool a1 = gather_rk_node<R, STAGE>(g, n0 + stride, e1);
+    if (STAGE == 4) {
+      if (a0) { s += e0; mx = fmax(mx, e0); mn = fmin(mn, e0); }
+      if (a1) { s += e1; mx = fmax(mx, e1); mn = fmin(mn, e1); }
     }
   }
 }
