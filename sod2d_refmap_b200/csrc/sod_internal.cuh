@@ -136,7 +136,7 @@ __device__ __forceinline__ void load_res6(const R* rel, size_t node, R (&v)[6]) 
 struct StepBuffers {
   int64_t npoin = 0, nelem = 0;
   double* ys = nullptr;      // stage state 5*npoin
-  double* rsum = nullptr;    // RK accumulators 6*npoin (mass, mom x3, ener, eta)
+  double* rsum = nullptr;    // RK accumulators 6*npoin (mass, mom x3, ener, eta); FP64, or FP32 in its first half on the mixed path
   void* rel = nullptr;       // element residuals nelem*6*64 (double or float)
   size_t rel_bytes = 0;
   double* red = nullptr;     // reduction partials

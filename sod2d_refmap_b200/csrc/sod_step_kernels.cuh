@@ -26,7 +26,8 @@ struct GatherArgs {
   // state (level pos=2) columns
   double* y[5];
   double* ys;    // stage state 5*N
-  double* rsum;  // 6*N
+  void* rsum;    // RK accumulators 6*N, stored at the residual precision R: the mixed path's
+                 // hold sums of FP32 element residuals, so FP32 storage loses nothing they carry
   // stage-0 outputs
   double* out[6];
   // stage-4 EOS outputs
@@ -82,6 +83,7 @@ __device__ __forceinline__ bool gather_rk_node(const GatherArgs& a, int n, doubl
   }
   if (act) {
     const R* rel = reinterpret_cast<const R*>(a.rel);
+    R* rsum = reinterpret_cast<R*>(a.rsum);
     const size_t N = (size_t)a.npoin;
     // node data independent of the gather, loaded first so their latency overlaps it
     double yv[5], rsv[6];
@@ -89,7 +91,7 @@ __device__ __forceinline__ bool gather_rk_node(const GatherArgs& a, int n, doubl
 #pragma unroll
       for (int f = 0; f < 5; ++f) yv[f] = a.y[f][n];
 #pragma unroll
-      for (int f = 0; f < 6; ++f) rsv[f] = STAGE == 1 ? 0.0 : a.rsum[f * N + n];
+      for (int f = 0; f < 6; ++f) rsv[f] = STAGE == 1 ? 0.0 : (double)rsum[f * N + n];
     }
     const double ml = a.Ml[n];
     double r[6] = {0, 0, 0, 0, 0, 0};
@@ -134,7 +136,7 @@ __device__ __forceinline__ bool gather_rk_node(const GatherArgs& a, int n, doubl
       for (int f = 0; f < 6; ++f) rs[f] = rsv[f] + a.b_cur * r[f];
       if constexpr (STAGE < 4) {
 #pragma unroll
-        for (int f = 0; f < 6; ++f) a.rsum[f * N + n] = rs[f];
+        for (int f = 0; f < 6; ++f) rsum[f * N + n] = (R)rs[f];
         const double da = dt * a.a_next;
 #pragma unroll
         for (int f = 0; f < 5; ++f) a.ys[f * N + n] = yv[f] - da * r[f];
@@ -250,6 +252,21 @@ __device__ __forceinline__ int nb_filter(int x) {
 
 constexpr int KV_EPB = 4;
 
+// Exact maximum of a double over the warp with two 32-bit integer reductions instead of ten
+// shuffles: the bit pattern is mapped to an unsigned key of the same order (sign bit flipped for
+// non-negative values, all bits for negative ones), the high words are reduced, then the low
+// words of the lanes that hold the maximal high word.  Equal to fmax over the lanes for every
+// non-NaN input (a NaN in some lane gives NaN here, where fmax would drop it).
+__device__ __forceinline__ double warp_max_f64(double v) {
+  const unsigned hi = (unsigned)__double2hiint(v), lo = (unsigned)__double2loint(v);
+  const unsigned neg = (unsigned)((int)hi >> 31);
+  const unsigned kh = hi ^ (neg | 0x80000000u), kl = lo ^ neg;
+  const unsigned mh = __reduce_max_sync(0xffffffffu, kh);
+  const unsigned ml = __reduce_max_sync(0xffffffffu, kh == mh ? kl : 0u);
+  const unsigned back = (mh & 0x80000000u) ? 0u : 0xffffffffu;   // key of a negative maximum
+  return __hiloint2double((int)(mh ^ (back | 0x80000000u)), (int)(ml ^ back));
+}
+
 // One element per 64 threads (d = the element node); sm holds the element's KV_SMEM doubles of
 // shared memory: ml[64], fl[64] (filter passes), wm[2][5] (per-warp maxima), elem_s[2] (ced and
 // the element's dt limit).  Every thread of the block calls it (it holds block barriers).
@@ -276,15 +293,8 @@ __device__ __forceinline__ void visc_dt_elem(const ViscArgs& a, int e, int d, do
   const double musgs = a.musgs ? a.musgs[(size_t)ee * NN + d] : 0.0;
   const double mun = (rho * musgs + a.mu_fluid[n]) / rho;
   // element maxima over the 64 nodes (two warps per element)
-  double mV = vmag, mC = cs, mB = beta_n, mL = L3n, mM = mun;
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    mV = fmax(mV, __shfl_xor_sync(0xffffffffu, mV, o));
-    mC = fmax(mC, __shfl_xor_sync(0xffffffffu, mC, o));
-    mB = fmax(mB, __shfl_xor_sync(0xffffffffu, mB, o));
-    mL = fmax(mL, __shfl_xor_sync(0xffffffffu, mL, o));
-    mM = fmax(mM, __shfl_xor_sync(0xffffffffu, mM, o));
-  }
+  double mV = warp_max_f64(vmag), mC = warp_max_f64(cs), mB = warp_max_f64(beta_n);
+  double mL = warp_max_f64(L3n), mM = warp_max_f64(mun);
   const int wi = d >> 5;
   if ((d & 31) == 0) { wm[5 * wi + 0] = mV; wm[5 * wi + 1] = mC; wm[5 * wi + 2] = mB; wm[5 * wi + 3] = mL; wm[5 * wi + 4] = mM; }
   __syncthreads();
