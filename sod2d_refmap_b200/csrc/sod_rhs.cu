@@ -340,9 +340,11 @@ __global__ void __launch_bounds__(64 * EPB) k_stage_fused(const StageArgs p) {
 }
 
 #ifndef SOD_KG_MIN_BLOCKS
-// resident 256-thread blocks per SM the register budget must allow: 4 leaves 64 registers, no
-// spills (7 blocks capped the kernel at 32 registers and spilled 140-244 bytes per thread)
-#define SOD_KG_MIN_BLOCKS 4
+// resident 256-thread blocks per SM the register budget must allow: 5 leaves 48 registers (the
+// FP32-accumulator stages spill 24 bytes, the FP64 ones 48-72) and measured 4% (mixed) / 1%
+// (FP64) faster than 4 blocks at 64 registers; 7 blocks capped the kernel at 32 registers and
+// spilled 140-244 bytes per thread
+#define SOD_KG_MIN_BLOCKS 5
 #endif
 template <typename R, int STAGE>
 __global__ void __launch_bounds__(256, SOD_KG_MIN_BLOCKS) k_gather_rk(const GatherArgs a) {
