@@ -15,7 +15,10 @@
 //   batch BC (fe,fue)x3 (feta,F0.)x3 (F1.,F2.)x3 (Fuu0.,Fuu1.)x3 (Fuu22,0)
 //   pass 2   (gradRho^,tauU^)x3 (gradT^,tauX^)x3 (tauY^,tauZ^)x3   (one slot per direction)
 // where fe = rho H' u, fue = H' u, F = (q-q_r) x (u-u_r), Fuu = (u-u_r) x (u-u_r) and ^ marks
-// contravariant fluxes.
+// contravariant fluxes.  The batch BC products are not stored: shared memory holds their 9
+// factors (5 slots), and each line point forms the 25 products from them, as its owning node
+// would; that reads 5 slots per line point instead of 13 (863 instead of 1,226 shared-memory
+// wavefronts per element).
 #include "sod_internal.cuh"
 #include "sod_step_kernels.cuh"
 #include <cmath>
@@ -26,9 +29,10 @@ namespace mx2 {
 
 constexpr double kC1 = 0.000001458;
 constexpr double kS = 110.4;
-constexpr int NBC = 13;  // batch B+C slots
+constexpr int NA = 6;    // batch A slots (field pairs)
+constexpr int NBC = NA + 5;  // batch A + the batch B+C factor slots
 constexpr int NP2 = 9;   // pass-2 slots
-constexpr int NSLOT = NBC + NP2;  // batch A (6 pairs) reuses the first slots of the BC area
+constexpr int NSLOT = NBC + NP2;
 constexpr int NREF = 16 + 36 + 18 + 6;  // node-0 refs, corner values of the batch-A fields, FP32 slopes, 12 FP32 refs
 
 __host__ __device__ constexpr size_t smem_bytes(int epb) {
@@ -230,6 +234,13 @@ __device__ __forceinline__ void rhs_mixed2_tile(const RhsArgs& a, int tile, unsi
     sef = vp[10] + lin[5].x;
     Tf = rf[9] + (vp[11] + lin[5].y);
   }
+  // factors of the batch B+C products, stored beside batch A: every line point forms its
+  // products from them (below), so the element holds 5 factor slots instead of 13 product slots
+  buf[(NA + 0) * FSTRIDE + s_me] = make_float2(su[0], su[1]);
+  buf[(NA + 1) * FSTRIDE + s_me] = make_float2(su[2], sq[0]);
+  buf[(NA + 2) * FSTRIDE + s_me] = make_float2(sq[1], sq[2]);
+  buf[(NA + 3) * FSTRIDE + s_me] = make_float2((rf[0] + drho) * sHf, sHf);
+  reinterpret_cast<float*>(buf + (NA + 4) * FSTRIDE)[s_me] = sef;
   const float muf = mufac * (float)kC1 * (Tf * sqrtf(Tf)) / (Tf + (float)kS);
   __syncthreads();
 
@@ -322,37 +333,72 @@ __device__ __forceinline__ void rhs_mixed2_tile(const RhsArgs& a, int tile, unsi
     emit(3, gradT, tau[0]);
     emit(6, tau[1], tau[2]);
   }
-  __syncthreads();  // batch A reads done
-
-  // ---- batch B+C (13 pairs)
+  // ---- batch B+C: divergences of the 13 deviation-product pairs
+  //   (rho H' u_c, H' u_c) (eta' u_c, q'_0 u'_c) (q'_1 u'_c, q'_2 u'_c) (u'_0 u'_c, u'_1 u'_c) (u'_2 u'_2)
+  // with u = u_r + u'.  Each line point forms the products from the factor slots exactly as its
+  // owning node would (the same FP32 operations on the same values), so the discrete derivative
+  // is that of the nodal products; per direction the 13 line sums are folded with He at once.
   {
-    const float sH = sHf, se = sef;
-    const float rsH = rhoR * sHf;
+    const float2* f0s = buf + (NA + 0) * FSTRIDE;  // (u'_0, u'_1)
+    const float2* f1s = buf + (NA + 1) * FSTRIDE;  // (u'_2, q'_0)
+    const float2* f2s = buf + (NA + 2) * FSTRIDE;  // (q'_1, q'_2)
+    const float2* f3s = buf + (NA + 3) * FSTRIDE;  // (rho H', H')
+    const float* f4s = reinterpret_cast<const float*>(buf + (NA + 4) * FSTRIDE);  // eta' (one float per node)
+    const float rU0 = rf[1], rU1 = rf[2], rU2 = rf[3];
+    float2 dA = make_float2(0.f, 0.f), dC = dA, dD = dA, dE = dA;
+    float dFuu2 = 0.f;
 #pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      buf[(0 + c) * FSTRIDE + s_me] = make_float2(rsH * uR[c], sH * uR[c]);
-      buf[(3 + c) * FSTRIDE + s_me] = make_float2(se * uR[c], sq[0] * su[c]);
-      buf[(6 + c) * FSTRIDE + s_me] = make_float2(sq[1] * su[c], sq[2] * su[c]);
-      buf[(9 + c) * FSTRIDE + s_me] = make_float2(su[0] * su[c], su[1] * su[c]);
-    }
-    buf[12 * FSTRIDE + s_me] = make_float2(su[2] * su[2], 0.0f);
-  }
-  __syncthreads();
-  {
-    // divergence of a pair of 3-vectors held in slots s0..s0+2
-    auto div2 = [&](int s0) {
-      float2 acc = make_float2(0.f, 0.f);
+    for (int dir = 0; dir < 3; ++dir) {
+      float2 g[12];
+#pragma unroll
+      for (int q = 0; q < 12; ++q) g[q] = make_float2(0.f, 0.f);
+      float g12 = 0.f;
+      auto point = [&](float2 w, float2 a0, float2 a1, float2 a2, float2 a3, float se) {
+        const float su_[3] = {a0.x, a0.y, a1.x};
+        const float uR_[3] = {rU0 + a0.x, rU1 + a0.y, rU2 + a1.x};
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          g[c] = FMA2(w, MUL2(a3, F2(uR_[c])), g[c]);
+          g[3 + c] = FMA2(w, MUL2(make_float2(se, a1.y), make_float2(uR_[c], su_[c])), g[3 + c]);
+          g[6 + c] = FMA2(w, MUL2(a2, F2(su_[c])), g[6 + c]);
+          g[9 + c] = FMA2(w, MUL2(a0, F2(su_[c])), g[9 + c]);
+        }
+        g12 = fmaf(w.x, __fmul_rn(su_[2], su_[2]), g12);
+      };
+      if (dir == 0) {
+        // the xi line of the node: two 16-byte loads per slot
+        const int s0 = sidx(0, j, k);
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const float4 b0 = *reinterpret_cast<const float4*>(f0s + s0 + 2 * h);
+          const float4 b1 = *reinterpret_cast<const float4*>(f1s + s0 + 2 * h);
+          const float4 b2 = *reinterpret_cast<const float4*>(f2s + s0 + 2 * h);
+          const float4 b3 = *reinterpret_cast<const float4*>(f3s + s0 + 2 * h);
+          const float2 e4 = *reinterpret_cast<const float2*>(f4s + s0 + 2 * h);  // eta' at both points
+          point(Dx[2 * h], make_float2(b0.x, b0.y), make_float2(b1.x, b1.y), make_float2(b2.x, b2.y),
+                make_float2(b3.x, b3.y), e4.x);
+          point(Dx[2 * h + 1], make_float2(b0.z, b0.w), make_float2(b1.z, b1.w), make_float2(b2.z, b2.w),
+                make_float2(b3.z, b3.w), e4.y);
+        }
+      } else {
+#pragma unroll
+        for (int m = 0; m < 4; ++m) {
+          const int sp = dir == 1 ? sidx(i, m, k) : sidx(i, j, m);
+          point(dir == 1 ? Dy[m] : Dz[m], f0s[sp], f1s[sp], f2s[sp], f3s[sp], f4s[sp]);
+        }
+      }
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
-        float2 gx, gy, gz;
-        giso2(buf + (s0 + c) * FSTRIDE, i, j, k, Dx, Dy, Dz, gx, gy, gz);
-        acc = FMA2(H2[3 * c + 2], gz, FMA2(H2[3 * c + 1], gy, FMA2(H2[3 * c], gx, acc)));
+        const float2 h = H2[3 * c + dir];
+        dA = FMA2(h, g[c], dA);
+        dC = FMA2(h, g[3 + c], dC);
+        dD = FMA2(h, g[6 + c], dD);
+        dE = FMA2(h, g[9 + c], dE);
       }
-      return acc;
-    };
-    const float2 dA = div2(0);   // (div fe, div fue)
-    const float2 dC = div2(3);   // (div feta, div F0.)
-    const float2 dD = div2(6);   // (div F1., div F2.)
+      // row 2 of u' x u' from (Fuu02, Fuu12, Fuu22)
+      dFuu2 += H[dir] * g[11].x + H[3 + dir] * g[11].y + H[6 + dir] * g12;
+    }
+    // dA = (div fe, div fue), dC = (div feta, div F0.), dD = (div F1., div F2.), dE = (div Fuu0., div Fuu1.)
     Ren += 0.25f * (dA.x + rhoR * dA.y);
     Ret += 0.5f * dC.x;
     if constexpr (TOTH) {
@@ -362,28 +408,11 @@ __device__ __forceinline__ void rhs_mixed2_tile(const RhsArgs& a, int tile, unsi
 #pragma unroll
       for (int c = 0; c < 3; ++c) Ren += 0.5f * (uR[c] * gradRH[c]);
     }
-    // Fuu rows 0,1 from slots 9..11 and row 2 from (Fuu02, Fuu12, Fuu22)
-    float2 dE = make_float2(0.f, 0.f);
-    float dFuu2 = 0.f;
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      float2 gx, gy, gz;
-      giso2(buf + (9 + c) * FSTRIDE, i, j, k, Dx, Dy, Dz, gx, gy, gz);
-      dE = FMA2(H2[3 * c + 2], gz, FMA2(H2[3 * c + 1], gy, FMA2(H2[3 * c], gx, dE)));
-      if (c == 2) {
-        dFuu2 += H[0] * gx.x + H[1] * gy.x + H[2] * gz.x;   // d/dx_0 Fuu20 (= Fuu02)
-        dFuu2 += H[3] * gx.y + H[4] * gy.y + H[5] * gz.y;   // d/dx_1 Fuu21 (= Fuu12)
-      }
-    }
-    {
-      float2 gx, gy, gz;
-      giso2(buf + 12 * FSTRIDE, i, j, k, Dx, Dy, Dz, gx, gy, gz);
-      dFuu2 += H[6] * gx.x + H[7] * gy.x + H[8] * gz.x;     // d/dx_2 Fuu22
-    }
     Rmo[0] += 0.25f * (dC.y + rhoR * dE.x);
     Rmo[1] += 0.25f * (dD.x + rhoR * dE.y);
     Rmo[2] += 0.25f * (dD.y + rhoR * dFuu2);
   }
+  __syncthreads();  // pass-1 fluxes visible
 
   // ---- diffusion pass 2 (elem_diffu.f90:142-194)
   float2 DTx[4], DTy[4], DTz[4];

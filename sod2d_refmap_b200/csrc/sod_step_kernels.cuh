@@ -256,7 +256,8 @@ constexpr int KV_EPB = 4;
 // shuffles: the bit pattern is mapped to an unsigned key of the same order (sign bit flipped for
 // non-negative values, all bits for negative ones), the high words are reduced, then the low
 // words of the lanes that hold the maximal high word.  Equal to fmax over the lanes for every
-// non-NaN input (a NaN in some lane gives NaN here, where fmax would drop it).
+// non-NaN input.  A NaN with a clear sign bit (the form the GPU's arithmetic produces) wins
+// here, where fmax would drop it; the step's non-finite flag reports such states anyway.
 __device__ __forceinline__ double warp_max_f64(double v) {
   const unsigned hi = (unsigned)__double2hiint(v), lo = (unsigned)__double2loint(v);
   const unsigned neg = (unsigned)((int)hi >> 31);
