@@ -233,70 +233,90 @@ __device__ __forceinline__ void rhs_fused_tile(const RhsArgs& a, int tile, unsig
     emit(4, tau[1][0], tau[1][1], tau[1][2]);
     emit(5, tau[2][0], tau[2][1], tau[2][2]);
   }
-  __syncthreads();  // batch A reads done
-
-  // ---- batch B: product vectors (rho h u, h u, rho k u, k u, eta u)
+  // ---- batches B and C: divergences of the product vectors (rho h u, h u, rho k u, k u, eta u;
+  // (E + p) u with flag_total_enthalpy) and tensors (q x u, u x u).  Every line point forms the 30
+  // products from batch A's slots exactly as its owning node would, so nothing more is staged;
+  // the line sums of each direction are folded with He before the next direction.
   {
-    const R sh = (R)h, sk = (R)kk, se = (R)eta_full;
-    const R rsh = (R)(rho * h), rsk = (R)(rho * kk);
+    R divFe = R(0), divFue = R(0), divFk = R(0), divFuk = R(0), divFeta = R(0);
+    R dF[3] = {R(0), R(0), R(0)}, dFuu[3] = {R(0), R(0), R(0)};
 #pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      buf[(0 + c) * FSTRIDE + s_me] = TOTH ? (R)((Et + p) * uv[c]) : rsh * uR[c];
-      buf[(3 + c) * FSTRIDE + s_me] = sh * uR[c];
-      buf[(6 + c) * FSTRIDE + s_me] = rsk * uR[c];
-      buf[(9 + c) * FSTRIDE + s_me] = sk * uR[c];
-      buf[(12 + c) * FSTRIDE + s_me] = se * uR[c];
+    for (int dir = 0; dir < 3; ++dir) {
+      const R* Dd = dir == 0 ? Dx : (dir == 1 ? Dy : Dz);
+      {
+        R gB[15];
+#pragma unroll
+        for (int q = 0; q < 15; ++q) gB[q] = R(0);
+#pragma unroll
+        for (int m = 0; m < 4; ++m) {
+          const int sp = dir == 0 ? sidx(m, j, k) : (dir == 1 ? sidx(i, m, k) : sidx(i, j, m));
+          const R w = Dd[m];
+          const R u0 = buf[1 * FSTRIDE + sp], u1 = buf[2 * FSTRIDE + sp], u2 = buf[3 * FSTRIDE + sp];
+          const R fe = TOTH ? buf[14 * FSTRIDE + sp] : buf[9 * FSTRIDE + sp];
+          const R fh = buf[8 * FSTRIDE + sp], frk = buf[11 * FSTRIDE + sp], fk = buf[10 * FSTRIDE + sp];
+          const R fet = buf[12 * FSTRIDE + sp];
+          const R u[3] = {u0, u1, u2};
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            gB[c] += w * (fe * u[c]);
+            gB[3 + c] += w * (fh * u[c]);
+            gB[6 + c] += w * (frk * u[c]);
+            gB[9 + c] += w * (fk * u[c]);
+            gB[12 + c] += w * (fet * u[c]);
+          }
+        }
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          const R hc = H[3 * c + dir];
+          divFe += hc * gB[c];
+          divFue += hc * gB[3 + c];
+          divFk += hc * gB[6 + c];
+          divFuk += hc * gB[9 + c];
+          divFeta += hc * gB[12 + c];
+        }
+      }
+      {
+        R gQ[9], gU[6];
+#pragma unroll
+        for (int q = 0; q < 9; ++q) gQ[q] = R(0);
+#pragma unroll
+        for (int q = 0; q < 6; ++q) gU[q] = R(0);
+#pragma unroll
+        for (int m = 0; m < 4; ++m) {
+          const int sp = dir == 0 ? sidx(m, j, k) : (dir == 1 ? sidx(i, m, k) : sidx(i, j, m));
+          const R w = Dd[m];
+          const R u[3] = {buf[1 * FSTRIDE + sp], buf[2 * FSTRIDE + sp], buf[3 * FSTRIDE + sp]};
+          const R q[3] = {buf[4 * FSTRIDE + sp], buf[5 * FSTRIDE + sp], buf[6 * FSTRIDE + sp]};
+#pragma unroll
+          for (int r = 0; r < 3; ++r)
+#pragma unroll
+            for (int c = 0; c < 3; ++c) gQ[3 * r + c] += w * (q[r] * u[c]);
+          gU[0] += w * (u[0] * u[0]);
+          gU[1] += w * (u[0] * u[1]);
+          gU[2] += w * (u[0] * u[2]);
+          gU[3] += w * (u[1] * u[1]);
+          gU[4] += w * (u[1] * u[2]);
+          gU[5] += w * (u[2] * u[2]);
+        }
+        // u x u is symmetric: component (r, c) is the stored product of min(r,c), max(r,c)
+        const int symidx[3][3] = {{0, 1, 2}, {1, 3, 4}, {2, 4, 5}};
+#pragma unroll
+        for (int r = 0; r < 3; ++r)
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            const R hc = H[3 * c + dir];
+            dF[r] += hc * gQ[3 * r + c];
+            dFuu[r] += hc * gU[symidx[r][c]];
+          }
+      }
     }
-  }
-  __syncthreads();
-  {
-    const R divFe = divv(buf + 0 * FSTRIDE, i, j, k, Dx, Dy, Dz, H);
-    const R divFue = divv(buf + 3 * FSTRIDE, i, j, k, Dx, Dy, Dz, H);
-    const R divFk = divv(buf + 6 * FSTRIDE, i, j, k, Dx, Dy, Dz, H);
-    const R divFuk = divv(buf + 9 * FSTRIDE, i, j, k, Dx, Dy, Dz, H);
-    const R divFeta = divv(buf + 12 * FSTRIDE, i, j, k, Dx, Dy, Dz, H);
     Ren += R(0.25) * (divFe + rhoR * divFue) + R(0.25) * (divFk + rhoR * divFuk);
     Ret += R(0.5) * divFeta;
     if constexpr (TOTH) Ren = R(0.5) * (divFe + (R)(Et + p) * divU) + uGradEp;  // elem_convec.f90:171-177
+#pragma unroll
+    for (int r = 0; r < 3; ++r) Rmo[r] += R(0.25) * (dF[r] + rhoR * dFuu[r]);
   }
-  __syncthreads();
-
-  // ---- batch C: tensors q x u and u x u (symmetric)
-  {
-    R sq[3], su[3];
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      sq[c] = (R)qv[c];
-      su[c] = (R)uv[c];
-    }
-#pragma unroll
-    for (int r = 0; r < 3; ++r)
-#pragma unroll
-      for (int c = 0; c < 3; ++c) buf[(3 * r + c) * FSTRIDE + s_me] = sq[r] * su[c];
-    buf[9 * FSTRIDE + s_me] = su[0] * su[0];
-    buf[10 * FSTRIDE + s_me] = su[0] * su[1];
-    buf[11 * FSTRIDE + s_me] = su[0] * su[2];
-    buf[12 * FSTRIDE + s_me] = su[1] * su[1];
-    buf[13 * FSTRIDE + s_me] = su[1] * su[2];
-    buf[14 * FSTRIDE + s_me] = su[2] * su[2];
-  }
-  __syncthreads();
-  {
-    const int symidx[3][3] = {{9, 10, 11}, {10, 12, 13}, {11, 13, 14}};
-#pragma unroll
-    for (int r = 0; r < 3; ++r) {
-      R dF = R(0), dFuu = R(0);
-#pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        R gx, gy, gz;
-        giso(buf + (3 * r + c) * FSTRIDE, i, j, k, Dx, Dy, Dz, gx, gy, gz);
-        dF += H[3 * c + 0] * gx + H[3 * c + 1] * gy + H[3 * c + 2] * gz;
-        giso(buf + symidx[r][c] * FSTRIDE, i, j, k, Dx, Dy, Dz, gx, gy, gz);
-        dFuu += H[3 * c + 0] * gx + H[3 * c + 1] * gy + H[3 * c + 2] * gz;
-      }
-      Rmo[r] += R(0.25) * (dF + rhoR * dFuu);
-    }
-  }
+  __syncthreads();  // pass-1 fluxes visible
 
   // ---- diffusion pass 2 (elem_diffu.f90:142-194): weak divergence with D^T
   R DTx[4], DTy[4], DTz[4];
