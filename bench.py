@@ -335,7 +335,8 @@ def bench_adjoint(n: int, steps: int, every: int):
     dls = {}
     for prec, name in ((S.FP64, "fp64"), (S.MIXED, "mixed")):
         run(2, prec)  # warm-up
-        run(2, prec, True)
+        # the kept trajectory of the full step count is allocated here, outside the timed runs
+        run(steps, prec, True)
         grads, loss, t_fwd, t_bwd = run(steps, prec)
         # the forward keeps every step's stage states in HBM: the backward is the VJPs alone
         grads_k, _, t_fwd_k, t_bwd_k = run(steps, prec, True)
