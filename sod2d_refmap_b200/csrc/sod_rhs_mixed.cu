@@ -16,9 +16,10 @@
 //   pass 2   (gradRho^,tauU^)x3 (gradT^,tauX^)x3 (tauY^,tauZ^)x3   (one slot per direction)
 // where fe = rho H' u, fue = H' u, F = (q-q_r) x (u-u_r), Fuu = (u-u_r) x (u-u_r) and ^ marks
 // contravariant fluxes.  The batch BC products are not stored: shared memory holds their 9
-// factors (5 slots), and each line point forms the 25 products from them, as its owning node
-// would; that reads 5 slots per line point instead of 13 (863 instead of 1,226 shared-memory
-// wavefronts per element).
+// factors (5 slots), and each line point forms the 25 weighted products D[x][m] a b from them as
+// (D[x][m] a) b; that reads 5 slots per line point instead of 13 (863 instead of 1,226
+// shared-memory wavefronts per element) and scales 4 factor pairs per point instead of 13
+// products.
 #include "sod_internal.cuh"
 #include "sod_step_kernels.cuh"
 #include <cmath>
@@ -335,9 +336,9 @@ __device__ __forceinline__ void rhs_mixed2_tile(const RhsArgs& a, int tile, unsi
   }
   // ---- batch B+C: divergences of the 13 deviation-product pairs
   //   (rho H' u_c, H' u_c) (eta' u_c, q'_0 u'_c) (q'_1 u'_c, q'_2 u'_c) (u'_0 u'_c, u'_1 u'_c) (u'_2 u'_2)
-  // with u = u_r + u'.  Each line point forms the products from the factor slots exactly as its
-  // owning node would (the same FP32 operations on the same values), so the discrete derivative
-  // is that of the nodal products; per direction the 13 line sums are folded with He at once.
+  // with u = u_r + u'.  Each line point m forms its terms D[x][m] a b of the line sums from the
+  // factor slots as (D[x][m] a) b (a rounding of the same order as D[x][m] (a b)); per direction
+  // the 13 line sums are folded with He at once.
   {
     const float2* f0s = buf + (NA + 0) * FSTRIDE;  // (u'_0, u'_1)
     const float2* f1s = buf + (NA + 1) * FSTRIDE;  // (u'_2, q'_0)
@@ -356,14 +357,17 @@ __device__ __forceinline__ void rhs_mixed2_tile(const RhsArgs& a, int tile, unsi
       auto point = [&](float2 w, float2 a0, float2 a1, float2 a2, float2 a3, float se) {
         const float su_[3] = {a0.x, a0.y, a1.x};
         const float uR_[3] = {rU0 + a0.x, rU1 + a0.y, rU2 + a1.x};
+        // the line weight scales the first factor of each product
+        const float2 w3 = MUL2(w, a3), w2 = MUL2(w, a2), w0 = MUL2(w, a0);
+        const float2 wsq = MUL2(w, make_float2(se, a1.y));
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
-          g[c] = FMA2(w, MUL2(a3, F2(uR_[c])), g[c]);
-          g[3 + c] = FMA2(w, MUL2(make_float2(se, a1.y), make_float2(uR_[c], su_[c])), g[3 + c]);
-          g[6 + c] = FMA2(w, MUL2(a2, F2(su_[c])), g[6 + c]);
-          g[9 + c] = FMA2(w, MUL2(a0, F2(su_[c])), g[9 + c]);
+          g[c] = FMA2(w3, F2(uR_[c]), g[c]);
+          g[3 + c] = FMA2(wsq, make_float2(uR_[c], su_[c]), g[3 + c]);
+          g[6 + c] = FMA2(w2, F2(su_[c]), g[6 + c]);
+          g[9 + c] = FMA2(w0, F2(su_[c]), g[9 + c]);
         }
-        g12 = fmaf(w.x, __fmul_rn(su_[2], su_[2]), g12);
+        g12 = fmaf(__fmul_rn(w.x, su_[2]), su_[2], g12);
       };
       if (dir == 0) {
         // the xi line of the node: two 16-byte loads per slot
