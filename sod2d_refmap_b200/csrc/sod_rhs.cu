@@ -234,9 +234,9 @@ __device__ __forceinline__ void rhs_fused_tile(const RhsArgs& a, int tile, unsig
     emit(5, tau[2][0], tau[2][1], tau[2][2]);
   }
   // ---- batches B and C: divergences of the product vectors (rho h u, h u, rho k u, k u, eta u;
-  // (E + p) u with flag_total_enthalpy) and tensors (q x u, u x u).  Every line point forms the 30
-  // products from batch A's slots exactly as its owning node would, so nothing more is staged;
-  // the line sums of each direction are folded with He before the next direction.
+  // (E + p) u with flag_total_enthalpy) and tensors (q x u, u x u).  Every line point m forms its
+  // 30 terms D[x][m] f u_c of the line sums from batch A's slots as (D[x][m] u_c) f, so nothing
+  // more is staged; the line sums of each direction are folded with He before the next direction.
   {
     R divFe = R(0), divFue = R(0), divFk = R(0), divFuk = R(0), divFeta = R(0);
     R dF[3] = {R(0), R(0), R(0)}, dFuu[3] = {R(0), R(0), R(0)};
@@ -255,14 +255,15 @@ __device__ __forceinline__ void rhs_fused_tile(const RhsArgs& a, int tile, unsig
           const R fe = TOTH ? buf[14 * FSTRIDE + sp] : buf[9 * FSTRIDE + sp];
           const R fh = buf[8 * FSTRIDE + sp], frk = buf[11 * FSTRIDE + sp], fk = buf[10 * FSTRIDE + sp];
           const R fet = buf[12 * FSTRIDE + sp];
-          const R u[3] = {u0, u1, u2};
+          // the line weight scales u_c, the factor all 15 products share
+          const R wu[3] = {w * u0, w * u1, w * u2};
 #pragma unroll
           for (int c = 0; c < 3; ++c) {
-            gB[c] += w * (fe * u[c]);
-            gB[3 + c] += w * (fh * u[c]);
-            gB[6 + c] += w * (frk * u[c]);
-            gB[9 + c] += w * (fk * u[c]);
-            gB[12 + c] += w * (fet * u[c]);
+            gB[c] += wu[c] * fe;
+            gB[3 + c] += wu[c] * fh;
+            gB[6 + c] += wu[c] * frk;
+            gB[9 + c] += wu[c] * fk;
+            gB[12 + c] += wu[c] * fet;
           }
         }
 #pragma unroll
@@ -287,16 +288,17 @@ __device__ __forceinline__ void rhs_fused_tile(const RhsArgs& a, int tile, unsig
           const R w = Dd[m];
           const R u[3] = {buf[1 * FSTRIDE + sp], buf[2 * FSTRIDE + sp], buf[3 * FSTRIDE + sp]};
           const R q[3] = {buf[4 * FSTRIDE + sp], buf[5 * FSTRIDE + sp], buf[6 * FSTRIDE + sp]};
+          const R wu[3] = {w * u[0], w * u[1], w * u[2]};
 #pragma unroll
           for (int r = 0; r < 3; ++r)
 #pragma unroll
-            for (int c = 0; c < 3; ++c) gQ[3 * r + c] += w * (q[r] * u[c]);
-          gU[0] += w * (u[0] * u[0]);
-          gU[1] += w * (u[0] * u[1]);
-          gU[2] += w * (u[0] * u[2]);
-          gU[3] += w * (u[1] * u[1]);
-          gU[4] += w * (u[1] * u[2]);
-          gU[5] += w * (u[2] * u[2]);
+            for (int c = 0; c < 3; ++c) gQ[3 * r + c] += wu[c] * q[r];
+          gU[0] += wu[0] * u[0];
+          gU[1] += wu[0] * u[1];
+          gU[2] += wu[0] * u[2];
+          gU[3] += wu[1] * u[1];
+          gU[4] += wu[1] * u[2];
+          gU[5] += wu[2] * u[2];
         }
         // u x u is symmetric: component (r, c) is the stored product of min(r,c), max(r,c)
         const int symidx[3][3] = {{0, 1, 2}, {1, 3, 4}, {2, 4, 5}};
@@ -340,7 +342,7 @@ __device__ __forceinline__ void rhs_fused_tile(const RhsArgs& a, int tile, unsig
 }
 
 template <typename R, int EPB, bool TOTH>
-__global__ void __launch_bounds__(64 * EPB) k_rhs_fused(const RhsArgs a) {
+__global__ void __launch_bounds__(64 * EPB, (EPB >= 6 ? 1 : 6 / EPB)) k_rhs_fused(const RhsArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   rhs_fused_tile<R, EPB, TOTH>(a, blockIdx.x, smem_raw);
 }
