@@ -150,16 +150,19 @@ __device__ __forceinline__ bool gather_rk_node(const GatherArgs& a, int n, doubl
         }
         if (!(isfinite(y[0]) && isfinite(y[1]) && isfinite(y[2]) && isfinite(y[3]) && isfinite(y[4])))
           atomicOr(a.nonfinite, 1u);
+        // one reciprocal of rho serves the divisions by rho, and log(p / rho^gamma) is formed
+        // as log p - gamma log rho (no pow): the same quantities to the last bits or so
         const double g = a.gamma;
         const double rho = y[0];
-        const double u0 = y[1] / rho, u1 = y[2] / rho, u2 = y[3] / rho;
+        const double irho = 1.0 / rho;
+        const double u0 = y[1] * irho, u1 = y[2] * irho, u2 = y[3] * irho;
         double umag = u0 * u0 + u1 * u1 + u2 * u2;
-        const double ei = (y[4] / rho) - 0.5 * umag;
+        const double ei = y[4] * irho - 0.5 * umag;
         const double pr = rho * (g - 1.0) * ei;
-        const double cs = sqrt(g * pr / rho);
+        const double cs = sqrt(g * pr * irho);
         umag = sqrt(umag);
-        const double T = pr / (rho * a.Rgas);
-        const double eta = (rho / (g - 1.0)) * log(pr / pow(rho, g));
+        const double T = pr * irho / a.Rgas;
+        const double eta = (rho / (g - 1.0)) * (log(pr) - g * log(rho));
         a.u0[n] = u0; a.u1[n] = u1; a.u2[n] = u2;
         a.e_int[n] = ei; a.pr[n] = pr; a.csound[n] = cs; a.machno[n] = umag / cs;
         a.Tem[n] = T; a.eta[n] = eta;
