@@ -95,7 +95,7 @@ def test_rhs_configs_bitwise_equal(env):
     operations: outputs bit for bit equal; unknown configurations are refused."""
     from sod2d_refmap_b200 import _lib
     S, gm, st1, torch = env["S"], env["gm"], env["st1"], env["torch"]
-    for prec, cfgs in ((S.FP64, (1, 2, 4)), (S.MIXED, (1, 2, 4, 8))):
+    for prec, cfgs in ((S.FP64, (1, 2, 4, 8)), (S.MIXED, (1, 2, 4, 8))):
         outs = []
         for c in cfgs:
             gm.set_rhs_config(prec, c)
