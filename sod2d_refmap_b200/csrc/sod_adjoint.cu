@@ -33,9 +33,9 @@ namespace adj {
 
 constexpr double kC1 = 0.000001458;
 constexpr double kS = 110.4;
-// forward fields staged in shared memory (H = h + k total enthalpy)
-enum { F_RHO = 0, F_H, F_RH, F_T, F_U0, F_U1, F_U2, F_Q0, F_Q1, F_Q2, F_HU0, F_HU1, F_HU2,
-       F_UU00, F_UU01, F_UU02, F_UU11, F_UU12, F_UU22, NF_FWD };
+// forward fields staged in shared memory (H = h + k total enthalpy); the products rho H, H u and
+// u (x) u are formed from them at the line points
+enum { F_RHO = 0, F_H, F_T, F_U0, F_U1, F_U2, F_Q0, F_Q1, F_Q2, NF_FWD };
 // nodal adjoint fields receiving D^T line sums: 11 gradient fields, rho H u and H u (divergence),
 // q (x) u and u (x) u (symmetric, divergence by rows)
 enum { A_RHO = 0, A_P, A_H, A_RH, A_T, A_U0, A_U1, A_U2, A_Q0, A_Q1, A_Q2,
@@ -127,16 +127,12 @@ __global__ void __launch_bounds__(64, SOD_VJP_MIN_BLOCKS) k_rhs_vjp(const VjpArg
   double* Fw = sm;
   Fw[F_RHO * FSTRIDE + s] = rho;
   Fw[F_H * FSTRIDE + s] = Ht;
-  Fw[F_RH * FSTRIDE + s] = rho * Ht;
   Fw[F_T * FSTRIDE + s] = T;
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
     Fw[(F_U0 + c) * FSTRIDE + s] = uv[c];
     Fw[(F_Q0 + c) * FSTRIDE + s] = qv[c];
-    Fw[(F_HU0 + c) * FSTRIDE + s] = Ht * uv[c];
   }
-#pragma unroll
-  for (int t = 0; t < 6; ++t) Fw[(F_UU00 + t) * FSTRIDE + s] = uv[sym_c(t)] * uv[sym_j(t)];
   __syncthreads();
   auto grad = [&](int f, double* o) {
     double gx, gy, gz;
@@ -144,21 +140,44 @@ __global__ void __launch_bounds__(64, SOD_VJP_MIN_BLOCKS) k_rhs_vjp(const VjpArg
 #pragma unroll
     for (int r = 0; r < 3; ++r) o[r] = H[3 * r] * gx + H[3 * r + 1] * gy + H[3 * r + 2] * gz;
   };
-  auto grad_c = [&](int f, int c) {
-    double gx, gy, gz;
-    giso_line(Fw + f * FSTRIDE, i, j, k, Ds.d, gx, gy, gz);
-    return H[3 * c] * gx + H[3 * c + 1] * gy + H[3 * c + 2] * gz;
-  };
   double gRho[3], gH[3], gRH[3], gT[3], gU[3][3], gQ[3][3];
-  grad(F_RHO, gRho); grad(F_H, gH); grad(F_RH, gRH); grad(F_T, gT);
+  grad(F_RHO, gRho); grad(F_H, gH); grad(F_T, gT);
 #pragma unroll
   for (int c = 0; c < 3; ++c) { grad(F_U0 + c, gU[c]); grad(F_Q0 + c, gQ[c]); }
-  const double divHu = grad_c(F_HU0, 0) + grad_c(F_HU1, 1) + grad_c(F_HU2, 2);
-  double divFuu[3];
-  // rows of the symmetric u (x) u: row0 = (00,01,02), row1 = (01,11,12), row2 = (02,12,22)
-  divFuu[0] = grad_c(F_UU00, 0) + grad_c(F_UU01, 1) + grad_c(F_UU02, 2);
-  divFuu[1] = grad_c(F_UU01, 0) + grad_c(F_UU11, 1) + grad_c(F_UU12, 2);
-  divFuu[2] = grad_c(F_UU02, 0) + grad_c(F_UU12, 1) + grad_c(F_UU22, 2);
+  // the product fields rho H, H u_c and u (x) u are formed at the line points from the staged
+  // factors (the line weight applied to the first factor), not staged themselves
+  double divHu = 0.0, divFuu[3] = {0.0, 0.0, 0.0};
+  {
+    double gRHi[3];
+#pragma unroll
+    for (int dir = 0; dir < 3; ++dir) {
+      double lRH = 0.0, lHu[3] = {0.0, 0.0, 0.0}, lUU[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+      const int x = dir == 0 ? i : (dir == 1 ? j : k);
+#pragma unroll
+      for (int m = 0; m < NP1; ++m) {
+        const int sp = dir == 0 ? sidx(m, j, k) : (dir == 1 ? sidx(i, m, k) : sidx(i, j, m));
+        const double w = Ds.d[x][m];
+        const double r_ = Fw[F_RHO * FSTRIDE + sp], H_ = Fw[F_H * FSTRIDE + sp];
+        const double u_[3] = {Fw[F_U0 * FSTRIDE + sp], Fw[F_U1 * FSTRIDE + sp], Fw[F_U2 * FSTRIDE + sp]};
+        const double wH = w * H_;
+        lRH += wH * r_;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) lHu[c] += wH * u_[c];
+        const double wu[3] = {w * u_[0], w * u_[1], w * u_[2]};
+#pragma unroll
+        for (int t = 0; t < 6; ++t) lUU[t] += wu[sym_c(t)] * u_[sym_j(t)];
+      }
+      gRHi[dir] = lRH;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) divHu += H[3 * c + dir] * lHu[c];
+      // rows of the symmetric u (x) u: row0 = (00,01,02), row1 = (01,11,12), row2 = (02,12,22)
+      divFuu[0] += H[dir] * lUU[0] + H[3 + dir] * lUU[1] + H[6 + dir] * lUU[2];
+      divFuu[1] += H[dir] * lUU[1] + H[3 + dir] * lUU[3] + H[6 + dir] * lUU[4];
+      divFuu[2] += H[dir] * lUU[2] + H[3 + dir] * lUU[4] + H[6 + dir] * lUU[5];
+    }
+#pragma unroll
+    for (int r = 0; r < 3; ++r) gRH[r] = H[3 * r] * gRHi[0] + H[3 * r + 1] * gRHi[1] + H[3 * r + 2] * gRHi[2];
+  }
   const double divU = gU[0][0] + gU[1][1] + gU[2][2];
   const double divQ = gQ[0][0] + gQ[1][1] + gQ[2][2];
   // diffusion pass 1 (stresses) and the contravariant gradRho / gradT fluxes for pass 2
