@@ -66,19 +66,34 @@ def _load(s: Sod2dState, c: _Ckpt):
 
 
 def rollout(mesh: Sod2dMesh, state: Sod2dState, nsteps: int, checkpoint_every: int = 10, precision: int = FP64,
-            stages=None):
+            stages=None, tail=None):
     """Run nsteps steps in place (dt from the CFL condition after every step, as rk_4_main)
     and return the checkpoints [(step index, _Ckpt)] at multiples of checkpoint_every.  With
-    stages (nsteps, 15*npoin) every step is a checkpoint and records its stage states there."""
+    stages (nsteps, 15*npoin) every step is a checkpoint and records its stage states there.
+    With tail (a list; stages None) the last segment runs with its stage states recorded into a
+    buffer of min(checkpoint_every, nsteps) steps, and tail receives [per-step states, buffer]:
+    the backward pass then starts without re-running that segment, and reuses the buffer for the
+    others (the size it would allocate itself)."""
+    torch = _torch()
     ck = []
     les = _les(mesh)
+    last = ((nsteps - 1) // checkpoint_every) * checkpoint_every if nsteps > 0 else 0
+    buf = stack = None
+    if tail is not None and stages is None and nsteps > 0:
+        buf = torch.empty(min(checkpoint_every, nsteps), 15 * state.npoin, dtype=torch.float64, device="cuda")
+        stack = []
     for n in range(nsteps):
         if stages is not None or n % checkpoint_every == 0:
             ck.append((n, _ckpt(state, les)))
         if stages is not None:
             mesh.rk_4_main_record(state, stages[n], update_dt=True, precision=precision)
+        elif buf is not None and n >= last:
+            stack.append(_ckpt(state, les))
+            mesh.rk_4_main_record(state, buf[n - last], update_dt=True, precision=precision)
         else:
             mesh.rk_4_main(state, precision, update_dt=True)
+    if buf is not None:
+        tail.extend([stack, buf])
     return ck
 
 
@@ -109,11 +124,12 @@ def trajectory_coefficients(mesh: Sod2dMesh, state: Sod2dState, nsteps: int, pre
 
 
 def backward_through(mesh: Sod2dMesh, template: Sod2dState, ckpts, nsteps: int, bar_rho, bar_q, bar_E,
-                     store_stages: bool = True, precision: int = FP64, trajectory=None):
+                     store_stages: bool = True, precision: int = FP64, trajectory=None, tail=None):
     """Adjoint of nsteps steps: (bar_rho, bar_q, bar_E) at step nsteps -> at step 0, in place.
     Each segment is re-run from its checkpoint; with store_stages the re-run keeps the RK stage
     states (15*npoin doubles per step) so that the step VJPs need no second recompute.  With
-    trajectory (the forward's per-step stage states, every step a checkpoint) nothing is re-run."""
+    trajectory (the forward's per-step stage states, every step a checkpoint) nothing is re-run;
+    with tail (rollout's record of the last segment) that segment is not re-run."""
     torch = _torch()
     if trajectory is not None:
         for t in range(nsteps - 1, -1, -1):
@@ -124,19 +140,26 @@ def backward_through(mesh: Sod2dMesh, template: Sod2dState, ckpts, nsteps: int, 
     s = _clone_state(template)
     bounds = [c[0] for c in ckpts] + [nsteps]
     longest = max(bounds[i + 1] - bounds[i] for i in range(len(ckpts)))
-    stages = (torch.empty(longest, 15 * s.npoin, dtype=torch.float64, device="cuda") if store_stages else None)
+    use_tail = bool(tail) and store_stages and tail[1].shape[0] >= longest
+    if use_tail:
+        stages = tail[1]
+    else:
+        stages = (torch.empty(longest, 15 * s.npoin, dtype=torch.float64, device="cuda") if store_stages else None)
     for seg in range(len(ckpts) - 1, -1, -1):
         n0, c = ckpts[seg]
         n1 = bounds[seg + 1]
-        _load(s, c)
-        stack = []
-        les = c.mu_sgs is not None
-        for t in range(n1 - n0):
-            stack.append(_ckpt(s, les))
-            if store_stages:
-                mesh.rk_4_main_record(s, stages[t], update_dt=True, precision=precision)
-            else:
-                mesh.rk_4_main(s, precision, update_dt=True)
+        if use_tail and seg == len(ckpts) - 1:
+            stack = tail[0]  # the forward pass recorded this segment's states and stage states
+        else:
+            _load(s, c)
+            stack = []
+            les = c.mu_sgs is not None
+            for t in range(n1 - n0):
+                stack.append(_ckpt(s, les))
+                if store_stages:
+                    mesh.rk_4_main_record(s, stages[t], update_dt=True, precision=precision)
+                else:
+                    mesh.rk_4_main(s, precision, update_dt=True)
         for t in range(n1 - n0 - 1, -1, -1):
             cs = stack[t]
             mesh.rk4_step_vjp(cs.rho, cs.q, cs.E, cs.mu_e, template.mu_factor, cs.dt, bar_rho, bar_q, bar_E,
@@ -166,9 +189,11 @@ class Sod2dRollout:
                 s.u.copy_(s.q / s.rho)  # u(pos) of the state (read by slip walls) is q / rho
                 traj = (torch.empty(nsteps, 15 * s.npoin, dtype=torch.float64, device="cuda")
                         if keep_trajectory else None)
-                ck = rollout(mesh, s, nsteps, checkpoint_every, precision, stages=traj)
+                tail = [] if (store_stages and not keep_trajectory) else None
+                ck = rollout(mesh, s, nsteps, checkpoint_every, precision, stages=traj, tail=tail)
                 ctx.ck = ck
                 ctx.traj = traj
+                ctx.tail = tail
                 ctx.template = state
                 return s.rho.clone(), s.q.clone(), s.E.clone()
 
@@ -177,8 +202,9 @@ class Sod2dRollout:
                 z = lambda g, like: torch.zeros_like(like) if g is None else g.contiguous().clone()
                 br, bq, bE = z(g_rho, rho), z(g_q, q), z(g_E, E)
                 backward_through(mesh, ctx.template, ctx.ck, nsteps, br, bq, bE, store_stages, precision,
-                                 trajectory=ctx.traj)
+                                 trajectory=ctx.traj, tail=ctx.tail)
                 ctx.traj = None
+                ctx.tail = None
                 return br, bq, bE
 
         return _Fn.apply(rho, q, E)
