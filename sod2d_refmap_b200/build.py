@@ -55,7 +55,22 @@ def build(force: bool = False, verbose: bool = False, extra: list | None = None)
     subprocess.run(cmd, check=True)
     for o in objs:
         os.remove(o)
+    _check_resolved(LIB)
     return LIB
+
+
+def _check_resolved(lib: str) -> None:
+    """A shared library links with undefined symbols and fails only when loaded; refuse a build
+    that leaves one of the library's own (namespace sod) functions undefined, e.g. a declaration
+    in one source file that no longer matches its definition in another."""
+    try:
+        out = subprocess.run(["nm", "-C", "-u", lib], capture_output=True, text=True, check=True).stdout
+    except (OSError, subprocess.CalledProcessError):
+        return  # no nm on this machine: nothing to check with
+    missing = [ln.strip() for ln in out.splitlines() if "sod::" in ln]
+    if missing:
+        os.remove(lib)
+        raise RuntimeError("libsod2d_b200 has undefined internal symbols:\n  " + "\n  ".join(missing))
 
 
 if __name__ == "__main__":

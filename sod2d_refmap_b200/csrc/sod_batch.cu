@@ -15,7 +15,7 @@
 
 namespace sod {
 int run_step(SodMesh* m, SodState* s, const double* dt_dev, double* dt_next, bool mixed, cudaStream_t st,
-             cudaEvent_t* ev, double* stage_store);
+             cudaEvent_t* ev, double* stage_store, cudaEvent_t state_done);
 int launch_visc_dt(SodMesh* m, const SodState* s, double* dt_out, float* mue32, cudaStream_t st);
 }  // namespace sod
 
@@ -280,7 +280,7 @@ int sod_batch_rk4_steps(SodBatch* B, int nsteps, SodPrecision prec, sod_stream_t
       cudaGraph_t graph;
       const int64_t before = g_launches.load();
       SOD_CUDA(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
-      rc = run_step(m, &B->st, B->dt, B->dt, mixed, cap, nullptr, nullptr);
+      rc = run_step(m, &B->st, B->dt, B->dt, mixed, cap, nullptr, nullptr, nullptr);
       cudaError_t ce = cudaStreamEndCapture(cap, &graph);
       cudaStreamDestroy(cap);
       if (rc) return rc;

@@ -286,6 +286,9 @@ struct SodMesh {
   struct TuneEntry { int epb, ctas; float ms; };
   std::vector<TuneEntry> tune_table[2];  // the last sod_autotune sweep per precision
   std::vector<double*> host_mirror;  // device buffers of sod_rk4_main_host
+  // sod_rk4_main_host's read-back: a stream and two events (created on first use)
+  cudaStream_t host_copy_stream = nullptr;
+  cudaEvent_t host_ev_state = nullptr, host_ev_copied = nullptr;
   // ensemble members (a SodBatch's concatenated mesh); nmember == 0 for a single mesh
   int nmember = 0;
   int32_t* node_member = nullptr;   // [npoin]

@@ -367,6 +367,9 @@ void sod_mesh_destroy(SodMesh* m) {
   for (void* p : ptrs)
     if (p) cudaFree(p);
   for (double* p : m->host_mirror) cudaFree(p);
+  if (m->host_copy_stream) cudaStreamDestroy(m->host_copy_stream);
+  if (m->host_ev_state) cudaEventDestroy(m->host_ev_state);
+  if (m->host_ev_copied) cudaEventDestroy(m->host_ev_copied);
   delete m;
 }
 

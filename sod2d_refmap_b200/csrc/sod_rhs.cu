@@ -701,8 +701,10 @@ static int run_step_persist(SodMesh* m, SodState* s, SodState& loc, const double
 // ev[2*slot] / ev[2*slot+1] bracket each kernel: slots 0-3 KR stages, 4-7 KG stages, 8 KV.
 // When stage_store is non-null the stage states Y2, Y3, Y4 (5 columns of npoin each) are
 // written there instead of the internal stage buffer (for the adjoint's reverse sweep).
+// state_done (optional) is recorded on st once the new state and its EOS fields are final, before
+// the entropy viscosity and dt (and LES's sgs viscosity) that end the step.
 int run_step(SodMesh* m, SodState* s, const double* dt_dev, double* dt_next, bool mixed, cudaStream_t st,
-             cudaEvent_t* ev = nullptr, double* stage_store = nullptr) {
+             cudaEvent_t* ev = nullptr, double* stage_store = nullptr, cudaEvent_t state_done = nullptr) {
   NvtxRange range(mixed ? "sod rk4 step (mixed)" : "sod rk4 step (fp64)");
   const size_t N = m->npoin;
   const int epb = m->tuned_epb[mixed ? 1 : 0] ? m->tuned_epb[mixed ? 1 : 0] : (mixed ? 4 : 2);
@@ -721,8 +723,12 @@ int run_step(SodMesh* m, SodState* s, const double* dt_dev, double* dt_next, boo
   const bool zone = m->zone.nb > 0;
   const bool pre = bc || zone;
   const int pctas = m->persist_ctas[mixed ? 1 : 0];
-  if (pctas > 0 && !pre && !les && m->wmodel.nw == 0 && !m->source && !ev && !stage_store)
-    return run_step_persist(m, s, loc, dt_dev, dt_next, mixed, epb, pctas, st);
+  if (pctas > 0 && !pre && !les && m->wmodel.nw == 0 && !m->source && !ev && !stage_store) {
+    // the one-launch stages form the entropy viscosity inside stage 4: the state is final at the end
+    rc = run_step_persist(m, s, loc, dt_dev, dt_next, mixed, epb, pctas, st);
+    if (!rc && state_done) SOD_CUDA(cudaEventRecord(state_done, st));
+    return rc;
+  }
   auto pre_stage = [&](double* ys, int stage_of) -> int {
     if (zone)
       if (int r = zone_stage(m, ys, st)) return r;
@@ -786,6 +792,7 @@ int run_step(SodMesh* m, SodState* s, const double* dt_dev, double* dt_next, boo
     if (ev) cudaEventRecord(ev[2 * (3 + stage) + 1], st);
   }
   if (ev) cudaEventRecord(ev[16], st);
+  if (state_done) SOD_CUDA(cudaEventRecord(state_done, st));
   if (les) {
     // sgs_visc after the step (time_integ.f90:498-506), before the dt of the next step uses it
     // (CFDSolverBase.f90:1592); independent of the entropy viscosity, so it may run first
@@ -811,8 +818,16 @@ static int check_state(SodMesh* m, SodState* s) {
 
 extern "C" {
 
+static int rk4_main_impl(SodMesh* m, SodState* s, const double* dt_dev, double* dt_next_dev, SodPrecision prec,
+                         sod_stream_t stream, cudaEvent_t state_done);
+
 int sod_rk4_main(SodMesh* m, SodState* s, const double* dt_dev, double* dt_next_dev, SodPrecision prec,
                  sod_stream_t stream) {
+  return rk4_main_impl(m, s, dt_dev, dt_next_dev, prec, stream, nullptr);
+}
+
+static int rk4_main_impl(SodMesh* m, SodState* s, const double* dt_dev, double* dt_next_dev, SodPrecision prec,
+                         sod_stream_t stream, cudaEvent_t state_done) {
   int rc = check_state(m, s);
   if (rc) return rc;
   SOD_ARG(dt_dev, "dt_dev null");
@@ -829,7 +844,7 @@ int sod_rk4_main(SodMesh* m, SodState* s, const double* dt_dev, double* dt_next_
     rc = launch_copy_f32(m->mue_int, m->mue32, (int64_t)m->nelem * NN, st);
     if (rc) return rc;
   }
-  rc = run_step(m, s, dt_dev, dt_next_dev, mixed, st);
+  rc = run_step(m, s, dt_dev, dt_next_dev, mixed, st, nullptr, nullptr, state_done);
   if (rc) return rc;
   rc = les_out(m, s, st);
   if (rc) return rc;
@@ -1188,11 +1203,26 @@ int sod_rk4_main_host(SodMesh* m, SodState* h, double dt_host, double* dt_next_h
     for (int i = 3; i < 11; ++i)
       if (outs[i].hst) SOD_CUDA(cudaMemcpyAsync(outs[i].dev, outs[i].hst, outs[i].n * 8, cudaMemcpyHostToDevice, st));
   if (m->has_slaves && h->Reta) SOD_CUDA(cudaMemcpyAsync(d.Reta, h->Reta, N * 8, cudaMemcpyHostToDevice, st));
-  int rc = sod_rk4_main(m, &d, ddt, ddt, prec, stream);
+  // the state fields are copied back on a second stream as soon as the step has formed them, so
+  // that the read-back overlaps the entropy viscosity and dt that end the step; mu_e (and mu_sgs)
+  // and dt follow on the caller's stream, which then waits for the copies
+  if (!m->host_copy_stream) {
+    SOD_CUDA(cudaStreamCreateWithFlags(&m->host_copy_stream, cudaStreamNonBlocking));
+    SOD_CUDA(cudaEventCreateWithFlags(&m->host_ev_state, cudaEventDisableTiming));
+    SOD_CUDA(cudaEventCreateWithFlags(&m->host_ev_copied, cudaEventDisableTiming));
+  }
+  cudaStream_t cs = m->host_copy_stream;
+  int rc = rk4_main_impl(m, &d, ddt, ddt, prec, stream, m->host_ev_state);
   if (rc) return rc;
-  for (auto& o : outs)
-    if (o.hst) SOD_CUDA(cudaMemcpyAsync(o.hst, o.dev, o.n * 8, cudaMemcpyDeviceToHost, st));
+  SOD_CUDA(cudaStreamWaitEvent(cs, m->host_ev_state, 0));
+  for (auto& o : outs) {
+    if (!o.hst) continue;
+    const bool tail = o.dev == d.mu_e || o.dev == d.mu_sgs;  // written after the state is final
+    SOD_CUDA(cudaMemcpyAsync(o.hst, o.dev, o.n * 8, cudaMemcpyDeviceToHost, tail ? st : cs));
+  }
+  SOD_CUDA(cudaEventRecord(m->host_ev_copied, cs));
   if (dt_next_host) SOD_CUDA(cudaMemcpyAsync(dt_next_host, ddt, 8, cudaMemcpyDeviceToHost, st));
+  SOD_CUDA(cudaStreamWaitEvent(st, m->host_ev_copied, 0));
   if (int rc2 = sync_stream(st)) return rc2;
   bool bad = false;
   if (int rc3 = take_nonfinite(m, st, &bad)) return rc3;
