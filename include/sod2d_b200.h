@@ -280,7 +280,9 @@ int sod_compute_field_derivs(SodMesh* mesh, const double* rho, const double* u, 
  * calls rk_4_main on host arrays): copies rho,q,E,mu_e,mu_factor in, runs one step and copies
  * rho,q,E,u,pr,Tem,e_int,eta,csound,machno,mu_fluid,mu_e back.  dt_host in, dt_next_host out.
  * On a mesh with periodic slave rows (lpoin_w) the fields it copies back are also copied in, so
- * that their slave rows come back as they were. */
+ * that their slave rows come back as they were.  The state fields are copied back on a stream
+ * the mesh owns, which starts once the step has formed them; the call returns after every copy
+ * has landed (pinned host arrays give the copies their full PCIe rate). */
 int sod_rk4_main_host(SodMesh* mesh, SodState* host_state, double dt_host, double* dt_next_host,
                       SodPrecision prec, sod_stream_t stream);
 
