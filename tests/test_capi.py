@@ -39,3 +39,23 @@ def test_library_has_no_cpu_fallback_symbols():
     from sod2d_refmap_b200 import _lib
     out = subprocess.run(["nm", "-D", _lib.LIB_PATH], capture_output=True, text=True, check=True).stdout
     assert "oracle_" not in out
+
+
+def test_library_resolves_its_own_symbols():
+    """No function of the library's own namespace is left undefined (a declaration in one source
+    file that no longer matches its definition links and fails only at load time)."""
+    from sod2d_refmap_b200 import _lib
+    out = subprocess.run(["nm", "-C", "-u", _lib.LIB_PATH], capture_output=True, text=True, check=True).stdout
+    assert not [ln for ln in out.splitlines() if "sod::" in ln]
+
+
+def test_build_check_refuses_unresolved_internal_symbol(tmp_path):
+    """build._check_resolved removes a library that references an undefined sod:: function."""
+    from sod2d_refmap_b200 import build
+    src = tmp_path / "bad.cpp"
+    src.write_text("namespace sod { int missing(int); }\nextern \"C\" int entry(int x) { return sod::missing(x); }\n")
+    lib = tmp_path / "libbad.so"
+    subprocess.run(["g++", "-shared", "-fPIC", "-o", str(lib), str(src)], check=True)
+    with pytest.raises(RuntimeError, match="undefined internal symbols"):
+        build._check_resolved(str(lib))
+    assert not lib.exists()
