@@ -67,7 +67,7 @@ __device__ __forceinline__ R divT(const R* fx, const R* fy, const R* fz, int i, 
          (DTz[0] * az[0] + DTz[1] * az[PLANE] + DTz[2] * az[2 * PLANE] + DTz[3] * az[3 * PLANE]);
 }
 
-constexpr int NBUF = 15;  // fields per batch buffer
+constexpr int NBUF = 13;  // batch-A fields (12, and p + E with flag_total_enthalpy)
 constexpr int NP2 = 18;   // 6 contravariant fluxes x 3 directions
 
 template <typename R>
@@ -136,17 +136,18 @@ __device__ __forceinline__ void rhs_fused_tile(const RhsArgs& a, int tile, unsig
     buf[(4 + c) * FSTRIDE + s_me] = (R)qv[c];
   }
   buf[7 * FSTRIDE + s_me] = (R)p;
-  buf[8 * FSTRIDE + s_me] = (R)h;
-  buf[9 * FSTRIDE + s_me] = (R)(rho * h);
-  buf[10 * FSTRIDE + s_me] = (R)kk;
-  buf[11 * FSTRIDE + s_me] = (R)(rho * kk);
-  buf[12 * FSTRIDE + s_me] = (R)eta_full;
-  buf[13 * FSTRIDE + s_me] = (R)T;
+  // the energy convection is linear in (h, k) and every h term of elem_convec.f90:415-425 has a k
+  // twin of the same form: both quartets are evaluated at once on the total enthalpy H = h + k
+  const double Ht = h + kk;
+  buf[8 * FSTRIDE + s_me] = (R)Ht;
+  buf[9 * FSTRIDE + s_me] = (R)(rho * Ht);
+  buf[10 * FSTRIDE + s_me] = (R)eta_full;
+  buf[11 * FSTRIDE + s_me] = (R)T;
   // flag_total_enthalpy: full_convec_ijk_H differentiates p + E and (E + p) u
-  if constexpr (TOTH) buf[14 * FSTRIDE + s_me] = (R)(p + Et);
+  if constexpr (TOTH) buf[12 * FSTRIDE + s_me] = (R)(p + Et);
   __syncthreads();
 
-  R gradRho[3], gradU[3][3], gradQ[3][3], gradP[3], gradH[3], gradRH[3], gradK[3], gradRK[3], gradEta[3], gradT[3];
+  R gradRho[3], gradU[3][3], gradQ[3][3], gradP[3], gradH[3], gradRH[3], gradEta[3], gradT[3];
   R uGradEp = R(0);  // flag_total_enthalpy: sum_c 0.5 u_c d(p + E)/dx_c
   {
     R gx, gy, gz;
@@ -166,16 +167,12 @@ __device__ __forceinline__ void rhs_fused_tile(const RhsArgs& a, int tile, unsig
     giso(buf + 9 * FSTRIDE, i, j, k, Dx, Dy, Dz, gx, gy, gz);
     phys(H, gx, gy, gz, gradRH[0], gradRH[1], gradRH[2]);
     giso(buf + 10 * FSTRIDE, i, j, k, Dx, Dy, Dz, gx, gy, gz);
-    phys(H, gx, gy, gz, gradK[0], gradK[1], gradK[2]);
-    giso(buf + 11 * FSTRIDE, i, j, k, Dx, Dy, Dz, gx, gy, gz);
-    phys(H, gx, gy, gz, gradRK[0], gradRK[1], gradRK[2]);
-    giso(buf + 12 * FSTRIDE, i, j, k, Dx, Dy, Dz, gx, gy, gz);
     phys(H, gx, gy, gz, gradEta[0], gradEta[1], gradEta[2]);
-    giso(buf + 13 * FSTRIDE, i, j, k, Dx, Dy, Dz, gx, gy, gz);
+    giso(buf + 11 * FSTRIDE, i, j, k, Dx, Dy, Dz, gx, gy, gz);
     phys(H, gx, gy, gz, gradT[0], gradT[1], gradT[2]);
     if constexpr (TOTH) {
       R gradEp[3];
-      giso(buf + 14 * FSTRIDE, i, j, k, Dx, Dy, Dz, gx, gy, gz);
+      giso(buf + 12 * FSTRIDE, i, j, k, Dx, Dy, Dz, gx, gy, gz);
       phys(H, gx, gy, gz, gradEp[0], gradEp[1], gradEp[2]);
 #pragma unroll
       for (int c = 0; c < 3; ++c) uGradEp = uGradEp + R(0.5) * ((R)uv[c] * gradEp[c]);
@@ -183,22 +180,21 @@ __device__ __forceinline__ void rhs_fused_tile(const RhsArgs& a, int tile, unsig
   }
   const R divU = gradU[0][0] + gradU[1][1] + gradU[2][2];
   const R divQ = gradQ[0][0] + gradQ[1][1] + gradQ[2][2];
-  const R rhoR = (R)rho, hR = (R)h, kR = (R)kk, etaR = (R)eta_full;
+  const R rhoR = (R)rho, HR = (R)Ht, etaR = (R)eta_full;
   const R uR[3] = {(R)uv[0], (R)uv[1], (R)uv[2]};
   const R qR[3] = {(R)qv[0], (R)qv[1], (R)qv[2]};
-  const R rhR = (R)(rho * h), rkR = (R)(rho * kk);
+  const R rHR = (R)(rho * Ht);
 
   // ---- convective terms available after batch A (elem_convec.f90:412-432)
   R Rm = R(0.5) * (divQ + rhoR * divU);
-  R Ren = R(0.25) * (hR * divQ + rhR * divU) + R(0.25) * (kR * divQ + rkR * divU);
+  R Ren = R(0.25) * (HR * divQ + rHR * divU);
   R Rmo[3];
   R Ret = R(0.5) * (etaR * divU);
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
     Rmo[c] = R(0.25) * (uR[c] * divQ + qR[c] * divU) + gradP[c];
     Rm += R(0.5) * (uR[c] * gradRho[c]);
-    Ren += R(0.25) * (qR[c] * gradH[c] + uR[c] * gradRH[c] + (hR * uR[c]) * gradRho[c]) +
-           R(0.25) * (qR[c] * gradK[c] + uR[c] * gradRK[c] + (kR * uR[c]) * gradRho[c]);
+    Ren += R(0.25) * (qR[c] * gradH[c] + uR[c] * gradRH[c] + (HR * uR[c]) * gradRho[c]);
     Ret += R(0.5) * (uR[c] * gradEta[c]);
 #pragma unroll
     for (int jd = 0; jd < 3; ++jd)
@@ -233,37 +229,35 @@ __device__ __forceinline__ void rhs_fused_tile(const RhsArgs& a, int tile, unsig
     emit(4, tau[1][0], tau[1][1], tau[1][2]);
     emit(5, tau[2][0], tau[2][1], tau[2][2]);
   }
-  // ---- batches B and C: divergences of the product vectors (rho h u, h u, rho k u, k u, eta u;
-  // (E + p) u with flag_total_enthalpy) and tensors (q x u, u x u).  Every line point m forms its
-  // 30 terms D[x][m] f u_c of the line sums from batch A's slots as (D[x][m] u_c) f, so nothing
-  // more is staged; the line sums of each direction are folded with He before the next direction.
+  // ---- batches B and C: divergences of the product vectors (rho H u, H u, eta u; (E + p) u with
+  // flag_total_enthalpy) and tensors (q x u, u x u).  Every line point m forms its 24 terms
+  // D[x][m] f u_c of the line sums from batch A's slots as (D[x][m] u_c) f, so nothing more is
+  // staged; the line sums of each direction are folded with He before the next direction.
   {
-    R divFe = R(0), divFue = R(0), divFk = R(0), divFuk = R(0), divFeta = R(0);
+    R divFe = R(0), divFue = R(0), divFeta = R(0);
     R dF[3] = {R(0), R(0), R(0)}, dFuu[3] = {R(0), R(0), R(0)};
 #pragma unroll
     for (int dir = 0; dir < 3; ++dir) {
       const R* Dd = dir == 0 ? Dx : (dir == 1 ? Dy : Dz);
       {
-        R gB[15];
+        R gB[9];
 #pragma unroll
-        for (int q = 0; q < 15; ++q) gB[q] = R(0);
+        for (int q = 0; q < 9; ++q) gB[q] = R(0);
 #pragma unroll
         for (int m = 0; m < 4; ++m) {
           const int sp = dir == 0 ? sidx(m, j, k) : (dir == 1 ? sidx(i, m, k) : sidx(i, j, m));
           const R w = Dd[m];
           const R u0 = buf[1 * FSTRIDE + sp], u1 = buf[2 * FSTRIDE + sp], u2 = buf[3 * FSTRIDE + sp];
-          const R fe = TOTH ? buf[14 * FSTRIDE + sp] : buf[9 * FSTRIDE + sp];
-          const R fh = buf[8 * FSTRIDE + sp], frk = buf[11 * FSTRIDE + sp], fk = buf[10 * FSTRIDE + sp];
-          const R fet = buf[12 * FSTRIDE + sp];
-          // the line weight scales u_c, the factor all 15 products share
+          const R fe = TOTH ? buf[12 * FSTRIDE + sp] : buf[9 * FSTRIDE + sp];
+          const R fh = buf[8 * FSTRIDE + sp];
+          const R fet = buf[10 * FSTRIDE + sp];
+          // the line weight scales u_c, the factor all 9 products share
           const R wu[3] = {w * u0, w * u1, w * u2};
 #pragma unroll
           for (int c = 0; c < 3; ++c) {
             gB[c] += wu[c] * fe;
             gB[3 + c] += wu[c] * fh;
-            gB[6 + c] += wu[c] * frk;
-            gB[9 + c] += wu[c] * fk;
-            gB[12 + c] += wu[c] * fet;
+            gB[6 + c] += wu[c] * fet;
           }
         }
 #pragma unroll
@@ -271,9 +265,7 @@ __device__ __forceinline__ void rhs_fused_tile(const RhsArgs& a, int tile, unsig
           const R hc = H[3 * c + dir];
           divFe += hc * gB[c];
           divFue += hc * gB[3 + c];
-          divFk += hc * gB[6 + c];
-          divFuk += hc * gB[9 + c];
-          divFeta += hc * gB[12 + c];
+          divFeta += hc * gB[6 + c];
         }
       }
       {
@@ -312,7 +304,7 @@ __device__ __forceinline__ void rhs_fused_tile(const RhsArgs& a, int tile, unsig
           }
       }
     }
-    Ren += R(0.25) * (divFe + rhoR * divFue) + R(0.25) * (divFk + rhoR * divFuk);
+    Ren += R(0.25) * (divFe + rhoR * divFue);
     Ret += R(0.5) * divFeta;
     if constexpr (TOTH) Ren = R(0.5) * (divFe + (R)(Et + p) * divU) + uGradEp;  // elem_convec.f90:171-177
 #pragma unroll
