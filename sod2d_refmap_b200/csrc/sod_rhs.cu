@@ -378,7 +378,17 @@ __global__ void __launch_bounds__(256, SOD_KG_MIN_BLOCKS) k_gather_rk(const Gath
 __global__ void __launch_bounds__(64 * KV_EPB, SOD_KV_MIN_BLOCKS) k_visc_dt(const ViscArgs a) {
   __shared__ double sm[KV_EPB][KV_SMEM];
   const int es = threadIdx.x >> 6;
-  visc_dt_elem(a, blockIdx.x * KV_EPB + es, threadIdx.x & 63, sm[es]);
+  // one mesh: one dt atomic per block on the minimum of its elements' limits (read after the
+  // element bodies' barriers), instead of one per element on the same address
+  const bool per_elem = a.elem_member != nullptr;
+  visc_dt_elem(a, blockIdx.x * KV_EPB + es, threadIdx.x & 63, sm[es], per_elem);
+  if (!per_elem && a.dt_out && threadIdx.x == 0) {
+    unsigned long long b = (unsigned long long)__double_as_longlong(sm[0][KV_DT_SLOT]);
+#pragma unroll
+    for (int q = 1; q < KV_EPB; ++q)
+      if (blockIdx.x * KV_EPB + q < a.nelem) b = min(b, (unsigned long long)__double_as_longlong(sm[q][KV_DT_SLOT]));
+    atomicMin(reinterpret_cast<unsigned long long*>(a.dt_bits), b);
+  }
 }
 
 // ---------------------------------------------------------------------------------------------

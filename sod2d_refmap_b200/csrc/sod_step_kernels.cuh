@@ -271,11 +271,20 @@ __device__ __forceinline__ double warp_max_f64(double v) {
   return __hiloint2double((int)(mh ^ (back | 0x80000000u)), (int)(ml ^ back));
 }
 
+// 8-byte asynchronous global -> shared copy (L1-allocating), completed by cp.async.wait_all
+__device__ __forceinline__ void cp_async8(double* sdst, const double* gsrc) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(sdst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gsrc) : "memory");
+}
+
 // One element per 64 threads (d = the element node); sm holds the element's KV_SMEM doubles of
-// shared memory: ml[64], fl[64] (filter passes), wm[2][5] (per-warp maxima), elem_s[2] (ced and
-// the element's dt limit).  Every thread of the block calls it (it holds block barriers).
-constexpr int KV_SMEM = 2 * NN + 10 + 2;
-__device__ __forceinline__ void visc_dt_elem(const ViscArgs& a, int e, int d, double* sm) {
+// shared memory: ml[64], fl[64] (filter passes), wm[2][5] (per-warp maxima), elem_s[4] (ced, the
+// element's dt limit, and the prefetched jratio and entropy norm).  Every thread of the block
+// calls it (it holds block barriers).  elem_atomic: the element's own dt atomic; a caller that
+// passes false reduces the limits elem_s[1] of its elements itself after the call.
+constexpr int KV_SMEM = 2 * NN + 10 + 4;
+constexpr int KV_DT_SLOT = 2 * NN + 10 + 1;   // elem_s[1] within an element's KV_SMEM doubles
+__device__ __forceinline__ void visc_dt_elem(const ViscArgs& a, int e, int d, double* sm, bool elem_atomic = true) {
   double* ml = sm;
   double* fl = sm + NN;
   double* wm = sm + 2 * NN;          // [warp][5]
@@ -287,6 +296,13 @@ __device__ __forceinline__ void visc_dt_elem(const ViscArgs& a, int e, int d, do
   // inputs of the second half, loaded before the element reductions so their latency overlaps them
   const double reta_n = a.Reta[n];
   const double hl = a.helem_l[(size_t)ee * NN + d];
+  // the element scalars read after the barriers (jratio by the element's scalar thread, the
+  // entropy norm by all) go to shared memory asynchronously, off the path behind the barriers
+  if (d == 0) {
+    cp_async8(elem_s + 2, a.jratio + ee);
+    cp_async8(elem_s + 3, a.elem_member ? a.member_scal + 2 * a.elem_member[ee] + 1 : a.scal + 1);
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+  }
   const double vmag = sqrt(u0 * u0 + u1 * u1 + u2 * u2);
   const double he = a.helem[ee];
   // betae node term (mod_entropy_viscosity.f90:90-95)
@@ -301,6 +317,7 @@ __device__ __forceinline__ void visc_dt_elem(const ViscArgs& a, int e, int d, do
   double mL = warp_max_f64(L3n), mM = warp_max_f64(mun);
   const int wi = d >> 5;
   if ((d & 31) == 0) { wm[5 * wi + 0] = mV; wm[5 * wi + 1] = mC; wm[5 * wi + 2] = mB; wm[5 * wi + 3] = mL; wm[5 * wi + 4] = mM; }
+  if (d == 0) asm volatile("cp.async.wait_all;\n" ::: "memory");
   __syncthreads();
   if (d == 0) {
     // shock sensor and cap, once per element (mod_entropy_viscosity.f90:81-84); M**15 as an
@@ -309,7 +326,7 @@ __device__ __forceinline__ void visc_dt_elem(const ViscArgs& a, int e, int d, do
     const double M2 = M * M, M4 = M2 * M2, M8 = M4 * M4;
     const double M15 = M8 * M4 * M2 * M;
     const double ceM = fmax(tanh(M15 * 3.141592653589793), a.prm.ce);
-    double ced = fmax(1.0 - a.jratio[ee], a.prm.ce);
+    double ced = fmax(1.0 - elem_s[2], a.prm.ce);
     elem_s[0] = fmax(ced, ceM);
     const double hh = he / (double)(2.0 * P + 1);
     const double L3 = fmax(wm[3], wm[8]);
@@ -319,12 +336,11 @@ __device__ __forceinline__ void visc_dt_elem(const ViscArgs& a, int e, int d, do
   __syncthreads();
   const double ced = elem_s[0];
   mB = fmax(wm[2], wm[7]);
-  const int mem = a.elem_member ? a.elem_member[ee] : 0;
-  const double norm = a.elem_member ? a.member_scal[2 * mem + 1] : a.scal[1];
+  const double norm = elem_s[3];
   const double R1 = (norm > 0.0) ? rho * fabs(reta_n) / norm : 0.0;
   const double Ve = ced * R1 * hl * hl;
   ml[d] = a.prm.cglob * fmin(Ve, mB);
-  __syncthreads();
+  __syncwarp();   // the xi and eta passes stay in the k-plane, and a warp holds two whole planes
   // 3x3x3 filter with weights (1/4,1/2,1/4) through convertIJK (mod_entropy_viscosity.f90:102-120):
   // the weights and the index map are separable, so it runs as three 3-point passes (xi, eta,
   // zeta) through shared memory, 9 reads per node instead of 27
@@ -334,7 +350,7 @@ __device__ __forceinline__ void visc_dt_elem(const ViscArgs& a, int e, int d, do
   const int kx[3] = {nb_filter(k - 1), k, nb_filter(k + 1)};
   const double w[3] = {0.25, 0.5, 0.25};
   fl[d] = w[0] * ml[ix[0] + 4 * j + 16 * k] + w[1] * ml[d] + w[2] * ml[ix[2] + 4 * j + 16 * k];
-  __syncthreads();
+  __syncwarp();
   // ml's first-pass reads all happened before the barrier above, so it takes the second pass
   ml[d] = w[0] * fl[i + 4 * jx[0] + 16 * k] + w[1] * fl[d] + w[2] * fl[i + 4 * jx[2] + 16 * k];
   __syncthreads();
@@ -343,8 +359,8 @@ __device__ __forceinline__ void visc_dt_elem(const ViscArgs& a, int e, int d, do
     a.mue[(size_t)e * NN + d] = acc;
     if (a.mue32) a.mue32[(size_t)e * NN + d] = (float)acc;
     // next dt: order-independent min over elements on the bit pattern of a positive double
-    if (a.dt_out && d == 0)
-      atomicMin(reinterpret_cast<unsigned long long*>(a.dt_bits) + mem,
+    if (elem_atomic && a.dt_out && d == 0)
+      atomicMin(reinterpret_cast<unsigned long long*>(a.dt_bits) + (a.elem_member ? a.elem_member[ee] : 0),
                 (unsigned long long)__double_as_longlong(elem_s[1]));
   }
 }
