@@ -373,21 +373,25 @@ __global__ void __launch_bounds__(256, SOD_KG_MIN_BLOCKS) k_gather_rk(const Gath
 }
 
 #ifndef SOD_KV_MIN_BLOCKS
-#define SOD_KV_MIN_BLOCKS 6  // resident blocks per SM the register budget must allow (6: 40 registers, measured 1% faster than 8)
+#define SOD_KV_MIN_BLOCKS 3  // resident blocks per SM the register budget must allow
 #endif
-__global__ void __launch_bounds__(64 * KV_EPB, SOD_KV_MIN_BLOCKS) k_visc_dt(const ViscArgs a) {
-  __shared__ double sm[KV_EPB][KV_SMEM];
-  const int es = threadIdx.x >> 6;
-  // one mesh: one dt atomic per block on the minimum of its elements' limits (read after the
-  // element bodies' barriers), instead of one per element on the same address
+__global__ void __launch_bounds__(32 * KV_WARPS, SOD_KV_MIN_BLOCKS) k_visc_dt(const ViscArgs a) {
+  __shared__ double sm[KV_WARPS][KV_WSMEM];
+  __shared__ unsigned long long lim[KV_WARPS];
+  const int wb = threadIdx.x >> 5, e = blockIdx.x * KV_WARPS + wb;
+  // one mesh: one dt atomic per block on the minimum of its elements' limits, instead of one per
+  // element on the same address; an ensemble's elements take their member's slot each
   const bool per_elem = a.elem_member != nullptr;
-  visc_dt_elem(a, blockIdx.x * KV_EPB + es, threadIdx.x & 63, sm[es], per_elem);
-  if (!per_elem && a.dt_out && threadIdx.x == 0) {
-    unsigned long long b = (unsigned long long)__double_as_longlong(sm[0][KV_DT_SLOT]);
+  unsigned long long b = ~0ull;
+  if (e < a.nelem) b = visc_dt_warp(a, e, threadIdx.x & 31, sm[wb], per_elem);
+  if (!per_elem && a.dt_out) {
+    if ((threadIdx.x & 31) == 0) lim[wb] = b;
+    __syncthreads();
+    if (threadIdx.x == 0) {
 #pragma unroll
-    for (int q = 1; q < KV_EPB; ++q)
-      if (blockIdx.x * KV_EPB + q < a.nelem) b = min(b, (unsigned long long)__double_as_longlong(sm[q][KV_DT_SLOT]));
-    atomicMin(reinterpret_cast<unsigned long long*>(a.dt_bits), b);
+      for (int q = 1; q < KV_WARPS; ++q) b = min(b, lim[q]);
+      if (b != ~0ull) atomicMin(reinterpret_cast<unsigned long long*>(a.dt_bits), b);
+    }
   }
 }
 
@@ -622,8 +626,8 @@ int launch_visc_dt(SodMesh* m, const SodState* s, double* dt_out, float* mue32, 
   const ViscArgs v = make_visc_args(m, s, dt_out, mue32);
   const int nm = m->nmember > 0 ? m->nmember : 1;
   if (dt_out) SOD_CUDA(cudaMemsetAsync(v.dt_bits, 0x7F, sizeof(double) * nm, st));  // 1.38e306 each
-  const int grid = (m->nelem + KV_EPB - 1) / KV_EPB;
-  k_visc_dt<<<grid, 64 * KV_EPB, 0, st>>>(v);
+  const int grid = (m->nelem + KV_WARPS - 1) / KV_WARPS;
+  k_visc_dt<<<grid, 32 * KV_WARPS, 0, st>>>(v);
   SOD_CHECK_LAUNCH();
   if (dt_out) SOD_CUDA(cudaMemcpyAsync(dt_out, v.dt_bits, sizeof(double) * nm, cudaMemcpyDeviceToDevice, st));
   return SOD_OK;

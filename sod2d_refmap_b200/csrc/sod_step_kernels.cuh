@@ -253,7 +253,7 @@ __device__ __forceinline__ int nb_filter(int x) {
   return (x < 0) ? 1 : ((x > 3) ? 1 : x);
 }
 
-constexpr int KV_EPB = 4;
+constexpr int KV_WARPS = 8;   // elements (one warp each) per block of the stand-alone KV kernel
 
 // Exact maximum of a double over the warp with two 32-bit integer reductions instead of ten
 // shuffles: the bit pattern is mapped to an unsigned key of the same order (sign bit flipped for
@@ -271,98 +271,112 @@ __device__ __forceinline__ double warp_max_f64(double v) {
   return __hiloint2double((int)(mh ^ (back | 0x80000000u)), (int)(ml ^ back));
 }
 
-// 8-byte asynchronous global -> shared copy (L1-allocating), completed by cp.async.wait_all
-__device__ __forceinline__ void cp_async8(double* sdst, const double* gsrc) {
-  const unsigned sa = (unsigned)__cvta_generic_to_shared(sdst);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gsrc) : "memory");
+// The larger of two doubles in the key order of warp_max_f64, so that the maximum over a lane's
+// two nodes and then over the warp is the one warp_max_f64 gives over all 64 values.
+__device__ __forceinline__ double max2_f64(double x, double y) {
+  const long long bx = __double_as_longlong(x), by = __double_as_longlong(y);
+  const unsigned long long kx = (unsigned long long)bx ^ ((unsigned long long)(bx >> 63) | 0x8000000000000000ull);
+  const unsigned long long ky = (unsigned long long)by ^ ((unsigned long long)(by >> 63) | 0x8000000000000000ull);
+  return kx >= ky ? x : y;
 }
 
-// One element per 64 threads (d = the element node); sm holds the element's KV_SMEM doubles of
-// shared memory: ml[64], fl[64] (filter passes), wm[2][5] (per-warp maxima), elem_s[4] (ced, the
-// element's dt limit, and the prefetched jratio and entropy norm).  Every thread of the block
-// calls it (it holds block barriers).  elem_atomic: the element's own dt atomic; a caller that
-// passes false reduces the limits elem_s[1] of its elements itself after the call.
-constexpr int KV_SMEM = 2 * NN + 10 + 4;
-constexpr int KV_DT_SLOT = 2 * NN + 10 + 1;   // elem_s[1] within an element's KV_SMEM doubles
-__device__ __forceinline__ void visc_dt_elem(const ViscArgs& a, int e, int d, double* sm, bool elem_atomic = true) {
+// One element per warp: lane l holds the element nodes d = l and d = l + 32 (k-planes 0-1 and
+// 2-3 of d = i + 4j + 16k).  The element maxima are warp reductions, so the element scalars
+// (shock sensor, cap, CFL limits) come out warp-uniform on every lane with no shared memory and
+// no block barrier; only the filter goes through sm (KV_WSMEM doubles: ml[64], fl[64]) with warp
+// barriers.  Returns the bit pattern of the element's dt limit (every lane); with elem_atomic
+// lane 0 also takes the atomic minimum into the element's dt slot itself.
+constexpr int KV_WSMEM = 2 * NN;
+__device__ __forceinline__ unsigned long long visc_dt_warp(const ViscArgs& a, int e, int l, double* sm,
+                                                           bool elem_atomic) {
   double* ml = sm;
   double* fl = sm + NN;
-  double* wm = sm + 2 * NN;          // [warp][5]
-  double* elem_s = sm + 2 * NN + 10;
-  const bool act = e < a.nelem;
-  const int ee = act ? e : a.nelem - 1;
-  const int n = a.econn[(size_t)ee * NN + d];
-  const double rho = a.rho[n], u0 = a.u0[n], u1 = a.u1[n], u2 = a.u2[n], cs = a.csound[n], T = a.Tem[n];
-  // inputs of the second half, loaded before the element reductions so their latency overlaps them
-  const double reta_n = a.Reta[n];
-  const double hl = a.helem_l[(size_t)ee * NN + d];
-  // the element scalars read after the barriers (jratio by the element's scalar thread, the
-  // entropy norm by all) go to shared memory asynchronously, off the path behind the barriers
-  if (d == 0) {
-    cp_async8(elem_s + 2, a.jratio + ee);
-    cp_async8(elem_s + 3, a.elem_member ? a.member_scal + 2 * a.elem_member[ee] + 1 : a.scal + 1);
-    asm volatile("cp.async.commit_group;\n" ::: "memory");
+  const size_t eb = (size_t)e * NN;
+  int nd[2];
+#pragma unroll
+  for (int h = 0; h < 2; ++h) nd[h] = a.econn[eb + l + 32 * h];
+  // element scalars, warp-uniform loads issued with the node gathers
+  const double he = a.helem[e];
+  const double jr = a.jratio[e];
+  const int mem = a.elem_member ? a.elem_member[e] : 0;
+  const double norm = a.elem_member ? a.member_scal[2 * mem + 1] : a.scal[1];
+  // every node input of both nodes before any arithmetic
+  double rho[2], u0[2], u1[2], u2[2], cs[2], T[2], reta[2], hl[2], msg[2], muf[2];
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const int n = nd[h];
+    rho[h] = a.rho[n]; u0[h] = a.u0[n]; u1[h] = a.u1[n]; u2[h] = a.u2[n];
+    cs[h] = a.csound[n]; T[h] = a.Tem[n]; reta[h] = a.Reta[n]; muf[h] = a.mu_fluid[n];
+    hl[h] = a.helem_l[eb + l + 32 * h];
+    msg[h] = a.musgs ? a.musgs[eb + l + 32 * h] : 0.0;
   }
-  const double vmag = sqrt(u0 * u0 + u1 * u1 + u2 * u2);
-  const double he = a.helem[ee];
-  // betae node term (mod_entropy_viscosity.f90:90-95)
-  const double beta_n = (rho * he) * (a.prm.cmax / (double)P) * (vmag + sqrt(a.prm.Rgas * a.prm.gamma * T));
-  // CFL node terms (mod_time_ops.f90:36-50)
-  const double umax = fmax(fmax(fabs(u0), fabs(u1)), fabs(u2));
-  const double L3n = umax + cs;
-  const double musgs = a.musgs ? a.musgs[(size_t)ee * NN + d] : 0.0;
-  const double mun = (rho * musgs + a.mu_fluid[n]) / rho;
-  // element maxima over the 64 nodes (two warps per element)
-  double mV = warp_max_f64(vmag), mC = warp_max_f64(cs), mB = warp_max_f64(beta_n);
-  double mL = warp_max_f64(L3n), mM = warp_max_f64(mun);
-  const int wi = d >> 5;
-  if ((d & 31) == 0) { wm[5 * wi + 0] = mV; wm[5 * wi + 1] = mC; wm[5 * wi + 2] = mB; wm[5 * wi + 3] = mL; wm[5 * wi + 4] = mM; }
-  if (d == 0) asm volatile("cp.async.wait_all;\n" ::: "memory");
-  __syncthreads();
-  if (d == 0) {
-    // shock sensor and cap, once per element (mod_entropy_viscosity.f90:81-84); M**15 as an
-    // integer power like the reference
-    const double M = fmax(wm[0], wm[5]) / fmax(wm[1], wm[6]);
-    const double M2 = M * M, M4 = M2 * M2, M8 = M4 * M4;
-    const double M15 = M8 * M4 * M2 * M;
-    const double ceM = fmax(tanh(M15 * 3.141592653589793), a.prm.ce);
-    double ced = fmax(1.0 - elem_s[2], a.prm.ce);
-    elem_s[0] = fmax(ced, ceM);
-    const double hh = he / (double)(2.0 * P + 1);
-    const double L3 = fmax(wm[3], wm[8]);
-    const double maxMU = fmax(wm[4], wm[9]);
-    elem_s[1] = fmin(a.prm.cfl_conv * hh / L3, a.prm.cfl_diff * (hh * hh) / maxMU);
+  double vmag[2], beta[2], L3n[2], mun[2], r1[2];
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    vmag[h] = sqrt(u0[h] * u0[h] + u1[h] * u1[h] + u2[h] * u2[h]);
+    // betae node term (mod_entropy_viscosity.f90:90-95)
+    beta[h] = (rho[h] * he) * (a.prm.cmax / (double)P) * (vmag[h] + sqrt(a.prm.Rgas * a.prm.gamma * T[h]));
+    // CFL node terms (mod_time_ops.f90:36-50)
+    const double umax = fmax(fmax(fabs(u0[h]), fabs(u1[h])), fabs(u2[h]));
+    L3n[h] = umax + cs[h];
+    mun[h] = (rho[h] * msg[h] + muf[h]) / rho[h];
+    r1[h] = rho[h] * fabs(reta[h]);
   }
-  __syncthreads();
-  const double ced = elem_s[0];
-  mB = fmax(wm[2], wm[7]);
-  const double norm = elem_s[3];
-  const double R1 = (norm > 0.0) ? rho * fabs(reta_n) / norm : 0.0;
-  const double Ve = ced * R1 * hl * hl;
-  ml[d] = a.prm.cglob * fmin(Ve, mB);
-  __syncwarp();   // the xi and eta passes stay in the k-plane, and a warp holds two whole planes
+  // element maxima over the 64 nodes
+  const double mV = warp_max_f64(max2_f64(vmag[0], vmag[1]));
+  const double mC = warp_max_f64(max2_f64(cs[0], cs[1]));
+  const double mB = warp_max_f64(max2_f64(beta[0], beta[1]));
+  const double L3 = warp_max_f64(max2_f64(L3n[0], L3n[1]));
+  const double maxMU = warp_max_f64(max2_f64(mun[0], mun[1]));
+  // shock sensor and cap (mod_entropy_viscosity.f90:81-84); M**15 as an integer power like the
+  // reference
+  const double M = mV / mC;
+  const double M2 = M * M, M4 = M2 * M2, M8 = M4 * M4;
+  const double M15 = M8 * M4 * M2 * M;
+  const double ceM = fmax(tanh(M15 * 3.141592653589793), a.prm.ce);
+  const double ced = fmax(fmax(1.0 - jr, a.prm.ce), ceM);
+  const double hh = he / (double)(2.0 * P + 1);
+  const double limit = fmin(a.prm.cfl_conv * hh / L3, a.prm.cfl_diff * (hh * hh) / maxMU);
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const double R1 = (norm > 0.0) ? r1[h] / norm : 0.0;
+    const double Ve = ced * R1 * hl[h] * hl[h];
+    ml[l + 32 * h] = a.prm.cglob * fmin(Ve, mB);
+  }
+  __syncwarp();
   // 3x3x3 filter with weights (1/4,1/2,1/4) through convertIJK (mod_entropy_viscosity.f90:102-120):
   // the weights and the index map are separable, so it runs as three 3-point passes (xi, eta,
   // zeta) through shared memory, 9 reads per node instead of 27
-  const int i = d & 3, j = (d >> 2) & 3, k = d >> 4;
+  const int i = l & 3, j = (l >> 2) & 3;
   const int ix[3] = {nb_filter(i - 1), i, nb_filter(i + 1)};
   const int jx[3] = {nb_filter(j - 1), j, nb_filter(j + 1)};
-  const int kx[3] = {nb_filter(k - 1), k, nb_filter(k + 1)};
   const double w[3] = {0.25, 0.5, 0.25};
-  fl[d] = w[0] * ml[ix[0] + 4 * j + 16 * k] + w[1] * ml[d] + w[2] * ml[ix[2] + 4 * j + 16 * k];
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const int k = (l >> 4) + 2 * h, d = l + 32 * h;
+    fl[d] = w[0] * ml[ix[0] + 4 * j + 16 * k] + w[1] * ml[d] + w[2] * ml[ix[2] + 4 * j + 16 * k];
+  }
   __syncwarp();
   // ml's first-pass reads all happened before the barrier above, so it takes the second pass
-  ml[d] = w[0] * fl[i + 4 * jx[0] + 16 * k] + w[1] * fl[d] + w[2] * fl[i + 4 * jx[2] + 16 * k];
-  __syncthreads();
-  const double acc = w[0] * ml[i + 4 * j + 16 * kx[0]] + w[1] * ml[d] + w[2] * ml[i + 4 * j + 16 * kx[2]];
-  if (act) {
-    a.mue[(size_t)e * NN + d] = acc;
-    if (a.mue32) a.mue32[(size_t)e * NN + d] = (float)acc;
-    // next dt: order-independent min over elements on the bit pattern of a positive double
-    if (elem_atomic && a.dt_out && d == 0)
-      atomicMin(reinterpret_cast<unsigned long long*>(a.dt_bits) + (a.elem_member ? a.elem_member[ee] : 0),
-                (unsigned long long)__double_as_longlong(elem_s[1]));
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const int k = (l >> 4) + 2 * h, d = l + 32 * h;
+    ml[d] = w[0] * fl[i + 4 * jx[0] + 16 * k] + w[1] * fl[d] + w[2] * fl[i + 4 * jx[2] + 16 * k];
   }
+  __syncwarp();
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const int k = (l >> 4) + 2 * h, d = l + 32 * h;
+    const int kx[3] = {nb_filter(k - 1), k, nb_filter(k + 1)};
+    const double acc = w[0] * ml[i + 4 * j + 16 * kx[0]] + w[1] * ml[d] + w[2] * ml[i + 4 * j + 16 * kx[2]];
+    a.mue[eb + d] = acc;
+    if (a.mue32) a.mue32[eb + d] = (float)acc;
+  }
+  __syncwarp();   // the filter's reads are done before a caller reuses sm
+  // next dt: order-independent min over elements on the bit pattern of a positive double
+  const unsigned long long bits = (unsigned long long)__double_as_longlong(limit);
+  if (elem_atomic && a.dt_out && l == 0) atomicMin(reinterpret_cast<unsigned long long*>(a.dt_bits) + mem, bits);
+  return bits;
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -439,13 +453,12 @@ __device__ __forceinline__ void persist_stage_tail(const StageArgs& p, unsigned 
     }
     grid.sync();
   }
-  // entropy viscosity and the CFL limits, EPB elements per block at a time
-  double* sm = reinterpret_cast<double*>(smem_raw) + (threadIdx.x >> 6) * KV_SMEM;
-  const int ntiles = (p.v.nelem + EPB - 1) / EPB;
-  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
-    visc_dt_elem(p.v, t * EPB + (threadIdx.x >> 6), threadIdx.x & 63, sm);
-    __syncthreads();
-  }
+  // entropy viscosity and the CFL limits, one element per warp (2 EPB per block) at a time; the
+  // RHS tile's shared memory (at least 2 KB per 64 threads) holds each warp's KV_WSMEM doubles
+  const int wb = threadIdx.x >> 5, nw = 2 * EPB;
+  double* sm = reinterpret_cast<double*>(smem_raw) + wb * KV_WSMEM;
+  for (int e = blockIdx.x * nw + wb; e < p.v.nelem; e += gridDim.x * nw)
+    visc_dt_warp(p.v, e, threadIdx.x & 31, sm, true);
 }
 
 }  // namespace sod
