@@ -353,15 +353,19 @@ __global__ void __launch_bounds__(64 * EPB) k_stage_fused(const StageArgs p) {
   persist_stage_tail<double, EPB>(p, smem_raw);
 }
 
+// resident 256-thread blocks per SM the register budget must allow.  FP32 residual rows (mixed
+// path): 4 blocks, 64 registers, no spill with the predicated groups of 4, 2% faster than full
+// groups at 5 blocks (the predicated groups at 5 blocks spilled 76 bytes and ran 4% slower
+// than that).  FP64 rows: 5 blocks, 48 registers (48-72 bytes of spill), 1% faster than 4
+// blocks; 7 blocks capped the kernel at 32 registers and spilled 140-244 bytes
 #ifndef SOD_KG_MIN_BLOCKS
-// resident 256-thread blocks per SM the register budget must allow: 5 leaves 48 registers (the
-// FP32-accumulator stages spill 24 bytes, the FP64 ones 48-72) and measured 4% (mixed) / 1%
-// (FP64) faster than 4 blocks at 64 registers; 7 blocks capped the kernel at 32 registers and
-// spilled 140-244 bytes per thread
-#define SOD_KG_MIN_BLOCKS 5
+#define SOD_KG_MIN_BLOCKS 4
+#endif
+#ifndef SOD_KG_MIN_BLOCKS_F64
+#define SOD_KG_MIN_BLOCKS_F64 5
 #endif
 template <typename R, int STAGE>
-__global__ void __launch_bounds__(256, SOD_KG_MIN_BLOCKS) k_gather_rk(const GatherArgs a) {
+__global__ void __launch_bounds__(256, sizeof(R) == 4 ? SOD_KG_MIN_BLOCKS : SOD_KG_MIN_BLOCKS_F64) k_gather_rk(const GatherArgs a) {
   const int n = blockIdx.x * blockDim.x + threadIdx.x;
   double eta_n = 0.0;
   const bool act = gather_rk_node<R, STAGE>(a, n, eta_n);
@@ -373,7 +377,7 @@ __global__ void __launch_bounds__(256, SOD_KG_MIN_BLOCKS) k_gather_rk(const Gath
 }
 
 #ifndef SOD_KV_MIN_BLOCKS
-#define SOD_KV_MIN_BLOCKS 3  // resident blocks per SM the register budget must allow
+#define SOD_KV_MIN_BLOCKS 3  // resident 256-thread blocks per SM: 80 registers, no spill (4 blocks: 64 registers with spills, the same time)
 #endif
 __global__ void __launch_bounds__(32 * KV_WARPS, SOD_KV_MIN_BLOCKS) k_visc_dt(const ViscArgs a) {
   __shared__ double sm[KV_WARPS][KV_WSMEM];

@@ -86,32 +86,52 @@ __device__ __forceinline__ bool gather_rk_node(const GatherArgs& a, int n, doubl
     R* rsum = reinterpret_cast<R*>(a.rsum);
     const size_t N = (size_t)a.npoin;
     // node data independent of the gather, loaded first so their latency overlaps it
-    double yv[5], rsv[6];
+    double yv[5];
+    R rsv[6];      // the accumulators at their stored precision (widened exactly where used)
     if constexpr (STAGE >= 1) {
 #pragma unroll
       for (int f = 0; f < 5; ++f) yv[f] = a.y[f][n];
 #pragma unroll
-      for (int f = 0; f < 6; ++f) rsv[f] = STAGE == 1 ? 0.0 : (double)rsum[f * N + n];
+      for (int f = 0; f < 6; ++f) rsv[f] = STAGE == 1 ? (R)0 : rsum[f * N + n];
     }
     const double ml = a.Ml[n];
     double r[6] = {0, 0, 0, 0, 0, 0};
     const int beg = a.ptr[n], end = a.ptr[n + 1];
     int c = beg;
-    // groups of 4 contributions: all loads issued before the (ascending, fixed-order) sums
-    for (; c + 4 <= end; c += 4) {
-      R v[4][6];
+    if constexpr (sizeof(R) == 4) {
+      // groups of up to 4 contributions (a partial group's missing ones predicated off): all
+      // loads of a group issued before its (ascending, fixed-order) sums, so a node with 1-4
+      // contributions waits on one chain of index -> residual loads
+      for (; c < end; c += 4) {
+        R v[4][6];
 #pragma unroll
-      for (int q = 0; q < 4; ++q) load_res6<R>(rel, (size_t)a.idx[c + q], v[q]);
+        for (int q = 0; q < 4; ++q)
+          if (c + q < end) load_res6<R>(rel, (size_t)a.idx[c + q], v[q]);
 #pragma unroll
-      for (int q = 0; q < 4; ++q)
+        for (int q = 0; q < 4; ++q)
+          if (c + q < end) {
 #pragma unroll
-        for (int f = 0; f < 6; ++f) r[f] += (double)v[q][f];
-    }
-    for (; c < end; ++c) {
-      R v[6];
-      load_res6<R>(rel, (size_t)a.idx[c], v);
+            for (int f = 0; f < 6; ++f) r[f] += (double)v[q][f];
+          }
+      }
+    } else {
+      // FP64 residual rows: full groups of 4, then one at a time (a predicated group's 24
+      // doubles do not fit the register budget)
+      for (; c + 4 <= end; c += 4) {
+        R v[4][6];
 #pragma unroll
-      for (int f = 0; f < 6; ++f) r[f] += (double)v[f];
+        for (int q = 0; q < 4; ++q) load_res6<R>(rel, (size_t)a.idx[c + q], v[q]);
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+#pragma unroll
+          for (int f = 0; f < 6; ++f) r[f] += (double)v[q][f];
+      }
+      for (; c < end; ++c) {
+        R v[6];
+        load_res6<R>(rel, (size_t)a.idx[c], v);
+#pragma unroll
+        for (int f = 0; f < 6; ++f) r[f] += (double)v[f];
+      }
     }
     if (a.src) {
       // mom_source_const_vect (elem_source.f90:20-55): - sum_e gpvol s = - Ml s on the momentum
@@ -133,7 +153,7 @@ __device__ __forceinline__ bool gather_rk_node(const GatherArgs& a, int n, doubl
       const double dt = a.node_member ? a.dt[a.node_member[n]] : *a.dt;
       double rs[6];
 #pragma unroll
-      for (int f = 0; f < 6; ++f) rs[f] = rsv[f] + a.b_cur * r[f];
+      for (int f = 0; f < 6; ++f) rs[f] = (double)rsv[f] + a.b_cur * r[f];
       if constexpr (STAGE < 4) {
 #pragma unroll
         for (int f = 0; f < 6; ++f) rsum[f * N + n] = (R)rs[f];
